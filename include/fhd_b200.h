@@ -1,0 +1,287 @@
+/*
+ * fhd_b200.h -- C ABI of the B200 (sm_100a) staggered-grid Stokes solver and
+ * stochastic flux library.
+ *
+ * The entry points replace, one for one, the hot-path routines of LowMachFHD
+ * (staggered_grid/src_gmres, src_lowMach).  Every declaration cites the
+ * reference routine it stands in for.  Two families exist:
+ *
+ *   fhd_dev_*  : operands are DEVICE pointers in the canonical layout below.
+ *                This is what device-resident callers (the time integrator,
+ *                batched and served solves) use.
+ *   fhd_*      : operands are HOST BoxLib fabs (Fortran column-major with
+ *                ghost cells, duplicated periodic faces).  This is the
+ *                drop-in boundary a Fortran driver binds through
+ *                iso_c_binding: same argument meaning as the reference.
+ *
+ * Canonical device layout (periodic domain, one box):
+ *   n = (nx, ny, nz) cells, nz = 1 in 2D; Nc = nx*ny*nz.
+ *   cell (i,j,k)  -> offset i + nx*(j + ny*k)
+ *   face array of direction d: Nc entries, entry (i,j,k) is the face on the
+ *       low-d side of cell (i,j,k) (periodic faces stored once).
+ *   2D node array: entry (i,j) is the node at the low-x, low-y corner.
+ *   3D edge arrays, order xy, xz, yz: entry (i,j,k) of the xy array is the
+ *       edge at the low-x, low-y corner, centred in z (likewise xz, yz).
+ * All arrays are FP64 at the boundary.
+ *
+ * Status codes: 0 = success, > 0 = warning (result usable), < 0 = error.
+ */
+#ifndef FHD_B200_H
+#define FHD_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ */
+/* status codes                                                        */
+/* ------------------------------------------------------------------ */
+#define FHD_OK                          0
+#define FHD_WARN_NOT_CONVERGED_MAXITER  1  /* gmres.f90:268-274 */
+#define FHD_WARN_NOT_CONVERGED_OUTER    2  /* gmres.f90:305-310 */
+#define FHD_WARN_TRUE_RESID             3  /* gmres.f90:286-289 */
+#define FHD_ERR_BAD_ARG                -1
+#define FHD_ERR_BAD_GHOSTS             -2  /* apply_matrix.f90:54-68 */
+#define FHD_ERR_DX_NOT_ISOTROPIC       -3  /* stag_applyop.f90:118-128 */
+#define FHD_ERR_ORTHO_BREAKDOWN        -4  /* gmres.f90:391 */
+#define FHD_ERR_UNSUPPORTED            -5  /* apply_precon.f90:426 */
+#define FHD_ERR_NONFINITE              -6
+#define FHD_ERR_OOM                    -7
+#define FHD_ERR_CUDA                   -8
+#define FHD_ERR_NO_DEVICE              -9
+
+/* precision modes of a context */
+#define FHD_PREC_FP64   0  /* everything in FP64 */
+#define FHD_PREC_MIXED  1  /* FP32 multigrid preconditioner and stochastic
+                              fluxes; FP64 outer residual, Arnoldi/Givens,
+                              mean-zero projection */
+
+/* ------------------------------------------------------------------ */
+/* parameters: mirror of namelist probin_gmres (probin_gmres.f90:12-163)*/
+/* ------------------------------------------------------------------ */
+typedef struct fhd_gmres_params {
+    int    precon_type;            /* 1..5 and negatives */
+    int    visc_schur_approx;      /* only 0 is supported */
+    double p_norm_weight;
+    double scale_factor;
+    int    mg_verbose, cg_verbose;
+    int    mg_max_vcycles, mg_minwidth, mg_bottom_solver;
+    int    mg_nsmooths_down, mg_nsmooths_up, mg_nsmooths_bottom;
+    int    mg_max_bottom_nlevels;
+    double mg_rel_tol, mg_abs_tol;
+    int    stag_mg_verbosity, stag_mg_max_vcycles, stag_mg_minwidth;
+    int    stag_mg_bottom_solver;
+    int    stag_mg_nsmooths_down, stag_mg_nsmooths_up, stag_mg_nsmooths_bottom;
+    int    stag_mg_max_bottom_nlevels;
+    double stag_mg_omega;
+    int    stag_mg_smoother;       /* 0 = Jacobi, 1 = 2*dim-colour Gauss-Seidel */
+    double stag_mg_rel_tol;
+    double gmres_rel_tol, gmres_abs_tol;
+    int    gmres_verbose, gmres_max_outer, gmres_max_inner;
+    int    gmres_max_iter, gmres_min_iter;
+    int    gmres_spatial_order;    /* only 2 is supported */
+} fhd_gmres_params;
+
+/* Fills the defaults of probin_gmres_init (probin_gmres.f90:122-163). */
+void fhd_gmres_params_default(fhd_gmres_params* p);
+
+/* Stochastic momentum flux parameters (probin_common: k_B,
+ * variance_coef_mom, stoch_stress_form, filtering_width;
+ * stochastic_m_fluxdiv.f90:137).  dV is the cell volume product(dx)
+ * (in 2D: dx*dy*cell_depth). */
+typedef struct fhd_stoch_params {
+    double k_B;
+    double variance_coef_mom;
+    double dV;
+    int    stoch_stress_form;      /* 0 non-symmetric, 1 symmetric */
+    int    filtering_width;        /* only 0 is supported */
+} fhd_stoch_params;
+
+/* Per-solve diagnostics (gmres.f90:72-85 locals, vcycle_counter.f90). */
+typedef struct fhd_solve_stats {
+    int    outer_iters;            /* gmres 'iter' */
+    int    total_iters;            /* gmres 'total_iter' */
+    int    vcycles;                /* vcycle_counter */
+    int    status;
+    double norm_b, norm_pre_b, norm_init_resid, norm_resid;
+    double norm_resid_Stokes, norm_init_Stokes, norm_resid_est;
+} fhd_solve_stats;
+
+/* ------------------------------------------------------------------ */
+/* context                                                             */
+/* ------------------------------------------------------------------ */
+typedef struct fhd_ctx fhd_ctx;
+
+/* Builds the solver for one periodic box: multigrid hierarchy
+ * (stag_mg_layout_build + compute_nlevs_mg, stag_mg_layout.f90:21-222;
+ * mgt_macproj_precon_build, macproject.f90:364-421), Krylov storage and a
+ * CUDA stream.  dim = 2 or 3; dx must be equal in all directions
+ * (stag_applyop.f90:118-128).  visc_type in {-3,-2,-1,1,2,3}
+ * (probin_common visc_type). */
+int  fhd_ctx_create(int dim, const int n_cells[3], const double dx[3],
+                    int visc_type, const fhd_gmres_params* params,
+                    int precision_mode, fhd_ctx** out);
+int  fhd_ctx_destroy(fhd_ctx* ctx);
+/* CUDA stream (cudaStream_t) the context launches on; may be set by the
+ * caller before any call (NULL = the context's own stream). */
+void* fhd_ctx_stream(fhd_ctx* ctx);
+int  fhd_ctx_set_stream(fhd_ctx* ctx, void* stream);
+/* Number of this library's kernels launched through ctx so far. */
+long long fhd_ctx_kernel_launches(fhd_ctx* ctx);
+const char* fhd_status_string(int status);
+
+/* ------------------------------------------------------------------ */
+/* device-pointer entry points (canonical layout)                      */
+/* u-type arguments are arrays of dim device pointers to face arrays;  */
+/* beta_ed has 1 (2D node) or 3 (3D edge) device pointers.             */
+/* ------------------------------------------------------------------ */
+
+/* apply_matrix (apply_matrix.f90:24-157):
+ *   b_u = theta_alpha*alpha_fc*x_u - L x_u + G x_p ;  b_p = -D x_u */
+int fhd_dev_apply_matrix(fhd_ctx* ctx,
+                         double* const b_u[], double* b_p,
+                         const double* const x_u[], const double* x_p,
+                         const double* const alpha_fc[], const double* beta,
+                         const double* const beta_ed[], const double* gamma,
+                         double theta_alpha);
+
+/* apply_precon (apply_precon.f90:29-475): x = M^{-1} b for precon_type
+ * 1..5 (visc_schur_approx = 0), including the null-space mean removal. */
+int fhd_dev_apply_precon(fhd_ctx* ctx,
+                         const double* const b_u[], const double* b_p,
+                         double* const x_u[], double* x_p,
+                         const double* const alpha_fc[], const double* beta,
+                         const double* const beta_ed[], const double* gamma,
+                         double theta_alpha);
+
+/* stag_mg_solver (stag_mg_solver.f90:37-863): V-cycles on
+ * (theta_alpha*alpha - L) phi = rhs; phi is the initial guess on entry. */
+int fhd_dev_stag_mg_solver(fhd_ctx* ctx,
+                           const double* const alpha_fc[], const double* beta,
+                           const double* const beta_ed[], const double* gamma,
+                           double theta_alpha,
+                           double* const phi[], const double* const rhs[]);
+
+/* gmres (gmres.f90:32-491): restarted left-preconditioned GMRES on the
+ * saddle-point system.  x_u, x_p: initial guess in, solution out.
+ * norm_pre_rhs (nullable) receives |M^{-1} b|. */
+int fhd_dev_gmres(fhd_ctx* ctx,
+                  const double* const b_u[], const double* b_p,
+                  double* const x_u[], double* x_p,
+                  const double* const alpha_fc[], const double* beta,
+                  const double* const beta_ed[], const double* gamma,
+                  double theta_alpha, double* norm_pre_rhs,
+                  fhd_solve_stats* stats);
+
+/* stochastic_m_fluxdiv (stochastic_m_fluxdiv.f90:42-602), periodic box:
+ *   force (+)= div( sqrt(variance_coef_mom*2 k_B/(dV dt)) * sqrt(eta T) *
+ *                   sum_r weights[r] W_r )
+ * W_cc: n_rngs*dim cell arrays (rng r, component c at index r*dim+c).
+ * W_ed: 2D: n_rngs*2 node arrays (index r*2+comp); 3D: n_rngs*6 edge arrays
+ *       (index r*6 + 2*edge_set + comp, edge sets xy, xz, yz).
+ * The random arrays follow fill_m_stochastic (stochastic_m_fluxdiv.f90:
+ * 781-860): for the symmetric form the cell entries carry variance 2 and
+ * comp 1 of every edge entry equals comp 0. */
+int fhd_dev_stochastic_m_fluxdiv(fhd_ctx* ctx, const fhd_stoch_params* sp,
+                                 double* const force[], int increment,
+                                 const double* eta, const double* const eta_ed[],
+                                 const double* temperature,
+                                 const double* const temperature_ed[],
+                                 double dt, const double* weights, int n_rngs,
+                                 const double* const W_cc[],
+                                 const double* const W_ed[]);
+
+/* advance_timestep_inertial (advance_timestep_inertial.f90:45-923) for a
+ * single-species fluid (nspecies = 1, centred advection, no gravity,
+ * periodic box): the Crank-Nicolson predictor-corrector with two GMRES
+ * solves (theta_alpha = 1/dt, eta/2 and kappa/2 as in lines 467-474 and
+ * 777-784).  umac, rho, pi are advanced in place.  W_cc/W_ed hold this
+ * step's random fields as for fhd_dev_stochastic_m_fluxdiv with n_rngs = 1;
+ * predictor and corrector use the same fields, as the reference does.
+ * stats (nullable) receives the two solves' diagnostics. */
+int fhd_dev_advance_inertial(fhd_ctx* ctx, const fhd_stoch_params* sp,
+                             double dt, double* const umac[], double* rho,
+                             double* pi, const double* eta,
+                             const double* const eta_ed[], const double* kappa,
+                             const double* temperature,
+                             const double* const temperature_ed[],
+                             const double* const W_cc[],
+                             const double* const W_ed[],
+                             fhd_solve_stats* stats2);
+
+/* Text of the last CUDA error seen by the calling thread. */
+const char* fhd_last_error(void);
+/* Bytes of device memory a context holds. */
+unsigned long long fhd_ctx_device_bytes(fhd_ctx* ctx);
+
+/* ------------------------------------------------------------------ */
+/* host BoxLib-fab entry points (drop-in boundary)                     */
+/* ------------------------------------------------------------------ */
+/* One fab: data(lo(1)-ng : hi(1)+nodal(1)+ng, ..., 1:ncomp) in Fortran
+ * column-major order, lo/hi the cell-centred box, nodal[d] = 1 for a face
+ * (or node/edge) direction.  Component 0 is used. */
+typedef struct fhd_fab {
+    double* data;
+    int lo[3], hi[3];
+    int nodal[3];
+    int ng;
+    int ncomp;
+} fhd_fab;
+
+/* A single-level multifab: the boxes of the level in BoxLib order. */
+typedef struct fhd_multifab {
+    int nfabs;
+    const fhd_fab* fabs;
+} fhd_multifab;
+
+/* gmres(mla,the_bc_tower,dx,b_u,b_p,x_u,x_p,alpha_fc,beta,beta_ed,gamma,
+ *       theta_alpha,norm_pre_rhs)  (gmres.f90:32-47).
+ * x_u/x_p are read as the initial guess and overwritten with the solution
+ * in the valid region and ghost cells (periodic fill).  Ghost-cell counts
+ * are checked as apply_matrix.f90:54-68 does (x_u, x_p need >= 1). */
+int fhd_gmres(fhd_ctx* ctx,
+              const fhd_multifab* b_u, const fhd_multifab* b_p,
+              const fhd_multifab* x_u, const fhd_multifab* x_p,
+              const fhd_multifab* alpha_fc, const fhd_multifab* beta,
+              const fhd_multifab* beta_ed, const fhd_multifab* gamma,
+              double* theta_alpha, double* norm_pre_rhs,
+              fhd_solve_stats* stats);
+
+/* apply_precon(mla,b_u,b_p,x_u,x_p,alpha_fc,beta,beta_ed,gamma,
+ *              theta_alpha,dx,the_bc_tower)  (apply_precon.f90:29-43) */
+int fhd_apply_precon(fhd_ctx* ctx,
+                     const fhd_multifab* b_u, const fhd_multifab* b_p,
+                     const fhd_multifab* x_u, const fhd_multifab* x_p,
+                     const fhd_multifab* alpha_fc, const fhd_multifab* beta,
+                     const fhd_multifab* beta_ed, const fhd_multifab* gamma,
+                     double theta_alpha);
+
+/* apply_matrix(mla,b_u,b_p,x_u,x_p,alpha_fc,beta,beta_ed,gamma,
+ *              theta_alpha,dx,the_bc_tower)  (apply_matrix.f90:24-40) */
+int fhd_apply_matrix(fhd_ctx* ctx,
+                     const fhd_multifab* b_u, const fhd_multifab* b_p,
+                     const fhd_multifab* x_u, const fhd_multifab* x_p,
+                     const fhd_multifab* alpha_fc, const fhd_multifab* beta,
+                     const fhd_multifab* beta_ed, const fhd_multifab* gamma,
+                     double theta_alpha);
+
+/* stochastic_m_fluxdiv(mla,the_bc_level,stoch_m_force,increment,eta,
+ *   eta_ed,temperature,temperature_ed,dx,dt,weights)
+ *   (stochastic_m_fluxdiv.f90:42-53).  The module-global random storage
+ *   mflux_cc/mflux_nd/mflux_ed of the reference is passed explicitly:
+ *   W_cc[r] is a dim-component cell multifab, W_ed[r*nE+e] a 2-component
+ *   node (2D, nE=1) or edge (3D, nE=3) multifab. */
+int fhd_stochastic_m_fluxdiv(fhd_ctx* ctx, const fhd_stoch_params* sp,
+                             const fhd_multifab* stoch_m_force, int increment,
+                             const fhd_multifab* eta,
+                             const fhd_multifab* eta_ed,
+                             const fhd_multifab* temperature,
+                             const fhd_multifab* temperature_ed,
+                             double dt, const double* weights, int n_rngs,
+                             const fhd_multifab* W_cc,
+                             const fhd_multifab* W_ed);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FHD_B200_H */

@@ -1,0 +1,272 @@
+"""lowmachfhd_b200 -- B200 (sm_100a) implementation of LowMachFHD's implicit
+staggered-grid Stokes solve and stochastic momentum flux.
+
+Python mirror of the reference interface (staggered_grid/src_gmres and
+src_lowMach of LowMachFHD): the same routine names and argument meaning as
+gmres, apply_precon, apply_matrix, stag_mg_solver, stochastic_m_fluxdiv and
+advance_timestep_inertial.  Every call goes through the C ABI of the CUDA
+library (include/fhd_b200.h); torch tensors serve only as device memory.
+
+Device arrays are flat float64 CUDA tensors in the canonical periodic layout
+(x fastest; face arrays hold the low face of each cell; see the header).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Sequence
+
+import numpy as np
+
+from . import _capi
+from ._capi import (FHD_PREC_FP64, FHD_PREC_MIXED, Fab, FhdError, GmresParams, Multifab, SolveStats,
+                    StochParams, check, lib)
+
+__all__ = ["StokesSolver", "GmresParams", "StochParams", "SolveStats", "default_params", "FhdError",
+           "FHD_PREC_FP64", "FHD_PREC_MIXED", "lib", "fab_from_canonical", "canonical_from_fab", "FabArray"]
+
+
+def default_params(**overrides) -> GmresParams:
+    """probin_gmres defaults (probin_gmres.f90:122-163) with overrides."""
+    p = GmresParams()
+    lib().fhd_gmres_params_default(C.byref(p))
+    for k, v in overrides.items():
+        if not hasattr(p, k):
+            raise AttributeError(f"probin_gmres has no parameter {k}")
+        setattr(p, k, v)
+    return p
+
+
+_DP = C.POINTER(C.c_double)
+
+
+def _dptr(t) -> _DP:
+    """device pointer of a contiguous float64 CUDA tensor"""
+    if t is None:
+        return None
+    if not (t.is_cuda and t.dtype.itemsize == 8 and t.is_contiguous()):
+        raise TypeError("expected a contiguous float64 CUDA tensor")
+    return C.cast(C.c_void_p(t.data_ptr()), _DP)
+
+
+def _dpp(ts: Sequence) -> C.Array:
+    arr = (_DP * max(1, len(ts)))()
+    for i, t in enumerate(ts):
+        arr[i] = _dptr(t)
+    return arr
+
+
+class StokesSolver:
+    """One periodic box and its solver state (the fhd_ctx of the C ABI):
+    multigrid hierarchies (stag_mg_layout_build, mgt_macproj_precon_build),
+    Krylov storage and a CUDA stream."""
+
+    def __init__(self, dim: int, n_cells: Sequence[int], dx: float | Sequence[float], visc_type: int,
+                 params: GmresParams | None = None, precision: str = "fp64"):
+        self.dim = int(dim)
+        n = list(n_cells) + [1] * (3 - len(n_cells))
+        self.n_cells = n[:3]
+        dxs = [float(dx)] * 3 if np.isscalar(dx) else list(dx) + [float(dx[0])] * (3 - len(dx))
+        self.dx = dxs[0]
+        self.visc_type = int(visc_type)
+        self.params = params if params is not None else default_params()
+        self.precision = precision
+        mode = FHD_PREC_MIXED if precision == "mixed" else FHD_PREC_FP64
+        h = C.c_void_p()
+        st = lib().fhd_ctx_create(self.dim, (C.c_int * 3)(*self.n_cells), (C.c_double * 3)(*dxs),
+                                  self.visc_type, C.byref(self.params), mode, C.byref(h))
+        check(st, "fhd_ctx_create")
+        self._h = h
+
+    # ----------------------------------------------------------------
+    @property
+    def nc(self) -> int:
+        return int(np.prod(self.n_cells[: self.dim]))
+
+    @property
+    def nedge(self) -> int:
+        return 1 if self.dim == 2 else 3
+
+    @property
+    def kernel_launches(self) -> int:
+        return int(lib().fhd_ctx_kernel_launches(self._h))
+
+    @property
+    def device_bytes(self) -> int:
+        return int(lib().fhd_ctx_device_bytes(self._h))
+
+    @property
+    def stream(self) -> int:
+        return int(lib().fhd_ctx_stream(self._h) or 0)
+
+    def set_stream(self, stream_handle: int | None):
+        check(lib().fhd_ctx_set_stream(self._h, C.c_void_p(stream_handle or 0)), "fhd_ctx_set_stream")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().fhd_ctx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # ----------------------------------------------------------------
+    # device-pointer mirror of the reference routines
+    # ----------------------------------------------------------------
+    def apply_matrix(self, b_u, b_p, x_u, x_p, alpha_fc, beta, beta_ed, gamma, theta_alpha):
+        """apply_matrix (apply_matrix.f90:24-157): b = A x."""
+        return check(lib().fhd_dev_apply_matrix(self._h, _dpp(b_u), _dptr(b_p), _dpp(x_u), _dptr(x_p),
+                                                _dpp(alpha_fc), _dptr(beta), _dpp(beta_ed), _dptr(gamma),
+                                                float(theta_alpha)), "apply_matrix")
+
+    def apply_precon(self, b_u, b_p, x_u, x_p, alpha_fc, beta, beta_ed, gamma, theta_alpha):
+        """apply_precon (apply_precon.f90:29-475): x = M^{-1} b."""
+        return check(lib().fhd_dev_apply_precon(self._h, _dpp(b_u), _dptr(b_p), _dpp(x_u), _dptr(x_p),
+                                                _dpp(alpha_fc), _dptr(beta), _dpp(beta_ed), _dptr(gamma),
+                                                float(theta_alpha)), "apply_precon")
+
+    def stag_mg_solver(self, alpha_fc, beta_cc, beta_ed, gamma_cc, theta_alpha, phi_fc, rhs_fc):
+        """stag_mg_solver (stag_mg_solver.f90:37-863); phi_fc in/out."""
+        return check(lib().fhd_dev_stag_mg_solver(self._h, _dpp(alpha_fc), _dptr(beta_cc), _dpp(beta_ed),
+                                                  _dptr(gamma_cc), float(theta_alpha), _dpp(phi_fc),
+                                                  _dpp(rhs_fc)), "stag_mg_solver")
+
+    def gmres(self, b_u, b_p, x_u, x_p, alpha_fc, beta, beta_ed, gamma, theta_alpha):
+        """gmres (gmres.f90:32-491).  x_u/x_p: initial guess in, solution
+        out.  Returns (status, norm_pre_rhs, stats dict); status > 0 is a
+        non-convergence warning as printed by the reference."""
+        npr = C.c_double(0.0)
+        st = SolveStats()
+        status = check(lib().fhd_dev_gmres(self._h, _dpp(b_u), _dptr(b_p), _dpp(x_u), _dptr(x_p),
+                                           _dpp(alpha_fc), _dptr(beta), _dpp(beta_ed), _dptr(gamma),
+                                           float(theta_alpha), C.byref(npr), C.byref(st)), "gmres")
+        return status, npr.value, st.as_dict()
+
+    def stochastic_m_fluxdiv(self, sp: StochParams, stoch_m_force, increment, eta, eta_ed, temperature,
+                             temperature_ed, dt, weights, W_cc, W_ed):
+        """stochastic_m_fluxdiv (stochastic_m_fluxdiv.f90:42-602).
+        W_cc: n_rngs*dim cell tensors, W_ed: n_rngs*2*nE node/edge tensors."""
+        w = (C.c_double * len(weights))(*[float(x) for x in weights])
+        return check(lib().fhd_dev_stochastic_m_fluxdiv(self._h, C.byref(sp), _dpp(stoch_m_force),
+                                                        int(bool(increment)), _dptr(eta), _dpp(eta_ed),
+                                                        _dptr(temperature), _dpp(temperature_ed), float(dt),
+                                                        C.cast(w, _DP), len(weights), _dpp(W_cc), _dpp(W_ed)),
+                     "stochastic_m_fluxdiv")
+
+    def advance_timestep_inertial(self, sp: StochParams, dt, umac, rho, pi, eta, eta_ed, kappa, temperature,
+                                  temperature_ed, W_cc, W_ed):
+        """One single-species inertial step (advance_timestep_inertial.f90)
+        in place on umac, rho, pi.  Returns (status, [stats_pred, stats_corr])."""
+        st = (SolveStats * 2)()
+        status = check(lib().fhd_dev_advance_inertial(self._h, C.byref(sp), float(dt), _dpp(umac), _dptr(rho),
+                                                      _dptr(pi), _dptr(eta), _dpp(eta_ed), _dptr(kappa),
+                                                      _dptr(temperature), _dpp(temperature_ed), _dpp(W_cc),
+                                                      _dpp(W_ed), st), "advance_timestep_inertial")
+        return status, [st[0].as_dict(), st[1].as_dict()]
+
+    # ----------------------------------------------------------------
+    # host BoxLib-fab mirror (the drop-in boundary)
+    # ----------------------------------------------------------------
+    def gmres_fab(self, b_u, b_p, x_u, x_p, alpha_fc, beta, beta_ed, gamma, theta_alpha):
+        """gmres on host FabArray multifabs (lists of FabArray per multifab)."""
+        keep = []
+        mfs = [_mf_vec(v, keep) for v in (b_u,)] + [_mf(b_p, keep)] + [_mf_vec(x_u, keep)] + [_mf(x_p, keep)]
+        mfs += [_mf_vec(alpha_fc, keep), _mf(beta, keep), _mf_vec(beta_ed, keep), _mf(gamma, keep)]
+        th = C.c_double(theta_alpha)
+        npr = C.c_double(0.0)
+        st = SolveStats()
+        status = check(lib().fhd_gmres(self._h, *mfs, C.byref(th), C.byref(npr), C.byref(st)), "fhd_gmres")
+        return status, npr.value, st.as_dict()
+
+    def apply_matrix_fab(self, b_u, b_p, x_u, x_p, alpha_fc, beta, beta_ed, gamma, theta_alpha):
+        keep = []
+        mfs = [_mf_vec(b_u, keep), _mf(b_p, keep), _mf_vec(x_u, keep), _mf(x_p, keep),
+               _mf_vec(alpha_fc, keep), _mf(beta, keep), _mf_vec(beta_ed, keep), _mf(gamma, keep)]
+        return check(lib().fhd_apply_matrix(self._h, *mfs, float(theta_alpha)), "fhd_apply_matrix")
+
+    def apply_precon_fab(self, b_u, b_p, x_u, x_p, alpha_fc, beta, beta_ed, gamma, theta_alpha):
+        keep = []
+        mfs = [_mf_vec(b_u, keep), _mf(b_p, keep), _mf_vec(x_u, keep), _mf(x_p, keep),
+               _mf_vec(alpha_fc, keep), _mf(beta, keep), _mf_vec(beta_ed, keep), _mf(gamma, keep)]
+        return check(lib().fhd_apply_precon(self._h, *mfs, float(theta_alpha)), "fhd_apply_precon")
+
+
+# ----------------------------------------------------------------------
+# host fab helpers (BoxLib layout <-> canonical layout, numpy)
+# ----------------------------------------------------------------------
+class FabArray:
+    """One BoxLib fab: Fortran-ordered float64 array covering
+    lo-ng .. hi+nodal+ng in each direction (component 0)."""
+
+    def __init__(self, data: np.ndarray, lo, hi, nodal, ng: int, ncomp: int = 1):
+        self.data = data
+        self.lo, self.hi, self.nodal, self.ng, self.ncomp = list(lo), list(hi), list(nodal), int(ng), int(ncomp)
+
+    def fab(self) -> Fab:
+        f = Fab()
+        assert self.data.dtype == np.float64 and self.data.flags.f_contiguous
+        f.data = self.data.ctypes.data_as(_DP)
+        for d in range(3):
+            f.lo[d] = self.lo[d] if d < len(self.lo) else 0
+            f.hi[d] = self.hi[d] if d < len(self.hi) else 0
+            f.nodal[d] = self.nodal[d] if d < len(self.nodal) else 0
+        f.ng = self.ng
+        f.ncomp = self.ncomp
+        return f
+
+
+def _mf(fa, keep):
+    boxes = fa if isinstance(fa, (list, tuple)) else [fa]
+    arr = (Fab * len(boxes))(*[b.fab() for b in boxes])
+    keep.append(arr)
+    mf = Multifab(len(boxes), C.cast(arr, C.POINTER(Fab)))
+    keep.append(mf)
+    return C.byref(mf)
+
+
+def _mf_vec(fas, keep):
+    mfs = []
+    for fa in fas:
+        boxes = fa if isinstance(fa, (list, tuple)) else [fa]
+        arr = (Fab * len(boxes))(*[b.fab() for b in boxes])
+        keep.append(arr)
+        mfs.append(Multifab(len(boxes), C.cast(arr, C.POINTER(Fab))))
+    a = (Multifab * len(mfs))(*mfs)
+    keep.append(a)
+    return C.cast(a, C.POINTER(Multifab))
+
+
+def fab_from_canonical(x: np.ndarray, dim: int, n_cells, nodal, ng: int, lo=None, hi=None) -> FabArray:
+    """Periodic canonical array -> one fab over box lo..hi (default the
+    whole domain), ghost cells and the duplicated nodal plane filled."""
+    n = list(n_cells)[:dim]
+    lo = list(lo) if lo is not None else [0] * dim
+    hi = list(hi) if hi is not None else [k - 1 for k in n]
+    nodal = list(nodal)[:dim]
+    idx = []
+    for d in range(dim):
+        rng = np.arange(lo[d] - ng, hi[d] + nodal[d] + ng + 1)
+        idx.append(np.mod(rng, n[d]))
+    can = x.reshape([n[d] for d in reversed(range(dim))])  # (z, y, x) C order
+    if dim == 2:
+        sub = can[np.ix_(idx[1], idx[0])]
+    else:
+        sub = can[np.ix_(idx[2], idx[1], idx[0])]
+    data = np.asfortranarray(sub.T)
+    return FabArray(data, lo + [0] * (3 - dim), hi + [0] * (3 - dim), nodal + [0] * (3 - dim), ng)
+
+
+def canonical_from_fab(fa: FabArray, dim: int, n_cells) -> np.ndarray:
+    """Valid cells lo..hi of one whole-domain fab -> canonical array."""
+    n = list(n_cells)[:dim]
+    g = fa.ng
+    sl = tuple(slice(g, g + fa.hi[d] - fa.lo[d] + 1) for d in range(dim))
+    return np.ascontiguousarray(fa.data[sl].T).reshape(-1)

@@ -1,0 +1,157 @@
+"""ctypes declarations of the C ABI in include/fhd_b200.h.
+
+The product path: every call goes to the sm_100a library _fhd_b200.so built
+in this directory.  There is no fallback; a missing library raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import re
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_fhd_b200.so")
+HEADER = os.path.join(HERE, "..", "include", "fhd_b200.h")
+
+FHD_OK = 0
+FHD_WARN_NOT_CONVERGED_MAXITER = 1
+FHD_WARN_NOT_CONVERGED_OUTER = 2
+FHD_WARN_TRUE_RESID = 3
+FHD_ERR_BAD_ARG = -1
+FHD_ERR_BAD_GHOSTS = -2
+FHD_ERR_DX_NOT_ISOTROPIC = -3
+FHD_ERR_ORTHO_BREAKDOWN = -4
+FHD_ERR_UNSUPPORTED = -5
+FHD_ERR_NONFINITE = -6
+FHD_ERR_OOM = -7
+FHD_ERR_CUDA = -8
+FHD_ERR_NO_DEVICE = -9
+
+FHD_PREC_FP64 = 0
+FHD_PREC_MIXED = 1
+
+
+class GmresParams(C.Structure):
+    """fhd_gmres_params: mirror of namelist probin_gmres (probin_gmres.f90:12-163)."""
+    _fields_ = [
+        ("precon_type", C.c_int), ("visc_schur_approx", C.c_int),
+        ("p_norm_weight", C.c_double), ("scale_factor", C.c_double),
+        ("mg_verbose", C.c_int), ("cg_verbose", C.c_int),
+        ("mg_max_vcycles", C.c_int), ("mg_minwidth", C.c_int), ("mg_bottom_solver", C.c_int),
+        ("mg_nsmooths_down", C.c_int), ("mg_nsmooths_up", C.c_int), ("mg_nsmooths_bottom", C.c_int),
+        ("mg_max_bottom_nlevels", C.c_int),
+        ("mg_rel_tol", C.c_double), ("mg_abs_tol", C.c_double),
+        ("stag_mg_verbosity", C.c_int), ("stag_mg_max_vcycles", C.c_int), ("stag_mg_minwidth", C.c_int),
+        ("stag_mg_bottom_solver", C.c_int),
+        ("stag_mg_nsmooths_down", C.c_int), ("stag_mg_nsmooths_up", C.c_int),
+        ("stag_mg_nsmooths_bottom", C.c_int), ("stag_mg_max_bottom_nlevels", C.c_int),
+        ("stag_mg_omega", C.c_double), ("stag_mg_smoother", C.c_int), ("stag_mg_rel_tol", C.c_double),
+        ("gmres_rel_tol", C.c_double), ("gmres_abs_tol", C.c_double),
+        ("gmres_verbose", C.c_int), ("gmres_max_outer", C.c_int), ("gmres_max_inner", C.c_int),
+        ("gmres_max_iter", C.c_int), ("gmres_min_iter", C.c_int), ("gmres_spatial_order", C.c_int),
+    ]
+
+
+class StochParams(C.Structure):
+    """fhd_stoch_params (stochastic_m_fluxdiv.f90:137)."""
+    _fields_ = [("k_B", C.c_double), ("variance_coef_mom", C.c_double), ("dV", C.c_double),
+                ("stoch_stress_form", C.c_int), ("filtering_width", C.c_int)]
+
+
+class SolveStats(C.Structure):
+    _fields_ = [("outer_iters", C.c_int), ("total_iters", C.c_int), ("vcycles", C.c_int),
+                ("status", C.c_int),
+                ("norm_b", C.c_double), ("norm_pre_b", C.c_double), ("norm_init_resid", C.c_double),
+                ("norm_resid", C.c_double), ("norm_resid_Stokes", C.c_double),
+                ("norm_init_Stokes", C.c_double), ("norm_resid_est", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class Fab(C.Structure):
+    """fhd_fab: one Fortran column-major box (lo-ng : hi+nodal+ng, ..., ncomp)."""
+    _fields_ = [("data", C.POINTER(C.c_double)), ("lo", C.c_int * 3), ("hi", C.c_int * 3),
+                ("nodal", C.c_int * 3), ("ng", C.c_int), ("ncomp", C.c_int)]
+
+
+class Multifab(C.Structure):
+    _fields_ = [("nfabs", C.c_int), ("fabs", C.POINTER(Fab))]
+
+
+_DP = C.POINTER(C.c_double)
+_PP = C.POINTER(_DP)
+_VP = C.c_void_p
+
+_PROTOS = {
+    "fhd_gmres_params_default": (None, [C.POINTER(GmresParams)]),
+    "fhd_ctx_create": (C.c_int, [C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double), C.c_int,
+                                 C.POINTER(GmresParams), C.c_int, C.POINTER(_VP)]),
+    "fhd_ctx_destroy": (C.c_int, [_VP]),
+    "fhd_ctx_stream": (_VP, [_VP]),
+    "fhd_ctx_set_stream": (C.c_int, [_VP, _VP]),
+    "fhd_ctx_kernel_launches": (C.c_longlong, [_VP]),
+    "fhd_ctx_device_bytes": (C.c_ulonglong, [_VP]),
+    "fhd_status_string": (C.c_char_p, [C.c_int]),
+    "fhd_last_error": (C.c_char_p, []),
+    "fhd_dev_apply_matrix": (C.c_int, [_VP, _PP, _DP, _PP, _DP, _PP, _DP, _PP, _DP, C.c_double]),
+    "fhd_dev_apply_precon": (C.c_int, [_VP, _PP, _DP, _PP, _DP, _PP, _DP, _PP, _DP, C.c_double]),
+    "fhd_dev_stag_mg_solver": (C.c_int, [_VP, _PP, _DP, _PP, _DP, C.c_double, _PP, _PP]),
+    "fhd_dev_gmres": (C.c_int, [_VP, _PP, _DP, _PP, _DP, _PP, _DP, _PP, _DP, C.c_double, _DP,
+                                C.POINTER(SolveStats)]),
+    "fhd_dev_stochastic_m_fluxdiv": (C.c_int, [_VP, C.POINTER(StochParams), _PP, C.c_int, _DP, _PP, _DP, _PP,
+                                               C.c_double, _DP, C.c_int, _PP, _PP]),
+    "fhd_dev_advance_inertial": (C.c_int, [_VP, C.POINTER(StochParams), C.c_double, _PP, _DP, _DP, _DP, _PP,
+                                           _DP, _DP, _PP, _PP, _PP, C.POINTER(SolveStats)]),
+    "fhd_gmres": (C.c_int, [_VP] + [C.POINTER(Multifab)] * 8 + [_DP, _DP, C.POINTER(SolveStats)]),
+    "fhd_apply_precon": (C.c_int, [_VP] + [C.POINTER(Multifab)] * 8 + [C.c_double]),
+    "fhd_apply_matrix": (C.c_int, [_VP] + [C.POINTER(Multifab)] * 8 + [C.c_double]),
+    "fhd_stochastic_m_fluxdiv": (C.c_int, [_VP, C.POINTER(StochParams), C.POINTER(Multifab), C.c_int,
+                                           C.POINTER(Multifab), C.POINTER(Multifab), C.POINTER(Multifab),
+                                           C.POINTER(Multifab), C.c_double, _DP, C.c_int, C.POINTER(Multifab),
+                                           C.POINTER(Multifab)]),
+}
+
+_lib = None
+
+
+def header_functions(path: str = HEADER) -> list[str]:
+    """Names of the functions include/fhd_b200.h declares."""
+    src = open(path).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    names = re.findall(r"\b(fhd_[a-z0-9_]+)\s*\(", src)
+    out = []
+    for n in names:
+        if n not in out:
+            out.append(n)
+    return out
+
+
+def lib() -> C.CDLL:
+    """Load the sm_100a library; raise if it was never built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"lowmachfhd_b200: {LIB_PATH} is missing -- run lowmachfhd_b200/build.py "
+                          "(nvcc, sm_100a); there is no CPU fallback")
+    L = C.CDLL(LIB_PATH)
+    for name, (res, args) in _PROTOS.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L
+
+
+class FhdError(RuntimeError):
+    def __init__(self, status: int, where: str):
+        msg = lib().fhd_status_string(status).decode()
+        super().__init__(f"{where}: status {status}: {msg}")
+        self.status = status
+
+
+def check(status: int, where: str) -> int:
+    if status < 0:
+        raise FhdError(status, where)
+    return status

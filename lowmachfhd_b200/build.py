@@ -1,0 +1,45 @@
+"""Builds the sm_100a shared library lowmachfhd_b200/_fhd_b200.so in place
+with nvcc (no JIT, no torch extension: the library exports a plain C ABI)."""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+SRC = os.path.join(HERE, "csrc")
+OUT = os.path.join(HERE, "_fhd_b200.so")
+SOURCES = ["fhd_solver.cu", "fhd_step.cu", "fhd_capi.cu"]
+NVCC_FLAGS = [
+    "-gencode", "arch=compute_100a,code=sm_100a",
+    "-lineinfo", "-O3", "-std=c++17",
+    # FP64 parity with the CPU restatement: no contraction into FMA
+    "--fmad=false",
+    "-Xcompiler", "-fPIC", "-shared",
+    "--expt-relaxed-constexpr",
+]
+
+
+def nvcc() -> str:
+    for p in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", "nvcc"):
+        if p and (os.path.sep not in p or os.path.exists(p)):
+            return p
+    return "nvcc"
+
+
+def build(verbose: bool = False, extra: list[str] | None = None) -> str:
+    srcs = [os.path.join(SRC, s) for s in SOURCES]
+    newest = max(os.path.getmtime(p) for p in srcs + [os.path.join(SRC, h) for h in os.listdir(SRC)]
+                 + [os.path.join(HERE, "..", "include", "fhd_b200.h")])
+    if os.path.exists(OUT) and os.path.getmtime(OUT) >= newest and not extra:
+        return OUT
+    cmd = [nvcc()] + NVCC_FLAGS + (extra or []) + ["-o", OUT + ".tmp"] + srcs + ["-lcudart"]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
+    os.replace(OUT + ".tmp", OUT)
+    return OUT
+
+
+if __name__ == "__main__":
+    print(build(verbose=True, extra=sys.argv[1:] or None))

@@ -1,0 +1,486 @@
+// fhd_kernels.cuh -- sm_100a device kernels of the staggered Stokes solver.
+//
+// Canonical layout (include/fhd_b200.h): one periodic box, x fastest, face
+// array d holds the face on the low-d side of each cell, edges/nodes at the
+// low corner.  The periodic wrap replaces the ghost-cell exchange
+// (multifab_fill_boundary) that the reference performs after every colour.
+//
+// All kernels are memory-bound stencils: one thread per cell (or per face of
+// a colour), x-contiguous warps for coalesced 128-byte rows, read-only loads
+// through the non-coherent path.  Templated on the storage/arithmetic type T
+// (double, or float in the mixed-precision preconditioner), the dimension
+// and visc_type so the stencil is fully specialised.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace fhd {
+
+typedef long long i64;
+
+struct Grid {
+    int dim;
+    int n[3];
+    i64 nc;
+    double dx;
+};
+
+__host__ __device__ __forceinline__ int wrapc(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }
+
+struct Cell {
+    int i, j, k;
+    int nx, ny, nz;
+    __device__ __forceinline__ i64 id(int di, int dj, int dk) const {
+        int a = wrapc(i + di, nx), b = wrapc(j + dj, ny), c = wrapc(k + dk, nz);
+        return (i64)a + (i64)nx * ((i64)b + (i64)ny * c);
+    }
+};
+
+template <typename T>
+__device__ __forceinline__ T ld(const T* p, i64 i) { return __ldg(p + i); }
+
+// Pointers of one staggered operator level.  alpha is multiplied by
+// alpha_scale on the fly (theta_alpha on the finest level).
+template <typename T>
+struct StagOp {
+    const T* alpha[3];
+    T alpha_scale;
+    const T* beta;
+    const T* gamma;
+    const T* bed[3];  // 2D: node; 3D: xy, xz, yz
+    T q;              // 1/dx^2
+};
+
+template <int DIM>
+__host__ __device__ constexpr int edge_of(int c, int d) {
+    return DIM == 2 ? 0 : ((c < d ? c : d) == 0 ? ((c > d ? c : d) == 1 ? 0 : 1) : 2);
+}
+
+template <int C, int D>
+struct Off {
+    static constexpr int x = (D == 0), y = (D == 1), z = (D == 2);
+};
+
+// (alpha_scale*alpha - L) phi on the face of component C at cell P, and the
+// diagonal coefficient: the stencils of stag_applyop_2d/_3d
+// (stag_applyop.f90:212-1075) and the 'fac' of stag_mg_update
+// (stag_mg_solver.f90:1764-2458).
+template <typename T, int DIM, int VISC, int C>
+__device__ __forceinline__ T stag_lface(const StagOp<T>& A, const T* const* phi, const Cell& P, T& diag) {
+    constexpr int ex = (C == 0), ey = (C == 1), ez = (C == 2);
+    const i64 f = P.id(0, 0, 0);
+    const i64 fpc = P.id(ex, ey, ez);
+    const i64 fmc = P.id(-ex, -ey, -ez);
+    const T* pc = phi[C];
+    const T ph = ld(pc, f);
+    const T a = A.alpha_scale * ld(A.alpha[C], f);
+    const T q = A.q;
+    if constexpr (VISC < 0) {
+        const T bp = ld(A.beta, f), bm = ld(A.beta, fmc);
+        T kp, km;
+        if constexpr (VISC == -1) {
+            kp = bp; km = bm;
+        } else if constexpr (VISC == -2) {
+            kp = T(2) * bp; km = T(2) * bm;
+        } else {
+            kp = T(4.0 / 3.0) * bp + ld(A.gamma, f);
+            km = T(4.0 / 3.0) * bm + ld(A.gamma, fmc);
+        }
+        T s = kp + km;
+        T nb = ld(pc, fpc) * kp + ld(pc, fmc) * km;
+        T cross = T(0);
+        T tp = T(0), tm = T(0);
+        if constexpr (VISC == -3) {
+            tp = -T(2.0 / 3.0) * bp + ld(A.gamma, f);
+            tm = -T(2.0 / 3.0) * bm + ld(A.gamma, fmc);
+        }
+#pragma unroll
+        for (int d = 0; d < DIM; d++) {
+            if (d == C) continue;
+            const int dx_ = (d == 0), dy_ = (d == 1), dz_ = (d == 2);
+            const i64 fpd = P.id(dx_, dy_, dz_);
+            const i64 fmd = P.id(-dx_, -dy_, -dz_);
+            const T* E = A.bed[edge_of<DIM>(C, d)];
+            const T elo = ld(E, f), ehi = ld(E, fpd);
+            s += elo + ehi;
+            nb += ld(pc, fpd) * ehi + ld(pc, fmd) * elo;
+            if constexpr (VISC != -1) {
+                const i64 fmcpd = P.id(dx_ - ex, dy_ - ey, dz_ - ez);
+                const T* pd = phi[d];
+                cross += ld(pd, fpd) * (ehi + tp) - ld(pd, f) * (elo + tp) - ld(pd, fmcpd) * (ehi + tm) +
+                         ld(pd, fmc) * (elo + tm);
+            }
+        }
+        diag = a + s * q;
+        return ph * diag - (nb + cross) * q;
+    } else {
+        const T b = ld(A.beta, 0);
+        const T own = ld(pc, fpc) + ld(pc, fmc);
+        T oth = T(0), cross = T(0);
+#pragma unroll
+        for (int d = 0; d < DIM; d++) {
+            if (d == C) continue;
+            const int dx_ = (d == 0), dy_ = (d == 1), dz_ = (d == 2);
+            const i64 fpd = P.id(dx_, dy_, dz_);
+            const i64 fmd = P.id(-dx_, -dy_, -dz_);
+            oth += ld(pc, fpd) + ld(pc, fmd);
+            if constexpr (VISC != 1) {
+                const i64 fmcpd = P.id(dx_ - ex, dy_ - ey, dz_ - ez);
+                const T* pd = phi[d];
+                cross += ld(pd, fpd) - ld(pd, f) - ld(pd, fmcpd) + ld(pd, fmc);
+            }
+        }
+        if constexpr (VISC == 1) {
+            diag = a + T(2 * DIM) * b * q;
+            return ph * diag - (own + oth) * b * q;
+        } else if constexpr (VISC == 2) {
+            diag = a + T(2 * DIM + 2) * b * q;
+            return ph * diag - (T(2) * own + oth + cross) * b * q;
+        } else {
+            const T cg = ld(A.gamma, 0);
+            diag = a + ((T(8.0 / 3.0) + T(2 * (DIM - 1))) * b + T(2) * cg) * q;
+            return ph * diag - (own * (T(4.0 / 3.0) * b + cg) + oth * b + cross * (T(1.0 / 3.0) * b + cg)) * q;
+        }
+    }
+}
+
+template <typename T, int DIM, int VISC>
+__device__ __forceinline__ T stag_lface_c(int c, const StagOp<T>& A, const T* const* phi, const Cell& P, T& diag) {
+    if (c == 0) return stag_lface<T, DIM, VISC, 0>(A, phi, P, diag);
+    if (DIM == 3 && c == 2) return stag_lface<T, DIM, VISC, (DIM == 3 ? 2 : 1)>(A, phi, P, diag);
+    return stag_lface<T, DIM, VISC, 1>(A, phi, P, diag);
+}
+
+__device__ __forceinline__ bool cell_of_thread(const Grid& g, Cell& P) {
+    P.nx = g.n[0]; P.ny = g.n[1]; P.nz = g.n[2];
+    P.i = blockIdx.x * blockDim.x + threadIdx.x;
+    P.j = blockIdx.y * blockDim.y + threadIdx.y;
+    P.k = blockIdx.z;
+    return P.i < P.nx && P.j < P.ny;
+}
+
+// ---------------------------------------------------------------------
+// staggered operator kernels
+// ---------------------------------------------------------------------
+
+// out[c] = L phi  (mode 0), rhs[c] - L phi (mode 1, residual)
+template <typename T, int DIM, int VISC>
+__global__ void __launch_bounds__(256) k_stag_apply(Grid g, StagOp<T> A, const T* __restrict__ p0,
+                                                    const T* __restrict__ p1, const T* __restrict__ p2,
+                                                    T* o0, T* o1, T* o2, const T* r0, const T* r1, const T* r2,
+                                                    int mode) {
+    Cell P;
+    if (!cell_of_thread(g, P)) return;
+    const T* phi[3] = {p0, p1, p2};
+    T* out[3] = {o0, o1, o2};
+    const T* rhs[3] = {r0, r1, r2};
+    const i64 f = P.id(0, 0, 0);
+#pragma unroll
+    for (int c = 0; c < DIM; c++) {
+        T dg;
+        T L = stag_lface_c<T, DIM, VISC>(c, A, phi, P, dg);
+        out[c][f] = mode ? ld(rhs[c], f) - L : L;
+    }
+}
+
+// One colour of the 2*dim-colour Gauss-Seidel smoother, fused: the
+// applyop(colour) of stag_applyop_level and the stag_mg_update(colour)
+// (stag_mg_solver.f90:360-396).  Faces of component C with parity
+// (i+j+k)%2 == par are updated.  Valid when every extent is even (no face
+// of the colour then neighbours another face of the same colour).
+// Thread x-index runs over half the row.
+template <typename T, int DIM, int VISC, int C>
+__global__ void __launch_bounds__(256) k_stag_gs(Grid g, StagOp<T> A, T* p0, T* p1, T* p2,
+                                                 const T* __restrict__ r, int par, T omega) {
+    Cell P;
+    P.nx = g.n[0]; P.ny = g.n[1]; P.nz = g.n[2];
+    const int ih = blockIdx.x * blockDim.x + threadIdx.x;
+    P.j = blockIdx.y * blockDim.y + threadIdx.y;
+    P.k = blockIdx.z;
+    if (P.j >= P.ny) return;
+    P.i = 2 * ih + ((P.j + P.k + par) & 1);
+    if (P.i >= P.nx) return;
+    const T* phi[3] = {p0, p1, p2};
+    T* pc = (C == 0) ? p0 : (C == 1 ? p1 : p2);
+    const i64 f = P.id(0, 0, 0);
+    T dg;
+    const T L = stag_lface<T, DIM, VISC, C>(A, phi, P, dg);
+    pc[f] = pc[f] + omega * (ld(r, f) - L) / dg;
+}
+
+// Two-pass colour smoother for levels with an odd extent or the Jacobi
+// smoother (colour 0): pass 1 stores L phi and the diagonal for the colour.
+template <typename T, int DIM, int VISC>
+__global__ void __launch_bounds__(256) k_stag_color_apply(Grid g, StagOp<T> A, const T* p0, const T* p1,
+                                                          const T* p2, T* L0, T* L1, T* L2, T* D0, T* D1, T* D2,
+                                                          int color) {
+    Cell P;
+    if (!cell_of_thread(g, P)) return;
+    const T* phi[3] = {p0, p1, p2};
+    T* Lo[3] = {L0, L1, L2};
+    T* Do[3] = {D0, D1, D2};
+    const i64 f = P.id(0, 0, 0);
+    const int par = (P.i + P.j + P.k) & 1;
+#pragma unroll
+    for (int c = 0; c < DIM; c++) {
+        if (color != 0 && ((color - 1) / 2 != c || par != ((color + 1) & 1))) continue;
+        T dg;
+        Lo[c][f] = stag_lface_c<T, DIM, VISC>(c, A, phi, P, dg);
+        Do[c][f] = dg;
+    }
+}
+
+template <typename T, int DIM>
+__global__ void __launch_bounds__(256) k_stag_color_update(Grid g, T* p0, T* p1, T* p2, const T* r0, const T* r1,
+                                                           const T* r2, const T* L0, const T* L1, const T* L2,
+                                                           const T* D0, const T* D1, const T* D2, int color,
+                                                           T omega) {
+    Cell P;
+    if (!cell_of_thread(g, P)) return;
+    T* ph[3] = {p0, p1, p2};
+    const T* rh[3] = {r0, r1, r2};
+    const T* Lo[3] = {L0, L1, L2};
+    const T* Do[3] = {D0, D1, D2};
+    const i64 f = P.id(0, 0, 0);
+    const int par = (P.i + P.j + P.k) & 1;
+#pragma unroll
+    for (int c = 0; c < DIM; c++) {
+        if (color != 0 && ((color - 1) / 2 != c || par != ((color + 1) & 1))) continue;
+        ph[c][f] = ph[c][f] + omega * (rh[c][f] - Lo[c][f]) / Do[c][f];
+    }
+}
+
+// stag_restriction (stag_mg_solver.f90:1028-1170): 6-point (2D) / 12-point
+// (3D) full stencil, or the 2/4-point 'simple' stencil.  Thread per coarse
+// cell, all components.
+template <typename T, int DIM>
+__global__ void __launch_bounds__(256) k_stag_restrict(Grid gf, Grid gc, const T* f0, const T* f1, const T* f2,
+                                                       T* c0, T* c1, T* c2, int simple) {
+    Cell Q;
+    if (!cell_of_thread(gc, Q)) return;
+    Cell F;
+    F.nx = gf.n[0]; F.ny = gf.n[1]; F.nz = gf.n[2];
+    F.i = 2 * Q.i; F.j = 2 * Q.j; F.k = (DIM == 3) ? 2 * Q.k : 0;
+    const T* fi[3] = {f0, f1, f2};
+    T* co[3] = {c0, c1, c2};
+    const i64 qc = Q.id(0, 0, 0);
+#pragma unroll
+    for (int c = 0; c < DIM; c++) {
+        const T* Fp = fi[c];
+        const int a = (c == 0) ? 1 : 0;
+        const int b = (c == 2) ? 1 : 2;
+        auto at = [&](int o, int pa, int pb) {
+            int off[3] = {0, 0, 0};
+            off[c] += o;
+            off[a] += pa;
+            if (DIM == 3) off[b] += pb;
+            return ld(Fp, F.id(off[0], off[1], off[2]));
+        };
+        T v;
+        if constexpr (DIM == 2) {
+            if (simple) v = T(0.5) * (at(0, 0, 0) + at(0, 1, 0));
+            else v = T(0.25) * (at(0, 0, 0) + at(0, 1, 0)) +
+                     T(0.125) * (at(1, 0, 0) + at(1, 1, 0) + at(-1, 0, 0) + at(-1, 1, 0));
+        } else {
+            if (simple) v = T(0.25) * (at(0, 0, 0) + at(0, 1, 0) + at(0, 0, 1) + at(0, 1, 1));
+            else v = T(0.125) * (at(0, 0, 0) + at(0, 1, 0) + at(0, 0, 1) + at(0, 1, 1)) +
+                     T(0.0625) * (at(1, 0, 0) + at(1, 1, 0) + at(1, 0, 1) + at(1, 1, 1)) +
+                     T(0.0625) * (at(-1, 0, 0) + at(-1, 1, 0) + at(-1, 0, 1) + at(-1, 1, 1));
+        }
+        co[c][qc] = v;
+    }
+}
+
+// stag_prolongation (stag_mg_solver.f90:1419-1628): fine += P coarse.
+template <typename T, int DIM>
+__global__ void __launch_bounds__(256) k_stag_prolong(Grid gf, Grid gc, T* f0, T* f1, T* f2, const T* c0,
+                                                      const T* c1, const T* c2) {
+    Cell P;
+    if (!cell_of_thread(gf, P)) return;
+    Cell H;
+    H.nx = gc.n[0]; H.ny = gc.n[1]; H.nz = gc.n[2];
+    H.i = P.i >> 1; H.j = P.j >> 1; H.k = P.k >> 1;
+    T* fo[3] = {f0, f1, f2};
+    const T* ci[3] = {c0, c1, c2};
+    const int I[3] = {P.i, P.j, P.k};
+    const i64 f = P.id(0, 0, 0);
+#pragma unroll
+    for (int c = 0; c < DIM; c++) {
+        const T* Cp = ci[c];
+        const int a = (c == 0) ? 1 : 0;
+        const int b = (c == 2) ? 1 : 2;
+        const int oa = (I[a] & 1) ? 1 : -1;
+        const int ob = (DIM == 3) ? ((I[b] & 1) ? 1 : -1) : 0;
+        auto at = [&](int o, int pa, int pb) {
+            int off[3] = {0, 0, 0};
+            off[c] += o;
+            off[a] += pa;
+            if (DIM == 3) off[b] += pb;
+            return ld(Cp, H.id(off[0], off[1], off[2]));
+        };
+        const bool even = (I[c] & 1) == 0;
+        T v;
+        if constexpr (DIM == 2) {
+            if (even) v = T(0.75) * at(0, 0, 0) + T(0.25) * at(0, oa, 0);
+            else v = T(0.375) * at(0, 0, 0) + T(0.125) * at(0, oa, 0) + T(0.375) * at(1, 0, 0) +
+                     T(0.125) * at(1, oa, 0);
+        } else {
+            if (even) v = T(9.0 / 16.0) * at(0, 0, 0) + T(3.0 / 16.0) * at(0, oa, 0) + T(3.0 / 16.0) * at(0, 0, ob) +
+                          T(1.0 / 16.0) * at(0, oa, ob);
+            else v = T(9.0 / 32.0) * at(0, 0, 0) + T(3.0 / 32.0) * at(0, oa, 0) + T(3.0 / 32.0) * at(0, 0, ob) +
+                     T(1.0 / 32.0) * at(0, oa, ob) + T(9.0 / 32.0) * at(1, 0, 0) + T(3.0 / 32.0) * at(1, oa, 0) +
+                     T(3.0 / 32.0) * at(1, 0, ob) + T(1.0 / 32.0) * at(1, oa, ob);
+        }
+        fo[c][f] = fo[c][f] + v;
+    }
+}
+
+// cc_restriction (stag_mg_solver.f90:919-963): average of 2^dim children
+template <typename T, int DIM>
+__global__ void __launch_bounds__(256) k_cc_average(Grid gf, Grid gc, const T* F, T* Cc) {
+    Cell Q;
+    if (!cell_of_thread(gc, Q)) return;
+    Cell P;
+    P.nx = gf.n[0]; P.ny = gf.n[1]; P.nz = gf.n[2];
+    P.i = 2 * Q.i; P.j = 2 * Q.j; P.k = (DIM == 3) ? 2 * Q.k : 0;
+    T v;
+    if constexpr (DIM == 2) {
+        v = T(0.25) * (ld(F, P.id(0, 0, 0)) + ld(F, P.id(1, 0, 0)) + ld(F, P.id(0, 1, 0)) + ld(F, P.id(1, 1, 0)));
+    } else {
+        v = T(0.125) * (ld(F, P.id(0, 0, 0)) + ld(F, P.id(1, 0, 0)) + ld(F, P.id(0, 1, 0)) + ld(F, P.id(1, 1, 0)) +
+                        ld(F, P.id(0, 0, 1)) + ld(F, P.id(1, 0, 1)) + ld(F, P.id(0, 1, 1)) + ld(F, P.id(1, 1, 1)));
+    }
+    Cc[Q.id(0, 0, 0)] = v;
+}
+
+// nodal_restriction (2D injection) / edge_restriction (3D 2-point),
+// stag_mg_solver.f90:1173-1362
+template <typename T, int DIM>
+__global__ void __launch_bounds__(256) k_edge_coarsen(Grid gf, Grid gc, const T* e0, const T* e1, const T* e2,
+                                                      T* c0, T* c1, T* c2) {
+    Cell Q;
+    if (!cell_of_thread(gc, Q)) return;
+    Cell P;
+    P.nx = gf.n[0]; P.ny = gf.n[1]; P.nz = gf.n[2];
+    P.i = 2 * Q.i; P.j = 2 * Q.j; P.k = (DIM == 3) ? 2 * Q.k : 0;
+    const i64 q = Q.id(0, 0, 0);
+    if constexpr (DIM == 2) {
+        c0[q] = ld(e0, P.id(0, 0, 0));
+    } else {
+        c0[q] = T(0.5) * (ld(e0, P.id(0, 0, 0)) + ld(e0, P.id(0, 0, 1)));
+        c1[q] = T(0.5) * (ld(e1, P.id(0, 0, 0)) + ld(e1, P.id(0, 1, 0)));
+        c2[q] = T(0.5) * (ld(e2, P.id(0, 0, 0)) + ld(e2, P.id(1, 0, 0)));
+    }
+}
+
+// ---------------------------------------------------------------------
+// cell-centred pressure multigrid (FBoxLib ml_cc_solve as used by
+// macproject.f90:294-298, semantics of PreconditionerNotes.tex:484-575)
+// ---------------------------------------------------------------------
+template <typename T>
+struct CCOp {
+    const T* a[3];  // face coefficient (alphainv), low side of each cell
+    T q;            // 1/dx^2 of the level
+};
+
+template <typename T, int DIM>
+__device__ __forceinline__ T cc_lap(const CCOp<T>& A, const T* phi, const Cell& P, T& diag) {
+    const i64 f = P.id(0, 0, 0);
+    const T pc = ld(phi, f);
+    T s = T(0), dg = T(0);
+#pragma unroll
+    for (int d = 0; d < DIM; d++) {
+        const int dx_ = (d == 0), dy_ = (d == 1), dz_ = (d == 2);
+        const i64 fp = P.id(dx_, dy_, dz_);
+        const i64 fm = P.id(-dx_, -dy_, -dz_);
+        const T ahi = ld(A.a[d], fp), alo = ld(A.a[d], f);
+        s += ahi * (ld(phi, fp) - pc) - alo * (pc - ld(phi, fm));
+        dg += ahi + alo;
+    }
+    diag = -dg * A.q;
+    return s * A.q;
+}
+
+// red-black Gauss-Seidel, one colour, fused; thread per cell of the colour
+template <typename T, int DIM>
+__global__ void __launch_bounds__(256) k_cc_gsrb(Grid g, CCOp<T> A, T* phi, const T* __restrict__ rhs, int par) {
+    Cell P;
+    P.nx = g.n[0]; P.ny = g.n[1]; P.nz = g.n[2];
+    const int ih = blockIdx.x * blockDim.x + threadIdx.x;
+    P.j = blockIdx.y * blockDim.y + threadIdx.y;
+    P.k = blockIdx.z;
+    if (P.j >= P.ny) return;
+    P.i = 2 * ih + ((P.j + P.k + par) & 1);
+    if (P.i >= P.nx) return;
+    T dg;
+    const T L = cc_lap<T, DIM>(A, phi, P, dg);
+    const i64 f = P.id(0, 0, 0);
+    phi[f] = phi[f] + (ld(rhs, f) - L) / dg;
+}
+
+// two-pass colour for odd extents: store the correction, then add it
+template <typename T, int DIM>
+__global__ void __launch_bounds__(256) k_cc_color_corr(Grid g, CCOp<T> A, const T* phi, const T* rhs, T* corr,
+                                                       int par) {
+    Cell P;
+    if (!cell_of_thread(g, P)) return;
+    if (((P.i + P.j + P.k) & 1) != par) return;
+    T dg;
+    const T L = cc_lap<T, DIM>(A, phi, P, dg);
+    const i64 f = P.id(0, 0, 0);
+    corr[f] = (ld(rhs, f) - L) / dg;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_cc_color_add(Grid g, T* phi, const T* corr, int par) {
+    Cell P;
+    if (!cell_of_thread(g, P)) return;
+    if (((P.i + P.j + P.k) & 1) != par) return;
+    const i64 f = P.id(0, 0, 0);
+    phi[f] = phi[f] + corr[f];
+}
+
+// residual on the 2^dim children of a coarse cell, averaged into the coarse
+// rhs (residual + restriction in one pass; every fine cell once)
+template <typename T, int DIM>
+__global__ void __launch_bounds__(256) k_cc_resid_restrict(Grid gf, Grid gc, CCOp<T> A, const T* phi, const T* rhs,
+                                                           T* crhs) {
+    Cell Q;
+    if (!cell_of_thread(gc, Q)) return;
+    Cell P;
+    P.nx = gf.n[0]; P.ny = gf.n[1]; P.nz = gf.n[2];
+    T acc = T(0);
+    const int kz = (DIM == 3) ? 2 : 1;
+#pragma unroll
+    for (int dk = 0; dk < kz; dk++)
+#pragma unroll
+        for (int dj = 0; dj < 2; dj++)
+#pragma unroll
+            for (int di = 0; di < 2; di++) {
+                P.i = 2 * Q.i + di; P.j = 2 * Q.j + dj; P.k = (DIM == 3) ? 2 * Q.k + dk : 0;
+                T dg;
+                const T L = cc_lap<T, DIM>(A, phi, P, dg);
+                acc += ld(rhs, P.id(0, 0, 0)) - L;
+            }
+    crhs[Q.id(0, 0, 0)] = acc * (DIM == 3 ? T(0.125) : T(0.25));
+}
+
+template <typename T, int DIM>
+__global__ void __launch_bounds__(256) k_cc_prolong(Grid gf, Grid gc, T* phi, const T* cphi) {
+    Cell P;
+    if (!cell_of_thread(gf, P)) return;
+    const i64 f = P.id(0, 0, 0);
+    const i64 c = (i64)(P.i >> 1) + (i64)gc.n[0] * ((i64)(P.j >> 1) + (i64)gc.n[1] * (P.k >> 1));
+    phi[f] = phi[f] + ld(cphi, c);
+}
+
+template <typename T, int DIM>
+__global__ void __launch_bounds__(256) k_cc_resid(Grid g, CCOp<T> A, const T* phi, const T* rhs, T* res) {
+    Cell P;
+    if (!cell_of_thread(g, P)) return;
+    T dg;
+    const i64 f = P.id(0, 0, 0);
+    res[f] = ld(rhs, f) - cc_lap<T, DIM>(A, phi, P, dg);
+}
+
+}  // namespace fhd

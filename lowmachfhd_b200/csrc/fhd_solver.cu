@@ -1,0 +1,1190 @@
+// fhd_solver.cu -- staggered multigrid, pressure multigrid, the
+// preconditioner, the saddle-point operator and GMRES, driven from the host
+// on one CUDA stream; plus the device-pointer C ABI.
+//
+// Follows staggered_grid/src_gmres of LowMachFHD: gmres.f90,
+// apply_matrix.f90, apply_precon.f90, stag_mg_solver.f90, macproject.f90.
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <type_traits>
+
+#include "fhd_solver.cuh"
+
+namespace fhd {
+
+static thread_local std::string g_last_error;
+void set_last_error(const std::string& s) { g_last_error = s; }
+
+int nlevs_mg(const Grid& g, int minwidth) {
+    // compute_nlevs_mg (stag_mg_layout.f90:179-222), one box
+    int nl = -1;
+    for (int d = 0; d < g.dim; d++) {
+        int t = g.n[d], r = 1;
+        while (t % 2 == 0 && t / minwidth != 1) {
+            t /= 2;
+            r++;
+        }
+        nl = (nl < 0) ? r : (r < nl ? r : nl);
+    }
+    return nl;
+}
+
+static inline int post(fhd_ctx* ctx) {
+    ctx->launches++;
+    cudaError_t e = cudaPeekAtLastError();
+    if (e != cudaSuccess) {
+        set_last_error(std::string("kernel launch: ") + cudaGetErrorString(e));
+        return FHD_ERR_CUDA;
+    }
+    return 0;
+}
+
+#define FHD_POST(ctx)                 \
+    do {                              \
+        int rc_ = post(ctx);          \
+        if (rc_) return rc_;          \
+    } while (0)
+
+template <typename T>
+static Multigrid<T>& mg_of(fhd_ctx* ctx);
+template <>
+Multigrid<double>& mg_of<double>(fhd_ctx* ctx) { return ctx->mg64; }
+template <>
+Multigrid<float>& mg_of<float>(fhd_ctx* ctx) { return ctx->mg32; }
+
+// ---------------------------------------------------------------------
+// hierarchy construction (stag_mg_layout_build / mgt_macproj_precon_build)
+// ---------------------------------------------------------------------
+template <typename T>
+static int build_mg(fhd_ctx* ctx, Multigrid<T>& M) {
+    const int dim = ctx->dim;
+    const int nE = dim == 2 ? 1 : 3;
+    Arena& A = ctx->arena;
+    const int ns = nlevs_mg(ctx->g0, ctx->p.stag_mg_minwidth);
+    M.s.resize(ns);
+    for (int l = 0; l < ns; l++) {
+        StagLevel<T>& L = M.s[l];
+        L.g = (l == 0) ? ctx->g0 : coarsen(M.s[l - 1].g);
+        const i64 nc = L.g.nc;
+        for (int c = 0; c < dim; c++) {
+            if (l > 0) {
+                L.alpha[c] = A.alloc<T>(nc);
+                L.phi[c] = A.alloc<T>(nc);
+                L.rhs[c] = A.alloc<T>(nc);
+                if (!L.alpha[c] || !L.phi[c] || !L.rhs[c]) return FHD_ERR_OOM;
+            }
+            L.tmp[c] = A.alloc<T>(nc);
+            if (!L.tmp[c]) return FHD_ERR_OOM;
+            if (!all_even(L.g) || ctx->p.stag_mg_smoother == 0) {
+                L.diag[c] = A.alloc<T>(nc);
+                if (!L.diag[c]) return FHD_ERR_OOM;
+            }
+        }
+        if (l > 0 || !std::is_same<T, double>::value) {
+            L.own_beta = A.alloc<T>(nc);
+            L.own_gamma = A.alloc<T>(nc);
+            if (!L.own_beta || !L.own_gamma) return FHD_ERR_OOM;
+            for (int e = 0; e < nE; e++) {
+                L.own_bed[e] = A.alloc<T>(nc);
+                if (!L.own_bed[e]) return FHD_ERR_OOM;
+            }
+            L.beta = L.own_beta;
+            L.gamma = L.own_gamma;
+            for (int e = 0; e < nE; e++) L.bed[e] = L.own_bed[e];
+        }
+        if (l == 0 && !std::is_same<T, double>::value) {
+            for (int c = 0; c < dim; c++) {
+                L.own_alpha0[c] = A.alloc<T>(nc);
+                if (!L.own_alpha0[c]) return FHD_ERR_OOM;
+                L.alpha[c] = L.own_alpha0[c];
+            }
+        }
+    }
+    const int ncl = nlevs_mg(ctx->g0, ctx->p.mg_minwidth);
+    M.c.resize(ncl);
+    for (int l = 0; l < ncl; l++) {
+        CCLevel<T>& C = M.c[l];
+        C.g = (l == 0) ? ctx->g0 : coarsen(M.c[l - 1].g);
+        const i64 nc = C.g.nc;
+        for (int c = 0; c < dim; c++) {
+            C.a[c] = A.alloc<T>(nc);
+            if (!C.a[c]) return FHD_ERR_OOM;
+        }
+        C.phi = A.alloc<T>(nc);
+        C.rhs = A.alloc<T>(nc);
+        C.tmp = A.alloc<T>(nc);
+        if (!C.phi || !C.rhs || !C.tmp) return FHD_ERR_OOM;
+    }
+    const i64 nc0 = ctx->g0.nc;
+    for (int c = 0; c < dim; c++) {
+        M.x_u[c] = A.alloc<T>(nc0);
+        M.b_u[c] = A.alloc<T>(nc0);
+        if (!M.x_u[c] || !M.b_u[c]) return FHD_ERR_OOM;
+    }
+    M.mac_rhs = A.alloc<T>(nc0);
+    if (!M.mac_rhs) return FHD_ERR_OOM;
+    return 0;
+}
+
+// coefficient hierarchy for the current operator (stag_mg_solver.f90:
+// 200-230; alphainv of apply_precon.f90:73-76 coarsened for the pressure
+// multigrid as face averages)
+template <typename T>
+static int prepare_T(fhd_ctx* ctx) {
+    Multigrid<T>& M = mg_of<T>(ctx);
+    const int dim = ctx->dim;
+    const int nE = dim == 2 ? 1 : 3;
+    const i64 nc0 = ctx->g0.nc;
+    cudaStream_t st = ctx->stream;
+    StagLevel<T>& L0 = M.s[0];
+    if (std::is_same<T, double>::value) {
+        for (int c = 0; c < dim; c++) L0.alpha[c] = (T*)ctx->alpha_fc[c];
+        L0.alpha_scale = (T)ctx->theta;
+        L0.beta = (const T*)ctx->beta;
+        L0.gamma = (const T*)ctx->gamma;
+        for (int e = 0; e < nE; e++) L0.bed[e] = (const T*)ctx->beta_ed[e];
+    } else {
+        const int nb = flat_blocks(nc0);
+        for (int c = 0; c < dim; c++) {
+            k_copy_conv<T, double><<<nb, 256, 0, st>>>(nc0, L0.own_alpha0[c], ctx->alpha_fc[c], ctx->theta);
+            FHD_POST(ctx);
+        }
+        L0.alpha_scale = T(1);
+        k_copy_conv<T, double><<<nb, 256, 0, st>>>(nc0, L0.own_beta, ctx->beta, 1.0);
+        FHD_POST(ctx);
+        k_copy_conv<T, double><<<nb, 256, 0, st>>>(nc0, L0.own_gamma, ctx->gamma, 1.0);
+        FHD_POST(ctx);
+        for (int e = 0; e < nE; e++) {
+            k_copy_conv<T, double><<<nb, 256, 0, st>>>(nc0, L0.own_bed[e], ctx->beta_ed[e], 1.0);
+            FHD_POST(ctx);
+        }
+    }
+    for (size_t l = 1; l < M.s.size(); l++) {
+        StagLevel<T>& F = M.s[l - 1];
+        StagLevel<T>& C = M.s[l];
+        int rc = 0;
+        with_dim(dim, [&](auto D) {
+            constexpr int DIM = decltype(D)::value;
+            k_cc_average<T, DIM><<<cell_grid(C.g), cell_block(), 0, st>>>(F.g, C.g, F.beta, C.own_beta);
+            rc |= post(ctx);
+            k_cc_average<T, DIM><<<cell_grid(C.g), cell_block(), 0, st>>>(F.g, C.g, F.gamma, C.own_gamma);
+            rc |= post(ctx);
+            k_edge_coarsen<T, DIM><<<cell_grid(C.g), cell_block(), 0, st>>>(
+                F.g, C.g, F.bed[0], F.bed[1], F.bed[2], C.own_bed[0], C.own_bed[1], C.own_bed[2]);
+            rc |= post(ctx);
+        });
+        if (rc) return rc;
+        if (l == 1 && F.alpha_scale != T(1)) {
+            // level 0 alpha carries theta_alpha through alpha_scale: form
+            // theta*alpha in the level-1 buffer first, then coarsen
+            // in place is not possible; scale while restricting instead
+            const int nb = flat_blocks(F.g.nc);
+            for (int c = 0; c < dim; c++) {
+                k_copy_conv<T, T><<<nb, 256, 0, st>>>(F.g.nc, F.tmp[c], F.alpha[c], (double)F.alpha_scale);
+                FHD_POST(ctx);
+            }
+            with_dim(dim, [&](auto D) {
+                constexpr int DIM = decltype(D)::value;
+                k_stag_restrict<T, DIM><<<cell_grid(C.g), cell_block(), 0, st>>>(
+                    F.g, C.g, F.tmp[0], F.tmp[1], F.tmp[2], C.alpha[0], C.alpha[1], C.alpha[2], 1);
+                rc |= post(ctx);
+            });
+        } else {
+            with_dim(dim, [&](auto D) {
+                constexpr int DIM = decltype(D)::value;
+                k_stag_restrict<T, DIM><<<cell_grid(C.g), cell_block(), 0, st>>>(
+                    F.g, C.g, F.alpha[0], F.alpha[1], F.alpha[2], C.alpha[0], C.alpha[1], C.alpha[2], 1);
+                rc |= post(ctx);
+            });
+        }
+        if (rc) return rc;
+        C.alpha_scale = T(1);
+    }
+    // pressure multigrid coefficients: alphainv on the finest level
+    {
+        const int nb = flat_blocks(nc0);
+        for (int c = 0; c < dim; c++) {
+            k_recip<T><<<nb, 256, 0, st>>>(nc0, M.c[0].a[c], ctx->alpha_fc[c]);
+            FHD_POST(ctx);
+        }
+        for (size_t l = 1; l < M.c.size(); l++) {
+            CCLevel<T>& F = M.c[l - 1];
+            CCLevel<T>& C = M.c[l];
+            int rc = 0;
+            with_dim(dim, [&](auto D) {
+                constexpr int DIM = decltype(D)::value;
+                k_stag_restrict<T, DIM><<<cell_grid(C.g), cell_block(), 0, st>>>(
+                    F.g, C.g, F.a[0], F.a[1], F.a[2], C.a[0], C.a[1], C.a[2], 1);
+                rc |= post(ctx);
+            });
+            if (rc) return rc;
+        }
+    }
+    return 0;
+}
+
+int prepare(fhd_ctx* ctx, const double* const alpha_fc[], const double* beta, const double* const beta_ed[],
+            const double* gamma, double theta) {
+    const int dim = ctx->dim;
+    for (int c = 0; c < 3; c++) ctx->alpha_fc[c] = c < dim ? alpha_fc[c] : nullptr;
+    ctx->beta = beta;
+    ctx->gamma = gamma;
+    for (int e = 0; e < 3; e++) ctx->beta_ed[e] = e < (dim == 2 ? 1 : 3) ? beta_ed[e] : nullptr;
+    ctx->theta = theta;
+    if (ctx->prec == FHD_PREC_MIXED) return prepare_T<float>(ctx);
+    return prepare_T<double>(ctx);
+}
+
+// ---------------------------------------------------------------------
+// staggered multigrid V-cycle (stag_mg_solver.f90:323-808)
+// ---------------------------------------------------------------------
+template <typename T>
+static int stag_smooth(fhd_ctx* ctx, StagLevel<T>& L, int color) {
+    cudaStream_t st = ctx->stream;
+    const T omega = (T)ctx->p.stag_mg_omega;
+    const StagOp<T> A = L.op();
+    int rc = 0;
+    if (color != 0 && all_even(L.g)) {
+        const int c = (color - 1) / 2;
+        const int par = (color + 1) & 1;
+        with_dim_visc(ctx->dim, ctx->visc, [&](auto D, auto V) {
+            constexpr int DIM = decltype(D)::value, VISC = decltype(V)::value;
+            if (c == 0)
+                k_stag_gs<T, DIM, VISC, 0><<<half_grid(L.g), cell_block(), 0, st>>>(L.g, A, L.phi[0], L.phi[1],
+                                                                                   L.phi[2], L.rhs[0], par, omega);
+            else if (c == 1)
+                k_stag_gs<T, DIM, VISC, 1><<<half_grid(L.g), cell_block(), 0, st>>>(L.g, A, L.phi[0], L.phi[1],
+                                                                                   L.phi[2], L.rhs[1], par, omega);
+            else
+                k_stag_gs<T, DIM, VISC, (DIM == 3 ? 2 : 1)><<<half_grid(L.g), cell_block(), 0, st>>>(
+                    L.g, A, L.phi[0], L.phi[1], L.phi[2], L.rhs[DIM == 3 ? 2 : 1], par, omega);
+            rc |= post(ctx);
+        });
+        return rc;
+    }
+    with_dim_visc(ctx->dim, ctx->visc, [&](auto D, auto V) {
+        constexpr int DIM = decltype(D)::value, VISC = decltype(V)::value;
+        k_stag_color_apply<T, DIM, VISC><<<cell_grid(L.g), cell_block(), 0, st>>>(
+            L.g, A, L.phi[0], L.phi[1], L.phi[2], L.tmp[0], L.tmp[1], L.tmp[2], L.diag[0], L.diag[1], L.diag[2],
+            color);
+        rc |= post(ctx);
+        k_stag_color_update<T, DIM><<<cell_grid(L.g), cell_block(), 0, st>>>(
+            L.g, L.phi[0], L.phi[1], L.phi[2], L.rhs[0], L.rhs[1], L.rhs[2], L.tmp[0], L.tmp[1], L.tmp[2],
+            L.diag[0], L.diag[1], L.diag[2], color, omega);
+        rc |= post(ctx);
+    });
+    return rc;
+}
+
+template <typename T>
+static int stag_smooths(fhd_ctx* ctx, StagLevel<T>& L, int count) {
+    const int dim = ctx->dim;
+    for (int m = 0; m < count; m++) {
+        if (ctx->p.stag_mg_smoother == 0) {
+            int rc = stag_smooth(ctx, L, 0);
+            if (rc) return rc;
+        } else {
+            for (int color = 1; color <= 2 * dim; color++) {
+                int rc = stag_smooth(ctx, L, color);
+                if (rc) return rc;
+            }
+        }
+    }
+    return 0;
+}
+
+template <typename T>
+static int stag_residual(fhd_ctx* ctx, StagLevel<T>& L) {
+    int rc = 0;
+    const StagOp<T> A = L.op();
+    with_dim_visc(ctx->dim, ctx->visc, [&](auto D, auto V) {
+        constexpr int DIM = decltype(D)::value, VISC = decltype(V)::value;
+        k_stag_apply<T, DIM, VISC><<<cell_grid(L.g), cell_block(), 0, ctx->stream>>>(
+            L.g, A, L.phi[0], L.phi[1], L.phi[2], L.tmp[0], L.tmp[1], L.tmp[2], L.rhs[0], L.rhs[1], L.rhs[2], 1);
+        rc |= post(ctx);
+    });
+    return rc;
+}
+
+template <typename T>
+static int stag_vcycle(fhd_ctx* ctx, Multigrid<T>& M) {
+    const int nl = (int)M.s.size();
+    const int dim = ctx->dim;
+    cudaStream_t st = ctx->stream;
+    for (int l = 1; l < nl; l++)
+        for (int c = 0; c < dim; c++) FHD_CUDA_TRY(cudaMemsetAsync(M.s[l].phi[c], 0, sizeof(T) * M.s[l].g.nc, st));
+    for (int l = 0; l < nl - 1; l++) {
+        StagLevel<T>& L = M.s[l];
+        StagLevel<T>& C = M.s[l + 1];
+        int rc = stag_smooths(ctx, L, ctx->p.stag_mg_nsmooths_down);
+        if (rc) return rc;
+        rc = stag_residual(ctx, L);
+        if (rc) return rc;
+        with_dim(dim, [&](auto D) {
+            constexpr int DIM = decltype(D)::value;
+            k_stag_restrict<T, DIM><<<cell_grid(C.g), cell_block(), 0, st>>>(L.g, C.g, L.tmp[0], L.tmp[1], L.tmp[2],
+                                                                           C.rhs[0], C.rhs[1], C.rhs[2], 0);
+            rc |= post(ctx);
+        });
+        if (rc) return rc;
+    }
+    int rc = stag_smooths(ctx, M.s[nl - 1], ctx->p.stag_mg_nsmooths_bottom);
+    if (rc) return rc;
+    for (int l = nl - 2; l >= 0; l--) {
+        StagLevel<T>& L = M.s[l];
+        StagLevel<T>& C = M.s[l + 1];
+        with_dim(dim, [&](auto D) {
+            constexpr int DIM = decltype(D)::value;
+            k_stag_prolong<T, DIM><<<cell_grid(L.g), cell_block(), 0, st>>>(L.g, C.g, L.phi[0], L.phi[1], L.phi[2],
+                                                                          C.phi[0], C.phi[1], C.phi[2]);
+            rc |= post(ctx);
+        });
+        if (rc) return rc;
+        rc = stag_smooths(ctx, L, ctx->p.stag_mg_nsmooths_up);
+        if (rc) return rc;
+    }
+    return 0;
+}
+
+template <typename T>
+static int maxabs_resid(fhd_ctx* ctx, StagLevel<T>& L, double* out);
+
+// max |a| per array, via sum-free reduction into host
+template <typename T>
+__global__ void __launch_bounds__(RED_THREADS) k_maxabs(i64 n, const T* a, RedSlot rs) {
+    double s = 0.0;
+    for (i64 f = blockIdx.x * (i64)blockDim.x + threadIdx.x; f < n; f += (i64)gridDim.x * blockDim.x)
+        s = fmax(s, fabs((double)a[f]));
+    // max-combine: reuse the sum tree on a monotone transform is not exact,
+    // so reduce the maxima explicitly
+    __shared__ double sh[RED_THREADS];
+    __shared__ bool last;
+    sh[threadIdx.x] = s;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) sh[threadIdx.x] = fmax(sh[threadIdx.x], sh[threadIdx.x + o]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        rs.partials[blockIdx.x] = sh[0];
+        __threadfence();
+        last = (atomicAdd(rs.counter, 1u) == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    if (threadIdx.x == 0) {
+        double m = 0.0;
+        for (int b = 0; b < (int)gridDim.x; b++) m = fmax(m, ((volatile double*)rs.partials)[b]);
+        *rs.out = m;
+        *rs.counter = 0u;
+    }
+}
+
+// stag_mg_solver (stag_mg_solver.f90:37-863) on level-0 phi/rhs of M
+template <typename T>
+static int stag_mg_run(fhd_ctx* ctx, Multigrid<T>& M) {
+    const int dim = ctx->dim;
+    const int maxv = ctx->p.stag_mg_max_vcycles;
+    StagLevel<T>& L0 = M.s[0];
+    const i64 nc = L0.g.nc;
+    double resid0[3] = {0, 0, 0};
+    if (maxv > 1) {
+        int rc = stag_residual(ctx, L0);
+        if (rc) return rc;
+        for (int c = 0; c < dim; c++) {
+            k_maxabs<T><<<flat_blocks(nc), RED_THREADS, 0, ctx->stream>>>(nc, L0.tmp[c], slot(ctx, S_NRM + c));
+            FHD_POST(ctx);
+        }
+        rc = sync_scalars(ctx, S_NRM, dim);
+        if (rc) return rc;
+        bool allzero = true, anyzero = false;
+        double rmax = 0;
+        for (int c = 0; c < dim; c++) {
+            resid0[c] = ctx->hscal[S_NRM + c];
+            allzero = allzero && resid0[c] == 0.0;
+            anyzero = anyzero || resid0[c] == 0.0;
+            rmax = fmax(rmax, resid0[c]);
+        }
+        if (allzero) return 0;
+        if (anyzero)
+            for (int c = 0; c < dim; c++) resid0[c] = rmax;
+    }
+    for (int vc = 1; vc <= maxv; vc++) {
+        int rc = stag_vcycle(ctx, M);
+        if (rc) return rc;
+        if (vc == maxv) break;
+        rc = stag_residual(ctx, L0);
+        if (rc) return rc;
+        for (int c = 0; c < dim; c++) {
+            k_maxabs<T><<<flat_blocks(nc), RED_THREADS, 0, ctx->stream>>>(nc, L0.tmp[c], slot(ctx, S_NRM + c));
+            FHD_POST(ctx);
+        }
+        rc = sync_scalars(ctx, S_NRM, dim);
+        if (rc) return rc;
+        bool done = true;
+        for (int c = 0; c < dim; c++) done = done && (ctx->hscal[S_NRM + c] / resid0[c] < ctx->p.stag_mg_rel_tol);
+        if (done) break;
+    }
+    ctx->vcycles += dim * maxv;
+    return 0;
+}
+
+// ---------------------------------------------------------------------
+// pressure multigrid (macproject.f90:34-316)
+// ---------------------------------------------------------------------
+template <typename T>
+static int cc_smooth(fhd_ctx* ctx, CCLevel<T>& C) {
+    cudaStream_t st = ctx->stream;
+    const CCOp<T> A = C.op();
+    int rc = 0;
+    for (int par = 0; par < 2; par++) {
+        with_dim(ctx->dim, [&](auto D) {
+            constexpr int DIM = decltype(D)::value;
+            if (all_even(C.g)) {
+                k_cc_gsrb<T, DIM><<<half_grid(C.g), cell_block(), 0, st>>>(C.g, A, C.phi, C.rhs, par);
+                rc |= post(ctx);
+            } else {
+                k_cc_color_corr<T, DIM><<<cell_grid(C.g), cell_block(), 0, st>>>(C.g, A, C.phi, C.rhs, C.tmp, par);
+                rc |= post(ctx);
+                k_cc_color_add<T><<<cell_grid(C.g), cell_block(), 0, st>>>(C.g, C.phi, C.tmp, par);
+                rc |= post(ctx);
+            }
+        });
+        if (rc) return rc;
+    }
+    return 0;
+}
+
+template <typename T>
+static int cc_vcycle(fhd_ctx* ctx, Multigrid<T>& M, int l) {
+    const int nl = (int)M.c.size();
+    CCLevel<T>& C = M.c[l];
+    if (l == nl - 1) {
+        for (int m = 0; m < ctx->p.mg_nsmooths_bottom; m++) {
+            int rc = cc_smooth(ctx, C);
+            if (rc) return rc;
+        }
+        return 0;
+    }
+    for (int m = 0; m < ctx->p.mg_nsmooths_down; m++) {
+        int rc = cc_smooth(ctx, C);
+        if (rc) return rc;
+    }
+    CCLevel<T>& D = M.c[l + 1];
+    int rc = 0;
+    with_dim(ctx->dim, [&](auto Dm) {
+        constexpr int DIM = decltype(Dm)::value;
+        k_cc_resid_restrict<T, DIM><<<cell_grid(D.g), cell_block(), 0, ctx->stream>>>(C.g, D.g, C.op(), C.phi, C.rhs,
+                                                                                     D.rhs);
+        rc |= post(ctx);
+    });
+    if (rc) return rc;
+    FHD_CUDA_TRY(cudaMemsetAsync(D.phi, 0, sizeof(T) * D.g.nc, ctx->stream));
+    rc = cc_vcycle(ctx, M, l + 1);
+    if (rc) return rc;
+    with_dim(ctx->dim, [&](auto Dm) {
+        constexpr int DIM = decltype(Dm)::value;
+        k_cc_prolong<T, DIM><<<cell_grid(C.g), cell_block(), 0, ctx->stream>>>(C.g, D.g, C.phi, D.phi);
+        rc |= post(ctx);
+    });
+    if (rc) return rc;
+    for (int m = 0; m < ctx->p.mg_nsmooths_up; m++) {
+        rc = cc_smooth(ctx, C);
+        if (rc) return rc;
+    }
+    return 0;
+}
+
+// Phi = 0, then mg_max_vcycles V-cycles on M.c[0].rhs
+template <typename T>
+static int cc_solve(fhd_ctx* ctx, Multigrid<T>& M) {
+    CCLevel<T>& C = M.c[0];
+    const i64 nc = C.g.nc;
+    FHD_CUDA_TRY(cudaMemsetAsync(C.phi, 0, sizeof(T) * nc, ctx->stream));
+    const int maxv = ctx->p.mg_max_vcycles;
+    double r0 = 1.0;
+    if (maxv > 1) {
+        k_maxabs<T><<<flat_blocks(nc), RED_THREADS, 0, ctx->stream>>>(nc, C.rhs, slot(ctx, S_NRM));
+        FHD_POST(ctx);
+        int rc = sync_scalars(ctx, S_NRM, 1);
+        if (rc) return rc;
+        r0 = ctx->hscal[S_NRM];
+        if (r0 == 0.0) return 0;
+    }
+    for (int vc = 1; vc <= maxv; vc++) {
+        int rc = cc_vcycle(ctx, M, 0);
+        if (rc) return rc;
+        if (vc == maxv) break;
+        with_dim(ctx->dim, [&](auto D) {
+            constexpr int DIM = decltype(D)::value;
+            k_cc_resid<T, DIM><<<cell_grid(C.g), cell_block(), 0, ctx->stream>>>(C.g, C.op(), C.phi, C.rhs, C.tmp);
+            rc |= post(ctx);
+        });
+        if (rc) return rc;
+        k_maxabs<T><<<flat_blocks(nc), RED_THREADS, 0, ctx->stream>>>(nc, C.tmp, slot(ctx, S_NRM));
+        FHD_POST(ctx);
+        rc = sync_scalars(ctx, S_NRM, 1);
+        if (rc) return rc;
+        if (ctx->hscal[S_NRM] <= fmax(ctx->p.mg_rel_tol * r0, ctx->p.mg_abs_tol)) break;
+    }
+    ctx->vcycles += maxv;
+    return 0;
+}
+
+// ---------------------------------------------------------------------
+// apply_precon (apply_precon.f90:29-475), visc_schur_approx = 0
+// ---------------------------------------------------------------------
+template <typename T>
+static int precon_T(fhd_ctx* ctx, CSVec<double> b, SVec<double> x) {
+    Multigrid<T>& M = mg_of<T>(ctx);
+    const int dim = ctx->dim;
+    const i64 nc = ctx->g0.nc;
+    const Grid g = ctx->g0;
+    cudaStream_t st = ctx->stream;
+    const int pt = ctx->p.precon_type, apt = pt < 0 ? -pt : pt;
+    const int av = ctx->visc < 0 ? -ctx->visc : ctx->visc;
+    const double theta = ctx->theta;
+    const bool fp64 = std::is_same<T, double>::value;
+    const int nb = flat_blocks(nc);
+    if (ctx->p.visc_schur_approx != 0 || apt < 1 || apt > 5) {
+        set_last_error("apply_precon: unsupported precon_type / visc_schur_approx");
+        return FHD_ERR_UNSUPPORTED;
+    }
+    StagLevel<T>& L0 = M.s[0];
+    // velocity unknowns of the multigrid: the FP64 output itself, or FP32
+    // work arrays in the mixed preconditioner
+    for (int c = 0; c < dim; c++) L0.phi[c] = fp64 ? (T*)x.c[c] : M.x_u[c];
+    for (int c = 0; c < dim; c++) FHD_CUDA_TRY(cudaMemsetAsync(L0.phi[c], 0, sizeof(T) * nc, st));
+    auto set_rhs_from_b = [&]() -> int {
+        for (int c = 0; c < dim; c++) {
+            if (fp64) {
+                L0.rhs[c] = (T*)b.c[c];
+            } else {
+                k_copy_conv<T, double><<<nb, 256, 0, st>>>(nc, M.b_u[c], b.c[c], 1.0);
+                FHD_POST(ctx);
+                L0.rhs[c] = M.b_u[c];
+            }
+        }
+        return 0;
+    };
+    auto phi_to_x = [&]() -> int {
+        if (fp64) return 0;
+        for (int c = 0; c < dim; c++) {
+            k_copy_conv<double, T><<<nb, 256, 0, st>>>(nc, x.c[c], L0.phi[c], 1.0);
+            FHD_POST(ctx);
+        }
+        return 0;
+    };
+    auto div_plus = [&](const double* bp) -> int {
+        int rc = 0;
+        with_dim(dim, [&](auto D) {
+            constexpr int DIM = decltype(D)::value;
+            k_div_plus<T, DIM><<<cell_grid(g), cell_block(), 0, st>>>(g, L0.phi[0], L0.phi[1], L0.phi[2], bp,
+                                                                    M.c[0].rhs, (T)(1.0 / g.dx));
+            rc |= post(ctx);
+        });
+        return rc;
+    };
+    auto schur = [&](int kind, int add_phi, int negate) -> int {
+        int rc = 0;
+        with_dim(dim, [&](auto D) {
+            constexpr int DIM = decltype(D)::value;
+            k_schur<T, DIM><<<cell_grid(g), cell_block(), 0, st>>>(g, M.c[0].op(), M.c[0].rhs, M.c[0].phi, ctx->beta,
+                                                                 ctx->gamma, theta, av, kind, add_phi, negate,
+                                                                 x.c[dim]);
+            rc |= post(ctx);
+        });
+        return rc;
+    };
+    // b_u - G x_p into the multigrid rhs (precon 3 and 5)
+    auto rhs_minus_grad_xp = [&]() -> int {
+        int rc = 0;
+        with_dim(dim, [&](auto D) {
+            constexpr int DIM = decltype(D)::value;
+            k_sub_grad_T<T, DIM><<<cell_grid(g), cell_block(), 0, st>>>(g, b.c[0], b.c[1], DIM == 3 ? b.c[2] : nullptr,
+                                                                      x.c[dim], M.b_u[0], M.b_u[1], M.b_u[2],
+                                                                      1.0 / g.dx);
+            rc |= post(ctx);
+        });
+        for (int c = 0; c < dim; c++) L0.rhs[c] = M.b_u[c];
+        return rc;
+    };
+    int rc = 0;
+    if (apt == 1) {
+        if ((rc = set_rhs_from_b())) return rc;
+        if ((rc = stag_mg_run(ctx, M))) return rc;
+        if ((rc = div_plus(b.c[dim]))) return rc;
+        if ((rc = cc_solve(ctx, M))) return rc;
+        with_dim(dim, [&](auto D) {
+            constexpr int DIM = decltype(D)::value;
+            k_sub_wgrad<T, DIM><<<cell_grid(g), cell_block(), 0, st>>>(
+                g, L0.phi[0], L0.phi[1], L0.phi[2], M.c[0].a[0], M.c[0].a[1], M.c[0].a[2], M.c[0].phi, x.c[0],
+                x.c[1], DIM == 3 ? x.c[2] : nullptr, (T)(1.0 / g.dx));
+            rc |= post(ctx);
+        });
+        if (rc) return rc;
+        const int kind = (pt == 1 || theta == 0.0) ? 0 : 1;
+        if ((rc = schur(kind, 1, 0))) return rc;
+    } else if (apt == 2 || apt == 5) {
+        if ((rc = set_rhs_from_b())) return rc;
+        if ((rc = stag_mg_run(ctx, M))) return rc;
+        if ((rc = div_plus(b.c[dim]))) return rc;
+        if (fabs(theta) > 0.0) {
+            if ((rc = cc_solve(ctx, M))) return rc;
+        }
+        if ((rc = schur(0, fabs(theta) > 0.0, (pt == -2 || pt == -5)))) return rc;
+        if (apt == 5) {
+            if ((rc = rhs_minus_grad_xp())) return rc;
+            if ((rc = stag_mg_run(ctx, M))) return rc;
+        }
+        if ((rc = phi_to_x())) return rc;
+    } else if (apt == 3) {
+        k_copy_conv<T, double><<<nb, 256, 0, st>>>(nc, M.c[0].rhs, b.c[dim], pt == -3 ? -1.0 : 1.0);
+        FHD_POST(ctx);
+        if (fabs(theta) > 0.0) {
+            if ((rc = cc_solve(ctx, M))) return rc;
+        }
+        if ((rc = schur(0, fabs(theta) > 0.0, 0))) return rc;
+        if ((rc = rhs_minus_grad_xp())) return rc;
+        if ((rc = stag_mg_run(ctx, M))) return rc;
+        if ((rc = phi_to_x())) return rc;
+    } else {  // 4
+        if ((rc = set_rhs_from_b())) return rc;
+        if ((rc = stag_mg_run(ctx, M))) return rc;
+        const bool use_phi = fabs(theta) > 0.0;
+        if (use_phi) {
+            k_copy_conv<T, double><<<nb, 256, 0, st>>>(nc, M.c[0].rhs, b.c[dim], 1.0);
+            FHD_POST(ctx);
+            if ((rc = cc_solve(ctx, M))) return rc;
+            // blockdiag kernel reads Phi in FP64: stage it through x_p
+            k_copy_conv<double, T><<<nb, 256, 0, st>>>(nc, x.c[dim], M.c[0].phi, 1.0);
+            FHD_POST(ctx);
+        }
+        k_schur_blockdiag<<<nb, 256, 0, st>>>(nc, b.c[dim], ctx->beta, ctx->gamma, x.c[dim], theta, use_phi ? 1 : 0,
+                                              av, pt, x.c[dim]);
+        FHD_POST(ctx);
+        if ((rc = phi_to_x())) return rc;
+    }
+    // null space: mean of p, and of u when theta_alpha = 0 (all walls are
+    // periodic here, so no no-slip wall exists) -- apply_precon.f90:429-460
+    k_sum<double><<<nb, RED_THREADS, 0, st>>>(nc, x.c[dim], slot(ctx, S_MEAN));
+    FHD_POST(ctx);
+    k_sub_mean<double><<<nb, 256, 0, st>>>(nc, x.c[dim], ctx->dscal + S_MEAN, (double)nc);
+    FHD_POST(ctx);
+    if (theta == 0.0) {
+        for (int c = 0; c < dim; c++) {
+            k_sum<double><<<nb, RED_THREADS, 0, st>>>(nc, x.c[c], slot(ctx, S_MEAN + 1 + c));
+            FHD_POST(ctx);
+            k_sub_mean<double><<<nb, 256, 0, st>>>(nc, x.c[c], ctx->dscal + S_MEAN + 1 + c, (double)nc);
+            FHD_POST(ctx);
+        }
+    }
+    return 0;
+}
+
+int precon(fhd_ctx* ctx, CSVec<double> b, SVec<double> x) {
+    if (ctx->prec == FHD_PREC_MIXED) return precon_T<float>(ctx, b, x);
+    return precon_T<double>(ctx, b, x);
+}
+
+int stag_mg_solve_dev(fhd_ctx* ctx, double* const phi[], const double* const rhs[]) {
+    const int dim = ctx->dim;
+    const i64 nc = ctx->g0.nc;
+    if (ctx->prec == FHD_PREC_MIXED) {
+        Multigrid<float>& M = ctx->mg32;
+        for (int c = 0; c < dim; c++) {
+            k_copy_conv<float, double><<<flat_blocks(nc), 256, 0, ctx->stream>>>(nc, M.x_u[c], phi[c], 1.0);
+            FHD_POST(ctx);
+            k_copy_conv<float, double><<<flat_blocks(nc), 256, 0, ctx->stream>>>(nc, M.b_u[c], rhs[c], 1.0);
+            FHD_POST(ctx);
+            M.s[0].phi[c] = M.x_u[c];
+            M.s[0].rhs[c] = M.b_u[c];
+        }
+        int rc = stag_mg_run(ctx, M);
+        if (rc) return rc;
+        for (int c = 0; c < dim; c++) {
+            k_copy_conv<double, float><<<flat_blocks(nc), 256, 0, ctx->stream>>>(nc, phi[c], M.x_u[c], 1.0);
+            FHD_POST(ctx);
+        }
+        return 0;
+    }
+    Multigrid<double>& M = ctx->mg64;
+    for (int c = 0; c < dim; c++) {
+        M.s[0].phi[c] = phi[c];
+        M.s[0].rhs[c] = (double*)rhs[c];
+    }
+    return stag_mg_run(ctx, M);
+}
+
+// ---------------------------------------------------------------------
+// apply_matrix (apply_matrix.f90:24-157), FP64 always
+// ---------------------------------------------------------------------
+int stokes_apply(fhd_ctx* ctx, CSVec<double> x, CSVec<double> rhs, SVec<double> out, int mode) {
+    StagOp<double> A;
+    for (int c = 0; c < 3; c++) {
+        A.alpha[c] = ctx->alpha_fc[c];
+        A.bed[c] = ctx->beta_ed[c];
+    }
+    A.alpha_scale = ctx->theta;
+    A.beta = ctx->beta;
+    A.gamma = ctx->gamma;
+    A.q = 1.0 / (ctx->dx * ctx->dx);
+    int rc = 0;
+    with_dim_visc(ctx->dim, ctx->visc, [&](auto D, auto V) {
+        constexpr int DIM = decltype(D)::value, VISC = decltype(V)::value;
+        k_stokes_apply<DIM, VISC><<<cell_grid(ctx->g0), cell_block(), 0, ctx->stream>>>(ctx->g0, A, x, rhs, out, mode,
+                                                                                      1.0 / ctx->dx);
+        rc |= post(ctx);
+    });
+    return rc;
+}
+
+int sync_scalars(fhd_ctx* ctx, int first, int count) {
+    FHD_CUDA_TRY(cudaMemcpyAsync(ctx->hscal + first, ctx->dscal + first, sizeof(double) * count,
+                                 cudaMemcpyDeviceToHost, ctx->stream));
+    FHD_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    return 0;
+}
+
+// ---------------------------------------------------------------------
+// gmres (gmres.f90:32-619)
+// ---------------------------------------------------------------------
+static SVec<double> svec(double* base, int dim, i64 nc) {
+    SVec<double> v;
+    for (int c = 0; c < 4; c++) v.c[c] = c <= dim ? base + (i64)c * nc : nullptr;
+    return v;
+}
+static CSVec<double> csv(SVec<double> v) {
+    CSVec<double> o;
+    for (int c = 0; c < 4; c++) o.c[c] = v.c[c];
+    return o;
+}
+
+static int wnorm2(fhd_ctx* ctx, CSVec<double> a, int slotid) {
+    const i64 nc = ctx->g0.nc;
+    const double wp = ctx->p.p_norm_weight;
+    k_sdot<double, double><<<flat_blocks(nc), RED_THREADS, 0, ctx->stream>>>(nc, ctx->dim + 1, a, a, wp * wp,
+                                                                          slot(ctx, slotid));
+    return post(ctx);
+}
+
+int gmres_dev(fhd_ctx* ctx, CSVec<double> b, SVec<double> x, double* norm_pre_rhs, fhd_solve_stats* stout) {
+    const int dim = ctx->dim, ncomp = dim + 1;
+    const i64 nc = ctx->g0.nc;
+    const fhd_gmres_params& p = ctx->p;
+    const int m = p.gmres_max_inner;
+    const double wp = p.p_norm_weight;
+    cudaStream_t st = ctx->stream;
+    const int nb = flat_blocks(nc);
+    const i64 vstride = (i64)ncomp * nc;
+    SVec<double> tmp = svec(ctx->tmp, dim, nc), r = svec(ctx->r, dim, nc), w = svec(ctx->w, dim, nc);
+    auto V = [&](int k) { return svec(ctx->V + (i64)k * vstride, dim, nc); };  // 0-based
+    fhd_solve_stats S;
+    memset(&S, 0, sizeof(S));
+    ctx->vcycles = 0;
+    int rc;
+    int status = 0;
+    // |M^-1 b|
+    if ((rc = precon(ctx, b, tmp))) return rc;
+    if ((rc = wnorm2(ctx, csv(tmp), S_NRM))) return rc;
+    if ((rc = wnorm2(ctx, b, S_NRM + 1))) return rc;
+    if ((rc = sync_scalars(ctx, S_NRM, 2))) return rc;
+    const double norm_pre_b = sqrt(ctx->hscal[S_NRM]);
+    const double norm_b = sqrt(ctx->hscal[S_NRM + 1]);
+    if (norm_pre_rhs) *norm_pre_rhs = norm_pre_b;
+    S.norm_b = norm_b;
+    S.norm_pre_b = norm_pre_b;
+    if (norm_b <= p.gmres_abs_tol) {
+        for (int c = 0; c <= dim; c++) FHD_CUDA_TRY(cudaMemsetAsync(x.c[c], 0, sizeof(double) * nc, st));
+        if (stout) *stout = S;
+        return 0;
+    }
+    std::vector<double> H((m + 2) * (m + 2), 0.0), cs(m + 2), sn(m + 2), s(m + 2), y(m + 2);
+    auto Hh = [&](int i, int j) -> double& { return H[i * (m + 2) + j]; };
+    int total_iter = 0, iter = 0, i_copy = 0;
+    double norm_resid = 0, norm_init_resid = 0, norm_resid_Stokes = 0, norm_init_Stokes = 0, norm_resid_est = 0;
+    for (;;) {
+        // tmp = b - A x
+        if ((rc = stokes_apply(ctx, csv(x), b, tmp, 1))) return rc;
+        if ((rc = wnorm2(ctx, csv(tmp), S_NRM))) return rc;
+        if ((rc = precon(ctx, csv(tmp), r))) return rc;
+        if ((rc = wnorm2(ctx, csv(r), S_NRM + 1))) return rc;
+        if ((rc = sync_scalars(ctx, S_NRM, 2))) return rc;
+        norm_resid_Stokes = sqrt(ctx->hscal[S_NRM]);
+        norm_resid = sqrt(ctx->hscal[S_NRM + 1]);
+        if (iter == 0) {
+            norm_init_Stokes = norm_resid_Stokes;
+            norm_init_resid = norm_resid;
+            norm_resid_est = norm_resid;
+        }
+        if (total_iter >= p.gmres_max_iter) {
+            status = FHD_WARN_NOT_CONVERGED_MAXITER;
+            break;
+        } else if (total_iter >= p.gmres_min_iter) {
+            if (norm_resid <= p.gmres_rel_tol * fmin(norm_pre_b, norm_init_resid)) {
+                if (norm_resid_Stokes >= 10 * p.gmres_rel_tol * fmin(norm_b, norm_init_Stokes))
+                    status = FHD_WARN_TRUE_RESID;
+                break;
+            } else if (norm_resid <= p.gmres_abs_tol) {
+                break;
+            }
+        }
+        if (iter >= p.gmres_max_outer) {
+            status = FHD_WARN_NOT_CONVERGED_OUTER;
+            break;
+        }
+        iter++;
+        k_scale_div<<<nb, 256, 0, st>>>(nc, ncomp, V(0), csv(r), norm_resid);
+        FHD_POST(ctx);
+        std::fill(s.begin(), s.end(), 0.0);
+        s[1] = norm_resid;
+        for (int i = 1; i <= m; i++) {
+            total_iter++;
+            i_copy = i;
+            if ((rc = stokes_apply(ctx, csv(V(i - 1)), csv(V(i - 1)), tmp, 0))) return rc;
+            if ((rc = precon(ctx, csv(tmp), w))) return rc;
+            // modified Gram-Schmidt with device-resident coefficients
+            for (int k = 1; k <= i; k++) {
+                CSVec<double> none;
+                for (int c = 0; c < 4; c++) none.c[c] = nullptr;
+                k_mgs<<<nb, RED_THREADS, 0, st>>>(nc, ncomp, w, k > 1 ? csv(V(k - 2)) : none,
+                                                  k > 1 ? ctx->dscal + S_H + k - 1 : nullptr, csv(V(k - 1)), wp * wp,
+                                                  slot(ctx, S_H + k));
+                FHD_POST(ctx);
+            }
+            {
+                CSVec<double> none;
+                for (int c = 0; c < 4; c++) none.c[c] = nullptr;
+                k_mgs<<<nb, RED_THREADS, 0, st>>>(nc, ncomp, w, csv(V(i - 1)), ctx->dscal + S_H + i, none, wp * wp,
+                                                  slot(ctx, S_NRM));
+                FHD_POST(ctx);
+            }
+            k_scale_by_norm<<<nb, 256, 0, st>>>(nc, ncomp, V(i), csv(w), ctx->dscal + S_NRM);
+            FHD_POST(ctx);
+            FHD_CUDA_TRY(cudaMemcpyAsync(ctx->hscal + S_H + 1, ctx->dscal + S_H + 1, sizeof(double) * i,
+                                         cudaMemcpyDeviceToHost, st));
+            if ((rc = sync_scalars(ctx, S_NRM, 1))) return rc;
+            for (int k = 1; k <= i; k++) Hh(k, i) = ctx->hscal[S_H + k];
+            Hh(i + 1, i) = sqrt(ctx->hscal[S_NRM]);
+            if (Hh(i + 1, i) == 0.0) {
+                set_last_error("gmres: error in orthogonalization");
+                return FHD_ERR_ORTHO_BREAKDOWN;
+            }
+            // least_squares + rotmat (gmres.f90:531-597)
+            for (int k = 1; k <= i - 1; k++) {
+                double t = cs[k] * Hh(k, i) + sn[k] * Hh(k + 1, i);
+                Hh(k + 1, i) = -sn[k] * Hh(k, i) + cs[k] * Hh(k + 1, i);
+                Hh(k, i) = t;
+            }
+            {
+                double a = Hh(i, i), bb = Hh(i + 1, i);
+                if (bb == 0.0) {
+                    cs[i] = 1.0;
+                    sn[i] = 0.0;
+                } else if (fabs(bb) > fabs(a)) {
+                    double t = a / bb;
+                    sn[i] = 1.0 / sqrt(1.0 + t * t);
+                    cs[i] = t * sn[i];
+                } else {
+                    double t = bb / a;
+                    cs[i] = 1.0 / sqrt(1.0 + t * t);
+                    sn[i] = t * cs[i];
+                }
+                double t = cs[i] * s[i];
+                s[i + 1] = -sn[i] * s[i];
+                s[i] = t;
+                Hh(i, i) = cs[i] * Hh(i, i) + sn[i] * Hh(i + 1, i);
+                Hh(i + 1, i) = 0.0;
+            }
+            norm_resid_est = fabs(s[i + 1]);
+            if (total_iter >= p.gmres_max_iter) break;
+            else if (total_iter >= p.gmres_min_iter) {
+                if (norm_resid_est <= p.gmres_rel_tol * fmin(norm_pre_b, norm_init_resid) ||
+                    norm_resid_est <= p.gmres_abs_tol)
+                    break;
+            }
+        }
+        // SolveUTriangular (gmres.f90:599-619) and update_sol
+        {
+            const int k = i_copy - 1;
+            y[k + 1] = s[k + 1] / Hh(k + 1, k + 1);
+            for (int ii = k; ii >= 1; ii--) {
+                double acc = 0.0;
+                for (int jj = ii + 1; jj <= k + 1; jj++) acc += Hh(ii, jj) * y[jj];
+                y[ii] = (s[ii] - acc) / Hh(ii, ii);
+            }
+            for (int it = 1; it <= i_copy; it++) ctx->hscal[S_Y + it - 1] = y[it];
+            FHD_CUDA_TRY(cudaMemcpyAsync(ctx->dscal + S_Y, ctx->hscal + S_Y, sizeof(double) * i_copy,
+                                         cudaMemcpyHostToDevice, st));
+            k_update_sol<<<nb, 256, 0, st>>>(nc, ncomp, x, ctx->V, vstride, ctx->dscal + S_Y, i_copy);
+            FHD_POST(ctx);
+            // the staged y must not be overwritten before the copy ran
+            FHD_CUDA_TRY(cudaStreamSynchronize(st));
+        }
+    }
+    S.outer_iters = iter;
+    S.total_iters = total_iter;
+    S.vcycles = ctx->vcycles;
+    S.status = status;
+    S.norm_init_resid = norm_init_resid;
+    S.norm_resid = norm_resid;
+    S.norm_resid_Stokes = norm_resid_Stokes;
+    S.norm_init_Stokes = norm_init_Stokes;
+    S.norm_resid_est = norm_resid_est;
+    if (stout) *stout = S;
+    return status;
+}
+
+}  // namespace fhd
+
+using namespace fhd;
+
+// =====================================================================
+// C ABI: context and device-pointer entry points
+// =====================================================================
+extern "C" {
+
+void fhd_gmres_params_default(fhd_gmres_params* p) {
+    // probin_gmres_init defaults (probin_gmres.f90:122-163)
+    memset(p, 0, sizeof(*p));
+    p->precon_type = 1;
+    p->visc_schur_approx = 0;
+    p->p_norm_weight = 1.0;
+    p->scale_factor = 1.0;
+    p->mg_verbose = 0;
+    p->cg_verbose = 0;
+    p->mg_max_vcycles = 1;
+    p->mg_minwidth = 2;
+    p->mg_bottom_solver = 4;
+    p->mg_nsmooths_down = 2;
+    p->mg_nsmooths_up = 2;
+    p->mg_nsmooths_bottom = 8;
+    p->mg_max_bottom_nlevels = 10;
+    p->mg_rel_tol = 1e-9;
+    p->mg_abs_tol = 1e-14;
+    p->stag_mg_verbosity = 0;
+    p->stag_mg_max_vcycles = 1;
+    p->stag_mg_minwidth = 2;
+    p->stag_mg_bottom_solver = 4;
+    p->stag_mg_nsmooths_down = 2;
+    p->stag_mg_nsmooths_up = 2;
+    p->stag_mg_nsmooths_bottom = 8;
+    p->stag_mg_max_bottom_nlevels = 10;
+    p->stag_mg_omega = 1.0;
+    p->stag_mg_smoother = 1;
+    p->stag_mg_rel_tol = 1e-9;
+    p->gmres_rel_tol = 1e-9;
+    p->gmres_abs_tol = 0.0;
+    p->gmres_verbose = 1;
+    p->gmres_max_outer = 20;
+    p->gmres_max_inner = 5;
+    p->gmres_max_iter = 100;
+    p->gmres_min_iter = 1;
+    p->gmres_spatial_order = 2;
+}
+
+const char* fhd_status_string(int s) {
+    switch (s) {
+        case FHD_OK: return "ok";
+        case FHD_WARN_NOT_CONVERGED_MAXITER: return "GMRES did not converge in max number of total inner iterations";
+        case FHD_WARN_NOT_CONVERGED_OUTER: return "GMRES did not converge in max number of outer iterations";
+        case FHD_WARN_TRUE_RESID: return "gmres may not have converged (true residual above tolerance)";
+        case FHD_ERR_BAD_ARG: return "bad argument";
+        case FHD_ERR_BAD_GHOSTS: return "x_u and x_p need at least 1 ghost cell";
+        case FHD_ERR_DX_NOT_ISOTROPIC: return "only dx=dy(=dz) is supported";
+        case FHD_ERR_ORTHO_BREAKDOWN: return "gmres: error in orthogonalization";
+        case FHD_ERR_UNSUPPORTED: return "unsupported option";
+        case FHD_ERR_NONFINITE: return "non-finite value";
+        case FHD_ERR_OOM: return "out of device memory";
+        case FHD_ERR_CUDA: return g_last_error.empty() ? "CUDA error" : g_last_error.c_str();
+        case FHD_ERR_NO_DEVICE: return "no CUDA device";
+    }
+    return "unknown status";
+}
+
+const char* fhd_last_error(void) { return g_last_error.c_str(); }
+
+int fhd_ctx_create(int dim, const int n_cells[3], const double dx[3], int visc_type, const fhd_gmres_params* params,
+                   int precision_mode, fhd_ctx** out) {
+    if (!out || !n_cells || !dx || (dim != 2 && dim != 3)) return FHD_ERR_BAD_ARG;
+    *out = nullptr;
+    if (visc_type == 0 || visc_type < -3 || visc_type > 3) return FHD_ERR_BAD_ARG;
+    for (int d = 0; d < dim; d++)
+        if (n_cells[d] < 2) return FHD_ERR_BAD_ARG;
+    for (int d = 1; d < dim; d++)
+        if (dx[d] >= (1.0 + 1e-12) * dx[0] || dx[d] <= (1.0 - 1e-12) * dx[0]) return FHD_ERR_DX_NOT_ISOTROPIC;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return FHD_ERR_NO_DEVICE;
+    fhd_ctx* c = new fhd_ctx();
+    c->dim = dim;
+    for (int d = 0; d < 3; d++) c->n[d] = (d < dim) ? n_cells[d] : 1;
+    c->dx = dx[0];
+    c->visc = visc_type;
+    c->prec = precision_mode == FHD_PREC_MIXED ? FHD_PREC_MIXED : FHD_PREC_FP64;
+    if (params) c->p = *params;
+    else fhd_gmres_params_default(&c->p);
+    if (c->p.gmres_spatial_order != 2 || c->p.gmres_max_inner < 1 || c->p.gmres_max_inner > 60) {
+        delete c;
+        return FHD_ERR_UNSUPPORTED;
+    }
+    c->m = c->p.gmres_max_inner;
+    c->g0 = make_grid(dim, c->n, c->dx);
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete c;
+        return FHD_ERR_CUDA;
+    }
+    c->own = c->stream;
+    int rc = (c->prec == FHD_PREC_MIXED) ? build_mg(c, c->mg32) : build_mg(c, c->mg64);
+    const i64 nc = c->g0.nc;
+    const i64 sv = (i64)(dim + 1) * nc;
+    if (!rc) {
+        c->V = c->arena.alloc<double>(sv * (c->m + 1));
+        c->r = c->arena.alloc<double>(sv);
+        c->w = c->arena.alloc<double>(sv);
+        c->tmp = c->arena.alloc<double>(sv);
+        c->xs = c->arena.alloc<double>(sv);
+        c->red_partials = c->arena.alloc<double>(RED_MAX_BLOCKS);
+        c->red_counter = (unsigned*)c->arena.alloc<double>(1);
+        c->dscal = c->arena.alloc<double>(NSCAL);
+        if (!c->V || !c->r || !c->w || !c->tmp || !c->xs || !c->red_partials || !c->red_counter || !c->dscal)
+            rc = FHD_ERR_OOM;
+    }
+    if (!rc && cudaMallocHost((void**)&c->hscal, sizeof(double) * NSCAL) != cudaSuccess) rc = FHD_ERR_OOM;
+    if (!rc && cudaMemsetAsync(c->red_counter, 0, sizeof(double), c->stream) != cudaSuccess) rc = FHD_ERR_CUDA;
+    if (!rc && cudaStreamSynchronize(c->stream) != cudaSuccess) rc = FHD_ERR_CUDA;
+    if (rc) {
+        fhd_ctx_destroy(c);
+        return rc;
+    }
+    *out = c;
+    return FHD_OK;
+}
+
+void fhd_host_path_release(fhd_ctx* ctx);
+
+int fhd_ctx_destroy(fhd_ctx* c) {
+    if (!c) return FHD_OK;
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    fhd_host_path_release(c);
+    c->arena.release();
+    if (c->hscal) cudaFreeHost(c->hscal);
+    if (c->own) cudaStreamDestroy(c->own);
+    delete c;
+    return FHD_OK;
+}
+
+void* fhd_ctx_stream(fhd_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
+int fhd_ctx_set_stream(fhd_ctx* c, void* s) {
+    if (!c) return FHD_ERR_BAD_ARG;
+    c->stream = s ? (cudaStream_t)s : c->own;
+    return FHD_OK;
+}
+
+long long fhd_ctx_kernel_launches(fhd_ctx* c) { return c ? c->launches : 0; }
+
+unsigned long long fhd_ctx_device_bytes(fhd_ctx* c) { return c ? (unsigned long long)c->arena.bytes : 0ull; }
+
+static int check_ptrs(fhd_ctx* ctx, const void* const* a, int n) {
+    if (!ctx) return FHD_ERR_BAD_ARG;
+    if (!a) return FHD_ERR_BAD_ARG;
+    for (int i = 0; i < n; i++)
+        if (!a[i]) return FHD_ERR_BAD_ARG;
+    return 0;
+}
+
+static int nE_of(fhd_ctx* c) { return c->dim == 2 ? 1 : 3; }
+
+static int finish(fhd_ctx* ctx, int rc) {
+    if (rc < 0) return rc;
+    if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
+        set_last_error(cudaGetErrorString(cudaGetLastError()));
+        return FHD_ERR_CUDA;
+    }
+    return rc;
+}
+
+int fhd_dev_apply_matrix(fhd_ctx* ctx, double* const b_u[], double* b_p, const double* const x_u[],
+                         const double* x_p, const double* const alpha_fc[], const double* beta,
+                         const double* const beta_ed[], const double* gamma, double theta_alpha) {
+    int rc = check_ptrs(ctx, (const void* const*)b_u, ctx ? ctx->dim : 0);
+    if (!rc) rc = check_ptrs(ctx, (const void* const*)x_u, ctx->dim);
+    if (!rc) rc = check_ptrs(ctx, (const void* const*)alpha_fc, ctx->dim);
+    if (!rc) rc = check_ptrs(ctx, (const void* const*)beta_ed, nE_of(ctx));
+    if (!rc && (!b_p || !x_p || !beta || !gamma)) rc = FHD_ERR_BAD_ARG;
+    if (rc) return rc;
+    for (int c = 0; c < 3; c++) ctx->alpha_fc[c] = c < ctx->dim ? alpha_fc[c] : nullptr;
+    for (int e = 0; e < 3; e++) ctx->beta_ed[e] = e < nE_of(ctx) ? beta_ed[e] : nullptr;
+    ctx->beta = beta;
+    ctx->gamma = gamma;
+    ctx->theta = theta_alpha;
+    CSVec<double> x;
+    SVec<double> o;
+    for (int c = 0; c < 4; c++) { x.c[c] = nullptr; o.c[c] = nullptr; }
+    for (int c = 0; c < ctx->dim; c++) { x.c[c] = x_u[c]; o.c[c] = b_u[c]; }
+    x.c[ctx->dim] = x_p;
+    o.c[ctx->dim] = b_p;
+    return finish(ctx, stokes_apply(ctx, x, x, o, 0));
+}
+
+int fhd_dev_apply_precon(fhd_ctx* ctx, const double* const b_u[], const double* b_p, double* const x_u[],
+                         double* x_p, const double* const alpha_fc[], const double* beta,
+                         const double* const beta_ed[], const double* gamma, double theta_alpha) {
+    int rc = check_ptrs(ctx, (const void* const*)b_u, ctx ? ctx->dim : 0);
+    if (!rc) rc = check_ptrs(ctx, (const void* const*)x_u, ctx->dim);
+    if (!rc) rc = check_ptrs(ctx, (const void* const*)alpha_fc, ctx->dim);
+    if (!rc) rc = check_ptrs(ctx, (const void* const*)beta_ed, nE_of(ctx));
+    if (!rc && (!b_p || !x_p || !beta || !gamma)) rc = FHD_ERR_BAD_ARG;
+    if (rc) return rc;
+    rc = prepare(ctx, alpha_fc, beta, beta_ed, gamma, theta_alpha);
+    if (rc) return rc;
+    CSVec<double> b;
+    SVec<double> x;
+    for (int c = 0; c < 4; c++) { b.c[c] = nullptr; x.c[c] = nullptr; }
+    for (int c = 0; c < ctx->dim; c++) { b.c[c] = b_u[c]; x.c[c] = x_u[c]; }
+    b.c[ctx->dim] = b_p;
+    x.c[ctx->dim] = x_p;
+    return finish(ctx, precon(ctx, b, x));
+}
+
+int fhd_dev_stag_mg_solver(fhd_ctx* ctx, const double* const alpha_fc[], const double* beta,
+                           const double* const beta_ed[], const double* gamma, double theta_alpha,
+                           double* const phi[], const double* const rhs[]) {
+    int rc = check_ptrs(ctx, (const void* const*)phi, ctx ? ctx->dim : 0);
+    if (!rc) rc = check_ptrs(ctx, (const void* const*)rhs, ctx->dim);
+    if (!rc) rc = check_ptrs(ctx, (const void* const*)alpha_fc, ctx->dim);
+    if (!rc) rc = check_ptrs(ctx, (const void* const*)beta_ed, nE_of(ctx));
+    if (!rc && (!beta || !gamma)) rc = FHD_ERR_BAD_ARG;
+    if (rc) return rc;
+    rc = prepare(ctx, alpha_fc, beta, beta_ed, gamma, theta_alpha);
+    if (rc) return rc;
+    return finish(ctx, stag_mg_solve_dev(ctx, phi, rhs));
+}
+
+int fhd_dev_gmres(fhd_ctx* ctx, const double* const b_u[], const double* b_p, double* const x_u[], double* x_p,
+                  const double* const alpha_fc[], const double* beta, const double* const beta_ed[],
+                  const double* gamma, double theta_alpha, double* norm_pre_rhs, fhd_solve_stats* stats) {
+    int rc = check_ptrs(ctx, (const void* const*)b_u, ctx ? ctx->dim : 0);
+    if (!rc) rc = check_ptrs(ctx, (const void* const*)x_u, ctx->dim);
+    if (!rc) rc = check_ptrs(ctx, (const void* const*)alpha_fc, ctx->dim);
+    if (!rc) rc = check_ptrs(ctx, (const void* const*)beta_ed, nE_of(ctx));
+    if (!rc && (!b_p || !x_p || !beta || !gamma)) rc = FHD_ERR_BAD_ARG;
+    if (rc) return rc;
+    if (ctx->p.scale_factor != 1.0) {
+        set_last_error("gmres: scale_factor != 1 is not supported");
+        return FHD_ERR_UNSUPPORTED;
+    }
+    rc = prepare(ctx, alpha_fc, beta, beta_ed, gamma, theta_alpha);
+    if (rc) return rc;
+    CSVec<double> b;
+    SVec<double> x;
+    for (int c = 0; c < 4; c++) { b.c[c] = nullptr; x.c[c] = nullptr; }
+    for (int c = 0; c < ctx->dim; c++) { b.c[c] = b_u[c]; x.c[c] = x_u[c]; }
+    b.c[ctx->dim] = b_p;
+    x.c[ctx->dim] = x_p;
+    return finish(ctx, gmres_dev(ctx, b, x, norm_pre_rhs, stats));
+}
+
+}  // extern "C"

@@ -1,0 +1,232 @@
+// fhd_solver.cuh -- host-side objects of the solver: the context, the
+// multigrid hierarchies and the launch helpers shared by the .cu files.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <string>
+#include <type_traits>
+#include <vector>
+
+#include "../../include/fhd_b200.h"
+#include "fhd_vec.cuh"
+
+namespace fhd {
+
+#define FHD_CUDA_TRY(x)                                                                       \
+    do {                                                                                      \
+        cudaError_t e_ = (x);                                                                 \
+        if (e_ != cudaSuccess) {                                                              \
+            fhd::set_last_error(std::string(#x) + ": " + cudaGetErrorString(e_));              \
+            return FHD_ERR_CUDA;                                                              \
+        }                                                                                     \
+    } while (0)
+
+void set_last_error(const std::string& s);
+
+inline dim3 cell_block() { return dim3(32, 8, 1); }
+inline dim3 cell_grid(const Grid& g) { return dim3((g.n[0] + 31) / 32, (g.n[1] + 7) / 8, g.n[2]); }
+inline dim3 half_grid(const Grid& g) { return dim3(((g.n[0] + 1) / 2 + 31) / 32, (g.n[1] + 7) / 8, g.n[2]); }
+inline int flat_blocks(i64 n) {
+    i64 b = (n + 255) / 256;
+    return (int)(b < RED_MAX_BLOCKS ? (b < 1 ? 1 : b) : RED_MAX_BLOCKS);
+}
+
+inline Grid make_grid(int dim, const int n[3], double dx) {
+    Grid g;
+    g.dim = dim;
+    g.n[0] = n[0];
+    g.n[1] = n[1];
+    g.n[2] = dim == 3 ? n[2] : 1;
+    g.nc = (i64)g.n[0] * g.n[1] * g.n[2];
+    g.dx = dx;
+    return g;
+}
+
+inline Grid coarsen(const Grid& g) {
+    int n[3] = {g.n[0] / 2, g.n[1] / 2, g.dim == 3 ? g.n[2] / 2 : 1};
+    return make_grid(g.dim, n, g.dx * 2.0);
+}
+
+inline bool all_even(const Grid& g) {
+    for (int d = 0; d < g.dim; d++)
+        if (g.n[d] & 1) return false;
+    return true;
+}
+
+int nlevs_mg(const Grid& g, int minwidth);
+
+// compile-time dispatch on (dim, visc_type)
+template <class F>
+inline void with_dim_visc(int dim, int visc, F&& f) {
+    using std::integral_constant;
+#define FHD_V(D, V) f(integral_constant<int, D>(), integral_constant<int, V>())
+    if (dim == 2) {
+        switch (visc) {
+            case -3: FHD_V(2, -3); break;
+            case -2: FHD_V(2, -2); break;
+            case -1: FHD_V(2, -1); break;
+            case 1: FHD_V(2, 1); break;
+            case 2: FHD_V(2, 2); break;
+            default: FHD_V(2, 3); break;
+        }
+    } else {
+        switch (visc) {
+            case -3: FHD_V(3, -3); break;
+            case -2: FHD_V(3, -2); break;
+            case -1: FHD_V(3, -1); break;
+            case 1: FHD_V(3, 1); break;
+            case 2: FHD_V(3, 2); break;
+            default: FHD_V(3, 3); break;
+        }
+    }
+#undef FHD_V
+}
+
+template <class F>
+inline void with_dim(int dim, F&& f) {
+    if (dim == 2) f(std::integral_constant<int, 2>());
+    else f(std::integral_constant<int, 3>());
+}
+
+
+
+struct fhd_ctx_impl;
+
+// device allocation owned by a context (freed at destroy)
+struct Arena {
+    std::vector<void*> blocks;
+    size_t bytes = 0;
+    template <typename T>
+    T* alloc(i64 n) {
+        void* p = nullptr;
+        if (n <= 0) n = 1;
+        if (cudaMalloc(&p, (size_t)n * sizeof(T)) != cudaSuccess) return nullptr;
+        blocks.push_back(p);
+        bytes += (size_t)n * sizeof(T);
+        return (T*)p;
+    }
+    void release() {
+        for (void* p : blocks) cudaFree(p);
+        blocks.clear();
+        bytes = 0;
+    }
+};
+
+template <typename T>
+struct StagLevel {
+    Grid g;
+    T* alpha[3] = {nullptr, nullptr, nullptr};  // owned on coarse levels
+    T alpha_scale = T(1);
+    const T* beta = nullptr;
+    const T* gamma = nullptr;
+    const T* bed[3] = {nullptr, nullptr, nullptr};
+    T* own_beta = nullptr;
+    T* own_gamma = nullptr;
+    T* own_bed[3] = {nullptr, nullptr, nullptr};
+    T* own_alpha0[3] = {nullptr, nullptr, nullptr};  // FP32 copy on level 0
+    T* phi[3] = {nullptr, nullptr, nullptr};
+    T* rhs[3] = {nullptr, nullptr, nullptr};
+    T* tmp[3] = {nullptr, nullptr, nullptr};   // residual / L phi
+    T* diag[3] = {nullptr, nullptr, nullptr};  // two-pass smoother
+    StagOp<T> op() const {
+        StagOp<T> A;
+        for (int c = 0; c < 3; c++) { A.alpha[c] = alpha[c]; A.bed[c] = bed[c]; }
+        A.alpha_scale = alpha_scale;
+        A.beta = beta;
+        A.gamma = gamma;
+        A.q = T(1.0 / (g.dx * g.dx));
+        return A;
+    }
+};
+
+template <typename T>
+struct CCLevel {
+    Grid g;
+    T* a[3] = {nullptr, nullptr, nullptr};
+    T* phi = nullptr;
+    T* rhs = nullptr;
+    T* tmp = nullptr;
+    CCOp<T> op() const {
+        CCOp<T> A;
+        for (int c = 0; c < 3; c++) A.a[c] = a[c];
+        A.q = T(1.0 / (g.dx * g.dx));
+        return A;
+    }
+};
+
+template <typename T>
+struct Multigrid {
+    std::vector<StagLevel<T>> s;
+    std::vector<CCLevel<T>> c;
+    // preconditioner work arrays at the finest level, precision T
+    T* x_u[3] = {nullptr, nullptr, nullptr};
+    T* b_u[3] = {nullptr, nullptr, nullptr};
+    T* mac_rhs = nullptr;
+};
+
+}  // namespace fhd
+
+struct fhd_ctx {
+    int dim = 2;
+    int n[3] = {1, 1, 1};
+    double dx = 1.0;
+    int visc = 1;
+    int prec = FHD_PREC_FP64;
+    fhd_gmres_params p;
+    fhd::Grid g0;
+    cudaStream_t stream = nullptr;  // stream the context launches on
+    cudaStream_t own = nullptr;     // stream created by the context
+    long long launches = 0;
+    int vcycles = 0;
+    fhd::Arena arena;
+    fhd::Multigrid<double> mg64;
+    fhd::Multigrid<float> mg32;
+    // prepared coefficients (per gmres / per standalone call)
+    const double* alpha_fc[3] = {nullptr, nullptr, nullptr};
+    const double* beta = nullptr;
+    const double* beta_ed[3] = {nullptr, nullptr, nullptr};
+    const double* gamma = nullptr;
+    double theta = 0.0;
+    // FP64 Stokes work vectors (contiguous: dim velocity comps then p)
+    double* V = nullptr;  // (m+1) vectors
+    double* r = nullptr;
+    double* w = nullptr;
+    double* tmp = nullptr;
+    double* xs = nullptr;  // solution copy for the host-fab path
+    double* scratch_fc[3] = {nullptr, nullptr, nullptr};
+    // reductions
+    double* red_partials = nullptr;
+    unsigned* red_counter = nullptr;
+    double* dscal = nullptr;  // device scalars
+    double* hscal = nullptr;  // pinned host mirror
+    int m = 5;
+    // inertial-step work arrays (allocated on the first step)
+    bool step_ready = false;
+    double* sb[64] = {nullptr};
+};
+
+namespace fhd {
+constexpr int NSCAL = 256;
+// scalar slots
+constexpr int S_H = 0;        // H column, 1..m+1
+constexpr int S_NRM = 128;    // norm squares
+constexpr int S_MEAN = 140;   // mean sums
+constexpr int S_Y = 160;      // least-squares y (m <= 64)
+
+inline RedSlot slot(fhd_ctx* c, int i) {
+    RedSlot r;
+    r.partials = c->red_partials + (size_t)i * 0;  // partials shared: reductions are stream-ordered
+    r.counter = c->red_counter;
+    r.out = c->dscal + i;
+    return r;
+}
+
+int precon(fhd_ctx* ctx, CSVec<double> b, SVec<double> x);
+int stokes_apply(fhd_ctx* ctx, CSVec<double> x, CSVec<double> rhs, SVec<double> out, int mode);
+int prepare(fhd_ctx* ctx, const double* const alpha_fc[], const double* beta, const double* const beta_ed[],
+            const double* gamma, double theta);
+int stag_mg_solve_dev(fhd_ctx* ctx, double* const phi[], const double* const rhs[]);
+int gmres_dev(fhd_ctx* ctx, CSVec<double> b, SVec<double> x, double* norm_pre_rhs, fhd_solve_stats* st);
+int sync_scalars(fhd_ctx* ctx, int first, int count);
+}  // namespace fhd

@@ -1,0 +1,524 @@
+// fhd_step.cu -- stochastic momentum flux divergence and the device-resident
+// inertial predictor-corrector step of a single-species fluid.
+//
+// stochastic_m_fluxdiv.f90:42-602 (periodic, filtering_width = 0) and
+// advance_timestep_inertial.f90:45-923 (nspecies = 1, centred advection,
+// no gravity, periodic walls).
+#include <cmath>
+#include <cstring>
+
+#include "fhd_solver.cuh"
+
+namespace fhd {
+
+struct StochArgs {
+    const double* Wcc[4 * 3];  // n_rngs * dim
+    const double* Wed[4 * 6];  // n_rngs * 2 * nE
+    double wts[4];
+    int n_rngs;
+    const double* eta;
+    const double* eta_ed[3];
+    const double* T;
+    const double* T_ed[3];
+    double variance;
+    double dxinv;
+};
+
+// scaled random stress at a cell (component c) or on an edge (edge set e,
+// component comp): variance * (sum_r w_r W_r) * sqrt(eta T)
+// (stochastic_m_fluxdiv.f90:115-125, 137, 280-361)
+template <typename T>
+__device__ __forceinline__ T stoch_cc(const StochArgs& a, int dim, int c, i64 f) {
+    T s = T(0);
+    for (int r = 0; r < a.n_rngs; r++) s = s + (T)a.wts[r] * (T)ld(a.Wcc[r * dim + c], f);
+    return ((T)a.variance * s) * (T)sqrt((T)ld(a.eta, f) * (T)ld(a.T, f));
+}
+template <typename T>
+__device__ __forceinline__ T stoch_ed(const StochArgs& a, int nE, int e, int comp, i64 f) {
+    T s = T(0);
+    for (int r = 0; r < a.n_rngs; r++) s = s + (T)a.wts[r] * (T)ld(a.Wed[r * 2 * nE + 2 * e + comp], f);
+    return ((T)a.variance * s) * (T)sqrt((T)ld(a.eta_ed[e], f) * (T)ld(a.T_ed[e], f));
+}
+
+// divergence of the scaled random stress onto the faces (stoch_m_force_2d /
+// _3d, stochastic_m_fluxdiv.f90:453-600), overwrite or increment.
+// T is the arithmetic precision (double, or float in the mixed mode).
+template <typename T, int DIM>
+__global__ void __launch_bounds__(256) k_stoch_m(Grid g, StochArgs a, double* o0, double* o1, double* o2,
+                                                 int increment) {
+    Cell P;
+    if (!cell_of_thread(g, P)) return;
+    const i64 f = P.id(0, 0, 0);
+    const T dxi = (T)a.dxinv;
+    T dv[3];
+    if constexpr (DIM == 2) {
+        dv[0] = (stoch_cc<T>(a, 2, 0, f) - stoch_cc<T>(a, 2, 0, P.id(-1, 0, 0))) * dxi +
+                (stoch_ed<T>(a, 1, 0, 0, P.id(0, 1, 0)) - stoch_ed<T>(a, 1, 0, 0, f)) * dxi;
+        dv[1] = (stoch_ed<T>(a, 1, 0, 1, P.id(1, 0, 0)) - stoch_ed<T>(a, 1, 0, 1, f)) * dxi +
+                (stoch_cc<T>(a, 2, 1, f) - stoch_cc<T>(a, 2, 1, P.id(0, -1, 0))) * dxi;
+    } else {
+        dv[0] = (stoch_cc<T>(a, 3, 0, f) - stoch_cc<T>(a, 3, 0, P.id(-1, 0, 0))) * dxi +
+                (stoch_ed<T>(a, 3, 0, 0, P.id(0, 1, 0)) - stoch_ed<T>(a, 3, 0, 0, f)) * dxi +
+                (stoch_ed<T>(a, 3, 1, 0, P.id(0, 0, 1)) - stoch_ed<T>(a, 3, 1, 0, f)) * dxi;
+        dv[1] = (stoch_ed<T>(a, 3, 0, 1, P.id(1, 0, 0)) - stoch_ed<T>(a, 3, 0, 1, f)) * dxi +
+                (stoch_cc<T>(a, 3, 1, f) - stoch_cc<T>(a, 3, 1, P.id(0, -1, 0))) * dxi +
+                (stoch_ed<T>(a, 3, 2, 0, P.id(0, 0, 1)) - stoch_ed<T>(a, 3, 2, 0, f)) * dxi;
+        dv[2] = (stoch_ed<T>(a, 3, 1, 1, P.id(1, 0, 0)) - stoch_ed<T>(a, 3, 1, 1, f)) * dxi +
+                (stoch_ed<T>(a, 3, 2, 1, P.id(0, 1, 0)) - stoch_ed<T>(a, 3, 2, 1, f)) * dxi +
+                (stoch_cc<T>(a, 3, 2, f) - stoch_cc<T>(a, 3, 2, P.id(0, 0, -1))) * dxi;
+    }
+    double* o[3] = {o0, o1, o2};
+#pragma unroll
+    for (int c = 0; c < DIM; c++) o[c][f] = increment ? o[c][f] + (double)dv[c] : (double)dv[c];
+}
+
+int stoch_launch(fhd_ctx* ctx, const fhd_stoch_params* sp, double* const force[], int increment, const double* eta,
+                 const double* const eta_ed[], const double* T, const double* const T_ed[], double dt,
+                 const double* weights, int n_rngs, const double* const W_cc[], const double* const W_ed[]) {
+    const int dim = ctx->dim, nE = dim == 2 ? 1 : 3;
+    if (n_rngs < 1 || n_rngs > 4 || sp->filtering_width != 0) {
+        set_last_error("stochastic_m_fluxdiv: n_rngs must be 1..4 and filtering_width 0");
+        return FHD_ERR_UNSUPPORTED;
+    }
+    StochArgs a;
+    memset(&a, 0, sizeof(a));
+    for (int i = 0; i < n_rngs * dim; i++) a.Wcc[i] = W_cc[i];
+    for (int i = 0; i < n_rngs * 2 * nE; i++) a.Wed[i] = W_ed[i];
+    for (int r = 0; r < n_rngs; r++) a.wts[r] = weights[r];
+    a.n_rngs = n_rngs;
+    a.eta = eta;
+    a.T = T;
+    for (int e = 0; e < nE; e++) {
+        a.eta_ed[e] = eta_ed[e];
+        a.T_ed[e] = T_ed[e];
+    }
+    a.variance = sqrt(sp->variance_coef_mom * 2.0 * sp->k_B / (sp->dV * dt));
+    a.dxinv = 1.0 / ctx->dx;
+    const Grid g = ctx->g0;
+    double* f2 = dim == 3 ? force[2] : nullptr;
+    const bool mixed = ctx->prec == FHD_PREC_MIXED;
+    with_dim(dim, [&](auto D) {
+        constexpr int DIM = decltype(D)::value;
+        if (mixed)
+            k_stoch_m<float, DIM><<<cell_grid(g), cell_block(), 0, ctx->stream>>>(g, a, force[0], force[1], f2,
+                                                                                increment);
+        else
+            k_stoch_m<double, DIM><<<cell_grid(g), cell_block(), 0, ctx->stream>>>(g, a, force[0], force[1], f2,
+                                                                                 increment);
+    });
+    ctx->launches++;
+    FHD_CUDA_TRY(cudaPeekAtLastError());
+    return 0;
+}
+
+// ---------------------------------------------------------------------
+// step glue kernels
+// ---------------------------------------------------------------------
+// average_cc_to_face (convert_stag.f90:229-292): face = (cc(i)+cc(i-1))/2
+template <int DIM>
+__global__ void __launch_bounds__(256) k_avg_face(Grid g, const double* cc, double* o0, double* o1, double* o2) {
+    Cell P;
+    if (!cell_of_thread(g, P)) return;
+    const i64 f = P.id(0, 0, 0);
+    const double v = ld(cc, f);
+    o0[f] = 0.5 * (v + ld(cc, P.id(-1, 0, 0)));
+    o1[f] = 0.5 * (v + ld(cc, P.id(0, -1, 0)));
+    if constexpr (DIM == 3) o2[f] = 0.5 * (v + ld(cc, P.id(0, 0, -1)));
+}
+
+// centred scalar advection (mk_advective_s_fluxdiv.f90:138-220),
+// upd = -div(s_fc u), folded into the scalar update:
+//   mode 0: s_out = s_a + dt*upd                   (predictor Euler)
+//   mode 1: s_out = ((s_out + s_a) + dt*upd)*0.5   (trapezoidal corrector)
+template <int DIM>
+__global__ void __launch_bounds__(256) k_adv_s_update(Grid g, CSVec<double> u, CSVec<double> sfc, const double* sa,
+                                                      double* sout, double dt, double dxinv, int mode) {
+    Cell P;
+    if (!cell_of_thread(g, P)) return;
+    const i64 f = P.id(0, 0, 0);
+    double s = 0.0;
+#pragma unroll
+    for (int d = 0; d < DIM; d++) {
+        const i64 fp = P.id(d == 0, d == 1, d == 2);
+        s += (ld(u.c[d], fp) * ld(sfc.c[d], fp) - ld(u.c[d], f) * ld(sfc.c[d], f)) * dxinv;
+    }
+    const double upd = -s;
+    if (mode == 0) {
+        sout[f] = sa[f] + dt * upd;
+    } else {
+        double v = sout[f] + sa[f];
+        v = v + dt * upd;
+        sout[f] = v * 0.5;
+    }
+}
+
+// centred momentum advection (mk_advective_m_fluxdiv.f90:184-346):
+// upd (+)= -div(m u); flux of m_c in direction d at q is
+// 0.25*(m_c(q-e_d)+m_c(q))*(u_d(q-e_c)+u_d(q))
+template <int DIM>
+__global__ void __launch_bounds__(256) k_adv_m(Grid g, CSVec<double> u, CSVec<double> m, SVec<double> upd,
+                                               int increment, double dxinv) {
+    Cell P;
+    if (!cell_of_thread(g, P)) return;
+    const i64 f = P.id(0, 0, 0);
+#pragma unroll
+    for (int c = 0; c < DIM; c++) {
+        const int cx = (c == 0), cy = (c == 1), cz = (c == 2);
+        double s = 0.0;
+#pragma unroll
+        for (int d = 0; d < DIM; d++) {
+            const int ex = (d == 0), ey = (d == 1), ez = (d == 2);
+            auto flux = [&](int qi, int qj, int qk) {
+                const i64 q = P.id(qi, qj, qk);
+                return 0.25 * (ld(m.c[c], P.id(qi - ex, qj - ey, qk - ez)) + ld(m.c[c], q)) *
+                       (ld(u.c[d], P.id(qi - cx, qj - cy, qk - cz)) + ld(u.c[d], q));
+            };
+            s += (flux(ex, ey, ez) - flux(0, 0, 0)) * dxinv;
+        }
+        upd.c[c][f] = increment ? upd.c[c][f] - s : -s;
+    }
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(256) k_grad(Grid g, const double* p, SVec<double> o, double dxinv) {
+    Cell P;
+    if (!cell_of_thread(g, P)) return;
+    const i64 f = P.id(0, 0, 0);
+    const double v = ld(p, f);
+#pragma unroll
+    for (int d = 0; d < DIM; d++) o.c[d][f] = (v - ld(p, P.id(-(d == 0), -(d == 1), -(d == 2)))) * dxinv;
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(256) k_div_inc(Grid g, CSVec<double> u, double* out, double dxinv) {
+    Cell P;
+    if (!cell_of_thread(g, P)) return;
+    const i64 f = P.id(0, 0, 0);
+    double s = 0.0;
+#pragma unroll
+    for (int d = 0; d < DIM; d++) s += (ld(u.c[d], P.id(d == 0, d == 1, d == 2)) - ld(u.c[d], f)) * dxinv;
+    out[f] = out[f] + s;
+}
+
+// y = (keep ? y : 0) + a0*x0 + a1*x1 + ... (left to right), per component
+struct Lin {
+    const double* x[4][3];
+    double a[4];
+    int nt;
+};
+__global__ void __launch_bounds__(256) k_lin(i64 n, int ncomp, SVec<double> y, Lin L, int keep) {
+    for (i64 f = blockIdx.x * (i64)blockDim.x + threadIdx.x; f < n; f += (i64)gridDim.x * blockDim.x) {
+        for (int c = 0; c < ncomp; c++) {
+            double v = keep ? y.c[c][f] : 0.0;
+            for (int t = 0; t < L.nt; t++) v = v + L.a[t] * L.x[t][c][f];
+            y.c[c][f] = v;
+        }
+    }
+}
+
+// y = s * u per component (convert_m_to_umac, m = rho_fc * umac)
+__global__ void __launch_bounds__(256) k_mul(i64 n, int ncomp, SVec<double> y, CSVec<double> s, CSVec<double> u) {
+    for (i64 f = blockIdx.x * (i64)blockDim.x + threadIdx.x; f < n; f += (i64)gridDim.x * blockDim.x)
+        for (int c = 0; c < ncomp; c++) y.c[c][f] = s.c[c][f] * u.c[c][f];
+}
+
+// ---------------------------------------------------------------------
+// inertial step (advance_timestep_inertial.f90:45-923), single species
+// ---------------------------------------------------------------------
+enum {
+    B_RFO = 0, B_RFN = 3, B_MOLD = 6, B_MTEMP = 9, B_ADV = 12, B_DIFF = 15, B_RHSV = 18, B_DU = 21, B_STOCH = 24,
+    B_GPI = 27, B_RHOOLD = 30, B_RHSP = 31, B_DPI = 32, B_ETAH = 33, B_KAPH = 34, B_ETAEDH = 35, B_ZERO = 38,
+    B_COUNT = 39
+};
+
+static int step_alloc(fhd_ctx* ctx) {
+    if (ctx->step_ready) return 0;
+    const i64 nc = ctx->g0.nc;
+    for (int i = 0; i < B_COUNT; i++) {
+        ctx->sb[i] = ctx->arena.alloc<double>(nc);
+        if (!ctx->sb[i]) return FHD_ERR_OOM;
+    }
+    FHD_CUDA_TRY(cudaMemsetAsync(ctx->sb[B_ZERO], 0, sizeof(double) * nc, ctx->stream));
+    ctx->step_ready = true;
+    return 0;
+}
+
+static SVec<double> sv(fhd_ctx* ctx, int base) {
+    SVec<double> v;
+    for (int c = 0; c < 4; c++) v.c[c] = (c < ctx->dim) ? ctx->sb[base + c] : nullptr;
+    return v;
+}
+static CSVec<double> cs(SVec<double> v) {
+    CSVec<double> o;
+    for (int c = 0; c < 4; c++) o.c[c] = v.c[c];
+    return o;
+}
+static SVec<double> svp(double* const* a, int dim) {
+    SVec<double> v;
+    for (int c = 0; c < 4; c++) v.c[c] = (c < dim) ? a[c] : nullptr;
+    return v;
+}
+
+// diffusive_m_fluxdiv (diffusive_m_fluxdiv.f90:25-...): -(stag_applyop with
+// alpha = 0) applied to u, written to out
+static int diff_m(fhd_ctx* ctx, SVec<double> out, CSVec<double> u, const double* eta, const double* const eta_ed[],
+                  const double* kappa) {
+    StagOp<double> A;
+    const int nE = ctx->dim == 2 ? 1 : 3;
+    for (int c = 0; c < 3; c++) {
+        A.alpha[c] = ctx->sb[B_ZERO];
+        A.bed[c] = c < nE ? eta_ed[c] : nullptr;
+    }
+    A.alpha_scale = 0.0;
+    A.beta = eta;
+    A.gamma = kappa;
+    A.q = 1.0 / (ctx->dx * ctx->dx);
+    const Grid g = ctx->g0;
+    with_dim_visc(ctx->dim, ctx->visc, [&](auto D, auto V) {
+        constexpr int DIM = decltype(D)::value, VISC = decltype(V)::value;
+        k_stag_apply<double, DIM, VISC><<<cell_grid(g), cell_block(), 0, ctx->stream>>>(
+            g, A, u.c[0], u.c[1], u.c[2], out.c[0], out.c[1], out.c[2], nullptr, nullptr, nullptr, 0);
+    });
+    ctx->launches++;
+    FHD_CUDA_TRY(cudaPeekAtLastError());
+    Lin L;
+    memset(&L, 0, sizeof(L));
+    L.nt = 1;
+    L.a[0] = -1.0;
+    for (int c = 0; c < ctx->dim; c++) L.x[0][c] = out.c[c];
+    k_lin<<<flat_blocks(g.nc), 256, 0, ctx->stream>>>(g.nc, ctx->dim, out, L, 0);
+    ctx->launches++;
+    FHD_CUDA_TRY(cudaPeekAtLastError());
+    return 0;
+}
+
+static int lin(fhd_ctx* ctx, SVec<double> y, int keep, std::initializer_list<std::pair<double, CSVec<double>>> terms) {
+    Lin L;
+    memset(&L, 0, sizeof(L));
+    int t = 0;
+    for (auto& pr : terms) {
+        L.a[t] = pr.first;
+        for (int c = 0; c < ctx->dim; c++) L.x[t][c] = pr.second.c[c];
+        t++;
+    }
+    L.nt = t;
+    k_lin<<<flat_blocks(ctx->g0.nc), 256, 0, ctx->stream>>>(ctx->g0.nc, ctx->dim, y, L, keep);
+    ctx->launches++;
+    FHD_CUDA_TRY(cudaPeekAtLastError());
+    return 0;
+}
+
+int advance_inertial(fhd_ctx* ctx, const fhd_stoch_params* sp, double dt, double* const umac[], double* rho,
+                     double* pi, const double* eta, const double* const eta_ed[], const double* kappa,
+                     const double* temperature, const double* const temperature_ed[], const double* const W_cc[],
+                     const double* const W_ed[], fhd_solve_stats* stats2) {
+    int rc = step_alloc(ctx);
+    if (rc) return rc;
+    const int dim = ctx->dim, nE = dim == 2 ? 1 : 3;
+    const Grid g = ctx->g0;
+    const i64 nc = g.nc;
+    const int nb = flat_blocks(nc);
+    cudaStream_t st = ctx->stream;
+    const double dxinv = 1.0 / ctx->dx;
+    const double theta = 1.0 / dt;
+    SVec<double> u = svp(umac, dim);
+    SVec<double> rfo = sv(ctx, B_RFO), rfn = sv(ctx, B_RFN), mold = sv(ctx, B_MOLD), mtemp = sv(ctx, B_MTEMP),
+                 adv = sv(ctx, B_ADV), diff = sv(ctx, B_DIFF), rhs_v = sv(ctx, B_RHSV), du = sv(ctx, B_DU),
+                 stoch = sv(ctx, B_STOCH), gpi = sv(ctx, B_GPI);
+    double* rho_old = ctx->sb[B_RHOOLD];
+    double* rhs_p = ctx->sb[B_RHSP];
+    double* dpi = ctx->sb[B_DPI];
+    double* eta_h = ctx->sb[B_ETAH];
+    double* kap_h = ctx->sb[B_KAPH];
+    const double* eta_ed_h[3] = {ctx->sb[B_ETAEDH], ctx->sb[B_ETAEDH + 1], ctx->sb[B_ETAEDH + 2]};
+    const double w1[1] = {1.0};
+    // eta/2, kappa/2 for the solves (advance_timestep_inertial.f90:467-474)
+    k_copy_conv<double, double><<<nb, 256, 0, st>>>(nc, eta_h, eta, 0.5);
+    ctx->launches++;
+    k_copy_conv<double, double><<<nb, 256, 0, st>>>(nc, kap_h, kappa, 0.5);
+    ctx->launches++;
+    for (int e = 0; e < nE; e++) {
+        k_copy_conv<double, double><<<nb, 256, 0, st>>>(nc, (double*)eta_ed_h[e], eta_ed[e], 0.5);
+        ctx->launches++;
+    }
+    FHD_CUDA_TRY(cudaMemcpyAsync(rho_old, rho, sizeof(double) * nc, cudaMemcpyDeviceToDevice, st));
+    auto launch_dim = [&](auto&& fn) { with_dim(dim, fn); ctx->launches++; };
+    // Step 2: predictor Euler step for rho
+    launch_dim([&](auto D) {
+        constexpr int DIM = decltype(D)::value;
+        k_avg_face<DIM><<<cell_grid(g), cell_block(), 0, st>>>(g, rho_old, rfo.c[0], rfo.c[1], rfo.c[2]);
+    });
+    launch_dim([&](auto D) {
+        constexpr int DIM = decltype(D)::value;
+        k_adv_s_update<DIM><<<cell_grid(g), cell_block(), 0, st>>>(g, cs(u), cs(rfo), rho_old, rho, dt, dxinv, 0);
+    });
+    launch_dim([&](auto D) {
+        constexpr int DIM = decltype(D)::value;
+        k_avg_face<DIM><<<cell_grid(g), cell_block(), 0, st>>>(g, rho, rfn.c[0], rfn.c[1], rfn.c[2]);
+    });
+    // Steps 3-4: predictor Crank-Nicolson right-hand side
+    k_mul<<<nb, 256, 0, st>>>(nc, dim, mold, cs(rfo), cs(u));
+    ctx->launches++;
+    if ((rc = lin(ctx, rhs_v, 0, {{1.0 / dt, cs(mold)}}))) return rc;
+    launch_dim([&](auto D) {
+        constexpr int DIM = decltype(D)::value;
+        k_grad<DIM><<<cell_grid(g), cell_block(), 0, st>>>(g, pi, gpi, dxinv);
+    });
+    if ((rc = lin(ctx, rhs_v, 1, {{-1.0, cs(gpi)}}))) return rc;
+    launch_dim([&](auto D) {
+        constexpr int DIM = decltype(D)::value;
+        k_adv_m<DIM><<<cell_grid(g), cell_block(), 0, st>>>(g, cs(u), cs(mold), adv, 0, dxinv);
+    });
+    if ((rc = lin(ctx, rhs_v, 1, {{1.0, cs(adv)}}))) return rc;
+    if ((rc = diff_m(ctx, diff, cs(u), eta, eta_ed, kappa))) return rc;
+    if ((rc = lin(ctx, rhs_v, 1, {{0.5, cs(diff)}}))) return rc;
+    if (sp->variance_coef_mom != 0.0) {
+        if ((rc = stoch_launch(ctx, sp, stoch.c, 0, eta, eta_ed, temperature, temperature_ed, dt, w1, 1, W_cc,
+                               W_ed)))
+            return rc;
+        if ((rc = lin(ctx, rhs_v, 1, {{1.0, cs(stoch)}}))) return rc;
+    }
+    FHD_CUDA_TRY(cudaMemsetAsync(rhs_p, 0, sizeof(double) * nc, st));
+    k_mul<<<nb, 256, 0, st>>>(nc, dim, mtemp, cs(rfn), cs(u));
+    ctx->launches++;
+    if ((rc = lin(ctx, rhs_v, 1, {{-1.0 / dt, cs(mtemp)}}))) return rc;
+    if ((rc = diff_m(ctx, mtemp, cs(u), eta, eta_ed, kappa))) return rc;
+    if ((rc = lin(ctx, rhs_v, 1, {{0.5, cs(mtemp)}}))) return rc;
+    launch_dim([&](auto D) {
+        constexpr int DIM = decltype(D)::value;
+        k_div_inc<DIM><<<cell_grid(g), cell_block(), 0, st>>>(g, cs(u), rhs_p, dxinv);
+    });
+    for (int c = 0; c < dim; c++) FHD_CUDA_TRY(cudaMemsetAsync(du.c[c], 0, sizeof(double) * nc, st));
+    FHD_CUDA_TRY(cudaMemsetAsync(dpi, 0, sizeof(double) * nc, st));
+    FHD_CUDA_TRY(cudaPeekAtLastError());
+    const double abs_tol_in = ctx->p.gmres_abs_tol;
+    double norm_pre_rhs = 0.0;
+    const double* rfn_c[3] = {rfn.c[0], rfn.c[1], rfn.c[2]};
+    auto solve = [&](fhd_solve_stats* s, double* npr) -> int {
+        int r2 = prepare(ctx, rfn_c, eta_h, eta_ed_h, kap_h, theta);
+        if (r2) return r2;
+        CSVec<double> b;
+        SVec<double> x;
+        for (int c = 0; c < 4; c++) { b.c[c] = nullptr; x.c[c] = nullptr; }
+        for (int c = 0; c < dim; c++) { b.c[c] = rhs_v.c[c]; x.c[c] = du.c[c]; }
+        b.c[dim] = rhs_p;
+        x.c[dim] = dpi;
+        return gmres_dev(ctx, b, x, npr, s);
+    };
+    int st1 = solve(stats2 ? &stats2[0] : nullptr, &norm_pre_rhs);
+    if (st1 < 0) return st1;
+    // corrector stopping criterion (advance_timestep_inertial.f90:493-496)
+    ctx->p.gmres_abs_tol = fmax(abs_tol_in, norm_pre_rhs * ctx->p.gmres_rel_tol);
+    if ((rc = lin(ctx, u, 1, {{1.0, cs(du)}}))) { ctx->p.gmres_abs_tol = abs_tol_in; return rc; }
+    {
+        SVec<double> pv;
+        for (int c = 0; c < 4; c++) pv.c[c] = nullptr;
+        pv.c[0] = pi;
+        Lin L;
+        memset(&L, 0, sizeof(L));
+        L.nt = 1;
+        L.a[0] = 1.0;
+        L.x[0][0] = dpi;
+        k_lin<<<nb, 256, 0, st>>>(nc, 1, pv, L, 1);
+        ctx->launches++;
+    }
+    k_mul<<<nb, 256, 0, st>>>(nc, dim, mtemp, cs(rfn), cs(u));
+    ctx->launches++;
+    // Step 5: trapezoidal scalar corrector
+    launch_dim([&](auto D) {
+        constexpr int DIM = decltype(D)::value;
+        k_adv_s_update<DIM><<<cell_grid(g), cell_block(), 0, st>>>(g, cs(u), cs(rfn), rho_old, rho, dt, dxinv, 1);
+    });
+    launch_dim([&](auto D) {
+        constexpr int DIM = decltype(D)::value;
+        k_avg_face<DIM><<<cell_grid(g), cell_block(), 0, st>>>(g, rho, rfn.c[0], rfn.c[1], rfn.c[2]);
+    });
+    // Steps 6-7: corrector Crank-Nicolson right-hand side
+    int rc2 = 0;
+    do {
+        if ((rc2 = lin(ctx, rhs_v, 0, {{1.0 / dt, cs(mold)}}))) break;
+        launch_dim([&](auto D) {
+            constexpr int DIM = decltype(D)::value;
+            k_grad<DIM><<<cell_grid(g), cell_block(), 0, st>>>(g, pi, gpi, dxinv);
+        });
+        if ((rc2 = lin(ctx, rhs_v, 1, {{-1.0, cs(gpi)}}))) break;
+        launch_dim([&](auto D) {
+            constexpr int DIM = decltype(D)::value;
+            k_adv_m<DIM><<<cell_grid(g), cell_block(), 0, st>>>(g, cs(u), cs(mtemp), adv, 1, dxinv);
+        });
+        if ((rc2 = lin(ctx, rhs_v, 1, {{0.5, cs(adv)}}))) break;
+        if ((rc2 = lin(ctx, rhs_v, 1, {{0.5, cs(diff)}}))) break;
+        if (sp->variance_coef_mom != 0.0) {
+            if ((rc2 = stoch_launch(ctx, sp, stoch.c, 1, eta, eta_ed, temperature, temperature_ed, dt, w1, 1, W_cc,
+                                    W_ed)))
+                break;
+            if ((rc2 = lin(ctx, rhs_v, 1, {{0.5, cs(stoch)}}))) break;
+        }
+        FHD_CUDA_TRY(cudaMemsetAsync(rhs_p, 0, sizeof(double) * nc, st));
+        k_mul<<<nb, 256, 0, st>>>(nc, dim, mtemp, cs(rfn), cs(u));
+        ctx->launches++;
+        if ((rc2 = lin(ctx, rhs_v, 1, {{-1.0 / dt, cs(mtemp)}}))) break;
+        if ((rc2 = diff_m(ctx, diff, cs(u), eta, eta_ed, kappa))) break;
+        if ((rc2 = lin(ctx, rhs_v, 1, {{0.5, cs(diff)}}))) break;
+        launch_dim([&](auto D) {
+            constexpr int DIM = decltype(D)::value;
+            k_div_inc<DIM><<<cell_grid(g), cell_block(), 0, st>>>(g, cs(u), rhs_p, dxinv);
+        });
+        for (int c = 0; c < dim; c++) FHD_CUDA_TRY(cudaMemsetAsync(du.c[c], 0, sizeof(double) * nc, st));
+        FHD_CUDA_TRY(cudaMemsetAsync(dpi, 0, sizeof(double) * nc, st));
+    } while (0);
+    if (rc2) { ctx->p.gmres_abs_tol = abs_tol_in; return rc2; }
+    int st2 = solve(stats2 ? &stats2[1] : nullptr, nullptr);
+    ctx->p.gmres_abs_tol = abs_tol_in;
+    if (st2 < 0) return st2;
+    if ((rc = lin(ctx, u, 1, {{1.0, cs(du)}}))) return rc;
+    {
+        SVec<double> pv;
+        for (int c = 0; c < 4; c++) pv.c[c] = nullptr;
+        pv.c[0] = pi;
+        Lin L;
+        memset(&L, 0, sizeof(L));
+        L.nt = 1;
+        L.a[0] = 1.0;
+        L.x[0][0] = dpi;
+        k_lin<<<nb, 256, 0, st>>>(nc, 1, pv, L, 1);
+        ctx->launches++;
+    }
+    FHD_CUDA_TRY(cudaPeekAtLastError());
+    return st1 > st2 ? st1 : st2;
+}
+
+}  // namespace fhd
+
+using namespace fhd;
+
+extern "C" {
+
+int fhd_dev_stochastic_m_fluxdiv(fhd_ctx* ctx, const fhd_stoch_params* sp, double* const force[], int increment,
+                                 const double* eta, const double* const eta_ed[], const double* temperature,
+                                 const double* const temperature_ed[], double dt, const double* weights, int n_rngs,
+                                 const double* const W_cc[], const double* const W_ed[]) {
+    if (!ctx || !sp || !force || !eta || !eta_ed || !temperature || !temperature_ed || !weights || !W_cc || !W_ed)
+        return FHD_ERR_BAD_ARG;
+    int rc = stoch_launch(ctx, sp, force, increment, eta, eta_ed, temperature, temperature_ed, dt, weights, n_rngs,
+                          W_cc, W_ed);
+    if (rc) return rc;
+    FHD_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    return 0;
+}
+
+int fhd_dev_advance_inertial(fhd_ctx* ctx, const fhd_stoch_params* sp, double dt, double* const umac[], double* rho,
+                             double* pi, const double* eta, const double* const eta_ed[], const double* kappa,
+                             const double* temperature, const double* const temperature_ed[],
+                             const double* const W_cc[], const double* const W_ed[], fhd_solve_stats* stats2) {
+    if (!ctx || !sp || !umac || !rho || !pi || !eta || !eta_ed || !kappa || !temperature || !temperature_ed ||
+        !W_cc || !W_ed || !(dt > 0.0))
+        return FHD_ERR_BAD_ARG;
+    int rc = advance_inertial(ctx, sp, dt, umac, rho, pi, eta, eta_ed, kappa, temperature, temperature_ed, W_cc,
+                              W_ed, stats2);
+    if (rc < 0) return rc;
+    FHD_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    return rc;
+}
+
+}  // extern "C"

@@ -1,0 +1,243 @@
+"""TEST INFRASTRUCTURE ONLY: ctypes bindings of the CPU FP64 oracle.
+
+The oracle (fhd_oracle.cpp) restates LowMachFHD's staggered Stokes solver and
+stochastic momentum flux on the CPU.  Only tests/, __graft_entry__.smoke()
+and bench.py's CPU-baseline leg import this module; the product library
+never does.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "_build", "liboracle.so")
+_lib = None
+
+
+class GmresParams(C.Structure):
+    _fields_ = [
+        ("precon_type", C.c_int), ("visc_schur_approx", C.c_int),
+        ("p_norm_weight", C.c_double), ("scale_factor", C.c_double),
+        ("mg_verbose", C.c_int), ("cg_verbose", C.c_int),
+        ("mg_max_vcycles", C.c_int), ("mg_minwidth", C.c_int), ("mg_bottom_solver", C.c_int),
+        ("mg_nsmooths_down", C.c_int), ("mg_nsmooths_up", C.c_int), ("mg_nsmooths_bottom", C.c_int),
+        ("mg_max_bottom_nlevels", C.c_int),
+        ("mg_rel_tol", C.c_double), ("mg_abs_tol", C.c_double),
+        ("stag_mg_verbosity", C.c_int), ("stag_mg_max_vcycles", C.c_int), ("stag_mg_minwidth", C.c_int),
+        ("stag_mg_bottom_solver", C.c_int),
+        ("stag_mg_nsmooths_down", C.c_int), ("stag_mg_nsmooths_up", C.c_int),
+        ("stag_mg_nsmooths_bottom", C.c_int), ("stag_mg_max_bottom_nlevels", C.c_int),
+        ("stag_mg_omega", C.c_double), ("stag_mg_smoother", C.c_int), ("stag_mg_rel_tol", C.c_double),
+        ("gmres_rel_tol", C.c_double), ("gmres_abs_tol", C.c_double),
+        ("gmres_verbose", C.c_int), ("gmres_max_outer", C.c_int), ("gmres_max_inner", C.c_int),
+        ("gmres_max_iter", C.c_int), ("gmres_min_iter", C.c_int), ("gmres_spatial_order", C.c_int),
+    ]
+
+
+def default_params(**kw) -> GmresParams:
+    """Defaults of probin_gmres_init (probin_gmres.f90:122-163)."""
+    p = GmresParams(
+        precon_type=1, visc_schur_approx=0, p_norm_weight=1.0, scale_factor=1.0,
+        mg_verbose=0, cg_verbose=0, mg_max_vcycles=1, mg_minwidth=2, mg_bottom_solver=4,
+        mg_nsmooths_down=2, mg_nsmooths_up=2, mg_nsmooths_bottom=8, mg_max_bottom_nlevels=10,
+        mg_rel_tol=1e-9, mg_abs_tol=1e-14,
+        stag_mg_verbosity=0, stag_mg_max_vcycles=1, stag_mg_minwidth=2, stag_mg_bottom_solver=4,
+        stag_mg_nsmooths_down=2, stag_mg_nsmooths_up=2, stag_mg_nsmooths_bottom=8,
+        stag_mg_max_bottom_nlevels=10, stag_mg_omega=1.0, stag_mg_smoother=1, stag_mg_rel_tol=1e-9,
+        gmres_rel_tol=1e-9, gmres_abs_tol=0.0, gmres_verbose=1, gmres_max_outer=20,
+        gmres_max_inner=5, gmres_max_iter=100, gmres_min_iter=1, gmres_spatial_order=2)
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+class StochParams(C.Structure):
+    _fields_ = [("k_B", C.c_double), ("variance_coef_mom", C.c_double), ("dV", C.c_double),
+                ("stoch_stress_form", C.c_int), ("filtering_width", C.c_int)]
+
+
+class SolveStats(C.Structure):
+    _fields_ = [("outer_iters", C.c_int), ("total_iters", C.c_int), ("vcycles", C.c_int),
+                ("status", C.c_int),
+                ("norm_b", C.c_double), ("norm_pre_b", C.c_double), ("norm_init_resid", C.c_double),
+                ("norm_resid", C.c_double), ("norm_resid_Stokes", C.c_double),
+                ("norm_init_Stokes", C.c_double), ("norm_resid_est", C.c_double)]
+
+
+def build() -> str:
+    """Compile the oracle with its Makefile (g++, OpenMP)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        _lib = C.CDLL(_LIB_PATH)
+    return _lib
+
+
+# ----------------------------------------------------------------------
+# array helpers
+# ----------------------------------------------------------------------
+_DP = C.POINTER(C.c_double)
+
+
+def _p(a: np.ndarray):
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data_as(_DP)
+
+
+def _pp(arrs):
+    """array of double* from a list of float64 arrays"""
+    arr = (_DP * max(1, len(arrs)))()
+    for i, a in enumerate(arrs):
+        arr[i] = _p(a)
+    return arr
+
+
+def _n3(n):
+    n = list(n) + [1] * (3 - len(n))
+    return (C.c_int * 3)(*n)
+
+
+def nedge(dim):
+    return 1 if dim == 2 else 3
+
+
+class Problem:
+    """Grid + coefficients of one Stokes problem (canonical layout; flat
+    arrays of nx*ny*nz, x fastest)."""
+
+    def __init__(self, dim, n, dx, visc_type, alpha_fc, beta, beta_ed, gamma):
+        self.dim, self.n, self.dx, self.visc_type = dim, list(n), float(dx), visc_type
+        self.alpha_fc = [np.ascontiguousarray(a, np.float64) for a in alpha_fc]
+        self.beta = np.ascontiguousarray(beta, np.float64)
+        self.beta_ed = [np.ascontiguousarray(a, np.float64) for a in beta_ed]
+        self.gamma = np.ascontiguousarray(gamma, np.float64)
+
+    @property
+    def nc(self):
+        return int(np.prod(self.n[: self.dim]))
+
+
+def stag_applyop(pb: Problem, phi, color=0, theta=1.0):
+    Lphi = [np.zeros(pb.nc) for _ in range(pb.dim)]
+    alpha = [a * theta for a in pb.alpha_fc]
+    lib().or_stag_applyop(pb.dim, _n3(pb.n), C.c_double(pb.dx), pb.visc_type, _pp(phi), _pp(Lphi),
+                          _pp(alpha), _p(pb.beta), _pp(pb.beta_ed), _p(pb.gamma), color)
+    return Lphi
+
+
+def stag_mg_solver(pb: Problem, params, theta, rhs, phi0=None):
+    phi = [np.zeros(pb.nc) if phi0 is None else phi0[d].copy() for d in range(pb.dim)]
+    rc = lib().or_stag_mg_solver(pb.dim, _n3(pb.n), C.c_double(pb.dx), pb.visc_type, C.byref(params),
+                                 _pp(pb.alpha_fc), _p(pb.beta), _pp(pb.beta_ed), _p(pb.gamma),
+                                 C.c_double(theta), _pp(phi), _pp(rhs))
+    assert rc == 0, rc
+    return phi
+
+
+def macproject(dim, n, dx, params, alphainv, rhs):
+    phi = np.zeros(int(np.prod(n[:dim])))
+    lib().or_macproject(dim, _n3(n), C.c_double(dx), C.byref(params), _p(phi), _pp(alphainv), _p(rhs))
+    return phi
+
+
+def apply_matrix(pb: Problem, theta, x_u, x_p):
+    b_u = [np.zeros(pb.nc) for _ in range(pb.dim)]
+    b_p = np.zeros(pb.nc)
+    lib().or_apply_matrix(pb.dim, _n3(pb.n), C.c_double(pb.dx), pb.visc_type, _pp(b_u), _p(b_p),
+                          _pp(x_u), _p(x_p), _pp(pb.alpha_fc), _p(pb.beta), _pp(pb.beta_ed),
+                          _p(pb.gamma), C.c_double(theta))
+    return b_u, b_p
+
+
+def apply_precon(pb: Problem, params, theta, b_u, b_p):
+    x_u = [np.zeros(pb.nc) for _ in range(pb.dim)]
+    x_p = np.zeros(pb.nc)
+    rc = lib().or_apply_precon(pb.dim, _n3(pb.n), C.c_double(pb.dx), pb.visc_type, C.byref(params),
+                               _pp(b_u), _p(b_p), _pp(x_u), _p(x_p), _pp(pb.alpha_fc), _p(pb.beta),
+                               _pp(pb.beta_ed), _p(pb.gamma), C.c_double(theta))
+    assert rc == 0, rc
+    return x_u, x_p
+
+
+def gmres(pb: Problem, params, theta, b_u, b_p, x_u0=None, x_p0=None):
+    x_u = [np.zeros(pb.nc) if x_u0 is None else x_u0[d].copy() for d in range(pb.dim)]
+    x_p = np.zeros(pb.nc) if x_p0 is None else x_p0.copy()
+    npr = C.c_double(0.0)
+    st = SolveStats()
+    rc = lib().or_gmres(pb.dim, _n3(pb.n), C.c_double(pb.dx), pb.visc_type, C.byref(params),
+                        _pp(b_u), _p(b_p), _pp(x_u), _p(x_p), _pp(pb.alpha_fc), _p(pb.beta),
+                        _pp(pb.beta_ed), _p(pb.gamma), C.c_double(theta), C.byref(npr), C.byref(st))
+    return rc, x_u, x_p, npr.value, st
+
+
+def stochastic_m_fluxdiv(dim, n, dx, sp, eta, eta_ed, temp, temp_ed, dt, weights, W_cc, W_ed,
+                         force=None, increment=False):
+    nc = int(np.prod(n[:dim]))
+    force = [np.zeros(nc) for _ in range(dim)] if force is None else [f.copy() for f in force]
+    w = np.ascontiguousarray(weights, np.float64)
+    rc = lib().or_stochastic_m_fluxdiv(dim, _n3(n), C.c_double(dx), C.byref(sp), _pp(force),
+                                       int(increment), _p(eta), _pp(eta_ed), _p(temp), _pp(temp_ed),
+                                       C.c_double(dt), _p(w), len(weights), _pp(W_cc), _pp(W_ed))
+    assert rc == 0, rc
+    return force
+
+
+def average_cc_to_edge(dim, n, cc):
+    nc = int(np.prod(n[:dim]))
+    ed = [np.zeros(nc) for _ in range(nedge(dim))]
+    lib().or_average_cc_to_edge(dim, _n3(n), _p(cc), _pp(ed))
+    return ed
+
+
+def average_cc_to_face(dim, n, cc):
+    nc = int(np.prod(n[:dim]))
+    fc = [np.zeros(nc) for _ in range(dim)]
+    lib().or_average_cc_to_face(dim, _n3(n), _p(cc), _pp(fc))
+    return fc
+
+
+def advance_inertial(dim, n, dx, visc_type, params, sp, dt, umac, rho, pi, eta, eta_ed, kappa,
+                     temp, temp_ed, W_cc, W_ed):
+    umac = [u.copy() for u in umac]
+    rho, pi = rho.copy(), pi.copy()
+    st = (SolveStats * 2)()
+    rc = lib().or_advance_inertial(dim, _n3(n), C.c_double(dx), visc_type, C.byref(params), C.byref(sp),
+                                   C.c_double(dt), _pp(umac), _p(rho), _p(pi), _p(eta), _pp(eta_ed),
+                                   _p(kappa), _p(temp), _pp(temp_ed), _pp(W_cc), _pp(W_ed), st)
+    return rc, umac, rho, pi, st
+
+
+def accuracy_test(dim, n, prob_coeff, prob_sol, visc_type):
+    err = np.zeros(4)
+    rc = lib().or_accuracy_test(dim, n, prob_coeff, prob_sol, visc_type, _p(err))
+    assert rc == 0
+    return err[: dim + 1]
+
+
+def compute_nlevs_mg(dim, n, minwidth=2):
+    return lib().or_compute_nlevs_mg(dim, _n3(n), minwidth)
+
+
+def num_threads():
+    return lib().or_num_threads()
+
+
+def stag_mg_history(pb: Problem, params, theta, rhs):
+    """per-V-cycle L2 residual ratios of stag_mg_solver from a zero guess"""
+    phi = [np.zeros(pb.nc) for _ in range(pb.dim)]
+    hist = np.zeros(params.stag_mg_max_vcycles)
+    rc = lib().or_stag_mg_history(pb.dim, _n3(pb.n), C.c_double(pb.dx), pb.visc_type, C.byref(params),
+                                  _pp(pb.alpha_fc), _p(pb.beta), _pp(pb.beta_ed), _p(pb.gamma),
+                                  C.c_double(theta), _pp(phi), _pp(rhs), _p(hist))
+    assert rc == 0
+    return hist

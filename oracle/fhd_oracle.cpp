@@ -1,0 +1,1514 @@
+/*
+ * fhd_oracle.cpp -- TEST INFRASTRUCTURE ONLY (parity checker and CPU
+ * baseline).  A plain C++ FP64 restatement of the LowMachFHD hot path for
+ * one periodic box, following the reference Fortran routine by routine.
+ * Citations are to files under staggered_grid/ of the reference.
+ *
+ * Layout: unique periodic degrees of freedom (see include/fhd_b200.h); the
+ * reference stores the periodic face twice and keeps both copies equal
+ * (multifab_internal_sync), which is the same discrete problem.
+ *
+ * Reductions are deterministic: per-row partial sums added in row order.
+ */
+#include "fhd_oracle.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+typedef std::vector<double> Vec;
+
+struct Geo {
+    int dim = 2;
+    int n[3] = {1, 1, 1};
+    long nc = 1;
+    double dx = 1.0;
+    Geo() {}
+    Geo(int d, const int nn[3], double h) : dim(d), dx(h) {
+        n[0] = nn[0];
+        n[1] = nn[1];
+        n[2] = (d == 3) ? nn[2] : 1;
+        nc = (long)n[0] * n[1] * n[2];
+    }
+    inline long id(int i, int j, int k) const {
+        if (i < 0) i += n[0]; else if (i >= n[0]) i -= n[0];
+        if (j < 0) j += n[1]; else if (j >= n[1]) j -= n[1];
+        if (k < 0) k += n[2]; else if (k >= n[2]) k -= n[2];
+        return i + (long)n[0] * (j + (long)n[1] * k);
+    }
+    Geo coarsen() const {
+        int nn[3] = {n[0] / 2, n[1] / 2, dim == 3 ? n[2] / 2 : 1};
+        return Geo(dim, nn, dx * 2.0);
+    }
+};
+
+inline int edge_of(int dim, int c, int d) {
+    if (dim == 2) return 0;
+    int a = std::min(c, d), b = std::max(c, d);
+    if (a == 0 && b == 1) return 0;  // xy
+    if (a == 0 && b == 2) return 1;  // xz
+    return 2;                        // yz
+}
+
+inline int n_edge(int dim) { return dim == 2 ? 1 : 3; }
+
+template <class F>
+inline void forall(const Geo& g, F f) {
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = 0; k < g.n[2]; k++)
+        for (int j = 0; j < g.n[1]; j++)
+            for (int i = 0; i < g.n[0]; i++) f(i, j, k);
+}
+
+// deterministic sum of f(i,j,k) over all cells
+template <class F>
+inline double reduce_sum(const Geo& g, F f) {
+    long rows = (long)g.n[1] * g.n[2];
+    std::vector<double> part(rows, 0.0);
+#pragma omp parallel for schedule(static)
+    for (long r = 0; r < rows; r++) {
+        int j = (int)(r % g.n[1]), k = (int)(r / g.n[1]);
+        double s = 0.0;
+        for (int i = 0; i < g.n[0]; i++) s += f(i, j, k);
+        part[r] = s;
+    }
+    double s = 0.0;
+    for (long r = 0; r < rows; r++) s += part[r];
+    return s;
+}
+
+template <class F>
+inline double reduce_max(const Geo& g, F f) {
+    long rows = (long)g.n[1] * g.n[2];
+    std::vector<double> part(rows, 0.0);
+#pragma omp parallel for schedule(static)
+    for (long r = 0; r < rows; r++) {
+        int j = (int)(r % g.n[1]), k = (int)(r / g.n[1]);
+        double s = 0.0;
+        for (int i = 0; i < g.n[0]; i++) s = std::max(s, f(i, j, k));
+        part[r] = s;
+    }
+    double s = 0.0;
+    for (long r = 0; r < rows; r++) s = std::max(s, part[r]);
+    return s;
+}
+
+// ---------------------------------------------------------------------
+// staggered multigrid level: coefficients and work arrays
+// ---------------------------------------------------------------------
+struct SLevel {
+    Geo g;
+    Vec alpha[3];  // theta_alpha * alpha on faces
+    Vec beta, gamma;
+    Vec bed[3];    // 2D: node; 3D: xy, xz, yz edges
+    Vec phi[3], rhs[3], Lphi[3];
+};
+
+// (theta*alpha - L) phi on one face of component c; returns the value and
+// the diagonal coefficient.  Restates stag_applyop_2d/_3d
+// (stag_applyop.f90:212-1075) for all visc_type, with the periodic wrap
+// standing in for the ghost-cell fill; the diagonal is the 'fac' of
+// stag_mg_update (stag_mg_solver.f90:1764-2458).
+inline double lface(const Geo& g, int visc, const Vec* alpha, const Vec& beta,
+                    const Vec& gamma, const Vec* bed, const double* const* phi,
+                    int c, int i, int j, int k, double* diag_out) {
+    const int dim = g.dim;
+    const double q = 1.0 / (g.dx * g.dx);
+    int ec[3] = {0, 0, 0};
+    ec[c] = 1;
+    const long f = g.id(i, j, k);
+    const long fpc = g.id(i + ec[0], j + ec[1], k + ec[2]);
+    const long fmc = g.id(i - ec[0], j - ec[1], k - ec[2]);
+    const double ph = phi[c][f];
+    const double a = alpha[c][f];
+    if (visc < 0) {
+        const double bp = beta[f], bm = beta[fmc];
+        double kp, km;
+        if (visc == -1) {
+            kp = bp; km = bm;
+        } else if (visc == -2) {
+            kp = 2.0 * bp; km = 2.0 * bm;
+        } else {
+            kp = (4.0 / 3.0) * bp + gamma[f];
+            km = (4.0 / 3.0) * bm + gamma[fmc];
+        }
+        double s = kp + km;
+        double nb = phi[c][fpc] * kp + phi[c][fmc] * km;
+        double cross = 0.0;
+        for (int d = 0; d < dim; d++) {
+            if (d == c) continue;
+            int ed[3] = {0, 0, 0};
+            ed[d] = 1;
+            const long fpd = g.id(i + ed[0], j + ed[1], k + ed[2]);
+            const long fmd = g.id(i - ed[0], j - ed[1], k - ed[2]);
+            const Vec& E = bed[edge_of(dim, c, d)];
+            const double elo = E[f], ehi = E[fpd];
+            s += elo + ehi;
+            nb += phi[c][fpd] * ehi + phi[c][fmd] * elo;
+            if (visc != -1) {
+                const long fmcpd = g.id(i - ec[0] + ed[0], j - ec[1] + ed[1], k - ec[2] + ed[2]);
+                double tp = 0.0, tm = 0.0;
+                if (visc == -3) {
+                    tp = -(2.0 / 3.0) * bp + gamma[f];
+                    tm = -(2.0 / 3.0) * bm + gamma[fmc];
+                }
+                cross += phi[d][fpd] * (ehi + tp) - phi[d][f] * (elo + tp)
+                       - phi[d][fmcpd] * (ehi + tm) + phi[d][fmc] * (elo + tm);
+            }
+        }
+        const double diag = a + s * q;
+        if (diag_out) *diag_out = diag;
+        return ph * diag - (nb + cross) * q;
+    }
+    // constant coefficients: beta, gamma taken from the first cell
+    // (stag_applyop.f90:654-656 'b = beta(xlo(1),xlo(2),xlo(3))')
+    const double b = beta[0], cg = gamma[0];
+    const double own = phi[c][fpc] + phi[c][fmc];
+    double oth = 0.0, cross = 0.0;
+    for (int d = 0; d < dim; d++) {
+        if (d == c) continue;
+        int ed[3] = {0, 0, 0};
+        ed[d] = 1;
+        const long fpd = g.id(i + ed[0], j + ed[1], k + ed[2]);
+        const long fmd = g.id(i - ed[0], j - ed[1], k - ed[2]);
+        oth += phi[c][fpd] + phi[c][fmd];
+        if (visc != 1) {
+            const long fmcpd = g.id(i - ec[0] + ed[0], j - ec[1] + ed[1], k - ec[2] + ed[2]);
+            cross += phi[d][fpd] - phi[d][f] - phi[d][fmcpd] + phi[d][fmc];
+        }
+    }
+    double diag, L;
+    if (visc == 1) {
+        diag = a + (2.0 * dim) * b * q;
+        L = ph * diag - (own + oth) * b * q;
+    } else if (visc == 2) {
+        diag = a + (2.0 * dim + 2.0) * b * q;
+        L = ph * diag - (2.0 * own + oth + cross) * b * q;
+    } else {
+        diag = a + ((8.0 / 3.0 + 2.0 * (dim - 1)) * b + 2.0 * cg) * q;
+        L = ph * diag - (own * ((4.0 / 3.0) * b + cg) + oth * b + cross * ((1.0 / 3.0) * b + cg)) * q;
+    }
+    if (diag_out) *diag_out = diag;
+    return L;
+}
+
+inline bool in_color(int color, int c, int i, int j, int k) {
+    if (color == 0) return true;
+    if ((color - 1) / 2 != c) return false;
+    return ((i + j + k) & 1) == ((color + 1) & 1);
+}
+
+// stag_applyop_level (stag_applyop.f90:70-210)
+void s_applyop(SLevel& L, int visc, int color) {
+    const Geo& g = L.g;
+    const double* ph[3] = {L.phi[0].data(), L.phi[1].data(), g.dim == 3 ? L.phi[2].data() : nullptr};
+    for (int c = 0; c < g.dim; c++) {
+        if (color != 0 && (color - 1) / 2 != c) continue;
+        double* out = L.Lphi[c].data();
+        forall(g, [&](int i, int j, int k) {
+            if (!in_color(color, c, i, j, k)) return;
+            out[g.id(i, j, k)] = lface(g, visc, L.alpha, L.beta, L.gamma, L.bed, ph, c, i, j, k, nullptr);
+        });
+    }
+}
+
+// one colour of the smoother: applyop(colour) then stag_mg_update(colour)
+// (stag_mg_solver.f90:360-396, 1632-2458).  Two passes, so the update of a
+// colour never sees another update of the same colour.
+void s_smooth(SLevel& L, int visc, double omega, int color) {
+    const Geo& g = L.g;
+    const double* ph[3] = {L.phi[0].data(), L.phi[1].data(), g.dim == 3 ? L.phi[2].data() : nullptr};
+    std::vector<Vec> diag(g.dim);
+    for (int c = 0; c < g.dim; c++) {
+        if (color != 0 && (color - 1) / 2 != c) continue;
+        diag[c].assign(g.nc, 0.0);
+        double* out = L.Lphi[c].data();
+        double* dg = diag[c].data();
+        forall(g, [&](int i, int j, int k) {
+            if (!in_color(color, c, i, j, k)) return;
+            long f = g.id(i, j, k);
+            out[f] = lface(g, visc, L.alpha, L.beta, L.gamma, L.bed, ph, c, i, j, k, &dg[f]);
+        });
+    }
+    for (int c = 0; c < g.dim; c++) {
+        if (color != 0 && (color - 1) / 2 != c) continue;
+        double* p = L.phi[c].data();
+        const double* r = L.rhs[c].data();
+        const double* lp = L.Lphi[c].data();
+        const double* dg = diag[c].data();
+        forall(g, [&](int i, int j, int k) {
+            if (!in_color(color, c, i, j, k)) return;
+            long f = g.id(i, j, k);
+            p[f] = p[f] + omega * (r[f] - lp[f]) / dg[f];
+        });
+    }
+}
+
+// stag_restriction (stag_mg_solver.f90:966-1170): full 6/12-point stencil,
+// or the 2/4-point 'simple' stencil used to coarsen alpha.
+void s_restrict(const Geo& gf, const Geo& gc, const Vec* fine, Vec* coarse, bool simple) {
+    const int dim = gf.dim;
+    for (int c = 0; c < dim; c++) {
+        const double* F = fine[c].data();
+        double* C = coarse[c].data();
+        int a = (c == 0) ? 1 : 0;
+        int b = (dim == 3) ? ((c == 2) ? 1 : 2) : -1;
+        forall(gc, [&](int i, int j, int k) {
+            int I[3] = {2 * i, 2 * j, 2 * k};
+            auto at = [&](int o, int pa, int pb) {
+                int q[3] = {I[0], I[1], I[2]};
+                q[c] += o;
+                q[a] += pa;
+                if (b >= 0) q[b] += pb;
+                return F[gf.id(q[0], q[1], q[2])];
+            };
+            double v;
+            if (dim == 2) {
+                if (simple) v = 0.5 * (at(0, 0, 0) + at(0, 1, 0));
+                else v = 0.25 * (at(0, 0, 0) + at(0, 1, 0))
+                       + 0.125 * (at(1, 0, 0) + at(1, 1, 0) + at(-1, 0, 0) + at(-1, 1, 0));
+            } else {
+                if (simple) v = 0.25 * (at(0, 0, 0) + at(0, 1, 0) + at(0, 0, 1) + at(0, 1, 1));
+                else v = 0.125 * (at(0, 0, 0) + at(0, 1, 0) + at(0, 0, 1) + at(0, 1, 1))
+                       + 0.0625 * (at(1, 0, 0) + at(1, 1, 0) + at(1, 0, 1) + at(1, 1, 1))
+                       + 0.0625 * (at(-1, 0, 0) + at(-1, 1, 0) + at(-1, 0, 1) + at(-1, 1, 1));
+            }
+            C[gc.id(i, j, k)] = v;
+        });
+    }
+}
+
+// cc_restriction (stag_mg_solver.f90:868-963): average of the 2^dim children
+void cc_average(const Geo& gf, const Geo& gc, const Vec& F, Vec& C) {
+    forall(gc, [&](int i, int j, int k) {
+        double v;
+        if (gf.dim == 2) {
+            v = 0.25 * (F[gf.id(2 * i, 2 * j, 0)] + F[gf.id(2 * i + 1, 2 * j, 0)]
+                      + F[gf.id(2 * i, 2 * j + 1, 0)] + F[gf.id(2 * i + 1, 2 * j + 1, 0)]);
+        } else {
+            v = 0.125 * (F[gf.id(2 * i, 2 * j, 2 * k)] + F[gf.id(2 * i + 1, 2 * j, 2 * k)]
+                       + F[gf.id(2 * i, 2 * j + 1, 2 * k)] + F[gf.id(2 * i + 1, 2 * j + 1, 2 * k)]
+                       + F[gf.id(2 * i, 2 * j, 2 * k + 1)] + F[gf.id(2 * i + 1, 2 * j, 2 * k + 1)]
+                       + F[gf.id(2 * i, 2 * j + 1, 2 * k + 1)] + F[gf.id(2 * i + 1, 2 * j + 1, 2 * k + 1)]);
+        }
+        C[gc.id(i, j, k)] = v;
+    });
+}
+
+// nodal_restriction (2D injection, stag_mg_solver.f90:1224-1239) and
+// edge_restriction (3D 2-point, stag_mg_solver.f90:1321-1362)
+void edge_coarsen(const Geo& gf, const Geo& gc, const Vec* F, Vec* C) {
+    if (gf.dim == 2) {
+        forall(gc, [&](int i, int j, int k) { C[0][gc.id(i, j, k)] = F[0][gf.id(2 * i, 2 * j, 0)]; });
+        return;
+    }
+    forall(gc, [&](int i, int j, int k) {
+        long c = gc.id(i, j, k);
+        C[0][c] = 0.5 * (F[0][gf.id(2 * i, 2 * j, 2 * k)] + F[0][gf.id(2 * i, 2 * j, 2 * k + 1)]);
+        C[1][c] = 0.5 * (F[1][gf.id(2 * i, 2 * j, 2 * k)] + F[1][gf.id(2 * i, 2 * j + 1, 2 * k)]);
+        C[2][c] = 0.5 * (F[2][gf.id(2 * i, 2 * j, 2 * k)] + F[2][gf.id(2 * i + 1, 2 * j, 2 * k)]);
+    });
+}
+
+// stag_prolongation (stag_mg_solver.f90:1365-1628): fine += P coarse
+void s_prolong_add(const Geo& gf, const Geo& gc, Vec* fine, const Vec* coarse) {
+    const int dim = gf.dim;
+    for (int c = 0; c < dim; c++) {
+        double* F = fine[c].data();
+        const double* C = coarse[c].data();
+        int a = (c == 0) ? 1 : 0;
+        int b = (dim == 3) ? ((c == 2) ? 1 : 2) : -1;
+        forall(gf, [&](int i, int j, int k) {
+            int I[3] = {i, j, k};
+            int h[3] = {i / 2, j / 2, k / 2};
+            int oa = (I[a] % 2 == 0) ? -1 : 1;
+            int ob = (b >= 0) ? ((I[b] % 2 == 0) ? -1 : 1) : 0;
+            auto at = [&](int o, int pa, int pb) {
+                int q[3] = {h[0], h[1], h[2]};
+                q[c] += o;
+                q[a] += pa;
+                if (b >= 0) q[b] += pb;
+                return C[gc.id(q[0], q[1], q[2])];
+            };
+            long f = gf.id(i, j, k);
+            bool even = (I[c] % 2 == 0);
+            double v;
+            if (dim == 2) {
+                if (even) v = 0.75 * at(0, 0, 0) + 0.25 * at(0, oa, 0);
+                else v = 0.375 * at(0, 0, 0) + 0.125 * at(0, oa, 0) + 0.375 * at(1, 0, 0) + 0.125 * at(1, oa, 0);
+            } else {
+                const double n16 = 9.0 / 16.0, t16 = 3.0 / 16.0, o16 = 1.0 / 16.0;
+                const double n32 = 9.0 / 32.0, t32 = 3.0 / 32.0, o32 = 1.0 / 32.0;
+                if (even) v = n16 * at(0, 0, 0) + t16 * at(0, oa, 0) + t16 * at(0, 0, ob) + o16 * at(0, oa, ob);
+                else v = n32 * at(0, 0, 0) + t32 * at(0, oa, 0) + t32 * at(0, 0, ob) + o32 * at(0, oa, ob)
+                       + n32 * at(1, 0, 0) + t32 * at(1, oa, 0) + t32 * at(1, 0, ob) + o32 * at(1, oa, ob);
+            }
+            F[f] = F[f] + v;
+        });
+    }
+}
+
+int nlevs_mg(const Geo& g, int minwidth) {
+    // compute_nlevs_mg (stag_mg_layout.f90:179-222), one box
+    int nl = -1;
+    for (int d = 0; d < g.dim; d++) {
+        int t = g.n[d], r = 1;
+        while (t % 2 == 0 && t / minwidth != 1) {
+            t /= 2;
+            r++;
+        }
+        nl = (nl < 0) ? r : std::min(nl, r);
+    }
+    return nl;
+}
+
+// stag_mg_solver (stag_mg_solver.f90:37-863), single box (the "fancy"
+// bottom solver needs n_cells/max_grid_size >= 2 and is never taken here)
+int stag_mg(const Geo& g0, int visc, const fhd_gmres_params* p, const double* const alpha_fc[],
+            const double* beta, const double* const beta_ed[], const double* gamma, double theta,
+            double* const phi[], const double* const rhs[], double* hist = nullptr) {
+    const int dim = g0.dim;
+    const int nl = nlevs_mg(g0, p->stag_mg_minwidth);
+    std::vector<SLevel> L(nl);
+    for (int l = 0; l < nl; l++) {
+        L[l].g = (l == 0) ? g0 : L[l - 1].g.coarsen();
+        const long nc = L[l].g.nc;
+        for (int c = 0; c < dim; c++) {
+            L[l].alpha[c].assign(nc, 0.0);
+            L[l].phi[c].assign(nc, 0.0);
+            L[l].rhs[c].assign(nc, 0.0);
+            L[l].Lphi[c].assign(nc, 0.0);
+        }
+        L[l].beta.assign(nc, 0.0);
+        L[l].gamma.assign(nc, 0.0);
+        for (int e = 0; e < n_edge(dim); e++) L[l].bed[e].assign(nc, 0.0);
+    }
+    const long nc0 = g0.nc;
+    for (int c = 0; c < dim; c++)
+        for (long f = 0; f < nc0; f++) L[0].alpha[c][f] = alpha_fc[c][f] * theta;
+    std::copy(beta, beta + nc0, L[0].beta.begin());
+    std::copy(gamma, gamma + nc0, L[0].gamma.begin());
+    for (int e = 0; e < n_edge(dim); e++) std::copy(beta_ed[e], beta_ed[e] + nc0, L[0].bed[e].begin());
+    for (int l = 1; l < nl; l++) {
+        cc_average(L[l - 1].g, L[l].g, L[l - 1].beta, L[l].beta);
+        cc_average(L[l - 1].g, L[l].g, L[l - 1].gamma, L[l].gamma);
+        s_restrict(L[l - 1].g, L[l].g, L[l - 1].alpha, L[l].alpha, true);
+        edge_coarsen(L[l - 1].g, L[l].g, L[l - 1].bed, L[l].bed);
+    }
+    for (int c = 0; c < dim; c++) {
+        std::copy(phi[c], phi[c] + nc0, L[0].phi[c].begin());
+        std::copy(rhs[c], rhs[c] + nc0, L[0].rhs[c].begin());
+    }
+    // initial residual (stag_mg_solver.f90:259-313)
+    double resid0[3] = {0, 0, 0};
+    s_applyop(L[0], visc, 0);
+    for (int c = 0; c < dim; c++) {
+        const double* lp = L[0].Lphi[c].data();
+        const double* r = L[0].rhs[c].data();
+        resid0[c] = reduce_max(g0, [&](int i, int j, int k) { long f = g0.id(i, j, k); return std::fabs(lp[f] - r[f]); });
+    }
+    // L2 norm of the initial residual, for the per-V-cycle history that
+    // stag_mg_verbosity >= 1 prints (stag_mg_solver.f90:782-785)
+    double r0l2 = 0.0;
+    if (hist) {
+        for (int c = 0; c < dim; c++) {
+            const double* lp = L[0].Lphi[c].data();
+            const double* r = L[0].rhs[c].data();
+            r0l2 += reduce_sum(g0, [&](int i, int j, int k) { long f = g0.id(i, j, k); double d = lp[f] - r[f]; return d * d; });
+        }
+    }
+    bool allzero = true, anyzero = false;
+    double rmax = 0.0;
+    for (int c = 0; c < dim; c++) {
+        allzero = allzero && (resid0[c] == 0.0);
+        anyzero = anyzero || (resid0[c] == 0.0);
+        rmax = std::max(rmax, resid0[c]);
+    }
+    if (allzero) return 0;
+    if (anyzero)
+        for (int c = 0; c < dim; c++) resid0[c] = rmax;
+
+    std::vector<int> colors;
+    if (p->stag_mg_smoother == 0) colors.push_back(0);
+    else for (int c = 1; c <= 2 * dim; c++) colors.push_back(c);
+    const double omega = p->stag_mg_omega;
+
+    for (int vc = 1; vc <= p->stag_mg_max_vcycles; vc++) {
+        for (int l = 1; l < nl; l++)
+            for (int c = 0; c < dim; c++) std::fill(L[l].phi[c].begin(), L[l].phi[c].end(), 0.0);
+        for (int l = 0; l < nl - 1; l++) {
+            for (int m = 0; m < p->stag_mg_nsmooths_down; m++)
+                for (int col : colors) s_smooth(L[l], visc, omega, col);
+            s_applyop(L[l], visc, 0);
+            for (int c = 0; c < dim; c++) {
+                double* lp = L[l].Lphi[c].data();
+                const double* r = L[l].rhs[c].data();
+                for (long f = 0; f < L[l].g.nc; f++) lp[f] = -(lp[f] - r[f]);
+            }
+            s_restrict(L[l].g, L[l + 1].g, L[l].Lphi, L[l + 1].rhs, false);
+        }
+        for (int m = 0; m < p->stag_mg_nsmooths_bottom; m++)
+            for (int col : colors) s_smooth(L[nl - 1], visc, omega, col);
+        for (int l = nl - 2; l >= 0; l--) {
+            s_prolong_add(L[l].g, L[l + 1].g, L[l].phi, L[l + 1].phi);
+            for (int m = 0; m < p->stag_mg_nsmooths_up; m++)
+                for (int col : colors) s_smooth(L[l], visc, omega, col);
+        }
+        if (vc == p->stag_mg_max_vcycles && !hist) break;  // the final residual decides nothing
+        s_applyop(L[0], visc, 0);
+        bool done = true;
+        double rl2 = 0.0;
+        for (int c = 0; c < dim; c++) {
+            const double* lp = L[0].Lphi[c].data();
+            const double* r = L[0].rhs[c].data();
+            double rr = reduce_max(g0, [&](int i, int j, int k) { long f = g0.id(i, j, k); return std::fabs(lp[f] - r[f]); });
+            done = done && (rr / resid0[c] < p->stag_mg_rel_tol);
+            if (hist) rl2 += reduce_sum(g0, [&](int i, int j, int k) { long f = g0.id(i, j, k); double d = lp[f] - r[f]; return d * d; });
+        }
+        if (hist) hist[vc - 1] = std::sqrt(rl2) / std::sqrt(r0l2);
+        if (done || vc == p->stag_mg_max_vcycles) break;
+    }
+    for (int c = 0; c < dim; c++) std::copy(L[0].phi[c].begin(), L[0].phi[c].end(), phi[c]);
+    return 0;
+}
+
+// ---------------------------------------------------------------------
+// cell-centred pressure multigrid (macproject.f90:34-316 calling FBoxLib
+// ml_cc_solve).  Semantics restated from PreconditionerNotes.tex:484-575:
+// red-black Gauss-Seidel (omega = 1), restriction by averaging the 2^dim
+// children, piecewise-constant prolongation, nu1/nu2 smooths per level,
+// mg_nsmooths_bottom smooths on the coarsest level, mg_max_vcycles cycles.
+// ---------------------------------------------------------------------
+struct CLevel {
+    Geo g;
+    Vec a[3];  // face coefficient (alphainv), low side of each cell
+    Vec phi, rhs, res;
+};
+
+inline double c_lap(const Geo& g, const Vec* a, const double* phi, int i, int j, int k, double* diag) {
+    const double q = 1.0 / (g.dx * g.dx);
+    const long f = g.id(i, j, k);
+    const double pc = phi[f];
+    double s = 0.0, dg = 0.0;
+    for (int d = 0; d < g.dim; d++) {
+        int e[3] = {0, 0, 0};
+        e[d] = 1;
+        const long fp = g.id(i + e[0], j + e[1], k + e[2]);
+        const long fm = g.id(i - e[0], j - e[1], k - e[2]);
+        const double ahi = a[d][fp], alo = a[d][f];
+        s += ahi * (phi[fp] - pc) - alo * (pc - phi[fm]);
+        dg += ahi + alo;
+    }
+    if (diag) *diag = -dg * q;
+    return s * q;
+}
+
+void c_gsrb(CLevel& L) {
+    const Geo& g = L.g;
+    for (int color = 0; color < 2; color++) {
+        double* r = L.res.data();
+        const double* ph = L.phi.data();
+        forall(g, [&](int i, int j, int k) {
+            if (((i + j + k) & 1) != color) return;
+            long f = g.id(i, j, k);
+            double dg;
+            double lp = c_lap(g, L.a, ph, i, j, k, &dg);
+            r[f] = (L.rhs[f] - lp) / dg;
+        });
+        double* p = L.phi.data();
+        forall(g, [&](int i, int j, int k) {
+            if (((i + j + k) & 1) != color) return;
+            long f = g.id(i, j, k);
+            p[f] = p[f] + r[f];
+        });
+    }
+}
+
+void c_vcycle(std::vector<CLevel>& L, int l, const fhd_gmres_params* p) {
+    CLevel& C = L[l];
+    const int nl = (int)L.size();
+    if (l == nl - 1) {
+        for (int m = 0; m < p->mg_nsmooths_bottom; m++) c_gsrb(C);
+        return;
+    }
+    for (int m = 0; m < p->mg_nsmooths_down; m++) c_gsrb(C);
+    const Geo& g = C.g;
+    forall(g, [&](int i, int j, int k) {
+        long f = g.id(i, j, k);
+        C.res[f] = C.rhs[f] - c_lap(g, C.a, C.phi.data(), i, j, k, nullptr);
+    });
+    CLevel& D = L[l + 1];
+    cc_average(g, D.g, C.res, D.rhs);
+    std::fill(D.phi.begin(), D.phi.end(), 0.0);
+    c_vcycle(L, l + 1, p);
+    forall(g, [&](int i, int j, int k) {
+        long f = g.id(i, j, k);
+        C.phi[f] = C.phi[f] + D.phi[D.g.id(i / 2, j / 2, k / 2)];
+    });
+    for (int m = 0; m < p->mg_nsmooths_up; m++) c_gsrb(C);
+}
+
+int macproject_impl(const Geo& g0, const fhd_gmres_params* p, double* phi, const double* const ainv[],
+                    const double* rhs) {
+    const int dim = g0.dim;
+    const int nl = nlevs_mg(g0, p->mg_minwidth);
+    std::vector<CLevel> L(nl);
+    for (int l = 0; l < nl; l++) {
+        L[l].g = (l == 0) ? g0 : L[l - 1].g.coarsen();
+        long nc = L[l].g.nc;
+        for (int d = 0; d < dim; d++) L[l].a[d].assign(nc, 0.0);
+        L[l].phi.assign(nc, 0.0);
+        L[l].rhs.assign(nc, 0.0);
+        L[l].res.assign(nc, 0.0);
+    }
+    for (int d = 0; d < dim; d++) std::copy(ainv[d], ainv[d] + g0.nc, L[0].a[d].begin());
+    for (int l = 1; l < nl; l++) s_restrict(L[l - 1].g, L[l].g, L[l - 1].a, L[l].a, true);
+    std::copy(rhs, rhs + g0.nc, L[0].rhs.begin());
+    const double r0 = reduce_max(g0, [&](int i, int j, int k) { return std::fabs(rhs[g0.id(i, j, k)]); });
+    if (r0 > 0.0) {
+        for (int vc = 1; vc <= p->mg_max_vcycles; vc++) {
+            c_vcycle(L, 0, p);
+            if (vc == p->mg_max_vcycles) break;
+            CLevel& C = L[0];
+            double rr = reduce_max(g0, [&](int i, int j, int k) {
+                return std::fabs(C.rhs[g0.id(i, j, k)] - c_lap(g0, C.a, C.phi.data(), i, j, k, nullptr));
+            });
+            if (rr <= std::max(p->mg_rel_tol * r0, p->mg_abs_tol)) break;
+        }
+    }
+    std::copy(L[0].phi.begin(), L[0].phi.end(), phi);
+    return 0;
+}
+
+// ---------------------------------------------------------------------
+// div / grad / norms (div_and_grad.f90:417-703, 884-1035;
+// norm_inner_product.f90)
+// ---------------------------------------------------------------------
+void c_div(const Geo& g, const double* const u[], double* div, bool increment) {
+    const double dxinv = 1.0 / g.dx;
+    forall(g, [&](int i, int j, int k) {
+        long f = g.id(i, j, k);
+        double s = (u[0][g.id(i + 1, j, k)] - u[0][f]) * dxinv + (u[1][g.id(i, j + 1, k)] - u[1][f]) * dxinv;
+        if (g.dim == 3) s += (u[2][g.id(i, j, k + 1)] - u[2][f]) * dxinv;
+        div[f] = increment ? div[f] + s : s;
+    });
+}
+
+void c_grad(const Geo& g, const double* p, double* const gp[]) {
+    const double dxinv = 1.0 / g.dx;
+    for (int d = 0; d < g.dim; d++) {
+        int e[3] = {0, 0, 0};
+        e[d] = 1;
+        forall(g, [&](int i, int j, int k) {
+            long f = g.id(i, j, k);
+            gp[d][f] = (p[f] - p[g.id(i - e[0], j - e[1], k - e[2])]) * dxinv;
+        });
+    }
+}
+
+double dot(const Geo& g, const double* a, const double* b) {
+    return reduce_sum(g, [&](int i, int j, int k) { long f = g.id(i, j, k); return a[f] * b[f]; });
+}
+
+double sum(const Geo& g, const double* a) {
+    return reduce_sum(g, [&](int i, int j, int k) { return a[g.id(i, j, k)]; });
+}
+
+// a Stokes vector (u_0..u_{dim-1}, p), each of nc entries
+struct SV {
+    Vec c[4];
+    int dim = 2;
+    void init(int d, long nc) {
+        dim = d;
+        for (int i = 0; i <= d; i++) c[i].assign(nc, 0.0);
+    }
+    double* u(int d) { return c[d].data(); }
+    double* p() { return c[dim].data(); }
+};
+
+void up_ptrs(SV& v, double** u, double*& p) {
+    for (int d = 0; d < v.dim; d++) u[d] = v.u(d);
+    p = v.p();
+}
+
+double stag_l2(const Geo& g, const double* const u[]) {
+    double s = 0.0;
+    for (int d = 0; d < g.dim; d++) s += dot(g, u[d], u[d]);
+    return std::sqrt(s);
+}
+
+int apply_matrix_impl(const Geo& g, int visc, double* const b_u[], double* b_p, const double* const x_u[],
+                      const double* x_p, const double* const alpha_fc[], const double* beta,
+                      const double* const beta_ed[], const double* gamma, double theta) {
+    const int dim = g.dim;
+    Vec alpha[3], bed[3];
+    Vec vb(beta, beta + g.nc), vg(gamma, gamma + g.nc);
+    for (int c = 0; c < dim; c++) {
+        alpha[c].resize(g.nc);
+        for (long f = 0; f < g.nc; f++) alpha[c][f] = alpha_fc[c][f] * theta;
+    }
+    for (int e = 0; e < n_edge(dim); e++) bed[e].assign(beta_ed[e], beta_ed[e] + g.nc);
+    const double* ph[3] = {x_u[0], x_u[1], dim == 3 ? x_u[2] : nullptr};
+    for (int c = 0; c < dim; c++) {
+        double* out = b_u[c];
+        forall(g, [&](int i, int j, int k) {
+            out[g.id(i, j, k)] = lface(g, visc, alpha, vb, vg, bed, ph, c, i, j, k, nullptr);
+        });
+    }
+    std::vector<Vec> gp(dim, Vec(g.nc));
+    double* gpp[3] = {gp[0].data(), gp[1].data(), dim == 3 ? gp[2].data() : nullptr};
+    c_grad(g, x_p, gpp);
+    for (int c = 0; c < dim; c++)
+        for (long f = 0; f < g.nc; f++) b_u[c][f] = b_u[c][f] + gp[c][f];
+    c_div(g, x_u, b_p, false);
+    for (long f = 0; f < g.nc; f++) b_p[f] = b_p[f] * -1.0;
+    return 0;
+}
+
+// apply_precon (apply_precon.f90:29-475), visc_schur_approx = 0
+int apply_precon_impl(const Geo& g, int visc, const fhd_gmres_params* p, const double* const b_u[],
+                      const double* b_p, double* const x_u[], double* x_p, const double* const alpha_fc[],
+                      const double* beta, const double* const beta_ed[], const double* gamma, double theta) {
+    const int dim = g.dim;
+    const long nc = g.nc;
+    const int pt = p->precon_type;
+    const int apt = std::abs(pt);
+    const int av = std::abs(visc);
+    if (p->visc_schur_approx != 0) return FHD_ERR_UNSUPPORTED;
+    if (apt < 1 || apt > 5) return FHD_ERR_UNSUPPORTED;
+    Vec phi(nc, 0.0), mac_rhs(nc, 0.0);
+    std::vector<Vec> ainv(dim, Vec(nc));
+    for (int c = 0; c < dim; c++)
+        for (long f = 0; f < nc; f++) ainv[c][f] = 1.0 / alpha_fc[c][f];
+    const double* ainvp[3] = {ainv[0].data(), ainv[1].data(), dim == 3 ? ainv[2].data() : nullptr};
+    for (int c = 0; c < dim; c++) std::fill(x_u[c], x_u[c] + nc, 0.0);
+
+    auto stagmg = [&](double* const ph[], const double* const rh[]) {
+        return stag_mg(g, visc, p, alpha_fc, beta, beta_ed, gamma, theta, ph, rh);
+    };
+    auto subtract_weighted_gradp = [&](double* const u[], const double* w[], const double* ph) {
+        std::vector<Vec> gp(dim, Vec(nc));
+        double* gpp[3] = {gp[0].data(), gp[1].data(), dim == 3 ? gp[2].data() : nullptr};
+        c_grad(g, ph, gpp);
+        for (int c = 0; c < dim; c++)
+            for (long f = 0; f < nc; f++) u[c][f] = u[c][f] + (-1.0) * (gp[c][f] * (w ? w[c][f] : 1.0));
+    };
+    // x_p = theta*Phi - c*beta*mac_rhs  (simple_schur_complement,
+    // apply_precon.f90:479-534); also case 1 with +precon_type
+    auto simple_schur = [&]() {
+        for (long f = 0; f < nc; f++) {
+            double v;
+            if (av == 1 || av == 2) {
+                v = mac_rhs[f] * -1.0;
+                v = v * beta[f];
+                if (av == 2) v = v * 2.0;
+            } else {
+                v = mac_rhs[f] * (-4.0 / 3.0);
+                v = v * beta[f];
+                double m = (mac_rhs[f] * -1.0) * gamma[f];
+                v = v + m;
+            }
+            if (std::fabs(theta) > 0.0) v = v + phi[f] * theta;
+            x_p[f] = v;
+        }
+    };
+
+    if (apt == 1) {
+        stagmg(x_u, b_u);
+        c_div(g, x_u, mac_rhs.data(), false);
+        for (long f = 0; f < nc; f++) mac_rhs[f] = mac_rhs[f] + b_p[f];
+        macproject_impl(g, p, phi.data(), ainvp, mac_rhs.data());
+        subtract_weighted_gradp(x_u, ainvp, phi.data());
+        Vec xp(nc);
+        if (pt == 1 || theta == 0.0) {
+            for (long f = 0; f < nc; f++) xp[f] = mac_rhs[f] * -1.0;
+        } else {
+            // x_p = -L_alpha Phi (cc_applyop with zero cell coefficient)
+            CLevel C;
+            C.g = g;
+            for (int d = 0; d < dim; d++) C.a[d] = ainv[d];
+            forall(g, [&](int i, int j, int k) {
+                xp[g.id(i, j, k)] = -c_lap(g, C.a, phi.data(), i, j, k, nullptr);
+            });
+        }
+        for (long f = 0; f < nc; f++) {
+            double v = xp[f];
+            if (av == 1 || av == 2) {
+                v = v * beta[f];
+                if (av == 2) v = v * 2.0;
+            } else {
+                double m = v * gamma[f];
+                v = v * beta[f];
+                v = v * (4.0 / 3.0);
+                v = v + m;
+            }
+            v = v + phi[f] * theta;
+            x_p[f] = v;
+        }
+    } else if (apt == 2 || apt == 5) {
+        stagmg(x_u, b_u);
+        c_div(g, x_u, mac_rhs.data(), false);
+        for (long f = 0; f < nc; f++) mac_rhs[f] = mac_rhs[f] + b_p[f];
+        if (std::fabs(theta) > 0.0) macproject_impl(g, p, phi.data(), ainvp, mac_rhs.data());
+        simple_schur();
+        if (pt == -2 || pt == -5)
+            for (long f = 0; f < nc; f++) x_p[f] = x_p[f] * -1.0;
+        if (apt == 5) {
+            std::vector<Vec> bt(dim);
+            for (int c = 0; c < dim; c++) bt[c].assign(b_u[c], b_u[c] + nc);
+            double* btp[3] = {bt[0].data(), bt[1].data(), dim == 3 ? bt[2].data() : nullptr};
+            subtract_weighted_gradp(btp, nullptr, x_p);
+            stagmg(x_u, btp);
+        }
+    } else if (apt == 3) {
+        for (long f = 0; f < nc; f++) mac_rhs[f] = (pt == -3) ? b_p[f] * -1.0 : b_p[f];
+        if (std::fabs(theta) > 0.0) macproject_impl(g, p, phi.data(), ainvp, mac_rhs.data());
+        simple_schur();
+        std::vector<Vec> bt(dim);
+        for (int c = 0; c < dim; c++) bt[c].assign(b_u[c], b_u[c] + nc);
+        double* btp[3] = {bt[0].data(), bt[1].data(), dim == 3 ? bt[2].data() : nullptr};
+        subtract_weighted_gradp(btp, nullptr, x_p);
+        stagmg(x_u, btp);
+    } else {  // 4: block diagonal
+        stagmg(x_u, b_u);
+        if (std::fabs(theta) > 0.0) {
+            for (long f = 0; f < nc; f++) mac_rhs[f] = b_p[f];
+            macproject_impl(g, p, phi.data(), ainvp, mac_rhs.data());
+        }
+        for (long f = 0; f < nc; f++) {
+            double ph = phi[f];
+            if (std::fabs(theta) > 0.0) ph = ph * theta;
+            double v = b_p[f] * beta[f];
+            v = v - ph;
+            if (av == 1 && pt == 4) v = v * -1.0;
+            else if (av == 2 && pt == 4) v = v * -2.0;
+            else if (av == 2 && pt == -4) v = v * 2.0;
+            else if (av == 3 && pt == 4) { v = v * (-4.0 / 3.0); v = v + (b_p[f] * gamma[f]) * -1.0; }
+            else if (av == 3 && pt == -4) { v = v * (4.0 / 3.0); v = v + b_p[f] * gamma[f]; }
+            x_p[f] = v;
+        }
+    }
+    // null space (apply_precon.f90:429-460)
+    const double mean_p = sum(g, x_p) / (double)nc;
+    for (long f = 0; f < nc; f++) x_p[f] = x_p[f] - mean_p;
+    if (theta == 0.0) {
+        for (int c = 0; c < dim; c++) {
+            const double mu = sum(g, x_u[c]) / (double)nc;
+            for (long f = 0; f < nc; f++) x_u[c][f] = x_u[c][f] - mu;
+        }
+    }
+    return 0;
+}
+
+// gmres (gmres.f90:32-619)
+int gmres_impl(const Geo& g, int visc, const fhd_gmres_params* p, const double* const b_u_in[],
+               const double* b_p, double* const x_u[], double* x_p, const double* const alpha_fc[],
+               const double* beta_in, const double* const beta_ed_in[], const double* gamma_in,
+               double theta_in, double* norm_pre_rhs, fhd_solve_stats* st) {
+    const int dim = g.dim;
+    const long nc = g.nc;
+    const int m = p->gmres_max_inner;
+    const double w = p->p_norm_weight;
+    const double sf = p->scale_factor;
+    // scaling (gmres.f90:118-135) is applied to private copies
+    std::vector<Vec> bu(dim), bed(n_edge(dim));
+    Vec beta(beta_in, beta_in + nc), gamma(gamma_in, gamma_in + nc);
+    for (int c = 0; c < dim; c++) bu[c].assign(b_u_in[c], b_u_in[c] + nc);
+    for (int e = 0; e < n_edge(dim); e++) bed[e].assign(beta_ed_in[e], beta_ed_in[e] + nc);
+    double theta = theta_in;
+    if (sf != 1.0) {
+        theta = theta * sf;
+        for (long f = 0; f < nc; f++) x_p[f] = x_p[f] * sf;
+        for (int c = 0; c < dim; c++)
+            for (long f = 0; f < nc; f++) bu[c][f] = bu[c][f] * sf;
+        for (long f = 0; f < nc; f++) { beta[f] = beta[f] * sf; gamma[f] = gamma[f] * sf; }
+        for (int e = 0; e < n_edge(dim); e++)
+            for (long f = 0; f < nc; f++) bed[e][f] = bed[e][f] * sf;
+    }
+    const double* bup[3] = {bu[0].data(), bu[1].data(), dim == 3 ? bu[2].data() : nullptr};
+    const double* bedp[3] = {bed[0].data(), dim == 3 ? bed[1].data() : nullptr, dim == 3 ? bed[2].data() : nullptr};
+
+    SV r, wv, tmp;
+    r.init(dim, nc); wv.init(dim, nc); tmp.init(dim, nc);
+    std::vector<SV> V(m + 1);
+    for (auto& v : V) v.init(dim, nc);
+    double* ru[3]; double* rp; up_ptrs(r, ru, rp);
+    double* wu[3]; double* wp; up_ptrs(wv, wu, wp);
+    double* tu[3]; double* tp; up_ptrs(tmp, tu, tp);
+
+    auto precon = [&](const double* const in_u[], const double* in_p, double* const out_u[], double* out_p) {
+        return apply_precon_impl(g, visc, p, in_u, in_p, out_u, out_p, alpha_fc, beta.data(), bedp,
+                                 gamma.data(), theta);
+    };
+    auto matrix = [&](double* const out_u[], double* out_p, const double* const in_u[], const double* in_p) {
+        return apply_matrix_impl(g, visc, out_u, out_p, in_u, in_p, alpha_fc, beta.data(), bedp, gamma.data(),
+                                 theta);
+    };
+    auto snorm = [&](const double* const u[], const double* pp) {
+        double nu = stag_l2(g, u);
+        double np = std::sqrt(dot(g, pp, pp)) * w;
+        return std::sqrt(nu * nu + np * np);
+    };
+
+    std::vector<double> cs(m + 1), sn(m + 1), y(m + 1), s(m + 2);
+    std::vector<double> H((m + 2) * (m + 1), 0.0);
+    auto Hh = [&](int i, int j) -> double& { return H[i * (m + 1) + j]; };  // 1-based i,j
+
+    precon(bup, b_p, tu, tp);
+    const double norm_pre_b = snorm(tu, tp);
+    if (norm_pre_rhs) *norm_pre_rhs = norm_pre_b;
+    const double norm_b = snorm(bup, b_p);
+    int status = 0;
+    if (st) { std::memset(st, 0, sizeof(*st)); st->norm_b = norm_b; st->norm_pre_b = norm_pre_b; }
+    if (norm_b <= p->gmres_abs_tol) {
+        for (int c = 0; c < dim; c++) std::fill(x_u[c], x_u[c] + nc, 0.0);
+        std::fill(x_p, x_p + nc, 0.0);
+        if (sf != 1.0)
+            for (long f = 0; f < nc; f++) x_p[f] = x_p[f] * (1.0 / sf);
+        return 0;
+    }
+    int total_iter = 0, iter = 0, i_copy = 0;
+    double norm_resid = 0, norm_init_resid = 0, norm_resid_Stokes = 0, norm_init_Stokes = 0, norm_resid_est = 0;
+    for (;;) {
+        matrix(tu, tp, x_u, x_p);
+        for (int c = 0; c < dim; c++)
+            for (long f = 0; f < nc; f++) tu[c][f] = (tu[c][f] - bu[c][f]) * -1.0;
+        for (long f = 0; f < nc; f++) tp[f] = (tp[f] - b_p[f]) * -1.0;
+        norm_resid_Stokes = snorm(tu, tp);
+        if (iter == 0) norm_init_Stokes = norm_resid_Stokes;
+        precon(tu, tp, ru, rp);
+        norm_resid = snorm(ru, rp);
+        if (iter == 0) { norm_init_resid = norm_resid; norm_resid_est = norm_resid; }
+        if (total_iter >= p->gmres_max_iter) { status = FHD_WARN_NOT_CONVERGED_MAXITER; break; }
+        else if (total_iter >= p->gmres_min_iter) {
+            if (norm_resid <= p->gmres_rel_tol * std::min(norm_pre_b, norm_init_resid)) {
+                if (norm_resid_Stokes >= 10 * p->gmres_rel_tol * std::min(norm_b, norm_init_Stokes))
+                    status = FHD_WARN_TRUE_RESID;
+                break;
+            } else if (norm_resid <= p->gmres_abs_tol) {
+                break;
+            }
+        }
+        if (iter >= p->gmres_max_outer) { status = FHD_WARN_NOT_CONVERGED_OUTER; break; }
+        iter++;
+        for (int c = 0; c <= dim; c++)
+            for (long f = 0; f < nc; f++) V[0].c[c][f] = r.c[c][f] / norm_resid;
+        std::fill(s.begin(), s.end(), 0.0);
+        s[1] = norm_resid;
+        int i;
+        for (i = 1; i <= m; i++) {
+            total_iter++;
+            i_copy = i;
+            double* vu[3]; double* vp; up_ptrs(V[i - 1], vu, vp);
+            matrix(tu, tp, vu, vp);
+            precon(tu, tp, wu, wp);
+            for (int k = 1; k <= i; k++) {
+                double ip = 0.0;
+                for (int c = 0; c < dim; c++) ip += dot(g, wu[c], V[k - 1].c[c].data());
+                double pp = dot(g, wp, V[k - 1].c[dim].data());
+                Hh(k, i) = ip + (w * w) * pp;
+                for (int c = 0; c <= dim; c++) {
+                    double* wc = wv.c[c].data();
+                    const double* vc = V[k - 1].c[c].data();
+                    for (long f = 0; f < nc; f++) wc[f] = wc[f] - vc[f] * Hh(k, i);
+                }
+            }
+            Hh(i + 1, i) = snorm(wu, wp);
+            if (Hh(i + 1, i) != 0.0) {
+                for (int c = 0; c <= dim; c++)
+                    for (long f = 0; f < nc; f++) V[i].c[c][f] = wv.c[c][f] / Hh(i + 1, i);
+            } else {
+                status = FHD_ERR_ORTHO_BREAKDOWN;
+                goto done;
+            }
+            // least_squares (gmres.f90:531-566)
+            for (int k = 1; k <= i - 1; k++) {
+                double t = cs[k] * Hh(k, i) + sn[k] * Hh(k + 1, i);
+                Hh(k + 1, i) = -sn[k] * Hh(k, i) + cs[k] * Hh(k + 1, i);
+                Hh(k, i) = t;
+            }
+            {   // rotmat (gmres.f90:568-597)
+                double a = Hh(i, i), b = Hh(i + 1, i);
+                if (b == 0.0) { cs[i] = 1.0; sn[i] = 0.0; }
+                else if (std::fabs(b) > std::fabs(a)) { double t = a / b; sn[i] = 1.0 / std::sqrt(1.0 + t * t); cs[i] = t * sn[i]; }
+                else { double t = b / a; cs[i] = 1.0 / std::sqrt(1.0 + t * t); sn[i] = t * cs[i]; }
+            }
+            {
+                double t = cs[i] * s[i];
+                s[i + 1] = -sn[i] * s[i];
+                s[i] = t;
+                Hh(i, i) = cs[i] * Hh(i, i) + sn[i] * Hh(i + 1, i);
+                Hh(i + 1, i) = 0.0;
+            }
+            norm_resid_est = std::fabs(s[i + 1]);
+            if (total_iter >= p->gmres_max_iter) break;
+            else if (total_iter >= p->gmres_min_iter) {
+                if (norm_resid_est <= p->gmres_rel_tol * std::min(norm_pre_b, norm_init_resid) ||
+                    norm_resid_est <= p->gmres_abs_tol)
+                    break;
+            }
+        }
+        {   // SolveUTriangular (gmres.f90:599-619) with k = i_copy-1
+            int k = i_copy - 1;
+            y[k + 1] = s[k + 1] / Hh(k + 1, k + 1);
+            for (int ii = k; ii >= 1; ii--) {
+                double acc = 0.0;
+                for (int jj = ii + 1; jj <= k + 1; jj++) acc += Hh(ii, jj) * y[jj];
+                y[ii] = (s[ii] - acc) / Hh(ii, ii);
+            }
+            // update_sol (gmres.f90:495-529)
+            for (int it = 1; it <= i_copy; it++) {
+                for (long f = 0; f < nc; f++) x_p[f] = x_p[f] + V[it - 1].c[dim][f] * y[it];
+                for (int c = 0; c < dim; c++)
+                    for (long f = 0; f < nc; f++) x_u[c][f] = x_u[c][f] + V[it - 1].c[c][f] * y[it];
+            }
+        }
+    }
+done:
+    if (sf != 1.0)
+        for (long f = 0; f < nc; f++) x_p[f] = x_p[f] * (1.0 / sf);
+    if (st) {
+        st->outer_iters = iter;
+        st->total_iters = total_iter;
+        st->status = status;
+        st->norm_init_resid = norm_init_resid;
+        st->norm_resid = norm_resid;
+        st->norm_resid_Stokes = norm_resid_Stokes;
+        st->norm_init_Stokes = norm_init_Stokes;
+        st->norm_resid_est = norm_resid_est;
+    }
+    return status;
+}
+
+// stochastic_m_fluxdiv (stochastic_m_fluxdiv.f90:42-602), periodic,
+// filtering_width = 0
+int stoch_m_impl(const Geo& g, const fhd_stoch_params* sp, double* const force[], int increment,
+                 const double* eta, const double* const eta_ed[], const double* T, const double* const T_ed[],
+                 double dt, const double* weights, int n_rngs, const double* const W_cc[],
+                 const double* const W_ed[]) {
+    const int dim = g.dim, nE = n_edge(dim);
+    const long nc = g.nc;
+    if (sp->filtering_width != 0) return FHD_ERR_UNSUPPORTED;
+    std::vector<Vec> fcc(dim, Vec(nc, 0.0)), fed(2 * nE, Vec(nc, 0.0));
+    for (int r = 0; r < n_rngs; r++) {
+        for (int c = 0; c < dim; c++)
+            for (long f = 0; f < nc; f++) fcc[c][f] = fcc[c][f] + weights[r] * W_cc[r * dim + c][f];
+        for (int e = 0; e < 2 * nE; e++)
+            for (long f = 0; f < nc; f++) fed[e][f] = fed[e][f] + weights[r] * W_ed[r * 2 * nE + e][f];
+    }
+    const double variance = std::sqrt(sp->variance_coef_mom * 2.0 * sp->k_B / (sp->dV * dt));
+    for (int c = 0; c < dim; c++)
+        for (long f = 0; f < nc; f++) fcc[c][f] = (variance * fcc[c][f]) * std::sqrt(eta[f] * T[f]);
+    for (int e = 0; e < nE; e++)
+        for (int comp = 0; comp < 2; comp++)
+            for (long f = 0; f < nc; f++)
+                fed[2 * e + comp][f] = (variance * fed[2 * e + comp][f]) * std::sqrt(eta_ed[e][f] * T_ed[e][f]);
+    const double dxinv = 1.0 / g.dx;
+    forall(g, [&](int i, int j, int k) {
+        long f = g.id(i, j, k);
+        double dv[3];
+        if (dim == 2) {
+            // stoch_m_force_2d (stochastic_m_fluxdiv.f90:453-506)
+            dv[0] = (fcc[0][f] - fcc[0][g.id(i - 1, j, k)]) * dxinv + (fed[0][g.id(i, j + 1, k)] - fed[0][f]) * dxinv;
+            dv[1] = (fed[1][g.id(i + 1, j, k)] - fed[1][f]) * dxinv + (fcc[1][f] - fcc[1][g.id(i, j - 1, k)]) * dxinv;
+        } else {
+            // stoch_m_force_3d (stochastic_m_fluxdiv.f90:508-600); edge
+            // arrays fed[2e+comp] for e = xy, xz, yz
+            dv[0] = (fcc[0][f] - fcc[0][g.id(i - 1, j, k)]) * dxinv + (fed[0][g.id(i, j + 1, k)] - fed[0][f]) * dxinv
+                  + (fed[2][g.id(i, j, k + 1)] - fed[2][f]) * dxinv;
+            dv[1] = (fed[1][g.id(i + 1, j, k)] - fed[1][f]) * dxinv + (fcc[1][f] - fcc[1][g.id(i, j - 1, k)]) * dxinv
+                  + (fed[4][g.id(i, j, k + 1)] - fed[4][f]) * dxinv;
+            dv[2] = (fed[3][g.id(i + 1, j, k)] - fed[3][f]) * dxinv + (fed[5][g.id(i, j + 1, k)] - fed[5][f]) * dxinv
+                  + (fcc[2][f] - fcc[2][g.id(i, j, k - 1)]) * dxinv;
+        }
+        for (int c = 0; c < dim; c++) force[c][f] = increment ? force[c][f] + dv[c] : dv[c];
+    });
+    return 0;
+}
+
+void avg_face(const Geo& g, const double* cc, double* const fc[]) {
+    for (int d = 0; d < g.dim; d++) {
+        int e[3] = {0, 0, 0};
+        e[d] = 1;
+        forall(g, [&](int i, int j, int k) {
+            long f = g.id(i, j, k);
+            fc[d][f] = 0.5 * (cc[f] + cc[g.id(i - e[0], j - e[1], k - e[2])]);
+        });
+    }
+}
+
+void avg_edge(const Geo& g, const double* cc, double* const ed[]) {
+    if (g.dim == 2) {
+        forall(g, [&](int i, int j, int k) {
+            ed[0][g.id(i, j, k)] = 0.25 * (cc[g.id(i, j, k)] + cc[g.id(i - 1, j, k)] + cc[g.id(i, j - 1, k)] +
+                                           cc[g.id(i - 1, j - 1, k)]);
+        });
+        return;
+    }
+    forall(g, [&](int i, int j, int k) {
+        long f = g.id(i, j, k);
+        ed[0][f] = 0.25 * (cc[f] + cc[g.id(i - 1, j, k)] + cc[g.id(i, j - 1, k)] + cc[g.id(i - 1, j - 1, k)]);
+        ed[1][f] = 0.25 * (cc[f] + cc[g.id(i - 1, j, k)] + cc[g.id(i, j, k - 1)] + cc[g.id(i - 1, j, k - 1)]);
+        ed[2][f] = 0.25 * (cc[f] + cc[g.id(i, j - 1, k)] + cc[g.id(i, j, k - 1)] + cc[g.id(i, j - 1, k - 1)]);
+    });
+}
+
+// mk_advective_m_fluxdiv, centred (mk_advective_m_fluxdiv.f90:184-346):
+// m_update (+)= -div(m u) with face-to-edge averages
+void adv_m(const Geo& g, const double* const u[], const double* const m[], double* const upd[], bool increment) {
+    const int dim = g.dim;
+    const double dxinv = 1.0 / g.dx;
+    for (int c = 0; c < dim; c++) {
+        int ec[3] = {0, 0, 0};
+        ec[c] = 1;
+        forall(g, [&](int i, int j, int k) {
+            long f = g.id(i, j, k);
+            double s = 0.0;
+            for (int d = 0; d < dim; d++) {
+                int ed[3] = {0, 0, 0};
+                ed[d] = 1;
+                // flux of m_c in direction d at position q:
+                // 0.25*(m_c(q-e_d)+m_c(q))*(u_d(q-e_c)+u_d(q))
+                auto flux = [&](int qi, int qj, int qk) {
+                    long q = g.id(qi, qj, qk);
+                    return 0.25 * (m[c][g.id(qi - ed[0], qj - ed[1], qk - ed[2])] + m[c][q]) *
+                           (u[d][g.id(qi - ec[0], qj - ec[1], qk - ec[2])] + u[d][q]);
+                };
+                s += (flux(i + ed[0], j + ed[1], k + ed[2]) - flux(i, j, k)) * dxinv;
+            }
+            upd[c][f] = increment ? upd[c][f] - s : -s;
+        });
+    }
+}
+
+// mk_advective_s_fluxdiv, centred (mk_advective_s_fluxdiv.f90:138-220):
+// s_update (+)= -div(s_fc u)
+void adv_s(const Geo& g, const double* const u[], const double* const s_fc[], double* upd, bool increment) {
+    const double dxinv = 1.0 / g.dx;
+    forall(g, [&](int i, int j, int k) {
+        long f = g.id(i, j, k);
+        double s = 0.0;
+        for (int d = 0; d < g.dim; d++) {
+            int e[3] = {0, 0, 0};
+            e[d] = 1;
+            long fp = g.id(i + e[0], j + e[1], k + e[2]);
+            s += (u[d][fp] * s_fc[d][fp] - u[d][f] * s_fc[d][f]) * dxinv;
+        }
+        upd[f] = increment ? upd[f] - s : -s;
+    });
+}
+
+}  // namespace
+
+// =====================================================================
+// extern "C" API
+// =====================================================================
+extern "C" {
+
+int or_num_threads(void) {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+
+int or_compute_nlevs_mg(int dim, const int n[3], int minwidth) {
+    Geo g(dim, n, 1.0);
+    return nlevs_mg(g, minwidth);
+}
+
+void or_stag_applyop(int dim, const int n[3], double dx, int visc_type, const double* const phi[],
+                     double* const Lphi[], const double* const alpha_fc[], const double* beta,
+                     const double* const beta_ed[], const double* gamma, int color) {
+    Geo g(dim, n, dx);
+    SLevel L;
+    L.g = g;
+    for (int c = 0; c < dim; c++) {
+        L.alpha[c].assign(alpha_fc[c], alpha_fc[c] + g.nc);
+        L.phi[c].assign(phi[c], phi[c] + g.nc);
+        L.Lphi[c].assign(Lphi[c], Lphi[c] + g.nc);
+    }
+    L.beta.assign(beta, beta + g.nc);
+    L.gamma.assign(gamma, gamma + g.nc);
+    for (int e = 0; e < n_edge(dim); e++) L.bed[e].assign(beta_ed[e], beta_ed[e] + g.nc);
+    s_applyop(L, visc_type, color);
+    for (int c = 0; c < dim; c++) std::copy(L.Lphi[c].begin(), L.Lphi[c].end(), Lphi[c]);
+}
+
+int or_stag_mg_solver(int dim, const int n[3], double dx, int visc_type, const fhd_gmres_params* p,
+                      const double* const alpha_fc[], const double* beta, const double* const beta_ed[],
+                      const double* gamma, double theta_alpha, double* const phi[], const double* const rhs[]) {
+    Geo g(dim, n, dx);
+    return stag_mg(g, visc_type, p, alpha_fc, beta, beta_ed, gamma, theta_alpha, phi, rhs);
+}
+
+int or_stag_mg_history(int dim, const int n[3], double dx, int visc_type, const fhd_gmres_params* p,
+                       const double* const alpha_fc[], const double* beta, const double* const beta_ed[],
+                       const double* gamma, double theta_alpha, double* const phi[], const double* const rhs[],
+                       double* hist) {
+    Geo g(dim, n, dx);
+    return stag_mg(g, visc_type, p, alpha_fc, beta, beta_ed, gamma, theta_alpha, phi, rhs, hist);
+}
+
+int or_macproject(int dim, const int n[3], double dx, const fhd_gmres_params* p, double* phi,
+                  const double* const alphainv_fc[], const double* rhs) {
+    Geo g(dim, n, dx);
+    return macproject_impl(g, p, phi, alphainv_fc, rhs);
+}
+
+int or_apply_matrix(int dim, const int n[3], double dx, int visc_type, double* const b_u[], double* b_p,
+                    const double* const x_u[], const double* x_p, const double* const alpha_fc[],
+                    const double* beta, const double* const beta_ed[], const double* gamma, double theta_alpha) {
+    Geo g(dim, n, dx);
+    return apply_matrix_impl(g, visc_type, b_u, b_p, x_u, x_p, alpha_fc, beta, beta_ed, gamma, theta_alpha);
+}
+
+int or_apply_precon(int dim, const int n[3], double dx, int visc_type, const fhd_gmres_params* p,
+                    const double* const b_u[], const double* b_p, double* const x_u[], double* x_p,
+                    const double* const alpha_fc[], const double* beta, const double* const beta_ed[],
+                    const double* gamma, double theta_alpha) {
+    Geo g(dim, n, dx);
+    return apply_precon_impl(g, visc_type, p, b_u, b_p, x_u, x_p, alpha_fc, beta, beta_ed, gamma, theta_alpha);
+}
+
+int or_gmres(int dim, const int n[3], double dx, int visc_type, const fhd_gmres_params* p,
+             const double* const b_u[], const double* b_p, double* const x_u[], double* x_p,
+             const double* const alpha_fc[], const double* beta, const double* const beta_ed[],
+             const double* gamma, double theta_alpha, double* norm_pre_rhs, fhd_solve_stats* stats) {
+    Geo g(dim, n, dx);
+    return gmres_impl(g, visc_type, p, b_u, b_p, x_u, x_p, alpha_fc, beta, beta_ed, gamma, theta_alpha,
+                      norm_pre_rhs, stats);
+}
+
+int or_stochastic_m_fluxdiv(int dim, const int n[3], double dx, const fhd_stoch_params* sp, double* const force[],
+                            int increment, const double* eta, const double* const eta_ed[],
+                            const double* temperature, const double* const temperature_ed[], double dt,
+                            const double* weights, int n_rngs, const double* const W_cc[],
+                            const double* const W_ed[]) {
+    Geo g(dim, n, dx);
+    return stoch_m_impl(g, sp, force, increment, eta, eta_ed, temperature, temperature_ed, dt, weights, n_rngs,
+                        W_cc, W_ed);
+}
+
+void or_average_cc_to_edge(int dim, const int n[3], const double* cc, double* const ed[]) {
+    Geo g(dim, n, 1.0);
+    avg_edge(g, cc, ed);
+}
+
+void or_average_cc_to_face(int dim, const int n[3], const double* cc, double* const fc[]) {
+    Geo g(dim, n, 1.0);
+    avg_face(g, cc, fc);
+}
+
+int or_advance_inertial(int dim, const int n[3], double dx, int visc_type, const fhd_gmres_params* p_in,
+                        const fhd_stoch_params* sp, double dt, double* const umac[], double* rho, double* pi,
+                        const double* eta, const double* const eta_ed[], const double* kappa,
+                        const double* temperature, const double* const temperature_ed[],
+                        const double* const W_cc[], const double* const W_ed[], fhd_solve_stats* stats2) {
+    Geo g(dim, n, dx);
+    const long nc = g.nc;
+    const int nE = n_edge(dim);
+    fhd_gmres_params p = *p_in;
+    const double theta = 1.0 / dt;
+    const double one = 1.0;
+    auto fvec = [&](std::vector<Vec>& v) { v.assign(dim, Vec(nc, 0.0)); };
+    auto ptrs = [&](std::vector<Vec>& v, double** out) { for (int c = 0; c < dim; c++) out[c] = v[c].data(); };
+    std::vector<Vec> rho_fc_old, rho_fc_new, mold, mtemp, adv, diff, rhs_v, dumac, stoch, gradpi, zero_a;
+    fvec(rho_fc_old); fvec(rho_fc_new); fvec(mold); fvec(mtemp); fvec(adv); fvec(diff); fvec(rhs_v);
+    fvec(dumac); fvec(stoch); fvec(gradpi); fvec(zero_a);
+    double *rfo[3], *rfn[3], *mo[3], *mt[3], *ad[3], *df[3], *rv[3], *du[3], *sto[3], *gpi[3], *za[3];
+    ptrs(rho_fc_old, rfo); ptrs(rho_fc_new, rfn); ptrs(mold, mo); ptrs(mtemp, mt); ptrs(adv, ad); ptrs(diff, df);
+    ptrs(rhs_v, rv); ptrs(dumac, du); ptrs(stoch, sto); ptrs(gradpi, gpi); ptrs(zero_a, za);
+    Vec rho_old(rho, rho + nc), rho_update(nc), rhs_p(nc), dpi(nc);
+    Vec eta_h(nc), kappa_h(nc);
+    std::vector<Vec> eta_ed_h(nE, Vec(nc));
+    for (long f = 0; f < nc; f++) { eta_h[f] = eta[f] * 0.5; kappa_h[f] = kappa[f] * 0.5; }
+    for (int e = 0; e < nE; e++)
+        for (long f = 0; f < nc; f++) eta_ed_h[e][f] = eta_ed[e][f] * 0.5;
+    const double* eh_ed[3] = {eta_ed_h[0].data(), nE == 3 ? eta_ed_h[1].data() : nullptr,
+                              nE == 3 ? eta_ed_h[2].data() : nullptr};
+    const double* zap[3] = {za[0], za[1], dim == 3 ? za[2] : nullptr};
+    const double* um[3] = {umac[0], umac[1], dim == 3 ? umac[2] : nullptr};
+    const double w1[1] = {1.0};
+    // diffusive_m_fluxdiv (diffusive_m_fluxdiv.f90:25-...): -(applyop with alpha=0)
+    auto diff_m = [&](double* const out[], const double* const u[]) {
+        SLevel L;
+        L.g = g;
+        for (int c = 0; c < dim; c++) { L.alpha[c].assign(nc, 0.0); L.phi[c].assign(u[c], u[c] + nc); L.Lphi[c].assign(nc, 0.0); }
+        L.beta.assign(eta, eta + nc);
+        L.gamma.assign(kappa, kappa + nc);
+        for (int e = 0; e < nE; e++) L.bed[e].assign(eta_ed[e], eta_ed[e] + nc);
+        s_applyop(L, visc_type, 0);
+        for (int c = 0; c < dim; c++)
+            for (long f = 0; f < nc; f++) out[c][f] = L.Lphi[c][f] * -1.0;
+    };
+    (void)one;
+    int st = 0;
+    double norm_pre_rhs = 0.0;
+    // Step 2: predictor Euler step for rho (centred advection)
+    avg_face(g, rho_old.data(), rfo);
+    adv_s(g, um, rfo, rho_update.data(), false);
+    for (long f = 0; f < nc; f++) rho[f] = rho_old[f] + dt * rho_update[f];
+    avg_face(g, rho, rfn);
+    // Steps 3-4: predictor Crank-Nicolson
+    for (int c = 0; c < dim; c++)
+        for (long f = 0; f < nc; f++) mold[c][f] = rho_fc_old[c][f] * umac[c][f];
+    for (int c = 0; c < dim; c++)
+        for (long f = 0; f < nc; f++) rhs_v[c][f] = (1.0 / dt) * mold[c][f];
+    c_grad(g, pi, gpi);
+    for (int c = 0; c < dim; c++)
+        for (long f = 0; f < nc; f++) rhs_v[c][f] = rhs_v[c][f] - gradpi[c][f];
+    {
+        const double* mop[3] = {mo[0], mo[1], dim == 3 ? mo[2] : nullptr};
+        adv_m(g, um, mop, ad, false);
+    }
+    for (int c = 0; c < dim; c++)
+        for (long f = 0; f < nc; f++) rhs_v[c][f] = rhs_v[c][f] + adv[c][f];
+    diff_m(df, um);
+    for (int c = 0; c < dim; c++)
+        for (long f = 0; f < nc; f++) rhs_v[c][f] = rhs_v[c][f] + 0.5 * diff[c][f];
+    if (sp->variance_coef_mom != 0.0) {
+        stoch_m_impl(g, sp, sto, 0, eta, eta_ed, temperature, temperature_ed, dt, w1, 1, W_cc, W_ed);
+        for (int c = 0; c < dim; c++)
+            for (long f = 0; f < nc; f++) rhs_v[c][f] = rhs_v[c][f] + stoch[c][f];
+    }
+    std::fill(rhs_p.begin(), rhs_p.end(), 0.0);
+    for (int c = 0; c < dim; c++)
+        for (long f = 0; f < nc; f++) mtemp[c][f] = rho_fc_new[c][f] * umac[c][f];
+    for (int c = 0; c < dim; c++)
+        for (long f = 0; f < nc; f++) rhs_v[c][f] = rhs_v[c][f] + (-1.0 / dt) * mtemp[c][f];
+    diff_m(mt, um);
+    for (int c = 0; c < dim; c++)
+        for (long f = 0; f < nc; f++) rhs_v[c][f] = rhs_v[c][f] + 0.5 * mtemp[c][f];
+    c_div(g, um, rhs_p.data(), true);
+    for (int c = 0; c < dim; c++) std::fill(dumac[c].begin(), dumac[c].end(), 0.0);
+    std::fill(dpi.begin(), dpi.end(), 0.0);
+    const double gmres_abs_tol_in = p.gmres_abs_tol;
+    {
+        const double* rvp[3] = {rv[0], rv[1], dim == 3 ? rv[2] : nullptr};
+        const double* rfnp[3] = {rfn[0], rfn[1], dim == 3 ? rfn[2] : nullptr};
+        int s1 = gmres_impl(g, visc_type, &p, rvp, rhs_p.data(), du, dpi.data(), rfnp, eta_h.data(), eh_ed,
+                            kappa_h.data(), theta, &norm_pre_rhs, stats2 ? &stats2[0] : nullptr);
+        if (s1 < 0) return s1;
+        st = std::max(st, s1);
+    }
+    p.gmres_abs_tol = std::max(gmres_abs_tol_in, norm_pre_rhs * p.gmres_rel_tol);
+    for (int c = 0; c < dim; c++)
+        for (long f = 0; f < nc; f++) umac[c][f] = umac[c][f] + dumac[c][f];
+    for (long f = 0; f < nc; f++) pi[f] = pi[f] + dpi[f];
+    for (int c = 0; c < dim; c++)
+        for (long f = 0; f < nc; f++) mtemp[c][f] = rho_fc_new[c][f] * umac[c][f];
+    // Step 5: trapezoidal scalar corrector
+    adv_s(g, um, rfn, rho_update.data(), false);
+    for (long f = 0; f < nc; f++) {
+        double v = rho[f] + rho_old[f];
+        v = v + dt * rho_update[f];
+        rho[f] = v * 0.5;
+    }
+    avg_face(g, rho, rfn);
+    // Steps 6-7: corrector Crank-Nicolson
+    for (int c = 0; c < dim; c++)
+        for (long f = 0; f < nc; f++) rhs_v[c][f] = (1.0 / dt) * mold[c][f];
+    c_grad(g, pi, gpi);
+    for (int c = 0; c < dim; c++)
+        for (long f = 0; f < nc; f++) rhs_v[c][f] = rhs_v[c][f] - gradpi[c][f];
+    {
+        const double* mtp[3] = {mt[0], mt[1], dim == 3 ? mt[2] : nullptr};
+        adv_m(g, um, mtp, ad, true);
+    }
+    for (int c = 0; c < dim; c++)
+        for (long f = 0; f < nc; f++) rhs_v[c][f] = rhs_v[c][f] + 0.5 * adv[c][f];
+    for (int c = 0; c < dim; c++)
+        for (long f = 0; f < nc; f++) rhs_v[c][f] = rhs_v[c][f] + 0.5 * diff[c][f];
+    if (sp->variance_coef_mom != 0.0) {
+        stoch_m_impl(g, sp, sto, 1, eta, eta_ed, temperature, temperature_ed, dt, w1, 1, W_cc, W_ed);
+        for (int c = 0; c < dim; c++)
+            for (long f = 0; f < nc; f++) rhs_v[c][f] = rhs_v[c][f] + 0.5 * stoch[c][f];
+    }
+    std::fill(rhs_p.begin(), rhs_p.end(), 0.0);
+    for (int c = 0; c < dim; c++)
+        for (long f = 0; f < nc; f++) mtemp[c][f] = rho_fc_new[c][f] * umac[c][f];
+    for (int c = 0; c < dim; c++)
+        for (long f = 0; f < nc; f++) rhs_v[c][f] = rhs_v[c][f] + (-1.0 / dt) * mtemp[c][f];
+    diff_m(df, um);
+    for (int c = 0; c < dim; c++)
+        for (long f = 0; f < nc; f++) rhs_v[c][f] = rhs_v[c][f] + 0.5 * diff[c][f];
+    c_div(g, um, rhs_p.data(), true);
+    for (int c = 0; c < dim; c++) std::fill(dumac[c].begin(), dumac[c].end(), 0.0);
+    std::fill(dpi.begin(), dpi.end(), 0.0);
+    {
+        const double* rvp[3] = {rv[0], rv[1], dim == 3 ? rv[2] : nullptr};
+        const double* rfnp[3] = {rfn[0], rfn[1], dim == 3 ? rfn[2] : nullptr};
+        int s2 = gmres_impl(g, visc_type, &p, rvp, rhs_p.data(), du, dpi.data(), rfnp, eta_h.data(), eh_ed,
+                            kappa_h.data(), theta, nullptr, stats2 ? &stats2[1] : nullptr);
+        if (s2 < 0) return s2;
+        st = std::max(st, s2);
+    }
+    for (int c = 0; c < dim; c++)
+        for (long f = 0; f < nc; f++) umac[c][f] = umac[c][f] + dumac[c][f];
+    for (long f = 0; f < nc; f++) pi[f] = pi[f] + dpi[f];
+    return st;
+}
+
+// ---------------------------------------------------------------------
+// discretisation-accuracy harness (exec/stokes_preconditioner
+// main_driver.f90:354-387).  The exact fields are those of init.f90
+// (prob_sol = 1 Taylor vortex at time 0; prob_sol = 31); the forcing is
+// the continuous operator applied to them, evaluated here from the
+// analytic derivatives.
+// ---------------------------------------------------------------------
+namespace {
+const double PI = 3.14159265358979323846;
+
+struct Exact {
+    int dim, sol, coeff, visc;
+    double k = 2.0 * PI;
+    // velocity component c and its derivatives at x
+    void u(int c, const double* x, double& v, double* d1, double d2[3][3]) const {
+        double s[3], co[3];
+        for (int d = 0; d < 3; d++) { s[d] = std::sin(k * x[d]); co[d] = std::cos(k * x[d]); }
+        for (int a = 0; a < 3; a++) { d1[a] = 0; for (int b = 0; b < 3; b++) d2[a][b] = 0; }
+        if (dim == 2) {
+            // f = A * X(x) * Y(y) with X, Y in {sin, cos}
+            double A = 1.0, off = 0.0;
+            int fx, fy;  // 0 sin, 1 cos
+            if (sol == 1) {
+                if (c == 0) { A = -2.0; off = 1.0; fx = 1; fy = 0; } else { A = 2.0; off = 1.0; fx = 0; fy = 1; }
+            } else {
+                if (c == 0) { fx = 0; fy = 0; } else { fx = 1; fy = 0; }
+            }
+            double X = fx ? co[0] : s[0], Xp = fx ? -k * s[0] : k * co[0], Xpp = -k * k * X;
+            double Y = fy ? co[1] : s[1], Yp = fy ? -k * s[1] : k * co[1], Ypp = -k * k * Y;
+            v = off + A * X * Y;
+            d1[0] = A * Xp * Y; d1[1] = A * X * Yp;
+            d2[0][0] = A * Xpp * Y; d2[1][1] = A * X * Ypp; d2[0][1] = d2[1][0] = A * Xp * Yp;
+        } else {
+            int f[3];
+            if (c == 0) { f[0] = 0; f[1] = 0; f[2] = 0; }
+            else if (c == 1) { f[0] = 1; f[1] = 0; f[2] = 0; }
+            else { f[0] = 0; f[1] = 0; f[2] = 1; }
+            double F[3], Fp[3], Fpp[3];
+            for (int d = 0; d < 3; d++) {
+                F[d] = f[d] ? co[d] : s[d];
+                Fp[d] = f[d] ? -k * s[d] : k * co[d];
+                Fpp[d] = -k * k * F[d];
+            }
+            v = F[0] * F[1] * F[2];
+            d1[0] = Fp[0] * F[1] * F[2]; d1[1] = F[0] * Fp[1] * F[2]; d1[2] = F[0] * F[1] * Fp[2];
+            d2[0][0] = Fpp[0] * F[1] * F[2]; d2[1][1] = F[0] * Fpp[1] * F[2]; d2[2][2] = F[0] * F[1] * Fpp[2];
+            d2[0][1] = d2[1][0] = Fp[0] * Fp[1] * F[2];
+            d2[0][2] = d2[2][0] = Fp[0] * F[1] * Fp[2];
+            d2[1][2] = d2[2][1] = F[0] * Fp[1] * Fp[2];
+        }
+    }
+    double p(const double* x, double* gp) const {
+        double v = 0;
+        for (int d = 0; d < dim; d++) {
+            if (sol == 1) { v += -std::cos(2 * k * x[d]); gp[d] = 2 * k * std::sin(2 * k * x[d]); }
+            else { v += std::cos(2 * k * x[d]); gp[d] = -2 * k * std::sin(2 * k * x[d]); }
+        }
+        return v;
+    }
+    // beta, gamma and gradients (init.f90 mat_val_2d/_3d): prob_coeff 1:
+    // constant 1; 5: beta = 1 + 0.5 cos(kx) sin(ky) [sin(kz)],
+    // gamma = sin(kx) sin(ky) [sin(kz)]
+    double beta(const double* x, double* gb) const {
+        if (coeff == 1) { gb[0] = gb[1] = gb[2] = 0; return 1.0; }
+        double sz = dim == 3 ? std::sin(k * x[2]) : 1.0, cz = dim == 3 ? std::cos(k * x[2]) : 0.0;
+        gb[0] = -0.5 * k * std::sin(k * x[0]) * std::sin(k * x[1]) * sz;
+        gb[1] = 0.5 * k * std::cos(k * x[0]) * std::cos(k * x[1]) * sz;
+        gb[2] = dim == 3 ? 0.5 * k * std::cos(k * x[0]) * std::sin(k * x[1]) * cz : 0.0;
+        return 1.0 + 0.5 * std::cos(k * x[0]) * std::sin(k * x[1]) * sz;
+    }
+    double gam(const double* x, double* gg) const {
+        if (coeff == 1) { gg[0] = gg[1] = gg[2] = 0; return 1.0; }
+        double sz = dim == 3 ? std::sin(k * x[2]) : 1.0, cz = dim == 3 ? std::cos(k * x[2]) : 0.0;
+        gg[0] = k * std::cos(k * x[0]) * std::sin(k * x[1]) * sz;
+        gg[1] = k * std::sin(k * x[0]) * std::cos(k * x[1]) * sz;
+        gg[2] = dim == 3 ? k * std::sin(k * x[0]) * std::sin(k * x[1]) * cz : 0.0;
+        return std::sin(k * x[0]) * std::sin(k * x[1]) * sz;
+    }
+    // forcing of the velocity row c: -div(tau) + dp/dx_c
+    double fu(int c, const double* x) const {
+        double vu[3], d1[3][3], d2[3][3][3];
+        for (int a = 0; a < dim; a++) u(a, x, vu[a], d1[a], d2[a]);
+        double gb[3], gg[3], gp[3];
+        double b = beta(x, gb), gm = gam(x, gg);
+        p(x, gp);
+        int av = std::abs(visc);
+        double lap = 0, gdiv = 0, div = 0, gbdu = 0, gbdut = 0;
+        for (int d = 0; d < dim; d++) {
+            lap += d2[c][d][d];
+            gdiv += d2[d][c][d];  // d/dx_c (du_d/dx_d)
+            div += d1[d][d];
+            gbdu += gb[d] * d1[c][d];
+            gbdut += gb[d] * d1[d][c];
+        }
+        double val = -(b * lap + gbdu);  // -div(beta grad u_c)
+        if (av >= 2) val += -(b * gdiv + gbdut);
+        if (av == 3) {
+            double lam = gm - (2.0 / 3.0) * b;
+            double glam = gg[c] - (2.0 / 3.0) * gb[c];
+            val += -(lam * gdiv + glam * div);
+        }
+        return val + gp[c];
+    }
+    double fp(const double* x) const {
+        double div = 0, vu, d1[3], d2[3][3];
+        for (int d = 0; d < dim; d++) { u(d, x, vu, d1, d2); div += d1[d]; }
+        return -div;
+    }
+};
+}  // namespace
+
+int or_accuracy_test(int dim, int n, int prob_coeff, int prob_sol, int visc_type, double* err) {
+    int nn[3] = {n, n, dim == 3 ? n : 1};
+    const double dx = 1.0 / n;
+    Geo g(dim, nn, dx);
+    const long nc = g.nc;
+    Exact ex{dim, prob_sol, prob_coeff, visc_type};
+    std::vector<Vec> xu(dim, Vec(nc)), bu(dim, Vec(nc)), fu(dim, Vec(nc)), alpha(dim, Vec(nc, 1.0));
+    Vec xp(nc), bp(nc), fpv(nc), beta(nc), gamma(nc);
+    std::vector<Vec> bed(n_edge(dim), Vec(nc));
+    forall(g, [&](int i, int j, int k) {
+        long f = g.id(i, j, k);
+        int I[3] = {i, j, k};
+        for (int c = 0; c < dim; c++) {
+            double x[3] = {0, 0, 0};
+            for (int d = 0; d < dim; d++) x[d] = (d == c) ? I[d] * dx : (I[d] + 0.5) * dx;
+            double v, d1[3], d2[3][3];
+            ex.u(c, x, v, d1, d2);
+            xu[c][f] = v;
+            fu[c][f] = ex.fu(c, x);
+        }
+        double x[3] = {0, 0, 0}, gd[3];
+        for (int d = 0; d < dim; d++) x[d] = (I[d] + 0.5) * dx;
+        xp[f] = ex.p(x, gd);
+        fpv[f] = ex.fp(x);
+        beta[f] = ex.beta(x, gd);
+        gamma[f] = ex.gam(x, gd);
+    });
+    double* bedp[3] = {bed[0].data(), dim == 3 ? bed[1].data() : nullptr, dim == 3 ? bed[2].data() : nullptr};
+    avg_edge(g, beta.data(), bedp);
+    const double* xup[3] = {xu[0].data(), xu[1].data(), dim == 3 ? xu[2].data() : nullptr};
+    double* bup[3] = {bu[0].data(), bu[1].data(), dim == 3 ? bu[2].data() : nullptr};
+    const double* ap[3] = {alpha[0].data(), alpha[1].data(), dim == 3 ? alpha[2].data() : nullptr};
+    const double* cbed[3] = {bedp[0], bedp[1], bedp[2]};
+    apply_matrix_impl(g, visc_type, bup, bp.data(), xup, xp.data(), ap, beta.data(), cbed, gamma.data(), 0.0);
+    for (int c = 0; c < dim; c++) {
+        const Vec& F = fu[c];
+        const Vec& B = bu[c];
+        err[c] = reduce_max(g, [&](int i, int j, int k) { long f = g.id(i, j, k); return std::fabs(F[f] - B[f]); });
+    }
+    err[dim] = reduce_max(g, [&](int i, int j, int k) { long f = g.id(i, j, k); return std::fabs(fpv[f] - bp[f]); });
+    return 0;
+}
+
+}  // extern "C"

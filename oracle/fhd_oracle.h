@@ -1,0 +1,128 @@
+/*
+ * fhd_oracle.h -- TEST INFRASTRUCTURE ONLY.
+ *
+ * CPU FP64 restatement of LowMachFHD's staggered Stokes solve and stochastic
+ * momentum flux (periodic single box), used as the parity checker of the
+ * CUDA library and as the timed CPU baseline.  Nothing in the product
+ * links or calls it; only tests/, __graft_entry__.smoke() and bench.py's
+ * CPU baseline leg load it.
+ *
+ * Arrays use the canonical layout of include/fhd_b200.h.  Vector arguments
+ * (u-type, beta_ed) are arrays of `dim` (or nE) host pointers.
+ */
+#ifndef FHD_ORACLE_H
+#define FHD_ORACLE_H
+
+#include "../include/fhd_b200.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* number of staggered MG levels (stag_mg_layout.f90:179-222) */
+int or_compute_nlevs_mg(int dim, const int n[3], int minwidth);
+
+/* stag_applyop_level with colour (stag_applyop.f90:70-1075); alpha_fc is
+ * used as given (already multiplied by theta_alpha). */
+void or_stag_applyop(int dim, const int n[3], double dx, int visc_type,
+                     const double* const phi[], double* const Lphi[],
+                     const double* const alpha_fc[], const double* beta,
+                     const double* const beta_ed[], const double* gamma,
+                     int color);
+
+int or_stag_mg_solver(int dim, const int n[3], double dx, int visc_type,
+                      const fhd_gmres_params* p,
+                      const double* const alpha_fc[], const double* beta,
+                      const double* const beta_ed[], const double* gamma,
+                      double theta_alpha, double* const phi[],
+                      const double* const rhs[]);
+
+/* as or_stag_mg_solver, also recording the L2 residual ratio |r|/|r0|
+ * after every V-cycle into hist[0 .. stag_mg_max_vcycles-1] (the history
+ * stag_mg_verbosity >= 1 prints, stag_mg_solver.f90:782-785) */
+int or_stag_mg_history(int dim, const int n[3], double dx, int visc_type,
+                       const fhd_gmres_params* p,
+                       const double* const alpha_fc[], const double* beta,
+                       const double* const beta_ed[], const double* gamma,
+                       double theta_alpha, double* const phi[],
+                       const double* const rhs[], double* hist);
+
+/* macproject (macproject.f90:34-316) with the pressure multigrid restated
+ * from PreconditionerNotes.tex:484-575: solves D (alphainv) G phi = rhs. */
+int or_macproject(int dim, const int n[3], double dx,
+                  const fhd_gmres_params* p,
+                  double* phi, const double* const alphainv_fc[],
+                  const double* rhs);
+
+int or_apply_matrix(int dim, const int n[3], double dx, int visc_type,
+                    double* const b_u[], double* b_p,
+                    const double* const x_u[], const double* x_p,
+                    const double* const alpha_fc[], const double* beta,
+                    const double* const beta_ed[], const double* gamma,
+                    double theta_alpha);
+
+int or_apply_precon(int dim, const int n[3], double dx, int visc_type,
+                    const fhd_gmres_params* p,
+                    const double* const b_u[], const double* b_p,
+                    double* const x_u[], double* x_p,
+                    const double* const alpha_fc[], const double* beta,
+                    const double* const beta_ed[], const double* gamma,
+                    double theta_alpha);
+
+int or_gmres(int dim, const int n[3], double dx, int visc_type,
+             const fhd_gmres_params* p,
+             const double* const b_u[], const double* b_p,
+             double* const x_u[], double* x_p,
+             const double* const alpha_fc[], const double* beta,
+             const double* const beta_ed[], const double* gamma,
+             double theta_alpha, double* norm_pre_rhs,
+             fhd_solve_stats* stats);
+
+int or_stochastic_m_fluxdiv(int dim, const int n[3], double dx,
+                            const fhd_stoch_params* sp,
+                            double* const force[], int increment,
+                            const double* eta, const double* const eta_ed[],
+                            const double* temperature,
+                            const double* const temperature_ed[],
+                            double dt, const double* weights, int n_rngs,
+                            const double* const W_cc[],
+                            const double* const W_ed[]);
+
+/* average_cc_to_node (2D) / average_cc_to_edge (3D) (convert_stag.f90:
+ * 395-864) and average_cc_to_face (convert_stag.f90:132-391). */
+void or_average_cc_to_edge(int dim, const int n[3], const double* cc,
+                           double* const ed[]);
+void or_average_cc_to_face(int dim, const int n[3], const double* cc,
+                           double* const fc[]);
+
+/* One inertial predictor-corrector step of a single-species fluid with
+ * centred advection (advance_timestep_inertial.f90:45-923 with
+ * nspecies=1, no mass diffusion, no gravity, periodic).  State umac, rho,
+ * pi is advanced in place.  W_cc/W_ed: the step's random fields (one set,
+ * n_rngs=1, weights=1), used by predictor and corrector as the reference
+ * does.  kappa plays the role of gamma in the solver. */
+int or_advance_inertial(int dim, const int n[3], double dx, int visc_type,
+                        const fhd_gmres_params* p, const fhd_stoch_params* sp,
+                        double dt, double* const umac[], double* rho,
+                        double* pi, const double* eta,
+                        const double* const eta_ed[], const double* kappa,
+                        const double* temperature,
+                        const double* const temperature_ed[],
+                        const double* const W_cc[], const double* const W_ed[],
+                        fhd_solve_stats* stats2);
+
+/* Discretisation-accuracy harness of exec/stokes_preconditioner
+ * (main_driver.f90:354-387, test_type=0): on [0,1]^dim with n cells per
+ * direction returns max|f - A x_exact| per velocity component (err[0..dim-1])
+ * and for the pressure row (err[dim]).  prob_coeff in {1,5}, prob_sol in
+ * {1,31}. */
+int or_accuracy_test(int dim, int n, int prob_coeff, int prob_sol,
+                     int visc_type, double* err);
+
+/* number of OpenMP threads the oracle uses */
+int or_num_threads(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
