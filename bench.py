@@ -1,0 +1,378 @@
+"""Benchmark: LowMachFHD inertial low-Mach timesteps on a 3D 256^3 periodic
+grid, mixed precision (FP32 multigrid preconditioner and stochastic flux
+inside FP64 GMRES) against the plain FP64 path on the same B200, GMRES
+relative residual 1e-8.
+
+A step is one Crank-Nicolson predictor-corrector step of
+advance_timestep_inertial (two preconditioned GMRES Stokes solves plus the
+stochastic momentum flux, advection and viscous terms) through the
+device-resident step entry point of the C ABI.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun every rank runs an independent replica (the path does not
+shard: "replicas only"); value = steps of all ranks / max-over-ranks time.
+Prints one JSON line on rank 0.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "3D 256³ steps/s: mixed vs FP64 (same B200, 1e-8 resid); served p50/p99 latency"
+N_CELLS = 256
+DT = 0.05
+KT = 1e-4
+REL_TOL = 1e-8
+WORKLOAD = "lowmach_inertial_step_3d_256cube_periodic"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=N_CELLS, help="cells per direction")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-sample-n", type=int, default=128)
+    return ap.parse_args()
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# ----------------------------------------------------------------------
+# clocks sampled during the timed region
+# ----------------------------------------------------------------------
+class Clocks:
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self.proc = None
+        self.thr = None
+
+    def start(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.index), "-lms", "200"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+            return
+
+        def rd():
+            for line in self.proc.stdout:
+                self.rows.append([x.strip() for x in line.split(",")])
+        self.thr = threading.Thread(target=rd, daemon=True)
+        self.thr.start()
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        if self.thr:
+            self.thr.join(timeout=2)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+                for nm, v in zip(names, r[5:9]):
+                    if v.strip().lower() == "active":
+                        reasons.add(nm)
+            except Exception:
+                pass
+        sm.sort()
+        med = sm[len(sm) // 2] if sm else None
+        return {"sm_mhz": med, "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ----------------------------------------------------------------------
+# problem set-up (seeded synthetic inputs; no dataset involved)
+# ----------------------------------------------------------------------
+def host_fields(n, seed, torch):
+    """one set of N(0,1) stochastic momentum fields, as fill_m_stochastic
+    prepares them (symmetric form: cell entries with variance 2, the two
+    edge components equal), pinned host float64"""
+    g = torch.Generator().manual_seed(seed)
+    nc = n ** 3
+    W_cc = [torch.randn(nc, generator=g, dtype=torch.float64).mul_(2.0 ** 0.5).pin_memory() for _ in range(3)]
+    W_ed = []
+    for _ in range(3):
+        a = torch.randn(nc, generator=g, dtype=torch.float64).pin_memory()
+        W_ed += [a, a]
+    return W_cc, W_ed
+
+
+class Case:
+    def __init__(self, L, torch, dev, n, precision, seed=7):
+        self.torch, self.dev, self.n = torch, dev, n
+        nc = n ** 3
+        self.nc = nc
+        params = L.default_params(gmres_rel_tol=REL_TOL)
+        self.s = L.StokesSolver(3, [n, n, n], 1.0, 1, params=params, precision=precision)
+        g = torch.Generator(device="cpu").manual_seed(seed)
+        f64 = dict(dtype=torch.float64)
+        self.umac = [(1e-3 * torch.randn(nc, generator=g, **f64)).to(dev) for _ in range(3)]
+        self.rho = (1.0 + 1e-3 * torch.randn(nc, generator=g, **f64)).to(dev)
+        self.pi = torch.zeros(nc, device=dev, **f64)
+        self.eta = torch.ones(nc, device=dev, **f64)
+        self.eta_ed = [torch.ones(nc, device=dev, **f64) for _ in range(3)]
+        self.kappa = torch.zeros(nc, device=dev, **f64)
+        self.T = torch.ones(nc, device=dev, **f64)
+        self.T_ed = [torch.ones(nc, device=dev, **f64) for _ in range(3)]
+        self.sp = L.StochParams(k_B=KT, variance_coef_mom=1.0, dV=1.0, stoch_stress_form=1, filtering_width=0)
+
+    def step(self, W_cc, W_ed):
+        return self.s.advance_timestep_inertial(self.sp, DT, self.umac, self.rho, self.pi, self.eta, self.eta_ed,
+                                                self.kappa, self.T, self.T_ed, W_cc, W_ed)
+
+
+def dist_init(args):
+    import torch
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+    return ws, rank, local
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def allmax(ws, v, torch, dev):
+    if ws == 1:
+        return v
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ----------------------------------------------------------------------
+# CPU baseline: the oracle (C++ FP64 restatement, OpenMP on all host
+# threads) on a bounded sample of the workload
+# ----------------------------------------------------------------------
+def cpu_sample(n_sample: int, n_full: int):
+    import numpy as np
+
+    import oracle as O
+    O.build()
+    nc = n_sample ** 3
+    rng = np.random.default_rng(7)
+    umac = [1e-3 * rng.standard_normal(nc) for _ in range(3)]
+    rho = 1.0 + 1e-3 * rng.standard_normal(nc)
+    pi = np.zeros(nc)
+    eta = np.ones(nc)
+    ee = [np.ones(nc)] * 3
+    W_cc = [rng.standard_normal(nc) * 2 ** 0.5 for _ in range(3)]
+    W_ed = []
+    for _ in range(3):
+        a = rng.standard_normal(nc)
+        W_ed += [a, a]
+    sp = O.StochParams(k_B=KT, variance_coef_mom=1.0, dV=1.0, stoch_stress_form=1, filtering_width=0)
+    t0 = time.perf_counter()
+    rc, *_ = O.advance_inertial(3, [n_sample] * 3, 1.0, 1, O.default_params(gmres_rel_tol=REL_TOL), sp, DT,
+                                umac, rho, pi, eta, ee, np.zeros(nc), np.ones(nc), ee, W_cc, W_ed)
+    sec = time.perf_counter() - t0
+    scale = (n_full / n_sample) ** 3
+    return {"value": 1.0 / (sec * scale), "unit": "steps/s", "cores": O.num_threads(), "kind": "port",
+            "sample": f"one FP64 inertial step at {n_sample}^3 on the CPU oracle ({sec:.2f} s), scaled by the "
+                      f"cell ratio {scale:g} to the {n_full}^3 step (the GMRES iteration count does not grow "
+                      f"with the grid under multigrid preconditioning)",
+            "sample_seconds": sec}
+
+
+def run_reference(args):
+    ws, rank, _ = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
+    if rank != 0:
+        return 0
+    n_s = args.cpu_sample_n
+    secs = []
+    for i in range(args.warmup + args.steps):
+        r = cpu_sample(n_s, args.n)
+        if i >= args.warmup:
+            secs.append(r["sample_seconds"] * (args.n / n_s) ** 3)
+        if i == 0 and args.warmup > 1:
+            # CPU runs need no warm-up beyond the first call
+            args.warmup = 1
+    sec = sum(secs) / len(secs)
+    v = 1.0 / sec
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "steps/s", "n_gpus": 0,
+            "steps": len(secs), "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded N(0,1) fields)",
+            "config": {"workload": WORKLOAD, "n_cells": [args.n] * 3, "dt": DT, "k_B": KT, "gmres_rel_tol": REL_TOL,
+                       "visc_type": 1, "species": 1},
+            "cpu_baseline": {"value": v, "unit": "steps/s", "cores": r["cores"], "kind": "port",
+                             "sample": r["sample"]},
+            "e2e": {"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    import torch
+
+    import lowmachfhd_b200 as L
+
+    ws, rank, local = dist_init(args)
+    dev = torch.device(f"cuda:{local}")
+    torch.cuda.set_device(dev)
+    n = args.n
+    nc = n ** 3
+    hbm, peak_kind = peaks()
+
+    # stochastic fields: a ring of device-resident sets for the device-timed
+    # run, and pinned host sets for the end-to-end run
+    host_sets = [host_fields(n, 100 + 10 * rank + i, torch) for i in range(2)]
+    dev_sets = [([w.to(dev) for w in a], [w.to(dev) for w in b]) for a, b in host_sets]
+    torch.cuda.synchronize()
+
+    results = {}
+    for precision in ("mixed", "fp64"):
+        case = Case(L, torch, dev, n, precision)
+        # the context launches on a torch-owned stream so that torch's
+        # pinned-memory and caching allocators never see a destroyed stream
+        stream = torch.cuda.Stream(device=dev)
+        case.s.set_stream(stream.cuda_stream)
+        for i in range(args.warmup):
+            case.step(*dev_sets[i % len(dev_sets)])
+        torch.cuda.synchronize()
+        barrier(ws)
+        clocks = Clocks(local)
+        if precision == "mixed":
+            clocks.start()
+        launches0 = case.s.kernel_launches
+        case.s.profile(True)
+        iters = []
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for i in range(args.steps):
+            st, stats = case.step(*dev_sets[i % len(dev_sets)])
+            iters.append([s["total_iters"] for s in stats])
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        ms = ev0.elapsed_time(ev1)
+        barrier(ws)
+        prof = case.s.profile_read()
+        case.s.profile(False)
+        launches = case.s.kernel_launches - launches0
+        clk = clocks.stop() if precision == "mixed" else None
+        ms_max = allmax(ws, ms, torch, dev)
+        results[precision] = dict(ms=ms_max, iters=iters, prof=prof, launches=launches, clocks=clk,
+                                  resid=stats[-1]["norm_resid"] / max(stats[-1]["norm_init_resid"], 1e-300))
+        if precision == "mixed":
+            # end to end: per step the host->device copy of the step's
+            # random fields from pinned memory, the step, and the read-back
+            # of its solver diagnostics
+            h2d = sum(w.numel() * 8 for w in host_sets[0][0] + host_sets[0][1])
+            stage = ([torch.empty(nc, dtype=torch.float64, device=dev) for _ in range(3)],
+                     [torch.empty(nc, dtype=torch.float64, device=dev) for _ in range(6)])
+            torch.cuda.synchronize()
+            barrier(ws)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            with torch.cuda.stream(stream):
+                for i in range(args.steps):
+                    hc, he = host_sets[i % len(host_sets)]
+                    for d_, h_ in zip(stage[0] + stage[1], hc + he):
+                        d_.copy_(h_, non_blocking=True)
+                    st, stats = case.step(*stage)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            e2e_ms = allmax(ws, e0.elapsed_time(e1), torch, dev)
+            d2h = 2 * 80  # the two solves' fhd_solve_stats read back by the step call
+            results["e2e"] = dict(ms=e2e_ms, h2d=h2d, d2h=d2h)
+            del stage
+        case.s.close()
+        del case
+        torch.cuda.empty_cache()
+
+    mixed, fp64 = results["mixed"], results["fp64"]
+    K = args.steps
+    value = ws * K / (mixed["ms"] / 1e3)
+    fp64_value = ws * K / (fp64["ms"] / 1e3)
+    n_l, ms_l, bytes_l = mixed["prof"]
+    achieved = (bytes_l / n_l) / ((ms_l / n_l) / 1e3) / 1e9 if n_l else None
+    n64, ms64, b64 = fp64["prof"]
+    achieved64 = (b64 / n64) / ((ms64 / n64) / 1e3) / 1e9 if n64 else None
+    line = {
+        "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": ws, "steps": K, "warmup": args.warmup,
+        "ms_per_step": mixed["ms"] / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 multigrid / f64 Krylov", "data": "synthetic (seeded N(0,1) stochastic fields)",
+        "config": {"workload": WORKLOAD, "n_cells": [n] * 3, "dt": DT, "k_B": KT, "rho": "1+1e-3 N(0,1)",
+                   "eta": 1.0, "visc_type": 1, "precon_type": 1, "gmres_rel_tol": REL_TOL, "species": 1,
+                   "parallelism": f"replicas x{ws}",
+                   "l2": "inputs larger than L2 (each 256^3 field is 134 MB)"},
+        "fp64": {"value": fp64_value, "unit": "steps/s", "ms_per_step": fp64["ms"] / K,
+                 "gmres_iters_per_step": [sum(x) for x in fp64["iters"]]},
+        "mixed_over_fp64": value / fp64_value,
+        "gmres_iters_per_step": [sum(x) for x in mixed["iters"]],
+        "gmres_iters_per_s": ws * sum(sum(x) for x in mixed["iters"]) / (mixed["ms"] / 1e3),
+        "final_rel_resid": mixed["resid"],
+        "gpu_launches": mixed["launches"],
+        "roofline": {"kernel": "k_stag_gs (finest-level colour Gauss-Seidel sweep)", "bound": "hbm",
+                     "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": (achieved / hbm) if achieved else None, "traffic": None,
+                     "peak_kind": peak_kind, "launches_timed": n_l,
+                     "avg_launch_us": (ms_l / n_l * 1e3) if n_l else None,
+                     "bytes_per_launch": (bytes_l / n_l) if n_l else None,
+                     "fp64_achieved": achieved64},
+        "clocks": mixed["clocks"],
+        "e2e": {"value": ws * K / (results["e2e"]["ms"] / 1e3), "unit": "steps/s",
+                "h2d_bytes_per_step": results["e2e"]["h2d"], "d2h_bytes_per_step": results["e2e"]["d2h"]},
+    }
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        try:
+            cb = cpu_sample(args.cpu_sample_n, n)
+            cb.pop("sample_seconds", None)
+            line["cpu_baseline"] = cb
+        except Exception as e:  # the baseline never decides the run
+            line["cpu_baseline"] = {"value": None, "error": str(e)}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -213,6 +213,13 @@ int fhd_dev_advance_inertial(fhd_ctx* ctx, const fhd_stoch_params* sp,
 const char* fhd_last_error(void);
 /* Bytes of device memory a context holds. */
 unsigned long long fhd_ctx_device_bytes(fhd_ctx* ctx);
+/* Timing of the finest-level colour smoother (the dominant kernel; the
+ * smooths of stag_mg_solver.f90:360-396): while enabled, CUDA events on the
+ * context stream bracket each launch.  read returns the launches, their
+ * summed device time (ms) and their algorithmic bytes since enable. */
+int fhd_ctx_profile(fhd_ctx* ctx, int enable);
+int fhd_ctx_profile_read(fhd_ctx* ctx, long long* launches, double* ms,
+                         double* bytes);
 
 /* ------------------------------------------------------------------ */
 /* host BoxLib-fab entry points (drop-in boundary)                     */

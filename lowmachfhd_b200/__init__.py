@@ -101,6 +101,16 @@ class StokesSolver:
     def set_stream(self, stream_handle: int | None):
         check(lib().fhd_ctx_set_stream(self._h, C.c_void_p(stream_handle or 0)), "fhd_ctx_set_stream")
 
+    def profile(self, enable: bool = True):
+        """time the finest-level smoother launches with CUDA events"""
+        check(lib().fhd_ctx_profile(self._h, int(enable)), "fhd_ctx_profile")
+
+    def profile_read(self):
+        """(launches, device ms, algorithmic bytes) since profile(True)"""
+        n, ms, b = C.c_longlong(0), C.c_double(0), C.c_double(0)
+        check(lib().fhd_ctx_profile_read(self._h, C.byref(n), C.byref(ms), C.byref(b)), "fhd_ctx_profile_read")
+        return n.value, ms.value, b.value
+
     def close(self):
         if getattr(self, "_h", None):
             lib().fhd_ctx_destroy(self._h)

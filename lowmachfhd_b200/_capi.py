@@ -92,6 +92,9 @@ _PROTOS = {
     "fhd_ctx_set_stream": (C.c_int, [_VP, _VP]),
     "fhd_ctx_kernel_launches": (C.c_longlong, [_VP]),
     "fhd_ctx_device_bytes": (C.c_ulonglong, [_VP]),
+    "fhd_ctx_profile": (C.c_int, [_VP, C.c_int]),
+    "fhd_ctx_profile_read": (C.c_int, [_VP, C.POINTER(C.c_longlong), C.POINTER(C.c_double),
+                                       C.POINTER(C.c_double)]),
     "fhd_status_string": (C.c_char_p, [C.c_int]),
     "fhd_last_error": (C.c_char_p, []),
     "fhd_dev_apply_matrix": (C.c_int, [_VP, _PP, _DP, _PP, _DP, _PP, _DP, _PP, _DP, C.c_double]),

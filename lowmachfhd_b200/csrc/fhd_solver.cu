@@ -239,6 +239,30 @@ int prepare(fhd_ctx* ctx, const double* const alpha_fc[], const double* beta, co
 // ---------------------------------------------------------------------
 // staggered multigrid V-cycle (stag_mg_solver.f90:323-808)
 // ---------------------------------------------------------------------
+// algorithmic bytes of one fused colour sweep of component c: the whole
+// component array is read (the colour and its neighbours), the colour's
+// rhs and alpha read and the colour written; variable coefficients add the
+// cell and edge viscosities, cross terms the other components
+template <typename T>
+static double gs_sweep_bytes(fhd_ctx* ctx, const StagLevel<T>& L) {
+    const double nc = (double)L.g.nc, s = (double)sizeof(T);
+    const int dim = ctx->dim, v = ctx->visc;
+    double words = nc + 1.5 * nc;
+    if (v < 0) words += nc + (dim - 1) * nc;
+    if (v == 2 || v == -2 || v == 3 || v == -3) words += (dim - 1) * nc;
+    if (v == -3) words += nc;
+    return words * s;
+}
+
+static cudaEvent_t prof_event(fhd_ctx* ctx) {
+    if (ctx->prof_used >= ctx->prof_ev.size()) {
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        ctx->prof_ev.push_back(e);
+    }
+    return ctx->prof_ev[ctx->prof_used++];
+}
+
 template <typename T>
 static int stag_smooth(fhd_ctx* ctx, StagLevel<T>& L, int color) {
     cudaStream_t st = ctx->stream;
@@ -246,6 +270,12 @@ static int stag_smooth(fhd_ctx* ctx, StagLevel<T>& L, int color) {
     const StagOp<T> A = L.op();
     int rc = 0;
     if (color != 0 && all_even(L.g)) {
+        const bool timed = ctx->prof && L.g.nc == ctx->g0.nc;
+        if (timed) {
+            cudaEventRecord(prof_event(ctx), st);
+            ctx->prof_bytes += gs_sweep_bytes(ctx, L);
+            ctx->prof_launches++;
+        }
         const int c = (color - 1) / 2;
         const int par = (color + 1) & 1;
         with_dim_visc(ctx->dim, ctx->visc, [&](auto D, auto V) {
@@ -261,6 +291,7 @@ static int stag_smooth(fhd_ctx* ctx, StagLevel<T>& L, int color) {
                     L.g, A, L.phi[0], L.phi[1], L.phi[2], L.rhs[DIM == 3 ? 2 : 1], par, omega);
             rc |= post(ctx);
         });
+        if (timed) cudaEventRecord(prof_event(ctx), st);
         return rc;
     }
     with_dim_visc(ctx->dim, ctx->visc, [&](auto D, auto V) {
@@ -1069,6 +1100,8 @@ int fhd_ctx_destroy(fhd_ctx* c) {
     if (c->stream) cudaStreamSynchronize(c->stream);
     fhd_host_path_release(c);
     c->arena.release();
+    for (cudaEvent_t e : c->prof_ev) cudaEventDestroy(e);
+    c->prof_ev.clear();
     if (c->hscal) cudaFreeHost(c->hscal);
     if (c->own) cudaStreamDestroy(c->own);
     delete c;
@@ -1084,6 +1117,31 @@ int fhd_ctx_set_stream(fhd_ctx* c, void* s) {
 }
 
 long long fhd_ctx_kernel_launches(fhd_ctx* c) { return c ? c->launches : 0; }
+
+int fhd_ctx_profile(fhd_ctx* c, int enable) {
+    if (!c) return FHD_ERR_BAD_ARG;
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess) return FHD_ERR_CUDA;
+    c->prof = enable != 0;
+    c->prof_used = 0;
+    c->prof_bytes = 0.0;
+    c->prof_launches = 0;
+    return FHD_OK;
+}
+
+int fhd_ctx_profile_read(fhd_ctx* c, long long* launches, double* ms, double* bytes) {
+    if (!c) return FHD_ERR_BAD_ARG;
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess) return FHD_ERR_CUDA;
+    double t = 0.0;
+    for (size_t i = 0; i + 1 < c->prof_used; i += 2) {
+        float m = 0.f;
+        if (cudaEventElapsedTime(&m, c->prof_ev[i], c->prof_ev[i + 1]) != cudaSuccess) return FHD_ERR_CUDA;
+        t += m;
+    }
+    if (launches) *launches = c->prof_launches;
+    if (ms) *ms = t;
+    if (bytes) *bytes = c->prof_bytes;
+    return FHD_OK;
+}
 
 unsigned long long fhd_ctx_device_bytes(fhd_ctx* c) { return c ? (unsigned long long)c->arena.bytes : 0ull; }
 

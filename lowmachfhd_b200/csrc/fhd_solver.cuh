@@ -204,6 +204,13 @@ struct fhd_ctx {
     // inertial-step work arrays (allocated on the first step)
     bool step_ready = false;
     double* sb[64] = {nullptr};
+    // optional timing of the finest-level smoother launches (CUDA events on
+    // the context stream) with their algorithmic bytes
+    bool prof = false;
+    std::vector<cudaEvent_t> prof_ev;  // start/stop pairs
+    size_t prof_used = 0;
+    double prof_bytes = 0.0;
+    long long prof_launches = 0;
 };
 
 namespace fhd {
