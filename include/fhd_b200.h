@@ -221,6 +221,31 @@ int fhd_ctx_profile(fhd_ctx* ctx, int enable);
 int fhd_ctx_profile_read(fhd_ctx* ctx, long long* launches, double* ms,
                          double* bytes);
 
+/* stag_mg_solver without device allocation -- no counterpart in the
+ * reference; a variant of fhd_dev_stag_mg_solver for callers that cannot
+ * call cudaMalloc (device memory owned by another runtime such as an OpenACC
+ * or CUDA Fortran data region, a fixed job pool, or code where an allocation
+ * must not synchronise the device).  It needs no context: every work array
+ * of the V-cycles comes from one static device array of
+ * FHD_NOALLOC_SCRATCH_BYTES that each device loading the library keeps until
+ * exit.  Grids whose work arrays do not fit (larger than about 64^3 cells in
+ * 3D or 512^2 in 2D) are rejected with FHD_ERR_BAD_ARG and a message in
+ * fhd_last_error().  FP64 only; arguments as fhd_dev_stag_mg_solver plus the
+ * grid, the parameters and the stream (NULL = legacy default stream).
+ * The first call on a device looks up the array's device address.  All calls
+ * share the array: calls whose work overlaps on the GPU race with each
+ * other; serialise them (one stream, or synchronise between calls). */
+#define FHD_NOALLOC_SCRATCH_BYTES (16ll * 1024 * 1024)
+int fhd_dev_stag_mg_solver_noalloc(int dim, const int n_cells[3], double dx,
+                                   int visc_type,
+                                   const fhd_gmres_params* params,
+                                   const double* const alpha_fc[],
+                                   const double* beta,
+                                   const double* const beta_ed[],
+                                   const double* gamma, double theta_alpha,
+                                   double* const phi[],
+                                   const double* const rhs[], void* stream);
+
 /* ------------------------------------------------------------------ */
 /* host BoxLib-fab entry points (drop-in boundary)                     */
 /* ------------------------------------------------------------------ */

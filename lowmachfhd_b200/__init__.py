@@ -209,6 +209,20 @@ class StokesSolver:
         return check(lib().fhd_apply_precon(self._h, *mfs, float(theta_alpha)), "fhd_apply_precon")
 
 
+def stag_mg_solver_noalloc(dim, n_cells, dx, visc_type, params, alpha_fc, beta_cc, beta_ed, gamma_cc,
+                           theta_alpha, phi_fc, rhs_fc, stream=None):
+    """stag_mg_solver that allocates no device memory (no context needed):
+    for callers that cannot call cudaMalloc.  Work arrays live in the
+    library's static device array; grids beyond its size are rejected and
+    calls that overlap on the GPU race on it."""
+    n = list(n_cells) + [1] * (3 - len(n_cells))
+    return check(lib().fhd_dev_stag_mg_solver_noalloc(int(dim), (C.c_int * 3)(*n[:3]), float(dx), int(visc_type),
+                                                      C.byref(params), _dpp(alpha_fc), _dptr(beta_cc),
+                                                      _dpp(beta_ed), _dptr(gamma_cc), float(theta_alpha),
+                                                      _dpp(phi_fc), _dpp(rhs_fc), C.c_void_p(stream or 0)),
+                 "stag_mg_solver_noalloc")
+
+
 # ----------------------------------------------------------------------
 # host fab helpers (BoxLib layout <-> canonical layout, numpy)
 # ----------------------------------------------------------------------

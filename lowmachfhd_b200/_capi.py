@@ -106,6 +106,9 @@ _PROTOS = {
                                                C.c_double, _DP, C.c_int, _PP, _PP]),
     "fhd_dev_advance_inertial": (C.c_int, [_VP, C.POINTER(StochParams), C.c_double, _PP, _DP, _DP, _DP, _PP,
                                            _DP, _DP, _PP, _PP, _PP, C.POINTER(SolveStats)]),
+    "fhd_dev_stag_mg_solver_noalloc": (C.c_int, [C.c_int, C.POINTER(C.c_int), C.c_double, C.c_int,
+                                                 C.POINTER(GmresParams), _PP, _DP, _PP, _DP, C.c_double, _PP,
+                                                 _PP, _VP]),
     "fhd_gmres": (C.c_int, [_VP] + [C.POINTER(Multifab)] * 8 + [_DP, _DP, C.POINTER(SolveStats)]),
     "fhd_apply_precon": (C.c_int, [_VP] + [C.POINTER(Multifab)] * 8 + [C.c_double]),
     "fhd_apply_matrix": (C.c_int, [_VP] + [C.POINTER(Multifab)] * 8 + [C.c_double]),
