@@ -33,7 +33,18 @@ N_CELLS = 256
 DT = 0.05
 KT = 1e-4
 REL_TOL = 1e-8
-WORKLOAD = "lowmach_inertial_step_3d_256cube_periodic"
+NSPECIES = 4
+MOLMASS = [1.0, 2.0, 3.0, 4.0]
+WORKLOAD = "lowmach_inertial_step_3d_256cube_periodic_4species"
+
+
+def mixture(seed=11):
+    """4-species ideal mixture: masses 1..4, Maxwell-Stefan coefficients
+    D_ij ~ U[0.5, 2] * 1e-2 (seeded, symmetric), rhobar = 1"""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    D = list(rng.uniform(0.5, 2.0, NSPECIES * (NSPECIES - 1) // 2) * 1e-2)
+    return dict(molmass=MOLMASS, Dbar=D, rhobar=[1.0] * NSPECIES, variance_coef_mass=1.0)
 
 
 def parse():
@@ -45,7 +56,38 @@ def parse():
     ap.add_argument("--n", type=int, default=N_CELLS, help="cells per direction")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample-n", type=int, default=128)
+    ap.add_argument("--only", choices=["mixed", "fp64"], default=None, help="run one precision only")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--probe", choices=["stagmg"], default=None,
+                    help="profiling probe: K stag_mg_solver calls (one V-cycle each) on one grid")
+    ap.add_argument("--precision", choices=["mixed", "fp64"], default="fp64", help="precision of --probe")
     return ap.parse_args()
+
+
+def run_probe(args):
+    """K staggered multigrid solves on a random right-hand side (a small,
+    self-contained workload for kernel captures)."""
+    import torch
+
+    import lowmachfhd_b200 as L
+    dev = torch.device("cuda:0")
+    n = args.n
+    nc = n ** 3
+    s = L.StokesSolver(3, [n, n, n], 1.0, 1, params=L.default_params(gmres_max_inner=1),
+                       precision=args.precision)
+    g = torch.Generator().manual_seed(3)
+    f64 = dict(dtype=torch.float64)
+    alpha = [(1.0 + 1e-3 * torch.randn(nc, generator=g, **f64)).to(dev) for _ in range(3)]
+    one = torch.ones(nc, device=dev, **f64)
+    rhs = [torch.randn(nc, generator=g, **f64).to(dev) for _ in range(3)]
+    phi = [torch.zeros(nc, device=dev, **f64) for _ in range(3)]
+    for _ in range(args.warmup + args.steps):
+        s.stag_mg_solver(alpha, one, [one, one, one], torch.zeros(nc, device=dev, **f64), 20.0, phi, rhs)
+    torch.cuda.synchronize()
+    print(json.dumps({"probe": "stagmg", "n": n, "precision": args.precision, "calls": args.warmup + args.steps,
+                      "launches": s.kernel_launches}))
+    s.close()
+    return 0
 
 
 def peaks():
@@ -115,9 +157,10 @@ class Clocks:
 # problem set-up (seeded synthetic inputs; no dataset involved)
 # ----------------------------------------------------------------------
 def host_fields(n, seed, torch):
-    """one set of N(0,1) stochastic momentum fields, as fill_m_stochastic
-    prepares them (symmetric form: cell entries with variance 2, the two
-    edge components equal), pinned host float64"""
+    """one step's N(0,1) random fields, pinned host float64: the momentum
+    fields as fill_m_stochastic prepares them (symmetric form: cell entries
+    with variance 2, the two edge components equal) and the mass-flux face
+    fields of fill_mass_stochastic (3 directions x 4 species)"""
     g = torch.Generator().manual_seed(seed)
     nc = n ** 3
     W_cc = [torch.randn(nc, generator=g, dtype=torch.float64).mul_(2.0 ** 0.5).pin_memory() for _ in range(3)]
@@ -125,7 +168,8 @@ def host_fields(n, seed, torch):
     for _ in range(3):
         a = torch.randn(nc, generator=g, dtype=torch.float64).pin_memory()
         W_ed += [a, a]
-    return W_cc, W_ed
+    W_m = [torch.randn(nc, generator=g, dtype=torch.float64).pin_memory() for _ in range(3 * NSPECIES)]
+    return W_cc, W_ed, W_m
 
 
 class Case:
@@ -138,7 +182,12 @@ class Case:
         g = torch.Generator(device="cpu").manual_seed(seed)
         f64 = dict(dtype=torch.float64)
         self.umac = [(1e-3 * torch.randn(nc, generator=g, **f64)).to(dev) for _ in range(3)]
-        self.rho = (1.0 + 1e-3 * torch.randn(nc, generator=g, **f64)).to(dev)
+        # mass fractions 0.25 + 1e-3 N(0,1), renormalised; total density 1
+        w = 0.25 + 1e-3 * torch.randn(NSPECIES, nc, generator=g, **f64)
+        w = w / w.sum(dim=0, keepdim=True)
+        self.rho = [w[i].contiguous().to(dev) for i in range(NSPECIES)]
+        self.F = [torch.zeros(nc, device=dev, **f64) for _ in range(NSPECIES)]
+        self.mp = L.mixture_params(**mixture())
         self.pi = torch.zeros(nc, device=dev, **f64)
         self.eta = torch.ones(nc, device=dev, **f64)
         self.eta_ed = [torch.ones(nc, device=dev, **f64) for _ in range(3)]
@@ -147,9 +196,15 @@ class Case:
         self.T_ed = [torch.ones(nc, device=dev, **f64) for _ in range(3)]
         self.sp = L.StochParams(k_B=KT, variance_coef_mom=1.0, dV=1.0, stoch_stress_form=1, filtering_width=0)
 
-    def step(self, W_cc, W_ed):
-        return self.s.advance_timestep_inertial(self.sp, DT, self.umac, self.rho, self.pi, self.eta, self.eta_ed,
-                                                self.kappa, self.T, self.T_ed, W_cc, W_ed)
+    def init_fluxes(self, W_m_prev):
+        """F^0 = compute_mass_fluxdiv at the initial state (main_driver.f90
+        start-up, before the time loop)"""
+        self.s.compute_mass_fluxdiv(self.mp, self.sp, self.rho, DT, [1.0], W_m_prev, self.F)
+
+    def step(self, W_cc, W_ed, W_m_prev, W_m_new):
+        return self.s.advance_timestep_inertial_multispecies(
+            self.sp, self.mp, DT, self.umac, self.rho, self.pi, self.F, self.eta, self.eta_ed, self.kappa, self.T,
+            self.T_ed, W_cc, W_ed, list(W_m_prev) + list(W_m_new))
 
 
 def dist_init(args):
@@ -203,14 +258,20 @@ def cpu_sample(n_sample: int, n_full: int):
     for _ in range(3):
         a = rng.standard_normal(nc)
         W_ed += [a, a]
+    W_m = [rng.standard_normal(nc) for _ in range(2 * 3 * NSPECIES)]
+    w = 0.25 + 1e-3 * rng.standard_normal((NSPECIES, nc))
+    w /= w.sum(axis=0)
+    rho = [np.ascontiguousarray(w[i]) for i in range(NSPECIES)]
     sp = O.StochParams(k_B=KT, variance_coef_mom=1.0, dV=1.0, stoch_stress_form=1, filtering_width=0)
+    mp = O.mixture_params(**mixture())
+    F0 = O.mass_fluxdiv(3, [n_sample] * 3, 1.0, sp, mp, rho, DT, [1.0], W_m[: 3 * NSPECIES])
     t0 = time.perf_counter()
-    rc, *_ = O.advance_inertial(3, [n_sample] * 3, 1.0, 1, O.default_params(gmres_rel_tol=REL_TOL), sp, DT,
-                                umac, rho, pi, eta, ee, np.zeros(nc), np.ones(nc), ee, W_cc, W_ed)
+    rc, *_ = O.advance_inertial_ms(3, [n_sample] * 3, 1.0, 1, O.default_params(gmres_rel_tol=REL_TOL), sp, mp, DT,
+                                   umac, rho, pi, F0, eta, ee, np.zeros(nc), np.ones(nc), ee, W_cc, W_ed, W_m)
     sec = time.perf_counter() - t0
     scale = (n_full / n_sample) ** 3
     return {"value": 1.0 / (sec * scale), "unit": "steps/s", "cores": O.num_threads(), "kind": "port",
-            "sample": f"one FP64 inertial step at {n_sample}^3 on the CPU oracle ({sec:.2f} s), scaled by the "
+            "sample": f"one FP64 4-species inertial step at {n_sample}^3 on the CPU oracle ({sec:.2f} s), scaled by the "
                       f"cell ratio {scale:g} to the {n_full}^3 step (the GMRES iteration count does not grow "
                       f"with the grid under multigrid preconditioning)",
             "sample_seconds": sec}
@@ -235,7 +296,7 @@ def run_reference(args):
             "steps": len(secs), "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded N(0,1) fields)",
             "config": {"workload": WORKLOAD, "n_cells": [args.n] * 3, "dt": DT, "k_B": KT, "gmres_rel_tol": REL_TOL,
-                       "visc_type": 1, "species": 1},
+                       "visc_type": 1, "species": NSPECIES, "molmass": MOLMASS},
             "cpu_baseline": {"value": v, "unit": "steps/s", "cores": r["cores"], "kind": "port",
                              "sample": r["sample"]},
             "e2e": {"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -247,6 +308,8 @@ def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.probe:
+        return run_probe(args)
     import torch
 
     import lowmachfhd_b200 as L
@@ -261,18 +324,25 @@ def main():
     # stochastic fields: a ring of device-resident sets for the device-timed
     # run, and pinned host sets for the end-to-end run
     host_sets = [host_fields(n, 100 + 10 * rank + i, torch) for i in range(2)]
-    dev_sets = [([w.to(dev) for w in a], [w.to(dev) for w in b]) for a, b in host_sets]
+    dev_sets = [tuple([w.to(dev) for w in part] for part in hs) for hs in host_sets]
     torch.cuda.synchronize()
 
     results = {}
-    for precision in ("mixed", "fp64"):
+    for precision in ((args.only,) if args.only else ("mixed", "fp64")):
         case = Case(L, torch, dev, n, precision)
         # the context launches on a torch-owned stream so that torch's
         # pinned-memory and caching allocators never see a destroyed stream
         stream = torch.cuda.Stream(device=dev)
         case.s.set_stream(stream.cuda_stream)
+        R = len(dev_sets)
+        case.init_fluxes(dev_sets[R - 1][2])
+
+        def run_step(i, sets):
+            wc, we, wm = sets[i % len(sets)]
+            return case.step(wc, we, sets[(i - 1) % len(sets)][2], wm)
+
         for i in range(args.warmup):
-            case.step(*dev_sets[i % len(dev_sets)])
+            run_step(i, dev_sets)
         torch.cuda.synchronize()
         barrier(ws)
         clocks = Clocks(local)
@@ -285,7 +355,7 @@ def main():
         torch.cuda.synchronize()
         ev0.record(stream)
         for i in range(args.steps):
-            st, stats = case.step(*dev_sets[i % len(dev_sets)])
+            st, stats = run_step(args.warmup + i, dev_sets)
             iters.append([s["total_iters"] for s in stats])
         ev1.record(stream)
         torch.cuda.synchronize()
@@ -298,23 +368,31 @@ def main():
         ms_max = allmax(ws, ms, torch, dev)
         results[precision] = dict(ms=ms_max, iters=iters, prof=prof, launches=launches, clocks=clk,
                                   resid=stats[-1]["norm_resid"] / max(stats[-1]["norm_init_resid"], 1e-300))
-        if precision == "mixed":
+        if precision == "mixed" and not args.no_e2e:
             # end to end: per step the host->device copy of the step's
             # random fields from pinned memory, the step, and the read-back
             # of its solver diagnostics
-            h2d = sum(w.numel() * 8 for w in host_sets[0][0] + host_sets[0][1])
-            stage = ([torch.empty(nc, dtype=torch.float64, device=dev) for _ in range(3)],
-                     [torch.empty(nc, dtype=torch.float64, device=dev) for _ in range(6)])
+            h2d = sum(w.numel() * 8 for part in host_sets[0] for w in part)
+            stage = [tuple([torch.empty(nc, dtype=torch.float64, device=dev) for _ in part] for part in host_sets[0])
+                     for _ in range(2)]
+            # the set the first timed step treats as the previous step's
+            # fields is staged before the timed region
+            for part_d, part_h in zip(stage[1], host_sets[-1]):
+                for d_, h_ in zip(part_d, part_h):
+                    d_.copy_(h_)
             torch.cuda.synchronize()
             barrier(ws)
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
             with torch.cuda.stream(stream):
                 for i in range(args.steps):
-                    hc, he = host_sets[i % len(host_sets)]
-                    for d_, h_ in zip(stage[0] + stage[1], hc + he):
-                        d_.copy_(h_, non_blocking=True)
-                    st, stats = case.step(*stage)
+                    # this step's new fields go into one staging set; the
+                    # previous step's set stays resident for the predictor
+                    tgt = stage[i % 2]
+                    for part_d, part_h in zip(tgt, host_sets[i % len(host_sets)]):
+                        for d_, h_ in zip(part_d, part_h):
+                            d_.copy_(h_, non_blocking=True)
+                    st, stats = case.step(tgt[0], tgt[1], stage[(i - 1) % 2][2], tgt[2])
             e1.record(stream)
             torch.cuda.synchronize()
             e2e_ms = allmax(ws, e0.elapsed_time(e1), torch, dev)
@@ -325,6 +403,13 @@ def main():
         del case
         torch.cuda.empty_cache()
 
+    if args.only or args.no_e2e:
+        if rank == 0:
+            print(json.dumps({"partial_run": True, "only": args.only, "n": n, "steps": args.steps,
+                              **{k: {"ms_per_step": v["ms"] / args.steps, "gpu_launches": v["launches"],
+                                     "gmres_iters_per_step": [sum(x) for x in v["iters"]]}
+                                 for k, v in results.items() if k in ("mixed", "fp64")}}), flush=True)
+        return 0
     mixed, fp64 = results["mixed"], results["fp64"]
     K = args.steps
     value = ws * K / (mixed["ms"] / 1e3)
@@ -337,8 +422,9 @@ def main():
         "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": ws, "steps": K, "warmup": args.warmup,
         "ms_per_step": mixed["ms"] / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32 multigrid / f64 Krylov", "data": "synthetic (seeded N(0,1) stochastic fields)",
-        "config": {"workload": WORKLOAD, "n_cells": [n] * 3, "dt": DT, "k_B": KT, "rho": "1+1e-3 N(0,1)",
-                   "eta": 1.0, "visc_type": 1, "precon_type": 1, "gmres_rel_tol": REL_TOL, "species": 1,
+        "config": {"workload": WORKLOAD, "n_cells": [n] * 3, "dt": DT, "k_B": KT, "rho_total": 1.0,
+                   "eta": 1.0, "visc_type": 1, "precon_type": 1, "gmres_rel_tol": REL_TOL, "species": NSPECIES,
+                   "molmass": MOLMASS, "Dbar": "U[0.5,2]*1e-2 seeded", "w0": "0.25 + 1e-3 N(0,1), renormalised",
                    "parallelism": f"replicas x{ws}",
                    "l2": "inputs larger than L2 (each 256^3 field is 134 MB)"},
         "fp64": {"value": fp64_value, "unit": "steps/s", "ms_per_step": fp64["ms"] / K,

@@ -97,6 +97,25 @@ typedef struct fhd_stoch_params {
     int    filtering_width;        /* only 0 is supported */
 } fhd_stoch_params;
 
+/* Multispecies mixture parameters (namelist probin_multispecies,
+ * probin_multispecies.f90:100-140): ideal isothermal mixture, constant
+ * Maxwell-Stefan coefficients (mixture_type 0).  Dbar holds the
+ * nspecies*(nspecies-1)/2 off-diagonal entries in the order
+ * (2,1),(3,1),(3,2),(4,1),... of compute_D_bar_local
+ * (compute_mixture_properties.f90:217-273). */
+#define FHD_MAX_SPECIES 8
+typedef struct fhd_mixture_params {
+    int    nspecies;
+    double molmass[FHD_MAX_SPECIES];
+    double Dbar[FHD_MAX_SPECIES * (FHD_MAX_SPECIES - 1) / 2];
+    double rhobar[FHD_MAX_SPECIES];
+    double variance_coef_mass;
+    int    chi_iterations;         /* Dbar2chi_iterative iterations (10) */
+    double fraction_tolerance;     /* trace-species threshold (1e-14) */
+    int    correct_flux;           /* last species = -sum of the others */
+    int    avg_type;               /* compute_nonnegative_rho_av: 1,2,3,10 */
+} fhd_mixture_params;
+
 /* Per-solve diagnostics (gmres.f90:72-85 locals, vcycle_counter.f90). */
 typedef struct fhd_solve_stats {
     int    outer_iters;            /* gmres 'iter' */
@@ -208,6 +227,43 @@ int fhd_dev_advance_inertial(fhd_ctx* ctx, const fhd_stoch_params* sp,
                              const double* const W_cc[],
                              const double* const W_ed[],
                              fhd_solve_stats* stats2);
+
+/* compute_mass_fluxdiv (compute_mass_fluxdiv.f90:29-183) for an ideal
+ * isothermal mixture: mass_fluxdiv[i] = div of the corrected diffusive
+ * (diffusive_mass_fluxdiv.f90) plus stochastic (stochastic_mass_fluxdiv.f90:
+ * 37-116, compute_sqrtLonsager_fc mass_flux_utilities.f90:1096-1522) flux
+ * of species i.  rho: nspecies cell arrays.  W_fc[(r*dim+d)*nspecies+i]:
+ * N(0,1) field of rng r on the faces of direction d for species i
+ * (fill_mass_stochastic, stochastic_mass_fluxdiv.f90:182-214).  Uses k_B
+ * and dV of sp.  nspecies 2..5. */
+int fhd_dev_compute_mass_fluxdiv(fhd_ctx* ctx, const fhd_mixture_params* mp,
+                                 const fhd_stoch_params* sp,
+                                 const double* const rho[], double dt,
+                                 const double* weights, int n_rngs,
+                                 const double* const W_fc[],
+                                 double* const mass_fluxdiv[]);
+
+/* advance_timestep_inertial (advance_timestep_inertial.f90:45-923) for an
+ * ideal isothermal mixture of mp->nspecies species (centred advection,
+ * periodic box).  rho (nspecies cell arrays), umac, pi advanced in place;
+ * mass_fluxdiv holds F^n = div(diffusive + stochastic mass flux) on entry
+ * (from the previous step or compute_mass_fluxdiv at start-up) and F^{n+1}
+ * on exit.  W_mass: 2*dim*nspecies face arrays, first the fields of the
+ * previous corrector (the predictor reuses them, as the reference does
+ * between fill_mass_stochastic calls), then this step's new fields. */
+int fhd_dev_advance_inertial_multispecies(fhd_ctx* ctx, const fhd_stoch_params* sp,
+                                          const fhd_mixture_params* mp, double dt,
+                                          double* const umac[], double* const rho[],
+                                          double* pi, double* const mass_fluxdiv[],
+                                          const double* eta,
+                                          const double* const eta_ed[],
+                                          const double* kappa,
+                                          const double* temperature,
+                                          const double* const temperature_ed[],
+                                          const double* const W_cc[],
+                                          const double* const W_ed[],
+                                          const double* const W_mass[],
+                                          fhd_solve_stats* stats2);
 
 /* Text of the last CUDA error seen by the calling thread. */
 const char* fhd_last_error(void);

@@ -18,10 +18,11 @@ from typing import Sequence
 import numpy as np
 
 from . import _capi
-from ._capi import (FHD_PREC_FP64, FHD_PREC_MIXED, Fab, FhdError, GmresParams, Multifab, SolveStats,
-                    StochParams, check, lib)
+from ._capi import (FHD_PREC_FP64, FHD_PREC_MIXED, Fab, FhdError, GmresParams, MixtureParams, Multifab,
+                    SolveStats, StochParams, check, lib, mixture_params)
 
-__all__ = ["StokesSolver", "GmresParams", "StochParams", "SolveStats", "default_params", "FhdError",
+__all__ = ["StokesSolver", "GmresParams", "StochParams", "SolveStats", "MixtureParams", "mixture_params",
+           "default_params", "FhdError",
            "FHD_PREC_FP64", "FHD_PREC_MIXED", "lib", "fab_from_canonical", "canonical_from_fab", "FabArray"]
 
 
@@ -180,6 +181,29 @@ class StokesSolver:
                                                       _dptr(pi), _dptr(eta), _dpp(eta_ed), _dptr(kappa),
                                                       _dptr(temperature), _dpp(temperature_ed), _dpp(W_cc),
                                                       _dpp(W_ed), st), "advance_timestep_inertial")
+        return status, [st[0].as_dict(), st[1].as_dict()]
+
+    def compute_mass_fluxdiv(self, mp: MixtureParams, sp: StochParams, rho, dt, weights, W_fc, mass_fluxdiv):
+        """compute_mass_fluxdiv (compute_mass_fluxdiv.f90:29-183), ideal
+        isothermal mixture: mass_fluxdiv = div(diffusive + stochastic flux).
+        W_fc[(r*dim+d)*nspecies+i]: N(0,1) face fields."""
+        w = (C.c_double * len(weights))(*[float(x) for x in weights])
+        return check(lib().fhd_dev_compute_mass_fluxdiv(self._h, C.byref(mp), C.byref(sp), _dpp(rho), float(dt),
+                                                        C.cast(w, _DP), len(weights), _dpp(W_fc),
+                                                        _dpp(mass_fluxdiv)), "compute_mass_fluxdiv")
+
+    def advance_timestep_inertial_multispecies(self, sp: StochParams, mp: MixtureParams, dt, umac, rho, pi,
+                                               mass_fluxdiv, eta, eta_ed, kappa, temperature, temperature_ed,
+                                               W_cc, W_ed, W_mass):
+        """One inertial step of an ideal isothermal mixture
+        (advance_timestep_inertial.f90) in place on umac, rho (species
+        list), pi and mass_fluxdiv (F^n in, F^{n+1} out).  W_mass: the
+        previous corrector's dim*nspecies face fields, then the new ones."""
+        st = (SolveStats * 2)()
+        status = check(lib().fhd_dev_advance_inertial_multispecies(
+            self._h, C.byref(sp), C.byref(mp), float(dt), _dpp(umac), _dpp(rho), _dptr(pi), _dpp(mass_fluxdiv),
+            _dptr(eta), _dpp(eta_ed), _dptr(kappa), _dptr(temperature), _dpp(temperature_ed), _dpp(W_cc),
+            _dpp(W_ed), _dpp(W_mass), st), "advance_timestep_inertial_multispecies")
         return status, [st[0].as_dict(), st[1].as_dict()]
 
     # ----------------------------------------------------------------

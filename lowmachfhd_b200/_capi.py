@@ -58,6 +58,33 @@ class StochParams(C.Structure):
                 ("stoch_stress_form", C.c_int), ("filtering_width", C.c_int)]
 
 
+class MixtureParams(C.Structure):
+    """fhd_mixture_params (probin_multispecies.f90:100-140), ideal mixture."""
+    _fields_ = [("nspecies", C.c_int), ("molmass", C.c_double * 8), ("Dbar", C.c_double * 28),
+                ("rhobar", C.c_double * 8), ("variance_coef_mass", C.c_double), ("chi_iterations", C.c_int),
+                ("fraction_tolerance", C.c_double), ("correct_flux", C.c_int), ("avg_type", C.c_int)]
+
+
+def mixture_params(molmass, Dbar, rhobar=None, variance_coef_mass=1.0, chi_iterations=10,
+                   fraction_tolerance=1e-14, correct_flux=1, avg_type=1):
+    ns = len(molmass)
+    m = MixtureParams()
+    m.nspecies = ns
+    for i, v in enumerate(molmass):
+        m.molmass[i] = v
+    assert len(Dbar) == ns * (ns - 1) // 2
+    for i, v in enumerate(Dbar):
+        m.Dbar[i] = v
+    for i, v in enumerate(rhobar if rhobar is not None else [1.0] * ns):
+        m.rhobar[i] = v
+    m.variance_coef_mass = variance_coef_mass
+    m.chi_iterations = chi_iterations
+    m.fraction_tolerance = fraction_tolerance
+    m.correct_flux = correct_flux
+    m.avg_type = avg_type
+    return m
+
+
 class SolveStats(C.Structure):
     _fields_ = [("outer_iters", C.c_int), ("total_iters", C.c_int), ("vcycles", C.c_int),
                 ("status", C.c_int),
@@ -109,6 +136,11 @@ _PROTOS = {
     "fhd_dev_stag_mg_solver_noalloc": (C.c_int, [C.c_int, C.POINTER(C.c_int), C.c_double, C.c_int,
                                                  C.POINTER(GmresParams), _PP, _DP, _PP, _DP, C.c_double, _PP,
                                                  _PP, _VP]),
+    "fhd_dev_compute_mass_fluxdiv": (C.c_int, [_VP, C.POINTER(MixtureParams), C.POINTER(StochParams), _PP,
+                                               C.c_double, _DP, C.c_int, _PP, _PP]),
+    "fhd_dev_advance_inertial_multispecies": (C.c_int, [_VP, C.POINTER(StochParams), C.POINTER(MixtureParams),
+                                                        C.c_double, _PP, _PP, _DP, _PP, _DP, _PP, _DP, _DP, _PP,
+                                                        _PP, _PP, _PP, C.POINTER(SolveStats)]),
     "fhd_gmres": (C.c_int, [_VP] + [C.POINTER(Multifab)] * 8 + [_DP, _DP, C.POINTER(SolveStats)]),
     "fhd_apply_precon": (C.c_int, [_VP] + [C.POINTER(Multifab)] * 8 + [C.c_double]),
     "fhd_apply_matrix": (C.c_int, [_VP] + [C.POINTER(Multifab)] * 8 + [C.c_double]),

@@ -1,0 +1,547 @@
+// fhd_mass.cu -- multispecies mass fluxes (compute_mass_fluxdiv of
+// LowMachFHD src_multiSpec) for an ideal isothermal mixture: the diffusive
+// flux rhoWchi * grad(x) and the stochastic flux sqrt(2 k_B var/(dV dt)) *
+// chol(L(rho_av)) * W, each corrected to a zero species sum, and their
+// divergence.
+//
+// Compute-bound per face (Dbar2chi_iterative: chi_iterations dense NS x NS
+// products, a Cholesky factorisation, two matrix-vector products); the
+// matrices live in registers, the species count is a template parameter.
+// T = double, or float in the mixed-precision mode.
+#include <cmath>
+#include <cstring>
+
+#include "fhd_solver.cuh"
+
+namespace fhd {
+
+struct MixDev {
+    int ns;
+    double molmass[FHD_MAX_SPECIES];
+    double D[FHD_MAX_SPECIES][FHD_MAX_SPECIES];
+    double var_mass;
+    int chi_it;
+    double frac_tol;
+    int correct;
+    int avg_type;
+    double kB, dV;
+};
+
+MixDev make_mixdev(const fhd_mixture_params* mp, const fhd_stoch_params* sp) {
+    MixDev m;
+    memset(&m, 0, sizeof(m));
+    m.ns = mp->nspecies;
+    for (int i = 0; i < m.ns; i++) m.molmass[i] = mp->molmass[i];
+    int k = 0;
+    for (int r = 0; r < m.ns; r++) {
+        for (int c = 0; c < r; c++) {
+            m.D[r][c] = mp->Dbar[k];
+            m.D[c][r] = mp->Dbar[k];
+            k++;
+        }
+        m.D[r][r] = 0.0;
+    }
+    m.var_mass = mp->variance_coef_mass;
+    m.chi_it = mp->chi_iterations;
+    m.frac_tol = mp->fraction_tolerance;
+    m.correct = mp->correct_flux;
+    m.avg_type = mp->avg_type;
+    m.kB = sp->k_B;
+    m.dV = sp->dV;
+    return m;
+}
+
+// compute_molconc_molmtot_local (mass_flux_utilities.f90:159-186)
+template <typename T, int NS>
+__device__ __forceinline__ void d_molconc(const MixDev& m, const T* rho, T rhotot, T* x, T& mtot) {
+    T W[NS];
+    T s = T(0);
+#pragma unroll
+    for (int n = 0; n < NS; n++) {
+        W[n] = rho[n] / rhotot;
+        s = s + W[n] / (T)m.molmass[n];
+    }
+    mtot = T(1) / s;
+#pragma unroll
+    for (int n = 0; n < NS; n++) x[n] = mtot * W[n] / (T)m.molmass[n];
+}
+
+// compute_chi (mass_flux_utilities.f90:743-922): closed form for two
+// species, Dbar2chi_iterative (matrix_utilities.f90:19-158) otherwise
+template <typename T, int NS>
+__device__ __forceinline__ void d_chi(const MixDev& m, const T* rho, T rhotot, const T* Xk, T (&chi)[NS][NS]) {
+    if constexpr (NS == 2) {
+        const T W0 = rho[0] / rhotot, W1 = rho[1] / rhotot;
+        T t = (T)m.molmass[0] * W1 + (T)m.molmass[1] * W0;
+        t = (T)m.D[0][1] * t * t / (T)m.molmass[0] / (T)m.molmass[1];
+        chi[0][0] = t * W1 / W0;
+        chi[0][1] = -t;
+        chi[1][0] = -t;
+        chi[1][1] = t * W0 / W1;
+    } else {
+        T mw = T(0), Y[NS], Minv[NS];
+#pragma unroll
+        for (int i = 0; i < NS; i++) mw = mw + Xk[i] * (T)m.molmass[i];
+#pragma unroll
+        for (int i = 0; i < NS; i++) Y[i] = (T)m.molmass[i] / mw * Xk[i];
+        T Mm[NS];
+#pragma unroll
+        for (int i = 0; i < NS; i++) {
+            T t2 = T(0);
+#pragma unroll
+            for (int j = 0; j < NS; j++)
+                if (j != i) t2 = t2 + Xk[j] / (T)m.D[i][j];
+            const T Di = (T(1) - Y[i]) / t2;
+            Mm[i] = Xk[i] / Di;
+            Minv[i] = Di / Xk[i];
+        }
+        // J = Minv * (M - Delta); PJ = P J with P = I - 1 Y^T
+        T J[NS][NS];
+#pragma unroll
+        for (int i = 0; i < NS; i++) {
+#pragma unroll
+            for (int j = 0; j < NS; j++) {
+                T dl;
+                if (i == j) {
+                    T t1 = T(0);
+#pragma unroll
+                    for (int k = 0; k < NS; k++)
+                        if (k != i) t1 = t1 + Xk[i] * Xk[k] / (T)m.D[i][k];
+                    dl = t1;
+                } else {
+                    dl = -Xk[i] * Xk[j] / (T)m.D[i][j];
+                }
+                T z = -dl;
+                if (i == j) z = z + Mm[i];
+                J[i][j] = Minv[i] * z;
+            }
+        }
+        T PJ[NS][NS], m2[NS][NS];
+#pragma unroll
+        for (int i = 0; i < NS; i++)
+#pragma unroll
+            for (int j = 0; j < NS; j++) {
+                T a = T(0);
+#pragma unroll
+                for (int k = 0; k < NS; k++) {
+                    const T pik = (i == k ? T(1) : T(0)) - Y[k];
+                    a = a + pik * J[k][j];
+                }
+                PJ[i][j] = a;
+            }
+#pragma unroll
+        for (int i = 0; i < NS; i++)
+#pragma unroll
+            for (int j = 0; j < NS; j++) {
+                T scr = T(0);
+#pragma unroll
+                for (int k = 0; k < NS; k++) {
+                    const T pik = (i == k ? T(1) : T(0)) - Y[k];
+                    const T pjk = (j == k ? T(1) : T(0)) - Y[k];
+                    scr = scr + pik * Minv[k] * pjk;
+                }
+                m2[i][j] = scr;
+                chi[i][j] = scr;
+            }
+        for (int it = 0; it < m.chi_it; it++) {
+            T m1[NS][NS];
+#pragma unroll
+            for (int i = 0; i < NS; i++)
+#pragma unroll
+                for (int j = 0; j < NS; j++) {
+                    T scr = T(0);
+#pragma unroll
+                    for (int k = 0; k < NS; k++) scr = scr + PJ[i][k] * chi[k][j];
+                    m1[i][j] = scr + m2[i][j];
+                }
+#pragma unroll
+            for (int i = 0; i < NS; i++)
+#pragma unroll
+                for (int j = 0; j < NS; j++) chi[i][j] = m1[i][j];
+        }
+    }
+}
+
+template <typename T, int NS>
+__device__ __forceinline__ int d_ntrace(const MixDev& m, const T* rho, T rhotot) {
+    int nt = 0;
+#pragma unroll
+    for (int i = 0; i < NS; i++)
+        if (rho[i] / rhotot < (T)m.frac_tol) nt++;
+    return nt;
+}
+
+// choldc (matrix_utilities.f90:162-241)
+template <typename T, int NS>
+__device__ __forceinline__ void d_choldc(T (&a)[NS][NS]) {
+    T p[NS];
+#pragma unroll
+    for (int i = 0; i < NS; i++) {
+        int ising = 0;
+#pragma unroll
+        for (int j = i; j < NS; j++) {
+            T s = a[i][j];
+#pragma unroll
+            for (int k = i - 1; k >= 0; k--) s = s - a[i][k] * a[j][k];
+            if (i == j) {
+                if (s <= T(0)) {
+                    p[i] = T(0);
+                    ising = 1;
+                } else {
+                    p[i] = sqrt(s);
+                }
+            } else {
+                a[j][i] = (ising == 0) ? s / p[i] : T(0);
+            }
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < NS; i++) {
+#pragma unroll
+        for (int j = i + 1; j < NS; j++) a[i][j] = T(0);
+        a[i][i] = p[i];
+    }
+}
+
+// ---------------------------------------------------------------------
+// per cell: rhoWchi (compute_rhoWchi_local) and the molar concentrations
+// ---------------------------------------------------------------------
+template <typename T, int NS>
+__global__ void __launch_bounds__(128) k_rhowchi(Grid g, MixDev m, const double* const* __restrict__ rho,
+                                                 T* const* rwc, T* const* xo, int* flag) {
+    const i64 n = g.nc;
+    for (i64 f = blockIdx.x * (i64)blockDim.x + threadIdx.x; f < n; f += (i64)gridDim.x * blockDim.x) {
+        T r[NS];
+        T rt = T(0);
+#pragma unroll
+        for (int s = 0; s < NS; s++) {
+            r[s] = (T)rho[s][f];
+            rt = rt + r[s];
+        }
+        T x[NS], mt;
+        d_molconc<T, NS>(m, r, rt, x, mt);
+#pragma unroll
+        for (int s = 0; s < NS; s++) xo[s][f] = x[s];
+        const int nt = d_ntrace<T, NS>(m, r, rt);
+        if (nt == NS - 1) {
+#pragma unroll
+            for (int q = 0; q < NS * NS; q++) rwc[q][f] = T(0);
+            continue;
+        }
+        if (nt != 0) {
+            atomicOr(flag, 1);
+            continue;
+        }
+        T chi[NS][NS];
+        d_chi<T, NS>(m, r, rt, x, chi);
+#pragma unroll
+        for (int i = 0; i < NS; i++)
+#pragma unroll
+            for (int j = 0; j < NS; j++) rwc[i * NS + j][f] = r[i] * chi[i][j];
+    }
+}
+
+// ---------------------------------------------------------------------
+// per face of direction D (the low face of each cell): diffusive +
+// stochastic flux, corrected (correction_flux.f90:17-226)
+// ---------------------------------------------------------------------
+template <typename T, int NS, int DIM>
+__global__ void __launch_bounds__(128) k_mass_flux(Grid g, MixDev m, int d, const double* const* __restrict__ rho,
+                                                   const T* const* __restrict__ rwc, const T* const* __restrict__ xc,
+                                                   const double* const* __restrict__ W, int n_rngs,
+                                                   const double* wts, T variance, T dxinv, T* const* flux, int* flag) {
+    Cell P;
+    if (!cell_of_thread(g, P)) return;
+    const i64 f = P.id(0, 0, 0);
+    const i64 fm = P.id(-(d == 0), -(d == 1), -(d == 2));
+    T fd[NS];
+    {
+        T gx[NS];
+#pragma unroll
+        for (int s = 0; s < NS; s++) gx[s] = (ld(xc[s], f) - ld(xc[s], fm)) * dxinv;
+#pragma unroll
+        for (int r = 0; r < NS; r++) {
+            T acc = T(0);
+#pragma unroll
+            for (int c = 0; c < NS; c++) acc = acc + T(0.5) * (ld(rwc[r * NS + c], fm) + ld(rwc[r * NS + c], f)) * gx[c];
+            fd[r] = acc;
+        }
+        if (m.correct && NS > 1) {
+            T sum = T(0);
+#pragma unroll
+            for (int s = 0; s < NS - 1; s++) sum = sum + fd[s];
+            fd[NS - 1] = -sum;
+        }
+    }
+    T fs[NS];
+#pragma unroll
+    for (int s = 0; s < NS; s++) fs[s] = T(0);
+    if (m.var_mass != 0.0) {
+        // compute_nonnegative_rho_av (mass_flux_utilities.f90:1231-1328)
+        T ra[NS];
+        T rt = T(0);
+#pragma unroll
+        for (int c = 0; c < NS; c++) {
+            const T mm = (T)m.molmass[c];
+            const T v1 = (T)ld(rho[c], fm) / mm, v2 = (T)ld(rho[c], f) / mm;
+            T o;
+            if (m.avg_type == 2) {
+                o = mm * sqrt(fmax(v1, T(0)) * fmax(v2, T(0)));
+            } else if (m.avg_type == 3) {
+                o = (v1 <= T(0) || v2 <= T(0)) ? T(0) : mm * T(2) / (T(1) / v1 + T(1) / v2);
+            } else if (m.avg_type == 10) {
+                o = (v1 <= T(0) || v2 <= T(0)) ? T(0) : mm * (v1 + v2) / T(2);
+            } else {
+                if (v1 <= T(0) || v2 <= T(0)) {
+                    o = T(0);
+                } else {
+                    const T t1 = fmin((T)m.dV * v1, T(1)), t2 = fmin((T)m.dV * v2, T(1));
+                    o = mm * (v1 + v2) / T(2) * t1 * t2;
+                }
+            }
+            ra[c] = o;
+            rt = rt + o;
+        }
+        // compute_sqrtLonsager_local (mass_flux_utilities.f90:1331-1522)
+        T L[NS][NS];
+        const int nt = d_ntrace<T, NS>(m, ra, rt);
+        if (nt == NS - 1) {
+#pragma unroll
+            for (int i = 0; i < NS; i++)
+#pragma unroll
+                for (int j = 0; j < NS; j++) L[i][j] = T(0);
+        } else {
+            if (nt != 0) atomicOr(flag, 1);
+            T Wf[NS], x[NS], mt;
+#pragma unroll
+            for (int i = 0; i < NS; i++) Wf[i] = ra[i] / rt;
+            d_molconc<T, NS>(m, ra, rt, x, mt);
+            T chi[NS][NS];
+            d_chi<T, NS>(m, ra, rt, x, chi);
+            const T kB = (T)m.kB;
+#pragma unroll
+            for (int c = 0; c < NS; c++)
+#pragma unroll
+                for (int r = 0; r < NS; r++) L[r][c] = mt * rt * Wf[r] * chi[r][c] * Wf[c] / kB;
+            d_choldc<T, NS>(L);
+        }
+        T w[NS];
+#pragma unroll
+        for (int s = 0; s < NS; s++) {
+            T acc = T(0);
+            for (int rr = 0; rr < n_rngs; rr++) acc = acc + (T)wts[rr] * (T)ld(W[(rr * DIM + d) * NS + s], f);
+            w[s] = acc;
+        }
+#pragma unroll
+        for (int r = 0; r < NS; r++) {
+            T acc = T(0);
+#pragma unroll
+            for (int c = 0; c < NS; c++) acc = acc + L[r][c] * w[c];
+            fs[r] = acc * variance;
+        }
+        if (m.correct && NS > 1) {
+            T sum = T(0);
+#pragma unroll
+            for (int s = 0; s < NS - 1; s++) sum = sum + fs[s];
+            fs[NS - 1] = -sum;
+        }
+    }
+#pragma unroll
+    for (int s = 0; s < NS; s++) flux[d * NS + s][f] = fd[s] + fs[s];
+}
+
+// fluxdiv_s = div(flux_s)  (compute_div, div_and_grad.f90:884-1035)
+template <typename T, int NS, int DIM>
+__global__ void __launch_bounds__(256) k_mass_div(Grid g, const T* const* __restrict__ flux, double* const* out,
+                                                  T dxinv) {
+    Cell P;
+    if (!cell_of_thread(g, P)) return;
+    const i64 f = P.id(0, 0, 0);
+#pragma unroll
+    for (int s = 0; s < NS; s++) {
+        T v = (ld(flux[0 * NS + s], P.id(1, 0, 0)) - ld(flux[0 * NS + s], f)) * dxinv +
+              (ld(flux[1 * NS + s], P.id(0, 1, 0)) - ld(flux[1 * NS + s], f)) * dxinv;
+        if constexpr (DIM == 3) v += (ld(flux[2 * NS + s], P.id(0, 0, 1)) - ld(flux[2 * NS + s], f)) * dxinv;
+        out[s][f] = (double)v;
+    }
+}
+
+// ---------------------------------------------------------------------
+// host driver: device work arrays in the context, pointer tables in a
+// small device block
+// ---------------------------------------------------------------------
+struct MassBufs {
+    bool ready = false;
+    int ns = 0;
+    void* rwc = nullptr;   // ns*ns arrays of T
+    void* xc = nullptr;    // ns arrays of T
+    void* flux = nullptr;  // dim*ns arrays of T
+    void** tab = nullptr;  // device pointer tables
+    int* flag = nullptr;
+    double* wts = nullptr;
+};
+
+template <typename T>
+static int mass_alloc(fhd_ctx* ctx, MassBufs& B, int ns) {
+    if (B.ready && B.ns == ns) return 0;
+    if (B.ready) {
+        set_last_error("mass fluxes: the species count of a context cannot change");
+        return FHD_ERR_BAD_ARG;
+    }
+    const i64 nc = ctx->g0.nc;
+    const int dim = ctx->dim;
+    T* rw = ctx->arena.alloc<T>((i64)ns * ns * nc);
+    T* xc = ctx->arena.alloc<T>((i64)ns * nc);
+    T* fl = ctx->arena.alloc<T>((i64)dim * ns * nc);
+    void** tab = (void**)ctx->arena.alloc<double>(4 * 128);
+    int* flag = (int*)ctx->arena.alloc<double>(1);
+    double* wts = ctx->arena.alloc<double>(8);
+    if (!rw || !xc || !fl || !tab || !flag || !wts) return FHD_ERR_OOM;
+    B.rwc = rw;
+    B.xc = xc;
+    B.flux = fl;
+    B.tab = tab;
+    B.flag = flag;
+    B.wts = wts;
+    B.ns = ns;
+    B.ready = true;
+    FHD_CUDA_TRY(cudaMemsetAsync(flag, 0, sizeof(int), ctx->stream));
+    return 0;
+}
+
+template <typename T, int NS>
+static int mass_fluxdiv_T(fhd_ctx* ctx, MassBufs& B, const MixDev& m, const double* const rho[], double dt,
+                          const double* weights, int n_rngs, const double* const W[], double* const fluxdiv[]) {
+    const int dim = ctx->dim;
+    const i64 nc = ctx->g0.nc;
+    const Grid g = ctx->g0;
+    cudaStream_t st = ctx->stream;
+    // pointer tables: [0,128) rho, [128,256) rwc, [256,384) xc/flux, [384,512) W/out
+    void* h[512];
+    memset(h, 0, sizeof(h));
+    for (int s = 0; s < NS; s++) h[s] = (void*)rho[s];
+    for (int q = 0; q < NS * NS; q++) h[128 + q] = (T*)B.rwc + (i64)q * nc;
+    for (int s = 0; s < NS; s++) h[256 + s] = (T*)B.xc + (i64)s * nc;
+    for (int q = 0; q < dim * NS; q++) h[256 + 16 + q] = (T*)B.flux + (i64)q * nc;
+    for (int q = 0; q < n_rngs * dim * NS; q++) h[384 + q] = (void*)W[q];
+    for (int s = 0; s < NS; s++) h[384 + 96 + s] = (void*)fluxdiv[s];
+    FHD_CUDA_TRY(cudaMemcpyAsync(B.tab, h, sizeof(h), cudaMemcpyHostToDevice, st));
+    double hw[8] = {0};
+    for (int r = 0; r < n_rngs; r++) hw[r] = weights[r];
+    FHD_CUDA_TRY(cudaMemcpyAsync(B.wts, hw, sizeof(hw), cudaMemcpyHostToDevice, st));
+    const double* const* d_rho = (const double* const*)(B.tab);
+    T* const* d_rwc = (T* const*)(B.tab + 128);
+    T* const* d_xc = (T* const*)(B.tab + 256);
+    T* const* d_flux = (T* const*)(B.tab + 256 + 16);
+    const double* const* d_W = (const double* const*)(B.tab + 384);
+    double* const* d_out = (double* const*)(B.tab + 384 + 96);
+    const int nb = flat_blocks(nc);
+    k_rhowchi<T, NS><<<nb, 128, 0, st>>>(g, m, d_rho, d_rwc, d_xc, B.flag);
+    ctx->launches++;
+    FHD_CUDA_TRY(cudaPeekAtLastError());
+    const T variance = (T)sqrt(2.0 * m.kB * m.var_mass / (m.dV * dt));
+    const T dxinv = (T)(1.0 / ctx->dx);
+    for (int d = 0; d < dim; d++) {
+        with_dim(dim, [&](auto D) {
+            constexpr int DIM = decltype(D)::value;
+            k_mass_flux<T, NS, DIM><<<dim3((g.n[0] + 31) / 32, (g.n[1] + 3) / 4, g.n[2]), dim3(32, 4, 1), 0, st>>>(
+                g, m, d, d_rho, (const T* const*)d_rwc, (const T* const*)d_xc, d_W, n_rngs, B.wts, variance, dxinv,
+                d_flux, B.flag);
+        });
+        ctx->launches++;
+        FHD_CUDA_TRY(cudaPeekAtLastError());
+    }
+    with_dim(dim, [&](auto D) {
+        constexpr int DIM = decltype(D)::value;
+        k_mass_div<T, NS, DIM><<<cell_grid(g), cell_block(), 0, st>>>(g, (const T* const*)d_flux, d_out, dxinv);
+    });
+    ctx->launches++;
+    FHD_CUDA_TRY(cudaPeekAtLastError());
+    return 0;
+}
+
+template <typename T>
+static int mass_fluxdiv_dispatch(fhd_ctx* ctx, MassBufs& B, const MixDev& m, const double* const rho[], double dt,
+                                 const double* weights, int n_rngs, const double* const W[],
+                                 double* const fluxdiv[]) {
+    switch (m.ns) {
+        case 2: return mass_fluxdiv_T<T, 2>(ctx, B, m, rho, dt, weights, n_rngs, W, fluxdiv);
+        case 3: return mass_fluxdiv_T<T, 3>(ctx, B, m, rho, dt, weights, n_rngs, W, fluxdiv);
+        case 4: return mass_fluxdiv_T<T, 4>(ctx, B, m, rho, dt, weights, n_rngs, W, fluxdiv);
+        case 5: return mass_fluxdiv_T<T, 5>(ctx, B, m, rho, dt, weights, n_rngs, W, fluxdiv);
+        default:
+            set_last_error("mass fluxes: nspecies must be 2..5");
+            return FHD_ERR_UNSUPPORTED;
+    }
+}
+
+}  // namespace fhd
+
+using namespace fhd;
+
+#include <map>
+#include <mutex>
+static std::mutex g_mass_mu;
+static std::map<fhd_ctx*, MassBufs*> g_mass;
+
+extern "C" void fhd_mass_release(fhd_ctx* ctx) {
+    std::lock_guard<std::mutex> lk(g_mass_mu);
+    auto it = g_mass.find(ctx);
+    if (it == g_mass.end()) return;
+    delete it->second;
+    g_mass.erase(it);
+}
+
+namespace fhd {
+static MassBufs& mass_bufs(fhd_ctx* ctx) {
+    std::lock_guard<std::mutex> lk(g_mass_mu);
+    auto it = g_mass.find(ctx);
+    if (it != g_mass.end()) return *it->second;
+    MassBufs* b = new MassBufs();
+    g_mass[ctx] = b;
+    return *b;
+}
+
+// compute_mass_fluxdiv on the context's stream; the trace-species flag is
+// checked by the caller after synchronising
+int mass_fluxdiv(fhd_ctx* ctx, const fhd_mixture_params* mp, const fhd_stoch_params* sp, const double* const rho[],
+                 double dt, const double* weights, int n_rngs, const double* const W[], double* const fluxdiv[]) {
+    if (!mp || mp->nspecies < 2 || mp->nspecies > 5 || n_rngs < 1 || n_rngs > 4) {
+        set_last_error("mass fluxes: nspecies must be 2..5 and n_rngs 1..4");
+        return FHD_ERR_UNSUPPORTED;
+    }
+    if (ctx->dim * mp->nspecies * n_rngs > 96) return FHD_ERR_UNSUPPORTED;
+    MassBufs& B = mass_bufs(ctx);
+    const MixDev m = make_mixdev(mp, sp);
+    int rc;
+    if (ctx->prec == FHD_PREC_MIXED) {
+        if ((rc = mass_alloc<float>(ctx, B, mp->nspecies))) return rc;
+        return mass_fluxdiv_dispatch<float>(ctx, B, m, rho, dt, weights, n_rngs, W, fluxdiv);
+    }
+    if ((rc = mass_alloc<double>(ctx, B, mp->nspecies))) return rc;
+    return mass_fluxdiv_dispatch<double>(ctx, B, m, rho, dt, weights, n_rngs, W, fluxdiv);
+}
+
+int mass_flag_check(fhd_ctx* ctx) {
+    MassBufs& B = mass_bufs(ctx);
+    if (!B.ready) return 0;
+    int h = 0;
+    FHD_CUDA_TRY(cudaMemcpyAsync(&h, B.flag, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    FHD_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    if (h) {
+        FHD_CUDA_TRY(cudaMemsetAsync(B.flag, 0, sizeof(int), ctx->stream));
+        set_last_error("mass fluxes: trace species (mass fraction below fraction_tolerance) are not supported");
+        return FHD_ERR_UNSUPPORTED;
+    }
+    return 0;
+}
+}  // namespace fhd
+
+extern "C" int fhd_dev_compute_mass_fluxdiv(fhd_ctx* ctx, const fhd_mixture_params* mp, const fhd_stoch_params* sp,
+                                            const double* const rho[], double dt, const double* weights, int n_rngs,
+                                            const double* const W_fc[], double* const out[]) {
+    if (!ctx || !mp || !sp || !rho || !weights || !W_fc || !out) return FHD_ERR_BAD_ARG;
+    int rc = fhd::mass_fluxdiv(ctx, mp, sp, rho, dt, weights, n_rngs, W_fc, out);
+    if (rc) return rc;
+    return mass_flag_check(ctx);
+}

@@ -1094,11 +1094,13 @@ int fhd_ctx_create(int dim, const int n_cells[3], const double dx[3], int visc_t
 }
 
 void fhd_host_path_release(fhd_ctx* ctx);
+void fhd_mass_release(fhd_ctx* ctx);
 
 int fhd_ctx_destroy(fhd_ctx* c) {
     if (!c) return FHD_OK;
     if (c->stream) cudaStreamSynchronize(c->stream);
     fhd_host_path_release(c);
+    fhd_mass_release(c);
     c->arena.release();
     for (cudaEvent_t e : c->prof_ev) cudaEventDestroy(e);
     c->prof_ev.clear();

@@ -203,7 +203,7 @@ struct fhd_ctx {
     int m = 5;
     // inertial-step work arrays (allocated on the first step)
     bool step_ready = false;
-    double* sb[64] = {nullptr};
+    double* sb[128] = {nullptr};
     // optional timing of the finest-level smoother launches (CUDA events on
     // the context stream) with their algorithmic bytes
     bool prof = false;
@@ -236,4 +236,7 @@ int prepare(fhd_ctx* ctx, const double* const alpha_fc[], const double* beta, co
 int stag_mg_solve_dev(fhd_ctx* ctx, double* const phi[], const double* const rhs[]);
 int gmres_dev(fhd_ctx* ctx, CSVec<double> b, SVec<double> x, double* norm_pre_rhs, fhd_solve_stats* st);
 int sync_scalars(fhd_ctx* ctx, int first, int count);
+int mass_fluxdiv(fhd_ctx* ctx, const fhd_mixture_params* mp, const fhd_stoch_params* sp, const double* const rho[],
+                 double dt, const double* weights, int n_rngs, const double* const W[], double* const fluxdiv[]);
+int mass_flag_check(fhd_ctx* ctx);
 }  // namespace fhd

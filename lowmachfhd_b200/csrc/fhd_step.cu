@@ -127,12 +127,14 @@ __global__ void __launch_bounds__(256) k_avg_face(Grid g, const double* cc, doub
 }
 
 // centred scalar advection (mk_advective_s_fluxdiv.f90:138-220),
-// upd = -div(s_fc u), folded into the scalar update:
-//   mode 0: s_out = s_a + dt*upd                   (predictor Euler)
-//   mode 1: s_out = ((s_out + s_a) + dt*upd)*0.5   (trapezoidal corrector)
+// upd = -div(s_fc u), folded into the scalar update; upd (nullable) is the
+// rho_update array of the step, accumulated in place
+//   mode 0: upd = -div;      s_out = s_a + dt*upd          (predictor)
+//   mode 2: upd = upd - div; s_out = s_a + dt*upd          (predictor with F^n)
+//   mode 1: upd = upd - div; s_out = ((s_out + s_a) + dt*upd)*0.5 (corrector)
 template <int DIM>
 __global__ void __launch_bounds__(256) k_adv_s_update(Grid g, CSVec<double> u, CSVec<double> sfc, const double* sa,
-                                                      double* sout, double dt, double dxinv, int mode) {
+                                                      double* sout, double dt, double dxinv, int mode, double* upd) {
     Cell P;
     if (!cell_of_thread(g, P)) return;
     const i64 f = P.id(0, 0, 0);
@@ -142,12 +144,13 @@ __global__ void __launch_bounds__(256) k_adv_s_update(Grid g, CSVec<double> u, C
         const i64 fp = P.id(d == 0, d == 1, d == 2);
         s += (ld(u.c[d], fp) * ld(sfc.c[d], fp) - ld(u.c[d], f) * ld(sfc.c[d], f)) * dxinv;
     }
-    const double upd = -s;
-    if (mode == 0) {
-        sout[f] = sa[f] + dt * upd;
+    double up = (mode == 0) ? -s : upd[f] - s;
+    if (upd) upd[f] = up;
+    if (mode != 1) {
+        sout[f] = sa[f] + dt * up;
     } else {
         double v = sout[f] + sa[f];
-        v = v + dt * upd;
+        v = v + dt * up;
         sout[f] = v * 0.5;
     }
 }
@@ -223,13 +226,16 @@ __global__ void __launch_bounds__(256) k_mul(i64 n, int ncomp, SVec<double> y, C
 }
 
 // ---------------------------------------------------------------------
-// inertial step (advance_timestep_inertial.f90:45-923), single species
+// inertial step (advance_timestep_inertial.f90:45-923) for ns species;
+// ns = 1 without a mixture is a single fluid without mass fluxes
 // ---------------------------------------------------------------------
 enum {
     B_RFO = 0, B_RFN = 3, B_MOLD = 6, B_MTEMP = 9, B_ADV = 12, B_DIFF = 15, B_RHSV = 18, B_DU = 21, B_STOCH = 24,
-    B_GPI = 27, B_RHOOLD = 30, B_RHSP = 31, B_DPI = 32, B_ETAH = 33, B_KAPH = 34, B_ETAEDH = 35, B_ZERO = 38,
-    B_COUNT = 39
+    B_GPI = 27, B_RHOTOT = 30, B_RHSP = 31, B_DPI = 32, B_ETAH = 33, B_KAPH = 34, B_ETAEDH = 35, B_ZERO = 38,
+    B_RHOOLD = 39, B_RUPD = 39 + FHD_MAX_SPECIES, B_SFC = 39 + 2 * FHD_MAX_SPECIES,
+    B_COUNT = 39 + 5 * FHD_MAX_SPECIES
 };
+static_assert(B_COUNT <= 128, "step buffer table");
 
 static int step_alloc(fhd_ctx* ctx) {
     if (ctx->step_ready) return 0;
@@ -256,6 +262,12 @@ static CSVec<double> cs(SVec<double> v) {
 static SVec<double> svp(double* const* a, int dim) {
     SVec<double> v;
     for (int c = 0; c < 4; c++) v.c[c] = (c < dim) ? a[c] : nullptr;
+    return v;
+}
+static SVec<double> one(double* a) {
+    SVec<double> v;
+    for (int c = 0; c < 4; c++) v.c[c] = nullptr;
+    v.c[0] = a;
     return v;
 }
 
@@ -292,29 +304,46 @@ static int diff_m(fhd_ctx* ctx, SVec<double> out, CSVec<double> u, const double*
     return 0;
 }
 
-static int lin(fhd_ctx* ctx, SVec<double> y, int keep, std::initializer_list<std::pair<double, CSVec<double>>> terms) {
+// y = (keep ? y : 0) + sum_t a_t x_t over the first ncomp components
+static int lin_n(fhd_ctx* ctx, int ncomp, SVec<double> y, int keep,
+                 std::initializer_list<std::pair<double, CSVec<double>>> terms) {
     Lin L;
     memset(&L, 0, sizeof(L));
     int t = 0;
     for (auto& pr : terms) {
         L.a[t] = pr.first;
-        for (int c = 0; c < ctx->dim; c++) L.x[t][c] = pr.second.c[c];
+        for (int c = 0; c < ncomp; c++) L.x[t][c] = pr.second.c[c];
         t++;
     }
     L.nt = t;
-    k_lin<<<flat_blocks(ctx->g0.nc), 256, 0, ctx->stream>>>(ctx->g0.nc, ctx->dim, y, L, keep);
+    k_lin<<<flat_blocks(ctx->g0.nc), 256, 0, ctx->stream>>>(ctx->g0.nc, ncomp, y, L, keep);
     ctx->launches++;
     FHD_CUDA_TRY(cudaPeekAtLastError());
     return 0;
 }
+static int lin(fhd_ctx* ctx, SVec<double> y, int keep, std::initializer_list<std::pair<double, CSVec<double>>> terms) {
+    return lin_n(ctx, ctx->dim, y, keep, terms);
+}
 
-int advance_inertial(fhd_ctx* ctx, const fhd_stoch_params* sp, double dt, double* const umac[], double* rho,
-                     double* pi, const double* eta, const double* const eta_ed[], const double* kappa,
-                     const double* temperature, const double* const temperature_ed[], const double* const W_cc[],
-                     const double* const W_ed[], fhd_solve_stats* stats2) {
+// out = sum over species (compute_rhotot)
+__global__ void __launch_bounds__(256) k_sum_species(i64 n, int ns, const double* const* __restrict__ r, double* out) {
+    for (i64 f = blockIdx.x * (i64)blockDim.x + threadIdx.x; f < n; f += (i64)gridDim.x * blockDim.x) {
+        double v = 0.0;
+        for (int s = 0; s < ns; s++) v = v + r[s][f];
+        out[f] = v;
+    }
+}
+
+int advance_inertial_ms(fhd_ctx* ctx, const fhd_stoch_params* sp, const fhd_mixture_params* mp, double dt,
+                        double* const umac[], double* const rho[], double* pi, double* const fluxdiv[],
+                        const double* eta, const double* const eta_ed[], const double* kappa,
+                        const double* temperature, const double* const temperature_ed[], const double* const W_cc[],
+                        const double* const W_ed[], const double* const W_mass[], fhd_solve_stats* stats2) {
     int rc = step_alloc(ctx);
     if (rc) return rc;
     const int dim = ctx->dim, nE = dim == 2 ? 1 : 3;
+    const int ns = mp ? mp->nspecies : 1;
+    if (ns < 1 || ns > FHD_MAX_SPECIES) return FHD_ERR_BAD_ARG;
     const Grid g = ctx->g0;
     const i64 nc = g.nc;
     const int nb = flat_blocks(nc);
@@ -325,37 +354,97 @@ int advance_inertial(fhd_ctx* ctx, const fhd_stoch_params* sp, double dt, double
     SVec<double> rfo = sv(ctx, B_RFO), rfn = sv(ctx, B_RFN), mold = sv(ctx, B_MOLD), mtemp = sv(ctx, B_MTEMP),
                  adv = sv(ctx, B_ADV), diff = sv(ctx, B_DIFF), rhs_v = sv(ctx, B_RHSV), du = sv(ctx, B_DU),
                  stoch = sv(ctx, B_STOCH), gpi = sv(ctx, B_GPI);
-    double* rho_old = ctx->sb[B_RHOOLD];
+    double* rhotot = ctx->sb[B_RHOTOT];
     double* rhs_p = ctx->sb[B_RHSP];
     double* dpi = ctx->sb[B_DPI];
     double* eta_h = ctx->sb[B_ETAH];
     double* kap_h = ctx->sb[B_KAPH];
     const double* eta_ed_h[3] = {ctx->sb[B_ETAEDH], ctx->sb[B_ETAEDH + 1], ctx->sb[B_ETAEDH + 2]};
+    double* rho_old[FHD_MAX_SPECIES];
+    double* rupd[FHD_MAX_SPECIES];
+    for (int s = 0; s < ns; s++) {
+        rho_old[s] = ctx->sb[B_RHOOLD + s];
+        rupd[s] = ctx->sb[B_RUPD + s];
+    }
+    auto sfc = [&](int s) { return sv(ctx, B_SFC + s * dim); };
     const double w1[1] = {1.0};
+    // pointer tables for the species sums live in the zero-initialised
+    // tail of the context's scalar block (slots 200..255)
+    double** rtab = (double**)(ctx->dscal + 200);
+    auto sum_species = [&](double* const* r, double* out) -> int {
+        double* h[FHD_MAX_SPECIES];
+        for (int s = 0; s < ns; s++) h[s] = r[s];
+        FHD_CUDA_TRY(cudaMemcpyAsync(rtab, h, sizeof(double*) * ns, cudaMemcpyHostToDevice, st));
+        k_sum_species<<<nb, 256, 0, st>>>(nc, ns, rtab, out);
+        ctx->launches++;
+        FHD_CUDA_TRY(cudaPeekAtLastError());
+        // the host table is reused by the next call: wait for the copy
+        FHD_CUDA_TRY(cudaStreamSynchronize(st));
+        return 0;
+    };
+    auto species_fc = [&](double* const* r) {
+        for (int s = 0; s < ns; s++) {
+            SVec<double> o = sfc(s);
+            with_dim(dim, [&](auto D) {
+                constexpr int DIM = decltype(D)::value;
+                k_avg_face<DIM><<<cell_grid(g), cell_block(), 0, st>>>(g, r[s], o.c[0], o.c[1], o.c[2]);
+            });
+            ctx->launches++;
+        }
+    };
+    auto mass_fluxes = [&](const double* const* Wm) -> int {
+        if (!mp) return 0;
+        const double* cr[FHD_MAX_SPECIES];
+        for (int s = 0; s < ns; s++) cr[s] = rho[s];
+        return mass_fluxdiv(ctx, mp, sp, cr, dt, w1, 1, Wm, fluxdiv);
+    };
+    // -S = sum_i -F_i/rhobar_i into rhs_p (advance_timestep_inertial.f90:420-430)
+    auto rhs_p_from_fluxes = [&]() -> int {
+        FHD_CUDA_TRY(cudaMemsetAsync(rhs_p, 0, sizeof(double) * nc, st));
+        if (!mp) return 0;
+        for (int s = 0; s < ns; s++) {
+            int r2 = lin_n(ctx, 1, one(rhs_p), 1, {{-1.0 / mp->rhobar[s], cs(one(fluxdiv[s]))}});
+            if (r2) return r2;
+        }
+        return 0;
+    };
+    auto launch_dim = [&](auto&& fn) {
+        with_dim(dim, fn);
+        ctx->launches++;
+    };
     // eta/2, kappa/2 for the solves (advance_timestep_inertial.f90:467-474)
     k_copy_conv<double, double><<<nb, 256, 0, st>>>(nc, eta_h, eta, 0.5);
-    ctx->launches++;
     k_copy_conv<double, double><<<nb, 256, 0, st>>>(nc, kap_h, kappa, 0.5);
-    ctx->launches++;
+    ctx->launches += 2;
     for (int e = 0; e < nE; e++) {
         k_copy_conv<double, double><<<nb, 256, 0, st>>>(nc, (double*)eta_ed_h[e], eta_ed[e], 0.5);
         ctx->launches++;
     }
-    FHD_CUDA_TRY(cudaMemcpyAsync(rho_old, rho, sizeof(double) * nc, cudaMemcpyDeviceToDevice, st));
-    auto launch_dim = [&](auto&& fn) { with_dim(dim, fn); ctx->launches++; };
-    // Step 2: predictor Euler step for rho
+    for (int s = 0; s < ns; s++)
+        FHD_CUDA_TRY(cudaMemcpyAsync(rho_old[s], rho[s], sizeof(double) * nc, cudaMemcpyDeviceToDevice, st));
+    // Step 2: predictor Euler step for the densities
+    if ((rc = sum_species(rho_old, rhotot))) return rc;
     launch_dim([&](auto D) {
         constexpr int DIM = decltype(D)::value;
-        k_avg_face<DIM><<<cell_grid(g), cell_block(), 0, st>>>(g, rho_old, rfo.c[0], rfo.c[1], rfo.c[2]);
+        k_avg_face<DIM><<<cell_grid(g), cell_block(), 0, st>>>(g, rhotot, rfo.c[0], rfo.c[1], rfo.c[2]);
     });
+    species_fc(rho_old);
+    for (int s = 0; s < ns; s++) {
+        if (mp) FHD_CUDA_TRY(cudaMemcpyAsync(rupd[s], fluxdiv[s], sizeof(double) * nc, cudaMemcpyDeviceToDevice, st));
+        // rho_new = rho_old + dt*(F^n - div(rho_fc u))
+        const SVec<double> f3 = sfc(s);
+        launch_dim([&](auto D) {
+            constexpr int DIM = decltype(D)::value;
+            k_adv_s_update<DIM><<<cell_grid(g), cell_block(), 0, st>>>(g, cs(u), cs(f3), rho_old[s], rho[s], dt, dxinv,
+                                                                      mp ? 2 : 0, rupd[s]);
+        });
+    }
+    if ((rc = sum_species(rho, rhotot))) return rc;
     launch_dim([&](auto D) {
         constexpr int DIM = decltype(D)::value;
-        k_adv_s_update<DIM><<<cell_grid(g), cell_block(), 0, st>>>(g, cs(u), cs(rfo), rho_old, rho, dt, dxinv, 0);
+        k_avg_face<DIM><<<cell_grid(g), cell_block(), 0, st>>>(g, rhotot, rfn.c[0], rfn.c[1], rfn.c[2]);
     });
-    launch_dim([&](auto D) {
-        constexpr int DIM = decltype(D)::value;
-        k_avg_face<DIM><<<cell_grid(g), cell_block(), 0, st>>>(g, rho, rfn.c[0], rfn.c[1], rfn.c[2]);
-    });
+    species_fc(rho);
     // Steps 3-4: predictor Crank-Nicolson right-hand side
     k_mul<<<nb, 256, 0, st>>>(nc, dim, mold, cs(rfo), cs(u));
     ctx->launches++;
@@ -373,17 +462,21 @@ int advance_inertial(fhd_ctx* ctx, const fhd_stoch_params* sp, double dt, double
     if ((rc = diff_m(ctx, diff, cs(u), eta, eta_ed, kappa))) return rc;
     if ((rc = lin(ctx, rhs_v, 1, {{0.5, cs(diff)}}))) return rc;
     if (sp->variance_coef_mom != 0.0) {
-        if ((rc = stoch_launch(ctx, sp, stoch.c, 0, eta, eta_ed, temperature, temperature_ed, dt, w1, 1, W_cc,
-                               W_ed)))
+        if ((rc = stoch_launch(ctx, sp, stoch.c, 0, eta, eta_ed, temperature, temperature_ed, dt, w1, 1, W_cc, W_ed)))
             return rc;
         if ((rc = lin(ctx, rhs_v, 1, {{1.0, cs(stoch)}}))) return rc;
     }
-    FHD_CUDA_TRY(cudaMemsetAsync(rhs_p, 0, sizeof(double) * nc, st));
+    if ((rc = mass_fluxes(W_mass))) return rc;
+    if ((rc = rhs_p_from_fluxes())) return rc;
     k_mul<<<nb, 256, 0, st>>>(nc, dim, mtemp, cs(rfn), cs(u));
     ctx->launches++;
     if ((rc = lin(ctx, rhs_v, 1, {{-1.0 / dt, cs(mtemp)}}))) return rc;
     if ((rc = diff_m(ctx, mtemp, cs(u), eta, eta_ed, kappa))) return rc;
     if ((rc = lin(ctx, rhs_v, 1, {{0.5, cs(mtemp)}}))) return rc;
+    for (int s = 0; s < ns; s++) {
+        if (mp) FHD_CUDA_TRY(cudaMemcpyAsync(rupd[s], fluxdiv[s], sizeof(double) * nc, cudaMemcpyDeviceToDevice, st));
+        else FHD_CUDA_TRY(cudaMemsetAsync(rupd[s], 0, sizeof(double) * nc, st));
+    }
     launch_dim([&](auto D) {
         constexpr int DIM = decltype(D)::value;
         k_div_inc<DIM><<<cell_grid(g), cell_block(), 0, st>>>(g, cs(u), rhs_p, dxinv);
@@ -409,33 +502,27 @@ int advance_inertial(fhd_ctx* ctx, const fhd_stoch_params* sp, double dt, double
     if (st1 < 0) return st1;
     // corrector stopping criterion (advance_timestep_inertial.f90:493-496)
     ctx->p.gmres_abs_tol = fmax(abs_tol_in, norm_pre_rhs * ctx->p.gmres_rel_tol);
-    if ((rc = lin(ctx, u, 1, {{1.0, cs(du)}}))) { ctx->p.gmres_abs_tol = abs_tol_in; return rc; }
-    {
-        SVec<double> pv;
-        for (int c = 0; c < 4; c++) pv.c[c] = nullptr;
-        pv.c[0] = pi;
-        Lin L;
-        memset(&L, 0, sizeof(L));
-        L.nt = 1;
-        L.a[0] = 1.0;
-        L.x[0][0] = dpi;
-        k_lin<<<nb, 256, 0, st>>>(nc, 1, pv, L, 1);
-        ctx->launches++;
-    }
-    k_mul<<<nb, 256, 0, st>>>(nc, dim, mtemp, cs(rfn), cs(u));
-    ctx->launches++;
-    // Step 5: trapezoidal scalar corrector
-    launch_dim([&](auto D) {
-        constexpr int DIM = decltype(D)::value;
-        k_adv_s_update<DIM><<<cell_grid(g), cell_block(), 0, st>>>(g, cs(u), cs(rfn), rho_old, rho, dt, dxinv, 1);
-    });
-    launch_dim([&](auto D) {
-        constexpr int DIM = decltype(D)::value;
-        k_avg_face<DIM><<<cell_grid(g), cell_block(), 0, st>>>(g, rho, rfn.c[0], rfn.c[1], rfn.c[2]);
-    });
-    // Steps 6-7: corrector Crank-Nicolson right-hand side
     int rc2 = 0;
     do {
+        if ((rc2 = lin(ctx, u, 1, {{1.0, cs(du)}}))) break;
+        if ((rc2 = lin_n(ctx, 1, one(pi), 1, {{1.0, cs(one(dpi))}}))) break;
+        k_mul<<<nb, 256, 0, st>>>(nc, dim, mtemp, cs(rfn), cs(u));
+        ctx->launches++;
+        // Step 5: trapezoidal scalar corrector
+        for (int s = 0; s < ns; s++) {
+            const SVec<double> f3 = sfc(s);
+            launch_dim([&](auto D) {
+                constexpr int DIM = decltype(D)::value;
+                k_adv_s_update<DIM><<<cell_grid(g), cell_block(), 0, st>>>(g, cs(u), cs(f3), rho_old[s], rho[s], dt,
+                                                                          dxinv, 1, rupd[s]);
+            });
+        }
+        if ((rc2 = sum_species(rho, rhotot))) break;
+        launch_dim([&](auto D) {
+            constexpr int DIM = decltype(D)::value;
+            k_avg_face<DIM><<<cell_grid(g), cell_block(), 0, st>>>(g, rhotot, rfn.c[0], rfn.c[1], rfn.c[2]);
+        });
+        // Steps 6-7: corrector Crank-Nicolson right-hand side
         if ((rc2 = lin(ctx, rhs_v, 0, {{1.0 / dt, cs(mold)}}))) break;
         launch_dim([&](auto D) {
             constexpr int DIM = decltype(D)::value;
@@ -454,7 +541,8 @@ int advance_inertial(fhd_ctx* ctx, const fhd_stoch_params* sp, double dt, double
                 break;
             if ((rc2 = lin(ctx, rhs_v, 1, {{0.5, cs(stoch)}}))) break;
         }
-        FHD_CUDA_TRY(cudaMemsetAsync(rhs_p, 0, sizeof(double) * nc, st));
+        if ((rc2 = mass_fluxes(W_mass ? W_mass + dim * ns : nullptr))) break;
+        if ((rc2 = rhs_p_from_fluxes())) break;
         k_mul<<<nb, 256, 0, st>>>(nc, dim, mtemp, cs(rfn), cs(u));
         ctx->launches++;
         if ((rc2 = lin(ctx, rhs_v, 1, {{-1.0 / dt, cs(mtemp)}}))) break;
@@ -464,26 +552,21 @@ int advance_inertial(fhd_ctx* ctx, const fhd_stoch_params* sp, double dt, double
             constexpr int DIM = decltype(D)::value;
             k_div_inc<DIM><<<cell_grid(g), cell_block(), 0, st>>>(g, cs(u), rhs_p, dxinv);
         });
-        for (int c = 0; c < dim; c++) FHD_CUDA_TRY(cudaMemsetAsync(du.c[c], 0, sizeof(double) * nc, st));
-        FHD_CUDA_TRY(cudaMemsetAsync(dpi, 0, sizeof(double) * nc, st));
+        for (int c = 0; c < dim; c++) {
+            if (cudaMemsetAsync(du.c[c], 0, sizeof(double) * nc, st) != cudaSuccess) rc2 = FHD_ERR_CUDA;
+        }
+        if (cudaMemsetAsync(dpi, 0, sizeof(double) * nc, st) != cudaSuccess) rc2 = FHD_ERR_CUDA;
     } while (0);
-    if (rc2) { ctx->p.gmres_abs_tol = abs_tol_in; return rc2; }
+    if (rc2) {
+        ctx->p.gmres_abs_tol = abs_tol_in;
+        return rc2;
+    }
     int st2 = solve(stats2 ? &stats2[1] : nullptr, nullptr);
     ctx->p.gmres_abs_tol = abs_tol_in;
     if (st2 < 0) return st2;
     if ((rc = lin(ctx, u, 1, {{1.0, cs(du)}}))) return rc;
-    {
-        SVec<double> pv;
-        for (int c = 0; c < 4; c++) pv.c[c] = nullptr;
-        pv.c[0] = pi;
-        Lin L;
-        memset(&L, 0, sizeof(L));
-        L.nt = 1;
-        L.a[0] = 1.0;
-        L.x[0][0] = dpi;
-        k_lin<<<nb, 256, 0, st>>>(nc, 1, pv, L, 1);
-        ctx->launches++;
-    }
+    if ((rc = lin_n(ctx, 1, one(pi), 1, {{1.0, cs(one(dpi))}}))) return rc;
+    if (mp && (rc = mass_flag_check(ctx))) return rc;
     FHD_CUDA_TRY(cudaPeekAtLastError());
     return st1 > st2 ? st1 : st2;
 }
@@ -514,8 +597,26 @@ int fhd_dev_advance_inertial(fhd_ctx* ctx, const fhd_stoch_params* sp, double dt
     if (!ctx || !sp || !umac || !rho || !pi || !eta || !eta_ed || !kappa || !temperature || !temperature_ed ||
         !W_cc || !W_ed || !(dt > 0.0))
         return FHD_ERR_BAD_ARG;
-    int rc = advance_inertial(ctx, sp, dt, umac, rho, pi, eta, eta_ed, kappa, temperature, temperature_ed, W_cc,
-                              W_ed, stats2);
+    double* r[1] = {rho};
+    int rc = advance_inertial_ms(ctx, sp, nullptr, dt, umac, r, pi, nullptr, eta, eta_ed, kappa, temperature,
+                                 temperature_ed, W_cc, W_ed, nullptr, stats2);
+    if (rc < 0) return rc;
+    FHD_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    return rc;
+}
+
+int fhd_dev_advance_inertial_multispecies(fhd_ctx* ctx, const fhd_stoch_params* sp, const fhd_mixture_params* mp,
+                                          double dt, double* const umac[], double* const rho[], double* pi,
+                                          double* const mass_fluxdiv[], const double* eta,
+                                          const double* const eta_ed[], const double* kappa,
+                                          const double* temperature, const double* const temperature_ed[],
+                                          const double* const W_cc[], const double* const W_ed[],
+                                          const double* const W_mass[], fhd_solve_stats* stats2) {
+    if (!ctx || !sp || !mp || !umac || !rho || !pi || !mass_fluxdiv || !eta || !eta_ed || !kappa || !temperature ||
+        !temperature_ed || !W_cc || !W_ed || !W_mass || !(dt > 0.0))
+        return FHD_ERR_BAD_ARG;
+    int rc = advance_inertial_ms(ctx, sp, mp, dt, umac, rho, pi, mass_fluxdiv, eta, eta_ed, kappa, temperature,
+                                 temperature_ed, W_cc, W_ed, W_mass, stats2);
     if (rc < 0) return rc;
     FHD_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
     return rc;

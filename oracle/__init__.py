@@ -60,6 +60,33 @@ class StochParams(C.Structure):
                 ("stoch_stress_form", C.c_int), ("filtering_width", C.c_int)]
 
 
+class MixtureParams(C.Structure):
+    """fhd_mixture_params (probin_multispecies.f90:100-140), ideal mixture."""
+    _fields_ = [("nspecies", C.c_int), ("molmass", C.c_double * 8), ("Dbar", C.c_double * 28),
+                ("rhobar", C.c_double * 8), ("variance_coef_mass", C.c_double), ("chi_iterations", C.c_int),
+                ("fraction_tolerance", C.c_double), ("correct_flux", C.c_int), ("avg_type", C.c_int)]
+
+
+def mixture_params(molmass, Dbar, rhobar=None, variance_coef_mass=1.0, chi_iterations=10,
+                   fraction_tolerance=1e-14, correct_flux=1, avg_type=1):
+    ns = len(molmass)
+    m = MixtureParams()
+    m.nspecies = ns
+    for i, v in enumerate(molmass):
+        m.molmass[i] = v
+    assert len(Dbar) == ns * (ns - 1) // 2
+    for i, v in enumerate(Dbar):
+        m.Dbar[i] = v
+    for i, v in enumerate(rhobar if rhobar is not None else [1.0] * ns):
+        m.rhobar[i] = v
+    m.variance_coef_mass = variance_coef_mass
+    m.chi_iterations = chi_iterations
+    m.fraction_tolerance = fraction_tolerance
+    m.correct_flux = correct_flux
+    m.avg_type = avg_type
+    return m
+
+
 class SolveStats(C.Structure):
     _fields_ = [("outer_iters", C.c_int), ("total_iters", C.c_int), ("vcycles", C.c_int),
                 ("status", C.c_int),
@@ -241,3 +268,38 @@ def stag_mg_history(pb: Problem, params, theta, rhs):
                                   C.c_double(theta), _pp(phi), _pp(rhs), _p(hist))
     assert rc == 0
     return hist
+
+
+def mass_fluxdiv(dim, n, dx, sp, mp, rho, dt, weights, W_fc, want_flux=False):
+    nc = int(np.prod(n[:dim]))
+    ns = mp.nspecies
+    out = [np.zeros(nc) for _ in range(ns)]
+    flux = [np.zeros(nc) for _ in range(dim * ns)] if want_flux else None
+    w = np.ascontiguousarray(weights, np.float64)
+    rc = lib().or_mass_fluxdiv(dim, _n3(n), C.c_double(dx), C.byref(sp), C.byref(mp), _pp(rho), C.c_double(dt),
+                               _p(w), len(weights), _pp(W_fc), _pp(out), _pp(flux) if want_flux else None)
+    assert rc == 0, rc
+    return (out, flux) if want_flux else out
+
+
+def advance_inertial_ms(dim, n, dx, visc_type, params, sp, mp, dt, umac, rho, pi, fluxdiv, eta, eta_ed, kappa,
+                        temp, temp_ed, W_cc, W_ed, W_mass):
+    umac = [u.copy() for u in umac]
+    rho = [r.copy() for r in rho]
+    fluxdiv = [f.copy() for f in fluxdiv]
+    pi = pi.copy()
+    st = (SolveStats * 2)()
+    rc = lib().or_advance_inertial_ms(dim, _n3(n), C.c_double(dx), visc_type, C.byref(params), C.byref(sp),
+                                      C.byref(mp), C.c_double(dt), _pp(umac), _pp(rho), _p(pi), _pp(fluxdiv),
+                                      _p(eta), _pp(eta_ed), _p(kappa), _p(temp), _pp(temp_ed), _pp(W_cc),
+                                      _pp(W_ed), _pp(W_mass), st)
+    return rc, umac, rho, pi, fluxdiv, st
+
+
+def mixture_local(mp, k_B, rho):
+    ns = mp.nspecies
+    chi = np.zeros(ns * ns)
+    L = np.zeros(ns * ns)
+    rc = lib().or_mixture_local(C.byref(mp), C.c_double(k_B), _p(np.ascontiguousarray(rho, np.float64)), _p(chi),
+                                _p(L))
+    return rc, chi.reshape(ns, ns), L.reshape(ns, ns)

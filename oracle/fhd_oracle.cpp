@@ -1104,6 +1104,343 @@ void adv_s(const Geo& g, const double* const u[], const double* const s_fc[], do
     });
 }
 
+
+// ---------------------------------------------------------------------
+// multispecies mass fluxes (src_multiSpec of LowMachFHD), ideal mixture,
+// isothermal, no barodiffusion, periodic
+// ---------------------------------------------------------------------
+struct Mix {
+    int ns;
+    double molmass[FHD_MAX_SPECIES];
+    double D[FHD_MAX_SPECIES][FHD_MAX_SPECIES];  // D_bar, zero diagonal
+    double rhobar[FHD_MAX_SPECIES];
+    double var_mass;
+    int chi_it;
+    double frac_tol;
+    int correct;
+    int avg_type;
+};
+
+Mix make_mix(const fhd_mixture_params* mp) {
+    Mix m;
+    m.ns = mp->nspecies;
+    for (int i = 0; i < m.ns; i++) {
+        m.molmass[i] = mp->molmass[i];
+        m.rhobar[i] = mp->rhobar[i];
+    }
+    // compute_D_bar_local (compute_mixture_properties.f90:217-273): the
+    // off-diagonal entries in the order (2,1),(3,1),(3,2),(4,1),...
+    int k = 0;
+    for (int r = 0; r < m.ns; r++) {
+        for (int c = 0; c < r; c++) {
+            m.D[r][c] = mp->Dbar[k];
+            m.D[c][r] = mp->Dbar[k];
+            k++;
+        }
+        m.D[r][r] = 0.0;
+    }
+    m.var_mass = mp->variance_coef_mass;
+    m.chi_it = mp->chi_iterations;
+    m.frac_tol = mp->fraction_tolerance;
+    m.correct = mp->correct_flux;
+    m.avg_type = mp->avg_type;
+    return m;
+}
+
+// compute_molconc_molmtot_local (mass_flux_utilities.f90:159-186)
+void molconc(int ns, const double* molmass, const double* rho, double rhotot, double* x, double* mtot) {
+    double W[FHD_MAX_SPECIES];
+    double s = 0.0;
+    for (int n = 0; n < ns; n++) {
+        W[n] = rho[n] / rhotot;
+        s = s + W[n] / molmass[n];
+    }
+    *mtot = 1.0 / s;
+    for (int n = 0; n < ns; n++) x[n] = *mtot * W[n] / molmass[n];
+}
+
+// Dbar2chi_iterative (matrix_utilities.f90:19-158)
+void dbar2chi(int ns, int iters, const double D[][FHD_MAX_SPECIES], const double* Xk, const double* molmass,
+              double chi[][FHD_MAX_SPECIES]) {
+    double mw = 0.0, Y[FHD_MAX_SPECIES], Di[FHD_MAX_SPECIES], M[FHD_MAX_SPECIES], Minv[FHD_MAX_SPECIES];
+    double Pm[FHD_MAX_SPECIES][FHD_MAX_SPECIES], Dl[FHD_MAX_SPECIES][FHD_MAX_SPECIES];
+    double Z[FHD_MAX_SPECIES][FHD_MAX_SPECIES], J[FHD_MAX_SPECIES][FHD_MAX_SPECIES];
+    double PJ[FHD_MAX_SPECIES][FHD_MAX_SPECIES], m2[FHD_MAX_SPECIES][FHD_MAX_SPECIES];
+    double m1[FHD_MAX_SPECIES][FHD_MAX_SPECIES];
+    for (int i = 0; i < ns; i++) mw = mw + Xk[i] * molmass[i];
+    for (int i = 0; i < ns; i++) Y[i] = molmass[i] / mw * Xk[i];
+    for (int i = 0; i < ns; i++) {
+        double t2 = 0.0;
+        for (int j = 0; j < ns; j++)
+            if (j != i) t2 = t2 + Xk[j] / D[i][j];
+        Di[i] = (1.0 - Y[i]) / t2;
+    }
+    for (int i = 0; i < ns; i++) {
+        M[i] = Xk[i] / Di[i];
+        Minv[i] = Di[i] / Xk[i];
+    }
+    for (int i = 0; i < ns; i++)
+        for (int j = 0; j < ns; j++) {
+            Pm[i][j] = -Y[j];
+            if (i == j) Pm[i][j] = Pm[i][j] + 1.0;
+        }
+    for (int i = 0; i < ns; i++)
+        for (int j = 0; j < ns; j++) {
+            if (i == j) {
+                double t1 = 0.0;
+                for (int k = 0; k < ns; k++)
+                    if (k != i) t1 = t1 + Xk[i] * Xk[k] / D[i][k];
+                Dl[i][i] = t1;
+            } else {
+                Dl[i][j] = -Xk[i] * Xk[j] / D[i][j];
+            }
+            Z[i][j] = -Dl[i][j];
+        }
+    for (int i = 0; i < ns; i++) Z[i][i] = Z[i][i] + M[i];
+    for (int i = 0; i < ns; i++)
+        for (int j = 0; j < ns; j++) J[i][j] = Minv[i] * Z[i][j];
+    for (int i = 0; i < ns; i++)
+        for (int j = 0; j < ns; j++) {
+            double a = 0.0;
+            for (int k = 0; k < ns; k++) a = a + Pm[i][k] * J[k][j];
+            PJ[i][j] = a;
+        }
+    for (int i = 0; i < ns; i++)
+        for (int j = 0; j < ns; j++) {
+            double scr = 0.0;
+            for (int k = 0; k < ns; k++) scr = scr + Pm[i][k] * Minv[k] * Pm[j][k];
+            m2[i][j] = scr;
+            chi[i][j] = scr;
+        }
+    for (int it = 0; it < iters; it++) {
+        for (int i = 0; i < ns; i++)
+            for (int j = 0; j < ns; j++) {
+                double scr = 0.0;
+                for (int k = 0; k < ns; k++) scr = scr + PJ[i][k] * chi[k][j];
+                m1[i][j] = scr + m2[i][j];
+            }
+        for (int i = 0; i < ns; i++)
+            for (int j = 0; j < ns; j++) chi[i][j] = m1[i][j];
+    }
+}
+
+// compute_chi (mass_flux_utilities.f90:743-922) without LAPACK
+void chi_of(const Mix& m, const double* rho, double rhotot, const double* x, double chi[][FHD_MAX_SPECIES]) {
+    if (m.ns == 2) {
+        double W0 = rho[0] / rhotot, W1 = rho[1] / rhotot;
+        double t = m.molmass[0] * W1 + m.molmass[1] * W0;
+        t = m.D[0][1] * t * t / m.molmass[0] / m.molmass[1];
+        chi[0][0] = t * W1 / W0;
+        chi[0][1] = -t;
+        chi[1][0] = -t;
+        chi[1][1] = t * W0 / W1;
+        return;
+    }
+    dbar2chi(m.ns, m.chi_it, m.D, x, m.molmass, chi);
+}
+
+// number of trace species (w < fraction_tolerance)
+int n_trace(const Mix& m, const double* rho, double rhotot) {
+    int nt = 0;
+    for (int i = 0; i < m.ns; i++)
+        if (rho[i] / rhotot < m.frac_tol) nt++;
+    return nt;
+}
+
+// compute_rhoWchi_local (mass_flux_utilities.f90:529-741); returns false
+// when trace species other than "all but one" are present
+bool rhowchi_local(const Mix& m, const double* rho, double out[][FHD_MAX_SPECIES]) {
+    const int ns = m.ns;
+    double rt = 0.0;
+    for (int i = 0; i < ns; i++) rt = rt + rho[i];
+    const int nt = n_trace(m, rho, rt);
+    if (nt == ns - 1) {
+        for (int i = 0; i < ns; i++)
+            for (int j = 0; j < ns; j++) out[i][j] = 0.0;
+        return true;
+    }
+    if (nt != 0) return false;
+    double x[FHD_MAX_SPECIES], mt, chi[FHD_MAX_SPECIES][FHD_MAX_SPECIES];
+    molconc(ns, m.molmass, rho, rt, x, &mt);
+    chi_of(m, rho, rt, x, chi);
+    for (int i = 0; i < ns; i++)
+        for (int j = 0; j < ns; j++) out[i][j] = rho[i] * chi[i][j];
+    return true;
+}
+
+// choldc (matrix_utilities.f90:162-241): lower Cholesky factor in place,
+// zero rows after a non-positive pivot
+void choldc(int np, double a[][FHD_MAX_SPECIES]) {
+    double p[FHD_MAX_SPECIES];
+    for (int i = 0; i < np; i++) {
+        int ising = 0;
+        for (int j = i; j < np; j++) {
+            double s = a[i][j];
+            for (int k = i - 1; k >= 0; k--) s = s - a[i][k] * a[j][k];
+            if (i == j) {
+                if (s <= 0.0) {
+                    p[i] = 0.0;
+                    ising = 1;
+                } else {
+                    p[i] = std::sqrt(s);
+                }
+            } else {
+                a[j][i] = (ising == 0) ? s / p[i] : 0.0;
+            }
+        }
+    }
+    for (int i = 0; i < np; i++) {
+        for (int j = i + 1; j < np; j++) a[i][j] = 0.0;
+        a[i][i] = p[i];
+    }
+}
+
+// compute_nonnegative_rho_av (mass_flux_utilities.f90:1231-1328)
+void rho_av(const Mix& m, const double* r1, const double* r2, double dv, double* out) {
+    for (int c = 0; c < m.ns; c++) {
+        const double v1 = r1[c] / m.molmass[c], v2 = r2[c] / m.molmass[c];
+        double o;
+        switch (m.avg_type) {
+            case 2:
+                o = m.molmass[c] * std::sqrt(std::max(v1, 0.0) * std::max(v2, 0.0));
+                break;
+            case 3:
+                o = (v1 <= 10.0 * 2.2250738585072014e-308 || v2 <= 10.0 * 2.2250738585072014e-308)
+                        ? 0.0 : m.molmass[c] * 2.0 / (1.0 / v1 + 1.0 / v2);
+                break;
+            case 10:
+                o = (v1 <= 0.0 || v2 <= 0.0) ? 0.0 : m.molmass[c] * (v1 + v2) / 2.0;
+                break;
+            default: {  // 1: arithmetic with a C0-smoothed Heaviside
+                if (v1 <= 0.0 || v2 <= 0.0) {
+                    o = 0.0;
+                } else {
+                    const double t1 = std::min(dv * v1, 1.0), t2 = std::min(dv * v2, 1.0);
+                    o = m.molmass[c] * (v1 + v2) / 2.0 * t1 * t2;
+                }
+            }
+        }
+        out[c] = o;
+    }
+}
+
+// compute_sqrtLonsager_local (mass_flux_utilities.f90:1331-1522), k_B
+bool sqrtL_local(const Mix& m, const double* rho, double kB, double out[][FHD_MAX_SPECIES]) {
+    const int ns = m.ns;
+    double rt = 0.0;
+    for (int i = 0; i < ns; i++) rt = rt + rho[i];
+    const int nt = n_trace(m, rho, rt);
+    if (nt == ns - 1) {
+        for (int i = 0; i < ns; i++)
+            for (int j = 0; j < ns; j++) out[i][j] = 0.0;
+        return true;
+    }
+    if (nt != 0) return false;
+    double W[FHD_MAX_SPECIES], x[FHD_MAX_SPECIES], mt, chi[FHD_MAX_SPECIES][FHD_MAX_SPECIES];
+    for (int i = 0; i < ns; i++) W[i] = rho[i] / rt;
+    molconc(ns, m.molmass, rho, rt, x, &mt);
+    chi_of(m, rho, rt, x, chi);
+    for (int c = 0; c < ns; c++)
+        for (int r = 0; r < ns; r++) out[r][c] = mt * rt * W[r] * chi[r][c] * W[c] / kB;
+    choldc(ns, out);
+    return true;
+}
+
+// compute_mass_fluxdiv (compute_mass_fluxdiv.f90:29-183) for an ideal
+// isothermal mixture: flux = rhoWchi_face * grad(x) + variance *
+// sqrtL_face * sum_r w_r W_r, each corrected to zero species sum
+// (correction_flux.f90:17-226), and its divergence.  Returns the faces'
+// total flux in flux[d*ns+i] (nullable) and div into fluxdiv[i].
+int mass_fluxdiv_impl(const Geo& g, const Mix& m, const fhd_stoch_params* sp, const double* const rho[], double dt,
+                      const double* weights, int n_rngs, const double* const W_fc[], double* const fluxdiv[],
+                      double* const flux_out[]) {
+    const int dim = g.dim, ns = m.ns;
+    const long nc = g.nc;
+    std::vector<Vec> rwc(ns * ns, Vec(nc)), xcc(ns, Vec(nc));
+    bool ok = true;
+#pragma omp parallel for reduction(&& : ok)
+    for (long f = 0; f < nc; f++) {
+        double r[FHD_MAX_SPECIES], a[FHD_MAX_SPECIES][FHD_MAX_SPECIES], x[FHD_MAX_SPECIES], mt;
+        double rt = 0.0;
+        for (int i = 0; i < ns; i++) {
+            r[i] = rho[i][f];
+            rt = rt + r[i];
+        }
+        ok = rhowchi_local(m, r, a) && ok;
+        molconc(ns, m.molmass, r, rt, x, &mt);
+        for (int i = 0; i < ns; i++) {
+            xcc[i][f] = x[i];
+            for (int j = 0; j < ns; j++) rwc[i * ns + j][f] = a[i][j];
+        }
+    }
+    if (!ok) return FHD_ERR_UNSUPPORTED;
+    const double variance = std::sqrt(2.0 * sp->k_B * m.var_mass / (sp->dV * dt));
+    const double dxinv = 1.0 / g.dx;
+    std::vector<Vec> flux(dim * ns, Vec(nc));
+    bool ok2 = true;
+    for (int d = 0; d < dim; d++) {
+        int e[3] = {0, 0, 0};
+        e[d] = 1;
+        forall(g, [&](int i, int j, int k) {
+            const long f = g.id(i, j, k), fm = g.id(i - e[0], j - e[1], k - e[2]);
+            // diffusive: rhoWchi face average times grad(molar concentration)
+            double gx[FHD_MAX_SPECIES], fd[FHD_MAX_SPECIES], fs[FHD_MAX_SPECIES];
+            for (int s = 0; s < ns; s++) gx[s] = (xcc[s][f] - xcc[s][fm]) * dxinv;
+            for (int r = 0; r < ns; r++) {
+                double acc = 0.0;
+                for (int c = 0; c < ns; c++) acc = acc + 0.5 * (rwc[r * ns + c][fm] + rwc[r * ns + c][f]) * gx[c];
+                fd[r] = acc;
+            }
+            if (m.correct && ns > 1) {
+                double sum = 0.0;
+                for (int s = 0; s < ns - 1; s++) sum = sum + fd[s];
+                fd[ns - 1] = -sum;
+            }
+            // stochastic: sqrtL(rho_av) times the weighted random vector
+            for (int s = 0; s < ns; s++) fs[s] = 0.0;
+            if (m.var_mass != 0.0) {
+                double r1[FHD_MAX_SPECIES], r2[FHD_MAX_SPECIES], ra[FHD_MAX_SPECIES];
+                double L[FHD_MAX_SPECIES][FHD_MAX_SPECIES], w[FHD_MAX_SPECIES];
+                for (int s = 0; s < ns; s++) {
+                    r1[s] = rho[s][fm];
+                    r2[s] = rho[s][f];
+                }
+                rho_av(m, r1, r2, sp->dV, ra);
+                if (!sqrtL_local(m, ra, sp->k_B, L)) ok2 = false;
+                for (int s = 0; s < ns; s++) {
+                    double acc = 0.0;
+                    for (int rr = 0; rr < n_rngs; rr++) acc = acc + weights[rr] * W_fc[(rr * dim + d) * ns + s][f];
+                    w[s] = acc;
+                }
+                for (int r = 0; r < ns; r++) {
+                    double acc = 0.0;
+                    for (int c = 0; c < ns; c++) acc = acc + L[r][c] * w[c];
+                    fs[r] = acc * variance;
+                }
+                if (m.correct && ns > 1) {
+                    double sum = 0.0;
+                    for (int s = 0; s < ns - 1; s++) sum = sum + fs[s];
+                    fs[ns - 1] = -sum;
+                }
+            }
+            for (int s = 0; s < ns; s++) flux[d * ns + s][f] = fd[s] + fs[s];
+        });
+    }
+    if (!ok2) return FHD_ERR_UNSUPPORTED;
+    forall(g, [&](int i, int j, int k) {
+        const long f = g.id(i, j, k);
+        for (int s = 0; s < ns; s++) {
+            double v = (flux[0 * ns + s][g.id(i + 1, j, k)] - flux[0 * ns + s][f]) * dxinv +
+                       (flux[1 * ns + s][g.id(i, j + 1, k)] - flux[1 * ns + s][f]) * dxinv;
+            if (dim == 3) v += (flux[2 * ns + s][g.id(i, j, k + 1)] - flux[2 * ns + s][f]) * dxinv;
+            fluxdiv[s][f] = v;
+        }
+    });
+    if (flux_out)
+        for (int q = 0; q < dim * ns; q++) std::copy(flux[q].begin(), flux[q].end(), flux_out[q]);
+    return 0;
+}
+
 }  // namespace
 
 // =====================================================================
@@ -1207,37 +1544,46 @@ void or_average_cc_to_face(int dim, const int n[3], const double* cc, double* co
     avg_face(g, cc, fc);
 }
 
-int or_advance_inertial(int dim, const int n[3], double dx, int visc_type, const fhd_gmres_params* p_in,
-                        const fhd_stoch_params* sp, double dt, double* const umac[], double* rho, double* pi,
-                        const double* eta, const double* const eta_ed[], const double* kappa,
-                        const double* temperature, const double* const temperature_ed[],
-                        const double* const W_cc[], const double* const W_ed[], fhd_solve_stats* stats2) {
-    Geo g(dim, n, dx);
+}  // extern "C" (reopened below)
+
+namespace {
+// advance_timestep_inertial (advance_timestep_inertial.f90:45-923),
+// periodic, centred advection, no gravity; ns species (ns = 1 with no
+// mixture: a single fluid without mass fluxes).  fluxdiv (ns arrays) holds
+// F^n = div(diffusive + stochastic mass flux) on entry and F^{n+1} on exit;
+// W_mass[0 .. dim*ns) are the mass-flux random fields of the previous
+// corrector (used again by this predictor), W_mass[dim*ns .. 2*dim*ns) the
+// new fields drawn for this corrector.
+int step_impl(const Geo& g, int visc_type, const fhd_gmres_params* p_in, const fhd_stoch_params* sp, const Mix* mix,
+              double dt, double* const umac[], double* const rho[], double* pi, double* const fluxdiv[],
+              const double* eta, const double* const eta_ed[], const double* kappa, const double* temperature,
+              const double* const temperature_ed[], const double* const W_cc[], const double* const W_ed[],
+              const double* const W_mass[], fhd_solve_stats* stats2) {
+    const int dim = g.dim;
     const long nc = g.nc;
     const int nE = n_edge(dim);
+    const int ns = mix ? mix->ns : 1;
     fhd_gmres_params p = *p_in;
     const double theta = 1.0 / dt;
-    const double one = 1.0;
     auto fvec = [&](std::vector<Vec>& v) { v.assign(dim, Vec(nc, 0.0)); };
     auto ptrs = [&](std::vector<Vec>& v, double** out) { for (int c = 0; c < dim; c++) out[c] = v[c].data(); };
-    std::vector<Vec> rho_fc_old, rho_fc_new, mold, mtemp, adv, diff, rhs_v, dumac, stoch, gradpi, zero_a;
+    std::vector<Vec> rho_fc_old, rho_fc_new, mold, mtemp, adv, diff, rhs_v, dumac, stoch, gradpi;
     fvec(rho_fc_old); fvec(rho_fc_new); fvec(mold); fvec(mtemp); fvec(adv); fvec(diff); fvec(rhs_v);
-    fvec(dumac); fvec(stoch); fvec(gradpi); fvec(zero_a);
-    double *rfo[3], *rfn[3], *mo[3], *mt[3], *ad[3], *df[3], *rv[3], *du[3], *sto[3], *gpi[3], *za[3];
+    fvec(dumac); fvec(stoch); fvec(gradpi);
+    double *rfo[3], *rfn[3], *mo[3], *mt[3], *ad[3], *df[3], *rv[3], *du[3], *sto[3], *gpi[3];
     ptrs(rho_fc_old, rfo); ptrs(rho_fc_new, rfn); ptrs(mold, mo); ptrs(mtemp, mt); ptrs(adv, ad); ptrs(diff, df);
-    ptrs(rhs_v, rv); ptrs(dumac, du); ptrs(stoch, sto); ptrs(gradpi, gpi); ptrs(zero_a, za);
-    Vec rho_old(rho, rho + nc), rho_update(nc), rhs_p(nc), dpi(nc);
-    Vec eta_h(nc), kappa_h(nc);
+    ptrs(rhs_v, rv); ptrs(dumac, du); ptrs(stoch, sto); ptrs(gradpi, gpi);
+    std::vector<Vec> rho_old(ns), rho_update(ns, Vec(nc)), sfc(ns * dim, Vec(nc));
+    for (int s = 0; s < ns; s++) rho_old[s].assign(rho[s], rho[s] + nc);
+    Vec rhotot(nc), rhs_p(nc), dpi(nc), eta_h(nc), kappa_h(nc);
     std::vector<Vec> eta_ed_h(nE, Vec(nc));
     for (long f = 0; f < nc; f++) { eta_h[f] = eta[f] * 0.5; kappa_h[f] = kappa[f] * 0.5; }
     for (int e = 0; e < nE; e++)
         for (long f = 0; f < nc; f++) eta_ed_h[e][f] = eta_ed[e][f] * 0.5;
     const double* eh_ed[3] = {eta_ed_h[0].data(), nE == 3 ? eta_ed_h[1].data() : nullptr,
                               nE == 3 ? eta_ed_h[2].data() : nullptr};
-    const double* zap[3] = {za[0], za[1], dim == 3 ? za[2] : nullptr};
     const double* um[3] = {umac[0], umac[1], dim == 3 ? umac[2] : nullptr};
     const double w1[1] = {1.0};
-    // diffusive_m_fluxdiv (diffusive_m_fluxdiv.f90:25-...): -(applyop with alpha=0)
     auto diff_m = [&](double* const out[], const double* const u[]) {
         SLevel L;
         L.g = g;
@@ -1249,14 +1595,49 @@ int or_advance_inertial(int dim, const int n[3], double dx, int visc_type, const
         for (int c = 0; c < dim; c++)
             for (long f = 0; f < nc; f++) out[c][f] = L.Lphi[c][f] * -1.0;
     };
-    (void)one;
-    int st = 0;
+    auto sum_species = [&](double* const* r, double* out) {
+        for (long f = 0; f < nc; f++) {
+            double v = 0.0;
+            for (int s = 0; s < ns; s++) v = v + r[s][f];
+            out[f] = v;
+        }
+    };
+    auto species_fc = [&](double* const* r) {
+        for (int s = 0; s < ns; s++) {
+            double* o[3] = {sfc[s * dim].data(), sfc[s * dim + 1].data(), dim == 3 ? sfc[s * dim + 2].data() : nullptr};
+            avg_face(g, r[s], o);
+        }
+    };
+    // -S = sum_i -F_i/rhobar_i (advance_timestep_inertial.f90:420-430)
+    auto rhs_p_from_fluxes = [&]() {
+        std::fill(rhs_p.begin(), rhs_p.end(), 0.0);
+        if (!mix) return;
+        for (int s = 0; s < ns; s++)
+            for (long f = 0; f < nc; f++) rhs_p[f] = rhs_p[f] + (-1.0 / mix->rhobar[s]) * fluxdiv[s][f];
+    };
+    auto mass_fluxes = [&](const double* const* Wm) -> int {
+        if (!mix) return 0;
+        const double* cr[FHD_MAX_SPECIES];
+        for (int s = 0; s < ns; s++) cr[s] = rho[s];
+        return mass_fluxdiv_impl(g, *mix, sp, cr, dt, w1, 1, Wm, fluxdiv, nullptr);
+    };
+    int st = 0, rc;
     double norm_pre_rhs = 0.0;
-    // Step 2: predictor Euler step for rho (centred advection)
-    avg_face(g, rho_old.data(), rfo);
-    adv_s(g, um, rfo, rho_update.data(), false);
-    for (long f = 0; f < nc; f++) rho[f] = rho_old[f] + dt * rho_update[f];
-    avg_face(g, rho, rfn);
+    // Step 2: predictor Euler step for the densities
+    double* ro[FHD_MAX_SPECIES];
+    for (int s = 0; s < ns; s++) ro[s] = rho_old[s].data();
+    sum_species(ro, rhotot.data());
+    avg_face(g, rhotot.data(), rfo);
+    species_fc(ro);
+    for (int s = 0; s < ns; s++) {
+        if (mix) std::copy(fluxdiv[s], fluxdiv[s] + nc, rho_update[s].begin());
+        const double* sp3[3] = {sfc[s * dim].data(), sfc[s * dim + 1].data(), dim == 3 ? sfc[s * dim + 2].data() : nullptr};
+        adv_s(g, um, sp3, rho_update[s].data(), mix != nullptr);
+        for (long f = 0; f < nc; f++) rho[s][f] = rho_old[s][f] + dt * rho_update[s][f];
+    }
+    sum_species(rho, rhotot.data());
+    avg_face(g, rhotot.data(), rfn);
+    species_fc(rho);
     // Steps 3-4: predictor Crank-Nicolson
     for (int c = 0; c < dim; c++)
         for (long f = 0; f < nc; f++) mold[c][f] = rho_fc_old[c][f] * umac[c][f];
@@ -1279,7 +1660,8 @@ int or_advance_inertial(int dim, const int n[3], double dx, int visc_type, const
         for (int c = 0; c < dim; c++)
             for (long f = 0; f < nc; f++) rhs_v[c][f] = rhs_v[c][f] + stoch[c][f];
     }
-    std::fill(rhs_p.begin(), rhs_p.end(), 0.0);
+    if ((rc = mass_fluxes(W_mass))) return rc;
+    rhs_p_from_fluxes();
     for (int c = 0; c < dim; c++)
         for (long f = 0; f < nc; f++) mtemp[c][f] = rho_fc_new[c][f] * umac[c][f];
     for (int c = 0; c < dim; c++)
@@ -1287,6 +1669,10 @@ int or_advance_inertial(int dim, const int n[3], double dx, int visc_type, const
     diff_m(mt, um);
     for (int c = 0; c < dim; c++)
         for (long f = 0; f < nc; f++) rhs_v[c][f] = rhs_v[c][f] + 0.5 * mtemp[c][f];
+    for (int s = 0; s < ns; s++) {
+        if (mix) std::copy(fluxdiv[s], fluxdiv[s] + nc, rho_update[s].begin());
+        else std::fill(rho_update[s].begin(), rho_update[s].end(), 0.0);
+    }
     c_div(g, um, rhs_p.data(), true);
     for (int c = 0; c < dim; c++) std::fill(dumac[c].begin(), dumac[c].end(), 0.0);
     std::fill(dpi.begin(), dpi.end(), 0.0);
@@ -1306,13 +1692,17 @@ int or_advance_inertial(int dim, const int n[3], double dx, int visc_type, const
     for (int c = 0; c < dim; c++)
         for (long f = 0; f < nc; f++) mtemp[c][f] = rho_fc_new[c][f] * umac[c][f];
     // Step 5: trapezoidal scalar corrector
-    adv_s(g, um, rfn, rho_update.data(), false);
-    for (long f = 0; f < nc; f++) {
-        double v = rho[f] + rho_old[f];
-        v = v + dt * rho_update[f];
-        rho[f] = v * 0.5;
+    for (int s = 0; s < ns; s++) {
+        const double* sp3[3] = {sfc[s * dim].data(), sfc[s * dim + 1].data(), dim == 3 ? sfc[s * dim + 2].data() : nullptr};
+        adv_s(g, um, sp3, rho_update[s].data(), true);
+        for (long f = 0; f < nc; f++) {
+            double v = rho[s][f] + rho_old[s][f];
+            v = v + dt * rho_update[s][f];
+            rho[s][f] = v * 0.5;
+        }
     }
-    avg_face(g, rho, rfn);
+    sum_species(rho, rhotot.data());
+    avg_face(g, rhotot.data(), rfn);
     // Steps 6-7: corrector Crank-Nicolson
     for (int c = 0; c < dim; c++)
         for (long f = 0; f < nc; f++) rhs_v[c][f] = (1.0 / dt) * mold[c][f];
@@ -1332,7 +1722,8 @@ int or_advance_inertial(int dim, const int n[3], double dx, int visc_type, const
         for (int c = 0; c < dim; c++)
             for (long f = 0; f < nc; f++) rhs_v[c][f] = rhs_v[c][f] + 0.5 * stoch[c][f];
     }
-    std::fill(rhs_p.begin(), rhs_p.end(), 0.0);
+    if ((rc = mass_fluxes(W_mass ? W_mass + dim * ns : nullptr))) return rc;
+    rhs_p_from_fluxes();
     for (int c = 0; c < dim; c++)
         for (long f = 0; f < nc; f++) mtemp[c][f] = rho_fc_new[c][f] * umac[c][f];
     for (int c = 0; c < dim; c++)
@@ -1355,6 +1746,59 @@ int or_advance_inertial(int dim, const int n[3], double dx, int visc_type, const
         for (long f = 0; f < nc; f++) umac[c][f] = umac[c][f] + dumac[c][f];
     for (long f = 0; f < nc; f++) pi[f] = pi[f] + dpi[f];
     return st;
+}
+}  // namespace
+
+extern "C" {
+
+int or_advance_inertial(int dim, const int n[3], double dx, int visc_type, const fhd_gmres_params* p_in,
+                        const fhd_stoch_params* sp, double dt, double* const umac[], double* rho, double* pi,
+                        const double* eta, const double* const eta_ed[], const double* kappa,
+                        const double* temperature, const double* const temperature_ed[],
+                        const double* const W_cc[], const double* const W_ed[], fhd_solve_stats* stats2) {
+    Geo g(dim, n, dx);
+    double* r[1] = {rho};
+    return step_impl(g, visc_type, p_in, sp, nullptr, dt, umac, r, pi, nullptr, eta, eta_ed, kappa, temperature,
+                     temperature_ed, W_cc, W_ed, nullptr, stats2);
+}
+
+int or_advance_inertial_ms(int dim, const int n[3], double dx, int visc_type, const fhd_gmres_params* p_in,
+                           const fhd_stoch_params* sp, const fhd_mixture_params* mp, double dt,
+                           double* const umac[], double* const rho[], double* pi, double* const fluxdiv[],
+                           const double* eta, const double* const eta_ed[], const double* kappa,
+                           const double* temperature, const double* const temperature_ed[],
+                           const double* const W_cc[], const double* const W_ed[], const double* const W_mass[],
+                           fhd_solve_stats* stats2) {
+    Geo g(dim, n, dx);
+    Mix m = make_mix(mp);
+    return step_impl(g, visc_type, p_in, sp, &m, dt, umac, rho, pi, fluxdiv, eta, eta_ed, kappa, temperature,
+                     temperature_ed, W_cc, W_ed, W_mass, stats2);
+}
+
+int or_mass_fluxdiv(int dim, const int n[3], double dx, const fhd_stoch_params* sp, const fhd_mixture_params* mp,
+                    const double* const rho[], double dt, const double* weights, int n_rngs,
+                    const double* const W_fc[], double* const fluxdiv[], double* const flux[]) {
+    Geo g(dim, n, dx);
+    Mix m = make_mix(mp);
+    return mass_fluxdiv_impl(g, m, sp, rho, dt, weights, n_rngs, W_fc, fluxdiv, flux);
+}
+
+// chi and the Cholesky factor of the Onsager matrix at one state (test hook)
+int or_mixture_local(const fhd_mixture_params* mp, double k_B, const double* rho, double* chi_out,
+                     double* sqrtL_out) {
+    Mix m = make_mix(mp);
+    double rt = 0.0;
+    for (int i = 0; i < m.ns; i++) rt = rt + rho[i];
+    double x[FHD_MAX_SPECIES], mt, chi[FHD_MAX_SPECIES][FHD_MAX_SPECIES], L[FHD_MAX_SPECIES][FHD_MAX_SPECIES];
+    molconc(m.ns, m.molmass, rho, rt, x, &mt);
+    chi_of(m, rho, rt, x, chi);
+    if (!sqrtL_local(m, rho, k_B, L)) return FHD_ERR_UNSUPPORTED;
+    for (int i = 0; i < m.ns; i++)
+        for (int j = 0; j < m.ns; j++) {
+            chi_out[i * m.ns + j] = chi[i][j];
+            sqrtL_out[i * m.ns + j] = L[i][j];
+        }
+    return 0;
 }
 
 // ---------------------------------------------------------------------

@@ -111,6 +111,36 @@ int or_advance_inertial(int dim, const int n[3], double dx, int visc_type,
                         const double* const W_cc[], const double* const W_ed[],
                         fhd_solve_stats* stats2);
 
+/* The inertial step for ns species (advance_timestep_inertial.f90 with
+ * compute_mass_fluxdiv, ideal isothermal mixture).  rho[ns] and
+ * fluxdiv[ns] (F^n in, F^{n+1} out) advanced in place; W_mass holds
+ * 2*dim*ns face arrays: the previous corrector's fields (reused by this
+ * predictor) then this corrector's new fields. */
+int or_advance_inertial_ms(int dim, const int n[3], double dx, int visc_type,
+                           const fhd_gmres_params* p, const fhd_stoch_params* sp,
+                           const fhd_mixture_params* mp, double dt,
+                           double* const umac[], double* const rho[], double* pi,
+                           double* const fluxdiv[], const double* eta,
+                           const double* const eta_ed[], const double* kappa,
+                           const double* temperature,
+                           const double* const temperature_ed[],
+                           const double* const W_cc[], const double* const W_ed[],
+                           const double* const W_mass[], fhd_solve_stats* stats2);
+
+/* compute_mass_fluxdiv (compute_mass_fluxdiv.f90:29-183): divergence of the
+ * corrected diffusive + stochastic mass flux; W_fc[(r*dim+d)*ns+i] is the
+ * random field of rng r on faces of direction d for species i; flux
+ * (nullable) receives the dim*ns face fluxes. */
+int or_mass_fluxdiv(int dim, const int n[3], double dx, const fhd_stoch_params* sp,
+                    const fhd_mixture_params* mp, const double* const rho[],
+                    double dt, const double* weights, int n_rngs,
+                    const double* const W_fc[], double* const fluxdiv[],
+                    double* const flux[]);
+
+/* chi (Dbar2chi_iterative) and chol(L) at one state rho[ns] (row-major) */
+int or_mixture_local(const fhd_mixture_params* mp, double k_B, const double* rho,
+                     double* chi, double* sqrtL);
+
 /* Discretisation-accuracy harness of exec/stokes_preconditioner
  * (main_driver.f90:354-387, test_type=0): on [0,1]^dim with n cells per
  * direction returns max|f - A x_exact| per velocity component (err[0..dim-1])
