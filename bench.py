@@ -374,26 +374,46 @@ def main():
             # random fields from pinned memory, the step, and the read-back
             # of its solver diagnostics
             h2d = sum(w.numel() * 8 for part in host_sets[0] for w in part)
+            # three staging sets: step i computes on set i%3 (and reads the
+            # previous step's mass noise from set (i-1)%3) while a copy
+            # stream uploads step i+1's fields into set (i+1)%3, which the
+            # step before last finished with
+            NS = 3
             stage = [tuple([torch.empty(nc, dtype=torch.float64, device=dev) for _ in part] for part in host_sets[0])
-                     for _ in range(2)]
+                     for _ in range(NS)]
             # the set the first timed step treats as the previous step's
             # fields is staged before the timed region
-            for part_d, part_h in zip(stage[1], host_sets[-1]):
+            for part_d, part_h in zip(stage[NS - 1], host_sets[-1]):
                 for d_, h_ in zip(part_d, part_h):
                     d_.copy_(h_)
             torch.cuda.synchronize()
             barrier(ws)
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            with torch.cuda.stream(stream):
-                for i in range(args.steps):
-                    # this step's new fields go into one staging set; the
-                    # previous step's set stays resident for the predictor
-                    tgt = stage[i % 2]
-                    for part_d, part_h in zip(tgt, host_sets[i % len(host_sets)]):
+            cs = torch.cuda.Stream(device=dev)
+            copied = [torch.cuda.Event() for _ in range(args.steps)]
+            stepped = [torch.cuda.Event() for _ in range(args.steps)]
+
+            def upload(i):
+                with torch.cuda.stream(cs):
+                    if i >= 2:
+                        cs.wait_event(stepped[i - 2])
+                    for part_d, part_h in zip(stage[i % NS], host_sets[i % len(host_sets)]):
                         for d_, h_ in zip(part_d, part_h):
                             d_.copy_(h_, non_blocking=True)
-                    st, stats = case.step(tgt[0], tgt[1], stage[(i - 1) % 2][2], tgt[2])
+                    copied[i].record(cs)
+
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            cs.wait_stream(stream)
+            upload(0)
+            with torch.cuda.stream(stream):
+                for i in range(args.steps):
+                    if i + 1 < args.steps:
+                        upload(i + 1)
+                    stream.wait_event(copied[i])
+                    tgt = stage[i % NS]
+                    st, stats = case.step(tgt[0], tgt[1], stage[(i - 1) % NS][2], tgt[2])
+                    stepped[i].record(stream)
+            stream.wait_stream(cs)
             e1.record(stream)
             torch.cuda.synchronize()
             e2e_ms = allmax(ws, e0.elapsed_time(e1), torch, dev)

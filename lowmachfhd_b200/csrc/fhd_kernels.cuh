@@ -65,15 +65,22 @@ struct Off {
 // diagonal coefficient: the stencils of stag_applyop_2d/_3d
 // (stag_applyop.f90:212-1075) and the 'fac' of stag_mg_update
 // (stag_mg_solver.f90:1764-2458).
-template <typename T, int DIM, int VISC, int C>
-__device__ __forceinline__ T stag_lface(const StagOp<T>& A, const T* const* phi, const Cell& P, T& diag) {
+//
+// The velocity values come through two accessors, own(dx,dy,dz) for
+// component C and oth(d,dx,dy,dz) for component d != C, both relative to P,
+// and alpha of the face through alp(); the other coefficients are read from
+// global memory.  Every smoother, residual and
+// operator kernel evaluates this one expression, so a value computed from
+// shared-memory planes equals the one computed from global memory bit for
+// bit.
+template <typename T, int DIM, int VISC, int C, class Own, class Oth, class Alp>
+__device__ __forceinline__ T stag_lface_acc(const StagOp<T>& A, const Cell& P, Own own, Oth oth, Alp alp,
+                                            T& diag) {
     constexpr int ex = (C == 0), ey = (C == 1), ez = (C == 2);
     const i64 f = P.id(0, 0, 0);
-    const i64 fpc = P.id(ex, ey, ez);
     const i64 fmc = P.id(-ex, -ey, -ez);
-    const T* pc = phi[C];
-    const T ph = ld(pc, f);
-    const T a = A.alpha_scale * ld(A.alpha[C], f);
+    const T ph = own(0, 0, 0);
+    const T a = A.alpha_scale * alp();
     const T q = A.q;
     if constexpr (VISC < 0) {
         const T bp = ld(A.beta, f), bm = ld(A.beta, fmc);
@@ -87,7 +94,7 @@ __device__ __forceinline__ T stag_lface(const StagOp<T>& A, const T* const* phi,
             km = T(4.0 / 3.0) * bm + ld(A.gamma, fmc);
         }
         T s = kp + km;
-        T nb = ld(pc, fpc) * kp + ld(pc, fmc) * km;
+        T nb = own(ex, ey, ez) * kp + own(-ex, -ey, -ez) * km;
         T cross = T(0);
         T tp = T(0), tm = T(0);
         if constexpr (VISC == -3) {
@@ -99,49 +106,53 @@ __device__ __forceinline__ T stag_lface(const StagOp<T>& A, const T* const* phi,
             if (d == C) continue;
             const int dx_ = (d == 0), dy_ = (d == 1), dz_ = (d == 2);
             const i64 fpd = P.id(dx_, dy_, dz_);
-            const i64 fmd = P.id(-dx_, -dy_, -dz_);
             const T* E = A.bed[edge_of<DIM>(C, d)];
             const T elo = ld(E, f), ehi = ld(E, fpd);
             s += elo + ehi;
-            nb += ld(pc, fpd) * ehi + ld(pc, fmd) * elo;
+            nb += own(dx_, dy_, dz_) * ehi + own(-dx_, -dy_, -dz_) * elo;
             if constexpr (VISC != -1) {
-                const i64 fmcpd = P.id(dx_ - ex, dy_ - ey, dz_ - ez);
-                const T* pd = phi[d];
-                cross += ld(pd, fpd) * (ehi + tp) - ld(pd, f) * (elo + tp) - ld(pd, fmcpd) * (ehi + tm) +
-                         ld(pd, fmc) * (elo + tm);
+                cross += oth(d, dx_, dy_, dz_) * (ehi + tp) - oth(d, 0, 0, 0) * (elo + tp) -
+                         oth(d, dx_ - ex, dy_ - ey, dz_ - ez) * (ehi + tm) + oth(d, -ex, -ey, -ez) * (elo + tm);
             }
         }
         diag = a + s * q;
         return ph * diag - (nb + cross) * q;
     } else {
         const T b = ld(A.beta, 0);
-        const T own = ld(pc, fpc) + ld(pc, fmc);
-        T oth = T(0), cross = T(0);
+        const T own_ = own(ex, ey, ez) + own(-ex, -ey, -ez);
+        T oth_ = T(0), cross = T(0);
 #pragma unroll
         for (int d = 0; d < DIM; d++) {
             if (d == C) continue;
             const int dx_ = (d == 0), dy_ = (d == 1), dz_ = (d == 2);
-            const i64 fpd = P.id(dx_, dy_, dz_);
-            const i64 fmd = P.id(-dx_, -dy_, -dz_);
-            oth += ld(pc, fpd) + ld(pc, fmd);
+            oth_ += own(dx_, dy_, dz_) + own(-dx_, -dy_, -dz_);
             if constexpr (VISC != 1) {
-                const i64 fmcpd = P.id(dx_ - ex, dy_ - ey, dz_ - ez);
-                const T* pd = phi[d];
-                cross += ld(pd, fpd) - ld(pd, f) - ld(pd, fmcpd) + ld(pd, fmc);
+                cross += oth(d, dx_, dy_, dz_) - oth(d, 0, 0, 0) - oth(d, dx_ - ex, dy_ - ey, dz_ - ez) +
+                         oth(d, -ex, -ey, -ez);
             }
         }
         if constexpr (VISC == 1) {
             diag = a + T(2 * DIM) * b * q;
-            return ph * diag - (own + oth) * b * q;
+            return ph * diag - (own_ + oth_) * b * q;
         } else if constexpr (VISC == 2) {
             diag = a + T(2 * DIM + 2) * b * q;
-            return ph * diag - (T(2) * own + oth + cross) * b * q;
+            return ph * diag - (T(2) * own_ + oth_ + cross) * b * q;
         } else {
             const T cg = ld(A.gamma, 0);
             diag = a + ((T(8.0 / 3.0) + T(2 * (DIM - 1))) * b + T(2) * cg) * q;
-            return ph * diag - (own * (T(4.0 / 3.0) * b + cg) + oth * b + cross * (T(1.0 / 3.0) * b + cg)) * q;
+            return ph * diag - (own_ * (T(4.0 / 3.0) * b + cg) + oth_ * b + cross * (T(1.0 / 3.0) * b + cg)) * q;
         }
     }
+}
+
+// the operator on global-memory velocity arrays
+template <typename T, int DIM, int VISC, int C>
+__device__ __forceinline__ T stag_lface(const StagOp<T>& A, const T* const* phi, const Cell& P, T& diag) {
+    const T* pc = phi[C];
+    return stag_lface_acc<T, DIM, VISC, C>(
+        A, P, [&](int a, int b, int c) { return ld(pc, P.id(a, b, c)); },
+        [&](int d, int a, int b, int c) { return ld(phi[d], P.id(a, b, c)); },
+        [&]() { return ld(A.alpha[C], P.id(0, 0, 0)); }, diag);
 }
 
 template <typename T, int DIM, int VISC>
@@ -383,22 +394,29 @@ struct CCOp {
     T q;            // 1/dx^2 of the level
 };
 
-template <typename T, int DIM>
-__device__ __forceinline__ T cc_lap(const CCOp<T>& A, const T* phi, const Cell& P, T& diag) {
+// D a G phi at cell P and its diagonal; phi through the accessor
+// ph(dx,dy,dz) relative to P (global memory or shared-memory planes, one
+// expression for both)
+template <typename T, int DIM, class Acc>
+__device__ __forceinline__ T cc_lap_acc(const CCOp<T>& A, const Cell& P, Acc ph, T& diag) {
     const i64 f = P.id(0, 0, 0);
-    const T pc = ld(phi, f);
+    const T pc = ph(0, 0, 0);
     T s = T(0), dg = T(0);
 #pragma unroll
     for (int d = 0; d < DIM; d++) {
         const int dx_ = (d == 0), dy_ = (d == 1), dz_ = (d == 2);
         const i64 fp = P.id(dx_, dy_, dz_);
-        const i64 fm = P.id(-dx_, -dy_, -dz_);
         const T ahi = ld(A.a[d], fp), alo = ld(A.a[d], f);
-        s += ahi * (ld(phi, fp) - pc) - alo * (pc - ld(phi, fm));
+        s += ahi * (ph(dx_, dy_, dz_) - pc) - alo * (pc - ph(-dx_, -dy_, -dz_));
         dg += ahi + alo;
     }
     diag = -dg * A.q;
     return s * A.q;
+}
+
+template <typename T, int DIM>
+__device__ __forceinline__ T cc_lap(const CCOp<T>& A, const T* phi, const Cell& P, T& diag) {
+    return cc_lap_acc<T, DIM>(A, P, [&](int a, int b, int c) { return ld(phi, P.id(a, b, c)); }, diag);
 }
 
 // red-black Gauss-Seidel, one colour, fused; thread per cell of the colour

@@ -8,6 +8,7 @@
 #include <cstring>
 #include <mutex>
 #include <type_traits>
+#include <map>
 
 #include "fhd_solver.cuh"
 
@@ -308,10 +309,112 @@ static int stag_smooth(fhd_ctx* ctx, StagLevel<T>& L, int color) {
     return rc;
 }
 
+// algorithmic bytes of one fused smooth launch (all colours of the
+// components it covers): src, rhs, alpha read and dst written per component,
+// plus the variable viscosities and, for coupled operators, the other
+// components
+template <typename T>
+static double rb_smooth_bytes(fhd_ctx* ctx, const StagLevel<T>& L) {
+    const double nc = (double)L.g.nc, s = (double)sizeof(T);
+    const int v = ctx->visc;
+    double words = 4.0 * nc;
+    if (v < 0) words += nc + 2.0 * nc;
+    if (v == -3) words += nc;
+    if (v != 1 && v != -1) words += 2.0 * nc;
+    return words * s * ((v == 1 || v == -1) ? 3.0 : 1.0);
+}
+
+// dynamic shared memory above the 48 KB default: raise each kernel's limit
+// (keyed by device and kernel address) to the largest size launched so far
+template <class K>
+static int rb_allow_smem(K kernel, size_t bytes) {
+    static std::mutex mu;
+    static std::map<std::pair<int, const void*>, size_t> done;
+    if (bytes <= 48 * 1024) return 0;
+    int dev = 0;
+    FHD_CUDA_TRY(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lk(mu);
+    size_t& d = done[std::make_pair(dev, (const void*)kernel)];
+    if (bytes <= d) return 0;
+    FHD_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    d = bytes;
+    return 0;
+}
+
+// one full smooth a -> b of every component (3D, even extents)
+template <typename T>
+static int stag_rb_smooth(fhd_ctx* ctx, StagLevel<T>& L, const RBGeom& G, T* const a[3], T* const b[3]) {
+    const StagOp<T> A = L.op();
+    const T omega = (T)ctx->p.stag_mg_omega;
+    const size_t smem = rb_smem<T>(G, 2);
+    cudaStream_t st = ctx->stream;
+    const dim3 blk(32, G.TY + 1);
+    int rc = 0;
+    RBArgs<T> R;
+    for (int c = 0; c < 3; c++) {
+        R.src[c] = a[c];
+        R.dst[c] = b[c];
+        R.rhs[c] = L.rhs[c];
+        R.oth[c] = nullptr;
+    }
+    const bool timed = ctx->prof && L.g.nc == ctx->g0.nc;
+    with_visc3(ctx->visc, [&](auto V) {
+        constexpr int VISC = decltype(V)::value;
+        if constexpr (VISC == 1 || VISC == -1) {
+            if (timed) {
+                cudaEventRecord(prof_event(ctx), st);
+                ctx->prof_bytes += rb_smooth_bytes(ctx, L);
+                ctx->prof_launches++;
+            }
+            rc |= rb_allow_smem(k_stag_rb<T, VISC, -1>, smem);
+            k_stag_rb<T, VISC, -1><<<dim3(G.tiles_x * G.tiles_y, G.chunks, 3), blk, smem, st>>>(L.g, G, A, R, omega);
+            rc |= post(ctx);
+            if (timed) cudaEventRecord(prof_event(ctx), st);
+        } else {
+            const dim3 grd(G.tiles_x * G.tiles_y, G.chunks, 1);
+            for (int c = 0; c < 3; c++) {
+                // components before c already hold this smooth's values
+                for (int d = 0; d < 3; d++) R.oth[d] = d < c ? b[d] : a[d];
+                if (timed) {
+                    cudaEventRecord(prof_event(ctx), st);
+                    ctx->prof_bytes += rb_smooth_bytes(ctx, L);
+                    ctx->prof_launches++;
+                }
+                rc |= rb_allow_smem(k_stag_rb<T, VISC, 0>, smem);
+                rc |= rb_allow_smem(k_stag_rb<T, VISC, 1>, smem);
+                rc |= rb_allow_smem(k_stag_rb<T, VISC, 2>, smem);
+                if (c == 0) k_stag_rb<T, VISC, 0><<<grd, blk, smem, st>>>(L.g, G, A, R, omega);
+                else if (c == 1) k_stag_rb<T, VISC, 1><<<grd, blk, smem, st>>>(L.g, G, A, R, omega);
+                else k_stag_rb<T, VISC, 2><<<grd, blk, smem, st>>>(L.g, G, A, R, omega);
+                rc |= post(ctx);
+                if (timed) cudaEventRecord(prof_event(ctx), st);
+            }
+        }
+    });
+    return rc;
+}
+
 template <typename T>
 static int stag_smooths(fhd_ctx* ctx, StagLevel<T>& L, int count) {
     const int dim = ctx->dim;
-    for (int m = 0; m < count; m++) {
+    int m0 = 0;
+    RBGeom G;
+    bool aligned = true;
+    for (int c = 0; c < dim; c++)
+        aligned = aligned && rb_aligned(L.phi[c]) && rb_aligned(L.tmp[c]) && rb_aligned(L.rhs[c]) &&
+                  rb_aligned(L.alpha[c]);
+    if (ctx->p.stag_mg_smoother != 0 && count >= 2 && aligned && rb_use(L.g) && rb_geom(L.g, 3, (int)sizeof(T), G)) {
+        // pairs of fused smooths phi -> tmp -> phi
+        T* a[3] = {L.phi[0], L.phi[1], L.phi[2]};
+        T* b[3] = {L.tmp[0], L.tmp[1], L.tmp[2]};
+        for (; m0 + 2 <= count; m0 += 2) {
+            int rc = stag_rb_smooth(ctx, L, G, a, b);
+            if (rc) return rc;
+            rc = stag_rb_smooth(ctx, L, G, b, a);
+            if (rc) return rc;
+        }
+    }
+    for (int m = m0; m < count; m++) {
         if (ctx->p.stag_mg_smoother == 0) {
             int rc = stag_smooth(ctx, L, 0);
             if (rc) return rc;
@@ -488,19 +591,38 @@ static int cc_smooth(fhd_ctx* ctx, CCLevel<T>& C) {
     return 0;
 }
 
+// count red-black smooths: fused pairs phi -> tmp -> phi where the level
+// allows, single colour-pair smooths otherwise
+template <typename T>
+static int cc_smooths(fhd_ctx* ctx, CCLevel<T>& C, int count) {
+    int m0 = 0;
+    RBGeom G;
+    const bool aligned = rb_aligned(C.phi) && rb_aligned(C.tmp) && rb_aligned(C.rhs);
+    if (count >= 2 && aligned && rb_use(C.g) && rb_geom(C.g, 1, (int)sizeof(T), G)) {
+        const size_t smem = rb_smem<T>(G, 1);
+        if (int rc = rb_allow_smem(k_cc_rb<T>, smem)) return rc;
+        const dim3 grd(G.tiles_x * G.tiles_y, G.chunks, 1), blk(32, G.TY + 1);
+        for (; m0 + 2 <= count; m0 += 2) {
+            k_cc_rb<T><<<grd, blk, smem, ctx->stream>>>(C.g, G, C.op(), C.phi, C.tmp, C.rhs);
+            FHD_POST(ctx);
+            k_cc_rb<T><<<grd, blk, smem, ctx->stream>>>(C.g, G, C.op(), C.tmp, C.phi, C.rhs);
+            FHD_POST(ctx);
+        }
+    }
+    for (int m = m0; m < count; m++) {
+        int rc = cc_smooth(ctx, C);
+        if (rc) return rc;
+    }
+    return 0;
+}
+
 template <typename T>
 static int cc_vcycle(fhd_ctx* ctx, Multigrid<T>& M, int l) {
     const int nl = (int)M.c.size();
     CCLevel<T>& C = M.c[l];
-    if (l == nl - 1) {
-        for (int m = 0; m < ctx->p.mg_nsmooths_bottom; m++) {
-            int rc = cc_smooth(ctx, C);
-            if (rc) return rc;
-        }
-        return 0;
-    }
-    for (int m = 0; m < ctx->p.mg_nsmooths_down; m++) {
-        int rc = cc_smooth(ctx, C);
+    if (l == nl - 1) return cc_smooths(ctx, C, ctx->p.mg_nsmooths_bottom);
+    {
+        int rc = cc_smooths(ctx, C, ctx->p.mg_nsmooths_down);
         if (rc) return rc;
     }
     CCLevel<T>& D = M.c[l + 1];
@@ -521,11 +643,7 @@ static int cc_vcycle(fhd_ctx* ctx, Multigrid<T>& M, int l) {
         rc |= post(ctx);
     });
     if (rc) return rc;
-    for (int m = 0; m < ctx->p.mg_nsmooths_up; m++) {
-        rc = cc_smooth(ctx, C);
-        if (rc) return rc;
-    }
-    return 0;
+    return cc_smooths(ctx, C, ctx->p.mg_nsmooths_up);
 }
 
 // Phi = 0, then mg_max_vcycles V-cycles on M.c[0].rhs

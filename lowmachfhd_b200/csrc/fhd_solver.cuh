@@ -10,6 +10,7 @@
 
 #include "../../include/fhd_b200.h"
 #include "fhd_vec.cuh"
+#include "fhd_rb.cuh"
 
 namespace fhd {
 
@@ -81,6 +82,20 @@ inline void with_dim_visc(int dim, int visc, F&& f) {
         }
     }
 #undef FHD_V
+}
+
+// 3D only (the fused smoothers)
+template <class F>
+inline void with_visc3(int visc, F&& f) {
+    using std::integral_constant;
+    switch (visc) {
+        case -3: f(integral_constant<int, -3>()); break;
+        case -2: f(integral_constant<int, -2>()); break;
+        case -1: f(integral_constant<int, -1>()); break;
+        case 1: f(integral_constant<int, 1>()); break;
+        case 2: f(integral_constant<int, 2>()); break;
+        default: f(integral_constant<int, 3>()); break;
+    }
 }
 
 template <class F>

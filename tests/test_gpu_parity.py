@@ -66,6 +66,40 @@ def test_stag_mg_one_vcycle(cuda, dim, n, visc):
     assert P.rel_inf(host(phi), ref) < 1e-12
 
 
+# grids whose finest levels span several x-y tiles and z runs of the fused
+# red-black smoothers (64x16 tiles; 96 -> 48-wide, 40 -> 10-high tiles), with
+# uncoupled and coupled viscous operators, through one V-cycle and through
+# the preconditioner (which adds the pressure multigrid)
+TILED = [(1, [128, 32, 64]), (-1, [96, 40, 24]), (2, [64, 48, 32]), (-3, [96, 40, 24])]
+
+
+@pytest.mark.parametrize("visc,n", TILED)
+def test_stag_mg_tiled(cuda, visc, n):
+    dim = 3
+    pb = P.problem(dim, n, visc, dx=1.0, seed=8)
+    rhs, _ = P.random_stokes(dim, n, seed=9)
+    ref = O.stag_mg_solver(pb, O.default_params(), 0.7, rhs)
+    with L.StokesSolver(dim, n, 1.0, visc, params=L.default_params()) as s:
+        phi = zeros(pb.nc, dim, cuda)
+        s.stag_mg_solver(dev(pb.alpha_fc, cuda), dev(pb.beta, cuda), dev(pb.beta_ed, cuda), dev(pb.gamma, cuda),
+                         0.7, phi, dev(rhs, cuda))
+    assert P.rel_inf(host(phi), ref) < 1e-12
+
+
+@pytest.mark.parametrize("visc,n", TILED[:2])
+def test_apply_precon_tiled(cuda, visc, n):
+    dim = 3
+    pb = P.problem(dim, n, visc, dx=1.0, seed=10)
+    b_u, b_p = P.random_stokes(dim, n, seed=11, zero_mean_p=False)
+    ref_u, ref_p = O.apply_precon(pb, O.default_params(), 1.5, b_u, b_p)
+    with L.StokesSolver(dim, n, 1.0, visc, params=L.default_params()) as s:
+        x_u, x_p = zeros(pb.nc, dim, cuda), zeros(pb.nc, 1, cuda)[0]
+        s.apply_precon(dev(b_u, cuda), dev(b_p, cuda), x_u, x_p, dev(pb.alpha_fc, cuda), dev(pb.beta, cuda),
+                       dev(pb.beta_ed, cuda), dev(pb.gamma, cuda), 1.5)
+    assert P.rel_inf(host(x_u), ref_u) < 1e-11
+    assert P.rel_inf([host(x_p)], [ref_p]) < 1e-11
+
+
 @pytest.mark.parametrize("case", ["vcycles3", "jacobi", "odd24", "odd12x20", "minwidth4"])
 def test_stag_mg_options(cuda, case):
     dim, n, kw, visc = 2, [32, 32], {}, -1
