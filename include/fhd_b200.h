@@ -265,6 +265,26 @@ int fhd_dev_advance_inertial_multispecies(fhd_ctx* ctx, const fhd_stoch_params* 
                                           const double* const W_mass[],
                                           fhd_solve_stats* stats2);
 
+/* advance_timestep_overdamped (advance_timestep_overdamped.f90:135-734):
+ * the two-stage overdamped step (theta_alpha = 0) of a single fluid
+ * (mp = NULL, rho one array) or an ideal isothermal mixture (rho nspecies
+ * arrays), periodic box, centred advection, midpoint_stoch_mass_flux_type
+ * 1.  umac, rho, pi advanced in place.  The step draws two random stages
+ * once (n_rngs = 2, main_driver.f90:534-536): W_cc 2*dim cell arrays,
+ * W_ed 2*2*nE node/edge arrays (indexing as fhd_dev_stochastic_m_fluxdiv
+ * with n_rngs = 2), W_mass 2*dim*nspecies face arrays
+ * (W_mass[(r*dim+d)*nspecies+i]; NULL without a mixture).  The predictor
+ * weighs the stages (1, 0) over dt/2, the corrector (1/sqrt2, 1/sqrt2)
+ * over dt.  stats (nullable) receives the two solves' diagnostics. */
+int fhd_dev_advance_overdamped(fhd_ctx* ctx, const fhd_stoch_params* sp,
+                               const fhd_mixture_params* mp, double dt,
+                               double* const umac[], double* const rho[], double* pi,
+                               const double* eta, const double* const eta_ed[],
+                               const double* kappa, const double* temperature,
+                               const double* const temperature_ed[],
+                               const double* const W_cc[], const double* const W_ed[],
+                               const double* const W_mass[], fhd_solve_stats* stats2);
+
 /* Text of the last CUDA error seen by the calling thread. */
 const char* fhd_last_error(void);
 /* Bytes of device memory a context holds. */

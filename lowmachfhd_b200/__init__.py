@@ -192,6 +192,19 @@ class StokesSolver:
                                                         C.cast(w, _DP), len(weights), _dpp(W_fc),
                                                         _dpp(mass_fluxdiv)), "compute_mass_fluxdiv")
 
+    def advance_timestep_overdamped(self, sp: StochParams, mp, dt, umac, rho, pi, eta, eta_ed, kappa, temperature,
+                                    temperature_ed, W_cc, W_ed, W_mass=None):
+        """One overdamped step (advance_timestep_overdamped.f90:135-734) in
+        place on umac, rho (list of species arrays; one array and mp=None
+        for a single fluid) and pi.  W_cc/W_ed/W_mass hold the step's two
+        random stages.  Returns (status, [stats_pred, stats_corr])."""
+        st = (SolveStats * 2)()
+        status = check(lib().fhd_dev_advance_overdamped(
+            self._h, C.byref(sp), C.byref(mp) if mp is not None else None, float(dt), _dpp(umac), _dpp(rho),
+            _dptr(pi), _dptr(eta), _dpp(eta_ed), _dptr(kappa), _dptr(temperature), _dpp(temperature_ed),
+            _dpp(W_cc), _dpp(W_ed), _dpp(W_mass) if W_mass is not None else None, st), "advance_timestep_overdamped")
+        return status, [st[0].as_dict(), st[1].as_dict()]
+
     def advance_timestep_inertial_multispecies(self, sp: StochParams, mp: MixtureParams, dt, umac, rho, pi,
                                                mass_fluxdiv, eta, eta_ed, kappa, temperature, temperature_ed,
                                                W_cc, W_ed, W_mass):

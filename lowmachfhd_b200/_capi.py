@@ -141,6 +141,9 @@ _PROTOS = {
     "fhd_dev_advance_inertial_multispecies": (C.c_int, [_VP, C.POINTER(StochParams), C.POINTER(MixtureParams),
                                                         C.c_double, _PP, _PP, _DP, _PP, _DP, _PP, _DP, _DP, _PP,
                                                         _PP, _PP, _PP, C.POINTER(SolveStats)]),
+    "fhd_dev_advance_overdamped": (C.c_int, [_VP, C.POINTER(StochParams), C.POINTER(MixtureParams), C.c_double,
+                                             _PP, _PP, _DP, _DP, _PP, _DP, _DP, _PP, _PP, _PP, _PP,
+                                             C.POINTER(SolveStats)]),
     "fhd_gmres": (C.c_int, [_VP] + [C.POINTER(Multifab)] * 8 + [_DP, _DP, C.POINTER(SolveStats)]),
     "fhd_apply_precon": (C.c_int, [_VP] + [C.POINTER(Multifab)] * 8 + [C.c_double]),
     "fhd_apply_matrix": (C.c_int, [_VP] + [C.POINTER(Multifab)] * 8 + [C.c_double]),

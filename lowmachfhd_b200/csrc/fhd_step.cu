@@ -571,11 +571,167 @@ int advance_inertial_ms(fhd_ctx* ctx, const fhd_stoch_params* sp, const fhd_mixt
     return st1 > st2 ? st1 : st2;
 }
 
+// ---------------------------------------------------------------------
+// overdamped step (advance_timestep_overdamped.f90:135-734): periodic,
+// centred advection, no gravity or reactions, barodiffusion off,
+// midpoint_stoch_mass_flux_type = 1; theta_alpha = 0.  Two random stages:
+// W_cc[r*dim+c], W_ed[r*2*nE+...], W_mass[(r*dim+d)*ns+i], r = 0, 1.
+// ---------------------------------------------------------------------
+int advance_overdamped(fhd_ctx* ctx, const fhd_stoch_params* sp, const fhd_mixture_params* mp, double dt,
+                       double* const umac[], double* const rho[], double* pi, const double* eta,
+                       const double* const eta_ed[], const double* kappa, const double* temperature,
+                       const double* const temperature_ed[], const double* const W_cc[], const double* const W_ed[],
+                       const double* const W_mass[], fhd_solve_stats* stats2) {
+    int rc = step_alloc(ctx);
+    if (rc) return rc;
+    const int dim = ctx->dim;
+    const int ns = mp ? mp->nspecies : 1;
+    if (ns < 1 || ns > FHD_MAX_SPECIES) return FHD_ERR_BAD_ARG;
+    const Grid g = ctx->g0;
+    const i64 nc = g.nc;
+    const int nb = flat_blocks(nc);
+    cudaStream_t st = ctx->stream;
+    const double dxinv = 1.0 / ctx->dx;
+    SVec<double> u = svp(umac, dim);
+    SVec<double> rtf = sv(ctx, B_RFN), diff = sv(ctx, B_DIFF), rhs_v = sv(ctx, B_RHSV), du = sv(ctx, B_DU),
+                 gpi = sv(ctx, B_GPI);
+    double* rhotot = ctx->sb[B_RHOTOT];
+    double* rhs_p = ctx->sb[B_RHSP];
+    double* dpi = ctx->sb[B_DPI];
+    double* rho_old[FHD_MAX_SPECIES];
+    double* rupd[FHD_MAX_SPECIES];
+    for (int s = 0; s < ns; s++) {
+        rho_old[s] = ctx->sb[B_RHOOLD + s];
+        rupd[s] = ctx->sb[B_RUPD + s];
+    }
+    auto sfc = [&](int s) { return sv(ctx, B_SFC + s * dim); };
+    double** rtab = (double**)(ctx->dscal + 200);
+    auto sum_species = [&](double* const* r, double* out) -> int {
+        double* h[FHD_MAX_SPECIES];
+        for (int s = 0; s < ns; s++) h[s] = r[s];
+        FHD_CUDA_TRY(cudaMemcpyAsync(rtab, h, sizeof(double*) * ns, cudaMemcpyHostToDevice, st));
+        k_sum_species<<<nb, 256, 0, st>>>(nc, ns, rtab, out);
+        ctx->launches++;
+        FHD_CUDA_TRY(cudaPeekAtLastError());
+        FHD_CUDA_TRY(cudaStreamSynchronize(st));
+        return 0;
+    };
+    auto launch_dim = [&](auto&& fn) {
+        with_dim(dim, fn);
+        ctx->launches++;
+    };
+    // faces of rho_tot and of every species (lines 181-183 / 410-411)
+    auto faces = [&](double* const* r) -> int {
+        int r2 = sum_species(r, rhotot);
+        if (r2) return r2;
+        launch_dim([&](auto D) {
+            constexpr int DIM = decltype(D)::value;
+            k_avg_face<DIM><<<cell_grid(g), cell_block(), 0, st>>>(g, rhotot, rtf.c[0], rtf.c[1], rtf.c[2]);
+        });
+        for (int s = 0; s < ns; s++) {
+            SVec<double> o = sfc(s);
+            launch_dim([&](auto D) {
+                constexpr int DIM = decltype(D)::value;
+                k_avg_face<DIM><<<cell_grid(g), cell_block(), 0, st>>>(g, r[s], o.c[0], o.c[1], o.c[2]);
+            });
+        }
+        return 0;
+    };
+    // one half of the step over h with the stage weights: rhs, GMRES,
+    // u += du, pi += dpi, rho = rho_old + h*(F - div(rho_fc u))
+    auto stage = [&](const double* wts, double h, double* npr, fhd_solve_stats* sst) -> int {
+        int r2;
+        launch_dim([&](auto D) {
+            constexpr int DIM = decltype(D)::value;
+            k_grad<DIM><<<cell_grid(g), cell_block(), 0, st>>>(g, pi, gpi, dxinv);
+        });
+        if ((r2 = lin(ctx, rhs_v, 0, {{-1.0, cs(gpi)}}))) return r2;
+        if (sp->variance_coef_mom != 0.0 &&
+            (r2 = stoch_launch(ctx, sp, rhs_v.c, 1, eta, eta_ed, temperature, temperature_ed, h, wts, 2, W_cc, W_ed)))
+            return r2;
+        if (mp) {
+            const double* cr[FHD_MAX_SPECIES];
+            for (int s = 0; s < ns; s++) cr[s] = rho[s];
+            if ((r2 = mass_fluxdiv(ctx, mp, sp, cr, h, wts, 2, W_mass, rupd))) return r2;
+        } else {
+            FHD_CUDA_TRY(cudaMemsetAsync(rupd[0], 0, sizeof(double) * nc, st));
+        }
+        FHD_CUDA_TRY(cudaMemsetAsync(rhs_p, 0, sizeof(double) * nc, st));
+        if (mp)
+            for (int s = 0; s < ns; s++)
+                if ((r2 = lin_n(ctx, 1, one(rhs_p), 1, {{-1.0 / mp->rhobar[s], cs(one(rupd[s]))}}))) return r2;
+        if ((r2 = diff_m(ctx, diff, cs(u), eta, eta_ed, kappa))) return r2;
+        if ((r2 = lin(ctx, rhs_v, 1, {{1.0, cs(diff)}}))) return r2;
+        launch_dim([&](auto D) {
+            constexpr int DIM = decltype(D)::value;
+            k_div_inc<DIM><<<cell_grid(g), cell_block(), 0, st>>>(g, cs(u), rhs_p, dxinv);
+        });
+        for (int c = 0; c < dim; c++) FHD_CUDA_TRY(cudaMemsetAsync(du.c[c], 0, sizeof(double) * nc, st));
+        FHD_CUDA_TRY(cudaMemsetAsync(dpi, 0, sizeof(double) * nc, st));
+        FHD_CUDA_TRY(cudaPeekAtLastError());
+        const double* rtf_c[3] = {rtf.c[0], rtf.c[1], rtf.c[2]};
+        if ((r2 = prepare(ctx, rtf_c, eta, eta_ed, kappa, 0.0))) return r2;
+        CSVec<double> b;
+        SVec<double> x;
+        for (int c = 0; c < 4; c++) { b.c[c] = nullptr; x.c[c] = nullptr; }
+        for (int c = 0; c < dim; c++) { b.c[c] = rhs_v.c[c]; x.c[c] = du.c[c]; }
+        b.c[dim] = rhs_p;
+        x.c[dim] = dpi;
+        const int sg = gmres_dev(ctx, b, x, npr, sst);
+        if (sg < 0) return sg;
+        if ((r2 = lin(ctx, u, 1, {{1.0, cs(du)}}))) return r2;
+        if ((r2 = lin_n(ctx, 1, one(pi), 1, {{1.0, cs(one(dpi))}}))) return r2;
+        for (int s = 0; s < ns; s++) {
+            const SVec<double> f3 = sfc(s);
+            launch_dim([&](auto D) {
+                constexpr int DIM = decltype(D)::value;
+                k_adv_s_update<DIM><<<cell_grid(g), cell_block(), 0, st>>>(g, cs(u), cs(f3), rho_old[s], rho[s], h,
+                                                                          dxinv, 2, rupd[s]);
+            });
+        }
+        FHD_CUDA_TRY(cudaPeekAtLastError());
+        return sg;
+    };
+    for (int s = 0; s < ns; s++)
+        FHD_CUDA_TRY(cudaMemcpyAsync(rho_old[s], rho[s], sizeof(double) * nc, cudaMemcpyDeviceToDevice, st));
+    if ((rc = faces(rho_old))) return rc;
+    const double w_pred[2] = {1.0, 0.0};
+    const double w_corr[2] = {1.0 / std::sqrt(2.0), 1.0 / std::sqrt(2.0)};
+    const double abs_tol_in = ctx->p.gmres_abs_tol;
+    double norm_pre_rhs = 0.0;
+    const int st1 = stage(w_pred, 0.5 * dt, &norm_pre_rhs, stats2 ? &stats2[0] : nullptr);
+    if (st1 < 0) return st1;
+    // the corrector stops at the predictor's preconditioned rhs (line 338);
+    // the tolerance is restored after it (line 587)
+    ctx->p.gmres_abs_tol = fmax(abs_tol_in, norm_pre_rhs * ctx->p.gmres_rel_tol);
+    int st2 = faces(rho);
+    if (!st2) st2 = stage(w_corr, dt, nullptr, stats2 ? &stats2[1] : nullptr);
+    ctx->p.gmres_abs_tol = abs_tol_in;
+    if (st2 < 0) return st2;
+    if (mp && (rc = mass_flag_check(ctx))) return rc;
+    return st1 > st2 ? st1 : st2;
+}
+
 }  // namespace fhd
 
 using namespace fhd;
 
 extern "C" {
+
+int fhd_dev_advance_overdamped(fhd_ctx* ctx, const fhd_stoch_params* sp, const fhd_mixture_params* mp, double dt,
+                               double* const umac[], double* const rho[], double* pi, const double* eta,
+                               const double* const eta_ed[], const double* kappa, const double* temperature,
+                               const double* const temperature_ed[], const double* const W_cc[],
+                               const double* const W_ed[], const double* const W_mass[], fhd_solve_stats* stats2) {
+    if (!ctx || !sp || !umac || !rho || !pi || !eta || !eta_ed || !kappa || !temperature || !temperature_ed ||
+        !W_cc || !W_ed || (mp && !W_mass) || !(dt > 0.0))
+        return FHD_ERR_BAD_ARG;
+    int rc = advance_overdamped(ctx, sp, mp, dt, umac, rho, pi, eta, eta_ed, kappa, temperature, temperature_ed, W_cc,
+                                W_ed, W_mass, stats2);
+    if (rc < 0) return rc;
+    FHD_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    return rc;
+}
 
 int fhd_dev_stochastic_m_fluxdiv(fhd_ctx* ctx, const fhd_stoch_params* sp, double* const force[], int increment,
                                  const double* eta, const double* const eta_ed[], const double* temperature,

@@ -282,6 +282,23 @@ def mass_fluxdiv(dim, n, dx, sp, mp, rho, dt, weights, W_fc, want_flux=False):
     return (out, flux) if want_flux else out
 
 
+def advance_overdamped(dim, n, dx, visc_type, params, sp, mp, dt, umac, rho, pi, eta, eta_ed, kappa, temp,
+                       temp_ed, W_cc, W_ed, W_mass=None):
+    """advance_timestep_overdamped (advance_timestep_overdamped.f90:135-734).
+    rho: list of species arrays (one array and mp=None for a single fluid).
+    W_cc: 2*dim cell fields, W_ed: 2*2*nE node/edge fields, W_mass:
+    2*dim*ns face fields (two random stages)."""
+    umac = [u.copy() for u in umac]
+    rho = [r.copy() for r in rho]
+    pi = pi.copy()
+    st = (SolveStats * 2)()
+    rc = lib().or_advance_overdamped(dim, _n3(n), C.c_double(dx), visc_type, C.byref(params), C.byref(sp),
+                                     C.byref(mp) if mp is not None else None, C.c_double(dt), _pp(umac), _pp(rho),
+                                     _p(pi), _p(eta), _pp(eta_ed), _p(kappa), _p(temp), _pp(temp_ed), _pp(W_cc),
+                                     _pp(W_ed), _pp(W_mass) if W_mass is not None else None, st)
+    return rc, umac, rho, pi, st
+
+
 def advance_inertial_ms(dim, n, dx, visc_type, params, sp, mp, dt, umac, rho, pi, fluxdiv, eta, eta_ed, kappa,
                         temp, temp_ed, W_cc, W_ed, W_mass):
     umac = [u.copy() for u in umac]

@@ -1747,6 +1747,141 @@ int step_impl(const Geo& g, int visc_type, const fhd_gmres_params* p_in, const f
     for (long f = 0; f < nc; f++) pi[f] = pi[f] + dpi[f];
     return st;
 }
+
+// advance_timestep_overdamped (advance_timestep_overdamped.f90:135-734),
+// periodic, centred advection, no gravity, no reactions, barodiffusion off,
+// midpoint_stoch_mass_flux_type = 1.  theta_alpha = 0 (line 135).  Two
+// random stages per step (n_rngs = 2 for this algorithm, main_driver.f90:
+// 534-536), drawn once at the predictor: W_cc[r*dim+c], W_ed[r*2*nE+...]
+// and W_mass[(r*dim+d)*ns+i] for r = 0, 1.  The predictor uses the weights
+// (1, 0) over dt/2 (lines 187-188, 228-229, 246-249), the corrector
+// (1/sqrt2, 1/sqrt2) over dt (lines 466-469, 485-490).
+int overdamped_impl(const Geo& g, int visc_type, const fhd_gmres_params* p_in, const fhd_stoch_params* sp,
+                    const Mix* mix, double dt, double* const umac[], double* const rho[], double* pi,
+                    const double* eta, const double* const eta_ed[], const double* kappa, const double* temperature,
+                    const double* const temperature_ed[], const double* const W_cc[], const double* const W_ed[],
+                    const double* const W_mass[], fhd_solve_stats* stats2) {
+    const int dim = g.dim;
+    const long nc = g.nc;
+    const int nE = n_edge(dim);
+    const int ns = mix ? mix->ns : 1;
+    fhd_gmres_params p = *p_in;
+    auto fvec = [&](std::vector<Vec>& v) { v.assign(dim, Vec(nc, 0.0)); };
+    auto ptrs = [&](std::vector<Vec>& v, double** out) { for (int c = 0; c < dim; c++) out[c] = v[c].data(); };
+    std::vector<Vec> rhotot_fc, rhs_v, dumac, gradpi, diff;
+    fvec(rhotot_fc); fvec(rhs_v); fvec(dumac); fvec(gradpi); fvec(diff);
+    double *rtf[3], *rv[3], *du[3], *gpi[3], *df[3];
+    ptrs(rhotot_fc, rtf); ptrs(rhs_v, rv); ptrs(dumac, du); ptrs(gradpi, gpi); ptrs(diff, df);
+    std::vector<Vec> rho_old(ns), rho_update(ns, Vec(nc)), sfc(ns * dim, Vec(nc)), fdiv(ns, Vec(nc, 0.0));
+    for (int s = 0; s < ns; s++) rho_old[s].assign(rho[s], rho[s] + nc);
+    Vec rhotot(nc), rhs_p(nc), dpi(nc);
+    const double* um[3] = {umac[0], umac[1], dim == 3 ? umac[2] : nullptr};
+    // diffusive_m_fluxdiv with the full viscosity (stag_applyop with alpha = 0,
+    // sign flipped): out = +L u
+    auto diff_m = [&](double* const out[]) {
+        SLevel L;
+        L.g = g;
+        for (int c = 0; c < dim; c++) { L.alpha[c].assign(nc, 0.0); L.phi[c].assign(um[c], um[c] + nc); L.Lphi[c].assign(nc, 0.0); }
+        L.beta.assign(eta, eta + nc);
+        L.gamma.assign(kappa, kappa + nc);
+        for (int e = 0; e < nE; e++) L.bed[e].assign(eta_ed[e], eta_ed[e] + nc);
+        s_applyop(L, visc_type, 0);
+        for (int c = 0; c < dim; c++)
+            for (long f = 0; f < nc; f++) out[c][f] = L.Lphi[c][f] * -1.0;
+    };
+    auto sum_species = [&](double* const* r, double* out) {
+        for (long f = 0; f < nc; f++) {
+            double v = 0.0;
+            for (int s = 0; s < ns; s++) v = v + r[s][f];
+            out[f] = v;
+        }
+    };
+    auto species_fc = [&](double* const* r) {
+        for (int s = 0; s < ns; s++) {
+            double* o[3] = {sfc[s * dim].data(), sfc[s * dim + 1].data(), dim == 3 ? sfc[s * dim + 2].data() : nullptr};
+            avg_face(g, r[s], o);
+        }
+    };
+    double* fd[FHD_MAX_SPECIES];
+    for (int s = 0; s < ns; s++) fd[s] = fdiv[s].data();
+    // one half of the step: mass fluxes at rho, rhs, GMRES, velocity and
+    // density update rho = rho_old + h * (F + advection)
+    auto stage = [&](const double* weights, double h, double* norm_pre_rhs, fhd_solve_stats* sst) -> int {
+        // -grad pi (lines 207-212 / 437-442)
+        c_grad(g, pi, gpi);
+        for (int c = 0; c < dim; c++)
+            for (long f = 0; f < nc; f++) rhs_v[c][f] = -1.0 * gradpi[c][f];
+        // += div(Sigma) with the stage weights over h (lines 214-220 / 444-449)
+        if (sp->variance_coef_mom != 0.0) {
+            int rc = stoch_m_impl(g, sp, rv, 1, eta, eta_ed, temperature, temperature_ed, h, weights, 2, W_cc, W_ed);
+            if (rc) return rc;
+        }
+        // mass fluxes at the current densities (lines 233-236 / 464-469)
+        if (mix) {
+            const double* cr[FHD_MAX_SPECIES];
+            for (int s = 0; s < ns; s++) cr[s] = rho[s];
+            int rc = mass_fluxdiv_impl(g, *mix, sp, cr, h, weights, 2, W_mass, fd, nullptr);
+            if (rc) return rc;
+        }
+        // rhs_p = sum_i -F_i/rhobar_i (lines 284-297 / 530-543)
+        std::fill(rhs_p.begin(), rhs_p.end(), 0.0);
+        if (mix)
+            for (int s = 0; s < ns; s++)
+                for (long f = 0; f < nc; f++) rhs_p[f] = rhs_p[f] + (-1.0 / mix->rhobar[s]) * fdiv[s][f];
+        for (int s = 0; s < ns; s++) {
+            if (mix) std::copy(fdiv[s].begin(), fdiv[s].end(), rho_update[s].begin());
+            else std::fill(rho_update[s].begin(), rho_update[s].end(), 0.0);
+        }
+        // += A_0 u^n, rhs_p += div u (lines 322-327 / 569-574)
+        diff_m(df);
+        for (int c = 0; c < dim; c++)
+            for (long f = 0; f < nc; f++) rhs_v[c][f] = rhs_v[c][f] + diff[c][f];
+        c_div(g, um, rhs_p.data(), true);
+        for (int c = 0; c < dim; c++) std::fill(dumac[c].begin(), dumac[c].end(), 0.0);
+        std::fill(dpi.begin(), dpi.end(), 0.0);
+        {
+            const double* rvp[3] = {rv[0], rv[1], dim == 3 ? rv[2] : nullptr};
+            const double* rtp[3] = {rtf[0], rtf[1], dim == 3 ? rtf[2] : nullptr};
+            int s1 = gmres_impl(g, visc_type, &p, rvp, rhs_p.data(), du, dpi.data(), rtp, eta, eta_ed, kappa, 0.0,
+                                norm_pre_rhs, sst);
+            if (s1 < 0) return s1;
+            for (int c = 0; c < dim; c++)
+                for (long f = 0; f < nc; f++) umac[c][f] = umac[c][f] + dumac[c][f];
+            for (long f = 0; f < nc; f++) pi[f] = pi[f] + dpi[f];
+            // rho_update += -div(rho_fc u); rho = rho_old + h rho_update
+            // (lines 390-391, 401-403 / 644-645, 651-653)
+            for (int s = 0; s < ns; s++) {
+                const double* sp3[3] = {sfc[s * dim].data(), sfc[s * dim + 1].data(),
+                                        dim == 3 ? sfc[s * dim + 2].data() : nullptr};
+                adv_s(g, um, sp3, rho_update[s].data(), true);
+                for (long f = 0; f < nc; f++) rho[s][f] = rho_old[s][f] + h * rho_update[s][f];
+            }
+            return s1;
+        }
+    };
+    // faces of rho^n and rho_tot^n (lines 181-183)
+    double* ro[FHD_MAX_SPECIES];
+    for (int s = 0; s < ns; s++) ro[s] = rho_old[s].data();
+    sum_species(ro, rhotot.data());
+    avg_face(g, rhotot.data(), rtf);
+    species_fc(ro);
+    const double w_pred[2] = {1.0, 0.0};
+    const double w_corr[2] = {1.0 / std::sqrt(2.0), 1.0 / std::sqrt(2.0)};
+    double norm_pre_rhs = 0.0;
+    const double gmres_abs_tol_in = p.gmres_abs_tol;
+    int st = stage(w_pred, 0.5 * dt, &norm_pre_rhs, stats2 ? &stats2[0] : nullptr);
+    if (st < 0) return st;
+    // the corrector's GMRES stops at the predictor's preconditioned rhs
+    // (line 338) and the tolerance is restored afterwards (line 587)
+    p.gmres_abs_tol = std::max(gmres_abs_tol_in, norm_pre_rhs * p.gmres_rel_tol);
+    // faces of the predicted densities (lines 410-411)
+    sum_species(rho, rhotot.data());
+    avg_face(g, rhotot.data(), rtf);
+    species_fc(rho);
+    const int s2 = stage(w_corr, dt, nullptr, stats2 ? &stats2[1] : nullptr);
+    if (s2 < 0) return s2;
+    return std::max(st, s2);
+}
 }  // namespace
 
 extern "C" {
@@ -1773,6 +1908,22 @@ int or_advance_inertial_ms(int dim, const int n[3], double dx, int visc_type, co
     Mix m = make_mix(mp);
     return step_impl(g, visc_type, p_in, sp, &m, dt, umac, rho, pi, fluxdiv, eta, eta_ed, kappa, temperature,
                      temperature_ed, W_cc, W_ed, W_mass, stats2);
+}
+
+int or_advance_overdamped(int dim, const int n[3], double dx, int visc_type, const fhd_gmres_params* p_in,
+                          const fhd_stoch_params* sp, const fhd_mixture_params* mp, double dt,
+                          double* const umac[], double* const rho[], double* pi, const double* eta,
+                          const double* const eta_ed[], const double* kappa, const double* temperature,
+                          const double* const temperature_ed[], const double* const W_cc[],
+                          const double* const W_ed[], const double* const W_mass[], fhd_solve_stats* stats2) {
+    Geo g(dim, n, dx);
+    if (mp) {
+        Mix m = make_mix(mp);
+        return overdamped_impl(g, visc_type, p_in, sp, &m, dt, umac, rho, pi, eta, eta_ed, kappa, temperature,
+                               temperature_ed, W_cc, W_ed, W_mass, stats2);
+    }
+    return overdamped_impl(g, visc_type, p_in, sp, nullptr, dt, umac, rho, pi, eta, eta_ed, kappa, temperature,
+                           temperature_ed, W_cc, W_ed, nullptr, stats2);
 }
 
 int or_mass_fluxdiv(int dim, const int n[3], double dx, const fhd_stoch_params* sp, const fhd_mixture_params* mp,

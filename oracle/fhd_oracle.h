@@ -116,6 +116,17 @@ int or_advance_inertial(int dim, const int n[3], double dx, int visc_type,
  * fluxdiv[ns] (F^n in, F^{n+1} out) advanced in place; W_mass holds
  * 2*dim*ns face arrays: the previous corrector's fields (reused by this
  * predictor) then this corrector's new fields. */
+/* advance_timestep_overdamped (advance_timestep_overdamped.f90:135-734);
+ * mp = NULL for a single fluid (rho: one array, W_mass unused).  W_cc:
+ * 2*dim, W_ed: 2*2*nE, W_mass: 2*dim*ns (two random stages). */
+int or_advance_overdamped(int dim, const int n[3], double dx, int visc_type,
+                          const fhd_gmres_params* p, const fhd_stoch_params* sp,
+                          const fhd_mixture_params* mp, double dt, double* const umac[],
+                          double* const rho[], double* pi, const double* eta,
+                          const double* const eta_ed[], const double* kappa,
+                          const double* temperature, const double* const temperature_ed[],
+                          const double* const W_cc[], const double* const W_ed[],
+                          const double* const W_mass[], fhd_solve_stats* stats2);
 int or_advance_inertial_ms(int dim, const int n[3], double dx, int visc_type,
                            const fhd_gmres_params* p, const fhd_stoch_params* sp,
                            const fhd_mixture_params* mp, double dt,
