@@ -145,6 +145,11 @@ int  fhd_ctx_destroy(fhd_ctx* ctx);
  * caller before any call (NULL = the context's own stream). */
 void* fhd_ctx_stream(fhd_ctx* ctx);
 int  fhd_ctx_set_stream(fhd_ctx* ctx, void* stream);
+/* Preconditioner applications inside GMRES as CUDA graphs: the first
+ * application for given operands and prepared coefficients is captured, later
+ * ones replay it (mode 1 on, 0 off, -1 default: on unless profiling is
+ * enabled or a multigrid runs more than one V-cycle per application). */
+int fhd_ctx_set_graphs(fhd_ctx* ctx, int mode);
 /* Number of this library's kernels launched through ctx so far. */
 long long fhd_ctx_kernel_launches(fhd_ctx* ctx);
 const char* fhd_status_string(int status);

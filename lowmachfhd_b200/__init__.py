@@ -102,6 +102,11 @@ class StokesSolver:
     def set_stream(self, stream_handle: int | None):
         check(lib().fhd_ctx_set_stream(self._h, C.c_void_p(stream_handle or 0)), "fhd_ctx_set_stream")
 
+    def set_graphs(self, mode: int):
+        """preconditioner applications inside GMRES as CUDA graphs: 1 on,
+        0 off, -1 default"""
+        check(lib().fhd_ctx_set_graphs(self._h, int(mode)), "fhd_ctx_set_graphs")
+
     def profile(self, enable: bool = True):
         """time the finest-level smoother launches with CUDA events"""
         check(lib().fhd_ctx_profile(self._h, int(enable)), "fhd_ctx_profile")

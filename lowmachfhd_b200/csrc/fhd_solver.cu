@@ -4,6 +4,7 @@
 //
 // Follows staggered_grid/src_gmres of LowMachFHD: gmres.f90,
 // apply_matrix.f90, apply_precon.f90, stag_mg_solver.f90, macproject.f90.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -16,6 +17,29 @@ namespace fhd {
 
 static thread_local std::string g_last_error;
 void set_last_error(const std::string& s) { g_last_error = s; }
+
+static std::mutex g_pinned_mu;
+static std::vector<double*> g_pinned_free;
+
+double* pinned_scalars_acquire() {
+    {
+        std::lock_guard<std::mutex> lk(g_pinned_mu);
+        if (!g_pinned_free.empty()) {
+            double* p = g_pinned_free.back();
+            g_pinned_free.pop_back();
+            return p;
+        }
+    }
+    double* p = nullptr;
+    if (cudaMallocHost((void**)&p, sizeof(double) * 256) != cudaSuccess) return nullptr;
+    return p;
+}
+
+void pinned_scalars_release(double* p) {
+    if (!p) return;
+    std::lock_guard<std::mutex> lk(g_pinned_mu);
+    g_pinned_free.push_back(p);
+}
 
 int nlevs_mg(const Grid& g, int minwidth) {
     // compute_nlevs_mg (stag_mg_layout.f90:179-222), one box
@@ -898,6 +922,97 @@ int sync_scalars(fhd_ctx* ctx, int first, int count) {
 }
 
 // ---------------------------------------------------------------------
+// preconditioner applications as CUDA graphs
+// ---------------------------------------------------------------------
+// Inside GMRES a preconditioner application is a fixed sequence of launches
+// on the context stream with no host synchronisation (one V-cycle of each
+// multigrid).  The first application for a given (b, x, prepared
+// coefficients, theta) is captured into a graph; later ones replay it, one
+// launch instead of a few hundred.  The values behind the pointers may
+// change between replays (new coefficients, new right-hand sides); the key
+// changes when a pointer or theta does.
+static const size_t GRAPH_CACHE = 8;
+
+static unsigned long long mix_key(unsigned long long h, unsigned long long v) {
+    h ^= v + 0x9E3779B97F4A7C15ull + (h << 6) + (h >> 2);
+    return h;
+}
+
+static bool graphs_on(fhd_ctx* ctx) {
+    if (ctx->prof || ctx->p.stag_mg_max_vcycles > 1 || ctx->p.mg_max_vcycles > 1) return false;
+    return ctx->graph_mode != 0;
+}
+
+void release_graphs(fhd_ctx* ctx) {
+    for (auto& gr : ctx->graphs) cudaGraphExecDestroy(gr.exec);
+    ctx->graphs.clear();
+}
+
+static int precon_graphed(fhd_ctx* ctx, CSVec<double> b, SVec<double> x) {
+    if (!graphs_on(ctx)) return precon(ctx, b, x);
+    unsigned long long key = 1469598103934665603ull;
+    for (int c = 0; c < 4; c++) {
+        key = mix_key(key, (unsigned long long)(uintptr_t)b.c[c]);
+        key = mix_key(key, (unsigned long long)(uintptr_t)x.c[c]);
+    }
+    for (int c = 0; c < 3; c++) {
+        key = mix_key(key, (unsigned long long)(uintptr_t)ctx->alpha_fc[c]);
+        key = mix_key(key, (unsigned long long)(uintptr_t)ctx->beta_ed[c]);
+    }
+    key = mix_key(key, (unsigned long long)(uintptr_t)ctx->beta);
+    key = mix_key(key, (unsigned long long)(uintptr_t)ctx->gamma);
+    unsigned long long tb;
+    memcpy(&tb, &ctx->theta, sizeof(tb));
+    key = mix_key(key, tb);
+    ctx->graph_clock++;
+    for (auto& gr : ctx->graphs) {
+        if (gr.key != key) continue;
+        gr.used = ctx->graph_clock;
+        FHD_CUDA_TRY(cudaGraphLaunch(gr.exec, ctx->stream));
+        ctx->launches += gr.launches;
+        ctx->vcycles += gr.vcycles;
+        return 0;
+    }
+    // capture this application (thread-local: other threads' CUDA calls are
+    // unaffected), then replay it
+    const long long l0 = ctx->launches;
+    const int v0 = ctx->vcycles;
+    if (cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        cudaGetLastError();
+        return precon(ctx, b, x);
+    }
+    int rc = precon(ctx, b, x);
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamEndCapture(ctx->stream, &graph);
+    cudaGraphExec_t exec = nullptr;
+    if (!rc && e == cudaSuccess && graph) e = cudaGraphInstantiate(&exec, graph, 0);
+    if (graph) cudaGraphDestroy(graph);
+    const long long n = ctx->launches - l0;
+    ctx->launches = l0;
+    if (rc || e != cudaSuccess || !exec) {
+        // not capturable here: run it directly
+        cudaGetLastError();
+        if (exec) cudaGraphExecDestroy(exec);
+        ctx->vcycles = v0;
+        if (rc) return rc;
+        ctx->graph_mode = 0;
+        return precon(ctx, b, x);
+    }
+    if (ctx->graphs.size() >= GRAPH_CACHE) {
+        auto it = std::min_element(ctx->graphs.begin(), ctx->graphs.end(),
+                                   [](const fhd_ctx::PreconGraph& a, const fhd_ctx::PreconGraph& b2) {
+                                       return a.used < b2.used;
+                                   });
+        cudaGraphExecDestroy(it->exec);
+        ctx->graphs.erase(it);
+    }
+    ctx->graphs.push_back({key, exec, n, ctx->vcycles - v0, ctx->graph_clock});
+    FHD_CUDA_TRY(cudaGraphLaunch(exec, ctx->stream));
+    ctx->launches += n;
+    return 0;
+}
+
+// ---------------------------------------------------------------------
 // gmres (gmres.f90:32-619)
 // ---------------------------------------------------------------------
 static SVec<double> svec(double* base, int dim, i64 nc) {
@@ -936,7 +1051,7 @@ int gmres_dev(fhd_ctx* ctx, CSVec<double> b, SVec<double> x, double* norm_pre_rh
     int rc;
     int status = 0;
     // |M^-1 b|
-    if ((rc = precon(ctx, b, tmp))) return rc;
+    if ((rc = precon_graphed(ctx, b, tmp))) return rc;
     if ((rc = wnorm2(ctx, csv(tmp), S_NRM))) return rc;
     if ((rc = wnorm2(ctx, b, S_NRM + 1))) return rc;
     if ((rc = sync_scalars(ctx, S_NRM, 2))) return rc;
@@ -958,7 +1073,7 @@ int gmres_dev(fhd_ctx* ctx, CSVec<double> b, SVec<double> x, double* norm_pre_rh
         // tmp = b - A x
         if ((rc = stokes_apply(ctx, csv(x), b, tmp, 1))) return rc;
         if ((rc = wnorm2(ctx, csv(tmp), S_NRM))) return rc;
-        if ((rc = precon(ctx, csv(tmp), r))) return rc;
+        if ((rc = precon_graphed(ctx, csv(tmp), r))) return rc;
         if ((rc = wnorm2(ctx, csv(r), S_NRM + 1))) return rc;
         if ((rc = sync_scalars(ctx, S_NRM, 2))) return rc;
         norm_resid_Stokes = sqrt(ctx->hscal[S_NRM]);
@@ -993,7 +1108,7 @@ int gmres_dev(fhd_ctx* ctx, CSVec<double> b, SVec<double> x, double* norm_pre_rh
             total_iter++;
             i_copy = i;
             if ((rc = stokes_apply(ctx, csv(V(i - 1)), csv(V(i - 1)), tmp, 0))) return rc;
-            if ((rc = precon(ctx, csv(tmp), w))) return rc;
+            if ((rc = precon_graphed(ctx, csv(tmp), w))) return rc;
             // modified Gram-Schmidt with device-resident coefficients
             for (int k = 1; k <= i; k++) {
                 CSVec<double> none;
@@ -1185,6 +1300,7 @@ int fhd_ctx_create(int dim, const int n_cells[3], const double dx[3], int visc_t
         return FHD_ERR_CUDA;
     }
     c->own = c->stream;
+    c->arena.stream = &c->stream;
     int rc = (c->prec == FHD_PREC_MIXED) ? build_mg(c, c->mg32) : build_mg(c, c->mg64);
     const i64 nc = c->g0.nc;
     const i64 sv = (i64)(dim + 1) * nc;
@@ -1200,7 +1316,7 @@ int fhd_ctx_create(int dim, const int n_cells[3], const double dx[3], int visc_t
         if (!c->V || !c->r || !c->w || !c->tmp || !c->xs || !c->red_partials || !c->red_counter || !c->dscal)
             rc = FHD_ERR_OOM;
     }
-    if (!rc && cudaMallocHost((void**)&c->hscal, sizeof(double) * NSCAL) != cudaSuccess) rc = FHD_ERR_OOM;
+    if (!rc && !(c->hscal = pinned_scalars_acquire())) rc = FHD_ERR_OOM;
     if (!rc && cudaMemsetAsync(c->red_counter, 0, sizeof(double), c->stream) != cudaSuccess) rc = FHD_ERR_CUDA;
     if (!rc && cudaStreamSynchronize(c->stream) != cudaSuccess) rc = FHD_ERR_CUDA;
     if (rc) {
@@ -1217,12 +1333,15 @@ void fhd_mass_release(fhd_ctx* ctx);
 int fhd_ctx_destroy(fhd_ctx* c) {
     if (!c) return FHD_OK;
     if (c->stream) cudaStreamSynchronize(c->stream);
+    // free on the context's own stream: a caller's stream may not outlive it
+    if (c->own) c->stream = c->own;
+    release_graphs(c);
     fhd_host_path_release(c);
     fhd_mass_release(c);
     c->arena.release();
     for (cudaEvent_t e : c->prof_ev) cudaEventDestroy(e);
     c->prof_ev.clear();
-    if (c->hscal) cudaFreeHost(c->hscal);
+    pinned_scalars_release(c->hscal);
     if (c->own) cudaStreamDestroy(c->own);
     delete c;
     return FHD_OK;
@@ -1260,6 +1379,14 @@ int fhd_ctx_profile_read(fhd_ctx* c, long long* launches, double* ms, double* by
     if (launches) *launches = c->prof_launches;
     if (ms) *ms = t;
     if (bytes) *bytes = c->prof_bytes;
+    return FHD_OK;
+}
+
+int fhd_ctx_set_graphs(fhd_ctx* c, int mode) {
+    if (!c || mode < -1 || mode > 1) return FHD_ERR_BAD_ARG;
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess) return FHD_ERR_CUDA;
+    c->graph_mode = mode;
+    if (mode == 0) release_graphs(c);
     return FHD_OK;
 }
 

@@ -108,25 +108,35 @@ inline void with_dim(int dim, F&& f) {
 
 struct fhd_ctx_impl;
 
-// device allocation owned by a context (freed at destroy)
+// device allocation owned by a context (freed at destroy).  Stream-ordered
+// (cudaMallocAsync on the context's current stream, *stream): a plain
+// cudaMalloc / cudaFree would serialise every other stream of the device,
+// which would stall the concurrent contexts of a serving process.
 struct Arena {
     std::vector<void*> blocks;
     size_t bytes = 0;
+    cudaStream_t* stream = nullptr;
     template <typename T>
     T* alloc(i64 n) {
         void* p = nullptr;
         if (n <= 0) n = 1;
-        if (cudaMalloc(&p, (size_t)n * sizeof(T)) != cudaSuccess) return nullptr;
+        if (cudaMallocAsync(&p, (size_t)n * sizeof(T), *stream) != cudaSuccess) return nullptr;
         blocks.push_back(p);
         bytes += (size_t)n * sizeof(T);
         return (T*)p;
     }
     void release() {
-        for (void* p : blocks) cudaFree(p);
+        for (void* p : blocks) cudaFreeAsync(p, *stream);
+        if (!blocks.empty()) cudaStreamSynchronize(*stream);
         blocks.clear();
         bytes = 0;
     }
 };
+
+// pinned host blocks of NSCAL doubles, reused across contexts (a pinned
+// allocation or free also serialises the device's streams)
+double* pinned_scalars_acquire();
+void pinned_scalars_release(double* p);
 
 template <typename T>
 struct StagLevel {
@@ -219,6 +229,19 @@ struct fhd_ctx {
     // inertial-step work arrays (allocated on the first step)
     bool step_ready = false;
     double* sb[128] = {nullptr};
+    // CUDA graphs of the preconditioner applications inside GMRES, keyed by
+    // the operand pointers and the prepared coefficients (-1 auto, 0 off,
+    // 1 on)
+    int graph_mode = -1;
+    struct PreconGraph {
+        unsigned long long key;
+        cudaGraphExec_t exec;
+        long long launches;
+        int vcycles;
+        long long used;
+    };
+    std::vector<PreconGraph> graphs;
+    long long graph_clock = 0;
     // optional timing of the finest-level smoother launches (CUDA events on
     // the context stream) with their algorithmic bytes
     bool prof = false;

@@ -237,15 +237,27 @@ enum {
 };
 static_assert(B_COUNT <= 128, "step buffer table");
 
-static int step_alloc(fhd_ctx* ctx) {
-    if (ctx->step_ready) return 0;
+// work arrays of the steps: the shared ones once, the per-species ones for
+// the species counts met so far
+static int step_alloc(fhd_ctx* ctx, int ns) {
     const i64 nc = ctx->g0.nc;
-    for (int i = 0; i < B_COUNT; i++) {
+    const int dim = ctx->dim;
+    auto need = [&](int i) -> int {
+        if (ctx->sb[i]) return 0;
         ctx->sb[i] = ctx->arena.alloc<double>(nc);
-        if (!ctx->sb[i]) return FHD_ERR_OOM;
+        return ctx->sb[i] ? 0 : FHD_ERR_OOM;
+    };
+    if (!ctx->step_ready) {
+        for (int i = 0; i < B_RHOOLD; i++)
+            if (need(i)) return FHD_ERR_OOM;
+        FHD_CUDA_TRY(cudaMemsetAsync(ctx->sb[B_ZERO], 0, sizeof(double) * nc, ctx->stream));
+        ctx->step_ready = true;
     }
-    FHD_CUDA_TRY(cudaMemsetAsync(ctx->sb[B_ZERO], 0, sizeof(double) * nc, ctx->stream));
-    ctx->step_ready = true;
+    for (int s = 0; s < ns; s++) {
+        if (need(B_RHOOLD + s) || need(B_RUPD + s)) return FHD_ERR_OOM;
+        for (int c = 0; c < dim; c++)
+            if (need(B_SFC + s * dim + c)) return FHD_ERR_OOM;
+    }
     return 0;
 }
 
@@ -339,11 +351,11 @@ int advance_inertial_ms(fhd_ctx* ctx, const fhd_stoch_params* sp, const fhd_mixt
                         const double* eta, const double* const eta_ed[], const double* kappa,
                         const double* temperature, const double* const temperature_ed[], const double* const W_cc[],
                         const double* const W_ed[], const double* const W_mass[], fhd_solve_stats* stats2) {
-    int rc = step_alloc(ctx);
-    if (rc) return rc;
     const int dim = ctx->dim, nE = dim == 2 ? 1 : 3;
     const int ns = mp ? mp->nspecies : 1;
     if (ns < 1 || ns > FHD_MAX_SPECIES) return FHD_ERR_BAD_ARG;
+    int rc = step_alloc(ctx, ns);
+    if (rc) return rc;
     const Grid g = ctx->g0;
     const i64 nc = g.nc;
     const int nb = flat_blocks(nc);
@@ -582,11 +594,11 @@ int advance_overdamped(fhd_ctx* ctx, const fhd_stoch_params* sp, const fhd_mixtu
                        const double* const eta_ed[], const double* kappa, const double* temperature,
                        const double* const temperature_ed[], const double* const W_cc[], const double* const W_ed[],
                        const double* const W_mass[], fhd_solve_stats* stats2) {
-    int rc = step_alloc(ctx);
-    if (rc) return rc;
     const int dim = ctx->dim;
     const int ns = mp ? mp->nspecies : 1;
     if (ns < 1 || ns > FHD_MAX_SPECIES) return FHD_ERR_BAD_ARG;
+    int rc = step_alloc(ctx, ns);
+    if (rc) return rc;
     const Grid g = ctx->g0;
     const i64 nc = g.nc;
     const int nb = flat_blocks(nc);
