@@ -18,6 +18,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
 import subprocess
 import sys
@@ -59,6 +60,7 @@ def parse():
     ap.add_argument("--cpu-sample-n", type=int, default=128)
     ap.add_argument("--only", choices=["mixed", "fp64"], default=None, help="run one precision only")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving and batched legs")
     ap.add_argument("--probe", choices=["stagmg"], default=None,
                     help="profiling probe: K stag_mg_solver calls (one V-cycle each) on one grid")
     ap.add_argument("--precision", choices=["mixed", "fp64"], default="fp64", help="precision of --probe")
@@ -89,6 +91,127 @@ def run_probe(args):
                       "launches": s.kernel_launches}))
     s.close()
     return 0
+
+
+# ----------------------------------------------------------------------
+# serving: a Poisson stream of Stokes / timestep requests of mixed sizes
+# ----------------------------------------------------------------------
+SERVE_RATE = 10.0      # requests per second (below the capacity of the mix)
+SERVE_REQUESTS = 120
+SERVE_SLOTS = 8
+SERVE_BUDGET = 96 << 30
+
+
+def serve_requests(L, count, seed, precision):
+    """Requests of the serving configuration: 2D 64^2-512^2 overdamped and
+    3D 32^3-192^3 inertial problems (sides log-uniform, multiples of 8),
+    1-4 species, eta ~ U[0.5, 5], k_B T ~ U[1e-4, 1e-3], 4 steps each,
+    seeded.  Mixtures use a cell volume of 1000 (dx = 10 in 3D, depth 1000
+    in 2D)."""
+    import numpy as np
+    reqs = []
+    for i in range(count):
+        rng = np.random.default_rng(seed + i)
+        dim = int(rng.integers(2, 4))
+        lo, hi = (64, 512) if dim == 2 else (32, 192)
+        side = max(lo, min(hi, int(round(math.exp(rng.uniform(math.log(lo), math.log(hi))) / 8)) * 8))
+        ns = int(rng.integers(1, 5))
+        eta = float(rng.uniform(0.5, 5.0))
+        kT = float(rng.uniform(1e-4, 1e-3))
+        D = list(rng.uniform(0.5, 2.0, max(1, ns * (ns - 1) // 2)) * 1e-2)
+        kw = dict(dim=dim, n_cells=[side] * dim, nspecies=ns, eta=eta, kT=kT, steps=4, seed=1000 + i,
+                  precision=L.FHD_PREC_MIXED if precision == "mixed" else L.FHD_PREC_FP64,
+                  params=L.default_params(gmres_rel_tol=REL_TOL))
+        if dim == 2:
+            kw.update(kind=L.FHD_REQ_OVERDAMPED, dx=1.0, cell_depth=1000.0, dt=0.1)
+        else:
+            kw.update(kind=L.FHD_REQ_INERTIAL, dx=10.0, dt=0.05 * 100.0 / eta)
+        if ns > 1:
+            kw["mix"] = L.mixture_params([1.0, 2.0, 3.0, 4.0][:ns], D[: ns * (ns - 1) // 2], rhobar=[1.0] * ns,
+                                         variance_coef_mass=1.0)
+        reqs.append(L.make_request(**kw))
+    return reqs
+
+
+def serve_warmup(L, srv, precision):
+    """one tiny request per (dimension, species count, kind) so that the
+    first launch of every kernel the mix uses is not inside the measurement"""
+    ids = []
+    for dim in (2, 3):
+        for ns in (1, 2, 3, 4):
+            kw = dict(dim=dim, n_cells=[16] * dim if dim == 2 else [8] * 3, nspecies=ns, steps=1, kT=1e-4,
+                      precision=L.FHD_PREC_MIXED if precision == "mixed" else L.FHD_PREC_FP64,
+                      kind=L.FHD_REQ_OVERDAMPED if dim == 2 else L.FHD_REQ_INERTIAL,
+                      dx=1.0 if dim == 2 else 10.0, cell_depth=1000.0, dt=0.1 if dim == 2 else 5.0)
+            if ns > 1:
+                kw["mix"] = L.mixture_params([1.0, 2.0, 3.0, 4.0][:ns], [1e-2] * (ns * (ns - 1) // 2),
+                                             rhobar=[1.0] * ns)
+            ids.append(srv.submit(L.make_request(**kw)))
+    for i in ids:
+        srv.wait(i)
+
+
+def run_serving(L, slots, precision, rate, count, seed=7):
+    """Poisson arrivals at `rate` (seeded; rate None: all at once, the
+    saturation throughput); returns latency percentiles (submit to result)
+    and completed requests per second."""
+    import numpy as np
+    reqs = serve_requests(L, count, seed, precision)
+    if rate:
+        gaps = np.random.default_rng(seed).exponential(1.0 / rate, count)
+        arrive = np.cumsum(gaps) - gaps[0]
+    else:
+        arrive = np.zeros(count)
+    with L.Server(slots, SERVE_BUDGET) as srv:
+        serve_warmup(L, srv, precision)
+        t0 = time.perf_counter()
+        ids = []
+        for r, a in zip(reqs, arrive):
+            d = a - (time.perf_counter() - t0)
+            if d > 0:
+                time.sleep(d)
+            ids.append(srv.submit(r))
+        res = [srv.wait(i) for i in ids]
+    lat = np.array([r["t_end"] - r["t_submit"] for r in res]) * 1e3
+    span = max(r["t_end"] for r in res) - min(r["t_submit"] for r in res)
+    bad = [r["status"] for r in res if r["status"] < 0]
+    return {"p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+            "solves_per_s": count / span, "requests": count, "errors": len(bad),
+            "gmres_iters": int(sum(r["gmres_iters"] for r in res))}
+
+
+# ----------------------------------------------------------------------
+# batched: many independent 2D realizations of uneven size
+# ----------------------------------------------------------------------
+BATCH_REALIZATIONS = 512
+BATCH_STEPS = 20
+BATCH_SLOTS = 16
+
+
+def run_batched(L, count=BATCH_REALIZATIONS, steps=BATCH_STEPS, slots=BATCH_SLOTS, seed=1):
+    """count 2D periodic realizations, sides log-uniform in [32, 256] rounded
+    to multiples of 8 (seeded), eta ~ U[0.5, 5], `steps` overdamped steps
+    each, FP32 preconditioner inside FP64 GMRES at 1e-8; all submitted at
+    once to one server.  Returns realization-steps per second."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    sides = np.clip(np.round(np.exp(rng.uniform(math.log(32), math.log(256), count)) / 8) * 8, 32, 256).astype(int)
+    etas = rng.uniform(0.5, 5.0, count)
+    reqs = [L.make_request(kind=L.FHD_REQ_OVERDAMPED, dim=2, n_cells=[int(n), int(n)], eta=float(e), kT=1.0,
+                           dt=0.1, steps=steps, seed=5000 + i, precision=L.FHD_PREC_MIXED,
+                           params=L.default_params(gmres_rel_tol=REL_TOL))
+            for i, (n, e) in enumerate(zip(sides, etas))]
+    with L.Server(slots, SERVE_BUDGET) as srv:
+        serve_warmup(L, srv, "mixed")
+        t0 = time.perf_counter()
+        ids = [srv.submit(r) for r in reqs]
+        res = [srv.wait(i) for i in ids]
+        wall = time.perf_counter() - t0
+    return {"realizations": count, "steps_each": steps, "slots": slots,
+            "sides": f"log-uniform 32-256, multiples of 8 (seed {seed})", "eta": "U[0.5, 5]",
+            "realization_steps_per_s": count * steps / wall, "wall_s": wall,
+            "gmres_iters": int(sum(r["gmres_iters"] for r in res)),
+            "errors": sum(1 for r in res if r["status"] < 0)}
 
 
 def peaks():
@@ -457,7 +580,11 @@ def main():
         "gpu_launches": mixed["launches"],
         "roofline": {"kernel": "k_stag_gs (finest-level colour Gauss-Seidel sweep)", "bound": "hbm",
                      "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                     "frac": (achieved / hbm) if achieved else None, "traffic": None,
+                     "frac": (achieved / hbm) if achieved else None,
+                     # ncu DRAM read+write of the same kernel captured at
+                     # 192^3 (85.0 + 3.5 MB), scaled by cells to 256^3
+                     "traffic": 88.5e6 * (256 / 192) ** 3,
+                     "traffic_source": "ncu capture at 192^3 scaled by cells",
                      "peak_kind": peak_kind, "launches_timed": n_l,
                      "avg_launch_us": (ms_l / n_l * 1e3) if n_l else None,
                      "bytes_per_launch": (bytes_l / n_l) if n_l else None,
@@ -466,6 +593,23 @@ def main():
         "e2e": {"value": ws * K / (results["e2e"]["ms"] / 1e3), "unit": "steps/s",
                 "h2d_bytes_per_step": results["e2e"]["h2d"], "d2h_bytes_per_step": results["e2e"]["d2h"]},
     }
+    if rank == 0 and not args.no_serve:
+        served = run_serving(L, SERVE_SLOTS, "mixed", SERVE_RATE, SERVE_REQUESTS)
+        saturated = run_serving(L, SERVE_SLOTS, "mixed", None, SERVE_REQUESTS)
+        plain = run_serving(L, 1, "fp64", SERVE_RATE, SERVE_REQUESTS)
+        line["served"] = {
+            "config": {"arrivals": f"Poisson {SERVE_RATE:g}/s, seeded", "requests": SERVE_REQUESTS,
+                       "sizes": "2D 64^2-512^2 overdamped, 3D 32^3-192^3 inertial, log-uniform, 1-4 species",
+                       "steps_per_request": 4, "slots": SERVE_SLOTS, "hbm_budget_gb": SERVE_BUDGET >> 30,
+                       "latency": "submit to result, after one warm-up request per kind"},
+            "p50_ms": served["p50_ms"], "p99_ms": served["p99_ms"],
+            "mixed_continuous": served,
+            "mixed_continuous_saturated": saturated,
+            "fp64_one_at_a_time": plain,
+        }
+        line["batched"] = run_batched(L)
+    if ws > 1:
+        barrier(ws)
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         try:
             cb = cpu_sample(args.cpu_sample_n, n)

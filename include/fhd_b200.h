@@ -290,6 +290,86 @@ int fhd_dev_advance_overdamped(fhd_ctx* ctx, const fhd_stoch_params* sp,
                                const double* const W_cc[], const double* const W_ed[],
                                const double* const W_mass[], fhd_solve_stats* stats2);
 
+/* ------------------------------------------------------------------ */
+/* device random numbers (fill_m_stochastic / fill_mass_stochastic,     */
+/* stochastic_m_fluxdiv.f90:781-860, stochastic_mass_fluxdiv.f90:182-214*/
+/* draw from the host RNG; this is the device-side replacement)         */
+/* ------------------------------------------------------------------ */
+/* out[0..n) = scale * N(0,1) from Philox-4x32-10 (Salmon et al., SC 2011)
+ * keyed by seed; element pair (2j, 2j+1) is the Box-Muller transform of
+ * the block at counter (j, field, stream_a, stream_b).  Launched on
+ * stream (cudaStream_t, NULL = legacy default stream). */
+int fhd_dev_fill_normal(double* out, long long n, unsigned long long seed,
+                        unsigned field, unsigned stream_a, unsigned stream_b,
+                        double scale, void* stream);
+/* The Philox-4x32-10 block function on the host (the same code as the
+ * device generator). */
+void fhd_philox4x32_10(const unsigned ctr[4], const unsigned key[2],
+                       unsigned out[4]);
+
+/* ------------------------------------------------------------------ */
+/* serving: many device-resident problems on one GPU (no counterpart in */
+/* the reference, whose driver runs one problem per process)           */
+/* ------------------------------------------------------------------ */
+#define FHD_REQ_OVERDAMPED 0   /* advance_timestep_overdamped steps */
+#define FHD_REQ_INERTIAL   1   /* advance_timestep_inertial steps   */
+/* One problem: a periodic box, a fluid (nspecies = 1) or an ideal
+ * mixture (2..5), uniform eta, k_B T and total density rho0 (mass
+ * fractions 1/nspecies), zero initial velocity and pressure, `steps`
+ * timesteps of `kind` with device-drawn noise from `seed`.  The final
+ * velocity (dim*Nc) and densities (nspecies*Nc) are copied to the host
+ * buffers out_umac / out_rho when those are not NULL. */
+typedef struct fhd_request {
+    int    kind;
+    int    dim;
+    int    n_cells[3];
+    double dx;
+    double cell_depth;             /* 2D: dV = dx*dx*cell_depth */
+    int    visc_type;
+    int    precision;              /* FHD_PREC_FP64 / FHD_PREC_MIXED */
+    int    nspecies;
+    fhd_mixture_params mix;        /* used when nspecies > 1 */
+    double rho0, eta, kT, dt;
+    int    steps;
+    unsigned long long seed;
+    fhd_gmres_params params;
+    double* out_umac;
+    double* out_rho;
+} fhd_request;
+typedef struct fhd_request_result {
+    long long id;
+    int    status;                 /* worst step status, or an error */
+    int    gmres_iters;            /* total over all solves */
+    long long launches;            /* kernels launched for the request */
+    double t_submit, t_start, t_end;   /* seconds on the server's clock */
+    double u_sumsq;                /* sum over faces of |u|^2 at the end */
+    unsigned long long bytes;      /* device bytes reserved at admission */
+} fhd_request_result;
+void fhd_request_default(fhd_request* r);
+/* Device bytes the server reserves for a request (an upper estimate). */
+unsigned long long fhd_request_bytes(const fhd_request* r);
+/* A server with `slots` worker threads (one CUDA stream each) on the
+ * current device.  Requests start in arrival order as soon as a slot is
+ * free and their bytes fit in hbm_budget_bytes beside the running ones;
+ * each result depends only on its request. */
+typedef struct fhd_server fhd_server;
+int fhd_server_create(int slots, unsigned long long hbm_budget_bytes, fhd_server** out);
+/* Queues a copy of *req; *id identifies it for fhd_server_wait.  A request
+ * larger than the whole budget is refused with FHD_ERR_OOM. */
+int fhd_server_submit(fhd_server* srv, const fhd_request* req, long long* id);
+/* Blocks until request id has finished. */
+int fhd_server_wait(fhd_server* srv, long long id, fhd_request_result* res);
+/* Seconds since the server was created (the clock of the results). */
+double fhd_server_clock(fhd_server* srv);
+/* Finishes the queued requests and joins the workers. */
+int fhd_server_destroy(fhd_server* srv);
+/* The admission policy on a synthetic trace without a GPU: n requests
+ * (arrival time, bytes, run time) on `slots` workers and a byte budget;
+ * writes each start time. */
+int fhd_sched_simulate(int slots, unsigned long long budget, int n,
+                       const double* arrive, const unsigned long long* bytes,
+                       const double* runtime, double* start);
+
 /* Text of the last CUDA error seen by the calling thread. */
 const char* fhd_last_error(void);
 /* Bytes of device memory a context holds. */

@@ -18,10 +18,13 @@ from typing import Sequence
 import numpy as np
 
 from . import _capi
-from ._capi import (FHD_PREC_FP64, FHD_PREC_MIXED, Fab, FhdError, GmresParams, MixtureParams, Multifab,
-                    SolveStats, StochParams, check, lib, mixture_params)
+from ._capi import (FHD_PREC_FP64, FHD_PREC_MIXED, FHD_REQ_INERTIAL, FHD_REQ_OVERDAMPED, Fab, FhdError,
+                    GmresParams, MixtureParams, Multifab, Request, RequestResult, SolveStats, StochParams, check, lib,
+                    mixture_params)
 
 __all__ = ["StokesSolver", "GmresParams", "StochParams", "SolveStats", "MixtureParams", "mixture_params",
+           "Server", "Request", "RequestResult", "make_request", "fill_normal", "philox4x32_10", "sched_simulate",
+           "FHD_REQ_OVERDAMPED", "FHD_REQ_INERTIAL",
            "default_params", "FhdError",
            "FHD_PREC_FP64", "FHD_PREC_MIXED", "lib", "fab_from_canonical", "canonical_from_fab", "FabArray"]
 
@@ -336,3 +339,106 @@ def canonical_from_fab(fa: FabArray, dim: int, n_cells) -> np.ndarray:
     g = fa.ng
     sl = tuple(slice(g, g + fa.hi[d] - fa.lo[d] + 1) for d in range(dim))
     return np.ascontiguousarray(fa.data[sl].T).reshape(-1)
+
+
+# ----------------------------------------------------------------------
+# device random numbers and serving
+# ----------------------------------------------------------------------
+def fill_normal(out, seed: int, field: int = 0, stream_a: int = 0, stream_b: int = 0, scale: float = 1.0,
+                stream: int | None = None):
+    """out (contiguous float64 CUDA tensor) = scale * N(0,1) from the
+    device Philox-4x32-10 generator (fill_m_stochastic's role)."""
+    check(lib().fhd_dev_fill_normal(C.c_void_p(out.data_ptr()), out.numel(), int(seed), int(field), int(stream_a),
+                                    int(stream_b), float(scale), C.c_void_p(stream or 0)), "fill_normal")
+
+
+def philox4x32_10(ctr, key):
+    """the Philox-4x32-10 block function (host side of the device generator)"""
+    c = (C.c_uint * 4)(*[int(x) & 0xFFFFFFFF for x in ctr])
+    k = (C.c_uint * 2)(*[int(x) & 0xFFFFFFFF for x in key])
+    o = (C.c_uint * 4)()
+    lib().fhd_philox4x32_10(c, k, o)
+    return list(o)
+
+
+def make_request(**kw) -> Request:
+    """an fhd_request with the library defaults, fields overridden by kw
+    (n_cells as a list; params as a GmresParams; mix as MixtureParams)"""
+    r = Request()
+    lib().fhd_request_default(C.byref(r))
+    for k, v in kw.items():
+        if k == "n_cells":
+            n = list(v) + [1] * (3 - len(v))
+            r.n_cells = (C.c_int * 3)(*n)
+        elif not hasattr(r, k):
+            raise AttributeError(f"fhd_request has no field {k}")
+        else:
+            setattr(r, k, v)
+    return r
+
+
+def sched_simulate(slots: int, budget: int, arrive, nbytes, runtime):
+    """start times the server's admission policy gives a synthetic trace"""
+    n = len(arrive)
+    a = (C.c_double * max(1, n))(*arrive)
+    b = (C.c_ulonglong * max(1, n))(*[int(x) for x in nbytes])
+    r = (C.c_double * max(1, n))(*runtime)
+    s = (C.c_double * max(1, n))()
+    check(lib().fhd_sched_simulate(int(slots), int(budget), n, C.cast(a, _DP), b, C.cast(r, _DP), C.cast(s, _DP)),
+          "sched_simulate")
+    return list(s)[:n]
+
+
+class Server:
+    """Many device-resident problems on one GPU (fhd_server_*): `slots`
+    worker threads with a CUDA stream each, admission in arrival order
+    within an HBM byte budget."""
+
+    def __init__(self, slots: int, hbm_budget_bytes: int):
+        h = C.c_void_p()
+        check(lib().fhd_server_create(int(slots), int(hbm_budget_bytes), C.byref(h)), "fhd_server_create")
+        self._h = h
+        self._keep = {}
+
+    @staticmethod
+    def request_bytes(req: Request) -> int:
+        return int(lib().fhd_request_bytes(C.byref(req)))
+
+    def clock(self) -> float:
+        return float(lib().fhd_server_clock(self._h))
+
+    def submit(self, req: Request, out_umac=None, out_rho=None) -> int:
+        """queue a copy of req; out_umac / out_rho: optional float64 numpy
+        arrays (dim*Nc, nspecies*Nc) that receive the final state"""
+        r = Request.from_buffer_copy(req)
+        if out_umac is not None:
+            r.out_umac = out_umac.ctypes.data_as(_DP)
+        if out_rho is not None:
+            r.out_rho = out_rho.ctypes.data_as(_DP)
+        rid = C.c_longlong()
+        check(lib().fhd_server_submit(self._h, C.byref(r), C.byref(rid)), "fhd_server_submit")
+        self._keep[rid.value] = (out_umac, out_rho)
+        return rid.value
+
+    def wait(self, rid: int) -> dict:
+        res = RequestResult()
+        check(lib().fhd_server_wait(self._h, int(rid), C.byref(res)), "fhd_server_wait")
+        self._keep.pop(rid, None)
+        return res.as_dict()
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().fhd_server_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -85,6 +85,28 @@ def mixture_params(molmass, Dbar, rhobar=None, variance_coef_mass=1.0, chi_itera
     return m
 
 
+FHD_REQ_OVERDAMPED = 0
+FHD_REQ_INERTIAL = 1
+
+
+class Request(C.Structure):
+    """fhd_request: one served problem (include/fhd_b200.h)."""
+    _fields_ = [("kind", C.c_int), ("dim", C.c_int), ("n_cells", C.c_int * 3), ("dx", C.c_double),
+                ("cell_depth", C.c_double), ("visc_type", C.c_int), ("precision", C.c_int), ("nspecies", C.c_int),
+                ("mix", MixtureParams), ("rho0", C.c_double), ("eta", C.c_double), ("kT", C.c_double),
+                ("dt", C.c_double), ("steps", C.c_int), ("seed", C.c_ulonglong), ("params", GmresParams),
+                ("out_umac", C.POINTER(C.c_double)), ("out_rho", C.POINTER(C.c_double))]
+
+
+class RequestResult(C.Structure):
+    _fields_ = [("id", C.c_longlong), ("status", C.c_int), ("gmres_iters", C.c_int), ("launches", C.c_longlong),
+                ("t_submit", C.c_double), ("t_start", C.c_double), ("t_end", C.c_double), ("u_sumsq", C.c_double),
+                ("bytes", C.c_ulonglong)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class SolveStats(C.Structure):
     _fields_ = [("outer_iters", C.c_int), ("total_iters", C.c_int), ("vcycles", C.c_int),
                 ("status", C.c_int),
@@ -145,6 +167,17 @@ _PROTOS = {
     "fhd_dev_advance_overdamped": (C.c_int, [_VP, C.POINTER(StochParams), C.POINTER(MixtureParams), C.c_double,
                                              _PP, _PP, _DP, _DP, _PP, _DP, _DP, _PP, _PP, _PP, _PP,
                                              C.POINTER(SolveStats)]),
+    "fhd_dev_fill_normal": (C.c_int, [_VP, C.c_longlong, C.c_ulonglong, C.c_uint, C.c_uint, C.c_uint, C.c_double,
+                                      _VP]),
+    "fhd_philox4x32_10": (None, [C.POINTER(C.c_uint), C.POINTER(C.c_uint), C.POINTER(C.c_uint)]),
+    "fhd_request_default": (None, [C.POINTER(Request)]),
+    "fhd_request_bytes": (C.c_ulonglong, [C.POINTER(Request)]),
+    "fhd_server_create": (C.c_int, [C.c_int, C.c_ulonglong, C.POINTER(_VP)]),
+    "fhd_server_submit": (C.c_int, [_VP, C.POINTER(Request), C.POINTER(C.c_longlong)]),
+    "fhd_server_wait": (C.c_int, [_VP, C.c_longlong, C.POINTER(RequestResult)]),
+    "fhd_server_clock": (C.c_double, [_VP]),
+    "fhd_server_destroy": (C.c_int, [_VP]),
+    "fhd_sched_simulate": (C.c_int, [C.c_int, C.c_ulonglong, C.c_int, _DP, C.POINTER(C.c_ulonglong), _DP, _DP]),
     "fhd_gmres": (C.c_int, [_VP] + [C.POINTER(Multifab)] * 8 + [_DP, _DP, C.POINTER(SolveStats)]),
     "fhd_apply_precon": (C.c_int, [_VP] + [C.POINTER(Multifab)] * 8 + [C.c_double]),
     "fhd_apply_matrix": (C.c_int, [_VP] + [C.POINTER(Multifab)] * 8 + [C.c_double]),

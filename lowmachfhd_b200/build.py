@@ -9,7 +9,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 SRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "_fhd_b200.so")
-SOURCES = ["fhd_solver.cu", "fhd_step.cu", "fhd_capi.cu", "fhd_noalloc.cu", "fhd_mass.cu"]
+SOURCES = ["fhd_solver.cu", "fhd_step.cu", "fhd_capi.cu", "fhd_noalloc.cu", "fhd_mass.cu", "fhd_server.cu"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-lineinfo", "-O3", "-std=c++17",
