@@ -147,8 +147,9 @@ void* fhd_ctx_stream(fhd_ctx* ctx);
 int  fhd_ctx_set_stream(fhd_ctx* ctx, void* stream);
 /* Preconditioner applications inside GMRES as CUDA graphs: the first
  * application for given operands and prepared coefficients is captured, later
- * ones replay it (mode 1 on, 0 off, -1 default: on unless profiling is
- * enabled or a multigrid runs more than one V-cycle per application). */
+ * ones replay it (mode 1 on, 0 off, -1 default: on unless a multigrid
+ * runs more than one V-cycle per application).  fhd_ctx_profile timing
+ * works in both modes. */
 int fhd_ctx_set_graphs(fhd_ctx* ctx, int mode);
 /* Number of this library's kernels launched through ctx so far. */
 long long fhd_ctx_kernel_launches(fhd_ctx* ctx);

@@ -288,6 +288,26 @@ static cudaEvent_t prof_event(fhd_ctx* ctx) {
     return ctx->prof_ev[ctx->prof_used++];
 }
 
+// one profiling timestamp on stream st.  Inside a graph capture the record
+// becomes an event-record node of the graph; its handle is kept (in capture
+// order) so that every replay can point it at a fresh event.
+static void prof_mark(fhd_ctx* ctx, cudaStream_t st) {
+    if (!ctx->capturing) {
+        cudaEventRecord(prof_event(ctx), st);
+        return;
+    }
+    // an external record is a graph node (a plain record inside a capture
+    // only orders streams and leaves no node)
+    cudaEventRecordWithFlags(prof_event(ctx), st, cudaEventRecordExternal);
+    cudaStreamCaptureStatus cs;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t nd = 0;
+    if (cudaStreamGetCaptureInfo(st, &cs, nullptr, nullptr, &deps, &nd) == cudaSuccess && nd == 1)
+        ctx->cap_nodes.push_back(deps[0]);
+    else
+        ctx->cap_fail = true;
+}
+
 template <typename T>
 static int stag_smooth(fhd_ctx* ctx, StagLevel<T>& L, int color) {
     cudaStream_t st = ctx->stream;
@@ -297,7 +317,7 @@ static int stag_smooth(fhd_ctx* ctx, StagLevel<T>& L, int color) {
     if (color != 0 && all_even(L.g)) {
         const bool timed = ctx->prof && L.g.nc == ctx->g0.nc;
         if (timed) {
-            cudaEventRecord(prof_event(ctx), st);
+            prof_mark(ctx, st);
             ctx->prof_bytes += gs_sweep_bytes(ctx, L);
             ctx->prof_launches++;
         }
@@ -316,7 +336,7 @@ static int stag_smooth(fhd_ctx* ctx, StagLevel<T>& L, int color) {
                     L.g, A, L.phi[0], L.phi[1], L.phi[2], L.rhs[DIM == 3 ? 2 : 1], par, omega);
             rc |= post(ctx);
         });
-        if (timed) cudaEventRecord(prof_event(ctx), st);
+        if (timed) prof_mark(ctx, st);
         return rc;
     }
     with_dim_visc(ctx->dim, ctx->visc, [&](auto D, auto V) {
@@ -386,21 +406,21 @@ static int stag_rb_smooth(fhd_ctx* ctx, StagLevel<T>& L, const RBGeom& G, T* con
         constexpr int VISC = decltype(V)::value;
         if constexpr (VISC == 1 || VISC == -1) {
             if (timed) {
-                cudaEventRecord(prof_event(ctx), st);
+                prof_mark(ctx, st);
                 ctx->prof_bytes += rb_smooth_bytes(ctx, L);
                 ctx->prof_launches++;
             }
             rc |= rb_allow_smem(k_stag_rb<T, VISC, -1>, smem);
             k_stag_rb<T, VISC, -1><<<dim3(G.tiles_x * G.tiles_y, G.chunks, 3), blk, smem, st>>>(L.g, G, A, R, omega);
             rc |= post(ctx);
-            if (timed) cudaEventRecord(prof_event(ctx), st);
+            if (timed) prof_mark(ctx, st);
         } else {
             const dim3 grd(G.tiles_x * G.tiles_y, G.chunks, 1);
             for (int c = 0; c < 3; c++) {
                 // components before c already hold this smooth's values
                 for (int d = 0; d < 3; d++) R.oth[d] = d < c ? b[d] : a[d];
                 if (timed) {
-                    cudaEventRecord(prof_event(ctx), st);
+                    prof_mark(ctx, st);
                     ctx->prof_bytes += rb_smooth_bytes(ctx, L);
                     ctx->prof_launches++;
                 }
@@ -411,7 +431,7 @@ static int stag_rb_smooth(fhd_ctx* ctx, StagLevel<T>& L, const RBGeom& G, T* con
                 else if (c == 1) k_stag_rb<T, VISC, 1><<<grd, blk, smem, st>>>(L.g, G, A, R, omega);
                 else k_stag_rb<T, VISC, 2><<<grd, blk, smem, st>>>(L.g, G, A, R, omega);
                 rc |= post(ctx);
-                if (timed) cudaEventRecord(prof_event(ctx), st);
+                if (timed) prof_mark(ctx, st);
             }
         }
     });
@@ -939,13 +959,31 @@ static unsigned long long mix_key(unsigned long long h, unsigned long long v) {
 }
 
 static bool graphs_on(fhd_ctx* ctx) {
-    if (ctx->prof || ctx->p.stag_mg_max_vcycles > 1 || ctx->p.mg_max_vcycles > 1) return false;
+    if (ctx->p.stag_mg_max_vcycles > 1 || ctx->p.mg_max_vcycles > 1) return false;
     return ctx->graph_mode != 0;
 }
 
+static void drop_graph(fhd_ctx::PreconGraph& gr) {
+    cudaGraphExecDestroy(gr.exec);
+    if (gr.graph) cudaGraphDestroy(gr.graph);
+}
+
 void release_graphs(fhd_ctx* ctx) {
-    for (auto& gr : ctx->graphs) cudaGraphExecDestroy(gr.exec);
+    for (auto& gr : ctx->graphs) drop_graph(gr);
     ctx->graphs.clear();
+}
+
+// launch a cached application: fresh events for its profiling nodes, the
+// profiling totals and the launch counters it stands for
+static int replay(fhd_ctx* ctx, fhd_ctx::PreconGraph& gr) {
+    for (cudaGraphNode_t nd : gr.ev_nodes)
+        FHD_CUDA_TRY(cudaGraphExecEventRecordNodeSetEvent(gr.exec, nd, prof_event(ctx)));
+    FHD_CUDA_TRY(cudaGraphLaunch(gr.exec, ctx->stream));
+    ctx->prof_bytes += gr.prof_bytes;
+    ctx->prof_launches += gr.prof_launches;
+    ctx->launches += gr.launches;
+    ctx->vcycles += gr.vcycles;
+    return 0;
 }
 
 static int precon_graphed(fhd_ctx* ctx, CSVec<double> b, SVec<double> x) {
@@ -964,52 +1002,79 @@ static int precon_graphed(fhd_ctx* ctx, CSVec<double> b, SVec<double> x) {
     unsigned long long tb;
     memcpy(&tb, &ctx->theta, sizeof(tb));
     key = mix_key(key, tb);
+    key = mix_key(key, ctx->prof ? 1ull : 0ull);
     ctx->graph_clock++;
     for (auto& gr : ctx->graphs) {
         if (gr.key != key) continue;
         gr.used = ctx->graph_clock;
-        FHD_CUDA_TRY(cudaGraphLaunch(gr.exec, ctx->stream));
-        ctx->launches += gr.launches;
-        ctx->vcycles += gr.vcycles;
-        return 0;
+        return replay(ctx, gr);
     }
     // capture this application (thread-local: other threads' CUDA calls are
-    // unaffected), then replay it
-    const long long l0 = ctx->launches;
+    // unaffected), then replay it.  The profiling events it records are made
+    // before the capture so that none is created inside it.
+    if (ctx->prof)
+        while (ctx->prof_ev.size() < ctx->prof_used + 512) {
+            cudaEvent_t ev;
+            FHD_CUDA_TRY(cudaEventCreate(&ev));
+            ctx->prof_ev.push_back(ev);
+        }
+    const long long l0 = ctx->launches, pl0 = ctx->prof_launches;
     const int v0 = ctx->vcycles;
+    const size_t pu0 = ctx->prof_used;
+    const double pb0 = ctx->prof_bytes;
     if (cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
         cudaGetLastError();
         return precon(ctx, b, x);
     }
+    ctx->capturing = true;
+    ctx->cap_fail = false;
+    ctx->cap_nodes.clear();
     int rc = precon(ctx, b, x);
+    ctx->capturing = false;
     cudaGraph_t graph = nullptr;
     cudaError_t e = cudaStreamEndCapture(ctx->stream, &graph);
     cudaGraphExec_t exec = nullptr;
-    if (!rc && e == cudaSuccess && graph) e = cudaGraphInstantiate(&exec, graph, 0);
-    if (graph) cudaGraphDestroy(graph);
-    const long long n = ctx->launches - l0;
+    if (!rc && e == cudaSuccess && graph && !ctx->cap_fail) e = cudaGraphInstantiate(&exec, graph, 0);
+    fhd_ctx::PreconGraph gr;
+    gr.key = key;
+    gr.launches = ctx->launches - l0;
+    gr.vcycles = ctx->vcycles - v0;
+    gr.prof_launches = ctx->prof_launches - pl0;
+    gr.prof_bytes = ctx->prof_bytes - pb0;
+    gr.ev_nodes = ctx->cap_nodes;
+    // nothing ran during the capture: undo its counts (the replay adds them)
     ctx->launches = l0;
-    if (rc || e != cudaSuccess || !exec) {
+    ctx->vcycles = v0;
+    ctx->prof_launches = pl0;
+    ctx->prof_bytes = pb0;
+    ctx->prof_used = pu0;
+    if (rc || e != cudaSuccess || !exec || ctx->cap_fail) {
         // not capturable here: run it directly
         cudaGetLastError();
         if (exec) cudaGraphExecDestroy(exec);
-        ctx->vcycles = v0;
+        if (graph) cudaGraphDestroy(graph);
         if (rc) return rc;
         ctx->graph_mode = 0;
         return precon(ctx, b, x);
     }
+    // the template graph stays alive while its event nodes are re-pointed
+    if (gr.ev_nodes.empty()) {
+        cudaGraphDestroy(graph);
+        graph = nullptr;
+    }
+    gr.exec = exec;
+    gr.graph = graph;
+    gr.used = ctx->graph_clock;
     if (ctx->graphs.size() >= GRAPH_CACHE) {
         auto it = std::min_element(ctx->graphs.begin(), ctx->graphs.end(),
                                    [](const fhd_ctx::PreconGraph& a, const fhd_ctx::PreconGraph& b2) {
                                        return a.used < b2.used;
                                    });
-        cudaGraphExecDestroy(it->exec);
+        drop_graph(*it);
         ctx->graphs.erase(it);
     }
-    ctx->graphs.push_back({key, exec, n, ctx->vcycles - v0, ctx->graph_clock});
-    FHD_CUDA_TRY(cudaGraphLaunch(exec, ctx->stream));
-    ctx->launches += n;
-    return 0;
+    ctx->graphs.push_back(gr);
+    return replay(ctx, ctx->graphs.back());
 }
 
 // ---------------------------------------------------------------------

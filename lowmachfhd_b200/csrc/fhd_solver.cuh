@@ -234,14 +234,21 @@ struct fhd_ctx {
     // 1 on)
     int graph_mode = -1;
     struct PreconGraph {
-        unsigned long long key;
-        cudaGraphExec_t exec;
-        long long launches;
-        int vcycles;
-        long long used;
+        unsigned long long key = 0;
+        cudaGraphExec_t exec = nullptr;
+        cudaGraph_t graph = nullptr;             // kept while ev_nodes is not empty
+        std::vector<cudaGraphNode_t> ev_nodes;   // profiling records, capture order
+        long long launches = 0;
+        int vcycles = 0;
+        long long prof_launches = 0;
+        double prof_bytes = 0.0;
+        long long used = 0;
     };
     std::vector<PreconGraph> graphs;
     long long graph_clock = 0;
+    bool capturing = false;
+    bool cap_fail = false;
+    std::vector<cudaGraphNode_t> cap_nodes;
     // optional timing of the finest-level smoother launches (CUDA events on
     // the context stream) with their algorithmic bytes
     bool prof = false;
