@@ -70,7 +70,9 @@ def test_stag_mg_one_vcycle(cuda, dim, n, visc):
 # red-black smoothers (64x16 tiles; 96 -> 48-wide, 40 -> 10-high tiles), with
 # uncoupled and coupled viscous operators, through one V-cycle and through
 # the preconditioner (which adds the pressure multigrid)
-TILED = [(1, [128, 32, 64]), (-1, [96, 40, 24]), (2, [64, 48, 32]), (-3, [96, 40, 24])]
+TILED = [(1, [128, 32, 64]), (-1, [96, 40, 24]), (2, [64, 48, 32]), (-3, [96, 40, 24]),
+         # above 96^3 cells the colour sweeps update two z-planes per thread
+         (1, [96, 96, 96]), (-1, [128, 96, 80])]
 
 
 @pytest.mark.parametrize("visc,n", TILED)
@@ -86,7 +88,7 @@ def test_stag_mg_tiled(cuda, visc, n):
     assert P.rel_inf(host(phi), ref) < 1e-12
 
 
-@pytest.mark.parametrize("visc,n", TILED[:2])
+@pytest.mark.parametrize("visc,n", TILED[:2] + TILED[4:5])
 def test_apply_precon_tiled(cuda, visc, n):
     dim = 3
     pb = P.problem(dim, n, visc, dx=1.0, seed=10)
