@@ -36,6 +36,37 @@ struct Cell {
     }
 };
 
+// A cell with its linear index and the six periodic +-1 offsets worked out
+// once; id() of a unit offset (compile-time at every call) is then one or
+// two additions instead of three wraps and a 64-bit index product.  Gives
+// the same indices as Cell.
+struct CellF {
+    int i, j, k;
+    i64 base;
+    int oxm, oxp, oym, oyp, ozm, ozp;
+    __device__ __forceinline__ void set(const Grid& g, int i_, int j_, int k_) {
+        i = i_; j = j_; k = k_;
+        const int nx = g.n[0], ny = g.n[1], nz = g.n[2], nxy = nx * ny;
+        base = (i64)i + (i64)nx * ((i64)j + (i64)ny * k);
+        oxm = i == 0 ? nx - 1 : -1;
+        oxp = i == nx - 1 ? 1 - nx : 1;
+        oym = j == 0 ? (ny - 1) * nx : -nx;
+        oyp = j == ny - 1 ? (1 - ny) * nx : nx;
+        ozm = k == 0 ? (nz - 1) * nxy : -nxy;
+        ozp = k == nz - 1 ? (1 - nz) * nxy : nxy;
+    }
+    __device__ __forceinline__ i64 id(int di, int dj, int dk) const {
+        i64 r = base;
+        if (di < 0) r += oxm;
+        else if (di > 0) r += oxp;
+        if (dj < 0) r += oym;
+        else if (dj > 0) r += oyp;
+        if (dk < 0) r += ozm;
+        else if (dk > 0) r += ozp;
+        return r;
+    }
+};
+
 template <typename T>
 __device__ __forceinline__ T ld(const T* p, i64 i) { return __ldg(p + i); }
 
@@ -73,8 +104,8 @@ struct Off {
 // operator kernel evaluates this one expression, so a value computed from
 // shared-memory planes equals the one computed from global memory bit for
 // bit.
-template <typename T, int DIM, int VISC, int C, class Own, class Oth, class Alp>
-__device__ __forceinline__ T stag_lface_acc(const StagOp<T>& A, const Cell& P, Own own, Oth oth, Alp alp,
+template <typename T, int DIM, int VISC, int C, class CellT, class Own, class Oth, class Alp>
+__device__ __forceinline__ T stag_lface_acc(const StagOp<T>& A, const CellT& P, Own own, Oth oth, Alp alp,
                                             T& diag) {
     constexpr int ex = (C == 0), ey = (C == 1), ez = (C == 2);
     const i64 f = P.id(0, 0, 0);
@@ -146,8 +177,8 @@ __device__ __forceinline__ T stag_lface_acc(const StagOp<T>& A, const Cell& P, O
 }
 
 // the operator on global-memory velocity arrays
-template <typename T, int DIM, int VISC, int C>
-__device__ __forceinline__ T stag_lface(const StagOp<T>& A, const T* const* phi, const Cell& P, T& diag) {
+template <typename T, int DIM, int VISC, int C, class CellT>
+__device__ __forceinline__ T stag_lface(const StagOp<T>& A, const T* const* phi, const CellT& P, T& diag) {
     const T* pc = phi[C];
     return stag_lface_acc<T, DIM, VISC, C>(
         A, P, [&](int a, int b, int c) { return ld(pc, P.id(a, b, c)); },
@@ -155,11 +186,18 @@ __device__ __forceinline__ T stag_lface(const StagOp<T>& A, const T* const* phi,
         [&]() { return ld(A.alpha[C], P.id(0, 0, 0)); }, diag);
 }
 
-template <typename T, int DIM, int VISC>
-__device__ __forceinline__ T stag_lface_c(int c, const StagOp<T>& A, const T* const* phi, const Cell& P, T& diag) {
+template <typename T, int DIM, int VISC, class CellT>
+__device__ __forceinline__ T stag_lface_c(int c, const StagOp<T>& A, const T* const* phi, const CellT& P, T& diag) {
     if (c == 0) return stag_lface<T, DIM, VISC, 0>(A, phi, P, diag);
     if (DIM == 3 && c == 2) return stag_lface<T, DIM, VISC, (DIM == 3 ? 2 : 1)>(A, phi, P, diag);
     return stag_lface<T, DIM, VISC, 1>(A, phi, P, diag);
+}
+
+__device__ __forceinline__ bool cellf_of_thread(const Grid& g, CellF& P) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i >= g.n[0] || j >= g.n[1]) return false;
+    P.set(g, i, j, blockIdx.z);
+    return true;
 }
 
 __device__ __forceinline__ bool cell_of_thread(const Grid& g, Cell& P) {
@@ -180,8 +218,8 @@ __global__ void __launch_bounds__(256) k_stag_apply(Grid g, StagOp<T> A, const T
                                                     const T* __restrict__ p1, const T* __restrict__ p2,
                                                     T* o0, T* o1, T* o2, const T* r0, const T* r1, const T* r2,
                                                     int mode) {
-    Cell P;
-    if (!cell_of_thread(g, P)) return;
+    CellF P;
+    if (!cellf_of_thread(g, P)) return;
     const T* phi[3] = {p0, p1, p2};
     T* out[3] = {o0, o1, o2};
     const T* rhs[3] = {r0, r1, r2};
@@ -203,14 +241,13 @@ __global__ void __launch_bounds__(256) k_stag_apply(Grid g, StagOp<T> A, const T
 template <typename T, int DIM, int VISC, int C>
 __global__ void __launch_bounds__(256) k_stag_gs(Grid g, StagOp<T> A, T* p0, T* p1, T* p2,
                                                  const T* __restrict__ r, int par, T omega) {
-    Cell P;
-    P.nx = g.n[0]; P.ny = g.n[1]; P.nz = g.n[2];
     const int ih = blockIdx.x * blockDim.x + threadIdx.x;
-    P.j = blockIdx.y * blockDim.y + threadIdx.y;
-    P.k = blockIdx.z;
-    if (P.j >= P.ny) return;
-    P.i = 2 * ih + ((P.j + P.k + par) & 1);
-    if (P.i >= P.nx) return;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.z;
+    if (j >= g.n[1]) return;
+    const int i = 2 * ih + ((j + k + par) & 1);
+    if (i >= g.n[0]) return;
+    CellF P;
+    P.set(g, i, j, k);
     const T* phi[3] = {p0, p1, p2};
     T* pc = (C == 0) ? p0 : (C == 1 ? p1 : p2);
     const i64 f = P.id(0, 0, 0);
@@ -397,8 +434,8 @@ struct CCOp {
 // D a G phi at cell P and its diagonal; phi through the accessor
 // ph(dx,dy,dz) relative to P (global memory or shared-memory planes, one
 // expression for both)
-template <typename T, int DIM, class Acc>
-__device__ __forceinline__ T cc_lap_acc(const CCOp<T>& A, const Cell& P, Acc ph, T& diag) {
+template <typename T, int DIM, class CellT, class Acc>
+__device__ __forceinline__ T cc_lap_acc(const CCOp<T>& A, const CellT& P, Acc ph, T& diag) {
     const i64 f = P.id(0, 0, 0);
     const T pc = ph(0, 0, 0);
     T s = T(0), dg = T(0);
@@ -414,22 +451,21 @@ __device__ __forceinline__ T cc_lap_acc(const CCOp<T>& A, const Cell& P, Acc ph,
     return s * A.q;
 }
 
-template <typename T, int DIM>
-__device__ __forceinline__ T cc_lap(const CCOp<T>& A, const T* phi, const Cell& P, T& diag) {
+template <typename T, int DIM, class CellT>
+__device__ __forceinline__ T cc_lap(const CCOp<T>& A, const T* phi, const CellT& P, T& diag) {
     return cc_lap_acc<T, DIM>(A, P, [&](int a, int b, int c) { return ld(phi, P.id(a, b, c)); }, diag);
 }
 
 // red-black Gauss-Seidel, one colour, fused; thread per cell of the colour
 template <typename T, int DIM>
 __global__ void __launch_bounds__(256) k_cc_gsrb(Grid g, CCOp<T> A, T* phi, const T* __restrict__ rhs, int par) {
-    Cell P;
-    P.nx = g.n[0]; P.ny = g.n[1]; P.nz = g.n[2];
     const int ih = blockIdx.x * blockDim.x + threadIdx.x;
-    P.j = blockIdx.y * blockDim.y + threadIdx.y;
-    P.k = blockIdx.z;
-    if (P.j >= P.ny) return;
-    P.i = 2 * ih + ((P.j + P.k + par) & 1);
-    if (P.i >= P.nx) return;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.z;
+    if (j >= g.n[1]) return;
+    const int i = 2 * ih + ((j + k + par) & 1);
+    if (i >= g.n[0]) return;
+    CellF P;
+    P.set(g, i, j, k);
     T dg;
     const T L = cc_lap<T, DIM>(A, phi, P, dg);
     const i64 f = P.id(0, 0, 0);

@@ -177,8 +177,8 @@ static __global__ void __launch_bounds__(256) k_recip(i64 n, T* o, const double*
 template <int DIM, int VISC>
 static __global__ void __launch_bounds__(256) k_stokes_apply(Grid g, StagOp<double> A, CSVec<double> x, CSVec<double> rhs,
                                                       SVec<double> out, int mode, double dxinv) {
-    Cell P;
-    if (!cell_of_thread(g, P)) return;
+    CellF P;
+    if (!cellf_of_thread(g, P)) return;
     const double* phi[3] = {x.c[0], x.c[1], DIM == 3 ? x.c[2] : nullptr};
     const double* p = x.c[DIM];
     const i64 f = P.id(0, 0, 0);
