@@ -70,6 +70,15 @@ struct CellF {
 template <typename T>
 __device__ __forceinline__ T ld(const T* p, i64 i) { return __ldg(p + i); }
 
+// x / d of a smoother update: the IEEE quotient in FP64 (bit-identical to
+// the oracle); the fast approximate quotient in the FP32 preconditioner,
+// where its last-bit error is noise
+template <typename T>
+__device__ __forceinline__ T sm_quot(T x, T d) {
+    if constexpr (sizeof(T) == 4) return __fdividef(x, d);
+    else return x / d;
+}
+
 // Pointers of one staggered operator level.  alpha is multiplied by
 // alpha_scale on the fly (theta_alpha on the finest level).
 template <typename T>
@@ -253,7 +262,7 @@ __global__ void __launch_bounds__(256) k_stag_gs(Grid g, StagOp<T> A, T* p0, T* 
     const i64 f = P.id(0, 0, 0);
     T dg;
     const T L = stag_lface<T, DIM, VISC, C>(A, phi, P, dg);
-    pc[f] = pc[f] + omega * (ld(r, f) - L) / dg;
+    pc[f] = pc[f] + sm_quot(omega * (ld(r, f) - L), dg);
 }
 
 // Two-pass colour smoother for levels with an odd extent or the Jacobi
@@ -294,7 +303,7 @@ __global__ void __launch_bounds__(256) k_stag_color_update(Grid g, T* p0, T* p1,
 #pragma unroll
     for (int c = 0; c < DIM; c++) {
         if (color != 0 && ((color - 1) / 2 != c || par != ((color + 1) & 1))) continue;
-        ph[c][f] = ph[c][f] + omega * (rh[c][f] - Lo[c][f]) / Do[c][f];
+        ph[c][f] = ph[c][f] + sm_quot(omega * (rh[c][f] - Lo[c][f]), Do[c][f]);
     }
 }
 
@@ -469,7 +478,7 @@ __global__ void __launch_bounds__(256) k_cc_gsrb(Grid g, CCOp<T> A, T* phi, cons
     T dg;
     const T L = cc_lap<T, DIM>(A, phi, P, dg);
     const i64 f = P.id(0, 0, 0);
-    phi[f] = phi[f] + (ld(rhs, f) - L) / dg;
+    phi[f] = phi[f] + sm_quot(ld(rhs, f) - L, dg);
 }
 
 // two-pass colour for odd extents: store the correction, then add it
@@ -482,7 +491,7 @@ __global__ void __launch_bounds__(256) k_cc_color_corr(Grid g, CCOp<T> A, const 
     T dg;
     const T L = cc_lap<T, DIM>(A, phi, P, dg);
     const i64 f = P.id(0, 0, 0);
-    corr[f] = (ld(rhs, f) - L) / dg;
+    corr[f] = sm_quot(ld(rhs, f) - L, dg);
 }
 
 template <typename T>
