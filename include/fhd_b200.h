@@ -151,6 +151,14 @@ int  fhd_ctx_set_stream(fhd_ctx* ctx, void* stream);
  * runs more than one V-cycle per application).  fhd_ctx_profile timing
  * works in both modes. */
 int fhd_ctx_set_graphs(fhd_ctx* ctx, int mode);
+/* The coarse end of both multigrid V-cycles (every level from the first
+ * whose unknowns, right-hand sides and residuals fit in one SM's shared
+ * memory down to the bottom) as one single-block kernel per V-cycle instead
+ * of one launch per smoother colour and transfer (mode 1 or -1 default: on,
+ * 0: per-level launches).  Same arithmetic either way.  Replaces no
+ * reference routine: the levels are those of stag_mg_solver.f90:301-599 and
+ * of the pressure multigrid behind macproject.f90:294-298. */
+int fhd_ctx_set_coarse(fhd_ctx* ctx, int mode);
 /* Number of this library's kernels launched through ctx so far. */
 long long fhd_ctx_kernel_launches(fhd_ctx* ctx);
 const char* fhd_status_string(int status);

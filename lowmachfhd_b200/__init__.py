@@ -110,6 +110,11 @@ class StokesSolver:
         0 off, -1 default"""
         check(lib().fhd_ctx_set_graphs(self._h, int(mode)), "fhd_ctx_set_graphs")
 
+    def set_coarse(self, mode: int):
+        """coarse multigrid levels in one single-block kernel per V-cycle: 1
+        or -1 (default) on, 0 one launch per smoother colour and transfer"""
+        check(lib().fhd_ctx_set_coarse(self._h, int(mode)), "fhd_ctx_set_coarse")
+
     def profile(self, enable: bool = True):
         """time the finest-level smoother launches with CUDA events"""
         check(lib().fhd_ctx_profile(self._h, int(enable)), "fhd_ctx_profile")

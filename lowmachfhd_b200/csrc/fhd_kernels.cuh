@@ -308,8 +308,57 @@ __global__ void __launch_bounds__(256) k_stag_color_update(Grid g, T* p0, T* p1,
 }
 
 // stag_restriction (stag_mg_solver.f90:1028-1170): 6-point (2D) / 12-point
-// (3D) full stencil, or the 2/4-point 'simple' stencil.  Thread per coarse
-// cell, all components.
+// (3D) full stencil, or the 2/4-point 'simple' stencil, of one component.
+// The fine values come through at(o, pa, pb): the fine face at offset o
+// along the component and pa, pb along the two other directions from the
+// fine cell 2Q of coarse cell Q.
+template <typename T, int DIM, class At>
+__device__ __forceinline__ T stag_restrict_expr(int simple, At at) {
+    if constexpr (DIM == 2) {
+        if (simple) return T(0.5) * (at(0, 0, 0) + at(0, 1, 0));
+        return T(0.25) * (at(0, 0, 0) + at(0, 1, 0)) +
+               T(0.125) * (at(1, 0, 0) + at(1, 1, 0) + at(-1, 0, 0) + at(-1, 1, 0));
+    } else {
+        if (simple) return T(0.25) * (at(0, 0, 0) + at(0, 1, 0) + at(0, 0, 1) + at(0, 1, 1));
+        return T(0.125) * (at(0, 0, 0) + at(0, 1, 0) + at(0, 0, 1) + at(0, 1, 1)) +
+               T(0.0625) * (at(1, 0, 0) + at(1, 1, 0) + at(1, 0, 1) + at(1, 1, 1)) +
+               T(0.0625) * (at(-1, 0, 0) + at(-1, 1, 0) + at(-1, 0, 1) + at(-1, 1, 1));
+    }
+}
+
+// stag_prolongation (stag_mg_solver.f90:1419-1628) of one component at a
+// fine face: coarse values through at(o, pa, pb) relative to the parent
+// cell; even = the face lies on a coarse face; oa, ob = the side of the
+// neighbouring coarse row in the two other directions
+template <typename T, int DIM, class At>
+__device__ __forceinline__ T stag_prolong_expr(bool even, int oa, int ob, At at) {
+    if constexpr (DIM == 2) {
+        if (even) return T(0.75) * at(0, 0, 0) + T(0.25) * at(0, oa, 0);
+        return T(0.375) * at(0, 0, 0) + T(0.125) * at(0, oa, 0) + T(0.375) * at(1, 0, 0) + T(0.125) * at(1, oa, 0);
+    } else {
+        if (even)
+            return T(9.0 / 16.0) * at(0, 0, 0) + T(3.0 / 16.0) * at(0, oa, 0) + T(3.0 / 16.0) * at(0, 0, ob) +
+                   T(1.0 / 16.0) * at(0, oa, ob);
+        return T(9.0 / 32.0) * at(0, 0, 0) + T(3.0 / 32.0) * at(0, oa, 0) + T(3.0 / 32.0) * at(0, 0, ob) +
+               T(1.0 / 32.0) * at(0, oa, ob) + T(9.0 / 32.0) * at(1, 0, 0) + T(3.0 / 32.0) * at(1, oa, 0) +
+               T(3.0 / 32.0) * at(1, 0, ob) + T(1.0 / 32.0) * at(1, oa, ob);
+    }
+}
+
+// fine face (or coarse cell) of component c at the offset (o, pa, pb) in
+// component-relative directions: the linear index through Cell X
+template <int DIM>
+__device__ __forceinline__ i64 comp_off_id(const Cell& X, int c, int o, int pa, int pb) {
+    const int a = (c == 0) ? 1 : 0;
+    const int b = (c == 2) ? 1 : 2;
+    int off[3] = {0, 0, 0};
+    off[c] += o;
+    off[a] += pa;
+    if (DIM == 3) off[b] += pb;
+    return X.id(off[0], off[1], off[2]);
+}
+
+// Thread per coarse cell, all components.
 template <typename T, int DIM>
 __global__ void __launch_bounds__(256) k_stag_restrict(Grid gf, Grid gc, const T* f0, const T* f1, const T* f2,
                                                        T* c0, T* c1, T* c2, int simple) {
@@ -324,31 +373,12 @@ __global__ void __launch_bounds__(256) k_stag_restrict(Grid gf, Grid gc, const T
 #pragma unroll
     for (int c = 0; c < DIM; c++) {
         const T* Fp = fi[c];
-        const int a = (c == 0) ? 1 : 0;
-        const int b = (c == 2) ? 1 : 2;
-        auto at = [&](int o, int pa, int pb) {
-            int off[3] = {0, 0, 0};
-            off[c] += o;
-            off[a] += pa;
-            if (DIM == 3) off[b] += pb;
-            return ld(Fp, F.id(off[0], off[1], off[2]));
-        };
-        T v;
-        if constexpr (DIM == 2) {
-            if (simple) v = T(0.5) * (at(0, 0, 0) + at(0, 1, 0));
-            else v = T(0.25) * (at(0, 0, 0) + at(0, 1, 0)) +
-                     T(0.125) * (at(1, 0, 0) + at(1, 1, 0) + at(-1, 0, 0) + at(-1, 1, 0));
-        } else {
-            if (simple) v = T(0.25) * (at(0, 0, 0) + at(0, 1, 0) + at(0, 0, 1) + at(0, 1, 1));
-            else v = T(0.125) * (at(0, 0, 0) + at(0, 1, 0) + at(0, 0, 1) + at(0, 1, 1)) +
-                     T(0.0625) * (at(1, 0, 0) + at(1, 1, 0) + at(1, 0, 1) + at(1, 1, 1)) +
-                     T(0.0625) * (at(-1, 0, 0) + at(-1, 1, 0) + at(-1, 0, 1) + at(-1, 1, 1));
-        }
-        co[c][qc] = v;
+        co[c][qc] = stag_restrict_expr<T, DIM>(
+            simple, [&](int o, int pa, int pb) { return ld(Fp, comp_off_id<DIM>(F, c, o, pa, pb)); });
     }
 }
 
-// stag_prolongation (stag_mg_solver.f90:1419-1628): fine += P coarse.
+// fine += P coarse, thread per fine cell, all components.
 template <typename T, int DIM>
 __global__ void __launch_bounds__(256) k_stag_prolong(Grid gf, Grid gc, T* f0, T* f1, T* f2, const T* c0,
                                                       const T* c1, const T* c2) {
@@ -368,26 +398,9 @@ __global__ void __launch_bounds__(256) k_stag_prolong(Grid gf, Grid gc, T* f0, T
         const int b = (c == 2) ? 1 : 2;
         const int oa = (I[a] & 1) ? 1 : -1;
         const int ob = (DIM == 3) ? ((I[b] & 1) ? 1 : -1) : 0;
-        auto at = [&](int o, int pa, int pb) {
-            int off[3] = {0, 0, 0};
-            off[c] += o;
-            off[a] += pa;
-            if (DIM == 3) off[b] += pb;
-            return ld(Cp, H.id(off[0], off[1], off[2]));
-        };
-        const bool even = (I[c] & 1) == 0;
-        T v;
-        if constexpr (DIM == 2) {
-            if (even) v = T(0.75) * at(0, 0, 0) + T(0.25) * at(0, oa, 0);
-            else v = T(0.375) * at(0, 0, 0) + T(0.125) * at(0, oa, 0) + T(0.375) * at(1, 0, 0) +
-                     T(0.125) * at(1, oa, 0);
-        } else {
-            if (even) v = T(9.0 / 16.0) * at(0, 0, 0) + T(3.0 / 16.0) * at(0, oa, 0) + T(3.0 / 16.0) * at(0, 0, ob) +
-                          T(1.0 / 16.0) * at(0, oa, ob);
-            else v = T(9.0 / 32.0) * at(0, 0, 0) + T(3.0 / 32.0) * at(0, oa, 0) + T(3.0 / 32.0) * at(0, 0, ob) +
-                     T(1.0 / 32.0) * at(0, oa, ob) + T(9.0 / 32.0) * at(1, 0, 0) + T(3.0 / 32.0) * at(1, oa, 0) +
-                     T(3.0 / 32.0) * at(1, 0, ob) + T(1.0 / 32.0) * at(1, oa, ob);
-        }
+        const T v = stag_prolong_expr<T, DIM>((I[c] & 1) == 0, oa, ob, [&](int o, int pa, int pb) {
+            return ld(Cp, comp_off_id<DIM>(H, c, o, pa, pb));
+        });
         fo[c][f] = fo[c][f] + v;
     }
 }
@@ -503,13 +516,12 @@ __global__ void __launch_bounds__(256) k_cc_color_add(Grid g, T* phi, const T* c
     phi[f] = phi[f] + corr[f];
 }
 
-// residual on the 2^dim children of a coarse cell, averaged into the coarse
-// rhs (residual + restriction in one pass; every fine cell once)
-template <typename T, int DIM>
-__global__ void __launch_bounds__(256) k_cc_resid_restrict(Grid gf, Grid gc, CCOp<T> A, const T* phi, const T* rhs,
-                                                           T* crhs) {
-    Cell Q;
-    if (!cell_of_thread(gc, Q)) return;
+// residual on the 2^dim children of coarse cell (qi, qj, qk), averaged:
+// the coarse rhs (residual + restriction in one pass; every fine cell once).
+// phi_at / rhs_at read the fine arrays by linear index.
+template <typename T, int DIM, class PhiAt, class RhsAt>
+__device__ __forceinline__ T cc_resid_avg(const CCOp<T>& A, const Grid& gf, int qi, int qj, int qk, PhiAt phi_at,
+                                          RhsAt rhs_at) {
     Cell P;
     P.nx = gf.n[0]; P.ny = gf.n[1]; P.nz = gf.n[2];
     T acc = T(0);
@@ -520,12 +532,21 @@ __global__ void __launch_bounds__(256) k_cc_resid_restrict(Grid gf, Grid gc, CCO
         for (int dj = 0; dj < 2; dj++)
 #pragma unroll
             for (int di = 0; di < 2; di++) {
-                P.i = 2 * Q.i + di; P.j = 2 * Q.j + dj; P.k = (DIM == 3) ? 2 * Q.k + dk : 0;
+                P.i = 2 * qi + di; P.j = 2 * qj + dj; P.k = (DIM == 3) ? 2 * qk + dk : 0;
                 T dg;
-                const T L = cc_lap<T, DIM>(A, phi, P, dg);
-                acc += ld(rhs, P.id(0, 0, 0)) - L;
+                const T L = cc_lap_acc<T, DIM>(A, P, [&](int a, int b, int c) { return phi_at(P.id(a, b, c)); }, dg);
+                acc += rhs_at(P.id(0, 0, 0)) - L;
             }
-    crhs[Q.id(0, 0, 0)] = acc * (DIM == 3 ? T(0.125) : T(0.25));
+    return acc * (DIM == 3 ? T(0.125) : T(0.25));
+}
+
+template <typename T, int DIM>
+__global__ void __launch_bounds__(256) k_cc_resid_restrict(Grid gf, Grid gc, CCOp<T> A, const T* phi, const T* rhs,
+                                                           T* crhs) {
+    Cell Q;
+    if (!cell_of_thread(gc, Q)) return;
+    crhs[Q.id(0, 0, 0)] = cc_resid_avg<T, DIM>(
+        A, gf, Q.i, Q.j, Q.k, [&](i64 i) { return ld(phi, i); }, [&](i64 i) { return ld(rhs, i); });
 }
 
 template <typename T, int DIM>

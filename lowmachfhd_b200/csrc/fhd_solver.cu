@@ -12,6 +12,7 @@
 #include <map>
 
 #include "fhd_solver.cuh"
+#include "fhd_coarse.cuh"
 
 namespace fhd {
 
@@ -485,14 +486,95 @@ static int stag_residual(fhd_ctx* ctx, StagLevel<T>& L) {
     return rc;
 }
 
+// shared memory one coarse kernel may take: the device's opt-in limit less a
+// margin for the L1 that caches the coefficients
+static size_t coarse_smem_cap() {
+    int dev = 0, optin = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+    if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) return 0;
+    const size_t cap = 200 * 1024;
+    return (size_t)optin < cap ? (size_t)optin : cap;
+}
+
+// first level of a hierarchy of n levels that the single-CTA coarse kernel
+// takes over (every level from it to the bottom fits the shared-memory
+// cap; level l needs bytes(l)); n when none does or the mode is off
+template <class F>
+static int coarse_first(fhd_ctx* ctx, int n, F bytes) {
+    if (ctx->coarse_mode == 0) return n;
+    const size_t cap = coarse_smem_cap();
+    size_t tot = 0;
+    int lc = n;
+    for (int l = n - 1; l >= 0 && n - l <= CS_MAXL; l--) {
+        tot += bytes(l);
+        if (tot > cap) break;
+        lc = l;
+    }
+    return lc;
+}
+
+template <typename T>
+static int stag_coarse_first(fhd_ctx* ctx, Multigrid<T>& M) {
+    const int dim = ctx->dim;
+    return coarse_first(ctx, (int)M.s.size(),
+                        [&](int l) { return (size_t)(3 * dim) * (size_t)M.s[l].g.nc * sizeof(T); });
+}
+
+template <typename T>
+static int cc_coarse_first(fhd_ctx* ctx, Multigrid<T>& M) {
+    return coarse_first(ctx, (int)M.c.size(), [&](int l) { return (size_t)3 * (size_t)M.c[l].g.nc * sizeof(T); });
+}
+
+// levels lc..bottom of the staggered V-cycle in one CTA: phi of level lc in
+// global memory is the input (lc == 0) or zero, and holds the result
+template <typename T>
+static int stag_coarse(fhd_ctx* ctx, Multigrid<T>& M, int lc) {
+    const int nl = (int)M.s.size();
+    const int dim = ctx->dim;
+    StagCoarseArgs<T> a;
+    memset(&a, 0, sizeof a);
+    a.nlev = nl - lc;
+    a.load_phi = lc == 0;
+    a.n_down = ctx->p.stag_mg_nsmooths_down;
+    a.n_up = ctx->p.stag_mg_nsmooths_up;
+    a.n_bottom = ctx->p.stag_mg_nsmooths_bottom;
+    a.jacobi = ctx->p.stag_mg_smoother == 0;
+    a.omega = (T)ctx->p.stag_mg_omega;
+    for (int c = 0; c < dim; c++) {
+        a.phi[c] = M.s[lc].phi[c];
+        a.rhs[c] = M.s[lc].rhs[c];
+    }
+    size_t off = 0;
+    for (int m = 0; m < a.nlev; m++) {
+        const StagLevel<T>& L = M.s[lc + m];
+        a.g[m] = L.g;
+        a.A[m] = L.op();
+        a.off[m] = (int)off;
+        off += (size_t)(3 * dim) * (size_t)L.g.nc;
+    }
+    const size_t smem = off * sizeof(T);
+    int rc = 0;
+    with_dim_visc(dim, ctx->visc, [&](auto D, auto V) {
+        constexpr int DIM = decltype(D)::value, VISC = decltype(V)::value;
+        rc |= rb_allow_smem(k_stag_coarse<T, DIM, VISC>, smem);
+        if (rc) return;
+        k_stag_coarse<T, DIM, VISC><<<1, CS_THREADS, smem, ctx->stream>>>(a);
+        rc |= post(ctx);
+    });
+    return rc;
+}
+
 template <typename T>
 static int stag_vcycle(fhd_ctx* ctx, Multigrid<T>& M) {
     const int nl = (int)M.s.size();
     const int dim = ctx->dim;
     cudaStream_t st = ctx->stream;
-    for (int l = 1; l < nl; l++)
+    // levels from lc down run in the coarse kernel, which zeroes their phi
+    const int lc = stag_coarse_first(ctx, M);
+    const int lt = lc < nl - 1 ? lc : nl - 1;  // last level of the per-level descent
+    for (int l = 1; l < lc; l++)
         for (int c = 0; c < dim; c++) FHD_CUDA_TRY(cudaMemsetAsync(M.s[l].phi[c], 0, sizeof(T) * M.s[l].g.nc, st));
-    for (int l = 0; l < nl - 1; l++) {
+    for (int l = 0; l < lt; l++) {
         StagLevel<T>& L = M.s[l];
         StagLevel<T>& C = M.s[l + 1];
         int rc = stag_smooths(ctx, L, ctx->p.stag_mg_nsmooths_down);
@@ -507,9 +589,9 @@ static int stag_vcycle(fhd_ctx* ctx, Multigrid<T>& M) {
         });
         if (rc) return rc;
     }
-    int rc = stag_smooths(ctx, M.s[nl - 1], ctx->p.stag_mg_nsmooths_bottom);
+    int rc = lc < nl ? stag_coarse(ctx, M, lc) : stag_smooths(ctx, M.s[nl - 1], ctx->p.stag_mg_nsmooths_bottom);
     if (rc) return rc;
-    for (int l = nl - 2; l >= 0; l--) {
+    for (int l = lt - 1; l >= 0; l--) {
         StagLevel<T>& L = M.s[l];
         StagLevel<T>& C = M.s[l + 1];
         with_dim(dim, [&](auto D) {
@@ -660,10 +742,46 @@ static int cc_smooths(fhd_ctx* ctx, CCLevel<T>& C, int count) {
     return 0;
 }
 
+// levels lc..bottom of the pressure V-cycle in one CTA (phi of level lc:
+// input when lc == 0, else zero; holds the result)
 template <typename T>
-static int cc_vcycle(fhd_ctx* ctx, Multigrid<T>& M, int l) {
+static int cc_coarse(fhd_ctx* ctx, Multigrid<T>& M, int lc) {
+    const int nl = (int)M.c.size();
+    CCCoarseArgs<T> a;
+    memset(&a, 0, sizeof a);
+    a.nlev = nl - lc;
+    a.load_phi = lc == 0;
+    a.n_down = ctx->p.mg_nsmooths_down;
+    a.n_up = ctx->p.mg_nsmooths_up;
+    a.n_bottom = ctx->p.mg_nsmooths_bottom;
+    a.phi = M.c[lc].phi;
+    a.rhs = M.c[lc].rhs;
+    size_t off = 0;
+    for (int m = 0; m < a.nlev; m++) {
+        const CCLevel<T>& C = M.c[lc + m];
+        a.g[m] = C.g;
+        a.A[m] = C.op();
+        a.off[m] = (int)off;
+        off += (size_t)3 * (size_t)C.g.nc;
+    }
+    const size_t smem = off * sizeof(T);
+    int rc = 0;
+    with_dim(ctx->dim, [&](auto D) {
+        constexpr int DIM = decltype(D)::value;
+        rc |= rb_allow_smem(k_cc_coarse<T, DIM>, smem);
+        if (rc) return;
+        k_cc_coarse<T, DIM><<<1, CS_THREADS, smem, ctx->stream>>>(a);
+        rc |= post(ctx);
+    });
+    return rc;
+}
+
+// V-cycle from level l; levels from lc down run in the coarse kernel
+template <typename T>
+static int cc_vcycle(fhd_ctx* ctx, Multigrid<T>& M, int l, int lc) {
     const int nl = (int)M.c.size();
     CCLevel<T>& C = M.c[l];
+    if (l == lc) return cc_coarse(ctx, M, lc);
     if (l == nl - 1) return cc_smooths(ctx, C, ctx->p.mg_nsmooths_bottom);
     {
         int rc = cc_smooths(ctx, C, ctx->p.mg_nsmooths_down);
@@ -678,8 +796,8 @@ static int cc_vcycle(fhd_ctx* ctx, Multigrid<T>& M, int l) {
         rc |= post(ctx);
     });
     if (rc) return rc;
-    FHD_CUDA_TRY(cudaMemsetAsync(D.phi, 0, sizeof(T) * D.g.nc, ctx->stream));
-    rc = cc_vcycle(ctx, M, l + 1);
+    if (l + 1 != lc) FHD_CUDA_TRY(cudaMemsetAsync(D.phi, 0, sizeof(T) * D.g.nc, ctx->stream));
+    rc = cc_vcycle(ctx, M, l + 1, lc);
     if (rc) return rc;
     with_dim(ctx->dim, [&](auto Dm) {
         constexpr int DIM = decltype(Dm)::value;
@@ -706,8 +824,9 @@ static int cc_solve(fhd_ctx* ctx, Multigrid<T>& M) {
         r0 = ctx->hscal[S_NRM];
         if (r0 == 0.0) return 0;
     }
+    const int lc = cc_coarse_first(ctx, M);
     for (int vc = 1; vc <= maxv; vc++) {
-        int rc = cc_vcycle(ctx, M, 0);
+        int rc = cc_vcycle(ctx, M, 0, lc);
         if (rc) return rc;
         if (vc == maxv) break;
         with_dim(ctx->dim, [&](auto D) {
@@ -1444,6 +1563,15 @@ int fhd_ctx_profile_read(fhd_ctx* c, long long* launches, double* ms, double* by
     if (launches) *launches = c->prof_launches;
     if (ms) *ms = t;
     if (bytes) *bytes = c->prof_bytes;
+    return FHD_OK;
+}
+
+int fhd_ctx_set_coarse(fhd_ctx* c, int mode) {
+    if (!c || mode < -1 || mode > 1) return FHD_ERR_BAD_ARG;
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess) return FHD_ERR_CUDA;
+    // captured preconditioner graphs hold the other launch sequence
+    release_graphs(c);
+    c->coarse_mode = mode;
     return FHD_OK;
 }
 

@@ -233,6 +233,8 @@ struct fhd_ctx {
     // the operand pointers and the prepared coefficients (-1 auto, 0 off,
     // 1 on)
     int graph_mode = -1;
+    // the coarse multigrid levels in one CTA (-1 default: on, 0 off)
+    int coarse_mode = -1;
     struct PreconGraph {
         unsigned long long key = 0;
         cudaGraphExec_t exec = nullptr;
