@@ -477,12 +477,16 @@ def main():
         iters = []
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
+        # an NVTX range around the timed steps, so that a profiler can be
+        # restricted to them (ncu --nvtx --nvtx-include "timed_mixed/")
+        torch.cuda.nvtx.range_push(f"timed_{precision}")
         ev0.record(stream)
         for i in range(args.steps):
             st, stats = run_step(args.warmup + i, dev_sets)
             iters.append([s["total_iters"] for s in stats])
         ev1.record(stream)
         torch.cuda.synchronize()
+        torch.cuda.nvtx.range_pop()
         ms = ev0.elapsed_time(ev1)
         barrier(ws)
         prof = case.s.profile_read()

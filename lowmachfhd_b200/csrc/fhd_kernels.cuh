@@ -378,31 +378,94 @@ __global__ void __launch_bounds__(256) k_stag_restrict(Grid gf, Grid gc, const T
     }
 }
 
-// fine += P coarse, thread per fine cell, all components.
+// two consecutive elements (an x-pair of fine cells), one vector access
+template <typename T>
+struct Pair2;
+template <>
+struct Pair2<float> {
+    typedef float2 V;
+};
+template <>
+struct Pair2<double> {
+    typedef double2 V;
+};
+
+// fine += P coarse.  Thread per coarse cell: per component the 18 coarse
+// faces that its 2x2x2 fine children read (offsets 0, 1 along the
+// component, -1..1 across it) are loaded once, and the children's x-pairs
+// are read and written as one vector each (vec: every fine array is aligned
+// to two elements; else two scalar accesses).  Every fine value is the
+// stag_prolong_expr of the per-fine-cell form.
 template <typename T, int DIM>
 __global__ void __launch_bounds__(256) k_stag_prolong(Grid gf, Grid gc, T* f0, T* f1, T* f2, const T* c0,
-                                                      const T* c1, const T* c2) {
-    Cell P;
-    if (!cell_of_thread(gf, P)) return;
-    Cell H;
-    H.nx = gc.n[0]; H.ny = gc.n[1]; H.nz = gc.n[2];
-    H.i = P.i >> 1; H.j = P.j >> 1; H.k = P.k >> 1;
+                                                      const T* c1, const T* c2, int vec) {
+    typedef typename Pair2<T>::V V2;
+    CellF H;
+    if ((int)blockIdx.z >= gc.n[2] || !cellf_of_thread(gc, H)) return;
+    const i64 nxf = gf.n[0], nxyf = (i64)gf.n[0] * gf.n[1];
+    const i64 fb = 2 * (i64)H.i + nxf * 2 * H.j + (DIM == 3 ? nxyf * 2 * H.k : 0);
     T* fo[3] = {f0, f1, f2};
     const T* ci[3] = {c0, c1, c2};
-    const int I[3] = {P.i, P.j, P.k};
-    const i64 f = P.id(0, 0, 0);
 #pragma unroll
     for (int c = 0; c < DIM; c++) {
-        const T* Cp = ci[c];
         const int a = (c == 0) ? 1 : 0;
         const int b = (c == 2) ? 1 : 2;
-        const int oa = (I[a] & 1) ? 1 : -1;
-        const int ob = (DIM == 3) ? ((I[b] & 1) ? 1 : -1) : 0;
-        const T v = stag_prolong_expr<T, DIM>((I[c] & 1) == 0, oa, ob, [&](int o, int pa, int pb) {
-            return ld(Cp, comp_off_id<DIM>(H, c, o, pa, pb));
-        });
-        fo[c][f] = fo[c][f] + v;
+        T cv[2][3][3];
+#pragma unroll
+        for (int o = 0; o < 2; o++)
+#pragma unroll
+            for (int pa = -1; pa <= 1; pa++)
+#pragma unroll
+                for (int pb = -1; pb <= 1; pb++) {
+                    if (DIM == 2 && pb != 0) continue;
+                    int off[3] = {0, 0, 0};
+                    off[c] += o;
+                    off[a] += pa;
+                    if (DIM == 3) off[b] += pb;
+                    cv[o][pa + 1][pb + 1] = ld(ci[c], H.id(off[0], off[1], off[2]));
+                }
+#pragma unroll
+        for (int pz = 0; pz < (DIM == 3 ? 2 : 1); pz++)
+#pragma unroll
+            for (int py = 0; py < 2; py++) {
+                T* row = fo[c] + fb + py * nxf + pz * nxyf;
+                T out[2];
+                if (vec) {
+                    const V2 v = *reinterpret_cast<const V2*>(row);
+                    out[0] = v.x;
+                    out[1] = v.y;
+                } else {
+                    out[0] = row[0];
+                    out[1] = row[1];
+                }
+#pragma unroll
+                for (int px = 0; px < 2; px++) {
+                    const int I[3] = {px, py, pz};  // parities of the fine indices
+                    const int oa = I[a] ? 1 : -1;
+                    const int ob = (DIM == 3) ? (I[b] ? 1 : -1) : 0;
+                    out[px] = out[px] + stag_prolong_expr<T, DIM>(
+                                            I[c] == 0, oa, ob,
+                                            [&](int o, int qa, int qb) { return cv[o][qa + 1][qb + 1]; });
+                }
+                if (vec) {
+                    V2 v;
+                    v.x = out[0];
+                    v.y = out[1];
+                    *reinterpret_cast<V2*>(row) = v;
+                } else {
+                    row[0] = out[0];
+                    row[1] = out[1];
+                }
+            }
     }
+}
+
+// k_stag_prolong's vector flag for the fine arrays f[0..dim)
+template <typename T>
+inline int pair_aligned(int dim, T* const* f) {
+    for (int c = 0; c < dim; c++)
+        if ((uintptr_t)f[c] % (2 * sizeof(T))) return 0;
+    return 1;
 }
 
 // cc_restriction (stag_mg_solver.f90:919-963): average of 2^dim children
@@ -549,13 +612,26 @@ __global__ void __launch_bounds__(256) k_cc_resid_restrict(Grid gf, Grid gc, CCO
         A, gf, Q.i, Q.j, Q.k, [&](i64 i) { return ld(phi, i); }, [&](i64 i) { return ld(rhs, i); });
 }
 
+// phi += coarse phi of the parent cell.  Thread per coarse cell, its fine
+// children written as x-pairs.
 template <typename T, int DIM>
 __global__ void __launch_bounds__(256) k_cc_prolong(Grid gf, Grid gc, T* phi, const T* cphi) {
-    Cell P;
-    if (!cell_of_thread(gf, P)) return;
-    const i64 f = P.id(0, 0, 0);
-    const i64 c = (i64)(P.i >> 1) + (i64)gc.n[0] * ((i64)(P.j >> 1) + (i64)gc.n[1] * (P.k >> 1));
-    phi[f] = phi[f] + ld(cphi, c);
+    typedef typename Pair2<T>::V V2;
+    Cell Q;
+    if ((int)blockIdx.z >= gc.n[2] || !cell_of_thread(gc, Q)) return;
+    const T cv = ld(cphi, Q.id(0, 0, 0));
+    const i64 nxf = gf.n[0], nxyf = (i64)gf.n[0] * gf.n[1];
+    const i64 fb = 2 * (i64)Q.i + nxf * 2 * Q.j + (DIM == 3 ? nxyf * 2 * Q.k : 0);
+#pragma unroll
+    for (int pz = 0; pz < (DIM == 3 ? 2 : 1); pz++)
+#pragma unroll
+        for (int py = 0; py < 2; py++) {
+            V2* row = reinterpret_cast<V2*>(phi + fb + py * nxf + pz * nxyf);
+            V2 v = *row;
+            v.x = v.x + cv;
+            v.y = v.y + cv;
+            *row = v;
+        }
 }
 
 template <typename T, int DIM>

@@ -25,6 +25,11 @@ struct MixDev {
     int correct;
     int avg_type;
     double kB, dV;
+    // FP32 mirrors for the mixed-precision kernels: the constants and the
+    // reciprocals of the constant divisors (Dinv_f[i][i] = 0)
+    float mm_f[FHD_MAX_SPECIES], imm_f[FHD_MAX_SPECIES];
+    float Dinv_f[FHD_MAX_SPECIES][FHD_MAX_SPECIES];
+    float ikB_f, dV_f, tol_f;
 };
 
 MixDev make_mixdev(const fhd_mixture_params* mp, const fhd_stoch_params* sp) {
@@ -48,7 +53,141 @@ MixDev make_mixdev(const fhd_mixture_params* mp, const fhd_stoch_params* sp) {
     m.avg_type = mp->avg_type;
     m.kB = sp->k_B;
     m.dV = sp->dV;
+    for (int i = 0; i < m.ns; i++) {
+        m.mm_f[i] = (float)m.molmass[i];
+        m.imm_f[i] = (float)(1.0 / m.molmass[i]);
+        for (int j = 0; j < m.ns; j++) m.Dinv_f[i][j] = (i == j) ? 0.0f : (float)(1.0 / m.D[i][j]);
+    }
+    m.ikB_f = (float)(1.0 / m.kB);
+    m.dV_f = (float)m.dV;
+    m.tol_f = (float)m.frac_tol;
     return m;
+}
+
+// FP32 arithmetic of the mixed-precision kernels: fused multiply-adds,
+// products with the host-computed reciprocals of the constant divisors
+// (molar masses, Dbar, k_B), one fast reciprocal per repeated divisor, and
+// the closed forms of two of Dbar2chi_iterative's products: P J = J - 1 (Y^T
+// J) and P diag(Minv) P^T = diag(Minv) - Y Minv 1^T - 1 (Y Minv)^T +
+// sum(Y^2 Minv), with P = I - 1 Y^T.  The FP64 kernels keep the
+// restatement's operations and order (parity with the CPU oracle).
+__device__ __forceinline__ float frcp(float x) { return __fdividef(1.0f, x); }
+
+template <int NS>
+__device__ __forceinline__ void d_molconc_f(const MixDev& m, const float* rho, float rhotot, float* x, float& mtot) {
+    const float ri = frcp(rhotot);
+    float W[NS];
+    float s = 0.0f;
+#pragma unroll
+    for (int n = 0; n < NS; n++) {
+        W[n] = rho[n] * ri;
+        s = __fmaf_rn(W[n], m.imm_f[n], s);
+    }
+    mtot = frcp(s);
+#pragma unroll
+    for (int n = 0; n < NS; n++) x[n] = mtot * W[n] * m.imm_f[n];
+}
+
+// Dbar2chi_iterative (matrix_utilities.f90:19-158), NS >= 3, FP32
+template <int NS>
+__device__ __forceinline__ void d_chi_f(const MixDev& m, const float* Xk, int chi_it, float (&chi)[NS][NS]) {
+    float mw = 0.0f;
+#pragma unroll
+    for (int i = 0; i < NS; i++) mw = __fmaf_rn(Xk[i], m.mm_f[i], mw);
+    const float imw = frcp(mw);
+    float Y[NS], Minv[NS], Mm[NS], t2[NS];
+#pragma unroll
+    for (int i = 0; i < NS; i++) {
+        Y[i] = m.mm_f[i] * imw * Xk[i];
+        float t = 0.0f;
+#pragma unroll
+        for (int j = 0; j < NS; j++) t = __fmaf_rn(Xk[j], m.Dinv_f[i][j], t);
+        t2[i] = t;
+        const float Di = __fdividef(1.0f - Y[i], t);
+        Mm[i] = __fdividef(Xk[i], Di);
+        Minv[i] = __fdividef(Di, Xk[i]);
+    }
+    // J = Minv (M - Delta): Delta_ii = X_i sum_k X_k / D_ik, Delta_ij = -X_i X_j / D_ij
+    float J[NS][NS];
+#pragma unroll
+    for (int i = 0; i < NS; i++)
+#pragma unroll
+        for (int j = 0; j < NS; j++)
+            J[i][j] = (i == j) ? Minv[i] * (Mm[i] - Xk[i] * t2[i]) : Minv[i] * (Xk[i] * Xk[j] * m.Dinv_f[i][j]);
+    float cs[NS];
+#pragma unroll
+    for (int j = 0; j < NS; j++) {
+        float a = 0.0f;
+#pragma unroll
+        for (int k = 0; k < NS; k++) a = __fmaf_rn(Y[k], J[k][j], a);
+        cs[j] = a;
+    }
+    float sY = 0.0f, YM[NS];
+#pragma unroll
+    for (int k = 0; k < NS; k++) {
+        YM[k] = Y[k] * Minv[k];
+        sY = __fmaf_rn(Y[k], YM[k], sY);
+    }
+    float PJ[NS][NS], m2[NS][NS];
+#pragma unroll
+    for (int i = 0; i < NS; i++)
+#pragma unroll
+        for (int j = 0; j < NS; j++) {
+            PJ[i][j] = J[i][j] - cs[j];
+            m2[i][j] = ((i == j) ? Minv[i] : 0.0f) - YM[i] - YM[j] + sY;
+            chi[i][j] = m2[i][j];
+        }
+    for (int it = 0; it < chi_it; it++) {
+        float m1[NS][NS];
+#pragma unroll
+        for (int i = 0; i < NS; i++)
+#pragma unroll
+            for (int j = 0; j < NS; j++) {
+                float a = m2[i][j];
+#pragma unroll
+                for (int k = 0; k < NS; k++) a = __fmaf_rn(PJ[i][k], chi[k][j], a);
+                m1[i][j] = a;
+            }
+#pragma unroll
+        for (int i = 0; i < NS; i++)
+#pragma unroll
+            for (int j = 0; j < NS; j++) chi[i][j] = m1[i][j];
+    }
+}
+
+// choldc (matrix_utilities.f90:162-241), FP32: 1/p from the fast
+// reciprocal square root
+template <int NS>
+__device__ __forceinline__ void d_choldc_f(float (&a)[NS][NS]) {
+    float p[NS];
+#pragma unroll
+    for (int i = 0; i < NS; i++) {
+        int ising = 0;
+        float r = 0.0f;
+#pragma unroll
+        for (int j = i; j < NS; j++) {
+            float s = a[i][j];
+#pragma unroll
+            for (int k = i - 1; k >= 0; k--) s = __fmaf_rn(-a[i][k], a[j][k], s);
+            if (i == j) {
+                if (s <= 0.0f) {
+                    p[i] = 0.0f;
+                    ising = 1;
+                } else {
+                    r = rsqrtf(s);
+                    p[i] = s * r;
+                }
+            } else {
+                a[j][i] = (ising == 0) ? s * r : 0.0f;
+            }
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < NS; i++) {
+#pragma unroll
+        for (int j = i + 1; j < NS; j++) a[i][j] = 0.0f;
+        a[i][i] = p[i];
+    }
 }
 
 // compute_molconc_molmtot_local (mass_flux_utilities.f90:159-186)
@@ -165,10 +304,30 @@ __device__ __forceinline__ void d_chi(const MixDev& m, const T* rho, T rhotot, c
 template <typename T, int NS>
 __device__ __forceinline__ int d_ntrace(const MixDev& m, const T* rho, T rhotot) {
     int nt = 0;
+    if constexpr (sizeof(T) == 4) {
+        const float ri = frcp(rhotot);
 #pragma unroll
-    for (int i = 0; i < NS; i++)
-        if (rho[i] / rhotot < (T)m.frac_tol) nt++;
+        for (int i = 0; i < NS; i++)
+            if (rho[i] * ri < m.tol_f) nt++;
+    } else {
+#pragma unroll
+        for (int i = 0; i < NS; i++)
+            if (rho[i] / rhotot < (T)m.frac_tol) nt++;
+    }
     return nt;
+}
+
+// molar concentrations and chi in the arithmetic of T
+template <typename T, int NS>
+__device__ __forceinline__ void d_molconc_t(const MixDev& m, const T* rho, T rhotot, T* x, T& mtot) {
+    if constexpr (sizeof(T) == 4) d_molconc_f<NS>(m, rho, rhotot, x, mtot);
+    else d_molconc<T, NS>(m, rho, rhotot, x, mtot);
+}
+
+template <typename T, int NS>
+__device__ __forceinline__ void d_chi_t(const MixDev& m, const T* rho, T rhotot, const T* Xk, T (&chi)[NS][NS]) {
+    if constexpr (sizeof(T) == 4 && NS >= 3) d_chi_f<NS>(m, Xk, m.chi_it, chi);
+    else d_chi<T, NS>(m, rho, rhotot, Xk, chi);
 }
 
 // choldc (matrix_utilities.f90:162-241)
@@ -219,7 +378,7 @@ __global__ void __launch_bounds__(128) k_rhowchi(Grid g, MixDev m, const double*
             rt = rt + r[s];
         }
         T x[NS], mt;
-        d_molconc<T, NS>(m, r, rt, x, mt);
+        d_molconc_t<T, NS>(m, r, rt, x, mt);
 #pragma unroll
         for (int s = 0; s < NS; s++) xo[s][f] = x[s];
         const int nt = d_ntrace<T, NS>(m, r, rt);
@@ -233,7 +392,7 @@ __global__ void __launch_bounds__(128) k_rhowchi(Grid g, MixDev m, const double*
             continue;
         }
         T chi[NS][NS];
-        d_chi<T, NS>(m, r, rt, x, chi);
+        d_chi_t<T, NS>(m, r, rt, x, chi);
 #pragma unroll
         for (int i = 0; i < NS; i++)
 #pragma unroll
@@ -263,7 +422,12 @@ __global__ void __launch_bounds__(128) k_mass_flux(Grid g, MixDev m, int d, cons
         for (int r = 0; r < NS; r++) {
             T acc = T(0);
 #pragma unroll
-            for (int c = 0; c < NS; c++) acc = acc + T(0.5) * (ld(rwc[r * NS + c], fm) + ld(rwc[r * NS + c], f)) * gx[c];
+            for (int c = 0; c < NS; c++) {
+                if constexpr (sizeof(T) == 4)
+                    acc = __fmaf_rn(0.5f * (ld(rwc[r * NS + c], fm) + ld(rwc[r * NS + c], f)), gx[c], acc);
+                else
+                    acc = acc + T(0.5) * (ld(rwc[r * NS + c], fm) + ld(rwc[r * NS + c], f)) * gx[c];
+            }
             fd[r] = acc;
         }
         if (m.correct && NS > 1) {
@@ -282,8 +446,16 @@ __global__ void __launch_bounds__(128) k_mass_flux(Grid g, MixDev m, int d, cons
         T rt = T(0);
 #pragma unroll
         for (int c = 0; c < NS; c++) {
-            const T mm = (T)m.molmass[c];
-            const T v1 = (T)ld(rho[c], fm) / mm, v2 = (T)ld(rho[c], f) / mm;
+            T mm, v1, v2;
+            if constexpr (sizeof(T) == 4) {
+                mm = m.mm_f[c];
+                v1 = (float)ld(rho[c], fm) * m.imm_f[c];
+                v2 = (float)ld(rho[c], f) * m.imm_f[c];
+            } else {
+                mm = (T)m.molmass[c];
+                v1 = (T)ld(rho[c], fm) / mm;
+                v2 = (T)ld(rho[c], f) / mm;
+            }
             T o;
             if (m.avg_type == 2) {
                 o = mm * sqrt(fmax(v1, T(0)) * fmax(v2, T(0)));
@@ -313,17 +485,29 @@ __global__ void __launch_bounds__(128) k_mass_flux(Grid g, MixDev m, int d, cons
         } else {
             if (nt != 0) atomicOr(flag, 1);
             T Wf[NS], x[NS], mt;
-#pragma unroll
-            for (int i = 0; i < NS; i++) Wf[i] = ra[i] / rt;
-            d_molconc<T, NS>(m, ra, rt, x, mt);
+            d_molconc_t<T, NS>(m, ra, rt, x, mt);
             T chi[NS][NS];
-            d_chi<T, NS>(m, ra, rt, x, chi);
-            const T kB = (T)m.kB;
+            d_chi_t<T, NS>(m, ra, rt, x, chi);
+            if constexpr (sizeof(T) == 4) {
+                const float ri = frcp(rt);
 #pragma unroll
-            for (int c = 0; c < NS; c++)
+                for (int i = 0; i < NS; i++) Wf[i] = ra[i] * ri;
+                const float fac = mt * rt * m.ikB_f;
 #pragma unroll
-                for (int r = 0; r < NS; r++) L[r][c] = mt * rt * Wf[r] * chi[r][c] * Wf[c] / kB;
-            d_choldc<T, NS>(L);
+                for (int c = 0; c < NS; c++)
+#pragma unroll
+                    for (int r = 0; r < NS; r++) L[r][c] = fac * Wf[r] * chi[r][c] * Wf[c];
+                d_choldc_f<NS>(L);
+            } else {
+#pragma unroll
+                for (int i = 0; i < NS; i++) Wf[i] = ra[i] / rt;
+                const T kB = (T)m.kB;
+#pragma unroll
+                for (int c = 0; c < NS; c++)
+#pragma unroll
+                    for (int r = 0; r < NS; r++) L[r][c] = mt * rt * Wf[r] * chi[r][c] * Wf[c] / kB;
+                d_choldc<T, NS>(L);
+            }
         }
         T w[NS];
 #pragma unroll
@@ -336,7 +520,10 @@ __global__ void __launch_bounds__(128) k_mass_flux(Grid g, MixDev m, int d, cons
         for (int r = 0; r < NS; r++) {
             T acc = T(0);
 #pragma unroll
-            for (int c = 0; c < NS; c++) acc = acc + L[r][c] * w[c];
+            for (int c = 0; c < NS; c++) {
+                if constexpr (sizeof(T) == 4) acc = __fmaf_rn(L[r][c], w[c], acc);
+                else acc = acc + L[r][c] * w[c];
+            }
             fs[r] = acc * variance;
         }
         if (m.correct && NS > 1) {

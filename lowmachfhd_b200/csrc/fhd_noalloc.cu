@@ -203,8 +203,8 @@ int na_vcycle(NA& S) {
         StagLevel<double>& C = S.L[l + 1];
         with_dim(dim, [&](auto D) {
             constexpr int DIM = decltype(D)::value;
-            k_stag_prolong<double, DIM><<<cell_grid(F.g), cell_block(), 0, S.st>>>(
-                F.g, C.g, F.phi[0], F.phi[1], F.phi[2], C.phi[0], C.phi[1], C.phi[2]);
+            k_stag_prolong<double, DIM><<<cell_grid(C.g), cell_block(), 0, S.st>>>(
+                F.g, C.g, F.phi[0], F.phi[1], F.phi[2], C.phi[0], C.phi[1], C.phi[2], pair_aligned(dim, F.phi));
         });
         NA_TRY_LAUNCH();
         if (int rc = na_smooths(S, F, S.p.stag_mg_nsmooths_up)) return rc;

@@ -596,8 +596,9 @@ static int stag_vcycle(fhd_ctx* ctx, Multigrid<T>& M) {
         StagLevel<T>& C = M.s[l + 1];
         with_dim(dim, [&](auto D) {
             constexpr int DIM = decltype(D)::value;
-            k_stag_prolong<T, DIM><<<cell_grid(L.g), cell_block(), 0, st>>>(L.g, C.g, L.phi[0], L.phi[1], L.phi[2],
-                                                                          C.phi[0], C.phi[1], C.phi[2]);
+            k_stag_prolong<T, DIM><<<cell_grid(C.g), cell_block(), 0, st>>>(L.g, C.g, L.phi[0], L.phi[1], L.phi[2],
+                                                                          C.phi[0], C.phi[1], C.phi[2],
+                                                                          pair_aligned(dim, L.phi));
             rc |= post(ctx);
         });
         if (rc) return rc;
@@ -801,7 +802,7 @@ static int cc_vcycle(fhd_ctx* ctx, Multigrid<T>& M, int l, int lc) {
     if (rc) return rc;
     with_dim(ctx->dim, [&](auto Dm) {
         constexpr int DIM = decltype(Dm)::value;
-        k_cc_prolong<T, DIM><<<cell_grid(C.g), cell_block(), 0, ctx->stream>>>(C.g, D.g, C.phi, D.phi);
+        k_cc_prolong<T, DIM><<<cell_grid(D.g), cell_block(), 0, ctx->stream>>>(C.g, D.g, C.phi, D.phi);
         rc |= post(ctx);
     });
     if (rc) return rc;
