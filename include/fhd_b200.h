@@ -159,6 +159,12 @@ int fhd_ctx_set_graphs(fhd_ctx* ctx, int mode);
  * reference routine: the levels are those of stag_mg_solver.f90:301-599 and
  * of the pressure multigrid behind macproject.f90:294-298. */
 int fhd_ctx_set_coarse(fhd_ctx* ctx, int mode);
+/* Whole smooths (both colours of every component) of the large FP32 levels
+ * of a visc_type 1 staggered multigrid as one row-tile launch each, staged
+ * by the bulk-copy engine, instead of one launch per colour (mode 1 or -1
+ * default: on where the level allows, 0: colour launches).  The colour
+ * sweeps of stag_mg_solver.f90:360-396, evaluated in the same order. */
+int fhd_ctx_set_fused(fhd_ctx* ctx, int mode);
 /* Number of this library's kernels launched through ctx so far. */
 long long fhd_ctx_kernel_launches(fhd_ctx* ctx);
 const char* fhd_status_string(int status);

@@ -115,6 +115,11 @@ class StokesSolver:
         or -1 (default) on, 0 one launch per smoother colour and transfer"""
         check(lib().fhd_ctx_set_coarse(self._h, int(mode)), "fhd_ctx_set_coarse")
 
+    def set_fused(self, mode: int):
+        """whole smooths of the large FP32 levels as one bulk-copy-staged
+        launch each: 1 or -1 (default) on, 0 one launch per colour"""
+        check(lib().fhd_ctx_set_fused(self._h, int(mode)), "fhd_ctx_set_fused")
+
     def profile(self, enable: bool = True):
         """time the finest-level smoother launches with CUDA events"""
         check(lib().fhd_ctx_profile(self._h, int(enable)), "fhd_ctx_profile")

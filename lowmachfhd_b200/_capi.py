@@ -142,6 +142,7 @@ _PROTOS = {
     "fhd_ctx_kernel_launches": (C.c_longlong, [_VP]),
     "fhd_ctx_set_graphs": (C.c_int, [_VP, C.c_int]),
     "fhd_ctx_set_coarse": (C.c_int, [_VP, C.c_int]),
+    "fhd_ctx_set_fused": (C.c_int, [_VP, C.c_int]),
     "fhd_ctx_device_bytes": (C.c_ulonglong, [_VP]),
     "fhd_ctx_profile": (C.c_int, [_VP, C.c_int]),
     "fhd_ctx_profile_read": (C.c_int, [_VP, C.POINTER(C.c_longlong), C.POINTER(C.c_double),

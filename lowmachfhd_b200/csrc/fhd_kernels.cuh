@@ -44,9 +44,10 @@ struct CellF {
     int i, j, k;
     i64 base;
     int oxm, oxp, oym, oyp, ozm, ozp;
-    __device__ __forceinline__ void set(const Grid& g, int i_, int j_, int k_) {
+    __device__ __forceinline__ void set(const Grid& g, int i_, int j_, int k_) { set(g.n[0], g.n[1], g.n[2], i_, j_, k_); }
+    __device__ __forceinline__ void set(int nx, int ny, int nz, int i_, int j_, int k_) {
         i = i_; j = j_; k = k_;
-        const int nx = g.n[0], ny = g.n[1], nz = g.n[2], nxy = nx * ny;
+        const int nxy = nx * ny;
         base = (i64)i + (i64)nx * ((i64)j + (i64)ny * k);
         oxm = i == 0 ? nx - 1 : -1;
         oxp = i == nx - 1 ? 1 - nx : 1;

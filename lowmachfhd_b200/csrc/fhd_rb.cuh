@@ -94,7 +94,10 @@ inline bool rb_geom(const Grid& g, int ncomp, int elem_bytes, RBGeom& G) {
 // 357 us, 128^3 106 vs 62 us, 64^3 26 vs 25 us, 32^3 and below ~19 vs
 // ~24 us.  Large levels stay on the colour kernels; the fused launch serves
 // the latency-bound coarse levels.
-constexpr long RB_MAX_CELLS = 64L * 64 * 64;
+#ifndef FHD_RB_MAX_CELLS
+#define FHD_RB_MAX_CELLS (64L * 64 * 64)
+#endif
+constexpr long RB_MAX_CELLS = FHD_RB_MAX_CELLS;
 inline bool rb_use(const Grid& g) { return g.nc <= RB_MAX_CELLS; }
 
 template <typename T>
@@ -168,12 +171,9 @@ struct RBTile {
     int x0, y0, nx, ny, nz;
     __device__ __forceinline__ T* pbuf(int p) const { return ph + pmod(p, RB_NPH) * plane; }
     __device__ __forceinline__ T* cbuf(int a, int p) const { return cf + (a * RB_NCF + pmod(p, RB_NCF)) * cplane; }
-    __device__ __forceinline__ Cell cell(int lx, int ly, int p) const {
-        Cell P;
-        P.nx = nx; P.ny = ny; P.nz = nz;
-        P.i = wrapc(x0 + lx, nx);
-        P.j = wrapc(y0 + ly, ny);
-        P.k = wrapc(p, nz);
+    __device__ __forceinline__ CellF cell(int lx, int ly, int p) const {
+        CellF P;
+        P.set(nx, ny, nz, wrapc(x0 + lx, nx), wrapc(y0 + ly, ny), wrapc(p, nz));
         return P;
     }
 };
@@ -208,44 +208,62 @@ __device__ __forceinline__ void rb_march(const RBGeom& G, const RBTile<T, NCOEF>
             for (int a = 0; a < NCOEF; a++) issue_chunks(pc, t.cbuf(a, p), coef[a] + (i64)wrapc(p, t.nz) * nxy);
     };
     const int W = G.W, XR = G.XR;
-    auto row = [&](int p, int ly) {
+    // the unknown planes p-1, p, p+1 and the coefficient planes p of one
+    // plane's update
+    struct Planes {
+        T *m, *c, *p;
+        T* cf[NCOEF > 0 ? NCOEF : 1];
+    };
+    auto planes_at = [&](int sm, int sc, int sp, int scf) {
+        Planes q;
+        q.m = t.ph + sm * t.plane;
+        q.c = t.ph + sc * t.plane;
+        q.p = t.ph + sp * t.plane;
+#pragma unroll
+        for (int a = 0; a < NCOEF; a++) q.cf[a] = t.cf + (a * RB_NCF + scf) * t.cplane;
+        return q;
+    };
+    auto planes_of = [&](int p) {
+        return planes_at(pmod(p - 1, RB_NPH), pmod(p, RB_NPH), pmod(p + 1, RB_NPH), pmod(p, RB_NCF));
+    };
+    auto row = [&](const Planes& q, int ly) {
         RBRow<T, NCOEF> R;
         const int base = (ly + 2) * W + XR;
-        R.r0 = t.pbuf(p) + base;
+        R.r0 = q.c + base;
         R.rm = R.r0 - W;
         R.rp = R.r0 + W;
-        R.zm = t.pbuf(p - 1) + base;
-        R.zp = t.pbuf(p + 1) + base;
+        R.zm = q.m + base;
+        R.zp = q.p + base;
 #pragma unroll
-        for (int a = 0; a < NCOEF; a++) R.cf[a] = t.cbuf(a, p) + (ly + 1) * W + XR;
+        for (int a = 0; a < NCOEF; a++) R.cf[a] = q.cf[a] + (ly + 1) * W + XR;
         return R;
     };
     const int hx = G.TX >> 1;  // cells of one colour per tile row
     // one row of colour par (0 red, 1 black) of plane p, over [0, TX)
-    auto sweep_row = [&](int p, int ly, int par) {
-        const RBRow<T, NCOEF> R = row(p, ly);
+    auto sweep_row = [&](const Planes& q, int p, int ly, int par) {
+        const RBRow<T, NCOEF> R = row(q, ly);
         const int s = (t.x0 + t.y0 + ly + p + par) & 1;
         for (int h = tx; h < hx; h += 32) upd(s + 2 * h, ly, p, R);
     };
     // red of plane p on the tile and ring 1 (corners excluded)
-    auto red_by_warp = [&](int p) {
+    auto red_by_warp = [&](const Planes& q, int p) {
         if (ty < G.TY) {
-            sweep_row(p, ty, 0);
+            sweep_row(q, p, ty, 0);
         } else {
-            sweep_row(p, -1, 0);
-            sweep_row(p, G.TY, 0);
+            sweep_row(q, p, -1, 0);
+            sweep_row(q, p, G.TY, 0);
             if (tx < G.TY) {
                 const int ly = tx;
-                upd(((t.x0 - 1 + t.y0 + ly + p) & 1) ? G.TX : -1, ly, p, row(p, ly));
+                upd(((t.x0 - 1 + t.y0 + ly + p) & 1) ? G.TX : -1, ly, p, row(q, ly));
             }
         }
     };
     // 16-byte vector store of the finished plane p
-    auto store = [&](int p) {
+    auto store = [&](int p, const T* buf) {
         const int vx = G.TX / XR;  // vectors per row
         if (tid < vx * G.TY) {
             const int r = tid / vx, c = (tid - r * vx) * XR;
-            const uint4 v = *reinterpret_cast<const uint4*>(t.pbuf(p) + (r + 2) * W + XR + c);
+            const uint4 v = *reinterpret_cast<const uint4*>(buf + (r + 2) * W + XR + c);
             *reinterpret_cast<uint4*>(dst + (i64)p * nxy + (i64)(t.y0 + r) * t.nx + t.x0 + c) = v;
         }
     };
@@ -263,9 +281,13 @@ __device__ __forceinline__ void rb_march(const RBGeom& G, const RBTile<T, NCOEF>
     cp_async_wait<RB_AHEAD>();
     __syncthreads();
     // red of k0-1 .. k0+1 read only black cells, which none of them writes
-    red_by_warp(k0 - 1);
-    red_by_warp(k0);
-    red_by_warp(k0 + 1);
+    red_by_warp(planes_of(k0 - 1), k0 - 1);
+    red_by_warp(planes_of(k0), k0);
+    red_by_warp(planes_of(k0 + 1), k0 + 1);
+    // ring slots of unknown plane k-1 and coefficient plane k, advanced by
+    // one per step (no modulo in the march)
+    int sm = pmod(k0 - 1, RB_NPH), sc = pmod(k0, RB_NCF);
+    auto ring = [](int s, int d, int n) { return s + d >= n ? s + d - n : s + d; };
     for (int k = k0; k < kend; k++) {
         // unknown plane k+3 and coefficient plane k+2 are in the group
         // committed AHEAD groups before the newest
@@ -276,22 +298,23 @@ __device__ __forceinline__ void rb_march(const RBGeom& G, const RBTile<T, NCOEF>
         issue_ph(k + 3 + RB_AHEAD);
         issue_cf(k + 2 + RB_AHEAD);
         cp_async_commit();
-        if (k > k0) store(k - 1);
-        if (ty < G.TY) sweep_row(k, ty, 1);
-        if (k + 2 <= kend) red_by_warp(k + 2);
+        const int s0 = ring(sm, 1, RB_NPH), s1 = ring(sm, 2, RB_NPH);
+        if (k > k0) store(k - 1, t.ph + sm * t.plane);
+        if (ty < G.TY) sweep_row(planes_at(sm, s0, s1, sc), k, ty, 1);
+        if (k + 2 <= kend)
+            red_by_warp(planes_at(s1, ring(sm, 3, RB_NPH), ring(sm, 4, RB_NPH), ring(sc, 2, RB_NCF)), k + 2);
+        sm = s0;
+        sc = ring(sc, 1, RB_NCF);
     }
     cp_async_wait<0>();
     __syncthreads();
-    store(kend - 1);
+    store(kend - 1, t.pbuf(kend - 1));
 }
 
-// x / d of the update: the IEEE quotient in FP64 (bit-identical to the
-// colour kernels and the oracle); x times the correctly rounded reciprocal in
-// the FP32 preconditioner, where the quotient's extra rounding is noise
+// x / d of the update: the quotient of the colour kernels (sm_quot)
 template <typename T>
 __device__ __forceinline__ T rb_quot(T x, T d) {
-    if constexpr (sizeof(T) == 4) return x * __frcp_rn(d);
-    else return x / d;
+    return sm_quot(x, d);
 }
 
 template <typename T>
@@ -325,7 +348,7 @@ __device__ __forceinline__ void stag_rb_run(const Grid& g, const RBGeom& G, cons
     const T* coef[2] = {A.alpha[C], R.rhs[C]};
     rb_march<T, 2>(G, t, R.src[C], R.dst[C], coef, blockIdx.y * G.KZ,
                    [&](int lx, int ly, int p, const RBRow<T, 2>& Rw) {
-                       const Cell P = t.cell(lx, ly, p);
+                       const CellF P = t.cell(lx, ly, p);
                        auto own = [&](int a, int b, int c) { return Rw.at(lx, a, b, c); };
                        auto othf = [&](int d, int a, int b, int c) { return ld(oth[d], P.id(a, b, c)); };
                        auto alp = [&]() { return Rw.cf[0][lx]; };
@@ -361,7 +384,7 @@ __global__ void __launch_bounds__(RB_MAXTHREADS) k_cc_rb(Grid g, RBGeom G, CCOp<
     const RBTile<T, 1> t = rb_tile<T, 1>(g, G, rb_smraw);
     const T* coef[1] = {rhs};
     rb_march<T, 1>(G, t, src, dst, coef, blockIdx.y * G.KZ, [&](int lx, int ly, int p, const RBRow<T, 1>& Rw) {
-        const Cell P = t.cell(lx, ly, p);
+        const CellF P = t.cell(lx, ly, p);
         auto ph = [&](int a, int b, int c) { return Rw.at(lx, a, b, c); };
         T dg;
         const T L = cc_lap_acc<T, 3>(A, P, ph, dg);

@@ -1,0 +1,352 @@
+// fhd_rbx.cuh -- one full red-black smooth per launch on the large levels
+// of the FP32 staggered multigrid, constant-coefficient operator
+// (visc_type 1), 3D, x extent of 64 to 256 cells.
+//
+// The same z-march as the tiled fused smoother (fhd_rb.cuh: red update of
+// plane k+2 on the tile and a ring, black update of plane k, store of plane
+// k-1, out of place src -> dst), with the tile widened to whole x rows so
+// that the periodic x wrap stays inside shared memory and no x ring is
+// recomputed, and with the planes staged by the bulk-copy engine:
+//
+//   * a producer warp copies the staged rows of a plane (unknown rows
+//     y0-2 .. y0+TY+1, alpha and rhs rows y0-1 .. y0+TY) with 1D
+//     cp.async.bulk copies, one per array and contiguous run of rows (the
+//     periodic y wrap splits a run), completing on the stage's mbarrier;
+//   * the finished plane's TY interior rows, contiguous in shared and in
+//     global memory, leave as one bulk store;
+//   * eight compute warps update four to five cells per thread and plane
+//     step, every update one evaluation of stag_lface_acc on shared memory
+//     (the same expression as the colour kernels and the oracle); the
+//     producer warp only copies.
+//
+// Every mbarrier wait is bounded; a wait that runs out sets *err, and the
+// CTA leaves together (after its copies in flight have landed, again with a
+// bound) through the step barrier's reduction.
+#pragma once
+#include "fhd_kernels.cuh"
+
+namespace fhd {
+
+constexpr int RBX_THREADS = 256;
+constexpr int RBX_AHEAD = 2;            // stages in flight beyond the one awaited
+constexpr int RBX_NPH = 5 + RBX_AHEAD;  // unknown planes k-1 .. k+3 + in flight
+constexpr int RBX_NCF = 3 + RBX_AHEAD;  // coefficient planes k .. k+2 + in flight
+constexpr int RBX_MAXNX = 256;
+constexpr long RBX_SPIN = 1L << 22;     // try_wait polls before a wait gives up
+// a thread updates the cells of one x column on rows gr, gr + RG, ..: with
+// RG = RBX_THREADS / (nx / 2) its rows lie RBX_ROWSTEP elements apart for
+// every nx, at most RBX_MAXR of them per sweep
+constexpr int RBX_ROWSTEP = 2 * RBX_THREADS;
+constexpr int RBX_MAXR = 5;
+// the block: RBX_THREADS compute threads and one producer warp
+constexpr int RBX_BLOCK = RBX_THREADS + 32;
+// every thread evaluates RBX_MAXR rows per sweep and stores only those of
+// the tile; the reads of the others may run up to this many elements past
+// the last staged buffer, into a pad at the end of shared memory
+constexpr int RBX_PAD = RBX_MAXR * RBX_ROWSTEP + 2 * RBX_MAXNX;
+
+struct RBXGeom {
+    int TY;       // tile rows (divides ny)
+    int KZ;       // planes of the longest z-run
+    int tiles_y, chunks;
+    int rows;     // TY + 4 staged unknown rows
+    int crows;    // TY + 2 staged coefficient rows
+    size_t smem;  // bytes of dynamic shared memory
+};
+
+// ---------------------------------------------------------------------
+// mbarrier and bulk-copy primitives (sm_90+ PTX, no cluster multicast)
+// ---------------------------------------------------------------------
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(unsigned long long* b, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(b)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_init_fence() {
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* b, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(b)), "r"(bytes)
+                 : "memory");
+}
+// true once the phase of parity `parity` has completed
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* b, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(b)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// bounded wait: false when the phase did not complete within RBX_SPIN polls
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* b, unsigned parity) {
+    for (long i = 0; i < RBX_SPIN; i++)
+        if (mbar_try_wait(b, parity)) return true;
+    return false;
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, unsigned long long* b) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(b))
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_s2g(void* dst, const void* src, unsigned bytes) {
+    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;\n" ::"l"(dst), "r"(smem_u32(src)),
+                 "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;\n" ::: "memory"); }
+// the bulk stores issued by this thread have finished reading shared memory
+__device__ __forceinline__ void bulk_wait_read0() { asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory"); }
+// ... and have completed
+__device__ __forceinline__ void bulk_wait0() { asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory"); }
+// generic-proxy shared-memory accesses ordered before later async-proxy ones
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+
+// ---------------------------------------------------------------------
+// the kernel
+// ---------------------------------------------------------------------
+struct RBXArgs {
+    const float* src[3];
+    float* dst[3];
+    const float* rhs[3];
+    const float* alpha[3];
+    unsigned* err;
+};
+
+template <int C>
+__device__ __forceinline__ void rbx_run(const Grid& g, const RBXGeom& G, const StagOp<float>& A, const RBXArgs& R,
+                                        float omega, unsigned char* raw, int tile_y, int chunk) {
+    const int nx = g.n[0], ny = g.n[1], nz = g.n[2];
+    const int TY = G.TY, rows = G.rows, crows = G.crows;
+    const int tid = threadIdx.x;
+    const i64 nxy = (i64)nx * ny;
+    const int y0 = tile_y * TY;
+    const int k0 = (int)((long)chunk * nz / G.chunks), kend = (int)((long)(chunk + 1) * nz / G.chunks);
+    unsigned long long* bar = reinterpret_cast<unsigned long long*>(raw);
+    float* ph = reinterpret_cast<float*>(raw + 64);
+    const int plane = rows * nx, cplane = crows * nx;
+    float* cf = ph + RBX_NPH * plane;  // [slot][0 alpha, 1 rhs][crows][nx]
+    const float* src = R.src[C];
+    float* dst = R.dst[C];
+    const float* alpha = R.alpha[C];
+    const float* rhs = R.rhs[C];
+    // stage j = unknown plane j (always) + coefficient plane j-1 (for
+    // j >= k0); q = j - (k0 - 2) counts the stages of this CTA from 0
+    const int qend = kend + 1 - (k0 - 2);  // last stage index
+    // stage q issued by the producer warp: lane 0 arms the barrier with the
+    // stage's bytes, then lane 0 copies the unknown rows, lanes 1 and 2 the
+    // alpha and rhs rows.  A tile's rows are consecutive in global memory
+    // except across the periodic y wrap, so each array goes as one to three
+    // contiguous copies.
+    auto issue = [&](int q) {
+        const int lane = tid - RBX_THREADS;
+        const int j = q + k0 - 2;
+        const int s = q % RBX_NPH;
+        if (lane == 0) mbar_expect_tx(&bar[s], (unsigned)(sizeof(float) * (plane + (j >= k0 ? 2 * cplane : 0))));
+        __syncwarp();
+        auto copy = [&](float* sdst, const float* gplane, int nrows, int ring) {
+            int r = 0;
+            while (r < nrows) {
+                const int ys = wrapc(y0 + r - ring, ny);
+                const int n = nrows - r < ny - ys ? nrows - r : ny - ys;
+                bulk_g2s(sdst + r * nx, gplane + (i64)ys * nx, (unsigned)(sizeof(float) * n * nx), &bar[s]);
+                r += n;
+            }
+        };
+        if (lane == 0) copy(ph + s * plane, src + (i64)wrapc(j, nz) * nxy, rows, 2);
+        if (j >= k0 && (lane == 1 || lane == 2)) {
+            const int cs = pmod(j - 1, RBX_NCF);
+            const i64 zo = (i64)wrapc(j - 1, nz) * nxy;
+            copy(cf + (cs * 2 + lane - 1) * cplane, (lane == 1 ? alpha : rhs) + zo, crows, 1);
+        }
+    };
+    // wait for stage q; false on time-out
+    auto wait_stage = [&](int q) { return mbar_wait_bounded(&bar[q % RBX_NPH], (unsigned)((q / RBX_NPH) & 1)); };
+
+    const int hx = nx >> 1;           // cells of one colour per row
+    const int RG = RBX_THREADS / hx;  // rows updated at once
+    // a warp takes 16 cells of a colour on each of two adjacent rows: their
+    // colour offsets differ by one, so the two half-warps read the even and
+    // the odd banks and every shared access is one wavefront
+    const int hgrp = hx >> 4;  // 16-cell groups per row
+    const int wi = tid >> 5, ln = tid & 31;
+    const int h = (wi % hgrp) * 16 + (ln & 15);
+    const int gr = 2 * (wi / hgrp) + (ln >> 4);
+    int issued = 0;  // stages issued so far (thread 0)
+    // update of the cells of parity par on rows ly = ly0 + gr, + RG, .. < ly1
+    // of plane p (slots: unknown planes p-1, p, p+1; coefficients p).  RG
+    // is even, so the thread's column lx is the same on all its rows.  The
+    // RBX_MAXR rows are evaluated without branches and all new values are
+    // computed before any is stored (no cell of the colour reads another),
+    // so the rows' loads overlap; rows past ly1 read staged or pad memory
+    // and are not stored.
+    auto sweep = [&](int p, int par, int ly0, int ly1) {
+        const int lyb = ly0 + gr;
+        const int lx = 2 * h + ((y0 + lyb + p + par) & 1);
+        const int lxm = lx == 0 ? nx - 1 : lx - 1;
+        const int lxp = lx == nx - 1 ? 0 : lx + 1;
+        const int o = (lyb + 2) * nx, co = (lyb + 1) * nx + lx;
+        float* c0 = ph + pmod(p - (k0 - 2), RBX_NPH) * plane + o;
+        const float* zm = ph + pmod(p - 1 - (k0 - 2), RBX_NPH) * plane + o + lx;
+        const float* zp = ph + pmod(p + 1 - (k0 - 2), RBX_NPH) * plane + o + lx;
+        const float* ca = cf + (pmod(p, RBX_NCF) * 2) * cplane + co;
+        const float* cr = ca + cplane;
+        CellF P;  // no index is read by the constant-coefficient stencil
+        P.base = 0;
+        P.oxm = P.oxp = P.oym = P.oyp = P.ozm = P.ozp = 0;
+        float nv[RBX_MAXR];
+#pragma unroll
+        for (int m = 0; m < RBX_MAXR; m++) {
+            const int r = m * RBX_ROWSTEP;
+            const float* c = c0 + r;
+            float dg;
+            const float L = stag_lface_acc<float, 3, 1, C>(
+                A, P,
+                [&](int a, int b, int cz) {
+                    return cz < 0   ? zm[r]
+                           : cz > 0 ? zp[r]
+                           : b < 0  ? c[lx - nx]
+                           : b > 0  ? c[lx + nx]
+                           : a < 0  ? c[lxm]
+                           : a > 0  ? c[lxp]
+                                    : c[lx];
+                },
+                [&](int, int, int, int) { return 0.0f; }, [&]() { return ca[r]; }, dg);
+            nv[m] = c[lx] + sm_quot(omega * (cr[r] - L), dg);
+        }
+#pragma unroll
+        for (int m = 0; m < RBX_MAXR; m++)
+            if (lyb + m * RG < ly1) c0[m * RBX_ROWSTEP + lx] = nv[m];
+    };
+    // prologue: stages q = 0 .. 4 (unknown planes k0-2 .. k0+2, coefficient
+    // planes k0-1 .. k0+1) and AHEAD more
+    const bool producer = tid >= RBX_THREADS;
+    const int lead = RBX_THREADS;  // producer lane 0: stores and clean-up
+    if (producer) {
+        for (int q = 0; q < 5 + RBX_AHEAD && q <= qend; q++) issue(q);
+        issued = 5 + RBX_AHEAD < qend + 1 ? 5 + RBX_AHEAD : qend + 1;
+    }
+    bool ok = true;
+    if (!producer)
+        for (int q = 0; q < 5; q++) ok = ok && wait_stage(q);
+    if (__syncthreads_or(!ok)) goto fail;
+    // red of k0-1 .. k0+1 read only black cells, which none of them writes
+    if (!producer) {
+        sweep(k0 - 1, 0, -1, TY + 1);
+        sweep(k0, 0, -1, TY + 1);
+        sweep(k0 + 1, 0, -1, TY + 1);
+    }
+    for (int k = k0; k < kend; k++) {
+        // this thread's shared-memory writes of the previous step become
+        // visible to the bulk store issued below
+        fence_proxy_async();
+        if (__syncthreads_or(!ok)) goto fail;
+        if (producer) {
+            // the store of plane k-2 (issued last step) has read its slot,
+            // which stage k+3+AHEAD refills
+            if (tid == lead) bulk_wait_read0();
+            __syncwarp();
+            fence_proxy_async();
+            const int qn = k + 3 + RBX_AHEAD - (k0 - 2);
+            if (qn <= qend) {
+                issue(qn);
+                issued = qn + 1;
+            }
+            if (tid == lead && k > k0) {
+                const float* sp = ph + pmod(k - 1 - (k0 - 2), RBX_NPH) * plane + 2 * nx;
+                bulk_s2g(dst + (i64)(k - 1) * nxy + (i64)y0 * nx, sp, (unsigned)(sizeof(float) * TY * nx));
+                bulk_commit();
+            }
+            continue;
+        }
+        // stage k+3: unknown plane k+3, coefficient plane k+2
+        if (k + 3 - (k0 - 2) <= qend) ok = wait_stage(k + 3 - (k0 - 2));
+        if (!ok) continue;  // leaves at the next barrier
+        sweep(k, 1, 0, TY);
+        if (k + 2 <= kend) sweep(k + 2, 0, -1, TY + 1);
+    }
+    fence_proxy_async();
+    if (__syncthreads_or(!ok)) goto fail;
+    if (tid == lead) {
+        const float* sp = ph + pmod(kend - 1 - (k0 - 2), RBX_NPH) * plane + 2 * nx;
+        bulk_s2g(dst + (i64)(kend - 1) * nxy + (i64)y0 * nx, sp, (unsigned)(sizeof(float) * TY * nx));
+        bulk_commit();
+        bulk_wait0();
+    }
+    return;
+fail:
+    // a stage did not arrive in time: flag it, let the copies in flight
+    // land (bounded) and leave
+    if (tid == lead) {
+        atomicOr(R.err, 1u);
+        bulk_wait0();
+        // stages before the last RBX_NPH issued completed before their
+        // barriers were re-armed
+        for (int q = issued > RBX_NPH ? issued - RBX_NPH : 0; q < issued; q++) wait_stage(q);
+    }
+}
+
+__global__ void __launch_bounds__(RBX_BLOCK, 1) k_stag_rbx(Grid g, RBXGeom G, StagOp<float> A, RBXArgs R,
+                                                            float omega) {
+    extern __shared__ __align__(128) unsigned char rbx_raw[];
+    if (threadIdx.x < RBX_NPH) mbar_init(reinterpret_cast<unsigned long long*>(rbx_raw) + threadIdx.x, 1);
+    if (threadIdx.x == 0) mbar_init_fence();
+    __syncthreads();
+    const int tile_y = blockIdx.x, chunk = blockIdx.y;
+    if (blockIdx.z == 0) rbx_run<0>(g, G, A, R, omega, rbx_raw, tile_y, chunk);
+    else if (blockIdx.z == 1) rbx_run<1>(g, G, A, R, omega, rbx_raw, tile_y, chunk);
+    else rbx_run<2>(g, G, A, R, omega, rbx_raw, tile_y, chunk);
+}
+
+// geometry for a level (sms: multiprocessors of the device); false when the
+// level cannot use this smoother
+inline bool rbx_geom(const Grid& g, int sms, RBXGeom& G) {
+    if (g.dim != 3) return false;
+    const int nx = g.n[0], ny = g.n[1], nz = g.n[2];
+    if (nx > RBX_MAXNX || nx < 64 || (nx & (nx - 1)) || (ny & 1) || (nz & 1) || nz < 4) return false;
+    const int hx = nx / 2;
+    if (RBX_THREADS % hx || hx % 16 || (RBX_THREADS / 32) % (hx / 16)) return false;
+    // tallest tile that fits the shared memory of one CTA per SM
+    G.TY = 0;
+    for (int ty = 32; ty >= 4; ty /= 2) {
+        if (ny % ty) continue;
+        const size_t smem = 64 + sizeof(float) * ((size_t)RBX_NPH * (ty + 4) * nx +
+                                                  (size_t)RBX_NCF * 2 * (ty + 2) * nx + RBX_PAD);
+        if (smem <= 200 * 1024) {
+            G.TY = ty;
+            G.smem = smem;
+            break;
+        }
+    }
+    if (!G.TY) return false;
+    // rows per thread and sweep (ring rows included) within RBX_MAXR
+    const int RG = RBX_THREADS / hx;
+    while (G.TY > 4 && (G.TY + 2 + RG - 1) / RG > RBX_MAXR) G.TY /= 2;
+    if ((G.TY + 2 + RG - 1) / RG > RBX_MAXR || ny % G.TY) return false;
+    G.smem = 64 + sizeof(float) * ((size_t)RBX_NPH * (G.TY + 4) * nx + (size_t)RBX_NCF * 2 * (G.TY + 2) * nx +
+                                   RBX_PAD);
+    G.rows = G.TY + 4;
+    G.crows = G.TY + 2;
+    G.tiles_y = ny / G.TY;
+    // z-runs: nz split into `chunks` runs of nz/chunks planes (rounded), the
+    // count that gives the busiest SM (one CTA per SM) the fewest plane
+    // steps, each run paying five prologue planes
+    long best = -1;
+    G.chunks = 0;
+    for (int c = 1; c <= nz / 4; c++) {
+        const long items = (long)G.tiles_y * 3 * c;
+        const long rounds = (items + sms - 1) / sms;
+        const long cost = rounds * ((nz + c - 1) / c + 5);
+        if (best < 0 || cost < best) {
+            best = cost;
+            G.chunks = c;
+        }
+    }
+    if (!G.chunks) return false;
+    G.KZ = (nz + G.chunks - 1) / G.chunks;
+    return true;
+}
+
+}  // namespace fhd

@@ -13,6 +13,7 @@
 
 #include "fhd_solver.cuh"
 #include "fhd_coarse.cuh"
+#include "fhd_rbx.cuh"
 
 namespace fhd {
 
@@ -439,6 +440,32 @@ static int stag_rb_smooth(fhd_ctx* ctx, StagLevel<T>& L, const RBGeom& G, T* con
     return rc;
 }
 
+// one full smooth a -> b of every component with the row-tile smoother
+// (FP32, visc_type 1)
+static int stag_rbx_smooth(fhd_ctx* ctx, StagLevel<float>& L, const RBXGeom& G, float* const a[3],
+                           float* const b[3]) {
+    RBXArgs R;
+    for (int c = 0; c < 3; c++) {
+        R.src[c] = a[c];
+        R.dst[c] = b[c];
+        R.rhs[c] = L.rhs[c];
+        R.alpha[c] = L.alpha[c];
+    }
+    R.err = ctx->dev_err;
+    const bool timed = ctx->prof && L.g.nc == ctx->g0.nc;
+    if (timed) {
+        prof_mark(ctx, ctx->stream);
+        ctx->prof_bytes += rb_smooth_bytes(ctx, L);
+        ctx->prof_launches++;
+    }
+    if (int rc = rb_allow_smem(k_stag_rbx, G.smem)) return rc;
+    k_stag_rbx<<<dim3(G.tiles_y, G.chunks, 3), RBX_BLOCK, G.smem, ctx->stream>>>(L.g, G, L.op(), R,
+                                                                                 (float)ctx->p.stag_mg_omega);
+    int rc = post(ctx);
+    if (timed) prof_mark(ctx, ctx->stream);
+    return rc;
+}
+
 template <typename T>
 static int stag_smooths(fhd_ctx* ctx, StagLevel<T>& L, int count) {
     const int dim = ctx->dim;
@@ -448,7 +475,22 @@ static int stag_smooths(fhd_ctx* ctx, StagLevel<T>& L, int count) {
     for (int c = 0; c < dim; c++)
         aligned = aligned && rb_aligned(L.phi[c]) && rb_aligned(L.tmp[c]) && rb_aligned(L.rhs[c]) &&
                   rb_aligned(L.alpha[c]);
-    if (ctx->p.stag_mg_smoother != 0 && count >= 2 && aligned && rb_use(L.g) && rb_geom(L.g, 3, (int)sizeof(T), G)) {
+    if constexpr (std::is_same<T, float>::value) {
+        RBXGeom X;
+        if (ctx->p.stag_mg_smoother != 0 && ctx->visc == 1 && count >= 2 && aligned && !rb_use(L.g) &&
+            ctx->fused_mode != 0 && rbx_geom(L.g, ctx->sms, X)) {
+            float* a[3] = {L.phi[0], L.phi[1], L.phi[2]};
+            float* b[3] = {L.tmp[0], L.tmp[1], L.tmp[2]};
+            for (; m0 + 2 <= count; m0 += 2) {
+                int rc = stag_rbx_smooth(ctx, L, X, a, b);
+                if (rc) return rc;
+                rc = stag_rbx_smooth(ctx, L, X, b, a);
+                if (rc) return rc;
+            }
+        }
+    }
+    if (ctx->p.stag_mg_smoother != 0 && count - m0 >= 2 && aligned && rb_use(L.g) &&
+        rb_geom(L.g, 3, (int)sizeof(T), G)) {
         // pairs of fused smooths phi -> tmp -> phi
         T* a[3] = {L.phi[0], L.phi[1], L.phi[2]};
         T* b[3] = {L.tmp[0], L.tmp[1], L.tmp[2]};
@@ -1054,6 +1096,20 @@ int stokes_apply(fhd_ctx* ctx, CSVec<double> x, CSVec<double> rhs, SVec<double> 
     return rc;
 }
 
+// a bounded wait inside a kernel that ran out (the kernel set the context's
+// error word and returned); cleared on read
+int dev_err_check(fhd_ctx* ctx) {
+    unsigned h = 0;
+    FHD_CUDA_TRY(cudaMemcpyAsync(&h, ctx->dev_err, sizeof(unsigned), cudaMemcpyDeviceToHost, ctx->stream));
+    FHD_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    if (h) {
+        FHD_CUDA_TRY(cudaMemsetAsync(ctx->dev_err, 0, sizeof(unsigned), ctx->stream));
+        set_last_error("a staging wait inside the fused smoother timed out");
+        return FHD_ERR_CUDA;
+    }
+    return 0;
+}
+
 int sync_scalars(fhd_ctx* ctx, int first, int count) {
     FHD_CUDA_TRY(cudaMemcpyAsync(ctx->hscal + first, ctx->dscal + first, sizeof(double) * count,
                                  cudaMemcpyDeviceToHost, ctx->stream));
@@ -1373,6 +1429,7 @@ int gmres_dev(fhd_ctx* ctx, CSVec<double> b, SVec<double> x, double* norm_pre_rh
             FHD_CUDA_TRY(cudaStreamSynchronize(st));
         }
     }
+    if ((rc = dev_err_check(ctx))) return rc;
     S.outer_iters = iter;
     S.total_iters = total_iter;
     S.vcycles = ctx->vcycles;
@@ -1498,11 +1555,20 @@ int fhd_ctx_create(int dim, const int n_cells[3], const double dx[3], int visc_t
         c->red_partials = c->arena.alloc<double>(RED_MAX_BLOCKS);
         c->red_counter = (unsigned*)c->arena.alloc<double>(1);
         c->dscal = c->arena.alloc<double>(NSCAL);
-        if (!c->V || !c->r || !c->w || !c->tmp || !c->xs || !c->red_partials || !c->red_counter || !c->dscal)
+        c->dev_err = (unsigned*)c->arena.alloc<double>(1);
+        if (!c->V || !c->r || !c->w || !c->tmp || !c->xs || !c->red_partials || !c->red_counter || !c->dscal ||
+            !c->dev_err)
             rc = FHD_ERR_OOM;
     }
     if (!rc && !(c->hscal = pinned_scalars_acquire())) rc = FHD_ERR_OOM;
     if (!rc && cudaMemsetAsync(c->red_counter, 0, sizeof(double), c->stream) != cudaSuccess) rc = FHD_ERR_CUDA;
+    if (!rc && cudaMemsetAsync(c->dev_err, 0, sizeof(double), c->stream) != cudaSuccess) rc = FHD_ERR_CUDA;
+    if (!rc) {
+        int dev = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+            rc = FHD_ERR_CUDA;
+    }
     if (!rc && cudaStreamSynchronize(c->stream) != cudaSuccess) rc = FHD_ERR_CUDA;
     if (rc) {
         fhd_ctx_destroy(c);
@@ -1576,6 +1642,15 @@ int fhd_ctx_set_coarse(fhd_ctx* c, int mode) {
     return FHD_OK;
 }
 
+int fhd_ctx_set_fused(fhd_ctx* c, int mode) {
+    if (!c || mode < -1 || mode > 1) return FHD_ERR_BAD_ARG;
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess) return FHD_ERR_CUDA;
+    // captured preconditioner graphs hold the other launch sequence
+    release_graphs(c);
+    c->fused_mode = mode;
+    return FHD_OK;
+}
+
 int fhd_ctx_set_graphs(fhd_ctx* c, int mode) {
     if (!c || mode < -1 || mode > 1) return FHD_ERR_BAD_ARG;
     if (cudaStreamSynchronize(c->stream) != cudaSuccess) return FHD_ERR_CUDA;
@@ -1602,6 +1677,7 @@ static int finish(fhd_ctx* ctx, int rc) {
         set_last_error(cudaGetErrorString(cudaGetLastError()));
         return FHD_ERR_CUDA;
     }
+    if (int e = dev_err_check(ctx)) return e;
     return rc;
 }
 

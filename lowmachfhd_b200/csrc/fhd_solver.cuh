@@ -235,6 +235,10 @@ struct fhd_ctx {
     int graph_mode = -1;
     // the coarse multigrid levels in one CTA (-1 default: on, 0 off)
     int coarse_mode = -1;
+    // the row-tile fused smoother on large FP32 levels (-1 default: on, 0 off)
+    int fused_mode = -1;
+    int sms = 148;                // multiprocessors of the device
+    unsigned* dev_err = nullptr;  // set by a kernel whose bounded wait ran out
     struct PreconGraph {
         unsigned long long key = 0;
         cudaGraphExec_t exec = nullptr;
@@ -283,6 +287,7 @@ int prepare(fhd_ctx* ctx, const double* const alpha_fc[], const double* beta, co
 int stag_mg_solve_dev(fhd_ctx* ctx, double* const phi[], const double* const rhs[]);
 int gmres_dev(fhd_ctx* ctx, CSVec<double> b, SVec<double> x, double* norm_pre_rhs, fhd_solve_stats* st);
 int sync_scalars(fhd_ctx* ctx, int first, int count);
+int dev_err_check(fhd_ctx* ctx);
 int mass_fluxdiv(fhd_ctx* ctx, const fhd_mixture_params* mp, const fhd_stoch_params* sp, const double* const rho[],
                  double dt, const double* weights, int n_rngs, const double* const W[], double* const fluxdiv[]);
 int mass_flag_check(fhd_ctx* ctx);
