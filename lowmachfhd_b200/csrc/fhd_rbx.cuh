@@ -23,12 +23,14 @@
 // CTA leaves together (after its copies in flight have landed, again with a
 // bound) through the step barrier's reduction.
 #pragma once
+#include <type_traits>
+
 #include "fhd_kernels.cuh"
 
 namespace fhd {
 
-constexpr int RBX_THREADS = 256;
-constexpr int RBX_AHEAD = 2;            // stages in flight beyond the one awaited
+constexpr int RBX_THREADS = 256;  // compute threads
+constexpr int RBX_AHEAD = 3;            // stages in flight beyond the one awaited
 constexpr int RBX_NPH = 5 + RBX_AHEAD;  // unknown planes k-1 .. k+3 + in flight
 constexpr int RBX_NCF = 3 + RBX_AHEAD;  // coefficient planes k .. k+2 + in flight
 constexpr int RBX_MAXNX = 256;
@@ -40,10 +42,20 @@ constexpr int RBX_ROWSTEP = 2 * RBX_THREADS;
 constexpr int RBX_MAXR = 5;
 // the block: RBX_THREADS compute threads and one producer warp
 constexpr int RBX_BLOCK = RBX_THREADS + 32;
-// every thread evaluates RBX_MAXR rows per sweep and stores only those of
-// the tile; the reads of the others may run up to this many elements past
-// the last staged buffer, into a pad at the end of shared memory
-constexpr int RBX_PAD = RBX_MAXR * RBX_ROWSTEP + 2 * RBX_MAXNX;
+// Every thread evaluates RBX_MAXR rows per sweep and stores only those of
+// the tile.  The reads of the others stay below RBX_MAXR * RBX_ROWSTEP +
+// 2 nx elements from the start of an unknown plane slot and below
+// RBX_MAXR * RBX_ROWSTEP from the start of a coefficient slot; shared memory
+// holds the coefficient ring, then the unknown ring, then a pad that covers
+// the last unknown slot's overrun.
+inline int rbx_pad(int nx, int rows) {
+    const int over = RBX_MAXR * RBX_ROWSTEP + 2 * nx - rows * nx;
+    return (over > 0 ? over : 0) + 32;
+}
+inline size_t rbx_smem_bytes(int nx, int ty) {
+    return 64 + sizeof(float) * ((size_t)RBX_NCF * 2 * (ty + 2) * nx + (size_t)RBX_NPH * (ty + 4) * nx +
+                                 rbx_pad(nx, ty + 4));
+}
 
 struct RBXGeom {
     int TY;       // tile rows (divides ny)
@@ -125,9 +137,9 @@ __device__ __forceinline__ void rbx_run(const Grid& g, const RBXGeom& G, const S
     const int y0 = tile_y * TY;
     const int k0 = (int)((long)chunk * nz / G.chunks), kend = (int)((long)(chunk + 1) * nz / G.chunks);
     unsigned long long* bar = reinterpret_cast<unsigned long long*>(raw);
-    float* ph = reinterpret_cast<float*>(raw + 64);
     const int plane = rows * nx, cplane = crows * nx;
-    float* cf = ph + RBX_NPH * plane;  // [slot][0 alpha, 1 rhs][crows][nx]
+    float* cf = reinterpret_cast<float*>(raw + 64);  // [slot][0 alpha, 1 rhs][crows][nx]
+    float* ph = cf + RBX_NCF * 2 * cplane;          // [slot][rows][nx]
     const float* src = R.src[C];
     float* dst = R.dst[C];
     const float* alpha = R.alpha[C];
@@ -182,23 +194,28 @@ __device__ __forceinline__ void rbx_run(const Grid& g, const RBXGeom& G, const S
     // computed before any is stored (no cell of the colour reads another),
     // so the rows' loads overlap; rows past ly1 read staged or pad memory
     // and are not stored.
-    auto sweep = [&](int p, int par, int ly0, int ly1) {
+    // NR rows per thread (RBX_MAXR - 1 cover the tile rows, RBX_MAXR the
+    // tile and its ring);
+    // sm / sc / sp: ring slots of unknown planes p-1, p, p+1, scf: the
+    // coefficient slot of plane p
+    auto sweep = [&](auto NRc, int sm, int sc, int sp, int scf, int p, int par, int ly0, int ly1) {
+        constexpr int NR = decltype(NRc)::value;
         const int lyb = ly0 + gr;
         const int lx = 2 * h + ((y0 + lyb + p + par) & 1);
         const int lxm = lx == 0 ? nx - 1 : lx - 1;
         const int lxp = lx == nx - 1 ? 0 : lx + 1;
         const int o = (lyb + 2) * nx, co = (lyb + 1) * nx + lx;
-        float* c0 = ph + pmod(p - (k0 - 2), RBX_NPH) * plane + o;
-        const float* zm = ph + pmod(p - 1 - (k0 - 2), RBX_NPH) * plane + o + lx;
-        const float* zp = ph + pmod(p + 1 - (k0 - 2), RBX_NPH) * plane + o + lx;
-        const float* ca = cf + (pmod(p, RBX_NCF) * 2) * cplane + co;
+        float* c0 = ph + sc * plane + o;
+        const float* zm = ph + sm * plane + o + lx;
+        const float* zp = ph + sp * plane + o + lx;
+        const float* ca = cf + (scf * 2) * cplane + co;
         const float* cr = ca + cplane;
         CellF P;  // no index is read by the constant-coefficient stencil
         P.base = 0;
         P.oxm = P.oxp = P.oym = P.oyp = P.ozm = P.ozp = 0;
-        float nv[RBX_MAXR];
+        float nv[NR];
 #pragma unroll
-        for (int m = 0; m < RBX_MAXR; m++) {
+        for (int m = 0; m < NR; m++) {
             const int r = m * RBX_ROWSTEP;
             const float* c = c0 + r;
             float dg;
@@ -217,7 +234,7 @@ __device__ __forceinline__ void rbx_run(const Grid& g, const RBXGeom& G, const S
             nv[m] = c[lx] + sm_quot(omega * (cr[r] - L), dg);
         }
 #pragma unroll
-        for (int m = 0; m < RBX_MAXR; m++)
+        for (int m = 0; m < NR; m++)
             if (lyb + m * RG < ly1) c0[m * RBX_ROWSTEP + lx] = nv[m];
     };
     // prologue: stages q = 0 .. 4 (unknown planes k0-2 .. k0+2, coefficient
@@ -228,16 +245,22 @@ __device__ __forceinline__ void rbx_run(const Grid& g, const RBXGeom& G, const S
         for (int q = 0; q < 5 + RBX_AHEAD && q <= qend; q++) issue(q);
         issued = 5 + RBX_AHEAD < qend + 1 ? 5 + RBX_AHEAD : qend + 1;
     }
+    using RRed = std::integral_constant<int, RBX_MAXR>;
+    using RBlack = std::integral_constant<int, RBX_MAXR - 1>;
+    auto slot = [&](int p) { return pmod(p - (k0 - 2), RBX_NPH); };
+    auto ring = [](int v, int d, int n) { return v + d >= n ? v + d - n : v + d; };
+    int sl, scl;
     bool ok = true;
     if (!producer)
         for (int q = 0; q < 5; q++) ok = ok && wait_stage(q);
     if (__syncthreads_or(!ok)) goto fail;
     // red of k0-1 .. k0+1 read only black cells, which none of them writes
-    if (!producer) {
-        sweep(k0 - 1, 0, -1, TY + 1);
-        sweep(k0, 0, -1, TY + 1);
-        sweep(k0 + 1, 0, -1, TY + 1);
-    }
+    if (!producer)
+        for (int p = k0 - 1; p <= k0 + 1; p++) sweep(RRed(), slot(p - 1), slot(p), slot(p + 1), pmod(p, RBX_NCF), p, 0, -1, TY + 1);
+    // ring slots of unknown plane k-1 and coefficient plane k, advanced by one
+    // per step
+    sl = slot(k0 - 1);
+    scl = pmod(k0, RBX_NCF);
     for (int k = k0; k < kend; k++) {
         // this thread's shared-memory writes of the previous step become
         // visible to the bulk store issued below
@@ -264,8 +287,12 @@ __device__ __forceinline__ void rbx_run(const Grid& g, const RBXGeom& G, const S
         // stage k+3: unknown plane k+3, coefficient plane k+2
         if (k + 3 - (k0 - 2) <= qend) ok = wait_stage(k + 3 - (k0 - 2));
         if (!ok) continue;  // leaves at the next barrier
-        sweep(k, 1, 0, TY);
-        if (k + 2 <= kend) sweep(k + 2, 0, -1, TY + 1);
+        const int s1 = ring(sl, 1, RBX_NPH), s2 = ring(sl, 2, RBX_NPH);
+        sweep(RBlack(), sl, s1, s2, scl, k, 1, 0, TY);
+        if (k + 2 <= kend)
+            sweep(RRed(), s2, ring(sl, 3, RBX_NPH), ring(sl, 4, RBX_NPH), ring(scl, 2, RBX_NCF), k + 2, 0, -1, TY + 1);
+        sl = s1;
+        scl = ring(scl, 1, RBX_NCF);
     }
     fence_proxy_async();
     if (__syncthreads_or(!ok)) goto fail;
@@ -302,7 +329,7 @@ __global__ void __launch_bounds__(RBX_BLOCK, 1) k_stag_rbx(Grid g, RBXGeom G, St
 
 // geometry for a level (sms: multiprocessors of the device); false when the
 // level cannot use this smoother
-inline bool rbx_geom(const Grid& g, int sms, RBXGeom& G) {
+inline bool rbx_geom(const Grid& g, int sms, size_t smem_max, RBXGeom& G) {
     if (g.dim != 3) return false;
     const int nx = g.n[0], ny = g.n[1], nz = g.n[2];
     if (nx > RBX_MAXNX || nx < 64 || (nx & (nx - 1)) || (ny & 1) || (nz & 1) || nz < 4) return false;
@@ -312,9 +339,8 @@ inline bool rbx_geom(const Grid& g, int sms, RBXGeom& G) {
     G.TY = 0;
     for (int ty = 32; ty >= 4; ty /= 2) {
         if (ny % ty) continue;
-        const size_t smem = 64 + sizeof(float) * ((size_t)RBX_NPH * (ty + 4) * nx +
-                                                  (size_t)RBX_NCF * 2 * (ty + 2) * nx + RBX_PAD);
-        if (smem <= 200 * 1024) {
+        const size_t smem = rbx_smem_bytes(nx, ty);
+        if (smem <= smem_max) {
             G.TY = ty;
             G.smem = smem;
             break;
@@ -324,9 +350,8 @@ inline bool rbx_geom(const Grid& g, int sms, RBXGeom& G) {
     // rows per thread and sweep (ring rows included) within RBX_MAXR
     const int RG = RBX_THREADS / hx;
     while (G.TY > 4 && (G.TY + 2 + RG - 1) / RG > RBX_MAXR) G.TY /= 2;
-    if ((G.TY + 2 + RG - 1) / RG > RBX_MAXR || ny % G.TY) return false;
-    G.smem = 64 + sizeof(float) * ((size_t)RBX_NPH * (G.TY + 4) * nx + (size_t)RBX_NCF * 2 * (G.TY + 2) * nx +
-                                   RBX_PAD);
+    if ((G.TY + 2 + RG - 1) / RG > RBX_MAXR || (G.TY + RG - 1) / RG > RBX_MAXR - 1 || ny % G.TY) return false;
+    G.smem = rbx_smem_bytes(nx, G.TY);
     G.rows = G.TY + 4;
     G.crows = G.TY + 2;
     G.tiles_y = ny / G.TY;

@@ -478,7 +478,7 @@ static int stag_smooths(fhd_ctx* ctx, StagLevel<T>& L, int count) {
     if constexpr (std::is_same<T, float>::value) {
         RBXGeom X;
         if (ctx->p.stag_mg_smoother != 0 && ctx->visc == 1 && count >= 2 && aligned && !rb_use(L.g) &&
-            ctx->fused_mode != 0 && rbx_geom(L.g, ctx->sms, X)) {
+            ctx->fused_mode != 0 && rbx_geom(L.g, ctx->sms, (size_t)ctx->smem_optin, X)) {
             float* a[3] = {L.phi[0], L.phi[1], L.phi[2]};
             float* b[3] = {L.tmp[0], L.tmp[1], L.tmp[2]};
             for (; m0 + 2 <= count; m0 += 2) {
@@ -1566,7 +1566,8 @@ int fhd_ctx_create(int dim, const int n_cells[3], const double dx[3], int visc_t
     if (!rc) {
         int dev = 0;
         if (cudaGetDevice(&dev) != cudaSuccess ||
-            cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+            cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&c->smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess)
             rc = FHD_ERR_CUDA;
     }
     if (!rc && cudaStreamSynchronize(c->stream) != cudaSuccess) rc = FHD_ERR_CUDA;

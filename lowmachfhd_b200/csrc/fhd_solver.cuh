@@ -238,6 +238,7 @@ struct fhd_ctx {
     // the row-tile fused smoother on large FP32 levels (-1 default: on, 0 off)
     int fused_mode = -1;
     int sms = 148;                // multiprocessors of the device
+    int smem_optin = 48 * 1024;   // shared memory a block may opt in to
     unsigned* dev_err = nullptr;  // set by a kernel whose bounded wait ran out
     struct PreconGraph {
         unsigned long long key = 0;
