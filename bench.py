@@ -582,16 +582,17 @@ def main():
         "gmres_iters_per_s": ws * sum(sum(x) for x in mixed["iters"]) / (mixed["ms"] / 1e3),
         "corrector_resid_over_pre_rhs": mixed["resid"],
         "gpu_launches": mixed["launches"],
-        "roofline": {"kernel": "k_stag_gs (finest-level colour Gauss-Seidel sweep)", "bound": "hbm",
-                     "achieved": achieved, "peak": hbm, "unit": "GB/s",
+        "roofline": {"kernel": "k_stag_rbx (finest-level fused red-black smooth of all three components)",
+                     "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": (achieved / hbm) if achieved else None,
-                     # ncu DRAM read+write of the same kernel captured at
-                     # 192^3 (85.0 + 3.5 MB), scaled by cells to 256^3
-                     "traffic": 88.5e6 * (256 / 192) ** 3,
-                     "traffic_source": "ncu capture at 192^3 scaled by cells",
+                     # ncu DRAM read + write of one launch of the same kernel
+                     # on the 256^3 finest level (622.7 + 178.5 MB)
+                     "traffic": (622.7 + 178.5) * 1e6,
+                     "traffic_source": "ncu capture of one 256^3 launch",
                      "peak_kind": peak_kind, "launches_timed": n_l,
                      "avg_launch_us": (ms_l / n_l * 1e3) if n_l else None,
                      "bytes_per_launch": (bytes_l / n_l) if n_l else None,
+                     "fp64_kernel": "k_stag_gs (FP64 finest-level colour sweep)",
                      "fp64_achieved": achieved64},
         "clocks": mixed["clocks"],
         "e2e": {"value": ws * K / (results["e2e"]["ms"] / 1e3), "unit": "steps/s",
