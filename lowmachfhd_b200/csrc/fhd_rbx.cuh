@@ -30,13 +30,7 @@
 namespace fhd {
 
 constexpr int RBX_THREADS = 256;  // compute threads
-#ifndef FHD_RBX_AHEAD
-#define FHD_RBX_AHEAD 3
-#endif
-#ifndef FHD_RBX_MAXTY
-#define FHD_RBX_MAXTY 32
-#endif
-constexpr int RBX_AHEAD = FHD_RBX_AHEAD;  // stages in flight beyond the one awaited
+constexpr int RBX_AHEAD = 3;            // stages in flight beyond the one awaited
 constexpr int RBX_NPH = 5 + RBX_AHEAD;  // unknown planes k-1 .. k+3 + in flight
 constexpr int RBX_NCF = 3 + RBX_AHEAD;  // coefficient planes k .. k+2 + in flight
 constexpr int RBX_MAXNX = 256;
@@ -343,7 +337,7 @@ inline bool rbx_geom(const Grid& g, int sms, size_t smem_max, RBXGeom& G) {
     if (RBX_THREADS % hx || hx % 16 || (RBX_THREADS / 32) % (hx / 16)) return false;
     // tallest tile that fits the shared memory of one CTA per SM
     G.TY = 0;
-    for (int ty = FHD_RBX_MAXTY; ty >= 4; ty /= 2) {
+    for (int ty = 32; ty >= 4; ty /= 2) {
         if (ny % ty) continue;
         const size_t smem = rbx_smem_bytes(nx, ty);
         if (smem <= smem_max) {

@@ -1307,7 +1307,6 @@ int gmres_dev(fhd_ctx* ctx, CSVec<double> b, SVec<double> x, double* norm_pre_rh
         return 0;
     }
     std::vector<double> H((m + 2) * (m + 2), 0.0), cs(m + 2), sn(m + 2), s(m + 2), y(m + 2);
-    std::vector<double> sv(m + 2, 1.0);  // scale of each stored Krylov vector
     auto Hh = [&](int i, int j) -> double& { return H[i * (m + 2) + j]; };
     int total_iter = 0, iter = 0, i_copy = 0;
     double norm_resid = 0, norm_init_resid = 0, norm_resid_Stokes = 0, norm_init_Stokes = 0, norm_resid_est = 0;
@@ -1344,7 +1343,6 @@ int gmres_dev(fhd_ctx* ctx, CSVec<double> b, SVec<double> x, double* norm_pre_rh
         iter++;
         k_scale_div<<<nb, 256, 0, st>>>(nc, ncomp, V(0), csv(r), norm_resid);
         FHD_POST(ctx);
-        sv[0] = 1.0;
         std::fill(s.begin(), s.end(), 0.0);
         s[1] = norm_resid;
         for (int i = 1; i <= m; i++) {
@@ -1352,37 +1350,33 @@ int gmres_dev(fhd_ctx* ctx, CSVec<double> b, SVec<double> x, double* norm_pre_rh
             i_copy = i;
             if ((rc = stokes_apply(ctx, csv(V(i - 1)), csv(V(i - 1)), tmp, 0))) return rc;
             if ((rc = precon_graphed(ctx, csv(tmp), w))) return rc;
-            // modified Gram-Schmidt with device-resident coefficients on the
-            // stored vectors u_k (V_k = sv[k] u_k): w here is
-            // M^-1 A u_{i-1} = (true w) / sv[i-1]; the last pass writes the
-            // orthogonalised vector into V(i) unnormalised
+            // modified Gram-Schmidt with device-resident coefficients
             for (int k = 1; k <= i; k++) {
                 CSVec<double> none;
                 for (int c = 0; c < 4; c++) none.c[c] = nullptr;
-                k_mgs<<<nb, RED_THREADS, 0, st>>>(nc, ncomp, csv(w), w, k > 1 ? csv(V(k - 2)) : none,
-                                                  k > 1 ? ctx->dscal + S_H + k - 1 : nullptr,
-                                                  k > 1 ? sv[k - 2] : 0.0, csv(V(k - 1)), sv[k - 1], wp * wp,
+                k_mgs<<<nb, RED_THREADS, 0, st>>>(nc, ncomp, w, k > 1 ? csv(V(k - 2)) : none,
+                                                  k > 1 ? ctx->dscal + S_H + k - 1 : nullptr, csv(V(k - 1)), wp * wp,
                                                   slot(ctx, S_H + k));
                 FHD_POST(ctx);
             }
             {
                 CSVec<double> none;
                 for (int c = 0; c < 4; c++) none.c[c] = nullptr;
-                k_mgs<<<nb, RED_THREADS, 0, st>>>(nc, ncomp, csv(w), V(i), csv(V(i - 1)), ctx->dscal + S_H + i,
-                                                  sv[i - 1], none, 1.0, wp * wp, slot(ctx, S_NRM));
+                k_mgs<<<nb, RED_THREADS, 0, st>>>(nc, ncomp, w, csv(V(i - 1)), ctx->dscal + S_H + i, none, wp * wp,
+                                                  slot(ctx, S_NRM));
                 FHD_POST(ctx);
             }
+            k_scale_by_norm<<<nb, 256, 0, st>>>(nc, ncomp, V(i), csv(w), ctx->dscal + S_NRM);
+            FHD_POST(ctx);
             FHD_CUDA_TRY(cudaMemcpyAsync(ctx->hscal + S_H + 1, ctx->dscal + S_H + 1, sizeof(double) * i,
                                          cudaMemcpyDeviceToHost, st));
             if ((rc = sync_scalars(ctx, S_NRM, 1))) return rc;
-            for (int k = 1; k <= i; k++) Hh(k, i) = sv[i - 1] * ctx->hscal[S_H + k];
-            const double nw = sqrt(ctx->hscal[S_NRM]);
-            Hh(i + 1, i) = sv[i - 1] * nw;
+            for (int k = 1; k <= i; k++) Hh(k, i) = ctx->hscal[S_H + k];
+            Hh(i + 1, i) = sqrt(ctx->hscal[S_NRM]);
             if (Hh(i + 1, i) == 0.0) {
                 set_last_error("gmres: error in orthogonalization");
                 return FHD_ERR_ORTHO_BREAKDOWN;
             }
-            sv[i] = 1.0 / nw;
             // least_squares + rotmat (gmres.f90:531-597)
             for (int k = 1; k <= i - 1; k++) {
                 double t = cs[k] * Hh(k, i) + sn[k] * Hh(k + 1, i);
@@ -1426,7 +1420,7 @@ int gmres_dev(fhd_ctx* ctx, CSVec<double> b, SVec<double> x, double* norm_pre_rh
                 for (int jj = ii + 1; jj <= k + 1; jj++) acc += Hh(ii, jj) * y[jj];
                 y[ii] = (s[ii] - acc) / Hh(ii, ii);
             }
-            for (int it = 1; it <= i_copy; it++) ctx->hscal[S_Y + it - 1] = y[it] * sv[it - 1];
+            for (int it = 1; it <= i_copy; it++) ctx->hscal[S_Y + it - 1] = y[it];
             FHD_CUDA_TRY(cudaMemcpyAsync(ctx->dscal + S_Y, ctx->hscal + S_Y, sizeof(double) * i_copy,
                                          cudaMemcpyHostToDevice, st));
             k_update_sol<<<nb, 256, 0, st>>>(nc, ncomp, x, ctx->V, vstride, ctx->dscal + S_Y, i_copy);

@@ -94,16 +94,13 @@ static __global__ void __launch_bounds__(RED_THREADS) k_sum(i64 n, const T* a, R
     red_finish(s, rs);
 }
 
-// One modified Gram-Schmidt pass of gmres (gmres.f90:352-378) on stored,
-// unnormalised Krylov vectors u_k (the basis vector is V_k = s_k u_k, the
-// scales s_k known on the host): x = w - (h_prev s_prev) u_prev (when
-// hprev), written to wout, and the weighted inner product of x with
-// s_next u_next (or with itself, the squared norm, when vnext is null)
-// reduced into rs.
-static __global__ void __launch_bounds__(RED_THREADS) k_mgs(i64 n, int ncomp, CSVec<double> w, SVec<double> wout,
-                                                     CSVec<double> vprev, const double* hprev, double sprev,
-                                                     CSVec<double> vnext, double snext, double wp2, RedSlot rs) {
-    const double h = hprev ? *hprev * sprev : 0.0;
+// Modified Gram-Schmidt step (gmres.f90:352-378), fused: w -= h*vprev with
+// h read from device memory, then the weighted dot of the updated w with
+// vnext (or with itself when vnext is null).
+static __global__ void __launch_bounds__(RED_THREADS) k_mgs(i64 n, int ncomp, SVec<double> w, CSVec<double> vprev,
+                                                     const double* hprev, CSVec<double> vnext, double wp2,
+                                                     RedSlot rs) {
+    const double h = hprev ? *hprev : 0.0;
     double s = 0.0;
     for (i64 f = blockIdx.x * (i64)blockDim.x + threadIdx.x; f < n; f += (i64)gridDim.x * blockDim.x) {
         double su = 0.0;
@@ -111,15 +108,23 @@ static __global__ void __launch_bounds__(RED_THREADS) k_mgs(i64 n, int ncomp, CS
             double x = w.c[c][f];
             if (hprev) {
                 x = x - vprev.c[c][f] * h;
-                wout.c[c][f] = x;
+                w.c[c][f] = x;
             }
-            const double y = vnext.c[0] ? vnext.c[c][f] * snext : x;
+            const double y = vnext.c[0] ? vnext.c[c][f] : x;
             const double t = x * y;
             su += (c == ncomp - 1) ? wp2 * t : t;
         }
         s += su;
     }
     red_finish(s, rs);
+}
+
+// v = w / sqrt(nrm2)  (gmres.f90:380-389 with H(i+1,i) = sqrt(nrm2))
+static __global__ void __launch_bounds__(256) k_scale_by_norm(i64 n, int ncomp, SVec<double> v, CSVec<double> w,
+                                                       const double* nrm2) {
+    const double h = sqrt(*nrm2);
+    for (i64 f = blockIdx.x * (i64)blockDim.x + threadIdx.x; f < n; f += (i64)gridDim.x * blockDim.x)
+        for (int c = 0; c < ncomp; c++) v.c[c][f] = w.c[c][f] / h;
 }
 
 // v = w / s (host scalar)
