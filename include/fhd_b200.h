@@ -148,8 +148,11 @@ int  fhd_ctx_set_stream(fhd_ctx* ctx, void* stream);
 /* Preconditioner applications inside GMRES as CUDA graphs: the first
  * application for given operands and prepared coefficients is captured, later
  * ones replay it (mode 1 on, 0 off, -1 default: on unless a multigrid
- * runs more than one V-cycle per application).  fhd_ctx_profile timing
- * works in both modes. */
+ * runs more than one V-cycle per application).  Mode 2 also replays each
+ * GMRES inner iteration (matrix apply, preconditioner, Gram-Schmidt passes,
+ * normalisation, Hessenberg column copy) as one graph per iteration index:
+ * one launch per iteration, worth its capture cost when a context runs many
+ * solves of small problems.  fhd_ctx_profile timing works in every mode. */
 int fhd_ctx_set_graphs(fhd_ctx* ctx, int mode);
 /* The coarse end of both multigrid V-cycles (every level from the first
  * whose unknowns, right-hand sides and residuals fit in one SM's shared

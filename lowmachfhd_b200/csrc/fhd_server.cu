@@ -36,6 +36,9 @@
 
 namespace fhd {
 
+// requests of at least this many steps run with GMRES iteration graphs
+constexpr int SERVE_ITER_GRAPH_STEPS = 16;
+
 int advance_overdamped(fhd_ctx* ctx, const fhd_stoch_params* sp, const fhd_mixture_params* mp, double dt,
                        double* const umac[], double* const rho[], double* pi, const double* eta,
                        const double* const eta_ed[], const double* kappa, const double* temperature,
@@ -183,6 +186,10 @@ static int run_request(const fhd_request& q, cudaStream_t st, fhd_request_result
     int rc = fhd_ctx_create(dim, q.n_cells, dx3, q.visc_type, &q.params, q.precision, &ctx);
     if (rc) return rc;
     fhd_ctx_set_stream(ctx, st);
+    // whole GMRES iterations as graphs once a request is long enough to
+    // amortise their capture (a short request would pay more in capture and
+    // instantiation than its replays save)
+    if (q.steps >= SERVE_ITER_GRAPH_STEPS) fhd_ctx_set_graphs(ctx, 2);
     i64 nc = 1;
     for (int d = 0; d < dim; d++) nc *= q.n_cells[d];
     // state and noise, stream-ordered on the worker's stream

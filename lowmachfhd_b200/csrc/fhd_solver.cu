@@ -1127,7 +1127,7 @@ int sync_scalars(fhd_ctx* ctx, int first, int count) {
 // launch instead of a few hundred.  The values behind the pointers may
 // change between replays (new coefficients, new right-hand sides); the key
 // changes when a pointer or theta does.
-static const size_t GRAPH_CACHE = 8;
+static const size_t GRAPH_CACHE = 32;
 
 static unsigned long long mix_key(unsigned long long h, unsigned long long v) {
     h ^= v + 0x9E3779B97F4A7C15ull + (h << 6) + (h >> 2);
@@ -1162,13 +1162,10 @@ static int replay(fhd_ctx* ctx, fhd_ctx::PreconGraph& gr) {
     return 0;
 }
 
-static int precon_graphed(fhd_ctx* ctx, CSVec<double> b, SVec<double> x) {
-    if (!graphs_on(ctx)) return precon(ctx, b, x);
+// key of the prepared operator: coefficient pointers, theta and whether
+// launches are being timed
+static unsigned long long operator_key(fhd_ctx* ctx) {
     unsigned long long key = 1469598103934665603ull;
-    for (int c = 0; c < 4; c++) {
-        key = mix_key(key, (unsigned long long)(uintptr_t)b.c[c]);
-        key = mix_key(key, (unsigned long long)(uintptr_t)x.c[c]);
-    }
     for (int c = 0; c < 3; c++) {
         key = mix_key(key, (unsigned long long)(uintptr_t)ctx->alpha_fc[c]);
         key = mix_key(key, (unsigned long long)(uintptr_t)ctx->beta_ed[c]);
@@ -1179,15 +1176,24 @@ static int precon_graphed(fhd_ctx* ctx, CSVec<double> b, SVec<double> x) {
     memcpy(&tb, &ctx->theta, sizeof(tb));
     key = mix_key(key, tb);
     key = mix_key(key, ctx->prof ? 1ull : 0ull);
+    return key;
+}
+
+// Run fn() (a fixed sequence of launches and copies on ctx->stream with no
+// host synchronisation) as a CUDA graph: the first call for a key captures
+// it (thread-local: other threads' CUDA calls are unaffected), later calls
+// replay it.  fn runs directly when graphs are off or the capture fails.
+template <class F>
+static int graphed(fhd_ctx* ctx, unsigned long long key, F&& fn) {
+    if (!graphs_on(ctx)) return fn();
     ctx->graph_clock++;
     for (auto& gr : ctx->graphs) {
         if (gr.key != key) continue;
         gr.used = ctx->graph_clock;
         return replay(ctx, gr);
     }
-    // capture this application (thread-local: other threads' CUDA calls are
-    // unaffected), then replay it.  The profiling events it records are made
-    // before the capture so that none is created inside it.
+    // the profiling events are made before the capture so that none is
+    // created inside it
     if (ctx->prof)
         while (ctx->prof_ev.size() < ctx->prof_used + 512) {
             cudaEvent_t ev;
@@ -1200,12 +1206,12 @@ static int precon_graphed(fhd_ctx* ctx, CSVec<double> b, SVec<double> x) {
     const double pb0 = ctx->prof_bytes;
     if (cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
         cudaGetLastError();
-        return precon(ctx, b, x);
+        return fn();
     }
     ctx->capturing = true;
     ctx->cap_fail = false;
     ctx->cap_nodes.clear();
-    int rc = precon(ctx, b, x);
+    int rc = fn();
     ctx->capturing = false;
     cudaGraph_t graph = nullptr;
     cudaError_t e = cudaStreamEndCapture(ctx->stream, &graph);
@@ -1231,7 +1237,7 @@ static int precon_graphed(fhd_ctx* ctx, CSVec<double> b, SVec<double> x) {
         if (graph) cudaGraphDestroy(graph);
         if (rc) return rc;
         ctx->graph_mode = 0;
-        return precon(ctx, b, x);
+        return fn();
     }
     // the template graph stays alive while its event nodes are re-pointed
     if (gr.ev_nodes.empty()) {
@@ -1251,6 +1257,15 @@ static int precon_graphed(fhd_ctx* ctx, CSVec<double> b, SVec<double> x) {
     }
     ctx->graphs.push_back(gr);
     return replay(ctx, ctx->graphs.back());
+}
+
+static int precon_graphed(fhd_ctx* ctx, CSVec<double> b, SVec<double> x) {
+    unsigned long long key = operator_key(ctx);
+    for (int c = 0; c < 4; c++) {
+        key = mix_key(key, (unsigned long long)(uintptr_t)b.c[c]);
+        key = mix_key(key, (unsigned long long)(uintptr_t)x.c[c]);
+    }
+    return graphed(ctx, key, [&]() { return precon(ctx, b, x); });
 }
 
 // ---------------------------------------------------------------------
@@ -1348,29 +1363,43 @@ int gmres_dev(fhd_ctx* ctx, CSVec<double> b, SVec<double> x, double* norm_pre_rh
         for (int i = 1; i <= m; i++) {
             total_iter++;
             i_copy = i;
-            if ((rc = stokes_apply(ctx, csv(V(i - 1)), csv(V(i - 1)), tmp, 0))) return rc;
-            if ((rc = precon_graphed(ctx, csv(tmp), w))) return rc;
-            // modified Gram-Schmidt with device-resident coefficients
-            for (int k = 1; k <= i; k++) {
-                CSVec<double> none;
-                for (int c = 0; c < 4; c++) none.c[c] = nullptr;
-                k_mgs<<<nb, RED_THREADS, 0, st>>>(nc, ncomp, w, k > 1 ? csv(V(k - 2)) : none,
-                                                  k > 1 ? ctx->dscal + S_H + k - 1 : nullptr, csv(V(k - 1)), wp * wp,
-                                                  slot(ctx, S_H + k));
+            // the iteration's launches -- A v_{i-1}, the preconditioner,
+            // modified Gram-Schmidt with device-resident coefficients, the
+            // normalisation -- and the copy of the new Hessenberg column to
+            // the host: in graph mode 2 replayed as one graph per i, else
+            // launched one by one around the preconditioner's graph
+            const bool igraph = ctx->graph_mode == 2;
+            auto body = [&]() -> int {
+                int r2;
+                if ((r2 = stokes_apply(ctx, csv(V(i - 1)), csv(V(i - 1)), tmp, 0))) return r2;
+                if ((r2 = igraph ? precon(ctx, csv(tmp), w) : precon_graphed(ctx, csv(tmp), w))) return r2;
+                for (int k = 1; k <= i; k++) {
+                    CSVec<double> none;
+                    for (int c = 0; c < 4; c++) none.c[c] = nullptr;
+                    k_mgs<<<nb, RED_THREADS, 0, st>>>(nc, ncomp, w, k > 1 ? csv(V(k - 2)) : none,
+                                                      k > 1 ? ctx->dscal + S_H + k - 1 : nullptr, csv(V(k - 1)),
+                                                      wp * wp, slot(ctx, S_H + k));
+                    FHD_POST(ctx);
+                }
+                {
+                    CSVec<double> none;
+                    for (int c = 0; c < 4; c++) none.c[c] = nullptr;
+                    k_mgs<<<nb, RED_THREADS, 0, st>>>(nc, ncomp, w, csv(V(i - 1)), ctx->dscal + S_H + i, none,
+                                                      wp * wp, slot(ctx, S_NRM));
+                    FHD_POST(ctx);
+                }
+                k_scale_by_norm<<<nb, 256, 0, st>>>(nc, ncomp, V(i), csv(w), ctx->dscal + S_NRM);
                 FHD_POST(ctx);
-            }
-            {
-                CSVec<double> none;
-                for (int c = 0; c < 4; c++) none.c[c] = nullptr;
-                k_mgs<<<nb, RED_THREADS, 0, st>>>(nc, ncomp, w, csv(V(i - 1)), ctx->dscal + S_H + i, none, wp * wp,
-                                                  slot(ctx, S_NRM));
-                FHD_POST(ctx);
-            }
-            k_scale_by_norm<<<nb, 256, 0, st>>>(nc, ncomp, V(i), csv(w), ctx->dscal + S_NRM);
-            FHD_POST(ctx);
-            FHD_CUDA_TRY(cudaMemcpyAsync(ctx->hscal + S_H + 1, ctx->dscal + S_H + 1, sizeof(double) * i,
-                                         cudaMemcpyDeviceToHost, st));
-            if ((rc = sync_scalars(ctx, S_NRM, 1))) return rc;
+                FHD_CUDA_TRY(cudaMemcpyAsync(ctx->hscal + S_H + 1, ctx->dscal + S_H + 1, sizeof(double) * i,
+                                             cudaMemcpyDeviceToHost, st));
+                FHD_CUDA_TRY(cudaMemcpyAsync(ctx->hscal + S_NRM, ctx->dscal + S_NRM, sizeof(double),
+                                             cudaMemcpyDeviceToHost, st));
+                return 0;
+            };
+            const unsigned long long ikey =
+                mix_key(mix_key(operator_key(ctx), 0x61726e6f6c6469ull), (unsigned long long)i);
+            if ((rc = igraph ? graphed(ctx, ikey, body) : body())) return rc;
+            FHD_CUDA_TRY(cudaStreamSynchronize(st));
             for (int k = 1; k <= i; k++) Hh(k, i) = ctx->hscal[S_H + k];
             Hh(i + 1, i) = sqrt(ctx->hscal[S_NRM]);
             if (Hh(i + 1, i) == 0.0) {
@@ -1653,7 +1682,7 @@ int fhd_ctx_set_fused(fhd_ctx* c, int mode) {
 }
 
 int fhd_ctx_set_graphs(fhd_ctx* c, int mode) {
-    if (!c || mode < -1 || mode > 1) return FHD_ERR_BAD_ARG;
+    if (!c || mode < -1 || mode > 2) return FHD_ERR_BAD_ARG;
     if (cudaStreamSynchronize(c->stream) != cudaSuccess) return FHD_ERR_CUDA;
     c->graph_mode = mode;
     if (mode == 0) release_graphs(c);

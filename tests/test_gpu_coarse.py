@@ -114,3 +114,29 @@ def test_unaligned_user_arrays(cuda):
         assert np.array_equal(a, b)
     ref = O.stag_mg_solver(pb, O.default_params(), 0.7, rhs)
     assert P.rel_inf(out[1], ref) < 1e-12
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_gmres_graph_modes_bitwise(cuda, precision):
+    """GMRES with no graphs, preconditioner graphs and whole-iteration graphs
+    (modes 0, 1, 2): each solve twice (the second replays the captured
+    graphs); every solution is bitwise the same, with the same iterations."""
+    dim, n, visc = 3, [32, 32, 16], -1
+    pb = P.problem(dim, n, visc, dx=1.0, seed=81)
+    b_u, b_p = P.random_stokes(dim, n, seed=82)
+    out = []
+    for mode in (0, 1, 2):
+        with L.StokesSolver(dim, n, 1.0, visc, params=L.default_params(gmres_rel_tol=1e-8),
+                            precision=precision) as s:
+            s.set_graphs(mode)
+            coef = (dev(pb.alpha_fc, cuda), dev(pb.beta, cuda), dev(pb.beta_ed, cuda), dev(pb.gamma, cuda))
+            bu, bp = dev(b_u, cuda), dev(b_p, cuda)
+            for _ in range(2):
+                x_u, x_p = zeros(pb.nc, dim, cuda), zeros(pb.nc, 1, cuda)[0]
+                status, _, st = s.gmres(bu, bp, x_u, x_p, *coef, 5.0)
+                assert status == 0
+                out.append((host(x_u) + [host(x_p)], st["total_iters"]))
+    for xs, it in out[1:]:
+        assert it == out[0][1]
+        for a, b in zip(xs, out[0][0]):
+            assert np.array_equal(a, b)
