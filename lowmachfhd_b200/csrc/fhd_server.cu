@@ -416,6 +416,18 @@ int fhd_server_create(int slots, unsigned long long hbm_budget_bytes, fhd_server
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return FHD_ERR_NO_DEVICE;
     fhd_server* sv = new fhd_server();
     cudaGetDevice(&sv->s.device);
+    // Requests allocate their state stream-ordered from the device's default
+    // pool.  Its default release threshold (0) hands every freed block back
+    // at the next synchronisation, so each request would map its memory
+    // again; keeping up to the budget in the pool makes admission cheap.
+    // A process-local allocator attribute, not a device setting.
+    {
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, sv->s.device) == cudaSuccess) {
+            unsigned long long thr = hbm_budget_bytes;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+        }
+    }
     sv->s.sched.slots = slots;
     sv->s.sched.budget = hbm_budget_bytes;
     for (int i = 0; i < slots; i++) sv->s.workers.emplace_back(worker_main, &sv->s);
