@@ -428,6 +428,15 @@ def run_reference(args):
     return 0
 
 
+# finest-level smoother kernel by the kind of plan the autotuner picked
+SMOOTHER_KERNEL = {
+    "rowtile": "k_stag_rbx (finest-level row-tile fused red-black smooth of all three components)",
+    "tiled": "k_stag_rb (finest-level tiled fused red-black smooth)",
+    "colour": "k_stag_gs (finest-level colour sweep)",
+    "rules": "finest-level smoother of the fixed size rules",
+}
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -491,10 +500,12 @@ def main():
         barrier(ws)
         prof = case.s.profile_read()
         case.s.profile(False)
+        # the smoother plans the autotuner picked for the finest levels
+        plan = {"stag_level0": case.s.tune_info("stag", 0), "cc_level0": case.s.tune_info("cc", 0)}
         launches = case.s.kernel_launches - launches0
         clk = clocks.stop() if precision == "mixed" else None
         ms_max = allmax(ws, ms, torch, dev)
-        results[precision] = dict(ms=ms_max, iters=iters, prof=prof, launches=launches, clocks=clk,
+        results[precision] = dict(ms=ms_max, iters=iters, prof=prof, launches=launches, clocks=clk, plan=plan,
                                   resid=stats[-1]["norm_resid"] / max(stats[0]["norm_pre_b"], 1e-300))
         if precision == "mixed" and not args.no_e2e:
             # end to end: per step the host->device copy of the step's
@@ -582,7 +593,8 @@ def main():
         "gmres_iters_per_s": ws * sum(sum(x) for x in mixed["iters"]) / (mixed["ms"] / 1e3),
         "corrector_resid_over_pre_rhs": mixed["resid"],
         "gpu_launches": mixed["launches"],
-        "roofline": {"kernel": "k_stag_rbx (finest-level fused red-black smooth of all three components)",
+        "autotuned_plans": {"mixed": mixed["plan"], "fp64": fp64["plan"]},
+        "roofline": {"kernel": SMOOTHER_KERNEL[mixed["plan"]["stag_level0"]["kind"]],
                      "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": (achieved / hbm) if achieved else None,
                      # ncu DRAM read + write of one launch of the same kernel
@@ -592,7 +604,7 @@ def main():
                      "peak_kind": peak_kind, "launches_timed": n_l,
                      "avg_launch_us": (ms_l / n_l * 1e3) if n_l else None,
                      "bytes_per_launch": (bytes_l / n_l) if n_l else None,
-                     "fp64_kernel": "k_stag_gs (FP64 finest-level colour sweep)",
+                     "fp64_kernel": SMOOTHER_KERNEL[fp64["plan"]["stag_level0"]["kind"]],
                      "fp64_achieved": achieved64},
         "clocks": mixed["clocks"],
         "e2e": {"value": ws * K / (results["e2e"]["ms"] / 1e3), "unit": "steps/s",

@@ -168,6 +168,30 @@ int fhd_ctx_set_coarse(fhd_ctx* ctx, int mode);
  * default: on where the level allows, 0: colour launches).  The colour
  * sweeps of stag_mg_solver.f90:360-396, evaluated in the same order. */
 int fhd_ctx_set_fused(fhd_ctx* ctx, int mode);
+/* Smoother autotuner.  Each multigrid level that smooths through launches
+ * (staggered and pressure multigrids, above the single-block coarse end) can
+ * smooth as colour launches with one of four thread-block shapes, as the
+ * tiled fused smooth with one of several tile sizes (3D), or as the row-tile
+ * smooth with one of the tile heights that fit, one CTA per SM with a deep
+ * copy ring or two with a short one (3D FP32 visc_type 1).  With
+ * the tuner on (mode 1 or -1 default), the first solve call that meets a
+ * level shape times every candidate on scratch unknowns with the level's
+ * coefficients and keeps the fastest for the process (per device,
+ * precision, visc_type and shape); later calls and contexts reuse it.
+ * Mode 0: the fixed size rules of fhd_ctx_set_fused.  Mode 2 + k: candidate
+ * k of every level (its first where it has fewer), untimed, for tests.
+ * Every candidate evaluates the update expression of the colour sweeps of
+ * stag_mg_solver.f90:360-396 (pressure: the red-black Gauss-Seidel of the
+ * macproject multigrid) in the same order; the choice changes time only. */
+int fhd_ctx_set_tune(fhd_ctx* ctx, int mode);
+/* Plan of staggered (which 0) or pressure (which 1) multigrid level `level`
+ * after the last solve call: kind -1 fixed rules, 0 colour launches, 1 tiled
+ * fused, 2 row-tile; ncand candidates considered; pair_us the measured time
+ * of one smooth pair (0 when not timed); shape = {block x, block y, 0, 1}
+ * for colour launches, {tile x, tile y, z-runs, CTAs per SM} for fused
+ * smooths.  Any output pointer may be NULL.  No reference counterpart. */
+int fhd_ctx_tune_info(fhd_ctx* ctx, int which, int level, int* kind, int* ncand, double* pair_us,
+                      int shape[4]);
 /* Number of this library's kernels launched through ctx so far. */
 long long fhd_ctx_kernel_launches(fhd_ctx* ctx);
 const char* fhd_status_string(int status);

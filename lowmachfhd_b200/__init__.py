@@ -120,6 +120,23 @@ class StokesSolver:
         launch each: 1 or -1 (default) on, 0 one launch per colour"""
         check(lib().fhd_ctx_set_fused(self._h, int(mode)), "fhd_ctx_set_fused")
 
+    def set_tune(self, mode: int):
+        """smoother autotuner: 1 or -1 (default) time the candidate plans of
+        each level shape once per process and keep the fastest, 0 the fixed
+        size rules, 2 + k force candidate k of every level (tests)"""
+        check(lib().fhd_ctx_set_tune(self._h, int(mode)), "fhd_ctx_set_tune")
+
+    def tune_info(self, which: str = "stag", level: int = 0) -> dict:
+        """plan of one level after the last solve call: kind (-1 fixed rules,
+        0 colour launches, 1 tiled fused, 2 row-tile), candidates considered,
+        measured time of a smooth pair, block or tile shape"""
+        kind, nc, us = C.c_int(0), C.c_int(0), C.c_double(0)
+        shape = (C.c_int * 4)()
+        check(lib().fhd_ctx_tune_info(self._h, 0 if which == "stag" else 1, int(level), C.byref(kind),
+                                      C.byref(nc), C.byref(us), shape), "fhd_ctx_tune_info")
+        names = {-1: "rules", 0: "colour", 1: "tiled", 2: "rowtile"}
+        return {"kind": names[kind.value], "candidates": nc.value, "pair_us": us.value, "shape": list(shape)}
+
     def profile(self, enable: bool = True):
         """time the finest-level smoother launches with CUDA events"""
         check(lib().fhd_ctx_profile(self._h, int(enable)), "fhd_ctx_profile")

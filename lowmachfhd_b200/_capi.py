@@ -143,6 +143,9 @@ _PROTOS = {
     "fhd_ctx_set_graphs": (C.c_int, [_VP, C.c_int]),
     "fhd_ctx_set_coarse": (C.c_int, [_VP, C.c_int]),
     "fhd_ctx_set_fused": (C.c_int, [_VP, C.c_int]),
+    "fhd_ctx_set_tune": (C.c_int, [_VP, C.c_int]),
+    "fhd_ctx_tune_info": (C.c_int, [_VP, C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                    C.POINTER(C.c_double), C.POINTER(C.c_int)]),
     "fhd_ctx_device_bytes": (C.c_ulonglong, [_VP]),
     "fhd_ctx_profile": (C.c_int, [_VP, C.c_int]),
     "fhd_ctx_profile_read": (C.c_int, [_VP, C.POINTER(C.c_longlong), C.POINTER(C.c_double),

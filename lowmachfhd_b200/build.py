@@ -5,6 +5,7 @@ from __future__ import annotations
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 SRC = os.path.join(HERE, "csrc")
@@ -33,10 +34,24 @@ def build(verbose: bool = False, extra: list[str] | None = None) -> str:
                  + [os.path.join(HERE, "..", "include", "fhd_b200.h")])
     if os.path.exists(OUT) and os.path.getmtime(OUT) >= newest and not extra:
         return OUT
-    cmd = [nvcc()] + NVCC_FLAGS + (extra or []) + ["-o", OUT + ".tmp"] + srcs + ["-lcudart"]
+    # one nvcc per translation unit, in parallel, then one link
+    objdir = os.path.join(HERE, "_build")
+    os.makedirs(objdir, exist_ok=True)
+    cflags = [f for f in NVCC_FLAGS if f != "-shared"] + (extra or [])
+    objs = [os.path.join(objdir, os.path.splitext(os.path.basename(p))[0] + ".o") for p in srcs]
+    cmds = [[nvcc()] + cflags + ["-c", src, "-o", obj] for src, obj in zip(srcs, objs)]
     if verbose:
-        print(" ".join(cmd), flush=True)
-    subprocess.run(cmd, check=True)
+        for c in cmds:
+            print(" ".join(c), flush=True)
+    with ThreadPoolExecutor(max_workers=min(len(cmds), os.cpu_count() or 1)) as ex:
+        for r in list(ex.map(lambda c: subprocess.run(c), cmds)):
+            if r.returncode:
+                raise subprocess.CalledProcessError(r.returncode, r.args)
+    link = [nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-Xcompiler", "-fPIC",
+            "-o", OUT + ".tmp"] + objs + ["-lcudart"]
+    if verbose:
+        print(" ".join(link), flush=True)
+    subprocess.run(link, check=True)
     os.replace(OUT + ".tmp", OUT)
     return OUT
 

@@ -42,6 +42,18 @@ constexpr int RB_NCF = 3 + RB_AHEAD;        // coefficient planes k .. k+2+AHEAD
 constexpr int RB_MAXTX = 64;
 constexpr int RB_CHUNKS = 3;                // 16-byte copies per thread per plane
 
+// geometry of the row-tile smoother (fhd_rbx.cuh: rbx_geom)
+struct RBXGeom {
+    int TY;       // tile rows (divides ny)
+    int KZ;       // planes of the longest z-run
+    int tiles_y, chunks;
+    int rows;     // TY + 4 staged unknown rows
+    int crows;    // TY + 2 staged coefficient rows
+    size_t smem;  // bytes of dynamic shared memory
+    int ahead;    // stages in flight beyond the one awaited
+    int per_sm;   // resident CTAs per SM the z-run split assumes
+};
+
 struct RBGeom {
     int TX, TY;        // tile interior (TX a multiple of XR, TY even)
     int KZ;            // planes per CTA (divides nz)
@@ -60,7 +72,9 @@ inline int largest_divisor_le(int n, int cap, int mult) {
 
 // tile geometry for a level; false when the level cannot use the fused
 // smoother (2D, an odd extent, or nx not a multiple of 16 bytes)
-inline bool rb_geom(const Grid& g, int ncomp, int elem_bytes, RBGeom& G) {
+// tx, ty > 0 ask for that tile (the autotuner's candidates); 0 takes the
+// widest and tallest tile that divides the level
+inline bool rb_geom(const Grid& g, int ncomp, int elem_bytes, RBGeom& G, int tx = 0, int ty = 0) {
     if (g.dim != 3) return false;
     for (int d = 0; d < 3; d++)
         if (g.n[d] < 2 || (g.n[d] & 1)) return false;
@@ -69,6 +83,8 @@ inline bool rb_geom(const Grid& g, int ncomp, int elem_bytes, RBGeom& G) {
     const int mx = G.XR < 2 ? 2 : G.XR;
     G.TX = largest_divisor_le(g.n[0], RB_MAXTX, mx);
     G.TY = largest_divisor_le(g.n[1], RB_MAXTY, 2);
+    if (tx > 0) G.TX = (tx <= RB_MAXTX && tx % mx == 0 && g.n[0] % tx == 0) ? tx : 0;
+    if (ty > 0) G.TY = (ty <= RB_MAXTY && ty % 2 == 0 && g.n[1] % ty == 0) ? ty : 0;
     if (!G.TX || !G.TY) return false;
     G.tiles_x = g.n[0] / G.TX;
     G.tiles_y = g.n[1] / G.TY;

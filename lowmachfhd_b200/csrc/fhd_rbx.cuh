@@ -30,9 +30,9 @@
 namespace fhd {
 
 constexpr int RBX_THREADS = 256;  // compute threads
-constexpr int RBX_AHEAD = 3;            // stages in flight beyond the one awaited
-constexpr int RBX_NPH = 5 + RBX_AHEAD;  // unknown planes k-1 .. k+3 + in flight
-constexpr int RBX_NCF = 3 + RBX_AHEAD;  // coefficient planes k .. k+2 + in flight
+// stages in flight beyond the one awaited (the rings then hold unknown
+// planes k-1 .. k+3 and coefficient planes k .. k+2 plus these)
+constexpr int RBX_AHEAD = 3;
 constexpr int RBX_MAXNX = 256;
 constexpr long RBX_SPIN = 1L << 22;     // try_wait polls before a wait gives up
 // a thread updates the cells of one x column on rows gr, gr + RG, ..: with
@@ -52,19 +52,12 @@ inline int rbx_pad(int nx, int rows) {
     const int over = RBX_MAXR * RBX_ROWSTEP + 2 * nx - rows * nx;
     return (over > 0 ? over : 0) + 32;
 }
-inline size_t rbx_smem_bytes(int nx, int ty) {
-    return 64 + sizeof(float) * ((size_t)RBX_NCF * 2 * (ty + 2) * nx + (size_t)RBX_NPH * (ty + 4) * nx +
+// ahead: stages in flight beyond the one awaited (RBX_AHEAD, or 1 for the
+// variant that fits two CTAs on an SM)
+inline size_t rbx_smem_bytes(int nx, int ty, int ahead = RBX_AHEAD) {
+    return 64 + sizeof(float) * ((size_t)(3 + ahead) * 2 * (ty + 2) * nx + (size_t)(5 + ahead) * (ty + 4) * nx +
                                  rbx_pad(nx, ty + 4));
 }
-
-struct RBXGeom {
-    int TY;       // tile rows (divides ny)
-    int KZ;       // planes of the longest z-run
-    int tiles_y, chunks;
-    int rows;     // TY + 4 staged unknown rows
-    int crows;    // TY + 2 staged coefficient rows
-    size_t smem;  // bytes of dynamic shared memory
-};
 
 // ---------------------------------------------------------------------
 // mbarrier and bulk-copy primitives (sm_90+ PTX, no cluster multicast)
@@ -127,9 +120,11 @@ struct RBXArgs {
     unsigned* err;
 };
 
-template <int C>
+template <int C, int AH>
 __device__ __forceinline__ void rbx_run(const Grid& g, const RBXGeom& G, const StagOp<float>& A, const RBXArgs& R,
                                         float omega, unsigned char* raw, int tile_y, int chunk) {
+    constexpr int NPH = 5 + AH;  // unknown planes k-1 .. k+3 + in flight
+    constexpr int NCF = 3 + AH;  // coefficient planes k .. k+2 + in flight
     const int nx = g.n[0], ny = g.n[1], nz = g.n[2];
     const int TY = G.TY, rows = G.rows, crows = G.crows;
     const int tid = threadIdx.x;
@@ -139,7 +134,7 @@ __device__ __forceinline__ void rbx_run(const Grid& g, const RBXGeom& G, const S
     unsigned long long* bar = reinterpret_cast<unsigned long long*>(raw);
     const int plane = rows * nx, cplane = crows * nx;
     float* cf = reinterpret_cast<float*>(raw + 64);  // [slot][0 alpha, 1 rhs][crows][nx]
-    float* ph = cf + RBX_NCF * 2 * cplane;          // [slot][rows][nx]
+    float* ph = cf + NCF * 2 * cplane;          // [slot][rows][nx]
     const float* src = R.src[C];
     float* dst = R.dst[C];
     const float* alpha = R.alpha[C];
@@ -155,7 +150,7 @@ __device__ __forceinline__ void rbx_run(const Grid& g, const RBXGeom& G, const S
     auto issue = [&](int q) {
         const int lane = tid - RBX_THREADS;
         const int j = q + k0 - 2;
-        const int s = q % RBX_NPH;
+        const int s = q % NPH;
         if (lane == 0) mbar_expect_tx(&bar[s], (unsigned)(sizeof(float) * (plane + (j >= k0 ? 2 * cplane : 0))));
         __syncwarp();
         auto copy = [&](float* sdst, const float* gplane, int nrows, int ring) {
@@ -169,13 +164,13 @@ __device__ __forceinline__ void rbx_run(const Grid& g, const RBXGeom& G, const S
         };
         if (lane == 0) copy(ph + s * plane, src + (i64)wrapc(j, nz) * nxy, rows, 2);
         if (j >= k0 && (lane == 1 || lane == 2)) {
-            const int cs = pmod(j - 1, RBX_NCF);
+            const int cs = pmod(j - 1, NCF);
             const i64 zo = (i64)wrapc(j - 1, nz) * nxy;
             copy(cf + (cs * 2 + lane - 1) * cplane, (lane == 1 ? alpha : rhs) + zo, crows, 1);
         }
     };
     // wait for stage q; false on time-out
-    auto wait_stage = [&](int q) { return mbar_wait_bounded(&bar[q % RBX_NPH], (unsigned)((q / RBX_NPH) & 1)); };
+    auto wait_stage = [&](int q) { return mbar_wait_bounded(&bar[q % NPH], (unsigned)((q / NPH) & 1)); };
 
     const int hx = nx >> 1;           // cells of one colour per row
     const int RG = RBX_THREADS / hx;  // rows updated at once
@@ -242,12 +237,12 @@ __device__ __forceinline__ void rbx_run(const Grid& g, const RBXGeom& G, const S
     const bool producer = tid >= RBX_THREADS;
     const int lead = RBX_THREADS;  // producer lane 0: stores and clean-up
     if (producer) {
-        for (int q = 0; q < 5 + RBX_AHEAD && q <= qend; q++) issue(q);
-        issued = 5 + RBX_AHEAD < qend + 1 ? 5 + RBX_AHEAD : qend + 1;
+        for (int q = 0; q < 5 + AH && q <= qend; q++) issue(q);
+        issued = 5 + AH < qend + 1 ? 5 + AH : qend + 1;
     }
     using RRed = std::integral_constant<int, RBX_MAXR>;
     using RBlack = std::integral_constant<int, RBX_MAXR - 1>;
-    auto slot = [&](int p) { return pmod(p - (k0 - 2), RBX_NPH); };
+    auto slot = [&](int p) { return pmod(p - (k0 - 2), NPH); };
     auto ring = [](int v, int d, int n) { return v + d >= n ? v + d - n : v + d; };
     int sl, scl;
     bool ok = true;
@@ -256,11 +251,11 @@ __device__ __forceinline__ void rbx_run(const Grid& g, const RBXGeom& G, const S
     if (__syncthreads_or(!ok)) goto fail;
     // red of k0-1 .. k0+1 read only black cells, which none of them writes
     if (!producer)
-        for (int p = k0 - 1; p <= k0 + 1; p++) sweep(RRed(), slot(p - 1), slot(p), slot(p + 1), pmod(p, RBX_NCF), p, 0, -1, TY + 1);
+        for (int p = k0 - 1; p <= k0 + 1; p++) sweep(RRed(), slot(p - 1), slot(p), slot(p + 1), pmod(p, NCF), p, 0, -1, TY + 1);
     // ring slots of unknown plane k-1 and coefficient plane k, advanced by one
     // per step
     sl = slot(k0 - 1);
-    scl = pmod(k0, RBX_NCF);
+    scl = pmod(k0, NCF);
     for (int k = k0; k < kend; k++) {
         // this thread's shared-memory writes of the previous step become
         // visible to the bulk store issued below
@@ -272,13 +267,13 @@ __device__ __forceinline__ void rbx_run(const Grid& g, const RBXGeom& G, const S
             if (tid == lead) bulk_wait_read0();
             __syncwarp();
             fence_proxy_async();
-            const int qn = k + 3 + RBX_AHEAD - (k0 - 2);
+            const int qn = k + 3 + AH - (k0 - 2);
             if (qn <= qend) {
                 issue(qn);
                 issued = qn + 1;
             }
             if (tid == lead && k > k0) {
-                const float* sp = ph + pmod(k - 1 - (k0 - 2), RBX_NPH) * plane + 2 * nx;
+                const float* sp = ph + pmod(k - 1 - (k0 - 2), NPH) * plane + 2 * nx;
                 bulk_s2g(dst + (i64)(k - 1) * nxy + (i64)y0 * nx, sp, (unsigned)(sizeof(float) * TY * nx));
                 bulk_commit();
             }
@@ -287,17 +282,17 @@ __device__ __forceinline__ void rbx_run(const Grid& g, const RBXGeom& G, const S
         // stage k+3: unknown plane k+3, coefficient plane k+2
         if (k + 3 - (k0 - 2) <= qend) ok = wait_stage(k + 3 - (k0 - 2));
         if (!ok) continue;  // leaves at the next barrier
-        const int s1 = ring(sl, 1, RBX_NPH), s2 = ring(sl, 2, RBX_NPH);
+        const int s1 = ring(sl, 1, NPH), s2 = ring(sl, 2, NPH);
         sweep(RBlack(), sl, s1, s2, scl, k, 1, 0, TY);
         if (k + 2 <= kend)
-            sweep(RRed(), s2, ring(sl, 3, RBX_NPH), ring(sl, 4, RBX_NPH), ring(scl, 2, RBX_NCF), k + 2, 0, -1, TY + 1);
+            sweep(RRed(), s2, ring(sl, 3, NPH), ring(sl, 4, NPH), ring(scl, 2, NCF), k + 2, 0, -1, TY + 1);
         sl = s1;
-        scl = ring(scl, 1, RBX_NCF);
+        scl = ring(scl, 1, NCF);
     }
     fence_proxy_async();
     if (__syncthreads_or(!ok)) goto fail;
     if (tid == lead) {
-        const float* sp = ph + pmod(kend - 1 - (k0 - 2), RBX_NPH) * plane + 2 * nx;
+        const float* sp = ph + pmod(kend - 1 - (k0 - 2), NPH) * plane + 2 * nx;
         bulk_s2g(dst + (i64)(kend - 1) * nxy + (i64)y0 * nx, sp, (unsigned)(sizeof(float) * TY * nx));
         bulk_commit();
         bulk_wait0();
@@ -309,27 +304,36 @@ fail:
     if (tid == lead) {
         atomicOr(R.err, 1u);
         bulk_wait0();
-        // stages before the last RBX_NPH issued completed before their
+        // stages before the last NPH issued completed before their
         // barriers were re-armed
-        for (int q = issued > RBX_NPH ? issued - RBX_NPH : 0; q < issued; q++) wait_stage(q);
+        for (int q = issued > NPH ? issued - NPH : 0; q < issued; q++) wait_stage(q);
     }
 }
 
-__global__ void __launch_bounds__(RBX_BLOCK, 1) k_stag_rbx(Grid g, RBXGeom G, StagOp<float> A, RBXArgs R,
-                                                            float omega) {
+// AH stages in flight beyond the one awaited: RBX_AHEAD with one CTA per SM,
+// or 1 with two (smaller rings, half the shared memory)
+template <int AH>
+__global__ void __launch_bounds__(RBX_BLOCK, AH == 1 ? 2 : 1) k_stag_rbx(Grid g, RBXGeom G, StagOp<float> A,
+                                                                         RBXArgs R, float omega) {
     extern __shared__ __align__(128) unsigned char rbx_raw[];
-    if (threadIdx.x < RBX_NPH) mbar_init(reinterpret_cast<unsigned long long*>(rbx_raw) + threadIdx.x, 1);
+    if (threadIdx.x < 5 + AH) mbar_init(reinterpret_cast<unsigned long long*>(rbx_raw) + threadIdx.x, 1);
     if (threadIdx.x == 0) mbar_init_fence();
     __syncthreads();
     const int tile_y = blockIdx.x, chunk = blockIdx.y;
-    if (blockIdx.z == 0) rbx_run<0>(g, G, A, R, omega, rbx_raw, tile_y, chunk);
-    else if (blockIdx.z == 1) rbx_run<1>(g, G, A, R, omega, rbx_raw, tile_y, chunk);
-    else rbx_run<2>(g, G, A, R, omega, rbx_raw, tile_y, chunk);
+    if (blockIdx.z == 0) rbx_run<0, AH>(g, G, A, R, omega, rbx_raw, tile_y, chunk);
+    else if (blockIdx.z == 1) rbx_run<1, AH>(g, G, A, R, omega, rbx_raw, tile_y, chunk);
+    else rbx_run<2, AH>(g, G, A, R, omega, rbx_raw, tile_y, chunk);
 }
 
 // geometry for a level (sms: multiprocessors of the device); false when the
-// level cannot use this smoother
-inline bool rbx_geom(const Grid& g, int sms, size_t smem_max, RBXGeom& G) {
+// level cannot use this smoother.  ty > 0 asks for that tile height (the
+// autotuner's candidates), 0 for the tallest that fits.
+// ahead: RBX_AHEAD, or 1 for two CTAs per SM where smem_sm (shared memory
+// of one SM) holds two.
+inline bool rbx_geom(const Grid& g, int sms, size_t smem_max, RBXGeom& G, int ty_req = 0, int ahead = RBX_AHEAD,
+                     size_t smem_sm = 0) {
+    if (ahead != RBX_AHEAD && ahead != 1) return false;
+    G.ahead = ahead;
     if (g.dim != 3) return false;
     const int nx = g.n[0], ny = g.n[1], nz = g.n[2];
     if (nx > RBX_MAXNX || nx < 64 || (nx & (nx - 1)) || (ny & 1) || (nz & 1) || nz < 4) return false;
@@ -338,8 +342,8 @@ inline bool rbx_geom(const Grid& g, int sms, size_t smem_max, RBXGeom& G) {
     // tallest tile that fits the shared memory of one CTA per SM
     G.TY = 0;
     for (int ty = 32; ty >= 4; ty /= 2) {
-        if (ny % ty) continue;
-        const size_t smem = rbx_smem_bytes(nx, ty);
+        if (ny % ty || (ty_req > 0 && ty != ty_req)) continue;
+        const size_t smem = rbx_smem_bytes(nx, ty, ahead);
         if (smem <= smem_max) {
             G.TY = ty;
             G.smem = smem;
@@ -349,9 +353,12 @@ inline bool rbx_geom(const Grid& g, int sms, size_t smem_max, RBXGeom& G) {
     if (!G.TY) return false;
     // rows per thread and sweep (ring rows included) within RBX_MAXR
     const int RG = RBX_THREADS / hx;
-    while (G.TY > 4 && (G.TY + 2 + RG - 1) / RG > RBX_MAXR) G.TY /= 2;
+    while (ty_req == 0 && G.TY > 4 && (G.TY + 2 + RG - 1) / RG > RBX_MAXR) G.TY /= 2;
     if ((G.TY + 2 + RG - 1) / RG > RBX_MAXR || (G.TY + RG - 1) / RG > RBX_MAXR - 1 || ny % G.TY) return false;
-    G.smem = rbx_smem_bytes(nx, G.TY);
+    G.smem = rbx_smem_bytes(nx, G.TY, ahead);
+    // resident CTAs per SM (1 KB of each CTA's shared memory is reserved)
+    G.per_sm = (ahead == 1 && 2 * (G.smem + 1024) <= smem_sm) ? 2 : 1;
+    if (ahead == 1 && G.per_sm == 1) return false;  // the short ring pays only with two CTAs
     G.rows = G.TY + 4;
     G.crows = G.TY + 2;
     G.tiles_y = ny / G.TY;
@@ -362,7 +369,8 @@ inline bool rbx_geom(const Grid& g, int sms, size_t smem_max, RBXGeom& G) {
     G.chunks = 0;
     for (int c = 1; c <= nz / 4; c++) {
         const long items = (long)G.tiles_y * 3 * c;
-        const long rounds = (items + sms - 1) / sms;
+        const long slots = (long)sms * G.per_sm;
+        const long rounds = (items + slots - 1) / slots;
         const long cost = rounds * ((nz + c - 1) / c + 5);
         if (best < 0 || cost < best) {
             best = cost;

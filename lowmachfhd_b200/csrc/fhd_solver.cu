@@ -251,6 +251,9 @@ static int prepare_T(fhd_ctx* ctx) {
     return 0;
 }
 
+template <typename T>
+static int tune_levels(fhd_ctx* ctx);
+
 int prepare(fhd_ctx* ctx, const double* const alpha_fc[], const double* beta, const double* const beta_ed[],
             const double* gamma, double theta) {
     const int dim = ctx->dim;
@@ -259,8 +262,12 @@ int prepare(fhd_ctx* ctx, const double* const alpha_fc[], const double* beta, co
     ctx->gamma = gamma;
     for (int e = 0; e < 3; e++) ctx->beta_ed[e] = e < (dim == 2 ? 1 : 3) ? beta_ed[e] : nullptr;
     ctx->theta = theta;
-    if (ctx->prec == FHD_PREC_MIXED) return prepare_T<float>(ctx);
-    return prepare_T<double>(ctx);
+    if (ctx->prec == FHD_PREC_MIXED) {
+        int rc = prepare_T<float>(ctx);
+        return rc ? rc : tune_levels<float>(ctx);
+    }
+    int rc = prepare_T<double>(ctx);
+    return rc ? rc : tune_levels<double>(ctx);
 }
 
 // ---------------------------------------------------------------------
@@ -310,9 +317,15 @@ static void prof_mark(fhd_ctx* ctx, cudaStream_t st) {
         ctx->cap_fail = true;
 }
 
+// colour launches over the cells of one colour with thread block blk
+inline dim3 half_grid_for(const Grid& g, dim3 blk) {
+    return dim3(((g.n[0] + 1) / 2 + blk.x - 1) / blk.x, (g.n[1] + blk.y - 1) / blk.y, g.n[2]);
+}
+
 template <typename T>
-static int stag_smooth(fhd_ctx* ctx, StagLevel<T>& L, int color) {
+static int stag_smooth(fhd_ctx* ctx, StagLevel<T>& L, int color, dim3 blk = cell_block()) {
     cudaStream_t st = ctx->stream;
+    const dim3 hg = half_grid_for(L.g, blk);
     const T omega = (T)ctx->p.stag_mg_omega;
     const StagOp<T> A = L.op();
     int rc = 0;
@@ -328,13 +341,13 @@ static int stag_smooth(fhd_ctx* ctx, StagLevel<T>& L, int color) {
         with_dim_visc(ctx->dim, ctx->visc, [&](auto D, auto V) {
             constexpr int DIM = decltype(D)::value, VISC = decltype(V)::value;
             if (c == 0)
-                k_stag_gs<T, DIM, VISC, 0><<<half_grid(L.g), cell_block(), 0, st>>>(L.g, A, L.phi[0], L.phi[1],
-                                                                                   L.phi[2], L.rhs[0], par, omega);
+                k_stag_gs<T, DIM, VISC, 0><<<hg, blk, 0, st>>>(L.g, A, L.phi[0], L.phi[1], L.phi[2], L.rhs[0], par,
+                                                               omega);
             else if (c == 1)
-                k_stag_gs<T, DIM, VISC, 1><<<half_grid(L.g), cell_block(), 0, st>>>(L.g, A, L.phi[0], L.phi[1],
-                                                                                   L.phi[2], L.rhs[1], par, omega);
+                k_stag_gs<T, DIM, VISC, 1><<<hg, blk, 0, st>>>(L.g, A, L.phi[0], L.phi[1], L.phi[2], L.rhs[1], par,
+                                                               omega);
             else
-                k_stag_gs<T, DIM, VISC, (DIM == 3 ? 2 : 1)><<<half_grid(L.g), cell_block(), 0, st>>>(
+                k_stag_gs<T, DIM, VISC, (DIM == 3 ? 2 : 1)><<<hg, blk, 0, st>>>(
                     L.g, A, L.phi[0], L.phi[1], L.phi[2], L.rhs[DIM == 3 ? 2 : 1], par, omega);
             rc |= post(ctx);
         });
@@ -372,8 +385,10 @@ static double rb_smooth_bytes(fhd_ctx* ctx, const StagLevel<T>& L) {
 
 // dynamic shared memory above the 48 KB default: raise each kernel's limit
 // (keyed by device and kernel address) to the largest size launched so far
+// (full_carveout: also ask for the whole unified L1 / shared-memory array as
+// shared memory, so that two large CTAs fit on one SM)
 template <class K>
-static int rb_allow_smem(K kernel, size_t bytes) {
+static int rb_allow_smem(K kernel, size_t bytes, bool full_carveout = false) {
     static std::mutex mu;
     static std::map<std::pair<int, const void*>, size_t> done;
     if (bytes <= 48 * 1024) return 0;
@@ -383,6 +398,9 @@ static int rb_allow_smem(K kernel, size_t bytes) {
     size_t& d = done[std::make_pair(dev, (const void*)kernel)];
     if (bytes <= d) return 0;
     FHD_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    if (full_carveout)
+        FHD_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                          (int)cudaSharedmemCarveoutMaxShared));
     d = bytes;
     return 0;
 }
@@ -458,12 +476,57 @@ static int stag_rbx_smooth(fhd_ctx* ctx, StagLevel<float>& L, const RBXGeom& G, 
         ctx->prof_bytes += rb_smooth_bytes(ctx, L);
         ctx->prof_launches++;
     }
-    if (int rc = rb_allow_smem(k_stag_rbx, G.smem)) return rc;
-    k_stag_rbx<<<dim3(G.tiles_y, G.chunks, 3), RBX_BLOCK, G.smem, ctx->stream>>>(L.g, G, L.op(), R,
-                                                                                 (float)ctx->p.stag_mg_omega);
+    const dim3 grd(G.tiles_y, G.chunks, 3);
+    if (G.ahead == 1) {
+        if (int rc = rb_allow_smem(k_stag_rbx<1>, G.smem, true)) return rc;
+        k_stag_rbx<1><<<grd, RBX_BLOCK, G.smem, ctx->stream>>>(L.g, G, L.op(), R, (float)ctx->p.stag_mg_omega);
+    } else {
+        if (int rc = rb_allow_smem(k_stag_rbx<RBX_AHEAD>, G.smem)) return rc;
+        k_stag_rbx<RBX_AHEAD><<<grd, RBX_BLOCK, G.smem, ctx->stream>>>(L.g, G, L.op(), R,
+                                                                      (float)ctx->p.stag_mg_omega);
+    }
     int rc = post(ctx);
     if (timed) prof_mark(ctx, ctx->stream);
     return rc;
+}
+
+template <typename T>
+static bool stag_aligned(const StagLevel<T>& L, int dim) {
+    bool aligned = true;
+    for (int c = 0; c < dim; c++)
+        aligned = aligned && rb_aligned(L.phi[c]) && rb_aligned(L.tmp[c]) && rb_aligned(L.rhs[c]) &&
+                  rb_aligned(L.alpha[c]);
+    return aligned;
+}
+
+// count smooths of a level as its tuned plan says: pairs of fused smooths
+// phi -> tmp -> phi (kinds 1, 2), colour launches for the rest
+template <typename T>
+static int stag_smooths_planned(fhd_ctx* ctx, StagLevel<T>& L, const SmoothPlan& P, int count) {
+    int m0 = 0;
+    T* a[3] = {L.phi[0], L.phi[1], L.phi[2]};
+    T* b[3] = {L.tmp[0], L.tmp[1], L.tmp[2]};
+    if constexpr (std::is_same<T, float>::value) {
+        if (P.kind == 2)
+            for (; m0 + 2 <= count; m0 += 2) {
+                int rc = stag_rbx_smooth(ctx, L, P.rbx, a, b);
+                if (!rc) rc = stag_rbx_smooth(ctx, L, P.rbx, b, a);
+                if (rc) return rc;
+            }
+    }
+    if (P.kind == 1)
+        for (; m0 + 2 <= count; m0 += 2) {
+            int rc = stag_rb_smooth(ctx, L, P.rb, a, b);
+            if (!rc) rc = stag_rb_smooth(ctx, L, P.rb, b, a);
+            if (rc) return rc;
+        }
+    const dim3 blk(P.kind == 0 ? P.bx : 32, P.kind == 0 ? P.by : 8, 1);
+    for (int m = m0; m < count; m++)
+        for (int color = 1; color <= 2 * ctx->dim; color++) {
+            int rc = stag_smooth(ctx, L, color, blk);
+            if (rc) return rc;
+        }
+    return 0;
 }
 
 template <typename T>
@@ -471,10 +534,9 @@ static int stag_smooths(fhd_ctx* ctx, StagLevel<T>& L, int count) {
     const int dim = ctx->dim;
     int m0 = 0;
     RBGeom G;
-    bool aligned = true;
-    for (int c = 0; c < dim; c++)
-        aligned = aligned && rb_aligned(L.phi[c]) && rb_aligned(L.tmp[c]) && rb_aligned(L.rhs[c]) &&
-                  rb_aligned(L.alpha[c]);
+    const bool aligned = stag_aligned(L, dim);
+    if (L.plan.kind >= 0 && ctx->fused_mode != 0 && ctx->p.stag_mg_smoother != 0 && aligned && all_even(L.g))
+        return stag_smooths_planned(ctx, L, L.plan, count);
     if constexpr (std::is_same<T, float>::value) {
         RBXGeom X;
         if (ctx->p.stag_mg_smoother != 0 && ctx->visc == 1 && count >= 2 && aligned && !rb_use(L.g) &&
@@ -738,15 +800,16 @@ static int stag_mg_run(fhd_ctx* ctx, Multigrid<T>& M) {
 // pressure multigrid (macproject.f90:34-316)
 // ---------------------------------------------------------------------
 template <typename T>
-static int cc_smooth(fhd_ctx* ctx, CCLevel<T>& C) {
+static int cc_smooth(fhd_ctx* ctx, CCLevel<T>& C, dim3 blk = cell_block()) {
     cudaStream_t st = ctx->stream;
     const CCOp<T> A = C.op();
+    const dim3 hg = half_grid_for(C.g, blk);
     int rc = 0;
     for (int par = 0; par < 2; par++) {
         with_dim(ctx->dim, [&](auto D) {
             constexpr int DIM = decltype(D)::value;
             if (all_even(C.g)) {
-                k_cc_gsrb<T, DIM><<<half_grid(C.g), cell_block(), 0, st>>>(C.g, A, C.phi, C.rhs, par);
+                k_cc_gsrb<T, DIM><<<hg, blk, 0, st>>>(C.g, A, C.phi, C.rhs, par);
                 rc |= post(ctx);
             } else {
                 k_cc_color_corr<T, DIM><<<cell_grid(C.g), cell_block(), 0, st>>>(C.g, A, C.phi, C.rhs, C.tmp, par);
@@ -762,11 +825,37 @@ static int cc_smooth(fhd_ctx* ctx, CCLevel<T>& C) {
 
 // count red-black smooths: fused pairs phi -> tmp -> phi where the level
 // allows, single colour-pair smooths otherwise
+// pairs of tiled fused smooths phi -> tmp -> phi with geometry G
+template <typename T>
+static int cc_rb_pairs(fhd_ctx* ctx, CCLevel<T>& C, const RBGeom& G, int pairs) {
+    const size_t smem = rb_smem<T>(G, 1);
+    if (int rc = rb_allow_smem(k_cc_rb<T>, smem)) return rc;
+    const dim3 grd(G.tiles_x * G.tiles_y, G.chunks, 1), blk(32, G.TY + 1);
+    for (int m = 0; m < pairs; m++) {
+        k_cc_rb<T><<<grd, blk, smem, ctx->stream>>>(C.g, G, C.op(), C.phi, C.tmp, C.rhs);
+        FHD_POST(ctx);
+        k_cc_rb<T><<<grd, blk, smem, ctx->stream>>>(C.g, G, C.op(), C.tmp, C.phi, C.rhs);
+        FHD_POST(ctx);
+    }
+    return 0;
+}
+
 template <typename T>
 static int cc_smooths(fhd_ctx* ctx, CCLevel<T>& C, int count) {
     int m0 = 0;
     RBGeom G;
     const bool aligned = rb_aligned(C.phi) && rb_aligned(C.tmp) && rb_aligned(C.rhs);
+    if (C.plan.kind >= 0 && aligned && all_even(C.g)) {
+        const SmoothPlan& P = C.plan;
+        if (P.kind == 1) {
+            if (int rc = cc_rb_pairs(ctx, C, P.rb, count / 2)) return rc;
+            m0 = count / 2 * 2;
+        }
+        const dim3 blk(P.kind == 0 ? P.bx : 32, P.kind == 0 ? P.by : 8, 1);
+        for (int m = m0; m < count; m++)
+            if (int rc = cc_smooth(ctx, C, blk)) return rc;
+        return 0;
+    }
     if (count >= 2 && aligned && rb_use(C.g) && rb_geom(C.g, 1, (int)sizeof(T), G)) {
         const size_t smem = rb_smem<T>(G, 1);
         if (int rc = rb_allow_smem(k_cc_rb<T>, smem)) return rc;
@@ -783,6 +872,233 @@ static int cc_smooths(fhd_ctx* ctx, CCLevel<T>& C, int count) {
         if (rc) return rc;
     }
     return 0;
+}
+
+// ---------------------------------------------------------------------
+// smoother autotuner
+// ---------------------------------------------------------------------
+// For every level that smooths through launches (above the single-CTA
+// coarse end), the candidate plans -- colour launches with four thread-block
+// shapes, the tiled fused smooth with several tile sizes, the row-tile
+// smooth with every tile height that fits -- are timed once per process,
+// device and level shape with CUDA events, and the fastest is kept.  The
+// timing runs on scratch unknowns and right-hand sides (zero) with the
+// level's own prepared coefficients, before any capture, so a solve's data
+// is never touched.  Every plan evaluates the same update expression on the
+// same operands in the same colour order: the choice changes time only.
+
+constexpr int TUNE_REPS = 3;  // timed smooth pairs per candidate (after one untimed)
+
+static std::mutex g_tune_mu;  // held while a context tunes
+static std::map<std::string, SmoothPlan> g_tune;
+
+static std::string tune_key(fhd_ctx* ctx, const Grid& g, int which, int elem) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    char b[160];
+    snprintf(b, sizeof b, "%d:%c:%d:%d:%d:%dx%dx%d", dev, which ? 'c' : 's', elem, g.dim, which ? 0 : ctx->visc,
+             g.n[0], g.n[1], g.n[2]);
+    return b;
+}
+
+static void colour_cands(std::vector<SmoothPlan>& v, const Grid& g) {
+    static const int shapes[4][2] = {{32, 8}, {64, 4}, {128, 2}, {16, 16}};
+    const int hx = (g.n[0] + 1) / 2;  // cells of one colour per row
+    for (const auto& sh : shapes) {
+        if (sh[0] > 32 && sh[0] > 2 * hx) continue;  // more than half of every block idle
+        SmoothPlan p;
+        p.kind = 0;
+        p.bx = sh[0];
+        p.by = sh[1];
+        v.push_back(p);
+    }
+}
+
+// tiled fused smooth: the default tile and its narrower / shorter variants
+static void rb_cands(std::vector<SmoothPlan>& v, const Grid& g, int ncomp, int elem, int ncoef, int smem_optin) {
+    RBGeom G0;
+    if (!rb_geom(g, ncomp, elem, G0)) return;
+    const int txs[3] = {G0.TX, 32, 16}, tys[3] = {G0.TY, 8, 4};
+    for (int tx : txs)
+        for (int ty : tys) {
+            RBGeom G;
+            if (!rb_geom(g, ncomp, elem, G, tx, ty)) continue;
+            const size_t smem = (size_t)elem * ((size_t)RB_NPH * G.W * G.rows + (size_t)ncoef * RB_NCF * G.W * G.crows);
+            if (smem > (size_t)smem_optin) continue;
+            bool dup = false;
+            for (const auto& q : v) dup = dup || (q.kind == 1 && q.rb.TX == G.TX && q.rb.TY == G.TY);
+            if (dup) continue;
+            SmoothPlan p;
+            p.kind = 1;
+            p.rb = G;
+            v.push_back(p);
+        }
+}
+
+template <typename T>
+static std::vector<SmoothPlan> stag_cands(fhd_ctx* ctx, const StagLevel<T>& L) {
+    std::vector<SmoothPlan> v;
+    colour_cands(v, L.g);
+    rb_cands(v, L.g, 3, (int)sizeof(T), 2, ctx->smem_optin);
+    if (std::is_same<T, float>::value && ctx->visc == 1)
+        for (int ahead : {RBX_AHEAD, 1})
+            for (int ty = 4; ty <= 32; ty *= 2) {
+                RBXGeom X;
+                if (!rbx_geom(L.g, ctx->sms, (size_t)ctx->smem_optin, X, ty, ahead, (size_t)ctx->smem_sm)) continue;
+                SmoothPlan p;
+                p.kind = 2;
+                p.rbx = X;
+                v.push_back(p);
+            }
+    return v;
+}
+
+template <typename T>
+static std::vector<SmoothPlan> cc_cands(fhd_ctx* ctx, const CCLevel<T>& C) {
+    std::vector<SmoothPlan> v;
+    colour_cands(v, C.g);
+    rb_cands(v, C.g, 1, (int)sizeof(T), 1, ctx->smem_optin);
+    return v;
+}
+
+// one untimed smooth pair, then TUNE_REPS timed pairs; us = time of a pair
+template <class F>
+static int time_pairs(fhd_ctx* ctx, cudaEvent_t e0, cudaEvent_t e1, F&& pair, float& us) {
+    if (int rc = pair()) return rc;
+    FHD_CUDA_TRY(cudaEventRecord(e0, ctx->stream));
+    for (int r = 0; r < TUNE_REPS; r++)
+        if (int rc = pair()) return rc;
+    FHD_CUDA_TRY(cudaEventRecord(e1, ctx->stream));
+    FHD_CUDA_TRY(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    FHD_CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
+    us = 1000.f * ms / TUNE_REPS;
+    return 0;
+}
+
+template <typename T>
+static int tune_levels_locked(fhd_ctx* ctx, Multigrid<T>& M, std::vector<T*>& scratch, cudaEvent_t ev[2]) {
+    const int dim = ctx->dim;
+    const int force = ctx->tune_mode >= 2 ? ctx->tune_mode - 2 : -1;
+    // scratch unknowns, right-hand sides and second buffers: 3 dim arrays of
+    // the largest level timed, zeroed
+    auto get_scratch = [&](i64 nc) -> int {
+        if (!scratch.empty()) return 0;
+        for (int i = 0; i < 3 * dim; i++) {
+            void* p = nullptr;
+            FHD_CUDA_TRY(cudaMallocAsync(&p, (size_t)nc * sizeof(T), ctx->stream));
+            scratch.push_back((T*)p);
+            FHD_CUDA_TRY(cudaMemsetAsync(p, 0, (size_t)nc * sizeof(T), ctx->stream));
+        }
+        return 0;
+    };
+    const int lcs = stag_coarse_first(ctx, M), lcc = cc_coarse_first(ctx, M);
+    const i64 nc_max = ctx->g0.nc;
+    for (int l = 0; l < (int)M.s.size(); l++) {
+        StagLevel<T>& L = M.s[l];
+        L.plan = SmoothPlan();
+        if (l >= lcs || !all_even(L.g) || ctx->p.stag_mg_smoother == 0) continue;
+        const std::string key = tune_key(ctx, L.g, 0, (int)sizeof(T));
+        auto it = g_tune.find(key);
+        if (force < 0 && it != g_tune.end()) {
+            L.plan = it->second;
+            continue;
+        }
+        std::vector<SmoothPlan> cands = stag_cands(ctx, L);
+        if (force >= 0) {
+            L.plan = cands[(size_t)force < cands.size() ? force : 0];
+            L.plan.ncand = (int)cands.size();
+            continue;
+        }
+        if (int rc = get_scratch(nc_max)) return rc;
+        StagLevel<T> S = L;  // scratch unknowns, the level's coefficients
+        for (int c = 0; c < dim; c++) {
+            S.phi[c] = scratch[c];
+            S.tmp[c] = scratch[dim + c];
+            S.rhs[c] = scratch[2 * dim + c];
+        }
+        if (!stag_aligned(S, dim)) continue;
+        int best = -1;
+        for (size_t i = 0; i < cands.size(); i++) {
+            float us = 0.f;
+            if (int rc = time_pairs(ctx, ev[0], ev[1], [&]() { return stag_smooths_planned(ctx, S, cands[i], 2); },
+                                    us))
+                return rc;
+            cands[i].us = us;
+            if (best < 0 || us < cands[best].us) best = (int)i;
+        }
+        L.plan = cands[best];
+        L.plan.ncand = (int)cands.size();
+        g_tune[key] = L.plan;
+    }
+    for (int l = 0; l < (int)M.c.size(); l++) {
+        CCLevel<T>& C = M.c[l];
+        C.plan = SmoothPlan();
+        if (l >= lcc || !all_even(C.g)) continue;
+        const std::string key = tune_key(ctx, C.g, 1, (int)sizeof(T));
+        auto it = g_tune.find(key);
+        if (force < 0 && it != g_tune.end()) {
+            C.plan = it->second;
+            continue;
+        }
+        std::vector<SmoothPlan> cands = cc_cands(ctx, C);
+        if (force >= 0) {
+            C.plan = cands[(size_t)force < cands.size() ? force : 0];
+            C.plan.ncand = (int)cands.size();
+            continue;
+        }
+        if (int rc = get_scratch(nc_max)) return rc;
+        CCLevel<T> S = C;
+        S.phi = scratch[0];
+        S.tmp = scratch[1];
+        S.rhs = scratch[2];
+        int best = -1;
+        for (size_t i = 0; i < cands.size(); i++) {
+            float us = 0.f;
+            if (int rc = time_pairs(ctx, ev[0], ev[1], [&]() {
+                    S.plan = cands[i];
+                    return cc_smooths(ctx, S, 2);
+                }, us))
+                return rc;
+            cands[i].us = us;
+            if (best < 0 || us < cands[best].us) best = (int)i;
+        }
+        C.plan = cands[best];
+        C.plan.ncand = (int)cands.size();
+        g_tune[key] = C.plan;
+    }
+    return 0;
+}
+
+template <typename T>
+static int tune_levels(fhd_ctx* ctx) {
+    Multigrid<T>& M = mg_of<T>(ctx);
+    if (ctx->tune_mode == 0) {
+        for (auto& L : M.s) L.plan = SmoothPlan();
+        for (auto& C : M.c) C.plan = SmoothPlan();
+        return 0;
+    }
+    // inside a capture the plans of the last solve call stand
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(ctx->stream, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return 0;
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    const bool prof = ctx->prof;
+    const long long launches = ctx->launches;
+    ctx->prof = false;
+    std::vector<T*> scratch;
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    int rc = 0;
+    if (cudaEventCreate(&ev[0]) != cudaSuccess || cudaEventCreate(&ev[1]) != cudaSuccess) {
+        set_last_error("autotuner: cudaEventCreate failed");
+        rc = FHD_ERR_CUDA;
+    }
+    if (!rc) rc = tune_levels_locked(ctx, M, scratch, ev);
+    for (T* p : scratch) cudaFreeAsync(p, ctx->stream);
+    for (cudaEvent_t e : ev)
+        if (e) cudaEventDestroy(e);
+    ctx->prof = prof;
+    ctx->launches = launches;
+    return rc;
 }
 
 // levels lc..bottom of the pressure V-cycle in one CTA (phi of level lc:
@@ -1596,7 +1912,8 @@ int fhd_ctx_create(int dim, const int n_cells[3], const double dx[3], int visc_t
         int dev = 0;
         if (cudaGetDevice(&dev) != cudaSuccess ||
             cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
-            cudaDeviceGetAttribute(&c->smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess)
+            cudaDeviceGetAttribute(&c->smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&c->smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) != cudaSuccess)
             rc = FHD_ERR_CUDA;
     }
     if (!rc && cudaStreamSynchronize(c->stream) != cudaSuccess) rc = FHD_ERR_CUDA;
@@ -1678,6 +1995,37 @@ int fhd_ctx_set_fused(fhd_ctx* c, int mode) {
     // captured preconditioner graphs hold the other launch sequence
     release_graphs(c);
     c->fused_mode = mode;
+    return FHD_OK;
+}
+
+int fhd_ctx_set_tune(fhd_ctx* c, int mode) {
+    if (!c || mode < -1 || mode > 64) return FHD_ERR_BAD_ARG;
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess) return FHD_ERR_CUDA;
+    release_graphs(c);
+    c->tune_mode = mode;
+    return FHD_OK;
+}
+
+int fhd_ctx_tune_info(fhd_ctx* c, int which, int level, int* kind, int* ncand, double* pair_us, int shape[4]) {
+    if (!c || (which != 0 && which != 1) || level < 0) return FHD_ERR_BAD_ARG;
+    const SmoothPlan* P = nullptr;
+    if (c->prec == FHD_PREC_MIXED) {
+        if (which == 0 && level < (int)c->mg32.s.size()) P = &c->mg32.s[level].plan;
+        if (which == 1 && level < (int)c->mg32.c.size()) P = &c->mg32.c[level].plan;
+    } else {
+        if (which == 0 && level < (int)c->mg64.s.size()) P = &c->mg64.s[level].plan;
+        if (which == 1 && level < (int)c->mg64.c.size()) P = &c->mg64.c[level].plan;
+    }
+    if (!P) return FHD_ERR_BAD_ARG;
+    if (kind) *kind = P->kind;
+    if (ncand) *ncand = P->ncand;
+    if (pair_us) *pair_us = P->us;
+    if (shape) {
+        shape[0] = P->kind == 0 ? P->bx : P->kind == 1 ? P->rb.TX : P->kind == 2 ? c->n[0] : 0;
+        shape[1] = P->kind == 0 ? P->by : P->kind == 1 ? P->rb.TY : P->kind == 2 ? P->rbx.TY : 0;
+        shape[2] = P->kind == 1 ? P->rb.chunks : P->kind == 2 ? P->rbx.chunks : 0;
+        shape[3] = P->kind == 2 ? P->rbx.per_sm : P->kind >= 0 ? 1 : 0;
+    }
     return FHD_OK;
 }
 

@@ -138,9 +138,22 @@ struct Arena {
 double* pinned_scalars_acquire();
 void pinned_scalars_release(double* p);
 
+// how one multigrid level smooths, as the autotuner picked it (kind -1:
+// not tuned, the fixed size rules choose).  Every plan evaluates the same
+// update expression on the same operands in the same colour order.
+struct SmoothPlan {
+    int kind = -1;        // 0 colour launches, 1 tiled fused smooth, 2 row-tile smooth (FP32 visc_type 1)
+    int bx = 32, by = 8;  // colour launches: thread block (bx * by = 256)
+    RBGeom rb;            // kind 1
+    RBXGeom rbx;          // kind 2
+    float us = 0.f;       // measured time of one smooth pair
+    int ncand = 0;        // candidates the tuner considered
+};
+
 template <typename T>
 struct StagLevel {
     Grid g;
+    SmoothPlan plan;
     T* alpha[3] = {nullptr, nullptr, nullptr};  // owned on coarse levels
     T alpha_scale = T(1);
     const T* beta = nullptr;
@@ -168,6 +181,7 @@ struct StagLevel {
 template <typename T>
 struct CCLevel {
     Grid g;
+    SmoothPlan plan;
     T* a[3] = {nullptr, nullptr, nullptr};
     T* phi = nullptr;
     T* rhs = nullptr;
@@ -237,8 +251,10 @@ struct fhd_ctx {
     int coarse_mode = -1;
     // the row-tile fused smoother on large FP32 levels (-1 default: on, 0 off)
     int fused_mode = -1;
+    int tune_mode = -1;           // smoother autotuner (fhd_ctx_set_tune)
     int sms = 148;                // multiprocessors of the device
     int smem_optin = 48 * 1024;   // shared memory a block may opt in to
+    int smem_sm = 0;              // shared memory of one multiprocessor
     unsigned* dev_err = nullptr;  // set by a kernel whose bounded wait ran out
     struct PreconGraph {
         unsigned long long key = 0;

@@ -209,13 +209,23 @@ struct Lin {
     double a[4];
     int nt;
 };
+// (all components of an element advance together, each term in order, and
+// are stored after every load of the element: ncomp * nt loads in flight)
 __global__ void __launch_bounds__(256) k_lin(i64 n, int ncomp, SVec<double> y, Lin L, int keep) {
     for (i64 f = blockIdx.x * (i64)blockDim.x + threadIdx.x; f < n; f += (i64)gridDim.x * blockDim.x) {
-        for (int c = 0; c < ncomp; c++) {
-            double v = keep ? y.c[c][f] : 0.0;
-            for (int t = 0; t < L.nt; t++) v = v + L.a[t] * L.x[t][c][f];
-            y.c[c][f] = v;
+        double v[3];  // ncomp <= 3 (Lin holds three components)
+#pragma unroll
+        for (int c = 0; c < 3; c++)
+            if (c < ncomp) v[c] = keep ? y.c[c][f] : 0.0;
+        for (int t = 0; t < L.nt; t++) {
+            const double a = L.a[t];
+#pragma unroll
+            for (int c = 0; c < 3; c++)
+                if (c < ncomp) v[c] = v[c] + a * L.x[t][c][f];
         }
+#pragma unroll
+        for (int c = 0; c < 3; c++)
+            if (c < ncomp) y.c[c][f] = v[c];
     }
 }
 

@@ -120,35 +120,70 @@ static __global__ void __launch_bounds__(RED_THREADS) k_mgs(i64 n, int ncomp, SV
 }
 
 // v = w / sqrt(nrm2)  (gmres.f90:380-389 with H(i+1,i) = sqrt(nrm2))
+// (every component of an element is loaded before any is stored, so a
+// thread keeps ncomp loads in flight although v and w may alias)
 static __global__ void __launch_bounds__(256) k_scale_by_norm(i64 n, int ncomp, SVec<double> v, CSVec<double> w,
                                                        const double* nrm2) {
     const double h = sqrt(*nrm2);
-    for (i64 f = blockIdx.x * (i64)blockDim.x + threadIdx.x; f < n; f += (i64)gridDim.x * blockDim.x)
-        for (int c = 0; c < ncomp; c++) v.c[c][f] = w.c[c][f] / h;
+    for (i64 f = blockIdx.x * (i64)blockDim.x + threadIdx.x; f < n; f += (i64)gridDim.x * blockDim.x) {
+        double a[4];
+#pragma unroll
+        for (int c = 0; c < 4; c++)
+            if (c < ncomp) a[c] = w.c[c][f];
+#pragma unroll
+        for (int c = 0; c < 4; c++)
+            if (c < ncomp) v.c[c][f] = a[c] / h;
+    }
 }
 
 // v = w / s (host scalar)
 static __global__ void __launch_bounds__(256) k_scale_div(i64 n, int ncomp, SVec<double> v, CSVec<double> w, double s) {
-    for (i64 f = blockIdx.x * (i64)blockDim.x + threadIdx.x; f < n; f += (i64)gridDim.x * blockDim.x)
-        for (int c = 0; c < ncomp; c++) v.c[c][f] = w.c[c][f] / s;
+    for (i64 f = blockIdx.x * (i64)blockDim.x + threadIdx.x; f < n; f += (i64)gridDim.x * blockDim.x) {
+        double a[4];
+#pragma unroll
+        for (int c = 0; c < 4; c++)
+            if (c < ncomp) a[c] = w.c[c][f];
+#pragma unroll
+        for (int c = 0; c < 4; c++)
+            if (c < ncomp) v.c[c][f] = a[c] / s;
+    }
 }
 
 // x += sum_{it < m} y[it] v_it (update_sol, gmres.f90:495-529; same order)
 static __global__ void __launch_bounds__(256) k_update_sol(i64 n, int ncomp, SVec<double> x, const double* __restrict__ V,
                                                     i64 vstride, const double* y, int m) {
     for (i64 f = blockIdx.x * (i64)blockDim.x + threadIdx.x; f < n; f += (i64)gridDim.x * blockDim.x) {
-        for (int c = 0; c < ncomp; c++) {
-            double acc = x.c[c][f];
-            for (int it = 0; it < m; it++) acc = acc + V[it * vstride + (i64)c * n + f] * y[it];
-            x.c[c][f] = acc;
+        // all components advance together (each in the order of update_sol),
+        // so the loads of every component are in flight at once
+        double acc[4];
+#pragma unroll
+        for (int c = 0; c < 4; c++)
+            if (c < ncomp) acc[c] = x.c[c][f];
+        for (int it = 0; it < m; it++) {
+            const double yi = y[it];
+#pragma unroll
+            for (int c = 0; c < 4; c++)
+                if (c < ncomp) acc[c] = acc[c] + V[it * vstride + (i64)c * n + f] * yi;
         }
+#pragma unroll
+        for (int c = 0; c < 4; c++)
+            if (c < ncomp) x.c[c][f] = acc[c];
     }
 }
 
 template <typename TO, typename TI>
 static __global__ void __launch_bounds__(256) k_copy_conv(i64 n, TO* __restrict__ o, const TI* __restrict__ in, double s) {
-    for (i64 f = blockIdx.x * (i64)blockDim.x + threadIdx.x; f < n; f += (i64)gridDim.x * blockDim.x)
-        o[f] = (TO)((double)in[f] * s);
+    // four grid strides per pass: four loads in flight per thread
+    const i64 st = (i64)gridDim.x * blockDim.x;
+    i64 f = blockIdx.x * (i64)blockDim.x + threadIdx.x;
+    for (; f + 3 * st < n; f += 4 * st) {
+        TI a[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) a[u] = in[f + u * st];
+#pragma unroll
+        for (int u = 0; u < 4; u++) o[f + u * st] = (TO)((double)a[u] * s);
+    }
+    for (; f < n; f += st) o[f] = (TO)((double)in[f] * s);
 }
 
 template <typename T>

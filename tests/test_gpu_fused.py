@@ -27,6 +27,7 @@ def _vcycle_and_precon(cuda, n, fused, seed=51):
     b_u, b_p = P.random_stokes(dim, n, seed=seed + 2, zero_mean_p=False)
     with L.StokesSolver(dim, n, 1.0, visc, params=L.default_params(), precision="mixed") as s:
         s.set_fused(fused)
+        s.set_tune(0)  # the fixed size rules: fused where the level allows
         coef = (dev(pb.alpha_fc, cuda), dev(pb.beta, cuda), dev(pb.beta_ed, cuda), dev(pb.gamma, cuda))
         phi = zeros(pb.nc, dim, cuda)
         s.stag_mg_solver(*coef, 0.7, phi, dev(rhs, cuda))
@@ -66,6 +67,7 @@ def test_fused_gmres(cuda):
         with L.StokesSolver(dim, n, 1.0, visc, params=L.default_params(gmres_rel_tol=1e-8),
                             precision="mixed") as s:
             s.set_fused(fused)
+            s.set_tune(0)
             x_u, x_p = zeros(pb.nc, dim, cuda), zeros(pb.nc, 1, cuda)[0]
             status, _, st = s.gmres(dev(b_u, cuda), dev(b_p, cuda), x_u, x_p, dev(pb.alpha_fc, cuda),
                                     dev(pb.beta, cuda), dev(pb.beta_ed, cuda), dev(pb.gamma, cuda), 20.0)
