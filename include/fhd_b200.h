@@ -416,6 +416,30 @@ int fhd_sched_simulate(int slots, unsigned long long budget, int n,
 const char* fhd_last_error(void);
 /* Bytes of device memory a context holds. */
 unsigned long long fhd_ctx_device_bytes(fhd_ctx* ctx);
+/* ------------------------------------------------------------------ */
+/* static structure factors on the device                              */
+/* ------------------------------------------------------------------ */
+/* Replaces HydroGrid's updateStructureFactors (HydroGrid/
+ * HydroGridModule.f90:1077-1180) and the normalisation of
+ * writeStructureFactors (1862-1868) for periodic boxes: per sample, the
+ * unnormalised forward DFT of each of nvars device fields (canonical layout,
+ * x fastest), the staggered-velocity phase shift exp(i s k_d pi / N_d) of
+ * variable d < dim when shift[d] = s is +1 or -1 (HydroGridModule.f90:
+ * 1119-1141; shift may be NULL), and for each of npairs pairs (a, b) =
+ * (pairs[2p], pairs[2p+1]) the running mean of Ua conj(Ub).  fhd_sk_read
+ * returns pair p times dV / N_cells (structFactMultiplier 1) on the half
+ * spectrum kx = 0 .. nx/2, index (kz, ky, kx) with kx fastest, in host
+ * arrays of fhd_sk_modes() doubles (re or im may be NULL).  update orders
+ * itself after the caller's stream (NULL: none) and makes that stream wait
+ * for it.  nvars <= 8, npairs <= 16. */
+typedef struct fhd_sk fhd_sk;
+int fhd_sk_create(int dim, const int n_cells[3], double dV, int nvars, const int* shift, int npairs,
+                  const int* pairs, fhd_sk** out);
+int fhd_sk_update(fhd_sk* sk, const double* const vars[], void* stream);
+int fhd_sk_read(fhd_sk* sk, int pair, double* re, double* im, long long* samples);
+long long fhd_sk_modes(fhd_sk* sk);
+int fhd_sk_destroy(fhd_sk* sk);
+
 /* Timing of the finest-level colour smoother (the dominant kernel; the
  * smooths of stag_mg_solver.f90:360-396): while enabled, CUDA events on the
  * context stream bracket each launch.  read returns the launches, their

@@ -23,7 +23,7 @@ from ._capi import (FHD_PREC_FP64, FHD_PREC_MIXED, FHD_REQ_INERTIAL, FHD_REQ_OVE
                     mixture_params)
 
 __all__ = ["StokesSolver", "GmresParams", "StochParams", "SolveStats", "MixtureParams", "mixture_params",
-           "Server", "Request", "RequestResult", "make_request", "fill_normal", "philox4x32_10", "sched_simulate",
+           "Server", "StructureFactor", "Request", "RequestResult", "make_request", "fill_normal", "philox4x32_10", "sched_simulate",
            "FHD_REQ_OVERDAMPED", "FHD_REQ_INERTIAL",
            "default_params", "FhdError",
            "FHD_PREC_FP64", "FHD_PREC_MIXED", "lib", "fab_from_canonical", "canonical_from_fab", "FabArray"]
@@ -414,6 +414,58 @@ def sched_simulate(slots: int, budget: int, arrive, nbytes, runtime):
     check(lib().fhd_sched_simulate(int(slots), int(budget), n, C.cast(a, _DP), b, C.cast(r, _DP), C.cast(s, _DP)),
           "sched_simulate")
     return list(s)[:n]
+
+
+class StructureFactor:
+    """Static structure factors on the device (fhd_sk_*; HydroGrid's
+    updateStructureFactors, HydroGrid/HydroGridModule.f90:1077-1180): per
+    update, the DFT of each of `nvars` fields, the staggered phase shift of
+    velocity component d when shift[d] is +1 or -1, and the running mean of
+    Ua conj(Ub) for every pair (a, b); read(p) returns pair p times dV/N_c
+    on the half spectrum as a complex array of shape (nz, ny, nx//2+1) (2D:
+    (ny, nx//2+1))."""
+
+    def __init__(self, dim: int, n_cells: Sequence[int], dV: float, nvars: int, pairs, shift=None):
+        n = (C.c_int * 3)(*(list(n_cells) + [1] * (3 - len(n_cells))))
+        pr = [int(x) for p in pairs for x in p]
+        parr = (C.c_int * len(pr))(*pr)
+        sarr = (C.c_int * nvars)(*[int(x) for x in shift]) if shift is not None else None
+        h = C.c_void_p()
+        check(lib().fhd_sk_create(int(dim), n, float(dV), int(nvars), sarr, len(pairs), parr, C.byref(h)),
+              "fhd_sk_create")
+        self._h = h
+        self.dim = dim
+        self.n = list(n_cells)
+        self.npairs = len(pairs)
+
+    def update(self, fields, stream_handle: int | None = None):
+        check(lib().fhd_sk_update(self._h, _dpp(fields), C.c_void_p(stream_handle or 0)), "fhd_sk_update")
+
+    def read(self, pair: int):
+        nm = int(lib().fhd_sk_modes(self._h))
+        re, im = np.empty(nm), np.empty(nm)
+        ns = C.c_longlong()
+        check(lib().fhd_sk_read(self._h, int(pair), re.ctypes.data_as(_DP), im.ctypes.data_as(_DP), C.byref(ns)),
+              "fhd_sk_read")
+        shape = ([self.n[2]] if self.dim == 3 else []) + [self.n[1], self.n[0] // 2 + 1]
+        return (re + 1j * im).reshape(shape), ns.value
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().fhd_sk_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class Server:

@@ -144,6 +144,13 @@ _PROTOS = {
     "fhd_ctx_set_coarse": (C.c_int, [_VP, C.c_int]),
     "fhd_ctx_set_fused": (C.c_int, [_VP, C.c_int]),
     "fhd_ctx_set_tune": (C.c_int, [_VP, C.c_int]),
+    "fhd_sk_create": (C.c_int, [C.c_int, C.POINTER(C.c_int), C.c_double, C.c_int, C.POINTER(C.c_int), C.c_int,
+                                C.POINTER(C.c_int), C.POINTER(_VP)]),
+    "fhd_sk_update": (C.c_int, [_VP, C.POINTER(C.POINTER(C.c_double)), _VP]),
+    "fhd_sk_read": (C.c_int, [_VP, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                              C.POINTER(C.c_longlong)]),
+    "fhd_sk_modes": (C.c_longlong, [_VP]),
+    "fhd_sk_destroy": (C.c_int, [_VP]),
     "fhd_ctx_tune_info": (C.c_int, [_VP, C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
                                     C.POINTER(C.c_double), C.POINTER(C.c_int)]),
     "fhd_ctx_device_bytes": (C.c_ulonglong, [_VP]),

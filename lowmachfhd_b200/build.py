@@ -10,7 +10,8 @@ from concurrent.futures import ThreadPoolExecutor
 HERE = os.path.dirname(os.path.abspath(__file__))
 SRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "_fhd_b200.so")
-SOURCES = ["fhd_solver.cu", "fhd_step.cu", "fhd_capi.cu", "fhd_noalloc.cu", "fhd_mass.cu", "fhd_server.cu"]
+SOURCES = ["fhd_solver.cu", "fhd_step.cu", "fhd_capi.cu", "fhd_noalloc.cu", "fhd_mass.cu", "fhd_server.cu",
+           "fhd_sk.cu"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-lineinfo", "-O3", "-std=c++17",
@@ -48,7 +49,7 @@ def build(verbose: bool = False, extra: list[str] | None = None) -> str:
             if r.returncode:
                 raise subprocess.CalledProcessError(r.returncode, r.args)
     link = [nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-Xcompiler", "-fPIC",
-            "-o", OUT + ".tmp"] + objs + ["-lcudart"]
+            "-o", OUT + ".tmp"] + objs + ["-lcufft", "-lcudart"]
     if verbose:
         print(" ".join(link), flush=True)
     subprocess.run(link, check=True)

@@ -59,6 +59,9 @@ def test_velocity_structure_factor_flat(cuda):
     counts = torch.bincount(shell, minlength=nshell).double()
     acc = torch.zeros(nshell, **f64)
     samples = 0
+    # the library's device structure factor of the same samples (HydroGrid's
+    # S_ii, no phase shift: |u_i(k)|^2 does not depend on it)
+    sk = L.StructureFactor(3, [n, n, n], 1.0, 3, [(0, 0), (1, 1), (2, 2)])
     with L.StokesSolver(3, [n, n, n], 1.0, 1, params=L.default_params(gmres_rel_tol=1e-9)) as s:
         for step in range(1, steps + 1):
             W_cc = [torch.randn(nc, generator=gen, **f64) * math.sqrt(2.0) for _ in range(3)]
@@ -72,8 +75,19 @@ def test_velocity_structure_factor_flat(cuda):
                 S = sum((torch.fft.fftn(x.reshape(n, n, n)).abs() ** 2) for x in u).reshape(-1) / (nc * 2)
                 acc += torch.bincount(shell, weights=S, minlength=nshell)
                 samples += 1
+                sk.update(u)
     acc = acc.cpu().numpy()
     counts = counts.cpu().numpy()
+    # device S(k): half spectrum, modes 0 < kx < n/2 stand for their mirror
+    # images too; shell sums of the running mean times the samples must equal
+    # the shell sums of the torch spectra above
+    dev_sk = sum(sk.read(p)[0].real for p in range(3)) / 2.0
+    sk.close()
+    w = np.full(n // 2 + 1, 2.0)
+    w[0] = w[n // 2] = 1.0
+    half = shell.reshape(n, n, n)[:, :, : n // 2 + 1].cpu().numpy().reshape(-1)
+    dev_acc = np.bincount(half, weights=(dev_sk * w[None, None, :]).reshape(-1), minlength=nshell) * samples
+    assert np.max(np.abs(dev_acc[:nshell] - acc)) <= 1e-10 * np.max(np.abs(acc))
     ref = kT
     # flatness: bands of 8 shells from |k| = 8 to 64 (each > 1e4 modes, so
     # the sampling error is well below the 2 % bar; the lowest shells hold
