@@ -192,6 +192,15 @@ int fhd_ctx_set_tune(fhd_ctx* ctx, int mode);
  * smooths.  Any output pointer may be NULL.  No reference counterpart. */
 int fhd_ctx_tune_info(fhd_ctx* ctx, int which, int level, int* kind, int* ncand, double* pair_us,
                       int shape[4]);
+/* The candidate list the tuner would time for one level (host only, no
+ * device): staggered (which 0) or pressure (1) multigrid, extents, precision
+ * mode, visc_type, and the device's SM count and shared-memory limits (per
+ * block opt-in, per SM).  Writes up to max_out records of 6 ints {kind,
+ * block x | tile x | nx, block y | tile y, z-runs, CTAs per SM, row-tile
+ * shared-memory bytes} and returns the number of candidates.  No reference
+ * counterpart. */
+int fhd_tune_candidates(int which, int dim, const int n_cells[3], int precision_mode, int visc_type, int sms,
+                        int smem_optin, int smem_sm, int* out, int max_out);
 /* Number of this library's kernels launched through ctx so far. */
 long long fhd_ctx_kernel_launches(fhd_ctx* ctx);
 const char* fhd_status_string(int status);

@@ -23,7 +23,7 @@ from ._capi import (FHD_PREC_FP64, FHD_PREC_MIXED, FHD_REQ_INERTIAL, FHD_REQ_OVE
                     mixture_params)
 
 __all__ = ["StokesSolver", "GmresParams", "StochParams", "SolveStats", "MixtureParams", "mixture_params",
-           "Server", "StructureFactor", "Request", "RequestResult", "make_request", "fill_normal", "philox4x32_10", "sched_simulate",
+           "Server", "StructureFactor", "tune_candidates", "Request", "RequestResult", "make_request", "fill_normal", "philox4x32_10", "sched_simulate",
            "FHD_REQ_OVERDAMPED", "FHD_REQ_INERTIAL",
            "default_params", "FhdError",
            "FHD_PREC_FP64", "FHD_PREC_MIXED", "lib", "fab_from_canonical", "canonical_from_fab", "FabArray"]
@@ -414,6 +414,20 @@ def sched_simulate(slots: int, budget: int, arrive, nbytes, runtime):
     check(lib().fhd_sched_simulate(int(slots), int(budget), n, C.cast(a, _DP), b, C.cast(r, _DP), C.cast(s, _DP)),
           "sched_simulate")
     return list(s)[:n]
+
+
+def tune_candidates(which: str, dim: int, n_cells, precision: str = "mixed", visc_type: int = 1, sms: int = 148,
+                    smem_optin: int = 232448, smem_sm: int = 233472) -> list[dict]:
+    """the smoother plans the autotuner would time for one level (host
+    only); defaults: the B200's 148 SMs and shared-memory limits"""
+    n = (C.c_int * 3)(*(list(n_cells) + [1] * (3 - len(n_cells))))
+    prec = FHD_PREC_MIXED if precision == "mixed" else FHD_PREC_FP64
+    out = (C.c_int * (6 * 64))()
+    k = check(lib().fhd_tune_candidates(0 if which == "stag" else 1, int(dim), n, prec, int(visc_type), int(sms),
+                                        int(smem_optin), int(smem_sm), out, 64), "fhd_tune_candidates")
+    names = {0: "colour", 1: "tiled", 2: "rowtile"}
+    return [dict(kind=names[out[6 * i]], x=out[6 * i + 1], y=out[6 * i + 2], zruns=out[6 * i + 3],
+                 per_sm=out[6 * i + 4], smem=out[6 * i + 5]) for i in range(min(k, 64))]
 
 
 class StructureFactor:

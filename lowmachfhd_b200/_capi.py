@@ -144,6 +144,8 @@ _PROTOS = {
     "fhd_ctx_set_coarse": (C.c_int, [_VP, C.c_int]),
     "fhd_ctx_set_fused": (C.c_int, [_VP, C.c_int]),
     "fhd_ctx_set_tune": (C.c_int, [_VP, C.c_int]),
+    "fhd_tune_candidates": (C.c_int, [C.c_int, C.c_int, C.POINTER(C.c_int), C.c_int, C.c_int, C.c_int, C.c_int,
+                                      C.c_int, C.POINTER(C.c_int), C.c_int]),
     "fhd_sk_create": (C.c_int, [C.c_int, C.POINTER(C.c_int), C.c_double, C.c_int, C.POINTER(C.c_int), C.c_int,
                                 C.POINTER(C.c_int), C.POINTER(_VP)]),
     "fhd_sk_update": (C.c_int, [_VP, C.POINTER(C.POINTER(C.c_double)), _VP]),

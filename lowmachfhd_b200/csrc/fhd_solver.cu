@@ -2006,6 +2006,56 @@ int fhd_ctx_set_tune(fhd_ctx* c, int mode) {
     return FHD_OK;
 }
 
+int fhd_tune_candidates(int which, int dim, const int n_cells[3], int precision_mode, int visc_type, int sms,
+                        int smem_optin, int smem_sm, int* out, int max_out) {
+    if ((which != 0 && which != 1) || (dim != 2 && dim != 3) || !n_cells || sms < 1 || smem_optin < 1 ||
+        max_out < 0 || (max_out > 0 && !out))
+        return FHD_ERR_BAD_ARG;
+    for (int d = 0; d < dim; d++)
+        if (n_cells[d] < 2) return FHD_ERR_BAD_ARG;
+    fhd_ctx c;  // only the fields the candidate lists read
+    c.dim = dim;
+    c.visc = visc_type;
+    c.sms = sms;
+    c.smem_optin = smem_optin;
+    c.smem_sm = smem_sm;
+    const Grid g = make_grid(dim, n_cells, 1.0);
+    std::vector<SmoothPlan> v;
+    const bool f32 = precision_mode == FHD_PREC_MIXED;
+    if (which == 0) {
+        if (f32) {
+            StagLevel<float> L;
+            L.g = g;
+            v = stag_cands(&c, L);
+        } else {
+            StagLevel<double> L;
+            L.g = g;
+            v = stag_cands(&c, L);
+        }
+    } else {
+        if (f32) {
+            CCLevel<float> C;
+            C.g = g;
+            v = cc_cands(&c, C);
+        } else {
+            CCLevel<double> C;
+            C.g = g;
+            v = cc_cands(&c, C);
+        }
+    }
+    for (int i = 0; i < (int)v.size() && i < max_out; i++) {
+        const SmoothPlan& P = v[i];
+        int* o = out + 6 * i;
+        o[0] = P.kind;
+        o[1] = P.kind == 0 ? P.bx : P.kind == 1 ? P.rb.TX : g.n[0];
+        o[2] = P.kind == 0 ? P.by : P.kind == 1 ? P.rb.TY : P.rbx.TY;
+        o[3] = P.kind == 1 ? P.rb.chunks : P.kind == 2 ? P.rbx.chunks : 0;
+        o[4] = P.kind == 2 ? P.rbx.per_sm : 1;
+        o[5] = P.kind == 2 ? (int)P.rbx.smem : 0;
+    }
+    return (int)v.size();
+}
+
 int fhd_ctx_tune_info(fhd_ctx* c, int which, int level, int* kind, int* ncand, double* pair_us, int shape[4]) {
     if (!c || (which != 0 && which != 1) || level < 0) return FHD_ERR_BAD_ARG;
     const SmoothPlan* P = nullptr;
