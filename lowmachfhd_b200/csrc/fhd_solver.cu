@@ -137,6 +137,10 @@ static int build_mg(fhd_ctx* ctx, Multigrid<T>& M) {
         for (int c = 0; c < dim; c++) {
             C.a[c] = A.alloc<T>(nc);
             if (!C.a[c]) return FHD_ERR_OOM;
+            if (ctx->p.visc_schur_approx != 0) {
+                C.amu[c] = A.alloc<T>(nc);
+                if (!C.amu[c]) return FHD_ERR_OOM;
+            }
         }
         C.phi = A.alloc<T>(nc);
         C.rhs = A.alloc<T>(nc);
@@ -151,6 +155,11 @@ static int build_mg(fhd_ctx* ctx, Multigrid<T>& M) {
     }
     M.mac_rhs = A.alloc<T>(nc0);
     if (!M.mac_rhs) return FHD_ERR_OOM;
+    if (ctx->p.visc_schur_approx != 0) {
+        for (int c = 0; c < dim; c++)
+            if (!(M.bf_g[c] = A.alloc<T>(nc0))) return FHD_ERR_OOM;
+        if (!(M.bf_phi = A.alloc<T>(nc0))) return FHD_ERR_OOM;
+    }
     return 0;
 }
 
@@ -247,6 +256,27 @@ static int prepare_T(fhd_ctx* ctx) {
             });
             if (rc) return rc;
         }
+    }
+    // the BFBt pressure multigrid: mu^-1 = 1/diag(viscous operator)
+    // (apply_precon.f90:589), coarsened as alpha^-1 is
+    if (ctx->p.visc_schur_approx != 0) {
+        int rc = 0;
+        CCLevel<T>& C0 = M.c[0];
+        with_dim(dim, [&](auto D) {
+            constexpr int DIM = decltype(D)::value;
+            k_inv_diag_lap<T, DIM><<<cell_grid(C0.g), cell_block(), 0, st>>>(
+                C0.g, ctx->visc, ctx->beta, ctx->beta_ed[0], ctx->beta_ed[1], ctx->beta_ed[2], C0.amu[0], C0.amu[1],
+                C0.amu[2]);
+            rc |= post(ctx);
+            for (size_t l = 1; l < M.c.size(); l++) {
+                CCLevel<T>& F = M.c[l - 1];
+                CCLevel<T>& C = M.c[l];
+                k_stag_restrict<T, DIM><<<cell_grid(C.g), cell_block(), 0, st>>>(
+                    F.g, C.g, F.amu[0], F.amu[1], F.amu[2], C.amu[0], C.amu[1], C.amu[2], 1);
+                rc |= post(ctx);
+            }
+        });
+        if (rc) return rc;
     }
     return 0;
 }
@@ -1205,7 +1235,8 @@ static int cc_solve(fhd_ctx* ctx, Multigrid<T>& M) {
 }
 
 // ---------------------------------------------------------------------
-// apply_precon (apply_precon.f90:29-475), visc_schur_approx = 0
+// apply_precon (apply_precon.f90:29-475); visc_schur_approx 0 (simple
+// Schur complements) or 1 (visc_schur_complement, 538-685)
 // ---------------------------------------------------------------------
 template <typename T>
 static int precon_T(fhd_ctx* ctx, CSVec<double> b, SVec<double> x) {
@@ -1219,8 +1250,11 @@ static int precon_T(fhd_ctx* ctx, CSVec<double> b, SVec<double> x) {
     const double theta = ctx->theta;
     const bool fp64 = std::is_same<T, double>::value;
     const int nb = flat_blocks(nc);
-    if (ctx->p.visc_schur_approx != 0 || apt < 1 || apt > 5) {
-        set_last_error("apply_precon: unsupported precon_type / visc_schur_approx");
+    const bool bfbt = ctx->p.visc_schur_approx != 0;
+    if (apt < 1 || apt > 5 || (bfbt && av == 3)) {
+        set_last_error(bfbt && av == 3 ? "apply_precon: visc_schur_approx needs |visc_type| 1 or 2 "
+                                         "(inverse_diag_lap.f90 has no |visc_type| = 3)"
+                                       : "apply_precon: unsupported precon_type");
         return FHD_ERR_UNSUPPORTED;
     }
     StagLevel<T>& L0 = M.s[0];
@@ -1269,6 +1303,47 @@ static int precon_T(fhd_ctx* ctx, CSVec<double> b, SVec<double> x) {
         });
         return rc;
     };
+    // visc_schur_complement (apply_precon.f90:538-685): x_p = Phi_mu2 (+
+    // theta Phi), Phi_mu = L_mu^-1 mac_rhs, Phi_mu2 = L_mu^-1 D mu^-1 L
+    // mu^-1 G Phi_mu; L_mu the pressure multigrid on the mu^-1 faces, L the
+    // viscous operator without the alpha term
+    auto visc_schur = [&](int add_phi, int negate) -> int {
+        CCLevel<T>& C0 = M.c[0];
+        int rc = 0;
+        if (add_phi) FHD_CUDA_TRY(cudaMemcpyAsync(M.bf_phi, C0.phi, sizeof(T) * nc, cudaMemcpyDeviceToDevice, st));
+        auto swap_coef = [&]() {
+            for (auto& C : M.c)
+                for (int c = 0; c < 3; c++) std::swap(C.a[c], C.amu[c]);
+        };
+        swap_coef();  // the pressure multigrid now runs on mu^-1
+        rc = cc_solve(ctx, M);
+        if (!rc) {
+            StagOp<T> A = L0.op();
+            A.alpha_scale = T(0);
+            with_dim_visc(dim, ctx->visc, [&](auto D, auto V) {
+                constexpr int DIM = decltype(D)::value, VISC = decltype(V)::value;
+                k_grad_mul<T, DIM><<<cell_grid(g), cell_block(), 0, st>>>(
+                    g, C0.phi, C0.a[0], C0.a[1], C0.a[2], M.bf_g[0], M.bf_g[1], M.bf_g[2], (T)(1.0 / g.dx));
+                rc |= post(ctx);
+                k_stag_apply<T, DIM, VISC><<<cell_grid(g), cell_block(), 0, st>>>(
+                    g, A, M.bf_g[0], M.bf_g[1], M.bf_g[2], L0.tmp[0], L0.tmp[1], L0.tmp[2], nullptr, nullptr,
+                    nullptr, 0);
+                rc |= post(ctx);
+                k_mul_faces<T><<<nb, 256, 0, st>>>(nc, DIM, L0.tmp[0], L0.tmp[1], L0.tmp[2], C0.a[0], C0.a[1],
+                                                   C0.a[2]);
+                rc |= post(ctx);
+                k_div_plus<T, DIM><<<cell_grid(g), cell_block(), 0, st>>>(g, L0.tmp[0], L0.tmp[1], L0.tmp[2],
+                                                                        nullptr, C0.rhs, (T)(1.0 / g.dx));
+                rc |= post(ctx);
+            });
+        }
+        if (!rc) rc = cc_solve(ctx, M);
+        swap_coef();
+        if (rc) return rc;
+        k_bfbt_out<T><<<nb, 256, 0, st>>>(nc, x.c[dim], C0.phi, M.bf_phi, theta, add_phi, negate);
+        FHD_POST(ctx);
+        return 0;
+    };
     // b_u - G x_p into the multigrid rhs (precon 3 and 5)
     auto rhs_minus_grad_xp = [&]() -> int {
         int rc = 0;
@@ -1297,7 +1372,7 @@ static int precon_T(fhd_ctx* ctx, CSVec<double> b, SVec<double> x) {
         });
         if (rc) return rc;
         const int kind = (pt == 1 || theta == 0.0) ? 0 : 1;
-        if ((rc = schur(kind, 1, 0))) return rc;
+        if ((rc = bfbt ? visc_schur(fabs(theta) > 0.0, 0) : schur(kind, 1, 0))) return rc;
     } else if (apt == 2 || apt == 5) {
         if ((rc = set_rhs_from_b())) return rc;
         if ((rc = stag_mg_run(ctx, M))) return rc;
@@ -1305,7 +1380,9 @@ static int precon_T(fhd_ctx* ctx, CSVec<double> b, SVec<double> x) {
         if (fabs(theta) > 0.0) {
             if ((rc = cc_solve(ctx, M))) return rc;
         }
-        if ((rc = schur(0, fabs(theta) > 0.0, (pt == -2 || pt == -5)))) return rc;
+        if ((rc = bfbt ? visc_schur(fabs(theta) > 0.0, (pt == -2 || pt == -5))
+                       : schur(0, fabs(theta) > 0.0, (pt == -2 || pt == -5))))
+            return rc;
         if (apt == 5) {
             if ((rc = rhs_minus_grad_xp())) return rc;
             if ((rc = stag_mg_run(ctx, M))) return rc;
@@ -1317,7 +1394,7 @@ static int precon_T(fhd_ctx* ctx, CSVec<double> b, SVec<double> x) {
         if (fabs(theta) > 0.0) {
             if ((rc = cc_solve(ctx, M))) return rc;
         }
-        if ((rc = schur(0, fabs(theta) > 0.0, 0))) return rc;
+        if ((rc = bfbt ? visc_schur(fabs(theta) > 0.0, 0) : schur(0, fabs(theta) > 0.0, 0))) return rc;
         if ((rc = rhs_minus_grad_xp())) return rc;
         if ((rc = stag_mg_run(ctx, M))) return rc;
         if ((rc = phi_to_x())) return rc;
@@ -1329,13 +1406,22 @@ static int precon_T(fhd_ctx* ctx, CSVec<double> b, SVec<double> x) {
             k_copy_conv<T, double><<<nb, 256, 0, st>>>(nc, M.c[0].rhs, b.c[dim], 1.0);
             FHD_POST(ctx);
             if ((rc = cc_solve(ctx, M))) return rc;
-            // blockdiag kernel reads Phi in FP64: stage it through x_p
-            k_copy_conv<double, T><<<nb, 256, 0, st>>>(nc, x.c[dim], M.c[0].phi, 1.0);
+        } else if (bfbt) {
+            // mac_rhs keeps its zero initial value when theta_alpha = 0
+            FHD_CUDA_TRY(cudaMemsetAsync(M.c[0].rhs, 0, sizeof(T) * nc, st));
+        }
+        if (bfbt) {
+            if ((rc = visc_schur(use_phi, 0))) return rc;
+        } else {
+            if (use_phi) {
+                // blockdiag kernel reads Phi in FP64: stage it through x_p
+                k_copy_conv<double, T><<<nb, 256, 0, st>>>(nc, x.c[dim], M.c[0].phi, 1.0);
+                FHD_POST(ctx);
+            }
+            k_schur_blockdiag<<<nb, 256, 0, st>>>(nc, b.c[dim], ctx->beta, ctx->gamma, x.c[dim], theta,
+                                                  use_phi ? 1 : 0, av, pt, x.c[dim]);
             FHD_POST(ctx);
         }
-        k_schur_blockdiag<<<nb, 256, 0, st>>>(nc, b.c[dim], ctx->beta, ctx->gamma, x.c[dim], theta, use_phi ? 1 : 0,
-                                              av, pt, x.c[dim]);
-        FHD_POST(ctx);
         if ((rc = phi_to_x())) return rc;
     }
     // null space: mean of p, and of u when theta_alpha = 0 (all walls are

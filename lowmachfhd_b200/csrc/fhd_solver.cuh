@@ -183,6 +183,7 @@ struct CCLevel {
     Grid g;
     SmoothPlan plan;
     T* a[3] = {nullptr, nullptr, nullptr};
+    T* amu[3] = {nullptr, nullptr, nullptr};  // mu^-1 faces (visc_schur_approx != 0)
     T* phi = nullptr;
     T* rhs = nullptr;
     T* tmp = nullptr;
@@ -202,6 +203,8 @@ struct Multigrid {
     T* x_u[3] = {nullptr, nullptr, nullptr};
     T* b_u[3] = {nullptr, nullptr, nullptr};
     T* mac_rhs = nullptr;
+    T* bf_g[3] = {nullptr, nullptr, nullptr};  // mu^-1 G Phi_mu (visc_schur_approx != 0)
+    T* bf_phi = nullptr;                       // Phi of the alpha^-1 solve, kept across the mu solves
 };
 
 }  // namespace fhd

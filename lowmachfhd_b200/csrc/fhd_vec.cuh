@@ -245,6 +245,83 @@ static __global__ void __launch_bounds__(256) k_div_plus(Grid g, const T* u0, co
     out[f] = bp ? s + (T)bp[f] : s;
 }
 
+// mu^-1 = 1 / diagonal of the viscous operator on the faces
+// (inverse_diag_lap.f90:17-330), evaluated in FP64 in the summation order of
+// its 2D and 3D loops; visc_type 1 / 2 take the first cell's beta
+template <typename T, int DIM>
+static __global__ void __launch_bounds__(256) k_inv_diag_lap(Grid g, int visc, const double* beta, const double* be0,
+                                                      const double* be1, const double* be2, T* o0, T* o1, T* o2) {
+    Cell P;
+    if (!cell_of_thread(g, P)) return;
+    const i64 f = P.id(0, 0, 0);
+    T* out[3] = {o0, o1, o2};
+    if (visc == 1 || visc == 2) {
+        const double m = (DIM == 2 ? (visc == 1 ? 4.0 : 6.0) : (visc == 1 ? 6.0 : 8.0)) * beta[0];
+#pragma unroll
+        for (int c = 0; c < DIM; c++) out[c][f] = (T)(1.0 / m);
+        return;
+    }
+    const double cb = visc == -2 ? 2.0 : 1.0;
+    const double* be[3] = {be0, be1, be2};
+#pragma unroll
+    for (int c = 0; c < DIM; c++) {
+        double s = cb * beta[f] + cb * beta[P.id(-(c == 0), -(c == 1), -(c == 2))];
+        if constexpr (DIM == 2) {
+            // x face: node (i, j+1) then (i, j); y face: (i+1, j) then (i, j)
+            s = s + be0[c == 0 ? P.id(0, 1, 0) : P.id(1, 0, 0)];
+            s = s + be0[f];
+        } else {
+#pragma unroll
+            for (int d = 0; d < 3; d++) {
+                if (d == c) continue;
+                const int e = (c + d == 1) ? 0 : (c + d == 2) ? 1 : 2;  // xy, xz, yz
+                s = s + be[e][f];
+                s = s + be[e][P.id(d == 0, d == 1, d == 2)];
+            }
+        }
+        out[c][f] = (T)(1.0 / s);
+    }
+}
+
+// out_d = (G Phi)_d * w_d on the faces (compute_grad, div_and_grad.f90:
+// 417-703, then the face product of visc_schur_complement)
+template <typename T, int DIM>
+static __global__ void __launch_bounds__(256) k_grad_mul(Grid g, const T* Phi, const T* w0, const T* w1, const T* w2,
+                                                  T* o0, T* o1, T* o2, T dxinv) {
+    Cell P;
+    if (!cell_of_thread(g, P)) return;
+    const i64 f = P.id(0, 0, 0);
+    const T* w[3] = {w0, w1, w2};
+    T* out[3] = {o0, o1, o2};
+#pragma unroll
+    for (int d = 0; d < DIM; d++) {
+        const T gp = (Phi[f] - Phi[P.id(-(d == 0), -(d == 1), -(d == 2))]) * dxinv;
+        out[d][f] = gp * w[d][f];
+    }
+}
+
+// a_c *= w_c on the faces
+template <typename T>
+static __global__ void __launch_bounds__(256) k_mul_faces(i64 n, int ncomp, T* a0, T* a1, T* a2, const T* w0,
+                                                   const T* w1, const T* w2) {
+    T* a[3] = {a0, a1, a2};
+    const T* w[3] = {w0, w1, w2};
+    for (i64 f = blockIdx.x * (i64)blockDim.x + threadIdx.x; f < n; f += (i64)gridDim.x * blockDim.x)
+        for (int c = 0; c < ncomp; c++) a[c][f] = a[c][f] * w[c][f];
+}
+
+// x_p = Phi_mu (+ theta Phi when add), negated on request
+// (visc_schur_complement's output, apply_precon.f90:664-683)
+template <typename T>
+static __global__ void __launch_bounds__(256) k_bfbt_out(i64 n, double* xp, const T* phimu, const T* phi,
+                                                  double theta, int add, int negate) {
+    for (i64 f = blockIdx.x * (i64)blockDim.x + threadIdx.x; f < n; f += (i64)gridDim.x * blockDim.x) {
+        double v = (double)phimu[f];
+        if (add) v = v + (double)phi[f] * theta;
+        xp[f] = negate ? v * -1.0 : v;
+    }
+}
+
 // x_u = phi - w * G Phi (subtract_weighted_gradp, macproject.f90:318-362),
 // written to FP64 output (w = alphainv or 1 when null)
 template <typename T, int DIM>

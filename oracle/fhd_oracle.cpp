@@ -671,7 +671,83 @@ int apply_matrix_impl(const Geo& g, int visc, double* const b_u[], double* b_p, 
     return 0;
 }
 
-// apply_precon (apply_precon.f90:29-475), visc_schur_approx = 0
+// 1 / diagonal of the viscous operator on faces (inverse_diag_lap.f90:
+// 17-330); the same summation order as the 2D and 3D loops there
+static void inverse_diag_lap(const Geo& g, int visc, const double* beta, const double* const beta_ed[],
+                             double* const minv[]) {
+    const int dim = g.dim;
+    if (visc == 1 || visc == 2) {
+        const double b = beta[0];
+        const double m = (dim == 2 ? (visc == 1 ? 4.0 : 6.0) : (visc == 1 ? 6.0 : 8.0)) * b;
+        for (int c = 0; c < dim; c++) std::fill(minv[c], minv[c] + g.nc, 1.0 / m);
+        return;
+    }
+    const double cb = visc == -2 ? 2.0 : 1.0;
+    for (int c = 0; c < dim; c++) {
+        int e[3] = {0, 0, 0};
+        e[c] = 1;
+        forall(g, [&](int i, int j, int k) {
+            const long f = g.id(i, j, k);
+            double s = cb * beta[f] + cb * beta[g.id(i - e[0], j - e[1], k - e[2])];
+            if (dim == 2) {
+                // x face: node (i, j+1) then (i, j); y face: node (i+1, j) then (i, j)
+                s = s + beta_ed[0][c == 0 ? g.id(i, j + 1, 0) : g.id(i + 1, j, 0)];
+                s = s + beta_ed[0][f];
+            } else {
+                for (int d = 0; d < 3; d++) {
+                    if (d == c) continue;
+                    const double* be = beta_ed[edge_of(3, c, d)];
+                    s = s + be[f];
+                    s = s + be[g.id(i + (d == 0), j + (d == 1), k + (d == 2))];
+                }
+            }
+            minv[c][f] = 1.0 / s;
+        });
+    }
+}
+
+// visc_schur_complement (apply_precon.f90:538-685): the BFBt
+// approximation of the Schur complement, x_p = L_mu^-1 D mu^-1 L mu^-1 G
+// L_mu^-1 rhs (+ theta phi), L_mu the pressure Laplacian with face
+// coefficients mu^-1 = 1/diag(viscous operator); rhs is overwritten
+static int visc_schur(const Geo& g, int visc, const fhd_gmres_params* p, double* rhs, double* x_out,
+                      const double* beta, const double* const beta_ed[], double theta, const double* phi) {
+    const int dim = g.dim;
+    const long nc = g.nc;
+    std::vector<Vec> mu(dim, Vec(nc)), gp(dim, Vec(nc)), lg(dim, Vec(nc));
+    double* mup[3] = {mu[0].data(), mu[1].data(), dim == 3 ? mu[2].data() : nullptr};
+    double* gpp[3] = {gp[0].data(), gp[1].data(), dim == 3 ? gp[2].data() : nullptr};
+    double* lgp[3] = {lg[0].data(), lg[1].data(), dim == 3 ? lg[2].data() : nullptr};
+    inverse_diag_lap(g, visc, beta, beta_ed, mup);
+    const double* muc[3] = {mup[0], mup[1], mup[2]};
+    Vec phi_mu(nc, 0.0);
+    macproject_impl(g, p, phi_mu.data(), muc, rhs);
+    c_grad(g, phi_mu.data(), gpp);
+    for (int c = 0; c < dim; c++)
+        for (long f = 0; f < nc; f++) gp[c][f] = gp[c][f] * mu[c][f];
+    // stag_applyop with zero alpha: theta*0*u - L u
+    Vec zero(nc, 0.0), vb(beta, beta + nc);
+    Vec alpha0[3], bed[3];
+    for (int c = 0; c < dim; c++) alpha0[c] = zero;
+    for (int e = 0; e < n_edge(dim); e++) bed[e].assign(beta_ed[e], beta_ed[e] + nc);
+    const double* ph[3] = {gpp[0], gpp[1], gpp[2]};
+    for (int c = 0; c < dim; c++)
+        forall(g, [&](int i, int j, int k) {
+            lg[c][g.id(i, j, k)] = lface(g, visc, alpha0, vb, zero, bed, ph, c, i, j, k, nullptr);
+        });
+    for (int c = 0; c < dim; c++)
+        for (long f = 0; f < nc; f++) lg[c][f] = lg[c][f] * mu[c][f];
+    c_div(g, lgp, rhs, false);
+    std::fill(phi_mu.begin(), phi_mu.end(), 0.0);
+    macproject_impl(g, p, phi_mu.data(), muc, rhs);
+    for (long f = 0; f < nc; f++) x_out[f] = phi_mu[f];
+    if (std::fabs(theta) > 0.0)
+        for (long f = 0; f < nc; f++) x_out[f] = x_out[f] + phi[f] * theta;
+    return 0;
+}
+
+// apply_precon (apply_precon.f90:29-475); visc_schur_approx 0 (the simple
+// Schur complements) or 1 (visc_schur_complement, |visc_type| 1 and 2)
 int apply_precon_impl(const Geo& g, int visc, const fhd_gmres_params* p, const double* const b_u[],
                       const double* b_p, double* const x_u[], double* x_p, const double* const alpha_fc[],
                       const double* beta, const double* const beta_ed[], const double* gamma, double theta) {
@@ -680,7 +756,8 @@ int apply_precon_impl(const Geo& g, int visc, const fhd_gmres_params* p, const d
     const int pt = p->precon_type;
     const int apt = std::abs(pt);
     const int av = std::abs(visc);
-    if (p->visc_schur_approx != 0) return FHD_ERR_UNSUPPORTED;
+    const bool bfbt = p->visc_schur_approx != 0;
+    if (bfbt && av == 3) return FHD_ERR_UNSUPPORTED;  // inverse_diag_lap.f90: no |visc_type| = 3
     if (apt < 1 || apt > 5) return FHD_ERR_UNSUPPORTED;
     Vec phi(nc, 0.0), mac_rhs(nc, 0.0);
     std::vector<Vec> ainv(dim, Vec(nc));
@@ -726,7 +803,9 @@ int apply_precon_impl(const Geo& g, int visc, const fhd_gmres_params* p, const d
         macproject_impl(g, p, phi.data(), ainvp, mac_rhs.data());
         subtract_weighted_gradp(x_u, ainvp, phi.data());
         Vec xp(nc);
-        if (pt == 1 || theta == 0.0) {
+        if (bfbt) {
+            visc_schur(g, visc, p, mac_rhs.data(), x_p, beta, beta_ed, theta, phi.data());
+        } else if (pt == 1 || theta == 0.0) {
             for (long f = 0; f < nc; f++) xp[f] = mac_rhs[f] * -1.0;
         } else {
             // x_p = -L_alpha Phi (cc_applyop with zero cell coefficient)
@@ -737,7 +816,7 @@ int apply_precon_impl(const Geo& g, int visc, const fhd_gmres_params* p, const d
                 xp[g.id(i, j, k)] = -c_lap(g, C.a, phi.data(), i, j, k, nullptr);
             });
         }
-        for (long f = 0; f < nc; f++) {
+        for (long f = 0; f < nc && !bfbt; f++) {
             double v = xp[f];
             if (av == 1 || av == 2) {
                 v = v * beta[f];
@@ -756,7 +835,8 @@ int apply_precon_impl(const Geo& g, int visc, const fhd_gmres_params* p, const d
         c_div(g, x_u, mac_rhs.data(), false);
         for (long f = 0; f < nc; f++) mac_rhs[f] = mac_rhs[f] + b_p[f];
         if (std::fabs(theta) > 0.0) macproject_impl(g, p, phi.data(), ainvp, mac_rhs.data());
-        simple_schur();
+        if (bfbt) visc_schur(g, visc, p, mac_rhs.data(), x_p, beta, beta_ed, theta, phi.data());
+        else simple_schur();
         if (pt == -2 || pt == -5)
             for (long f = 0; f < nc; f++) x_p[f] = x_p[f] * -1.0;
         if (apt == 5) {
@@ -769,7 +849,8 @@ int apply_precon_impl(const Geo& g, int visc, const fhd_gmres_params* p, const d
     } else if (apt == 3) {
         for (long f = 0; f < nc; f++) mac_rhs[f] = (pt == -3) ? b_p[f] * -1.0 : b_p[f];
         if (std::fabs(theta) > 0.0) macproject_impl(g, p, phi.data(), ainvp, mac_rhs.data());
-        simple_schur();
+        if (bfbt) visc_schur(g, visc, p, mac_rhs.data(), x_p, beta, beta_ed, theta, phi.data());
+        else simple_schur();
         std::vector<Vec> bt(dim);
         for (int c = 0; c < dim; c++) bt[c].assign(b_u[c], b_u[c] + nc);
         double* btp[3] = {bt[0].data(), bt[1].data(), dim == 3 ? bt[2].data() : nullptr};
@@ -781,7 +862,8 @@ int apply_precon_impl(const Geo& g, int visc, const fhd_gmres_params* p, const d
             for (long f = 0; f < nc; f++) mac_rhs[f] = b_p[f];
             macproject_impl(g, p, phi.data(), ainvp, mac_rhs.data());
         }
-        for (long f = 0; f < nc; f++) {
+        if (bfbt) visc_schur(g, visc, p, mac_rhs.data(), x_p, beta, beta_ed, theta, phi.data());
+        for (long f = 0; f < nc && !bfbt; f++) {
             double ph = phi[f];
             if (std::fabs(theta) > 0.0) ph = ph * theta;
             double v = b_p[f] * beta[f];
