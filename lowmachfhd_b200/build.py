@@ -11,7 +11,10 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 SRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "_fhd_b200.so")
 SOURCES = ["fhd_solver.cu", "fhd_step.cu", "fhd_capi.cu", "fhd_noalloc.cu", "fhd_mass.cu", "fhd_server.cu",
-           "fhd_sk.cu"]
+           "fhd_sk.cu", "fhd_mass_f32.cu"]
+# translation units whose FP32 arithmetic may contract into FMA (tolerance-
+# checked, no FP64 parity path inside)
+FMA_SOURCES = {"fhd_mass_f32.cu"}
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-lineinfo", "-O3", "-std=c++17",
@@ -40,7 +43,11 @@ def build(verbose: bool = False, extra: list[str] | None = None) -> str:
     os.makedirs(objdir, exist_ok=True)
     cflags = [f for f in NVCC_FLAGS if f != "-shared"] + (extra or [])
     objs = [os.path.join(objdir, os.path.splitext(os.path.basename(p))[0] + ".o") for p in srcs]
-    cmds = [[nvcc()] + cflags + ["-c", src, "-o", obj] for src, obj in zip(srcs, objs)]
+    def flags_for(src):
+        if os.path.basename(src) in FMA_SOURCES:
+            return ["--fmad=true" if f == "--fmad=false" else f for f in cflags]
+        return cflags
+    cmds = [[nvcc()] + flags_for(src) + ["-c", src, "-o", obj] for src, obj in zip(srcs, objs)]
     if verbose:
         for c in cmds:
             print(" ".join(c), flush=True)

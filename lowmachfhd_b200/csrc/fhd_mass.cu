@@ -32,6 +32,7 @@ struct MixDev {
     float ikB_f, dV_f, tol_f;
 };
 
+#ifndef FHD_MASS_F32_TU
 MixDev make_mixdev(const fhd_mixture_params* mp, const fhd_stoch_params* sp) {
     MixDev m;
     memset(&m, 0, sizeof(m));
@@ -63,6 +64,7 @@ MixDev make_mixdev(const fhd_mixture_params* mp, const fhd_stoch_params* sp) {
     m.tol_f = (float)m.frac_tol;
     return m;
 }
+#endif
 
 // FP32 arithmetic of the mixed-precision kernels: fused multiply-adds,
 // products with the host-computed reciprocals of the constant divisors
@@ -662,7 +664,22 @@ static int mass_fluxdiv_dispatch(fhd_ctx* ctx, MassBufs& B, const MixDev& m, con
     }
 }
 
+// the FP32 instantiation lives in its own translation unit, compiled with
+// FMA contraction (fhd_mass_f32.cu); FP64 stays uncontracted for parity
+int mass_fluxdiv_f32(fhd_ctx* ctx, MassBufs& B, const MixDev& m, const double* const rho[], double dt,
+                     const double* weights, int n_rngs, const double* const W[], double* const fluxdiv[]);
+
 }  // namespace fhd
+
+#ifdef FHD_MASS_F32_TU
+namespace fhd {
+int mass_fluxdiv_f32(fhd_ctx* ctx, MassBufs& B, const MixDev& m, const double* const rho[], double dt,
+                     const double* weights, int n_rngs, const double* const W[], double* const fluxdiv[]) {
+    if (int rc = mass_alloc<float>(ctx, B, m.ns)) return rc;
+    return mass_fluxdiv_dispatch<float>(ctx, B, m, rho, dt, weights, n_rngs, W, fluxdiv);
+}
+}  // namespace fhd
+#else
 
 using namespace fhd;
 
@@ -701,10 +718,7 @@ int mass_fluxdiv(fhd_ctx* ctx, const fhd_mixture_params* mp, const fhd_stoch_par
     MassBufs& B = mass_bufs(ctx);
     const MixDev m = make_mixdev(mp, sp);
     int rc;
-    if (ctx->prec == FHD_PREC_MIXED) {
-        if ((rc = mass_alloc<float>(ctx, B, mp->nspecies))) return rc;
-        return mass_fluxdiv_dispatch<float>(ctx, B, m, rho, dt, weights, n_rngs, W, fluxdiv);
-    }
+    if (ctx->prec == FHD_PREC_MIXED) return mass_fluxdiv_f32(ctx, B, m, rho, dt, weights, n_rngs, W, fluxdiv);
     if ((rc = mass_alloc<double>(ctx, B, mp->nspecies))) return rc;
     return mass_fluxdiv_dispatch<double>(ctx, B, m, rho, dt, weights, n_rngs, W, fluxdiv);
 }
@@ -732,3 +746,4 @@ extern "C" int fhd_dev_compute_mass_fluxdiv(fhd_ctx* ctx, const fhd_mixture_para
     if (rc) return rc;
     return mass_flag_check(ctx);
 }
+#endif  // FHD_MASS_F32_TU
