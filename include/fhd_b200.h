@@ -61,7 +61,7 @@ extern "C" {
 /* ------------------------------------------------------------------ */
 typedef struct fhd_gmres_params {
     int    precon_type;            /* 1..5 and negatives */
-    int    visc_schur_approx;      /* only 0 is supported */
+    int    visc_schur_approx;      /* 0 simple Schur complements; 1 BFBt (|visc_type| 1, 2) */
     double p_norm_weight;
     double scale_factor;
     int    mg_verbose, cg_verbose;
@@ -221,7 +221,8 @@ int fhd_dev_apply_matrix(fhd_ctx* ctx,
                          double theta_alpha);
 
 /* apply_precon (apply_precon.f90:29-475): x = M^{-1} b for precon_type
- * 1..5 (visc_schur_approx = 0), including the null-space mean removal. */
+ * 1..5, including the null-space mean removal; visc_schur_approx = 1 takes
+ * the BFBt Schur complement of visc_schur_complement (538-685). */
 int fhd_dev_apply_precon(fhd_ctx* ctx,
                          const double* const b_u[], const double* b_p,
                          double* const x_u[], double* x_p,
