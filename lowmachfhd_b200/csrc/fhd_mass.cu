@@ -406,8 +406,11 @@ __global__ void __launch_bounds__(128) k_rhowchi(Grid g, MixDev m, const double*
 // per face of direction D (the low face of each cell): diffusive +
 // stochastic flux, corrected (correction_flux.f90:17-226)
 // ---------------------------------------------------------------------
+// (FP32 with up to 4 species: a 64-register cap for 8 CTAs = 32 warps per
+// SM to hide the dependent chains; 20 bytes of spills)
 template <typename T, int NS, int DIM>
-__global__ void __launch_bounds__(128) k_mass_flux(Grid g, MixDev m, int d, const double* const* __restrict__ rho,
+__global__ void __launch_bounds__(128, (sizeof(T) == 4 && NS <= 4) ? 8 : 1)
+    k_mass_flux(Grid g, MixDev m, int d, const double* const* __restrict__ rho,
                                                    const T* const* __restrict__ rwc, const T* const* __restrict__ xc,
                                                    const double* const* __restrict__ W, int n_rngs,
                                                    const double* wts, T variance, T dxinv, T* const* flux, int* flag) {
