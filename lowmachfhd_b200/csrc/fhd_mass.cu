@@ -368,7 +368,8 @@ __device__ __forceinline__ void d_choldc(T (&a)[NS][NS]) {
 // per cell: rhoWchi (compute_rhoWchi_local) and the molar concentrations
 // ---------------------------------------------------------------------
 template <typename T, int NS>
-__global__ void __launch_bounds__(128) k_rhowchi(Grid g, MixDev m, const double* const* __restrict__ rho,
+__global__ void __launch_bounds__(128, (sizeof(T) == 4 && NS <= 4) ? 8 : 1)
+    k_rhowchi(Grid g, MixDev m, const double* const* __restrict__ rho,
                                                  T* const* rwc, T* const* xo, int* flag) {
     const i64 n = g.nc;
     for (i64 f = blockIdx.x * (i64)blockDim.x + threadIdx.x; f < n; f += (i64)gridDim.x * blockDim.x) {
