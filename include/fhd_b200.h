@@ -173,7 +173,8 @@ int fhd_ctx_set_fused(fhd_ctx* ctx, int mode);
  * smooth as colour launches with one of four thread-block shapes, as the
  * tiled fused smooth with one of several tile sizes (3D), or as the row-tile
  * smooth with one of the tile heights that fit, one CTA per SM with a deep
- * copy ring or two with a short one (3D FP32 visc_type 1).  With
+ * copy ring (256 or 512 compute threads) or two with a short one (3D FP32
+ * visc_type 1).  With
  * the tuner on (mode 1 or -1 default), the first solve call that meets a
  * level shape times every candidate on scratch unknowns with the level's
  * coefficients and keeps the fastest for the process (per device,
@@ -187,18 +188,19 @@ int fhd_ctx_set_tune(fhd_ctx* ctx, int mode);
 /* Plan of staggered (which 0) or pressure (which 1) multigrid level `level`
  * after the last solve call: kind -1 fixed rules, 0 colour launches, 1 tiled
  * fused, 2 row-tile; ncand candidates considered; pair_us the measured time
- * of one smooth pair (0 when not timed); shape = {block x, block y, 0, 1}
- * for colour launches, {tile x, tile y, z-runs, CTAs per SM} for fused
- * smooths.  Any output pointer may be NULL.  No reference counterpart. */
+ * of one smooth pair (0 when not timed); shape = {block x, block y, 0, 1,
+ * threads} for colour launches, {tile x, tile y, z-runs, CTAs per SM,
+ * compute threads} for fused smooths.  Any output pointer may be NULL.  No
+ * reference counterpart. */
 int fhd_ctx_tune_info(fhd_ctx* ctx, int which, int level, int* kind, int* ncand, double* pair_us,
-                      int shape[4]);
+                      int shape[5]);
 /* The candidate list the tuner would time for one level (host only, no
  * device): staggered (which 0) or pressure (1) multigrid, extents, precision
  * mode, visc_type, and the device's SM count and shared-memory limits (per
- * block opt-in, per SM).  Writes up to max_out records of 6 ints {kind,
+ * block opt-in, per SM).  Writes up to max_out records of 7 ints {kind,
  * block x | tile x | nx, block y | tile y, z-runs, CTAs per SM, row-tile
- * shared-memory bytes} and returns the number of candidates.  No reference
- * counterpart. */
+ * shared-memory bytes, threads} and returns the number of candidates.  No
+ * reference counterpart. */
 int fhd_tune_candidates(int which, int dim, const int n_cells[3], int precision_mode, int visc_type, int sms,
                         int smem_optin, int smem_sm, int* out, int max_out);
 /* Number of this library's kernels launched through ctx so far. */

@@ -131,7 +131,7 @@ class StokesSolver:
         0 colour launches, 1 tiled fused, 2 row-tile), candidates considered,
         measured time of a smooth pair, block or tile shape"""
         kind, nc, us = C.c_int(0), C.c_int(0), C.c_double(0)
-        shape = (C.c_int * 4)()
+        shape = (C.c_int * 5)()
         check(lib().fhd_ctx_tune_info(self._h, 0 if which == "stag" else 1, int(level), C.byref(kind),
                                       C.byref(nc), C.byref(us), shape), "fhd_ctx_tune_info")
         names = {-1: "rules", 0: "colour", 1: "tiled", 2: "rowtile"}
@@ -422,12 +422,12 @@ def tune_candidates(which: str, dim: int, n_cells, precision: str = "mixed", vis
     only); defaults: the B200's 148 SMs and shared-memory limits"""
     n = (C.c_int * 3)(*(list(n_cells) + [1] * (3 - len(n_cells))))
     prec = FHD_PREC_MIXED if precision == "mixed" else FHD_PREC_FP64
-    out = (C.c_int * (6 * 64))()
+    out = (C.c_int * (7 * 64))()
     k = check(lib().fhd_tune_candidates(0 if which == "stag" else 1, int(dim), n, prec, int(visc_type), int(sms),
                                         int(smem_optin), int(smem_sm), out, 64), "fhd_tune_candidates")
     names = {0: "colour", 1: "tiled", 2: "rowtile"}
-    return [dict(kind=names[out[6 * i]], x=out[6 * i + 1], y=out[6 * i + 2], zruns=out[6 * i + 3],
-                 per_sm=out[6 * i + 4], smem=out[6 * i + 5]) for i in range(min(k, 64))]
+    return [dict(kind=names[out[7 * i]], x=out[7 * i + 1], y=out[7 * i + 2], zruns=out[7 * i + 3],
+                 per_sm=out[7 * i + 4], smem=out[7 * i + 5], threads=out[7 * i + 6]) for i in range(min(k, 64))]
 
 
 class StructureFactor:

@@ -52,6 +52,7 @@ struct RBXGeom {
     size_t smem;  // bytes of dynamic shared memory
     int ahead;    // stages in flight beyond the one awaited
     int per_sm;   // resident CTAs per SM the z-run split assumes
+    int threads;  // compute threads (256 or 512)
 };
 
 struct RBGeom {

@@ -29,7 +29,7 @@
 
 namespace fhd {
 
-constexpr int RBX_THREADS = 256;  // compute threads
+constexpr int RBX_THREADS = 256;  // compute threads (the wide form: 512)
 // stages in flight beyond the one awaited (the rings then hold unknown
 // planes k-1 .. k+3 and coefficient planes k .. k+2 plus these)
 constexpr int RBX_AHEAD = 3;
@@ -42,21 +42,24 @@ constexpr int RBX_ROWSTEP = 2 * RBX_THREADS;
 constexpr int RBX_MAXR = 5;
 // the block: RBX_THREADS compute threads and one producer warp
 constexpr int RBX_BLOCK = RBX_THREADS + 32;
+// rows per thread and sweep for nt compute threads: 5 with 256, 3 with 512
+// (twice the warps to hide the update chains, each taking fewer rows)
+constexpr int rbx_maxr(int nt) { return nt == 256 ? 5 : 3; }
 // Every thread evaluates RBX_MAXR rows per sweep and stores only those of
 // the tile.  The reads of the others stay below RBX_MAXR * RBX_ROWSTEP +
 // 2 nx elements from the start of an unknown plane slot and below
 // RBX_MAXR * RBX_ROWSTEP from the start of a coefficient slot; shared memory
 // holds the coefficient ring, then the unknown ring, then a pad that covers
 // the last unknown slot's overrun.
-inline int rbx_pad(int nx, int rows) {
-    const int over = RBX_MAXR * RBX_ROWSTEP + 2 * nx - rows * nx;
+inline int rbx_pad(int nx, int rows, int nt = RBX_THREADS) {
+    const int over = rbx_maxr(nt) * 2 * nt + 2 * nx - rows * nx;
     return (over > 0 ? over : 0) + 32;
 }
 // ahead: stages in flight beyond the one awaited (RBX_AHEAD, or 1 for the
-// variant that fits two CTAs on an SM)
-inline size_t rbx_smem_bytes(int nx, int ty, int ahead = RBX_AHEAD) {
+// variant that fits two CTAs on an SM); nt: compute threads
+inline size_t rbx_smem_bytes(int nx, int ty, int ahead = RBX_AHEAD, int nt = RBX_THREADS) {
     return 64 + sizeof(float) * ((size_t)(3 + ahead) * 2 * (ty + 2) * nx + (size_t)(5 + ahead) * (ty + 4) * nx +
-                                 rbx_pad(nx, ty + 4));
+                                 rbx_pad(nx, ty + 4, nt));
 }
 
 // ---------------------------------------------------------------------
@@ -120,11 +123,13 @@ struct RBXArgs {
     unsigned* err;
 };
 
-template <int C, int AH>
+template <int C, int AH, int NT>
 __device__ __forceinline__ void rbx_run(const Grid& g, const RBXGeom& G, const StagOp<float>& A, const RBXArgs& R,
                                         float omega, unsigned char* raw, int tile_y, int chunk) {
     constexpr int NPH = 5 + AH;  // unknown planes k-1 .. k+3 + in flight
     constexpr int NCF = 3 + AH;  // coefficient planes k .. k+2 + in flight
+    constexpr int MR = rbx_maxr(NT);  // rows per thread and red sweep
+    constexpr int ROWSTEP = 2 * NT;   // elements between a thread's rows
     const int nx = g.n[0], ny = g.n[1], nz = g.n[2];
     const int TY = G.TY, rows = G.rows, crows = G.crows;
     const int tid = threadIdx.x;
@@ -148,7 +153,7 @@ __device__ __forceinline__ void rbx_run(const Grid& g, const RBXGeom& G, const S
     // except across the periodic y wrap, so each array goes as one to three
     // contiguous copies.
     auto issue = [&](int q) {
-        const int lane = tid - RBX_THREADS;
+        const int lane = tid - NT;
         const int j = q + k0 - 2;
         const int s = q % NPH;
         if (lane == 0) mbar_expect_tx(&bar[s], (unsigned)(sizeof(float) * (plane + (j >= k0 ? 2 * cplane : 0))));
@@ -173,7 +178,7 @@ __device__ __forceinline__ void rbx_run(const Grid& g, const RBXGeom& G, const S
     auto wait_stage = [&](int q) { return mbar_wait_bounded(&bar[q % NPH], (unsigned)((q / NPH) & 1)); };
 
     const int hx = nx >> 1;           // cells of one colour per row
-    const int RG = RBX_THREADS / hx;  // rows updated at once
+    const int RG = NT / hx;  // rows updated at once
     // a warp takes 16 cells of a colour on each of two adjacent rows: their
     // colour offsets differ by one, so the two half-warps read the even and
     // the odd banks and every shared access is one wavefront
@@ -211,7 +216,7 @@ __device__ __forceinline__ void rbx_run(const Grid& g, const RBXGeom& G, const S
         float nv[NR];
 #pragma unroll
         for (int m = 0; m < NR; m++) {
-            const int r = m * RBX_ROWSTEP;
+            const int r = m * ROWSTEP;
             const float* c = c0 + r;
             float dg;
             const float L = stag_lface_acc<float, 3, 1, C>(
@@ -230,18 +235,18 @@ __device__ __forceinline__ void rbx_run(const Grid& g, const RBXGeom& G, const S
         }
 #pragma unroll
         for (int m = 0; m < NR; m++)
-            if (lyb + m * RG < ly1) c0[m * RBX_ROWSTEP + lx] = nv[m];
+            if (lyb + m * RG < ly1) c0[m * ROWSTEP + lx] = nv[m];
     };
     // prologue: stages q = 0 .. 4 (unknown planes k0-2 .. k0+2, coefficient
     // planes k0-1 .. k0+1) and AHEAD more
-    const bool producer = tid >= RBX_THREADS;
-    const int lead = RBX_THREADS;  // producer lane 0: stores and clean-up
+    const bool producer = tid >= NT;
+    const int lead = NT;  // producer lane 0: stores and clean-up
     if (producer) {
         for (int q = 0; q < 5 + AH && q <= qend; q++) issue(q);
         issued = 5 + AH < qend + 1 ? 5 + AH : qend + 1;
     }
-    using RRed = std::integral_constant<int, RBX_MAXR>;
-    using RBlack = std::integral_constant<int, RBX_MAXR - 1>;
+    using RRed = std::integral_constant<int, MR>;
+    using RBlack = std::integral_constant<int, MR - 1>;
     auto slot = [&](int p) { return pmod(p - (k0 - 2), NPH); };
     auto ring = [](int v, int d, int n) { return v + d >= n ? v + d - n : v + d; };
     int sl, scl;
@@ -312,17 +317,18 @@ fail:
 
 // AH stages in flight beyond the one awaited: RBX_AHEAD with one CTA per SM,
 // or 1 with two (smaller rings, half the shared memory)
-template <int AH>
-__global__ void __launch_bounds__(RBX_BLOCK, AH == 1 ? 2 : 1) k_stag_rbx(Grid g, RBXGeom G, StagOp<float> A,
-                                                                         RBXArgs R, float omega) {
+// NT compute threads (256, or 512 in the wide form) and one producer warp
+template <int AH, int NT = RBX_THREADS>
+__global__ void __launch_bounds__(NT + 32, AH == 1 ? 2 : 1) k_stag_rbx(Grid g, RBXGeom G, StagOp<float> A,
+                                                                       RBXArgs R, float omega) {
     extern __shared__ __align__(128) unsigned char rbx_raw[];
     if (threadIdx.x < 5 + AH) mbar_init(reinterpret_cast<unsigned long long*>(rbx_raw) + threadIdx.x, 1);
     if (threadIdx.x == 0) mbar_init_fence();
     __syncthreads();
     const int tile_y = blockIdx.x, chunk = blockIdx.y;
-    if (blockIdx.z == 0) rbx_run<0, AH>(g, G, A, R, omega, rbx_raw, tile_y, chunk);
-    else if (blockIdx.z == 1) rbx_run<1, AH>(g, G, A, R, omega, rbx_raw, tile_y, chunk);
-    else rbx_run<2, AH>(g, G, A, R, omega, rbx_raw, tile_y, chunk);
+    if (blockIdx.z == 0) rbx_run<0, AH, NT>(g, G, A, R, omega, rbx_raw, tile_y, chunk);
+    else if (blockIdx.z == 1) rbx_run<1, AH, NT>(g, G, A, R, omega, rbx_raw, tile_y, chunk);
+    else rbx_run<2, AH, NT>(g, G, A, R, omega, rbx_raw, tile_y, chunk);
 }
 
 // geometry for a level (sms: multiprocessors of the device); false when the
@@ -330,20 +336,24 @@ __global__ void __launch_bounds__(RBX_BLOCK, AH == 1 ? 2 : 1) k_stag_rbx(Grid g,
 // autotuner's candidates), 0 for the tallest that fits.
 // ahead: RBX_AHEAD, or 1 for two CTAs per SM where smem_sm (shared memory
 // of one SM) holds two.
+// nt: compute threads, 256 or (with the deep ring) 512.
 inline bool rbx_geom(const Grid& g, int sms, size_t smem_max, RBXGeom& G, int ty_req = 0, int ahead = RBX_AHEAD,
-                     size_t smem_sm = 0) {
+                     size_t smem_sm = 0, int nt = RBX_THREADS) {
     if (ahead != RBX_AHEAD && ahead != 1) return false;
+    if (nt != RBX_THREADS && !(nt == 512 && ahead == RBX_AHEAD)) return false;
+    const int MR = rbx_maxr(nt);
     G.ahead = ahead;
+    G.threads = nt;
     if (g.dim != 3) return false;
     const int nx = g.n[0], ny = g.n[1], nz = g.n[2];
     if (nx > RBX_MAXNX || nx < 64 || (nx & (nx - 1)) || (ny & 1) || (nz & 1) || nz < 4) return false;
     const int hx = nx / 2;
-    if (RBX_THREADS % hx || hx % 16 || (RBX_THREADS / 32) % (hx / 16)) return false;
+    if (nt % hx || hx % 16 || (nt / 32) % (hx / 16)) return false;
     // tallest tile that fits the shared memory of one CTA per SM
     G.TY = 0;
     for (int ty = 32; ty >= 4; ty /= 2) {
         if (ny % ty || (ty_req > 0 && ty != ty_req)) continue;
-        const size_t smem = rbx_smem_bytes(nx, ty, ahead);
+        const size_t smem = rbx_smem_bytes(nx, ty, ahead, nt);
         if (smem <= smem_max) {
             G.TY = ty;
             G.smem = smem;
@@ -351,11 +361,12 @@ inline bool rbx_geom(const Grid& g, int sms, size_t smem_max, RBXGeom& G, int ty
         }
     }
     if (!G.TY) return false;
-    // rows per thread and sweep (ring rows included) within RBX_MAXR
-    const int RG = RBX_THREADS / hx;
-    while (ty_req == 0 && G.TY > 4 && (G.TY + 2 + RG - 1) / RG > RBX_MAXR) G.TY /= 2;
-    if ((G.TY + 2 + RG - 1) / RG > RBX_MAXR || (G.TY + RG - 1) / RG > RBX_MAXR - 1 || ny % G.TY) return false;
-    G.smem = rbx_smem_bytes(nx, G.TY, ahead);
+    // rows per thread and sweep (ring rows included) within MR
+    const int RG = nt / hx;
+    while (ty_req == 0 && G.TY > 4 && (G.TY + 2 + RG - 1) / RG > MR) G.TY /= 2;
+    if ((G.TY + 2 + RG - 1) / RG > MR || (G.TY + RG - 1) / RG > MR - 1 || ny % G.TY) return false;
+    G.smem = rbx_smem_bytes(nx, G.TY, ahead, nt);
+    if (G.smem > smem_max) return false;
     // resident CTAs per SM (1 KB of each CTA's shared memory is reserved)
     G.per_sm = (ahead == 1 && 2 * (G.smem + 1024) <= smem_sm) ? 2 : 1;
     if (ahead == 1 && G.per_sm == 1) return false;  // the short ring pays only with two CTAs

@@ -510,6 +510,10 @@ static int stag_rbx_smooth(fhd_ctx* ctx, StagLevel<float>& L, const RBXGeom& G, 
     if (G.ahead == 1) {
         if (int rc = rb_allow_smem(k_stag_rbx<1>, G.smem, true)) return rc;
         k_stag_rbx<1><<<grd, RBX_BLOCK, G.smem, ctx->stream>>>(L.g, G, L.op(), R, (float)ctx->p.stag_mg_omega);
+    } else if (G.threads == 512) {
+        if (int rc = rb_allow_smem(k_stag_rbx<RBX_AHEAD, 512>, G.smem)) return rc;
+        k_stag_rbx<RBX_AHEAD, 512><<<grd, 512 + 32, G.smem, ctx->stream>>>(L.g, G, L.op(), R,
+                                                                          (float)ctx->p.stag_mg_omega);
     } else {
         if (int rc = rb_allow_smem(k_stag_rbx<RBX_AHEAD>, G.smem)) return rc;
         k_stag_rbx<RBX_AHEAD><<<grd, RBX_BLOCK, G.smem, ctx->stream>>>(L.g, G, L.op(), R,
@@ -971,10 +975,12 @@ static std::vector<SmoothPlan> stag_cands(fhd_ctx* ctx, const StagLevel<T>& L) {
     colour_cands(v, L.g);
     rb_cands(v, L.g, 3, (int)sizeof(T), 2, ctx->smem_optin);
     if (std::is_same<T, float>::value && ctx->visc == 1)
-        for (int ahead : {RBX_AHEAD, 1})
+        for (int form = 0; form < 3; form++)  // deep ring; short ring, two CTAs per SM; deep ring, 512 threads
             for (int ty = 4; ty <= 32; ty *= 2) {
                 RBXGeom X;
-                if (!rbx_geom(L.g, ctx->sms, (size_t)ctx->smem_optin, X, ty, ahead, (size_t)ctx->smem_sm)) continue;
+                const int ahead = form == 1 ? 1 : RBX_AHEAD, nt = form == 2 ? 512 : RBX_THREADS;
+                if (!rbx_geom(L.g, ctx->sms, (size_t)ctx->smem_optin, X, ty, ahead, (size_t)ctx->smem_sm, nt))
+                    continue;
                 SmoothPlan p;
                 p.kind = 2;
                 p.rbx = X;
@@ -2131,18 +2137,19 @@ int fhd_tune_candidates(int which, int dim, const int n_cells[3], int precision_
     }
     for (int i = 0; i < (int)v.size() && i < max_out; i++) {
         const SmoothPlan& P = v[i];
-        int* o = out + 6 * i;
+        int* o = out + 7 * i;
         o[0] = P.kind;
         o[1] = P.kind == 0 ? P.bx : P.kind == 1 ? P.rb.TX : g.n[0];
         o[2] = P.kind == 0 ? P.by : P.kind == 1 ? P.rb.TY : P.rbx.TY;
         o[3] = P.kind == 1 ? P.rb.chunks : P.kind == 2 ? P.rbx.chunks : 0;
         o[4] = P.kind == 2 ? P.rbx.per_sm : 1;
         o[5] = P.kind == 2 ? (int)P.rbx.smem : 0;
+        o[6] = P.kind == 0 ? P.bx * P.by : P.kind == 1 ? P.rb.threads : P.rbx.threads;
     }
     return (int)v.size();
 }
 
-int fhd_ctx_tune_info(fhd_ctx* c, int which, int level, int* kind, int* ncand, double* pair_us, int shape[4]) {
+int fhd_ctx_tune_info(fhd_ctx* c, int which, int level, int* kind, int* ncand, double* pair_us, int shape[5]) {
     if (!c || (which != 0 && which != 1) || level < 0) return FHD_ERR_BAD_ARG;
     const SmoothPlan* P = nullptr;
     if (c->prec == FHD_PREC_MIXED) {
@@ -2161,6 +2168,7 @@ int fhd_ctx_tune_info(fhd_ctx* c, int which, int level, int* kind, int* ncand, d
         shape[1] = P->kind == 0 ? P->by : P->kind == 1 ? P->rb.TY : P->kind == 2 ? P->rbx.TY : 0;
         shape[2] = P->kind == 1 ? P->rb.chunks : P->kind == 2 ? P->rbx.chunks : 0;
         shape[3] = P->kind == 2 ? P->rbx.per_sm : P->kind >= 0 ? 1 : 0;
+        shape[4] = P->kind == 0 ? P->bx * P->by : P->kind == 1 ? P->rb.threads : P->kind == 2 ? P->rbx.threads : 0;
     }
     return FHD_OK;
 }

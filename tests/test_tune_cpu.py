@@ -17,12 +17,14 @@ def test_fp32_visc1_large_level_has_every_kind():
     c = L.tune_candidates("stag", 3, [256, 256, 256], "mixed", 1)
     assert kinds(c) == {"colour", "tiled", "rowtile"}
     rows = [x for x in c if x["kind"] == "rowtile"]
-    # one CTA per SM with the deep ring for 4- and 8-row tiles; the short
-    # ring only where two CTAs fit on one SM
-    assert {(x["y"], x["per_sm"]) for x in rows} == {(4, 1), (8, 1), (4, 2)}
+    # one CTA per SM with the deep ring for 4- and 8-row tiles (256 or 512
+    # compute threads); the short ring only where two CTAs fit on one SM
+    assert {(x["y"], x["per_sm"], x["threads"]) for x in rows} == {(4, 1, 256), (8, 1, 256), (4, 2, 256),
+                                                                  (4, 1, 512), (8, 1, 512)}
     for x in rows:
         assert 256 % x["y"] == 0 and x["zruns"] >= 1
         assert x["per_sm"] * (x["smem"] + 1024) <= SMEM_SM
+        assert x["smem"] <= 232448
     for x in c:
         if x["kind"] == "tiled":
             assert 256 % x["x"] == 0 and x["x"] % 4 == 0 and x["x"] <= 64
