@@ -64,6 +64,9 @@ def parse():
     ap.add_argument("--probe", choices=["stagmg"], default=None,
                     help="profiling probe: K stag_mg_solver calls (one V-cycle each) on one grid")
     ap.add_argument("--precision", choices=["mixed", "fp64"], default="fp64", help="precision of --probe")
+    ap.add_argument("--tune", type=int, default=-1,
+                    help="smoother autotuner mode of --probe (fhd_ctx_set_tune: -1 tune, 0 fixed rules, 2+k "
+                         "candidate k on every level)")
     return ap.parse_args()
 
 
@@ -78,6 +81,7 @@ def run_probe(args):
     nc = n ** 3
     s = L.StokesSolver(3, [n, n, n], 1.0, 1, params=L.default_params(gmres_max_inner=1),
                        precision=args.precision)
+    s.set_tune(args.tune)
     g = torch.Generator().manual_seed(3)
     f64 = dict(dtype=torch.float64)
     alpha = [(1.0 + 1e-3 * torch.randn(nc, generator=g, **f64)).to(dev) for _ in range(3)]
