@@ -203,6 +203,19 @@ int fhd_ctx_tune_info(fhd_ctx* ctx, int which, int level, int* kind, int* ncand,
  * reference counterpart. */
 int fhd_tune_candidates(int which, int dim, const int n_cells[3], int precision_mode, int visc_type, int sms,
                         int smem_optin, int smem_sm, int* out, int max_out);
+/* The autotuner's table as text, so that a long-running host (a server)
+ * can start with the plans an earlier process measured: one line per level
+ * shape, "<key> <candidate index>", the key naming device, multigrid,
+ * element size, dimension, visc_type and extents.  export writes the table
+ * (measured and imported plans) into buf (len bytes, NUL-terminated,
+ * truncated if short) and returns the bytes the whole text needs; import
+ * reads such text, returns the number of lines taken, or FHD_ERR_BAD_ARG
+ * (nothing taken) on a malformed line.  An imported choice is used, untimed,
+ * by the first solve that meets its shape; an index beyond that level's
+ * candidate list is ignored and the level is timed.  No reference
+ * counterpart. */
+long long fhd_tune_export(char* buf, long long len);
+int fhd_tune_import(const char* text);
 /* Number of this library's kernels launched through ctx so far. */
 long long fhd_ctx_kernel_launches(fhd_ctx* ctx);
 const char* fhd_status_string(int status);

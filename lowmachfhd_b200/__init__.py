@@ -23,7 +23,7 @@ from ._capi import (FHD_PREC_FP64, FHD_PREC_MIXED, FHD_REQ_INERTIAL, FHD_REQ_OVE
                     mixture_params)
 
 __all__ = ["StokesSolver", "GmresParams", "StochParams", "SolveStats", "MixtureParams", "mixture_params",
-           "Server", "StructureFactor", "tune_candidates", "Request", "RequestResult", "make_request", "fill_normal", "philox4x32_10", "sched_simulate",
+           "Server", "StructureFactor", "tune_candidates", "tune_export", "tune_import", "Request", "RequestResult", "make_request", "fill_normal", "philox4x32_10", "sched_simulate",
            "FHD_REQ_OVERDAMPED", "FHD_REQ_INERTIAL",
            "default_params", "FhdError",
            "FHD_PREC_FP64", "FHD_PREC_MIXED", "lib", "fab_from_canonical", "canonical_from_fab", "FabArray"]
@@ -428,6 +428,19 @@ def tune_candidates(which: str, dim: int, n_cells, precision: str = "mixed", vis
     names = {0: "colour", 1: "tiled", 2: "rowtile"}
     return [dict(kind=names[out[7 * i]], x=out[7 * i + 1], y=out[7 * i + 2], zruns=out[7 * i + 3],
                  per_sm=out[7 * i + 4], smem=out[7 * i + 5], threads=out[7 * i + 6]) for i in range(min(k, 64))]
+
+
+def tune_export() -> str:
+    """the autotuner's table as text (fhd_tune_export)"""
+    need = int(lib().fhd_tune_export(None, 0))
+    buf = C.create_string_buffer(need)
+    lib().fhd_tune_export(buf, need)
+    return buf.value.decode()
+
+
+def tune_import(text: str) -> int:
+    """add plans from text written by tune_export (fhd_tune_import)"""
+    return check(lib().fhd_tune_import(text.encode()), "fhd_tune_import")
 
 
 class StructureFactor:

@@ -144,6 +144,8 @@ _PROTOS = {
     "fhd_ctx_set_coarse": (C.c_int, [_VP, C.c_int]),
     "fhd_ctx_set_fused": (C.c_int, [_VP, C.c_int]),
     "fhd_ctx_set_tune": (C.c_int, [_VP, C.c_int]),
+    "fhd_tune_export": (C.c_longlong, [C.c_char_p, C.c_longlong]),
+    "fhd_tune_import": (C.c_int, [C.c_char_p]),
     "fhd_tune_candidates": (C.c_int, [C.c_int, C.c_int, C.POINTER(C.c_int), C.c_int, C.c_int, C.c_int, C.c_int,
                                       C.c_int, C.POINTER(C.c_int), C.c_int]),
     "fhd_sk_create": (C.c_int, [C.c_int, C.POINTER(C.c_int), C.c_double, C.c_int, C.POINTER(C.c_int), C.c_int,

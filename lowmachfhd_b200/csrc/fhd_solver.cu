@@ -6,6 +6,7 @@
 // apply_matrix.f90, apply_precon.f90, stag_mg_solver.f90, macproject.f90.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <type_traits>
@@ -925,6 +926,7 @@ constexpr int TUNE_REPS = 3;  // timed smooth pairs per candidate (after one unt
 
 static std::mutex g_tune_mu;  // held while a context tunes
 static std::map<std::string, SmoothPlan> g_tune;
+static std::map<std::string, int> g_tune_import;  // imported choices (candidate index) not yet used
 
 static std::string tune_key(fhd_ctx* ctx, const Grid& g, int which, int elem) {
     int dev = 0;
@@ -1046,6 +1048,14 @@ static int tune_levels_locked(fhd_ctx* ctx, Multigrid<T>& M, std::vector<T*>& sc
             L.plan.ncand = (int)cands.size();
             continue;
         }
+        auto im = g_tune_import.find(key);
+        if (im != g_tune_import.end() && im->second < (int)cands.size()) {
+            L.plan = cands[im->second];
+            L.plan.ncand = (int)cands.size();
+            L.plan.index = im->second;
+            g_tune[key] = L.plan;
+            continue;
+        }
         if (int rc = get_scratch(nc_max)) return rc;
         StagLevel<T> S = L;  // scratch unknowns, the level's coefficients
         for (int c = 0; c < dim; c++) {
@@ -1065,6 +1075,7 @@ static int tune_levels_locked(fhd_ctx* ctx, Multigrid<T>& M, std::vector<T*>& sc
         }
         L.plan = cands[best];
         L.plan.ncand = (int)cands.size();
+        L.plan.index = best;
         g_tune[key] = L.plan;
     }
     for (int l = 0; l < (int)M.c.size(); l++) {
@@ -1081,6 +1092,14 @@ static int tune_levels_locked(fhd_ctx* ctx, Multigrid<T>& M, std::vector<T*>& sc
         if (force >= 0) {
             C.plan = cands[(size_t)force < cands.size() ? force : 0];
             C.plan.ncand = (int)cands.size();
+            continue;
+        }
+        auto im = g_tune_import.find(key);
+        if (im != g_tune_import.end() && im->second < (int)cands.size()) {
+            C.plan = cands[im->second];
+            C.plan.ncand = (int)cands.size();
+            C.plan.index = im->second;
+            g_tune[key] = C.plan;
             continue;
         }
         if (int rc = get_scratch(nc_max)) return rc;
@@ -1101,6 +1120,7 @@ static int tune_levels_locked(fhd_ctx* ctx, Multigrid<T>& M, std::vector<T*>& sc
         }
         C.plan = cands[best];
         C.plan.ncand = (int)cands.size();
+        C.plan.index = best;
         g_tune[key] = C.plan;
     }
     return 0;
@@ -2096,6 +2116,52 @@ int fhd_ctx_set_tune(fhd_ctx* c, int mode) {
     release_graphs(c);
     c->tune_mode = mode;
     return FHD_OK;
+}
+
+long long fhd_tune_export(char* buf, long long len) {
+    std::string out;
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        std::map<std::string, int> all = g_tune_import;
+        for (const auto& kv : g_tune)
+            if (kv.second.index >= 0) all[kv.first] = kv.second.index;
+        for (const auto& kv : all) out += kv.first + " " + std::to_string(kv.second) + "\n";
+    }
+    const long long need = (long long)out.size() + 1;
+    if (buf && len > 0) {
+        const long long n = need <= len ? need - 1 : len - 1;
+        memcpy(buf, out.data(), (size_t)n);
+        buf[n] = '\0';
+    }
+    return need;
+}
+
+int fhd_tune_import(const char* text) {
+    if (!text) return FHD_ERR_BAD_ARG;
+    std::map<std::string, int> got;
+    const char* p = text;
+    while (*p) {
+        const char* e = strchr(p, '\n');
+        const std::string line(p, e ? (size_t)(e - p) : strlen(p));
+        p = e ? e + 1 : p + line.size();
+        if (line.empty()) continue;
+        const size_t sp = line.find(' ');
+        if (sp == std::string::npos || sp == 0 || line.find(' ', sp + 1) != std::string::npos)
+            return FHD_ERR_BAD_ARG;
+        const std::string key = line.substr(0, sp), num = line.substr(sp + 1);
+        if (num.empty() || num.size() > 4 || num.find_first_not_of("0123456789") != std::string::npos)
+            return FHD_ERR_BAD_ARG;
+        // device:which:element size:dim:visc_type:extents, as the tuner writes them
+        int dev, elem, dim, visc, n0, n1, n2;
+        char which;
+        if (sscanf(key.c_str(), "%d:%c:%d:%d:%d:%dx%dx%d", &dev, &which, &elem, &dim, &visc, &n0, &n1, &n2) != 8 ||
+            (which != 's' && which != 'c') || (elem != 4 && elem != 8) || (dim != 2 && dim != 3))
+            return FHD_ERR_BAD_ARG;
+        got[key] = atoi(num.c_str());
+    }
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    for (const auto& kv : got) g_tune_import[kv.first] = kv.second;
+    return (int)got.size();
 }
 
 int fhd_tune_candidates(int which, int dim, const int n_cells[3], int precision_mode, int visc_type, int sms,

@@ -148,6 +148,7 @@ struct SmoothPlan {
     RBXGeom rbx;          // kind 2
     float us = 0.f;       // measured time of one smooth pair
     int ncand = 0;        // candidates the tuner considered
+    int index = -1;       // position of this plan in the level's candidate list
 };
 
 template <typename T>

@@ -76,3 +76,20 @@ def test_tuned_plan_is_timed_cached_and_equal(cuda, dim, n, visc, precision):
     assert info1 == info2
     assert _agree(out1, ref, precision)
     assert _agree(out2, out1, "fp64")
+
+
+def test_imported_plan_is_used_untimed(cuda):
+    """a plan imported as text (fhd_tune_import) is taken, untimed, by the
+    first solve of its shape, and gives the rules' result"""
+    dim, n, visc, precision = 3, [64, 64, 32], 1, "mixed"  # a shape no other test tunes
+    cands = L.tune_candidates("stag", dim, n, precision, visc)
+    idx = next(i for i, c in enumerate(cands) if c["kind"] == "tiled")
+    line = f"0:s:4:3:1:64x64x32 {idx}"
+    assert L.tune_import(line + "\n") == 1
+    ref, _ = _run(cuda, dim, n, visc, precision, 0)
+    out, info = _run(cuda, dim, n, visc, precision, -1)
+    st = info[0]
+    assert st["kind"] == "tiled" and st["pair_us"] == 0 and st["candidates"] == len(cands)
+    assert st["shape"][:2] == [cands[idx]["x"], cands[idx]["y"]]
+    assert _agree(out, ref, precision)
+    assert line in L.tune_export().splitlines()

@@ -73,3 +73,24 @@ def test_bad_arguments():
         L.tune_candidates("stag", 4, [8, 8, 8])
     with pytest.raises(L.FhdError):
         L.tune_candidates("stag", 3, [1, 8, 8])
+
+
+def test_table_import_export_roundtrip():
+    text = "0:s:4:3:1:96x96x96 11\n0:c:4:3:0:96x96x96 2\n"
+    assert L.tune_import(text) == 2
+    out = L.tune_export()
+    for line in text.splitlines():
+        assert line in out.splitlines()
+    # re-importing replaces, and an empty text adds nothing
+    assert L.tune_import("0:s:4:3:1:96x96x96 3\n") == 1
+    assert "0:s:4:3:1:96x96x96 3" in L.tune_export().splitlines()
+    assert L.tune_import("") == 0
+
+
+@pytest.mark.parametrize("bad", ["0:s:4:3:1:96x96x96\n", "nonsense 1\n", "0:s:4:3:1:96x96x96 x\n",
+                                 "0:q:4:3:1:96x96x96 1\n", "0:s:4:3:1:96x96x96 1 2\n"])
+def test_table_import_rejects_malformed_lines(bad):
+    before = L.tune_export()
+    with pytest.raises(L.FhdError):
+        L.tune_import("0:s:4:3:1:40x40x40 1\n" + bad)
+    assert L.tune_export() == before
