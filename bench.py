@@ -306,23 +306,61 @@ class Clocks:
 # ----------------------------------------------------------------------
 # problem set-up (seeded synthetic inputs; no dataset involved)
 # ----------------------------------------------------------------------
-def host_fields(n, seed, torch):
-    """one step's N(0,1) random fields, pinned host float64: the momentum
-    fields as fill_m_stochastic prepares them (symmetric form: cell entries
-    with variance 2, the two edge components equal) and the mass-flux face
-    fields of fill_mass_stochastic (3 directions x 4 species)"""
-    g = torch.Generator().manual_seed(seed)
+NOISE_SEED = 20261204
+
+
+def neighbour_shifts(n):
+    """offsets, modulo the n^3 field size, from a cell to its periodic
+    neighbours (shifts of -1, 0, 1 in x, y and z) and to itself"""
     nc = n ** 3
-    W_cc = [torch.randn(nc, generator=g, dtype=torch.float64).mul_(2.0 ** 0.5).pin_memory() for _ in range(3)]
-    W_ed = []
-    for _ in range(3):
-        a = torch.randn(nc, generator=g, dtype=torch.float64).pin_memory()
-        W_ed += [a, a]
-    W_m = [torch.randn(nc, generator=g, dtype=torch.float64).pin_memory() for _ in range(3 * NSPECIES)]
-    return W_cc, W_ed, W_m
+    sh = {0, 1, -1, n - 1, 1 - n}
+    return {(a + n * b + n * n * c) % nc for a in sh for b in sh for c in sh}
+
+
+def pool_stride(n, steps):
+    """Stride between steps in the end-to-end leg's host noise pools: step i
+    reads field f from the window starting at f*nc + i*stride.  Two windows
+    of different steps i, j differ in offset, modulo nc, by (i - j)*stride;
+    the stride is the first odd multiple of 512 (4 KiB-aligned windows) near
+    nc/16 for which no step difference up to `steps` gives zero or a
+    neighbour's offset, so no cell or neighbour sees a pool element twice."""
+    nc = n ** 3
+    near = neighbour_shifts(n)
+    q = max(1, nc // (16 * 512)) | 1
+    while True:
+        s = 512 * q
+        if all((k * s) % nc not in near for k in range(1, steps + 1)):
+            return s
+        q += 2
+
+
+class HostNoisePool:
+    """pinned host N(0,1) pools from which every step of the end-to-end leg
+    uploads fields no earlier step used: the cell fields of the symmetric
+    momentum stress (variance 2), and the unit-variance edge and mass-face
+    fields"""
+
+    def __init__(self, torch, n, steps, seed):
+        g = torch.Generator().manual_seed(seed)
+        nc = n ** 3
+        self.stride = pool_stride(n, steps)
+        span = (steps + 1) * self.stride
+        self.nc = nc
+        self.cc = (torch.randn(3 * nc + span, generator=g, dtype=torch.float64) * 2.0 ** 0.5).pin_memory()
+        self.unit = torch.randn((3 + 3 * NSPECIES) * nc + span, generator=g, dtype=torch.float64).pin_memory()
+
+    def fields(self, i):
+        """(W_cc[3], W_ed[3] distinct, W_mass[3*ns]) host views of step i"""
+        o, nc = i * self.stride, self.nc
+        cc = [self.cc[c * nc + o: (c + 1) * nc + o] for c in range(3)]
+        un = [self.unit[f * nc + o: (f + 1) * nc + o] for f in range(3 + 3 * NSPECIES)]
+        return cc, un[:3], un[3:]
 
 
 class Case:
+    """the bench state: velocity, species densities, pressure and the mass
+    flux divergence of one 256^3 periodic box, in place"""
+
     def __init__(self, L, torch, dev, n, precision, seed=7):
         self.torch, self.dev, self.n = torch, dev, n
         nc = n ** 3
@@ -345,16 +383,37 @@ class Case:
         self.T = torch.ones(nc, device=dev, **f64)
         self.T_ed = [torch.ones(nc, device=dev, **f64) for _ in range(3)]
         self.sp = L.StochParams(k_B=KT, variance_coef_mom=1.0, dV=DX ** 3, stoch_stress_form=1, filtering_width=0)
+        torch.cuda.synchronize()  # the context launches on its own stream
 
-    def init_fluxes(self, W_m_prev):
+    def init_fluxes(self, W_m0):
         """F^0 = compute_mass_fluxdiv at the initial state (main_driver.f90
         start-up, before the time loop)"""
-        self.s.compute_mass_fluxdiv(self.mp, self.sp, self.rho, DT, [1.0], W_m_prev, self.F)
+        self.s.compute_mass_fluxdiv(self.mp, self.sp, self.rho, DT, [1.0], W_m0, self.F)
 
-    def step(self, W_cc, W_ed, W_m_prev, W_m_new):
+    def step(self, W_cc, W_ed, W_mass):
         return self.s.advance_timestep_inertial_multispecies(
             self.sp, self.mp, DT, self.umac, self.rho, self.pi, self.F, self.eta, self.eta_ed, self.kappa, self.T,
-            self.T_ed, W_cc, W_ed, list(W_m_prev) + list(W_m_new))
+            self.T_ed, W_cc, W_ed, W_mass)
+
+    def snapshot(self):
+        return [t.clone() for t in self.umac + self.rho + [self.pi]]
+
+
+def mixed_vs_fp64(mix, f64, rho0):
+    """relative infinity-norm differences of the mixed run's final fields
+    from the FP64 run's (same inputs, same noise, same step count): velocity
+    components and pressure against the FP64 field's largest magnitude, each
+    species density against the FP64 run's largest change of that density
+    over the run"""
+    out = {}
+    for c in range(3):
+        out[f"u{c}"] = float((mix[c] - f64[c]).abs().max() / f64[c].abs().max())
+    for i in range(NSPECIES):
+        d = (mix[3 + i] - f64[3 + i]).abs().max()
+        out[f"rho{i}_vs_change"] = float(d / (f64[3 + i] - rho0[i]).abs().max())
+        out[f"rho{i}"] = float(d / f64[3 + i].abs().max())
+    out["pi"] = float((mix[-1] - f64[-1]).abs().max() / f64[-1].abs().max())
+    return out
 
 
 def dist_init(args):
@@ -391,64 +450,104 @@ def allmax(ws, v, torch, dev):
 # CPU baseline: the oracle (C++ FP64 restatement, OpenMP on all host
 # threads) on a bounded sample of the workload
 # ----------------------------------------------------------------------
-def cpu_sample(n_sample: int, n_full: int):
-    import numpy as np
+class OracleCase:
+    """the bench workload on the CPU oracle at n^3 (a sample of the 256^3
+    step: the same mixture, scales and tolerances, 1/8 of the cells at
+    128^3), stepped with fresh host noise every step"""
 
-    import oracle as O
-    O.build()
-    nc = n_sample ** 3
-    rng = np.random.default_rng(7)
-    umac = [1e-3 * rng.standard_normal(nc) for _ in range(3)]
-    rho = 1.0 + 1e-3 * rng.standard_normal(nc)
-    pi = np.zeros(nc)
-    eta = np.ones(nc)
-    ee = [np.ones(nc)] * 3
-    W_cc = [rng.standard_normal(nc) * 2 ** 0.5 for _ in range(3)]
-    W_ed = []
-    for _ in range(3):
-        a = rng.standard_normal(nc)
-        W_ed += [a, a]
-    W_m = [rng.standard_normal(nc) for _ in range(2 * 3 * NSPECIES)]
-    w = 0.25 + 1e-3 * rng.standard_normal((NSPECIES, nc))
-    w /= w.sum(axis=0)
-    rho = [np.ascontiguousarray(w[i]) for i in range(NSPECIES)]
-    sp = O.StochParams(k_B=KT, variance_coef_mom=1.0, dV=DX ** 3, stoch_stress_form=1, filtering_width=0)
-    mp = O.mixture_params(**mixture())
-    F0 = O.mass_fluxdiv(3, [n_sample] * 3, DX, sp, mp, rho, DT, [1.0], W_m[: 3 * NSPECIES])
-    t0 = time.perf_counter()
-    rc, *_ = O.advance_inertial_ms(3, [n_sample] * 3, DX, 1, O.default_params(gmres_rel_tol=REL_TOL), sp, mp, DT,
-                                   umac, rho, pi, F0, eta, ee, np.zeros(nc), np.ones(nc), ee, W_cc, W_ed, W_m)
-    sec = time.perf_counter() - t0
+    def __init__(self, n):
+        import numpy as np
+
+        import oracle as O
+        O.build()
+        self.O, self.np, self.n = O, np, n
+        nc = n ** 3
+        self.nc = nc
+        rng = np.random.default_rng(7)
+        self.umac = [1e-3 * rng.standard_normal(nc) for _ in range(3)]
+        w = 0.25 + 1e-3 * rng.standard_normal((NSPECIES, nc))
+        w /= w.sum(axis=0)
+        self.rho = [np.ascontiguousarray(w[i]) for i in range(NSPECIES)]
+        self.pi = np.zeros(nc)
+        self.ones = np.ones(nc)
+        self.sp = O.StochParams(k_B=KT, variance_coef_mom=1.0, dV=DX ** 3, stoch_stress_form=1, filtering_width=0)
+        self.mp = O.mixture_params(**mixture())
+        self.params = O.default_params(gmres_rel_tol=REL_TOL)
+        self.W_prev = self.mass_noise(0)
+        self.F = O.mass_fluxdiv(3, [n] * 3, DX, self.sp, self.mp, self.rho, DT, [1.0], self.W_prev)
+
+    def mass_noise(self, k):
+        r = self.np.random.default_rng(1000 + k)
+        return [r.standard_normal(self.nc) for _ in range(3 * NSPECIES)]
+
+    def noise(self, k):
+        r = self.np.random.default_rng(5000 + k)
+        W_cc = [r.standard_normal(self.nc) * 2 ** 0.5 for _ in range(3)]
+        W_ed = []
+        for _ in range(3):
+            a = r.standard_normal(self.nc)
+            W_ed += [a, a]
+        return W_cc, W_ed, self.mass_noise(k)
+
+    def step(self, k):
+        """one timed inertial step k (its noise is drawn before the clock
+        starts); returns the seconds it took"""
+        W_cc, W_ed, W_new = self.noise(k)
+        t0 = time.perf_counter()
+        rc, self.umac, self.rho, self.pi, self.F, _ = self.O.advance_inertial_ms(
+            3, [self.n] * 3, DX, 1, self.params, self.sp, self.mp, DT, self.umac, self.rho, self.pi, self.F,
+            self.ones, [self.ones] * 3, self.np.zeros(self.nc), self.ones, [self.ones] * 3, W_cc, W_ed,
+            list(self.W_prev) + list(W_new))
+        sec = time.perf_counter() - t0
+        if rc < 0:
+            raise RuntimeError(f"oracle step failed: {rc}")
+        self.W_prev = W_new
+        return sec
+
+
+def sample_text(n_sample, n_full, sec):
     scale = (n_full / n_sample) ** 3
-    return {"value": 1.0 / (sec * scale), "unit": "steps/s", "cores": O.num_threads(), "kind": "port",
-            "sample": f"one FP64 4-species inertial step at {n_sample}^3 on the CPU oracle ({sec:.2f} s), scaled by the "
-                      f"cell ratio {scale:g} to the {n_full}^3 step (the GMRES iteration count does not grow "
-                      f"with the grid under multigrid preconditioning)",
-            "sample_seconds": sec}
+    return (f"FP64 4-species inertial steps of this workload at {n_sample}^3 (1/{scale:g} of the {n_full}^3 cells; "
+            f"{sec:.2f} s each) on the CPU oracle, OpenMP on all host threads; value = 1 / ({scale:g} x seconds "
+            f"per {n_sample}^3 step), since the GMRES iteration count does not grow with the grid under multigrid "
+            f"preconditioning")
+
+
+def cpu_sample(n_sample: int, n_full: int):
+    oc = OracleCase(n_sample)
+    sec = oc.step(1)
+    scale = (n_full / n_sample) ** 3
+    return {"value": 1.0 / (sec * scale), "unit": "steps/s", "cores": oc.O.num_threads(), "kind": "port",
+            "sample": "one of the " + sample_text(n_sample, n_full, sec)}
 
 
 def run_reference(args):
-    ws, rank, _ = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
-    if rank != 0:
+    """the reference arm: the CPU oracle (the reference itself cannot be
+    built here: Fortran on FBoxLib) on W untimed and K timed sample steps of
+    the workload; rank 0 only"""
+    if int(os.environ.get("RANK", "0")) != 0:
         return 0
     n_s = args.cpu_sample_n
+    oc = OracleCase(n_s)
     secs = []
-    for i in range(args.warmup + args.steps):
-        r = cpu_sample(n_s, args.n)
-        if i >= args.warmup:
-            secs.append(r["sample_seconds"] * (args.n / n_s) ** 3)
-        if i == 0 and args.warmup > 1:
-            # CPU runs need no warm-up beyond the first call
-            args.warmup = 1
+    for k in range(1, args.warmup + args.steps + 1):
+        sec = oc.step(k)
+        if k > args.warmup:
+            secs.append(sec)
     sec = sum(secs) / len(secs)
-    v = 1.0 / sec
+    scale = (args.n / n_s) ** 3
+    v = 1.0 / (sec * scale)
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "steps/s", "n_gpus": 0,
-            "steps": len(secs), "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True,
+            "steps": len(secs), "warmup": args.warmup, "ms_per_step": sec * 1e3,
+            "value_from_ms_per_step": f"value = 1 / ({scale:g} x ms_per_step / 1000): each timed step is a {n_s}^3 "
+                                      f"step, 1/{scale:g} of the {args.n}^3 step's cells",
+            "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded N(0,1) fields)",
-            "config": {"workload": WORKLOAD, "n_cells": [args.n] * 3, "dx": DX, "dt": DT, "k_B": KT, "gmres_rel_tol": REL_TOL,
-                       "visc_type": 1, "species": NSPECIES, "molmass": MOLMASS},
-            "cpu_baseline": {"value": v, "unit": "steps/s", "cores": r["cores"], "kind": "port",
-                             "sample": r["sample"]},
+            "config": {"workload": WORKLOAD, "n_cells": [args.n] * 3, "dx": DX, "dt": DT, "k_B": KT,
+                       "gmres_rel_tol": REL_TOL, "visc_type": 1, "species": NSPECIES, "molmass": MOLMASS,
+                       "sample_n_cells": [n_s] * 3},
+            "cpu_baseline": {"value": v, "unit": "steps/s", "cores": oc.O.num_threads(), "kind": "port",
+                             "sample": sample_text(n_s, args.n, sec)},
             "e2e": {"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -457,10 +556,129 @@ def run_reference(args):
 # finest-level smoother kernel by the kind of plan the autotuner picked
 SMOOTHER_KERNEL = {
     "rowtile": "k_stag_rbx (finest-level row-tile fused red-black smooth of all three components)",
+    "rowtile2": "k_stag_rbx two-cell form (finest-level row-tile fused red-black smooth, two cells per thread "
+                "and row from 128-bit shared-memory accesses)",
     "tiled": "k_stag_rb (finest-level tiled fused red-black smooth)",
     "colour": "k_stag_gs (finest-level colour sweep)",
     "rules": "finest-level smoother of the fixed size rules",
 }
+
+
+def run_leg(L, torch, dev, args, precision, rank, ws, e2e):
+    """W warm-up and K timed steps of one precision with fresh device noise
+    every step (drawn inside the timed region); then, if e2e, K more steps
+    through the same public call with every step's noise uploaded from
+    pinned host memory inside the timed region"""
+    n, K, W = args.n, args.steps, args.warmup
+    nc = n ** 3
+    case = Case(L, torch, dev, n, precision)
+    # the context launches on a torch-owned stream so that torch's
+    # pinned-memory and caching allocators never see a destroyed stream
+    stream = torch.cuda.Stream(device=dev)
+    case.s.set_stream(stream.cuda_stream)
+    noise = L.StepNoise(3, [n] * 3, NSPECIES, NOISE_SEED + rank, dev, stream.cuda_stream)
+    torch.cuda.synchronize()
+    noise.draw_mass(0)
+    case.init_fluxes(noise.mass(0))
+    rho0 = [r.clone() for r in case.rho]
+
+    def step(k):
+        noise.draw(k)
+        return case.step(*noise.inertial_args(k))
+
+    for k in range(1, W + 1):
+        step(k)
+    torch.cuda.synchronize()
+    barrier(ws)
+    clocks = Clocks(dev.index or 0)
+    if precision == "mixed":
+        clocks.start()
+    launches0 = case.s.kernel_launches
+    case.s.profile(True)
+    iters = []
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    # an NVTX range around the timed steps, so that a profiler can be
+    # restricted to them (ncu --nvtx --nvtx-include "timed_mixed/")
+    torch.cuda.nvtx.range_push(f"timed_{precision}")
+    ev0.record(stream)
+    for k in range(W + 1, W + K + 1):
+        st, stats = step(k)
+        iters.append([x["total_iters"] for x in stats])
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    torch.cuda.nvtx.range_pop()
+    ms = ev0.elapsed_time(ev1)
+    barrier(ws)
+    prof = case.s.profile_read()
+    case.s.profile(False)
+    # the smoother plans the autotuner picked for the finest levels
+    plan = {"stag_level0": case.s.tune_info("stag", 0), "cc_level0": case.s.tune_info("cc", 0)}
+    launches = case.s.kernel_launches - launches0 + K * noise.launches_per_draw()
+    clk = clocks.stop() if precision == "mixed" else None
+    res = dict(ms=allmax(ws, ms, torch, dev), iters=iters, prof=prof, launches=launches, clocks=clk, plan=plan,
+               resid=stats[-1]["norm_resid"] / max(stats[0]["norm_pre_b"], 1e-300), final=case.snapshot(),
+               rho0=rho0, rho_min=min(float(r.min()) for r in case.rho))
+    if e2e:
+        res["e2e"] = run_e2e(torch, dev, case, stream, noise.mass(W + K), K, rank, ws)
+    case.s.close()
+    del case
+    torch.cuda.empty_cache()
+    return res
+
+
+def run_e2e(torch, dev, case, stream, mass_prev, K, rank, ws):
+    """K steps through the public step call, each step's N(0,1) fields
+    copied from pinned host memory inside the timed region (18 fields of
+    nc doubles: 3 cell, 3 edge, 12 mass-face), overlapped with the previous
+    step on a copy stream, and each step's solver diagnostics read back"""
+    nc = case.nc
+    pool = HostNoisePool(torch, case.n, K, NOISE_SEED + 7919 * (rank + 1))
+    h2d = (3 + 3 + 3 * NSPECIES) * nc * 8
+    # three staging sets: step i computes on set i%3 (and reads the previous
+    # step's mass noise from set (i-1)%3) while a copy stream uploads step
+    # i+1's fields into set (i+1)%3, which the step before last finished with
+    NS = 3
+    mk = lambda m: [torch.empty(nc, dtype=torch.float64, device=dev) for _ in range(m)]
+    stage = [(mk(3), mk(3), mk(3 * NSPECIES)) for _ in range(NS)]
+    # the mass noise of the device-noise run's last step is the first e2e
+    # step's previous-step noise
+    for d_, s_ in zip(stage[NS - 1][2], mass_prev):
+        d_.copy_(s_)
+    torch.cuda.synchronize()
+    barrier(ws)
+    cs = torch.cuda.Stream(device=dev)
+    copied = [torch.cuda.Event() for _ in range(K)]
+    stepped = [torch.cuda.Event() for _ in range(K)]
+
+    def upload(i):
+        with torch.cuda.stream(cs):
+            if i >= 2:
+                cs.wait_event(stepped[i - 2])
+            for part_d, part_h in zip(stage[i % NS], pool.fields(i)):
+                for d_, h_ in zip(part_d, part_h):
+                    d_.copy_(h_, non_blocking=True)
+            copied[i].record(cs)
+
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    cs.wait_stream(stream)
+    upload(0)
+    with torch.cuda.stream(stream):
+        for i in range(K):
+            if i + 1 < K:
+                upload(i + 1)
+            stream.wait_event(copied[i])
+            cur, prev = stage[i % NS], stage[(i - 1) % NS]
+            W_ed = [e for e in cur[1] for _ in range(2)]
+            case.step(cur[0], W_ed, list(prev[2]) + list(cur[2]))
+            stepped[i].record(stream)
+    stream.wait_stream(cs)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = allmax(ws, e0.elapsed_time(e1), torch, dev)
+    del stage, pool
+    return dict(ms=ms, h2d=h2d, d2h=2 * 80)  # the two solves' fhd_solve_stats per step
 
 
 def main():
@@ -477,125 +695,23 @@ def main():
     dev = torch.device(f"cuda:{local}")
     torch.cuda.set_device(dev)
     n = args.n
-    nc = n ** 3
     hbm, peak_kind = peaks()
-
-    # stochastic fields: a ring of device-resident sets for the device-timed
-    # run, and pinned host sets for the end-to-end run
-    host_sets = [host_fields(n, 100 + 10 * rank + i, torch) for i in range(2)]
-    dev_sets = [tuple([w.to(dev) for w in part] for part in hs) for hs in host_sets]
-    torch.cuda.synchronize()
 
     results = {}
     for precision in ((args.only,) if args.only else ("mixed", "fp64")):
-        case = Case(L, torch, dev, n, precision)
-        # the context launches on a torch-owned stream so that torch's
-        # pinned-memory and caching allocators never see a destroyed stream
-        stream = torch.cuda.Stream(device=dev)
-        case.s.set_stream(stream.cuda_stream)
-        R = len(dev_sets)
-        case.init_fluxes(dev_sets[R - 1][2])
-
-        def run_step(i, sets):
-            wc, we, wm = sets[i % len(sets)]
-            return case.step(wc, we, sets[(i - 1) % len(sets)][2], wm)
-
-        for i in range(args.warmup):
-            run_step(i, dev_sets)
-        torch.cuda.synchronize()
-        barrier(ws)
-        clocks = Clocks(local)
-        if precision == "mixed":
-            clocks.start()
-        launches0 = case.s.kernel_launches
-        case.s.profile(True)
-        iters = []
-        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        torch.cuda.synchronize()
-        # an NVTX range around the timed steps, so that a profiler can be
-        # restricted to them (ncu --nvtx --nvtx-include "timed_mixed/")
-        torch.cuda.nvtx.range_push(f"timed_{precision}")
-        ev0.record(stream)
-        for i in range(args.steps):
-            st, stats = run_step(args.warmup + i, dev_sets)
-            iters.append([s["total_iters"] for s in stats])
-        ev1.record(stream)
-        torch.cuda.synchronize()
-        torch.cuda.nvtx.range_pop()
-        ms = ev0.elapsed_time(ev1)
-        barrier(ws)
-        prof = case.s.profile_read()
-        case.s.profile(False)
-        # the smoother plans the autotuner picked for the finest levels
-        plan = {"stag_level0": case.s.tune_info("stag", 0), "cc_level0": case.s.tune_info("cc", 0)}
-        launches = case.s.kernel_launches - launches0
-        clk = clocks.stop() if precision == "mixed" else None
-        ms_max = allmax(ws, ms, torch, dev)
-        results[precision] = dict(ms=ms_max, iters=iters, prof=prof, launches=launches, clocks=clk, plan=plan,
-                                  resid=stats[-1]["norm_resid"] / max(stats[0]["norm_pre_b"], 1e-300))
-        if precision == "mixed" and not args.no_e2e:
-            # end to end: per step the host->device copy of the step's
-            # random fields from pinned memory, the step, and the read-back
-            # of its solver diagnostics
-            h2d = sum(w.numel() * 8 for part in host_sets[0] for w in part)
-            # three staging sets: step i computes on set i%3 (and reads the
-            # previous step's mass noise from set (i-1)%3) while a copy
-            # stream uploads step i+1's fields into set (i+1)%3, which the
-            # step before last finished with
-            NS = 3
-            stage = [tuple([torch.empty(nc, dtype=torch.float64, device=dev) for _ in part] for part in host_sets[0])
-                     for _ in range(NS)]
-            # the set the first timed step treats as the previous step's
-            # fields is staged before the timed region
-            for part_d, part_h in zip(stage[NS - 1], host_sets[-1]):
-                for d_, h_ in zip(part_d, part_h):
-                    d_.copy_(h_)
-            torch.cuda.synchronize()
-            barrier(ws)
-            cs = torch.cuda.Stream(device=dev)
-            copied = [torch.cuda.Event() for _ in range(args.steps)]
-            stepped = [torch.cuda.Event() for _ in range(args.steps)]
-
-            def upload(i):
-                with torch.cuda.stream(cs):
-                    if i >= 2:
-                        cs.wait_event(stepped[i - 2])
-                    for part_d, part_h in zip(stage[i % NS], host_sets[i % len(host_sets)]):
-                        for d_, h_ in zip(part_d, part_h):
-                            d_.copy_(h_, non_blocking=True)
-                    copied[i].record(cs)
-
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            cs.wait_stream(stream)
-            upload(0)
-            with torch.cuda.stream(stream):
-                for i in range(args.steps):
-                    if i + 1 < args.steps:
-                        upload(i + 1)
-                    stream.wait_event(copied[i])
-                    tgt = stage[i % NS]
-                    st, stats = case.step(tgt[0], tgt[1], stage[(i - 1) % NS][2], tgt[2])
-                    stepped[i].record(stream)
-            stream.wait_stream(cs)
-            e1.record(stream)
-            torch.cuda.synchronize()
-            e2e_ms = allmax(ws, e0.elapsed_time(e1), torch, dev)
-            d2h = 2 * 80  # the two solves' fhd_solve_stats read back by the step call
-            results["e2e"] = dict(ms=e2e_ms, h2d=h2d, d2h=d2h)
-            del stage
-        case.s.close()
-        del case
-        torch.cuda.empty_cache()
+        results[precision] = run_leg(L, torch, dev, args, precision, rank, ws,
+                                     e2e=(precision == "mixed" and not args.no_e2e))
 
     if args.only or args.no_e2e:
         if rank == 0:
             print(json.dumps({"partial_run": True, "only": args.only, "n": n, "steps": args.steps,
                               **{k: {"ms_per_step": v["ms"] / args.steps, "gpu_launches": v["launches"],
+                                     "rho_min": v["rho_min"],
                                      "gmres_iters_per_step": [sum(x) for x in v["iters"]]}
-                                 for k, v in results.items() if k in ("mixed", "fp64")}}), flush=True)
+                                 for k, v in results.items()}}), flush=True)
         return 0
     mixed, fp64 = results["mixed"], results["fp64"]
+    errs = mixed_vs_fp64(mixed.pop("final"), fp64.pop("final"), fp64["rho0"])
     K = args.steps
     value = ws * K / (mixed["ms"] / 1e3)
     fp64_value = ws * K / (fp64["ms"] / 1e3)
@@ -606,18 +722,25 @@ def main():
     line = {
         "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": ws, "steps": K, "warmup": args.warmup,
         "ms_per_step": mixed["ms"] / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32 multigrid / f64 Krylov", "data": "synthetic (seeded N(0,1) stochastic fields)",
+        "dtype": "f32 multigrid / f64 Krylov",
+        "data": "synthetic: seeded initial state; fresh N(0,1) stochastic fields every step",
         "config": {"workload": WORKLOAD, "n_cells": [n] * 3, "dx": DX, "dt": DT, "k_B": KT, "rho_total": 1.0,
                    "eta": 1.0, "visc_type": 1, "precon_type": 1, "gmres_rel_tol": REL_TOL, "species": NSPECIES,
                    "molmass": MOLMASS, "Dbar": "U[0.5,2]*1e-2 seeded", "w0": "0.25 + 1e-3 N(0,1), renormalised",
+                   "noise": "drawn on the device every step inside the timed region (Philox-4x32-10, "
+                            "18 fields of 16.8M doubles); e2e: uploaded from pinned host memory every step",
                    "parallelism": f"replicas x{ws}",
                    "l2": "inputs larger than L2 (each 256^3 field is 134 MB)"},
         "fp64": {"value": fp64_value, "unit": "steps/s", "ms_per_step": fp64["ms"] / K,
                  "gmres_iters_per_step": [sum(x) for x in fp64["iters"]]},
         "mixed_over_fp64": value / fp64_value,
+        "mixed_vs_fp64": dict(errs, steps=args.warmup + K,
+                              note="relative inf-norm differences of the mixed run's final fields from the FP64 "
+                                   "run's; same initial state and noise"),
         "gmres_iters_per_step": [sum(x) for x in mixed["iters"]],
         "gmres_iters_per_s": ws * sum(sum(x) for x in mixed["iters"]) / (mixed["ms"] / 1e3),
         "corrector_resid_over_pre_rhs": mixed["resid"],
+        "rho_min_final": mixed["rho_min"],
         "gpu_launches": mixed["launches"],
         "autotuned_plans": {"mixed": mixed["plan"], "fp64": fp64["plan"]},
         "roofline": {"kernel": SMOOTHER_KERNEL[mixed["plan"]["stag_level0"]["kind"]],
@@ -633,8 +756,8 @@ def main():
                      "fp64_kernel": SMOOTHER_KERNEL[fp64["plan"]["stag_level0"]["kind"]],
                      "fp64_achieved": achieved64},
         "clocks": mixed["clocks"],
-        "e2e": {"value": ws * K / (results["e2e"]["ms"] / 1e3), "unit": "steps/s",
-                "h2d_bytes_per_step": results["e2e"]["h2d"], "d2h_bytes_per_step": results["e2e"]["d2h"]},
+        "e2e": {"value": ws * K / (mixed["e2e"]["ms"] / 1e3), "unit": "steps/s",
+                "h2d_bytes_per_step": mixed["e2e"]["h2d"], "d2h_bytes_per_step": mixed["e2e"]["d2h"]},
     }
     if rank == 0 and not args.no_serve:
         served = run_serving(L, SERVE_SLOTS, "mixed", SERVE_RATE, SERVE_REQUESTS)
@@ -655,9 +778,7 @@ def main():
         barrier(ws)
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         try:
-            cb = cpu_sample(args.cpu_sample_n, n)
-            cb.pop("sample_seconds", None)
-            line["cpu_baseline"] = cb
+            line["cpu_baseline"] = cpu_sample(args.cpu_sample_n, n)
         except Exception as e:  # the baseline never decides the run
             line["cpu_baseline"] = {"value": None, "error": str(e)}
     if rank == 0:

@@ -187,7 +187,8 @@ int fhd_ctx_set_fused(fhd_ctx* ctx, int mode);
 int fhd_ctx_set_tune(fhd_ctx* ctx, int mode);
 /* Plan of staggered (which 0) or pressure (which 1) multigrid level `level`
  * after the last solve call: kind -1 fixed rules, 0 colour launches, 1 tiled
- * fused, 2 row-tile; ncand candidates considered; pair_us the measured time
+ * fused, 2 row-tile, 3 row-tile with two cells per thread and row;
+ * ncand candidates considered; pair_us the measured time
  * of one smooth pair (0 when not timed); shape = {block x, block y, 0, 1,
  * threads} for colour launches, {tile x, tile y, z-runs, CTAs per SM,
  * compute threads} for fused smooths.  Any output pointer may be NULL.  No
@@ -197,25 +198,32 @@ int fhd_ctx_tune_info(fhd_ctx* ctx, int which, int level, int* kind, int* ncand,
 /* The candidate list the tuner would time for one level (host only, no
  * device): staggered (which 0) or pressure (1) multigrid, extents, precision
  * mode, visc_type, and the device's SM count and shared-memory limits (per
- * block opt-in, per SM).  Writes up to max_out records of 7 ints {kind,
- * block x | tile x | nx, block y | tile y, z-runs, CTAs per SM, row-tile
- * shared-memory bytes, threads} and returns the number of candidates.  No
- * reference counterpart. */
+ * block opt-in, per SM).  Writes up to max_out records of 7 ints {kind (as
+ * fhd_ctx_tune_info), block x | tile x | nx, block y | tile y, z-runs, CTAs
+ * per SM, row-tile shared-memory bytes, threads} and returns the number of
+ * candidates.  No reference counterpart. */
 int fhd_tune_candidates(int which, int dim, const int n_cells[3], int precision_mode, int visc_type, int sms,
                         int smem_optin, int smem_sm, int* out, int max_out);
 /* The autotuner's table as text, so that a long-running host (a server)
  * can start with the plans an earlier process measured: one line per level
- * shape, "<key> <candidate index>", the key naming device, multigrid,
- * element size, dimension, visc_type and extents.  export writes the table
- * (measured and imported plans) into buf (len bytes, NUL-terminated,
- * truncated if short) and returns the bytes the whole text needs; import
- * reads such text, returns the number of lines taken, or FHD_ERR_BAD_ARG
- * (nothing taken) on a malformed line.  An imported choice is used, untimed,
- * by the first solve that meets its shape; an index beyond that level's
- * candidate list is ignored and the level is timed.  No reference
- * counterpart. */
+ * shape, "<key> <candidate index>".  The key names the candidate-list
+ * version, device ordinal, multigrid, element size, dimension, visc_type,
+ * extents, and the device's SM count and shared-memory limits (per block
+ * opt-in, per SM) -- everything the candidate list depends on, so a table
+ * from another GPU model or library version matches no level.  export
+ * writes the table (measured and imported plans) into buf (len bytes,
+ * NUL-terminated, truncated if short) and returns the bytes the whole text
+ * needs; import reads such text, returns the number of lines taken (lines of
+ * another candidate-list version are skipped), or FHD_ERR_BAD_ARG (nothing
+ * taken) on a malformed line.  An imported choice is used, untimed, by the
+ * first solve that meets its shape; an index beyond that level's candidate
+ * list is ignored and the level is timed.  fhd_tune_key writes the key of
+ * one level shape for the given device figures (host only) and returns the
+ * bytes it needs, or FHD_ERR_BAD_ARG.  No reference counterpart. */
 long long fhd_tune_export(char* buf, long long len);
 int fhd_tune_import(const char* text);
+long long fhd_tune_key(int which, int dim, const int n_cells[3], int precision_mode, int visc_type, int sms,
+                       int smem_optin, int smem_sm, int device, char* buf, long long len);
 /* Number of this library's kernels launched through ctx so far. */
 long long fhd_ctx_kernel_launches(fhd_ctx* ctx);
 const char* fhd_status_string(int status);
@@ -314,6 +322,36 @@ int fhd_dev_compute_mass_fluxdiv(fhd_ctx* ctx, const fhd_mixture_params* mp,
                                  const double* weights, int n_rngs,
                                  const double* const W_fc[],
                                  double* const mass_fluxdiv[]);
+
+/* compute_sqrtLonsager_fc (mass_flux_utilities.f90:1096-1229): on every
+ * face of direction d, the Cholesky factor of the Onsager matrix at the
+ * face-averaged density (compute_nonnegative_rho_av, avg_type of mp;
+ * compute_sqrtLonsager_local, trace species through the non-trace
+ * subsystem).  rho: nspecies cell arrays.  sqrtLonsager_fc: dim*ns*ns face
+ * arrays, entry (r, c) of direction d at index d*ns*ns + r + ns*c (the
+ * column-major component order of the reference's ns^2-component
+ * multifab).  FP64.  nspecies 2..5. */
+int fhd_dev_compute_sqrtLonsager_fc(fhd_ctx* ctx, const fhd_mixture_params* mp,
+                                    const fhd_stoch_params* sp,
+                                    const double* const rho[],
+                                    double* const sqrtLonsager_fc[]);
+
+/* stochastic_mass_fluxdiv (stochastic_mass_fluxdiv.f90:37-116) with the
+ * face factors of fhd_dev_compute_sqrtLonsager_fc: per face the flux
+ * sqrt(2 k_B variance_coef_mass/(dV dt)) * sqrtL * sum_r weights[r] W_r,
+ * corrected to a zero species sum when mp->correct_flux
+ * (correction_flux.f90:17-226), and its divergence (compute_div), written
+ * to stoch_mass_fluxdiv[i] or added to it when increment (increment_in).
+ * W_fc[(r*dim+d)*nspecies+i] as in fhd_dev_compute_mass_fluxdiv.
+ * stoch_mass_flux (nullable): dim*nspecies face arrays [d*ns+i] receiving the
+ * flux.  FP64.  nspecies 2..5, n_rngs 1..4. */
+int fhd_dev_stochastic_mass_fluxdiv(fhd_ctx* ctx, const fhd_mixture_params* mp,
+                                    const fhd_stoch_params* sp,
+                                    const double* const sqrtLonsager_fc[],
+                                    double dt, const double* weights, int n_rngs,
+                                    const double* const W_fc[], int increment,
+                                    double* const stoch_mass_fluxdiv[],
+                                    double* const stoch_mass_flux[]);
 
 /* advance_timestep_inertial (advance_timestep_inertial.f90:45-923) for an
  * ideal isothermal mixture of mp->nspecies species (centred advection,
@@ -484,7 +522,8 @@ int fhd_ctx_profile_read(fhd_ctx* ctx, long long* launches, double* ms,
  * 3D or 512^2 in 2D) are rejected with FHD_ERR_BAD_ARG and a message in
  * fhd_last_error().  FP64 only; arguments as fhd_dev_stag_mg_solver plus the
  * grid, the parameters and the stream (NULL = legacy default stream).
- * The first call on a device looks up the array's device address.  All calls
+ * Every call looks up the array's device address on the current device
+ * (cudaGetSymbolAddress), so no address outlives a device reset.  All calls
  * share the array: calls whose work overlaps on the GPU race with each
  * other; serialise them (one stream, or synchronise between calls). */
 #define FHD_NOALLOC_SCRATCH_BYTES (16ll * 1024 * 1024)
@@ -564,6 +603,46 @@ int fhd_stochastic_m_fluxdiv(fhd_ctx* ctx, const fhd_stoch_params* sp,
                              double dt, const double* weights, int n_rngs,
                              const fhd_multifab* W_cc,
                              const fhd_multifab* W_ed);
+
+/* stag_mg_solver(mla,la_mg,alpha_fc,beta_cc,beta_ed,gamma_cc,theta_alpha,
+ *                phi_fc,rhs_fc,dx,the_bc_tower)  (stag_mg_solver.f90:37-50):
+ * staggered multigrid V-cycles on (theta_alpha alpha - L) phi = rhs.  phi_fc
+ * is read as the initial guess and overwritten (valid region and ghost
+ * cells, periodic fill); it needs >= 1 ghost cell. */
+int fhd_stag_mg_solve(fhd_ctx* ctx,
+                      const fhd_multifab* alpha_fc, const fhd_multifab* beta_cc,
+                      const fhd_multifab* beta_ed, const fhd_multifab* gamma_cc,
+                      double theta_alpha,
+                      const fhd_multifab* phi_fc, const fhd_multifab* rhs_fc);
+
+/* compute_sqrtLonsager_fc(mla,rho,rhotot,sqrtLonsager_fc,dx)
+ * (mass_flux_utilities.f90:1096-1229): rho an nspecies-component cell
+ * multifab with >= 1 ghost cell; rhotot (nullable; the reference does not
+ * read it here); sqrtLonsager_fc[d] an nspecies^2-component face multifab of
+ * direction d, component r + ns*c = entry (r, c) of the lower Cholesky
+ * factor, written over the whole fab (periodic fill). */
+int fhd_compute_sqrtLonsager_fc(fhd_ctx* ctx, const fhd_mixture_params* mp,
+                                const fhd_stoch_params* sp,
+                                const fhd_multifab* rho, const fhd_multifab* rhotot,
+                                const fhd_multifab* sqrtLonsager_fc);
+
+/* stochastic_mass_fluxdiv(mla,rho,rhotot,sqrtLonsager_fc,stoch_mass_fluxdiv,
+ *   stoch_mass_flux,dx,dt,weights,the_bc_level,increment_in)
+ *   (stochastic_mass_fluxdiv.f90:37-51).  The module-global random storage
+ *   stoch_W_fc of the reference is passed explicitly: W_fc[r*dim+d] is an
+ *   nspecies-component face multifab of stage r, direction d.
+ *   stoch_mass_fluxdiv: nspecies-component cell multifab (read too when
+ *   increment); stoch_mass_flux (nullable): dim nspecies-component face
+ *   multifabs.  rho, rhotot (nullable) are the correction_flux arguments of
+ *   the reference, whose correction reads only the fluxes. */
+int fhd_stochastic_mass_fluxdiv(fhd_ctx* ctx, const fhd_mixture_params* mp,
+                                const fhd_stoch_params* sp,
+                                const fhd_multifab* rho, const fhd_multifab* rhotot,
+                                const fhd_multifab* sqrtLonsager_fc,
+                                const fhd_multifab* stoch_mass_fluxdiv,
+                                const fhd_multifab* stoch_mass_flux,
+                                double dt, const double* weights, int n_rngs,
+                                const fhd_multifab* W_fc, int increment);
 
 #ifdef __cplusplus
 }

@@ -23,10 +23,10 @@ from ._capi import (FHD_PREC_FP64, FHD_PREC_MIXED, FHD_REQ_INERTIAL, FHD_REQ_OVE
                     mixture_params)
 
 __all__ = ["StokesSolver", "GmresParams", "StochParams", "SolveStats", "MixtureParams", "mixture_params",
-           "Server", "StructureFactor", "tune_candidates", "tune_export", "tune_import", "Request", "RequestResult", "make_request", "fill_normal", "philox4x32_10", "sched_simulate",
+           "Server", "StructureFactor", "tune_candidates", "tune_export", "tune_import", "tune_key", "Request", "RequestResult", "make_request", "fill_normal", "StepNoise", "philox4x32_10", "sched_simulate",
            "FHD_REQ_OVERDAMPED", "FHD_REQ_INERTIAL",
            "default_params", "FhdError",
-           "FHD_PREC_FP64", "FHD_PREC_MIXED", "lib", "fab_from_canonical", "canonical_from_fab", "FabArray"]
+           "FHD_PREC_FP64", "FHD_PREC_MIXED", "lib", "fab_from_canonical", "fab_from_components", "canonical_from_fab", "FabArray"]
 
 
 def default_params(**overrides) -> GmresParams:
@@ -134,7 +134,7 @@ class StokesSolver:
         shape = (C.c_int * 5)()
         check(lib().fhd_ctx_tune_info(self._h, 0 if which == "stag" else 1, int(level), C.byref(kind),
                                       C.byref(nc), C.byref(us), shape), "fhd_ctx_tune_info")
-        names = {-1: "rules", 0: "colour", 1: "tiled", 2: "rowtile"}
+        names = {-1: "rules", 0: "colour", 1: "tiled", 2: "rowtile", 3: "rowtile2"}
         return {"kind": names[kind.value], "candidates": nc.value, "pair_us": us.value, "shape": list(shape)}
 
     def profile(self, enable: bool = True):
@@ -227,6 +227,23 @@ class StokesSolver:
                                                         C.cast(w, _DP), len(weights), _dpp(W_fc),
                                                         _dpp(mass_fluxdiv)), "compute_mass_fluxdiv")
 
+    def compute_sqrtLonsager_fc(self, mp: MixtureParams, sp: StochParams, rho, sqrtLonsager_fc):
+        """compute_sqrtLonsager_fc (mass_flux_utilities.f90:1096-1229):
+        sqrtLonsager_fc[d*ns*ns + r + ns*c] = entry (r, c) of the face
+        Cholesky factors of direction d"""
+        return check(lib().fhd_dev_compute_sqrtLonsager_fc(self._h, C.byref(mp), C.byref(sp), _dpp(rho),
+                                                           _dpp(sqrtLonsager_fc)), "compute_sqrtLonsager_fc")
+
+    def stochastic_mass_fluxdiv(self, mp: MixtureParams, sp: StochParams, sqrtLonsager_fc, dt, weights, W_fc,
+                                stoch_mass_fluxdiv, stoch_mass_flux=None, increment=False):
+        """stochastic_mass_fluxdiv (stochastic_mass_fluxdiv.f90:37-116) with
+        the face factors of compute_sqrtLonsager_fc"""
+        w = (C.c_double * len(weights))(*[float(x) for x in weights])
+        return check(lib().fhd_dev_stochastic_mass_fluxdiv(
+            self._h, C.byref(mp), C.byref(sp), _dpp(sqrtLonsager_fc), float(dt), C.cast(w, _DP), len(weights),
+            _dpp(W_fc), int(bool(increment)), _dpp(stoch_mass_fluxdiv),
+            _dpp(stoch_mass_flux) if stoch_mass_flux is not None else None), "stochastic_mass_fluxdiv")
+
     def advance_timestep_overdamped(self, sp: StochParams, mp, dt, umac, rho, pi, eta, eta_ed, kappa, temperature,
                                     temperature_ed, W_cc, W_ed, W_mass=None):
         """One overdamped step (advance_timestep_overdamped.f90:135-734) in
@@ -279,6 +296,35 @@ class StokesSolver:
         mfs = [_mf_vec(b_u, keep), _mf(b_p, keep), _mf_vec(x_u, keep), _mf(x_p, keep),
                _mf_vec(alpha_fc, keep), _mf(beta, keep), _mf_vec(beta_ed, keep), _mf(gamma, keep)]
         return check(lib().fhd_apply_precon(self._h, *mfs, float(theta_alpha)), "fhd_apply_precon")
+
+    def stag_mg_solver_fab(self, alpha_fc, beta_cc, beta_ed, gamma_cc, theta_alpha, phi_fc, rhs_fc):
+        """stag_mg_solver on host multifabs; phi_fc (>= 1 ghost cell) in/out"""
+        keep = []
+        return check(lib().fhd_stag_mg_solve(self._h, _mf_vec(alpha_fc, keep), _mf(beta_cc, keep),
+                                             _mf_vec(beta_ed, keep), _mf(gamma_cc, keep), float(theta_alpha),
+                                             _mf_vec(phi_fc, keep), _mf_vec(rhs_fc, keep)), "fhd_stag_mg_solve")
+
+    def compute_sqrtLonsager_fc_fab(self, mp: MixtureParams, sp: StochParams, rho, rhotot, sqrtLonsager_fc):
+        """compute_sqrtLonsager_fc on host multifabs: rho (nspecies
+        components, >= 1 ghost cell), sqrtLonsager_fc (dim face multifabs of
+        nspecies^2 components, written)"""
+        keep = []
+        return check(lib().fhd_compute_sqrtLonsager_fc(self._h, C.byref(mp), C.byref(sp), _mf(rho, keep),
+                                                       _mf(rhotot, keep) if rhotot is not None else None,
+                                                       _mf_vec(sqrtLonsager_fc, keep)), "fhd_compute_sqrtLonsager_fc")
+
+    def stochastic_mass_fluxdiv_fab(self, mp: MixtureParams, sp: StochParams, rho, rhotot, sqrtLonsager_fc,
+                                    stoch_mass_fluxdiv, stoch_mass_flux, dt, weights, W_fc, increment=False):
+        """stochastic_mass_fluxdiv on host multifabs; W_fc[r*dim+d]: the
+        nspecies-component N(0,1) face multifab of stage r, direction d"""
+        keep = []
+        w = (C.c_double * len(weights))(*[float(x) for x in weights])
+        return check(lib().fhd_stochastic_mass_fluxdiv(
+            self._h, C.byref(mp), C.byref(sp), _mf(rho, keep) if rho is not None else None,
+            _mf(rhotot, keep) if rhotot is not None else None, _mf_vec(sqrtLonsager_fc, keep),
+            _mf(stoch_mass_fluxdiv, keep), _mf_vec(stoch_mass_flux, keep) if stoch_mass_flux is not None else None,
+            float(dt), C.cast(w, _DP), len(weights), _mf_vec(W_fc, keep), int(bool(increment))),
+            "fhd_stochastic_mass_fluxdiv")
 
 
 def stag_mg_solver_noalloc(dim, n_cells, dx, visc_type, params, alpha_fc, beta_cc, beta_ed, gamma_cc,
@@ -360,6 +406,15 @@ def fab_from_canonical(x: np.ndarray, dim: int, n_cells, nodal, ng: int, lo=None
     return FabArray(data, lo + [0] * (3 - dim), hi + [0] * (3 - dim), nodal + [0] * (3 - dim), ng)
 
 
+def fab_from_components(xs, dim: int, n_cells, nodal, ng: int, lo=None, hi=None) -> FabArray:
+    """Periodic canonical arrays, one per component -> one multi-component
+    fab (Fortran order, the component index slowest)."""
+    fabs = [fab_from_canonical(x, dim, n_cells, nodal, ng, lo, hi) for x in xs]
+    data = np.asfortranarray(np.stack([f.data for f in fabs], axis=-1))
+    f0 = fabs[0]
+    return FabArray(data, f0.lo, f0.hi, f0.nodal, ng, ncomp=len(xs))
+
+
 def canonical_from_fab(fa: FabArray, dim: int, n_cells) -> np.ndarray:
     """Valid cells lo..hi of one whole-domain fab -> canonical array."""
     n = list(n_cells)[:dim]
@@ -386,6 +441,61 @@ def philox4x32_10(ctr, key):
     o = (C.c_uint * 4)()
     lib().fhd_philox4x32_10(c, k, o)
     return list(o)
+
+
+class StepNoise:
+    """Fresh N(0,1) stochastic fields for every inertial step, drawn on the
+    device by the Philox generator: the work of fill_m_stochastic
+    (stochastic_m_fluxdiv.f90:781-860, symmetric stress form: cell entries
+    with variance 2, the two components of a node/edge equal) and
+    fill_mass_stochastic (stochastic_mass_fluxdiv.f90:182-214).
+
+    The counters follow the server's: momentum field c counted by the step,
+    mass field 1000 + d*ns + i counted by the noise index.  Step k of
+    advance_timestep_inertial reads the mass noise M_{k-1} (predictor) and M_k
+    (corrector); F^0 comes from M_0.  So two runs with the same seed (say
+    mixed precision and FP64) see the same fields, and no two steps do."""
+
+    def __init__(self, dim: int, n_cells, nspecies: int, seed: int, device, stream: int | None = None):
+        import torch
+        self.dim, self.ns, self.seed, self.stream = dim, nspecies, int(seed), stream
+        nc = int(np.prod(list(n_cells)[:dim]))
+        ne = 1 if dim == 2 else 3
+        z = lambda: torch.empty(nc, dtype=torch.float64, device=device)
+        self.W_cc = [z() for _ in range(dim)]
+        self._ed = [z() for _ in range(ne)]
+        # both components of a node/edge point at the same field
+        self.W_ed = [e for e in self._ed for _ in range(2)]
+        self._mass = [[z() for _ in range(dim * nspecies)] for _ in range(2)] if nspecies > 1 else None
+
+    def _fill(self, out, field, count, scale=1.0):
+        fill_normal(out, self.seed, field, count, 0x5EED, scale, self.stream)
+
+    def draw_mass(self, j: int):
+        """mass noise M_j into its ring slot"""
+        for i, w in enumerate(self._mass[j % 2]):
+            self._fill(w, 1000 + i, j)
+
+    def mass(self, j: int):
+        return self._mass[j % 2]
+
+    def draw(self, step: int):
+        """the fields of inertial step `step` (>= 1): momentum, and M_step"""
+        for c, w in enumerate(self.W_cc):
+            self._fill(w, c, step, 2.0 ** 0.5)
+        for e, w in enumerate(self._ed):
+            self._fill(w, self.dim + e, step)
+        if self._mass is not None:
+            self.draw_mass(step)
+
+    def launches_per_draw(self) -> int:
+        return len(self.W_cc) + len(self._ed) + (len(self._mass[0]) if self._mass is not None else 0)
+
+    def inertial_args(self, step: int):
+        """(W_cc, W_ed, W_mass) of step `step` as the multispecies inertial
+        step takes them: W_mass = M_{step-1} followed by M_step"""
+        wm = (list(self.mass(step - 1)) + list(self.mass(step))) if self._mass is not None else None
+        return self.W_cc, self.W_ed, wm
 
 
 def make_request(**kw) -> Request:
@@ -425,7 +535,7 @@ def tune_candidates(which: str, dim: int, n_cells, precision: str = "mixed", vis
     out = (C.c_int * (7 * 64))()
     k = check(lib().fhd_tune_candidates(0 if which == "stag" else 1, int(dim), n, prec, int(visc_type), int(sms),
                                         int(smem_optin), int(smem_sm), out, 64), "fhd_tune_candidates")
-    names = {0: "colour", 1: "tiled", 2: "rowtile"}
+    names = {0: "colour", 1: "tiled", 2: "rowtile", 3: "rowtile2"}
     return [dict(kind=names[out[7 * i]], x=out[7 * i + 1], y=out[7 * i + 2], zruns=out[7 * i + 3],
                  per_sm=out[7 * i + 4], smem=out[7 * i + 5], threads=out[7 * i + 6]) for i in range(min(k, 64))]
 
@@ -441,6 +551,21 @@ def tune_export() -> str:
 def tune_import(text: str) -> int:
     """add plans from text written by tune_export (fhd_tune_import)"""
     return check(lib().fhd_tune_import(text.encode()), "fhd_tune_import")
+
+
+def tune_key(which: str, dim: int, n_cells, precision: str = "mixed", visc_type: int = 1, sms: int = 148,
+             smem_optin: int = 232448, smem_sm: int = 233472, device: int = 0) -> str:
+    """the autotuner's table key of one level shape (fhd_tune_key; host
+    only); defaults: device 0 with the B200's 148 SMs and shared-memory
+    limits"""
+    n = (C.c_int * 3)(*(list(n_cells) + [1] * (3 - len(n_cells))))
+    prec = FHD_PREC_MIXED if precision == "mixed" else FHD_PREC_FP64
+    args = (0 if which == "stag" else 1, int(dim), n, prec, int(visc_type), int(sms), int(smem_optin), int(smem_sm),
+            int(device))
+    need = check(int(lib().fhd_tune_key(*args, None, 0)), "fhd_tune_key")
+    buf = C.create_string_buffer(need)
+    lib().fhd_tune_key(*args, buf, need)
+    return buf.value.decode()
 
 
 class StructureFactor:

@@ -146,6 +146,8 @@ _PROTOS = {
     "fhd_ctx_set_tune": (C.c_int, [_VP, C.c_int]),
     "fhd_tune_export": (C.c_longlong, [C.c_char_p, C.c_longlong]),
     "fhd_tune_import": (C.c_int, [C.c_char_p]),
+    "fhd_tune_key": (C.c_longlong, [C.c_int, C.c_int, C.POINTER(C.c_int), C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                    C.c_int, C.c_char_p, C.c_longlong]),
     "fhd_tune_candidates": (C.c_int, [C.c_int, C.c_int, C.POINTER(C.c_int), C.c_int, C.c_int, C.c_int, C.c_int,
                                       C.c_int, C.POINTER(C.c_int), C.c_int]),
     "fhd_sk_create": (C.c_int, [C.c_int, C.POINTER(C.c_int), C.c_double, C.c_int, C.POINTER(C.c_int), C.c_int,
@@ -194,6 +196,15 @@ _PROTOS = {
     "fhd_server_clock": (C.c_double, [_VP]),
     "fhd_server_destroy": (C.c_int, [_VP]),
     "fhd_sched_simulate": (C.c_int, [C.c_int, C.c_ulonglong, C.c_int, _DP, C.POINTER(C.c_ulonglong), _DP, _DP]),
+    "fhd_dev_compute_sqrtLonsager_fc": (C.c_int, [_VP, C.POINTER(MixtureParams), C.POINTER(StochParams), _PP, _PP]),
+    "fhd_dev_stochastic_mass_fluxdiv": (C.c_int, [_VP, C.POINTER(MixtureParams), C.POINTER(StochParams), _PP,
+                                                  C.c_double, _DP, C.c_int, _PP, C.c_int, _PP, _PP]),
+    "fhd_stag_mg_solve": (C.c_int, [_VP] + [C.POINTER(Multifab)] * 4 + [C.c_double] + [C.POINTER(Multifab)] * 2),
+    "fhd_compute_sqrtLonsager_fc": (C.c_int, [_VP, C.POINTER(MixtureParams), C.POINTER(StochParams)]
+                                    + [C.POINTER(Multifab)] * 3),
+    "fhd_stochastic_mass_fluxdiv": (C.c_int, [_VP, C.POINTER(MixtureParams), C.POINTER(StochParams)]
+                                    + [C.POINTER(Multifab)] * 5 + [C.c_double, _DP, C.c_int, C.POINTER(Multifab),
+                                                                   C.c_int]),
     "fhd_gmres": (C.c_int, [_VP] + [C.POINTER(Multifab)] * 8 + [_DP, _DP, C.POINTER(SolveStats)]),
     "fhd_apply_precon": (C.c_int, [_VP] + [C.POINTER(Multifab)] * 8 + [C.c_double]),
     "fhd_apply_matrix": (C.c_int, [_VP] + [C.POINTER(Multifab)] * 8 + [C.c_double]),
@@ -238,8 +249,11 @@ def lib() -> C.CDLL:
 class FhdError(RuntimeError):
     def __init__(self, status: int, where: str):
         msg = lib().fhd_status_string(status).decode()
-        super().__init__(f"{where}: status {status}: {msg}")
+        # the library's own message names the site that failed
+        detail = (lib().fhd_last_error() or b"").decode(errors="replace")
+        super().__init__(f"{where}: status {status}: {msg}" + (f" ({detail})" if detail else ""))
         self.status = status
+        self.detail = detail
 
 
 def check(status: int, where: str) -> int:

@@ -217,6 +217,62 @@ int load_coeffs(fhd_ctx* ctx, HostPath* H, Operands& o, const fhd_multifab* alph
     return 0;
 }
 
+// one component of a multi-component multifab, as a one-component view
+// (the data pointer of each fab advanced by comp whole components)
+void comp_view(const fhd_multifab& mf, int dim, int comp, std::vector<fhd_fab>& store, fhd_multifab& out) {
+    store.assign(mf.fabs, mf.fabs + mf.nfabs);
+    for (auto& f : store) {
+        FabDesc d = desc_of(f, dim);
+        f.data = f.data + (i64)comp * fab_elems(d);
+    }
+    out.nfabs = mf.nfabs;
+    out.fabs = store.data();
+}
+
+int check_ncomp(const fhd_multifab& mf, int want) {
+    for (int b = 0; b < mf.nfabs; b++)
+        if (mf.fabs[b].ncomp < want) return FHD_ERR_BAD_ARG;
+    return 0;
+}
+
+// every component of a multifab to its own canonical device array
+int mf_comps_to_dev(fhd_ctx* ctx, const fhd_multifab& mf, int ncomp, double* const dst[]) {
+    std::vector<fhd_fab> store;
+    fhd_multifab one;
+    for (int c = 0; c < ncomp; c++) {
+        comp_view(mf, ctx->dim, c, store, one);
+        if (int rc = mf_to_dev(ctx, &one, dst[c])) return rc;
+        // the view's fab descriptors live in store until the copies are queued
+        FHD_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    }
+    return 0;
+}
+
+int dev_to_mf_comps(fhd_ctx* ctx, const double* const src[], int ncomp, const fhd_multifab& mf) {
+    std::vector<fhd_fab> store;
+    fhd_multifab one;
+    for (int c = 0; c < ncomp; c++) {
+        comp_view(mf, ctx->dim, c, store, one);
+        if (int rc = dev_to_mf(ctx, src[c], &one)) return rc;
+    }
+    return 0;
+}
+
+// per-call device arrays of nc doubles, freed on scope exit
+struct DevArrays {
+    std::vector<double*> a;
+    int alloc(int n, i64 nc) {
+        a.assign(n, nullptr);
+        for (int i = 0; i < n; i++)
+            if (cudaMalloc(&a[i], sizeof(double) * (size_t)nc) != cudaSuccess) return FHD_ERR_OOM;
+        return 0;
+    }
+    ~DevArrays() {
+        for (double* p : a)
+            if (p) cudaFree(p);
+    }
+};
+
 }  // namespace
 
 extern "C" {
@@ -394,6 +450,108 @@ int fhd_stochastic_m_fluxdiv(fhd_ctx* ctx, const fhd_stoch_params* sp, const fhd
     cudaStreamSynchronize(ctx->stream);
     cleanup();
     return rc;
+}
+
+int fhd_stag_mg_solve(fhd_ctx* ctx, const fhd_multifab* alpha_fc, const fhd_multifab* beta_cc,
+                      const fhd_multifab* beta_ed, const fhd_multifab* gamma_cc, double theta_alpha,
+                      const fhd_multifab* phi_fc, const fhd_multifab* rhs_fc) {
+    if (!ctx || !alpha_fc || !beta_cc || !beta_ed || !gamma_cc || !phi_fc || !rhs_fc) return FHD_ERR_BAD_ARG;
+    const int dim = ctx->dim;
+    int rc;
+    for (int c = 0; c < dim; c++)
+        if ((rc = check_mf(ctx, &phi_fc[c], 1)) || (rc = check_mf(ctx, &rhs_fc[c], 0))) return rc;
+    HostPath* H;
+    if ((rc = host_arrays(ctx, H))) return rc;
+    Operands o;
+    if ((rc = load_coeffs(ctx, H, o, alpha_fc, beta_cc, beta_ed, gamma_cc))) return rc;
+    for (int c = 0; c < dim; c++) {
+        if ((rc = mf_to_dev(ctx, &rhs_fc[c], o.b_u[c]))) return rc;
+        if ((rc = mf_to_dev(ctx, &phi_fc[c], o.x_u[c]))) return rc;
+    }
+    const double* cr[3] = {o.b_u[0], o.b_u[1], o.b_u[2]};
+    const double* ca[3] = {o.al[0], o.al[1], o.al[2]};
+    const double* ce[3] = {o.bed[0], o.bed[1], o.bed[2]};
+    rc = fhd_dev_stag_mg_solver(ctx, ca, o.be, ce, o.ga, theta_alpha, o.x_u, cr);
+    if (rc < 0) return rc;
+    for (int c = 0; c < dim; c++)
+        if (int r2 = dev_to_mf(ctx, o.x_u[c], &phi_fc[c])) return r2;
+    return rc;
+}
+
+int fhd_compute_sqrtLonsager_fc(fhd_ctx* ctx, const fhd_mixture_params* mp, const fhd_stoch_params* sp,
+                                const fhd_multifab* rho, const fhd_multifab* rhotot,
+                                const fhd_multifab* sqrtLonsager_fc) {
+    if (!ctx || !mp || !sp || !rho || !sqrtLonsager_fc) return FHD_ERR_BAD_ARG;
+    if (mp->nspecies < 2 || mp->nspecies > 5) return FHD_ERR_UNSUPPORTED;
+    const int dim = ctx->dim, ns = mp->nspecies;
+    int rc;
+    // rho is read on both sides of every face: one ghost cell
+    if ((rc = check_mf(ctx, rho, 1)) || (rc = check_ncomp(*rho, ns))) return rc;
+    if (rhotot && (rc = check_mf(ctx, rhotot, 0))) return rc;
+    for (int d = 0; d < dim; d++)
+        if ((rc = check_mf(ctx, &sqrtLonsager_fc[d], 0)) || (rc = check_ncomp(sqrtLonsager_fc[d], ns * ns))) return rc;
+    DevArrays A;
+    if ((rc = A.alloc(ns + dim * ns * ns, ctx->g0.nc))) return rc;
+    double** d_rho = A.a.data();
+    double** d_L = A.a.data() + ns;
+    if ((rc = mf_comps_to_dev(ctx, *rho, ns, d_rho))) return rc;
+    std::vector<const double*> crho(d_rho, d_rho + ns);
+    if ((rc = fhd_dev_compute_sqrtLonsager_fc(ctx, mp, sp, crho.data(), d_L))) return rc;
+    for (int d = 0; d < dim; d++) {
+        std::vector<const double*> src(d_L + d * ns * ns, d_L + (d + 1) * ns * ns);
+        if ((rc = dev_to_mf_comps(ctx, src.data(), ns * ns, sqrtLonsager_fc[d]))) return rc;
+    }
+    return 0;
+}
+
+int fhd_stochastic_mass_fluxdiv(fhd_ctx* ctx, const fhd_mixture_params* mp, const fhd_stoch_params* sp,
+                                const fhd_multifab* rho, const fhd_multifab* rhotot,
+                                const fhd_multifab* sqrtLonsager_fc, const fhd_multifab* stoch_mass_fluxdiv,
+                                const fhd_multifab* stoch_mass_flux, double dt, const double* weights, int n_rngs,
+                                const fhd_multifab* W_fc, int increment) {
+    if (!ctx || !mp || !sp || !sqrtLonsager_fc || !stoch_mass_fluxdiv || !weights || !W_fc || !(dt > 0.0))
+        return FHD_ERR_BAD_ARG;
+    if (mp->nspecies < 2 || mp->nspecies > 5 || n_rngs < 1 || n_rngs > 4) return FHD_ERR_UNSUPPORTED;
+    const int dim = ctx->dim, ns = mp->nspecies;
+    int rc;
+    // rho and rhotot are the reference's correction_flux arguments; the
+    // correction itself reads only the fluxes, so they are checked when given
+    if (rho && (rc = check_mf(ctx, rho, 0))) return rc;
+    if (rhotot && (rc = check_mf(ctx, rhotot, 0))) return rc;
+    if ((rc = check_mf(ctx, stoch_mass_fluxdiv, 0)) || (rc = check_ncomp(*stoch_mass_fluxdiv, ns))) return rc;
+    for (int d = 0; d < dim; d++) {
+        if ((rc = check_mf(ctx, &sqrtLonsager_fc[d], 0)) || (rc = check_ncomp(sqrtLonsager_fc[d], ns * ns))) return rc;
+        if (stoch_mass_flux && ((rc = check_mf(ctx, &stoch_mass_flux[d], 0)) ||
+                                (rc = check_ncomp(stoch_mass_flux[d], ns))))
+            return rc;
+    }
+    for (int q = 0; q < n_rngs * dim; q++)
+        if ((rc = check_mf(ctx, &W_fc[q], 0)) || (rc = check_ncomp(W_fc[q], ns))) return rc;
+    const int nL = dim * ns * ns, nW = n_rngs * dim * ns, nF = dim * ns;
+    DevArrays A;
+    if ((rc = A.alloc(nL + nW + ns + nF, ctx->g0.nc))) return rc;
+    double** d_L = A.a.data();
+    double** d_W = d_L + nL;
+    double** d_div = d_W + nW;
+    double** d_F = d_div + ns;
+    for (int d = 0; d < dim; d++)
+        if ((rc = mf_comps_to_dev(ctx, sqrtLonsager_fc[d], ns * ns, d_L + d * ns * ns))) return rc;
+    // W_fc[r*dim + d] holds the ns species components of stage r, direction d
+    for (int q = 0; q < n_rngs * dim; q++)
+        if ((rc = mf_comps_to_dev(ctx, W_fc[q], ns, d_W + q * ns))) return rc;
+    if (increment && (rc = mf_comps_to_dev(ctx, *stoch_mass_fluxdiv, ns, d_div))) return rc;
+    std::vector<const double*> cL(d_L, d_L + nL), cW(d_W, d_W + nW);
+    if ((rc = fhd_dev_stochastic_mass_fluxdiv(ctx, mp, sp, cL.data(), dt, weights, n_rngs, cW.data(), increment,
+                                              d_div, d_F)))
+        return rc;
+    std::vector<const double*> cdiv(d_div, d_div + ns);
+    if ((rc = dev_to_mf_comps(ctx, cdiv.data(), ns, *stoch_mass_fluxdiv))) return rc;
+    if (stoch_mass_flux)
+        for (int d = 0; d < dim; d++) {
+            std::vector<const double*> src(d_F + d * ns, d_F + (d + 1) * ns);
+            if ((rc = dev_to_mf_comps(ctx, src.data(), ns, stoch_mass_flux[d]))) return rc;
+        }
+    return 0;
 }
 
 }  // extern "C"

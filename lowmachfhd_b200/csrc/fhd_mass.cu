@@ -303,20 +303,269 @@ __device__ __forceinline__ void d_chi(const MixDev& m, const T* rho, T rhotot, c
     }
 }
 
+// trace species (mass fraction below fraction_tolerance): returns the
+// mask of the non-trace species and their count in *nact
 template <typename T, int NS>
-__device__ __forceinline__ int d_ntrace(const MixDev& m, const T* rho, T rhotot) {
-    int nt = 0;
+__device__ __forceinline__ unsigned d_active(const MixDev& m, const T* rho, T rhotot, int* nact) {
+    unsigned act = 0u;
+    int na = 0;
     if constexpr (sizeof(T) == 4) {
         const float ri = frcp(rhotot);
 #pragma unroll
         for (int i = 0; i < NS; i++)
-            if (rho[i] * ri < m.tol_f) nt++;
+            if (!(rho[i] * ri < m.tol_f)) {
+                act |= 1u << i;
+                na++;
+            }
     } else {
 #pragma unroll
         for (int i = 0; i < NS; i++)
-            if (rho[i] / rhotot < (T)m.frac_tol) nt++;
+            if (!(rho[i] / rhotot < (T)m.frac_tol)) {
+                act |= 1u << i;
+                na++;
+            }
     }
-    return nt;
+    *nact = na;
+    return act;
+}
+
+// ---------------------------------------------------------------------
+// the subsystem of non-trace species (compute_chi_sub and
+// compute_sqrtLonsager_sub, mass_flux_utilities.f90:654-739, 1425-1502),
+// on the full NS-sized register arrays: a trace species' entries are
+// skipped by the mask `act`, and every sum runs over the non-trace species
+// in increasing order, which is the order of the reference's compacted
+// subsystem arrays (dest).  A face or cell takes this branch only when some
+// but not all-but-one species are trace.
+// ---------------------------------------------------------------------
+template <typename T, int NS>
+struct SubSys {
+    T rt, mt;          // subsystem total density, molar mass
+    T x[NS];           // subsystem molar concentrations (0 for trace species)
+    T chi[NS][NS];     // subsystem chi (0 on trace rows and columns)
+};
+
+template <typename T, int NS, class MX>
+__device__ __forceinline__ void d_subsys(const MX& m, unsigned act, int nsub, const T* rho, SubSys<T, NS>& S) {
+    const auto on = [&](int i) { return (act >> i) & 1u; };
+    S.rt = T(0);
+#pragma unroll
+    for (int i = 0; i < NS; i++)
+        if (on(i)) S.rt = S.rt + rho[i];
+    // compute_molconc_molmtot_local on the subsystem
+    T W[NS];
+    T s = T(0);
+#pragma unroll
+    for (int i = 0; i < NS; i++) {
+        W[i] = T(0);
+        if (on(i)) {
+            W[i] = rho[i] / S.rt;
+            s = s + W[i] / (T)m.molmass[i];
+        }
+    }
+    S.mt = T(1) / s;
+#pragma unroll
+    for (int i = 0; i < NS; i++) S.x[i] = on(i) ? S.mt * W[i] / (T)m.molmass[i] : T(0);
+#pragma unroll
+    for (int i = 0; i < NS; i++)
+#pragma unroll
+        for (int j = 0; j < NS; j++) S.chi[i][j] = T(0);
+    if (nsub == 2) {
+        // compute_chi's closed form for two species (mass_flux_utilities.f90:767-786)
+        int a = -1, b = -1;
+#pragma unroll
+        for (int i = 0; i < NS; i++)
+            if (on(i)) {
+                if (a < 0) a = i;
+                else b = i;
+            }
+        T ra = T(0), rb = T(0);
+#pragma unroll
+        for (int i = 0; i < NS; i++) {
+            if (i == a) ra = rho[i];
+            if (i == b) rb = rho[i];
+        }
+        const T W0 = ra / S.rt, W1 = rb / S.rt;
+        const T ma = (T)m.molmass[a], mb = (T)m.molmass[b];
+        T t = ma * W1 + mb * W0;
+        t = (T)m.D[a][b] * t * t / ma / mb;
+#pragma unroll
+        for (int i = 0; i < NS; i++)
+#pragma unroll
+            for (int j = 0; j < NS; j++) {
+                if (i == a && j == a) S.chi[i][j] = t * W1 / W0;
+                if ((i == a && j == b) || (i == b && j == a)) S.chi[i][j] = -t;
+                if (i == b && j == b) S.chi[i][j] = t * W0 / W1;
+            }
+        return;
+    }
+    // Dbar2chi_iterative (matrix_utilities.f90:19-158) on the subsystem
+    const T* Xk = S.x;
+    T mw = T(0), Y[NS], Minv[NS], Mm[NS];
+#pragma unroll
+    for (int i = 0; i < NS; i++)
+        if (on(i)) mw = mw + Xk[i] * (T)m.molmass[i];
+#pragma unroll
+    for (int i = 0; i < NS; i++) {
+        Y[i] = on(i) ? (T)m.molmass[i] / mw * Xk[i] : T(0);
+        Mm[i] = T(0);
+        Minv[i] = T(0);
+        if (on(i)) {
+            T t2 = T(0);
+#pragma unroll
+            for (int j = 0; j < NS; j++)
+                if (j != i && on(j)) t2 = t2 + Xk[j] / (T)m.D[i][j];
+            const T Di = (T(1) - Y[i]) / t2;
+            Mm[i] = Xk[i] / Di;
+            Minv[i] = Di / Xk[i];
+        }
+    }
+    T J[NS][NS];
+#pragma unroll
+    for (int i = 0; i < NS; i++)
+#pragma unroll
+        for (int j = 0; j < NS; j++) {
+            J[i][j] = T(0);
+            if (!on(i) || !on(j)) continue;
+            T dl;
+            if (i == j) {
+                T t1 = T(0);
+#pragma unroll
+                for (int k = 0; k < NS; k++)
+                    if (k != i && on(k)) t1 = t1 + Xk[i] * Xk[k] / (T)m.D[i][k];
+                dl = t1;
+            } else {
+                dl = -Xk[i] * Xk[j] / (T)m.D[i][j];
+            }
+            T z = -dl;
+            if (i == j) z = z + Mm[i];
+            J[i][j] = Minv[i] * z;
+        }
+    T PJ[NS][NS], m2[NS][NS];
+#pragma unroll
+    for (int i = 0; i < NS; i++)
+#pragma unroll
+        for (int j = 0; j < NS; j++) {
+            T a = T(0), scr = T(0);
+            if (on(i) && on(j)) {
+#pragma unroll
+                for (int k = 0; k < NS; k++) {
+                    if (!on(k)) continue;
+                    const T pik = (i == k ? T(1) : T(0)) - Y[k];
+                    const T pjk = (j == k ? T(1) : T(0)) - Y[k];
+                    a = a + pik * J[k][j];
+                    scr = scr + pik * Minv[k] * pjk;
+                }
+            }
+            PJ[i][j] = a;
+            m2[i][j] = scr;
+            S.chi[i][j] = scr;
+        }
+    for (int it = 0; it < m.chi_it; it++) {
+        T m1[NS][NS];
+#pragma unroll
+        for (int i = 0; i < NS; i++)
+#pragma unroll
+            for (int j = 0; j < NS; j++) {
+                T scr = T(0);
+#pragma unroll
+                for (int k = 0; k < NS; k++)
+                    if (on(k)) scr = scr + PJ[i][k] * S.chi[k][j];
+                m1[i][j] = (on(i) && on(j)) ? scr + m2[i][j] : T(0);
+            }
+#pragma unroll
+        for (int i = 0; i < NS; i++)
+#pragma unroll
+            for (int j = 0; j < NS; j++) S.chi[i][j] = m1[i][j];
+    }
+}
+
+// compute_chi_sub's rho W chi (mass_flux_utilities.f90:698-738): the
+// subsystem's rho chi, and for a trace species' column its effective
+// diffusion coefficient terms
+template <typename T, int NS, class MX>
+__device__ __forceinline__ void d_rhowchi_sub(const MX& m, unsigned act, int nsub, const T* rho, T (&out)[NS][NS]) {
+    const auto on = [&](int i) { return (act >> i) & 1u; };
+    SubSys<T, NS> S;
+    d_subsys<T, NS, MX>(m, act, nsub, rho, S);
+#pragma unroll
+    for (int col = 0; col < NS; col++) {
+        if (!on(col)) {
+            T deff = T(0);
+#pragma unroll
+            for (int k = 0; k < NS; k++)
+                if (on(k)) deff = deff + S.x[k] / (T)m.D[k][col];
+            deff = T(1) / deff;
+#pragma unroll
+            for (int row = 0; row < NS; row++) {
+                if (row == col) {
+                    out[row][col] = S.rt * deff * (T)m.molmass[row] / S.mt;
+                } else if (!on(row)) {
+                    out[row][col] = T(0);
+                } else {
+                    T tmp = T(0);
+#pragma unroll
+                    for (int k = 0; k < NS; k++)
+                        if (on(k)) tmp = tmp + S.chi[row][k] * S.x[k] / (T)m.D[k][col];
+                    out[row][col] = deff * rho[row] * (tmp - (T)m.molmass[col] / S.mt);
+                }
+            }
+        } else {
+#pragma unroll
+            for (int row = 0; row < NS; row++) out[row][col] = on(row) ? rho[row] * S.chi[row][col] : T(0);
+        }
+    }
+}
+
+// compute_sqrtLonsager_sub (mass_flux_utilities.f90:1440-1500): the
+// Cholesky factor of the subsystem's Onsager matrix, expanded with zeros
+template <typename T, int NS, class MX>
+__device__ __forceinline__ void d_sqrtL_sub(const MX& m, unsigned act, int nsub, const T* rho, T (&L)[NS][NS]) {
+    const auto on = [&](int i) { return (act >> i) & 1u; };
+    SubSys<T, NS> S;
+    d_subsys<T, NS, MX>(m, act, nsub, rho, S);
+    T Ws[NS];
+#pragma unroll
+    for (int i = 0; i < NS; i++) Ws[i] = on(i) ? rho[i] / S.rt : T(0);
+    const T kB = (T)m.kB;
+#pragma unroll
+    for (int c = 0; c < NS; c++)
+#pragma unroll
+        for (int r = 0; r < NS; r++)
+            L[r][c] = (on(r) && on(c)) ? S.mt * S.rt * Ws[r] * S.chi[r][c] * Ws[c] / kB : T(0);
+    // choldc (matrix_utilities.f90:162-241) over the non-trace rows; the
+    // inner sums run downwards, as the reference's do
+    T p[NS];
+#pragma unroll
+    for (int i = 0; i < NS; i++) {
+        p[i] = T(0);
+        if (!on(i)) continue;
+        int ising = 0;
+#pragma unroll
+        for (int j = i; j < NS; j++) {
+            if (!on(j)) continue;
+            T s = L[i][j];
+#pragma unroll
+            for (int k = i - 1; k >= 0; k--)
+                if (on(k)) s = s - L[i][k] * L[j][k];
+            if (i == j) {
+                if (s <= T(0)) {
+                    p[i] = T(0);
+                    ising = 1;
+                } else {
+                    p[i] = sqrt(s);
+                }
+            } else {
+                L[j][i] = (ising == 0) ? s / p[i] : T(0);
+            }
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < NS; i++) {
+#pragma unroll
+        for (int j = i + 1; j < NS; j++) L[i][j] = T(0);
+        L[i][i] = p[i];
+    }
 }
 
 // molar concentrations and chi in the arithmetic of T
@@ -364,13 +613,26 @@ __device__ __forceinline__ void d_choldc(T (&a)[NS][NS]) {
     }
 }
 
+// Faces and cells with some but not all-but-one trace species take the
+// subsystem branch.  It is rare, and its registers would lower the
+// occupancy of the latency-bound main kernels, so those append the index to
+// a list and skip it; a follow-up kernel finishes exactly the listed ones.
+struct TraceList {
+    int* idx;          // capacity: one entry per cell of the level
+    unsigned* count;   // entries appended (cleared before each main kernel)
+};
+
+__device__ __forceinline__ void trace_push(const TraceList& tl, i64 f) {
+    const unsigned q = atomicAdd(tl.count, 1u);
+    tl.idx[q] = (int)f;
+}
+
 // ---------------------------------------------------------------------
 // per cell: rhoWchi (compute_rhoWchi_local) and the molar concentrations
 // ---------------------------------------------------------------------
 template <typename T, int NS>
 __global__ void __launch_bounds__(128, (sizeof(T) == 4 && NS <= 4) ? 8 : 1)
-    k_rhowchi(Grid g, MixDev m, const double* const* __restrict__ rho,
-                                                 T* const* rwc, T* const* xo, int* flag) {
+    k_rhowchi(Grid g, MixDev m, const double* const* __restrict__ rho, T* const* rwc, T* const* xo, TraceList tl) {
     const i64 n = g.nc;
     for (i64 f = blockIdx.x * (i64)blockDim.x + threadIdx.x; f < n; f += (i64)gridDim.x * blockDim.x) {
         T r[NS];
@@ -384,14 +646,15 @@ __global__ void __launch_bounds__(128, (sizeof(T) == 4 && NS <= 4) ? 8 : 1)
         d_molconc_t<T, NS>(m, r, rt, x, mt);
 #pragma unroll
         for (int s = 0; s < NS; s++) xo[s][f] = x[s];
-        const int nt = d_ntrace<T, NS>(m, r, rt);
-        if (nt == NS - 1) {
+        int na;
+        d_active<T, NS>(m, r, rt, &na);
+        if (na == 1) {
 #pragma unroll
             for (int q = 0; q < NS * NS; q++) rwc[q][f] = T(0);
             continue;
         }
-        if (nt != 0) {
-            atomicOr(flag, 1);
+        if (na != NS) {
+            trace_push(tl, f);
             continue;
         }
         T chi[NS][NS];
@@ -403,18 +666,182 @@ __global__ void __launch_bounds__(128, (sizeof(T) == 4 && NS <= 4) ? 8 : 1)
     }
 }
 
+// the listed cells of k_rhowchi: compute_chi_sub's rho W chi
+template <typename T, int NS>
+__global__ void __launch_bounds__(128) k_rhowchi_trace(MixDev m, const double* const* __restrict__ rho,
+                                                       T* const* rwc, TraceList tl) {
+    const unsigned cnt = *tl.count;
+    for (unsigned q = blockIdx.x * blockDim.x + threadIdx.x; q < cnt; q += gridDim.x * blockDim.x) {
+        const i64 f = tl.idx[q];
+        T r[NS];
+        T rt = T(0);
+#pragma unroll
+        for (int s = 0; s < NS; s++) {
+            r[s] = (T)rho[s][f];
+            rt = rt + r[s];
+        }
+        int na;
+        const unsigned act = d_active<T, NS>(m, r, rt, &na);
+        T a[NS][NS];
+        d_rhowchi_sub<T, NS>(m, act, na, r, a);
+#pragma unroll
+        for (int i = 0; i < NS; i++)
+#pragma unroll
+            for (int j = 0; j < NS; j++) rwc[i * NS + j][f] = a[i][j];
+    }
+}
+
+// compute_nonnegative_rho_av (mass_flux_utilities.f90:1231-1328) on the face
+// between cells fm and f, and the sum of the averages
+template <typename T, int NS>
+__device__ __forceinline__ void d_face_rho_av(const MixDev& m, const double* const* __restrict__ rho, i64 f, i64 fm,
+                                              T (&ra)[NS], T& rt) {
+    rt = T(0);
+#pragma unroll
+    for (int c = 0; c < NS; c++) {
+        T mm, v1, v2;
+        if constexpr (sizeof(T) == 4) {
+            mm = m.mm_f[c];
+            v1 = (float)ld(rho[c], fm) * m.imm_f[c];
+            v2 = (float)ld(rho[c], f) * m.imm_f[c];
+        } else {
+            mm = (T)m.molmass[c];
+            v1 = (T)ld(rho[c], fm) / mm;
+            v2 = (T)ld(rho[c], f) / mm;
+        }
+        T o;
+        if (m.avg_type == 2) {
+            o = mm * sqrt(fmax(v1, T(0)) * fmax(v2, T(0)));
+        } else if (m.avg_type == 3) {
+            o = (v1 <= T(0) || v2 <= T(0)) ? T(0) : mm * T(2) / (T(1) / v1 + T(1) / v2);
+        } else if (m.avg_type == 10) {
+            o = (v1 <= T(0) || v2 <= T(0)) ? T(0) : mm * (v1 + v2) / T(2);
+        } else {
+            if (v1 <= T(0) || v2 <= T(0)) {
+                o = T(0);
+            } else {
+                const T t1 = fmin((T)m.dV * v1, T(1)), t2 = fmin((T)m.dV * v2, T(1));
+                o = mm * (v1 + v2) / T(2) * t1 * t2;
+            }
+        }
+        ra[c] = o;
+        rt = rt + o;
+    }
+}
+
+// compute_sqrtLonsager_local (mass_flux_utilities.f90:1331-1522) without
+// trace species: chol(mtot rhotot W chi W / k_B)
+template <typename T, int NS>
+__device__ __forceinline__ void d_sqrtL_full(const MixDev& m, const T (&ra)[NS], T rt, T (&L)[NS][NS]) {
+    T Wf[NS], x[NS], mt;
+    d_molconc_t<T, NS>(m, ra, rt, x, mt);
+    T chi[NS][NS];
+    d_chi_t<T, NS>(m, ra, rt, x, chi);
+    if constexpr (sizeof(T) == 4) {
+        const float ri = frcp(rt);
+#pragma unroll
+        for (int i = 0; i < NS; i++) Wf[i] = ra[i] * ri;
+        const float fac = mt * rt * m.ikB_f;
+#pragma unroll
+        for (int c = 0; c < NS; c++)
+#pragma unroll
+            for (int r = 0; r < NS; r++) L[r][c] = fac * Wf[r] * chi[r][c] * Wf[c];
+        d_choldc_f<NS>(L);
+    } else {
+#pragma unroll
+        for (int i = 0; i < NS; i++) Wf[i] = ra[i] / rt;
+        const T kB = (T)m.kB;
+#pragma unroll
+        for (int c = 0; c < NS; c++)
+#pragma unroll
+            for (int r = 0; r < NS; r++) L[r][c] = mt * rt * Wf[r] * chi[r][c] * Wf[c] / kB;
+        d_choldc<T, NS>(L);
+    }
+}
+
+// the subsystem's factor (compute_sqrtLonsager_sub).  Its Onsager matrix is
+// singular (the rows sum to zero), so its last Cholesky pivot is a roundoff
+// residue.  In the full system that pivot only reaches the last species,
+// whose flux correction_flux replaces; in a subsystem it can belong to a
+// kept species, and its square root would be sqrt(FP32 eps) ~ 2e-4 of the
+// factor there.  So the subsystem factorises in FP64 in the
+// mixed-precision mode too.
+template <typename T, int NS>
+__device__ __forceinline__ void d_sqrtL_trace(const MixDev& m, unsigned act, int na, const T (&ra)[NS],
+                                              T (&L)[NS][NS]) {
+    double rd[NS], Ld[NS][NS];
+#pragma unroll
+    for (int i = 0; i < NS; i++) rd[i] = (double)ra[i];
+    d_sqrtL_sub<double, NS>(m, act, na, rd, Ld);
+#pragma unroll
+    for (int i = 0; i < NS; i++)
+#pragma unroll
+        for (int j = 0; j < NS; j++) L[i][j] = (T)Ld[i][j];
+}
+
+// every case of compute_sqrtLonsager_local on one face
+template <typename T, int NS>
+__device__ __forceinline__ void d_face_sqrtL(const MixDev& m, const double* const* __restrict__ rho, i64 f, i64 fm,
+                                             T (&L)[NS][NS]) {
+    T ra[NS], rt;
+    d_face_rho_av<T, NS>(m, rho, f, fm, ra, rt);
+    int na;
+    const unsigned act = d_active<T, NS>(m, ra, rt, &na);
+    if (na == 1) {
+#pragma unroll
+        for (int i = 0; i < NS; i++)
+#pragma unroll
+            for (int j = 0; j < NS; j++) L[i][j] = T(0);
+    } else if (na != NS) {
+        d_sqrtL_trace<T, NS>(m, act, na, ra, L);
+    } else {
+        d_sqrtL_full<T, NS>(m, ra, rt, L);
+    }
+}
+
+// stochastic_mass_fluxdiv.f90:70-102 on one face: variance * sqrtL * sum_r
+// w_r W_r, corrected (correction_flux.f90:17-226)
+template <typename T, int NS, int DIM>
+__device__ __forceinline__ void d_stoch_face(const MixDev& m, int d, i64 f, const T (&L)[NS][NS],
+                                             const double* const* __restrict__ W, int n_rngs, const double* wts,
+                                             T variance, T (&fs)[NS]) {
+    T w[NS];
+#pragma unroll
+    for (int s = 0; s < NS; s++) {
+        T acc = T(0);
+        for (int rr = 0; rr < n_rngs; rr++) acc = acc + (T)wts[rr] * (T)ld(W[(rr * DIM + d) * NS + s], f);
+        w[s] = acc;
+    }
+#pragma unroll
+    for (int r = 0; r < NS; r++) {
+        T acc = T(0);
+#pragma unroll
+        for (int c = 0; c < NS; c++) {
+            if constexpr (sizeof(T) == 4) acc = __fmaf_rn(L[r][c], w[c], acc);
+            else acc = acc + L[r][c] * w[c];
+        }
+        fs[r] = acc * variance;
+    }
+    if (m.correct && NS > 1) {
+        T sum = T(0);
+#pragma unroll
+        for (int s = 0; s < NS - 1; s++) sum = sum + fs[s];
+        fs[NS - 1] = -sum;
+    }
+}
+
 // ---------------------------------------------------------------------
 // per face of direction D (the low face of each cell): diffusive +
 // stochastic flux, corrected (correction_flux.f90:17-226)
 // ---------------------------------------------------------------------
 // (FP32 with up to 4 species: a 64-register cap for 8 CTAs = 32 warps per
-// SM to hide the dependent chains; 20 bytes of spills)
+// SM to hide the dependent chains)
 template <typename T, int NS, int DIM>
 __global__ void __launch_bounds__(128, (sizeof(T) == 4 && NS <= 4) ? 8 : 1)
     k_mass_flux(Grid g, MixDev m, int d, const double* const* __restrict__ rho,
-                                                   const T* const* __restrict__ rwc, const T* const* __restrict__ xc,
-                                                   const double* const* __restrict__ W, int n_rngs,
-                                                   const double* wts, T variance, T dxinv, T* const* flux, int* flag) {
+                const T* const* __restrict__ rwc, const T* const* __restrict__ xc,
+                const double* const* __restrict__ W, int n_rngs, const double* wts, T variance, T dxinv,
+                T* const* flux, TraceList tl) {
     Cell P;
     if (!cell_of_thread(g, P)) return;
     const i64 f = P.id(0, 0, 0);
@@ -447,100 +874,136 @@ __global__ void __launch_bounds__(128, (sizeof(T) == 4 && NS <= 4) ? 8 : 1)
 #pragma unroll
     for (int s = 0; s < NS; s++) fs[s] = T(0);
     if (m.var_mass != 0.0) {
-        // compute_nonnegative_rho_av (mass_flux_utilities.f90:1231-1328)
-        T ra[NS];
-        T rt = T(0);
-#pragma unroll
-        for (int c = 0; c < NS; c++) {
-            T mm, v1, v2;
-            if constexpr (sizeof(T) == 4) {
-                mm = m.mm_f[c];
-                v1 = (float)ld(rho[c], fm) * m.imm_f[c];
-                v2 = (float)ld(rho[c], f) * m.imm_f[c];
-            } else {
-                mm = (T)m.molmass[c];
-                v1 = (T)ld(rho[c], fm) / mm;
-                v2 = (T)ld(rho[c], f) / mm;
-            }
-            T o;
-            if (m.avg_type == 2) {
-                o = mm * sqrt(fmax(v1, T(0)) * fmax(v2, T(0)));
-            } else if (m.avg_type == 3) {
-                o = (v1 <= T(0) || v2 <= T(0)) ? T(0) : mm * T(2) / (T(1) / v1 + T(1) / v2);
-            } else if (m.avg_type == 10) {
-                o = (v1 <= T(0) || v2 <= T(0)) ? T(0) : mm * (v1 + v2) / T(2);
-            } else {
-                if (v1 <= T(0) || v2 <= T(0)) {
-                    o = T(0);
-                } else {
-                    const T t1 = fmin((T)m.dV * v1, T(1)), t2 = fmin((T)m.dV * v2, T(1));
-                    o = mm * (v1 + v2) / T(2) * t1 * t2;
-                }
-            }
-            ra[c] = o;
-            rt = rt + o;
+        T ra[NS], rt;
+        d_face_rho_av<T, NS>(m, rho, f, fm, ra, rt);
+        int na;
+        d_active<T, NS>(m, ra, rt, &na);
+        if (na == NS) {
+            T L[NS][NS];
+            d_sqrtL_full<T, NS>(m, ra, rt, L);
+            d_stoch_face<T, NS, DIM>(m, d, f, L, W, n_rngs, wts, variance, fs);
+        } else if (na != 1) {
+            // finished by k_mass_flux_trace, which adds the stochastic flux
+            trace_push(tl, f);
         }
-        // compute_sqrtLonsager_local (mass_flux_utilities.f90:1331-1522)
-        T L[NS][NS];
-        const int nt = d_ntrace<T, NS>(m, ra, rt);
-        if (nt == NS - 1) {
-#pragma unroll
-            for (int i = 0; i < NS; i++)
-#pragma unroll
-                for (int j = 0; j < NS; j++) L[i][j] = T(0);
-        } else {
-            if (nt != 0) atomicOr(flag, 1);
-            T Wf[NS], x[NS], mt;
-            d_molconc_t<T, NS>(m, ra, rt, x, mt);
-            T chi[NS][NS];
-            d_chi_t<T, NS>(m, ra, rt, x, chi);
-            if constexpr (sizeof(T) == 4) {
-                const float ri = frcp(rt);
-#pragma unroll
-                for (int i = 0; i < NS; i++) Wf[i] = ra[i] * ri;
-                const float fac = mt * rt * m.ikB_f;
-#pragma unroll
-                for (int c = 0; c < NS; c++)
-#pragma unroll
-                    for (int r = 0; r < NS; r++) L[r][c] = fac * Wf[r] * chi[r][c] * Wf[c];
-                d_choldc_f<NS>(L);
-            } else {
-#pragma unroll
-                for (int i = 0; i < NS; i++) Wf[i] = ra[i] / rt;
-                const T kB = (T)m.kB;
-#pragma unroll
-                for (int c = 0; c < NS; c++)
-#pragma unroll
-                    for (int r = 0; r < NS; r++) L[r][c] = mt * rt * Wf[r] * chi[r][c] * Wf[c] / kB;
-                d_choldc<T, NS>(L);
-            }
-        }
-        T w[NS];
-#pragma unroll
-        for (int s = 0; s < NS; s++) {
-            T acc = T(0);
-            for (int rr = 0; rr < n_rngs; rr++) acc = acc + (T)wts[rr] * (T)ld(W[(rr * DIM + d) * NS + s], f);
-            w[s] = acc;
-        }
-#pragma unroll
-        for (int r = 0; r < NS; r++) {
-            T acc = T(0);
-#pragma unroll
-            for (int c = 0; c < NS; c++) {
-                if constexpr (sizeof(T) == 4) acc = __fmaf_rn(L[r][c], w[c], acc);
-                else acc = acc + L[r][c] * w[c];
-            }
-            fs[r] = acc * variance;
-        }
-        if (m.correct && NS > 1) {
-            T sum = T(0);
-#pragma unroll
-            for (int s = 0; s < NS - 1; s++) sum = sum + fs[s];
-            fs[NS - 1] = -sum;
-        }
+        // na == 1: zero factor, no stochastic flux
     }
 #pragma unroll
     for (int s = 0; s < NS; s++) flux[d * NS + s][f] = fd[s] + fs[s];
+}
+
+// the listed faces of k_mass_flux: the stochastic flux through the
+// subsystem of non-trace species, added to the stored diffusive flux
+template <typename T, int NS, int DIM>
+__global__ void __launch_bounds__(128) k_mass_flux_trace(Grid g, MixDev m, int d, const double* const* __restrict__ rho,
+                                                         const double* const* __restrict__ W, int n_rngs,
+                                                         const double* wts, T variance, T* const* flux,
+                                                         TraceList tl) {
+    const unsigned cnt = *tl.count;
+    for (unsigned q = blockIdx.x * blockDim.x + threadIdx.x; q < cnt; q += gridDim.x * blockDim.x) {
+        const i64 f = tl.idx[q];
+        const int i = (int)(f % g.n[0]), j = (int)((f / g.n[0]) % g.n[1]), k = (int)(f / ((i64)g.n[0] * g.n[1]));
+        const int im = d == 0 ? (i == 0 ? g.n[0] - 1 : i - 1) : i;
+        const int jm = d == 1 ? (j == 0 ? g.n[1] - 1 : j - 1) : j;
+        const int km = d == 2 ? (k == 0 ? g.n[2] - 1 : k - 1) : k;
+        const i64 fm = (i64)im + (i64)g.n[0] * ((i64)jm + (i64)g.n[1] * km);
+        T ra[NS], rt;
+        d_face_rho_av<T, NS>(m, rho, f, fm, ra, rt);
+        int na;
+        const unsigned act = d_active<T, NS>(m, ra, rt, &na);
+        T L[NS][NS], fs[NS];
+        d_sqrtL_trace<T, NS>(m, act, na, ra, L);
+        d_stoch_face<T, NS, DIM>(m, d, f, L, W, n_rngs, wts, variance, fs);
+#pragma unroll
+        for (int s = 0; s < NS; s++) flux[d * NS + s][f] = flux[d * NS + s][f] + fs[s];
+    }
+}
+
+// ---------------------------------------------------------------------
+// the split form of the drop-in boundary: compute_sqrtLonsager_fc and
+// stochastic_mass_fluxdiv with the face factors materialised (FP64; the
+// pointer tables travel as kernel parameters)
+// ---------------------------------------------------------------------
+struct SqrtLArgs {
+    const double* rho[FHD_MAX_SPECIES];
+    double* out[FHD_MAX_SPECIES * FHD_MAX_SPECIES];  // this direction, entry (r, c) at r + ns*c
+};
+
+// compute_sqrtLonsager_fc (mass_flux_utilities.f90:1096-1229): every face
+// of direction d
+template <int NS>
+__global__ void __launch_bounds__(128) k_sqrtL_fc(Grid g, MixDev m, int d, SqrtLArgs a) {
+    Cell P;
+    if (!cell_of_thread(g, P)) return;
+    const i64 f = P.id(0, 0, 0);
+    const i64 fm = P.id(-(d == 0), -(d == 1), -(d == 2));
+    double L[NS][NS];
+    d_face_sqrtL<double, NS>(m, a.rho, f, fm, L);
+#pragma unroll
+    for (int r = 0; r < NS; r++)
+#pragma unroll
+        for (int c = 0; c < NS; c++) a.out[r + NS * c][f] = L[r][c];
+}
+
+struct StochMassArgs {
+    const double* L[FHD_MAX_SPECIES * FHD_MAX_SPECIES];  // this direction's factors, (r, c) at r + ns*c
+    const double* W[4 * FHD_MAX_SPECIES];                 // this direction's fields, [rr*ns + s]
+    double wts[4];
+    double* flux[FHD_MAX_SPECIES];                        // this direction's flux
+};
+
+// stochastic_mass_fluxdiv.f90:70-102: flux = variance * sqrtL (sum_r w_r W_r)
+// (setval, saxpy per stage, matvec_mul, scaling), then correction_flux
+template <int NS>
+__global__ void __launch_bounds__(256) k_stoch_mass_flux(Grid g, MixDev m, int n_rngs, double variance,
+                                                         StochMassArgs a) {
+    Cell P;
+    if (!cell_of_thread(g, P)) return;
+    const i64 f = P.id(0, 0, 0);
+    double w[NS], fs[NS];
+#pragma unroll
+    for (int s = 0; s < NS; s++) {
+        double acc = 0.0;
+        for (int rr = 0; rr < n_rngs; rr++) acc = acc + a.wts[rr] * ld(a.W[rr * NS + s], f);
+        w[s] = acc;
+    }
+#pragma unroll
+    for (int r = 0; r < NS; r++) {
+        double acc = 0.0;
+#pragma unroll
+        for (int c = 0; c < NS; c++) acc = acc + ld(a.L[r + NS * c], f) * w[c];
+        fs[r] = acc * variance;
+    }
+    if (m.correct && NS > 1) {
+        double sum = 0.0;
+#pragma unroll
+        for (int s = 0; s < NS - 1; s++) sum = sum + fs[s];
+        fs[NS - 1] = -sum;
+    }
+#pragma unroll
+    for (int s = 0; s < NS; s++) a.flux[s][f] = fs[s];
+}
+
+struct DivArgs {
+    const double* flux[3 * FHD_MAX_SPECIES];  // [d*ns + s]
+    double* out[FHD_MAX_SPECIES];
+};
+
+// compute_div (div_and_grad.f90:884-1035) of every species' face flux,
+// overwriting or (increment) adding to out in the reference's order
+template <int NS, int DIM>
+__global__ void __launch_bounds__(256) k_species_div(Grid g, double dxinv, int increment, DivArgs a) {
+    Cell P;
+    if (!cell_of_thread(g, P)) return;
+    const i64 f = P.id(0, 0, 0);
+#pragma unroll
+    for (int s = 0; s < NS; s++) {
+        const double x = (ld(a.flux[0 * NS + s], P.id(1, 0, 0)) - ld(a.flux[0 * NS + s], f)) * dxinv;
+        const double y = (ld(a.flux[1 * NS + s], P.id(0, 1, 0)) - ld(a.flux[1 * NS + s], f)) * dxinv;
+        double v = increment ? a.out[s][f] + x + y : x + y;
+        if constexpr (DIM == 3) v = v + (ld(a.flux[2 * NS + s], P.id(0, 0, 1)) - ld(a.flux[2 * NS + s], f)) * dxinv;
+        a.out[s][f] = v;
+    }
 }
 
 // fluxdiv_s = div(flux_s)  (compute_div, div_and_grad.f90:884-1035)
@@ -570,8 +1033,8 @@ struct MassBufs {
     void* xc = nullptr;    // ns arrays of T
     void* flux = nullptr;  // dim*ns arrays of T
     void** tab = nullptr;  // device pointer tables
-    int* flag = nullptr;
     double* wts = nullptr;
+    TraceList tl{nullptr, nullptr};  // deferred trace cells / faces
 };
 
 template <typename T>
@@ -587,18 +1050,18 @@ static int mass_alloc(fhd_ctx* ctx, MassBufs& B, int ns) {
     T* xc = ctx->arena.alloc<T>((i64)ns * nc);
     T* fl = ctx->arena.alloc<T>((i64)dim * ns * nc);
     void** tab = (void**)ctx->arena.alloc<double>(4 * 128);
-    int* flag = (int*)ctx->arena.alloc<double>(1);
     double* wts = ctx->arena.alloc<double>(8);
-    if (!rw || !xc || !fl || !tab || !flag || !wts) return FHD_ERR_OOM;
+    int* tidx = (int*)ctx->arena.alloc<float>(nc);
+    unsigned* tcnt = (unsigned*)ctx->arena.alloc<double>(1);
+    if (!rw || !xc || !fl || !tab || !wts || !tidx || !tcnt) return FHD_ERR_OOM;
+    B.tl = TraceList{tidx, tcnt};
     B.rwc = rw;
     B.xc = xc;
     B.flux = fl;
     B.tab = tab;
-    B.flag = flag;
     B.wts = wts;
     B.ns = ns;
     B.ready = true;
-    FHD_CUDA_TRY(cudaMemsetAsync(flag, 0, sizeof(int), ctx->stream));
     return 0;
 }
 
@@ -629,19 +1092,29 @@ static int mass_fluxdiv_T(fhd_ctx* ctx, MassBufs& B, const MixDev& m, const doub
     const double* const* d_W = (const double* const*)(B.tab + 384);
     double* const* d_out = (double* const*)(B.tab + 384 + 96);
     const int nb = flat_blocks(nc);
-    k_rhowchi<T, NS><<<nb, 128, 0, st>>>(g, m, d_rho, d_rwc, d_xc, B.flag);
+    // the follow-up kernels of the deferred trace cells and faces: a few
+    // blocks, which leave at once when the list is empty
+    const int nbt = 2 * ctx->sms;
+    FHD_CUDA_TRY(cudaMemsetAsync(B.tl.count, 0, sizeof(unsigned), st));
+    k_rhowchi<T, NS><<<nb, 128, 0, st>>>(g, m, d_rho, d_rwc, d_xc, B.tl);
+    ctx->launches++;
+    FHD_CUDA_TRY(cudaPeekAtLastError());
+    k_rhowchi_trace<T, NS><<<nbt, 128, 0, st>>>(m, d_rho, d_rwc, B.tl);
     ctx->launches++;
     FHD_CUDA_TRY(cudaPeekAtLastError());
     const T variance = (T)sqrt(2.0 * m.kB * m.var_mass / (m.dV * dt));
     const T dxinv = (T)(1.0 / ctx->dx);
     for (int d = 0; d < dim; d++) {
+        FHD_CUDA_TRY(cudaMemsetAsync(B.tl.count, 0, sizeof(unsigned), st));
         with_dim(dim, [&](auto D) {
             constexpr int DIM = decltype(D)::value;
             k_mass_flux<T, NS, DIM><<<dim3((g.n[0] + 31) / 32, (g.n[1] + 3) / 4, g.n[2]), dim3(32, 4, 1), 0, st>>>(
                 g, m, d, d_rho, (const T* const*)d_rwc, (const T* const*)d_xc, d_W, n_rngs, B.wts, variance, dxinv,
-                d_flux, B.flag);
+                d_flux, B.tl);
+            k_mass_flux_trace<T, NS, DIM><<<nbt, 128, 0, st>>>(g, m, d, d_rho, d_W, n_rngs, B.wts, variance, d_flux,
+                                                               B.tl);
         });
-        ctx->launches++;
+        ctx->launches += 2;
         FHD_CUDA_TRY(cudaPeekAtLastError());
     }
     with_dim(dim, [&](auto D) {
@@ -710,8 +1183,8 @@ static MassBufs& mass_bufs(fhd_ctx* ctx) {
     return *b;
 }
 
-// compute_mass_fluxdiv on the context's stream; the trace-species flag is
-// checked by the caller after synchronising
+// compute_mass_fluxdiv on the context's stream (trace species are handled
+// per face and cell by the non-trace subsystem)
 int mass_fluxdiv(fhd_ctx* ctx, const fhd_mixture_params* mp, const fhd_stoch_params* sp, const double* const rho[],
                  double dt, const double* weights, int n_rngs, const double* const W[], double* const fluxdiv[]) {
     if (!mp || mp->nspecies < 2 || mp->nspecies > 5 || n_rngs < 1 || n_rngs > 4) {
@@ -727,27 +1200,130 @@ int mass_fluxdiv(fhd_ctx* ctx, const fhd_mixture_params* mp, const fhd_stoch_par
     return mass_fluxdiv_dispatch<double>(ctx, B, m, rho, dt, weights, n_rngs, W, fluxdiv);
 }
 
-int mass_flag_check(fhd_ctx* ctx) {
-    MassBufs& B = mass_bufs(ctx);
-    if (!B.ready) return 0;
-    int h = 0;
-    FHD_CUDA_TRY(cudaMemcpyAsync(&h, B.flag, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
-    FHD_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
-    if (h) {
-        FHD_CUDA_TRY(cudaMemsetAsync(B.flag, 0, sizeof(int), ctx->stream));
-        set_last_error("mass fluxes: trace species (mass fraction below fraction_tolerance) are not supported");
+}  // namespace fhd
+
+namespace fhd {
+template <int NS>
+static int sqrtL_fc_T(fhd_ctx* ctx, const MixDev& m, const double* const rho[], double* const sqrtL[]) {
+    const Grid g = ctx->g0;
+    for (int d = 0; d < ctx->dim; d++) {
+        SqrtLArgs a;
+        memset(&a, 0, sizeof(a));
+        for (int s = 0; s < NS; s++) a.rho[s] = rho[s];
+        for (int q = 0; q < NS * NS; q++) a.out[q] = sqrtL[d * NS * NS + q];
+        k_sqrtL_fc<NS><<<dim3((g.n[0] + 31) / 32, (g.n[1] + 3) / 4, g.n[2]), dim3(32, 4, 1), 0, ctx->stream>>>(g, m,
+                                                                                                           d, a);
+        ctx->launches++;
+        FHD_CUDA_TRY(cudaPeekAtLastError());
+    }
+    return 0;
+}
+
+template <int NS>
+static int stoch_mass_T(fhd_ctx* ctx, const MixDev& m, const double* const sqrtL[], double dt, const double* weights,
+                        int n_rngs, const double* const W[], int increment, double* const div[],
+                        double* const flux[]) {
+    const Grid g = ctx->g0;
+    const int dim = ctx->dim;
+    const double variance = sqrt(2.0 * m.kB * m.var_mass / (m.dV * dt));
+    for (int d = 0; d < dim; d++) {
+        StochMassArgs a;
+        memset(&a, 0, sizeof(a));
+        for (int q = 0; q < NS * NS; q++) a.L[q] = sqrtL[d * NS * NS + q];
+        for (int rr = 0; rr < n_rngs; rr++)
+            for (int sp = 0; sp < NS; sp++) a.W[rr * NS + sp] = W[(rr * dim + d) * NS + sp];
+        for (int rr = 0; rr < n_rngs; rr++) a.wts[rr] = weights[rr];
+        for (int sp = 0; sp < NS; sp++) a.flux[sp] = flux[d * NS + sp];
+        k_stoch_mass_flux<NS><<<cell_grid(g), cell_block(), 0, ctx->stream>>>(g, m, n_rngs, variance, a);
+        ctx->launches++;
+        FHD_CUDA_TRY(cudaPeekAtLastError());
+    }
+    DivArgs a;
+    memset(&a, 0, sizeof(a));
+    for (int q = 0; q < dim * NS; q++) a.flux[q] = flux[q];
+    for (int sp = 0; sp < NS; sp++) a.out[sp] = div[sp];
+    const double dxinv = 1.0 / ctx->dx;
+    with_dim(dim, [&](auto D) {
+        constexpr int DIM = decltype(D)::value;
+        k_species_div<NS, DIM><<<cell_grid(g), cell_block(), 0, ctx->stream>>>(g, dxinv, increment, a);
+    });
+    ctx->launches++;
+    FHD_CUDA_TRY(cudaPeekAtLastError());
+    return 0;
+}
+
+static int check_mix(const fhd_mixture_params* mp) {
+    if (!mp || mp->nspecies < 2 || mp->nspecies > 5) {
+        set_last_error("mass fluxes: nspecies must be 2..5");
         return FHD_ERR_UNSUPPORTED;
     }
     return 0;
 }
 }  // namespace fhd
 
+extern "C" int fhd_dev_compute_sqrtLonsager_fc(fhd_ctx* ctx, const fhd_mixture_params* mp,
+                                               const fhd_stoch_params* sp, const double* const rho[],
+                                               double* const sqrtLonsager_fc[]) {
+    if (!ctx || !mp || !sp || !rho || !sqrtLonsager_fc) return FHD_ERR_BAD_ARG;
+    if (int rc = check_mix(mp)) return rc;
+    const MixDev m = make_mixdev(mp, sp);
+    int rc;
+    switch (m.ns) {
+        case 2: rc = sqrtL_fc_T<2>(ctx, m, rho, sqrtLonsager_fc); break;
+        case 3: rc = sqrtL_fc_T<3>(ctx, m, rho, sqrtLonsager_fc); break;
+        case 4: rc = sqrtL_fc_T<4>(ctx, m, rho, sqrtLonsager_fc); break;
+        default: rc = sqrtL_fc_T<5>(ctx, m, rho, sqrtLonsager_fc); break;
+    }
+    if (rc < 0) return rc;
+    FHD_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    return 0;
+}
+
+extern "C" int fhd_dev_stochastic_mass_fluxdiv(fhd_ctx* ctx, const fhd_mixture_params* mp,
+                                               const fhd_stoch_params* sp, const double* const sqrtLonsager_fc[],
+                                               double dt, const double* weights, int n_rngs,
+                                               const double* const W_fc[], int increment,
+                                               double* const stoch_mass_fluxdiv[],
+                                               double* const stoch_mass_flux[]) {
+    if (!ctx || !mp || !sp || !sqrtLonsager_fc || !weights || !W_fc || !stoch_mass_fluxdiv || !(dt > 0.0))
+        return FHD_ERR_BAD_ARG;
+    if (n_rngs < 1 || n_rngs > 4) {
+        set_last_error("stochastic_mass_fluxdiv: n_rngs must be 1..4");
+        return FHD_ERR_UNSUPPORTED;
+    }
+    if (int rc = check_mix(mp)) return rc;
+    const MixDev m = make_mixdev(mp, sp);
+    const int ns = m.ns, dim = ctx->dim;
+    // the face flux: the caller's arrays, or stream-ordered scratch
+    double* own = nullptr;
+    double* fl[3 * FHD_MAX_SPECIES];
+    if (stoch_mass_flux) {
+        for (int q = 0; q < dim * ns; q++) fl[q] = stoch_mass_flux[q];
+    } else {
+        FHD_CUDA_TRY(cudaMallocAsync((void**)&own, sizeof(double) * (size_t)ctx->g0.nc * dim * ns, ctx->stream));
+        for (int q = 0; q < dim * ns; q++) fl[q] = own + (i64)q * ctx->g0.nc;
+    }
+    int rc;
+    switch (ns) {
+        case 2: rc = stoch_mass_T<2>(ctx, m, sqrtLonsager_fc, dt, weights, n_rngs, W_fc, increment, stoch_mass_fluxdiv, fl); break;
+        case 3: rc = stoch_mass_T<3>(ctx, m, sqrtLonsager_fc, dt, weights, n_rngs, W_fc, increment, stoch_mass_fluxdiv, fl); break;
+        case 4: rc = stoch_mass_T<4>(ctx, m, sqrtLonsager_fc, dt, weights, n_rngs, W_fc, increment, stoch_mass_fluxdiv, fl); break;
+        default: rc = stoch_mass_T<5>(ctx, m, sqrtLonsager_fc, dt, weights, n_rngs, W_fc, increment, stoch_mass_fluxdiv, fl); break;
+    }
+    if (own) cudaFreeAsync(own, ctx->stream);
+    if (rc < 0) return rc;
+    FHD_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    return 0;
+}
+
 extern "C" int fhd_dev_compute_mass_fluxdiv(fhd_ctx* ctx, const fhd_mixture_params* mp, const fhd_stoch_params* sp,
                                             const double* const rho[], double dt, const double* weights, int n_rngs,
                                             const double* const W_fc[], double* const out[]) {
     if (!ctx || !mp || !sp || !rho || !weights || !W_fc || !out) return FHD_ERR_BAD_ARG;
-    int rc = fhd::mass_fluxdiv(ctx, mp, sp, rho, dt, weights, n_rngs, W_fc, out);
-    if (rc) return rc;
-    return mass_flag_check(ctx);
+    const int rc = fhd::mass_fluxdiv(ctx, mp, sp, rho, dt, weights, n_rngs, W_fc, out);
+    if (rc < 0) return rc;
+    // like every device entry point, the call returns with its work done
+    FHD_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    return rc;
 }
 #endif  // FHD_MASS_F32_TU

@@ -13,14 +13,12 @@
 // that loads this library holds it until the process exits.
 //
 // In host code the array's name is only a host-side handle: its device
-// address is looked up once per device, with that device current, through
-// cudaGetSymbolAddress, and passed to the kernels.
+// address is looked up on every call, with the caller's device current,
+// through cudaGetSymbolAddress, and passed to the kernels.
 //
 // All calls share the one array and it keeps the contents of the last call:
 // each call clears what must start at zero, and calls whose work overlaps on
 // the GPU (on different streams, or from different host threads) race on it.
-#include <mutex>
-
 #include "fhd_solver.cuh"
 
 namespace fhd {
@@ -28,34 +26,22 @@ namespace {
 
 constexpr long long NA_DOUBLES = (long long)FHD_NOALLOC_SCRATCH_BYTES / 8;
 constexpr int NA_MAX_LEVELS = 32;
-constexpr int NA_MAX_DEVICES = 64;
 constexpr long long NA_RED = 2048;  // reduction partials, counter, results
 
 __device__ __align__(256) double g_noalloc_scratch[NA_DOUBLES];
 
-std::mutex g_na_mu;
-double* g_na_addr[NA_MAX_DEVICES] = {nullptr};
-
-// device address of the scratch array on the current device (looked up on
-// the first call made with that device current)
+// device address of the scratch array on the current device.  It is looked
+// up on every call, with the caller's device current: the lookup is cheap,
+// and an address kept from an earlier call would be stale after the host
+// reset the device (cudaDeviceReset) and the module was loaded again.
 int scratch_address(double** out) {
-    int dev = 0;
-    FHD_CUDA_TRY(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= NA_MAX_DEVICES) {
-        set_last_error("stag_mg_solver_noalloc: device index out of range");
-        return FHD_ERR_BAD_ARG;
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || p == nullptr) {
+        set_last_error(std::string("cudaGetSymbolAddress(noalloc scratch): ") + cudaGetErrorString(e));
+        return FHD_ERR_CUDA;
     }
-    std::lock_guard<std::mutex> lk(g_na_mu);
-    if (!g_na_addr[dev]) {
-        void* p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess || p == nullptr) {
-            set_last_error(std::string("cudaGetSymbolAddress(noalloc scratch): ") + cudaGetErrorString(e));
-            return FHD_ERR_CUDA;
-        }
-        g_na_addr[dev] = (double*)p;
-    }
-    *out = g_na_addr[dev];
+    *out = (double*)p;
     return 0;
 }
 

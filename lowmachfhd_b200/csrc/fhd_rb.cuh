@@ -53,6 +53,7 @@ struct RBXGeom {
     int ahead;    // stages in flight beyond the one awaited
     int per_sm;   // resident CTAs per SM the z-run split assumes
     int threads;  // compute threads (256 or 512)
+    int vw = 1;   // cells per thread and row: 1, or 2 in the two-cell form
 };
 
 struct RBGeom {

@@ -511,6 +511,10 @@ static int stag_rbx_smooth(fhd_ctx* ctx, StagLevel<float>& L, const RBXGeom& G, 
     if (G.ahead == 1) {
         if (int rc = rb_allow_smem(k_stag_rbx<1>, G.smem, true)) return rc;
         k_stag_rbx<1><<<grd, RBX_BLOCK, G.smem, ctx->stream>>>(L.g, G, L.op(), R, (float)ctx->p.stag_mg_omega);
+    } else if (G.vw == 2) {
+        if (int rc = rb_allow_smem(k_stag_rbx<RBX_AHEAD, RBX_THREADS, 2>, G.smem)) return rc;
+        k_stag_rbx<RBX_AHEAD, RBX_THREADS, 2><<<grd, RBX_BLOCK, G.smem, ctx->stream>>>(L.g, G, L.op(), R,
+                                                                                   (float)ctx->p.stag_mg_omega);
     } else if (G.threads == 512) {
         if (int rc = rb_allow_smem(k_stag_rbx<RBX_AHEAD, 512>, G.smem)) return rc;
         k_stag_rbx<RBX_AHEAD, 512><<<grd, 512 + 32, G.smem, ctx->stream>>>(L.g, G, L.op(), R,
@@ -928,13 +932,24 @@ static std::mutex g_tune_mu;  // held while a context tunes
 static std::map<std::string, SmoothPlan> g_tune;
 static std::map<std::string, int> g_tune_import;  // imported choices (candidate index) not yet used
 
+// A plan is keyed by the level shape and by what decides the candidate
+// list: the device's SM count and shared-memory limits, and the version of
+// the candidate lists (bumped whenever a list or its order changes), so a
+// table from another GPU model or library version selects nothing.
+constexpr int TUNE_CANDS_VERSION = 3;
+
+static std::string tune_key_of(int dev, int which, int elem, int dim, int visc, const int n[3], int sms, int optin,
+                               int smem_sm) {
+    char b[200];
+    snprintf(b, sizeof b, "v%d:%d:%c:%d:%d:%d:%dx%dx%d:%d:%d:%d", TUNE_CANDS_VERSION, dev, which ? 'c' : 's', elem, dim,
+             which ? 0 : visc, n[0], n[1], n[2], sms, optin, smem_sm);
+    return b;
+}
+
 static std::string tune_key(fhd_ctx* ctx, const Grid& g, int which, int elem) {
     int dev = 0;
     cudaGetDevice(&dev);
-    char b[160];
-    snprintf(b, sizeof b, "%d:%c:%d:%d:%d:%dx%dx%d", dev, which ? 'c' : 's', elem, g.dim, which ? 0 : ctx->visc,
-             g.n[0], g.n[1], g.n[2]);
-    return b;
+    return tune_key_of(dev, which, elem, g.dim, ctx->visc, g.n, ctx->sms, ctx->smem_optin, ctx->smem_sm);
 }
 
 static void colour_cands(std::vector<SmoothPlan>& v, const Grid& g) {
@@ -977,11 +992,14 @@ static std::vector<SmoothPlan> stag_cands(fhd_ctx* ctx, const StagLevel<T>& L) {
     colour_cands(v, L.g);
     rb_cands(v, L.g, 3, (int)sizeof(T), 2, ctx->smem_optin);
     if (std::is_same<T, float>::value && ctx->visc == 1)
-        for (int form = 0; form < 3; form++)  // deep ring; short ring, two CTAs per SM; deep ring, 512 threads
+        // deep ring; short ring, two CTAs per SM; deep ring, 512 threads;
+        // deep ring, two cells per thread and row
+        for (int form = 0; form < 4; form++)
             for (int ty = 4; ty <= 32; ty *= 2) {
                 RBXGeom X;
                 const int ahead = form == 1 ? 1 : RBX_AHEAD, nt = form == 2 ? 512 : RBX_THREADS;
-                if (!rbx_geom(L.g, ctx->sms, (size_t)ctx->smem_optin, X, ty, ahead, (size_t)ctx->smem_sm, nt))
+                const int vw = form == 3 ? 2 : 1;
+                if (!rbx_geom(L.g, ctx->sms, (size_t)ctx->smem_optin, X, ty, ahead, (size_t)ctx->smem_sm, nt, vw))
                     continue;
                 SmoothPlan p;
                 p.kind = 2;
@@ -2151,17 +2169,39 @@ int fhd_tune_import(const char* text) {
         const std::string key = line.substr(0, sp), num = line.substr(sp + 1);
         if (num.empty() || num.size() > 4 || num.find_first_not_of("0123456789") != std::string::npos)
             return FHD_ERR_BAD_ARG;
-        // device:which:element size:dim:visc_type:extents, as the tuner writes them
-        int dev, elem, dim, visc, n0, n1, n2;
+        // version:device:which:element size:dim:visc_type:extents:SMs:shared
+        // memory per block (opt-in):per SM, as the tuner writes them
+        int ver, dev, elem, dim, visc, n0, n1, n2, sms, optin, smsm;
         char which;
-        if (sscanf(key.c_str(), "%d:%c:%d:%d:%d:%dx%dx%d", &dev, &which, &elem, &dim, &visc, &n0, &n1, &n2) != 8 ||
+        if (sscanf(key.c_str(), "v%d:%d:%c:%d:%d:%d:%dx%dx%d:%d:%d:%d", &ver, &dev, &which, &elem, &dim, &visc, &n0,
+                   &n1, &n2, &sms, &optin, &smsm) != 12 ||
             (which != 's' && which != 'c') || (elem != 4 && elem != 8) || (dim != 2 && dim != 3))
             return FHD_ERR_BAD_ARG;
+        // a line of another candidate-list version is well formed but names
+        // plans of other lists: it is skipped
+        if (ver != TUNE_CANDS_VERSION) continue;
         got[key] = atoi(num.c_str());
     }
     std::lock_guard<std::mutex> lk(g_tune_mu);
     for (const auto& kv : got) g_tune_import[kv.first] = kv.second;
     return (int)got.size();
+}
+
+long long fhd_tune_key(int which, int dim, const int n_cells[3], int precision_mode, int visc_type, int sms,
+                       int smem_optin, int smem_sm, int device, char* buf, long long len) {
+    if ((which != 0 && which != 1) || (dim != 2 && dim != 3) || !n_cells || sms < 1 || smem_optin < 1 ||
+        smem_sm < 1 || device < 0)
+        return FHD_ERR_BAD_ARG;
+    int n[3] = {n_cells[0], n_cells[1], dim == 3 ? n_cells[2] : 1};
+    const std::string k = tune_key_of(device, which, precision_mode == FHD_PREC_MIXED ? 4 : 8, dim, visc_type, n, sms,
+                                      smem_optin, smem_sm);
+    const long long need = (long long)k.size() + 1;
+    if (buf && len > 0) {
+        const long long m = need <= len ? need - 1 : len - 1;
+        memcpy(buf, k.data(), (size_t)m);
+        buf[m] = '\0';
+    }
+    return need;
 }
 
 int fhd_tune_candidates(int which, int dim, const int n_cells[3], int precision_mode, int visc_type, int sms,
@@ -2204,7 +2244,7 @@ int fhd_tune_candidates(int which, int dim, const int n_cells[3], int precision_
     for (int i = 0; i < (int)v.size() && i < max_out; i++) {
         const SmoothPlan& P = v[i];
         int* o = out + 7 * i;
-        o[0] = P.kind;
+        o[0] = (P.kind == 2 && P.rbx.vw == 2) ? 3 : P.kind;
         o[1] = P.kind == 0 ? P.bx : P.kind == 1 ? P.rb.TX : g.n[0];
         o[2] = P.kind == 0 ? P.by : P.kind == 1 ? P.rb.TY : P.rbx.TY;
         o[3] = P.kind == 1 ? P.rb.chunks : P.kind == 2 ? P.rbx.chunks : 0;
@@ -2226,7 +2266,8 @@ int fhd_ctx_tune_info(fhd_ctx* c, int which, int level, int* kind, int* ncand, d
         if (which == 1 && level < (int)c->mg64.c.size()) P = &c->mg64.c[level].plan;
     }
     if (!P) return FHD_ERR_BAD_ARG;
-    if (kind) *kind = P->kind;
+    // kind 3 reports the two-cell form of the row-tile smooth
+    if (kind) *kind = (P->kind == 2 && P->rbx.vw == 2) ? 3 : P->kind;
     if (ncand) *ncand = P->ncand;
     if (pair_us) *pair_us = P->us;
     if (shape) {
@@ -2335,19 +2376,60 @@ int fhd_dev_gmres(fhd_ctx* ctx, const double* const b_u[], const double* b_p, do
     if (!rc) rc = check_ptrs(ctx, (const void* const*)beta_ed, nE_of(ctx));
     if (!rc && (!b_p || !x_p || !beta || !gamma)) rc = FHD_ERR_BAD_ARG;
     if (rc) return rc;
-    if (ctx->p.scale_factor != 1.0) {
-        set_last_error("gmres: scale_factor != 1 is not supported");
-        return FHD_ERR_UNSUPPORTED;
+    // scale_factor (gmres.f90:118-135, 442-459): solve for scale*x_p with
+    // theta_alpha, b_u and the viscosities scaled.  The reference scales the
+    // caller's multifabs in place and unscales them on exit; here the scaled
+    // operands are private stream-ordered copies, so the caller's b_u, beta,
+    // gamma and beta_ed are not touched.  x_p is scaled in place and
+    // unscaled by the reference's multiplication with 1/scale_factor.
+    const double sf = ctx->p.scale_factor;
+    if (!(sf > 0.0) && !(sf < 0.0)) {
+        set_last_error("gmres: scale_factor must be non-zero");
+        return FHD_ERR_BAD_ARG;
     }
-    rc = prepare(ctx, alpha_fc, beta, beta_ed, gamma, theta_alpha);
-    if (rc) return rc;
+    const int dim = ctx->dim, nE = nE_of(ctx);
+    const i64 nc = ctx->g0.nc;
+    cudaStream_t st = ctx->stream;
+    const double* bu_s[3] = {b_u[0], dim > 1 ? b_u[1] : nullptr, dim > 2 ? b_u[2] : nullptr};
+    const double* bed_s[3] = {beta_ed[0], nE > 1 ? beta_ed[1] : nullptr, nE > 2 ? beta_ed[2] : nullptr};
+    const double *beta_s = beta, *gamma_s = gamma;
+    double theta = theta_alpha;
+    double* own = nullptr;
+    const int nb = flat_blocks(nc);
+    if (sf != 1.0) {
+        FHD_CUDA_TRY(cudaMallocAsync((void**)&own, sizeof(double) * (size_t)nc * (dim + 2 + nE), st));
+        int slot = 0;
+        auto scaled = [&](const double* in) {
+            double* o = own + (i64)(slot++) * nc;
+            k_copy_conv<double, double><<<nb, 256, 0, st>>>(nc, o, in, sf);
+            ctx->launches++;
+            return (const double*)o;
+        };
+        theta = theta * sf;
+        k_copy_conv<double, double><<<nb, 256, 0, st>>>(nc, x_p, x_p, sf);
+        ctx->launches++;
+        for (int c = 0; c < dim; c++) bu_s[c] = scaled(b_u[c]);
+        beta_s = scaled(beta);
+        gamma_s = scaled(gamma);
+        for (int e = 0; e < nE; e++) bed_s[e] = scaled(beta_ed[e]);
+        FHD_CUDA_TRY(cudaPeekAtLastError());
+    }
+    rc = prepare(ctx, alpha_fc, beta_s, bed_s, gamma_s, theta);
     CSVec<double> b;
     SVec<double> x;
     for (int c = 0; c < 4; c++) { b.c[c] = nullptr; x.c[c] = nullptr; }
-    for (int c = 0; c < ctx->dim; c++) { b.c[c] = b_u[c]; x.c[c] = x_u[c]; }
-    b.c[ctx->dim] = b_p;
-    x.c[ctx->dim] = x_p;
-    return finish(ctx, gmres_dev(ctx, b, x, norm_pre_rhs, stats));
+    for (int c = 0; c < dim; c++) { b.c[c] = bu_s[c]; x.c[c] = x_u[c]; }
+    b.c[dim] = b_p;
+    x.c[dim] = x_p;
+    if (!rc) rc = gmres_dev(ctx, b, x, norm_pre_rhs, stats);
+    if (sf != 1.0) {
+        if (rc >= 0) {
+            k_copy_conv<double, double><<<nb, 256, 0, st>>>(nc, x_p, x_p, 1.0 / sf);
+            ctx->launches++;
+        }
+        cudaFreeAsync(own, st);
+    }
+    return finish(ctx, rc);
 }
 
 }  // extern "C"

@@ -311,5 +311,4 @@ int sync_scalars(fhd_ctx* ctx, int first, int count);
 int dev_err_check(fhd_ctx* ctx);
 int mass_fluxdiv(fhd_ctx* ctx, const fhd_mixture_params* mp, const fhd_stoch_params* sp, const double* const rho[],
                  double dt, const double* weights, int n_rngs, const double* const W[], double* const fluxdiv[]);
-int mass_flag_check(fhd_ctx* ctx);
 }  // namespace fhd

@@ -588,7 +588,6 @@ int advance_inertial_ms(fhd_ctx* ctx, const fhd_stoch_params* sp, const fhd_mixt
     if (st2 < 0) return st2;
     if ((rc = lin(ctx, u, 1, {{1.0, cs(du)}}))) return rc;
     if ((rc = lin_n(ctx, 1, one(pi), 1, {{1.0, cs(one(dpi))}}))) return rc;
-    if (mp && (rc = mass_flag_check(ctx))) return rc;
     FHD_CUDA_TRY(cudaPeekAtLastError());
     return st1 > st2 ? st1 : st2;
 }
@@ -730,7 +729,6 @@ int advance_overdamped(fhd_ctx* ctx, const fhd_stoch_params* sp, const fhd_mixtu
     if (!st2) st2 = stage(w_corr, dt, nullptr, stats2 ? &stats2[1] : nullptr);
     ctx->p.gmres_abs_tol = abs_tol_in;
     if (st2 < 0) return st2;
-    if (mp && (rc = mass_flag_check(ctx))) return rc;
     return st1 > st2 ? st1 : st2;
 }
 

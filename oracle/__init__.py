@@ -320,3 +320,39 @@ def mixture_local(mp, k_B, rho):
     rc = lib().or_mixture_local(C.byref(mp), C.c_double(k_B), _p(np.ascontiguousarray(rho, np.float64)), _p(chi),
                                 _p(L))
     return rc, chi.reshape(ns, ns), L.reshape(ns, ns)
+
+
+def mixture_trace_local(mp, k_B, rho):
+    """rho W chi and the Cholesky factor of the Onsager matrix at one state
+    (compute_rhoWchi_local, compute_sqrtLonsager_local), trace species
+    included"""
+    ns = mp.nspecies
+    a = np.zeros(ns * ns)
+    L = np.zeros(ns * ns)
+    lib().or_mixture_trace_local(C.byref(mp), C.c_double(k_B), _p(np.ascontiguousarray(rho, np.float64)), _p(a),
+                                 _p(L))
+    return a.reshape(ns, ns), L.reshape(ns, ns)
+
+
+def sqrtLonsager_fc(dim, n, sp, mp, rho):
+    """compute_sqrtLonsager_fc: list of dim*ns*ns face arrays, entry (r, c)
+    of direction d at index d*ns*ns + r + ns*c"""
+    ns = mp.nspecies
+    nc = int(np.prod(list(n)[:dim]))
+    out = [np.zeros(nc) for _ in range(dim * ns * ns)]
+    lib().or_sqrtLonsager_fc(dim, _n3(n), C.byref(sp), C.byref(mp), _pp(rho), _pp(out))
+    return out
+
+
+def stochastic_mass_fluxdiv(dim, n, dx, sp, mp, sqrtL, dt, weights, W_fc, increment=False, div0=None,
+                            want_flux=False):
+    """stochastic_mass_fluxdiv with given face factors: (div, flux|None)"""
+    ns = mp.nspecies
+    nc = int(np.prod(list(n)[:dim]))
+    div = [np.array(d, dtype=np.float64) for d in div0] if div0 is not None else [np.zeros(nc) for _ in range(ns)]
+    flux = [np.zeros(nc) for _ in range(dim * ns)] if want_flux else None
+    w = (C.c_double * len(weights))(*weights)
+    lib().or_stochastic_mass_fluxdiv(dim, _n3(n), C.c_double(dx), C.byref(sp), C.byref(mp), _pp(sqrtL),
+                                     C.c_double(dt), C.cast(w, _DP), len(weights), _pp(W_fc), int(bool(increment)),
+                                     _pp(div), _pp(flux) if flux is not None else None)
+    return div, flux

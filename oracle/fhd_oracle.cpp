@@ -1306,48 +1306,121 @@ void dbar2chi(int ns, int iters, const double D[][FHD_MAX_SPECIES], const double
     }
 }
 
-// compute_chi (mass_flux_utilities.f90:743-922) without LAPACK
-void chi_of(const Mix& m, const double* rho, double rhotot, const double* x, double chi[][FHD_MAX_SPECIES]) {
-    if (m.ns == 2) {
+// compute_chi (mass_flux_utilities.f90:743-922) without LAPACK, for a
+// system of n species with molar masses mm and Maxwell-Stefan matrix D:
+// the closed form for two species (767-786), Dbar2chi_iterative otherwise
+void chi_n(int n, int iters, const double* mm, const double D[][FHD_MAX_SPECIES], const double* rho, double rhotot,
+           const double* x, double chi[][FHD_MAX_SPECIES]) {
+    if (n == 2) {
         double W0 = rho[0] / rhotot, W1 = rho[1] / rhotot;
-        double t = m.molmass[0] * W1 + m.molmass[1] * W0;
-        t = m.D[0][1] * t * t / m.molmass[0] / m.molmass[1];
+        double t = mm[0] * W1 + mm[1] * W0;
+        t = D[0][1] * t * t / mm[0] / mm[1];
         chi[0][0] = t * W1 / W0;
         chi[0][1] = -t;
         chi[1][0] = -t;
         chi[1][1] = t * W0 / W1;
         return;
     }
-    dbar2chi(m.ns, m.chi_it, m.D, x, m.molmass, chi);
+    dbar2chi(n, iters, D, x, mm, chi);
 }
 
-// number of trace species (w < fraction_tolerance)
-int n_trace(const Mix& m, const double* rho, double rhotot) {
+void chi_of(const Mix& m, const double* rho, double rhotot, const double* x, double chi[][FHD_MAX_SPECIES]) {
+    chi_n(m.ns, m.chi_it, m.molmass, m.D, rho, rhotot, x, chi);
+}
+
+// number of trace species (w < fraction_tolerance) and the map dest of
+// mass_flux_utilities.f90:583-594 (0-based here: dest[i] = index of species
+// i in the subsystem of non-trace species, or -1 for a trace species)
+int n_trace(const Mix& m, const double* rho, double rhotot, int* dest = nullptr) {
     int nt = 0;
-    for (int i = 0; i < m.ns; i++)
-        if (rho[i] / rhotot < m.frac_tol) nt++;
+    for (int i = 0; i < m.ns; i++) {
+        if (rho[i] / rhotot < m.frac_tol) {
+            nt++;
+            if (dest) dest[i] = -1;
+        } else if (dest) {
+            dest[i] = i - nt;
+        }
+    }
     return nt;
 }
 
-// compute_rhoWchi_local (mass_flux_utilities.f90:529-741); returns false
-// when trace species other than "all but one" are present
-bool rhowchi_local(const Mix& m, const double* rho, double out[][FHD_MAX_SPECIES]) {
+// the subsystem of non-trace species (compute_chi_sub and
+// compute_sqrtLonsager_sub, mass_flux_utilities.f90:654-688 and 1440-1482):
+// densities, molar masses and D_bar restricted through dest, the subsystem
+// total density, molar concentrations and chi
+struct SubMix {
+    int n;
+    double rho[FHD_MAX_SPECIES], mm[FHD_MAX_SPECIES], D[FHD_MAX_SPECIES][FHD_MAX_SPECIES];
+    double rt, x[FHD_MAX_SPECIES], mt, chi[FHD_MAX_SPECIES][FHD_MAX_SPECIES];
+};
+
+void sub_mix(const Mix& m, const double* rho, const int* dest, int nsub, SubMix& S) {
+    S.n = nsub;
+    for (int r = 0; r < m.ns; r++)
+        if (dest[r] >= 0) {
+            S.mm[dest[r]] = m.molmass[r];
+            S.rho[dest[r]] = rho[r];
+        }
+    S.rt = 0.0;
+    for (int r = 0; r < nsub; r++) S.rt = S.rt + S.rho[r];
+    for (int r = 0; r < m.ns; r++) {
+        if (dest[r] < 0) continue;
+        for (int c = 0; c < m.ns; c++)
+            if (dest[c] >= 0) S.D[dest[r]][dest[c]] = m.D[r][c];
+    }
+    molconc(nsub, S.mm, S.rho, S.rt, S.x, &S.mt);
+    chi_n(nsub, m.chi_it, S.mm, S.D, S.rho, S.rt, S.x, S.chi);
+}
+
+// compute_rhoWchi_local (mass_flux_utilities.f90:529-741): rho W chi of
+// the full system, of the non-trace subsystem expanded with the effective
+// diffusion coefficients of the trace species (compute_chi_sub, 654-739), or
+// zero when every species but one is trace
+void rhowchi_local(const Mix& m, const double* rho, double out[][FHD_MAX_SPECIES]) {
     const int ns = m.ns;
     double rt = 0.0;
     for (int i = 0; i < ns; i++) rt = rt + rho[i];
-    const int nt = n_trace(m, rho, rt);
+    int dest[FHD_MAX_SPECIES];
+    const int nt = n_trace(m, rho, rt, dest);
     if (nt == ns - 1) {
         for (int i = 0; i < ns; i++)
             for (int j = 0; j < ns; j++) out[i][j] = 0.0;
-        return true;
+        return;
     }
-    if (nt != 0) return false;
-    double x[FHD_MAX_SPECIES], mt, chi[FHD_MAX_SPECIES][FHD_MAX_SPECIES];
-    molconc(ns, m.molmass, rho, rt, x, &mt);
-    chi_of(m, rho, rt, x, chi);
-    for (int i = 0; i < ns; i++)
-        for (int j = 0; j < ns; j++) out[i][j] = rho[i] * chi[i][j];
-    return true;
+    if (nt == 0) {
+        double x[FHD_MAX_SPECIES], mt, chi[FHD_MAX_SPECIES][FHD_MAX_SPECIES];
+        molconc(ns, m.molmass, rho, rt, x, &mt);
+        chi_of(m, rho, rt, x, chi);
+        for (int i = 0; i < ns; i++)
+            for (int j = 0; j < ns; j++) out[i][j] = rho[i] * chi[i][j];
+        return;
+    }
+    SubMix S;
+    sub_mix(m, rho, dest, ns - nt, S);
+    for (int col = 0; col < ns; col++) {
+        if (dest[col] < 0) {
+            // a trace species' column: its effective diffusion coefficient
+            double deff = 0.0;
+            for (int k = 0; k < ns; k++)
+                if (dest[k] >= 0) deff = deff + S.x[dest[k]] / m.D[k][col];
+            deff = 1.0 / deff;
+            for (int row = 0; row < ns; row++) {
+                if (row == col) {
+                    out[row][col] = S.rt * deff * m.molmass[row] / S.mt;
+                } else if (dest[row] < 0) {
+                    out[row][col] = 0.0;
+                } else {
+                    double tmp = 0.0;
+                    for (int k = 0; k < ns; k++)
+                        if (dest[k] >= 0) tmp = tmp + S.chi[dest[row]][dest[k]] * S.x[dest[k]] / m.D[k][col];
+                    out[row][col] = deff * S.rho[dest[row]] * (tmp - m.molmass[col] / S.mt);
+                }
+            }
+        } else {
+            for (int row = 0; row < ns; row++)
+                out[row][col] = (dest[row] < 0) ? 0.0 : S.rho[dest[row]] * S.chi[dest[row]][dest[col]];
+        }
+    }
 }
 
 // choldc (matrix_utilities.f90:162-241): lower Cholesky factor in place,
@@ -1406,26 +1479,41 @@ void rho_av(const Mix& m, const double* r1, const double* r2, double dv, double*
     }
 }
 
-// compute_sqrtLonsager_local (mass_flux_utilities.f90:1331-1522), k_B
-bool sqrtL_local(const Mix& m, const double* rho, double kB, double out[][FHD_MAX_SPECIES]) {
+// compute_sqrtLonsager_local (mass_flux_utilities.f90:1331-1522), k_B: the
+// Cholesky factor of L = mtot rhotot W chi W / k_B of the full system, of the
+// non-trace subsystem expanded with zeros (compute_sqrtLonsager_sub,
+// 1425-1502), or zero when every species but one is trace
+void sqrtL_local(const Mix& m, const double* rho, double kB, double out[][FHD_MAX_SPECIES]) {
     const int ns = m.ns;
     double rt = 0.0;
     for (int i = 0; i < ns; i++) rt = rt + rho[i];
-    const int nt = n_trace(m, rho, rt);
+    int dest[FHD_MAX_SPECIES];
+    const int nt = n_trace(m, rho, rt, dest);
     if (nt == ns - 1) {
         for (int i = 0; i < ns; i++)
             for (int j = 0; j < ns; j++) out[i][j] = 0.0;
-        return true;
+        return;
     }
-    if (nt != 0) return false;
-    double W[FHD_MAX_SPECIES], x[FHD_MAX_SPECIES], mt, chi[FHD_MAX_SPECIES][FHD_MAX_SPECIES];
-    for (int i = 0; i < ns; i++) W[i] = rho[i] / rt;
-    molconc(ns, m.molmass, rho, rt, x, &mt);
-    chi_of(m, rho, rt, x, chi);
-    for (int c = 0; c < ns; c++)
-        for (int r = 0; r < ns; r++) out[r][c] = mt * rt * W[r] * chi[r][c] * W[c] / kB;
-    choldc(ns, out);
-    return true;
+    if (nt == 0) {
+        double W[FHD_MAX_SPECIES], x[FHD_MAX_SPECIES], mt, chi[FHD_MAX_SPECIES][FHD_MAX_SPECIES];
+        for (int i = 0; i < ns; i++) W[i] = rho[i] / rt;
+        molconc(ns, m.molmass, rho, rt, x, &mt);
+        chi_of(m, rho, rt, x, chi);
+        for (int c = 0; c < ns; c++)
+            for (int r = 0; r < ns; r++) out[r][c] = mt * rt * W[r] * chi[r][c] * W[c] / kB;
+        choldc(ns, out);
+        return;
+    }
+    SubMix S;
+    const int nsub = ns - nt;
+    sub_mix(m, rho, dest, nsub, S);
+    double Ws[FHD_MAX_SPECIES], Ls[FHD_MAX_SPECIES][FHD_MAX_SPECIES];
+    for (int r = 0; r < nsub; r++) Ws[r] = S.rho[r] / S.rt;
+    for (int c = 0; c < nsub; c++)
+        for (int r = 0; r < nsub; r++) Ls[r][c] = S.mt * S.rt * Ws[r] * S.chi[r][c] * Ws[c] / kB;
+    choldc(nsub, Ls);
+    for (int r = 0; r < ns; r++)
+        for (int c = 0; c < ns; c++) out[r][c] = (dest[r] >= 0 && dest[c] >= 0) ? Ls[dest[r]][dest[c]] : 0.0;
 }
 
 // compute_mass_fluxdiv (compute_mass_fluxdiv.f90:29-183) for an ideal
@@ -1439,8 +1527,7 @@ int mass_fluxdiv_impl(const Geo& g, const Mix& m, const fhd_stoch_params* sp, co
     const int dim = g.dim, ns = m.ns;
     const long nc = g.nc;
     std::vector<Vec> rwc(ns * ns, Vec(nc)), xcc(ns, Vec(nc));
-    bool ok = true;
-#pragma omp parallel for reduction(&& : ok)
+#pragma omp parallel for
     for (long f = 0; f < nc; f++) {
         double r[FHD_MAX_SPECIES], a[FHD_MAX_SPECIES][FHD_MAX_SPECIES], x[FHD_MAX_SPECIES], mt;
         double rt = 0.0;
@@ -1448,18 +1535,16 @@ int mass_fluxdiv_impl(const Geo& g, const Mix& m, const fhd_stoch_params* sp, co
             r[i] = rho[i][f];
             rt = rt + r[i];
         }
-        ok = rhowchi_local(m, r, a) && ok;
+        rhowchi_local(m, r, a);
         molconc(ns, m.molmass, r, rt, x, &mt);
         for (int i = 0; i < ns; i++) {
             xcc[i][f] = x[i];
             for (int j = 0; j < ns; j++) rwc[i * ns + j][f] = a[i][j];
         }
     }
-    if (!ok) return FHD_ERR_UNSUPPORTED;
     const double variance = std::sqrt(2.0 * sp->k_B * m.var_mass / (sp->dV * dt));
     const double dxinv = 1.0 / g.dx;
     std::vector<Vec> flux(dim * ns, Vec(nc));
-    bool ok2 = true;
     for (int d = 0; d < dim; d++) {
         int e[3] = {0, 0, 0};
         e[d] = 1;
@@ -1488,7 +1573,7 @@ int mass_fluxdiv_impl(const Geo& g, const Mix& m, const fhd_stoch_params* sp, co
                     r2[s] = rho[s][f];
                 }
                 rho_av(m, r1, r2, sp->dV, ra);
-                if (!sqrtL_local(m, ra, sp->k_B, L)) ok2 = false;
+                sqrtL_local(m, ra, sp->k_B, L);
                 for (int s = 0; s < ns; s++) {
                     double acc = 0.0;
                     for (int rr = 0; rr < n_rngs; rr++) acc = acc + weights[rr] * W_fc[(rr * dim + d) * ns + s][f];
@@ -1508,7 +1593,6 @@ int mass_fluxdiv_impl(const Geo& g, const Mix& m, const fhd_stoch_params* sp, co
             for (int s = 0; s < ns; s++) flux[d * ns + s][f] = fd[s] + fs[s];
         });
     }
-    if (!ok2) return FHD_ERR_UNSUPPORTED;
     forall(g, [&](int i, int j, int k) {
         const long f = g.id(i, j, k);
         for (int s = 0; s < ns; s++) {
@@ -2025,13 +2109,116 @@ int or_mixture_local(const fhd_mixture_params* mp, double k_B, const double* rho
     double x[FHD_MAX_SPECIES], mt, chi[FHD_MAX_SPECIES][FHD_MAX_SPECIES], L[FHD_MAX_SPECIES][FHD_MAX_SPECIES];
     molconc(m.ns, m.molmass, rho, rt, x, &mt);
     chi_of(m, rho, rt, x, chi);
-    if (!sqrtL_local(m, rho, k_B, L)) return FHD_ERR_UNSUPPORTED;
+    sqrtL_local(m, rho, k_B, L);
     for (int i = 0; i < m.ns; i++)
         for (int j = 0; j < m.ns; j++) {
             chi_out[i * m.ns + j] = chi[i][j];
             sqrtL_out[i * m.ns + j] = L[i][j];
         }
     return 0;
+}
+
+// compute_sqrtLonsager_fc (mass_flux_utilities.f90:1096-1229): on every
+// face of direction d, the Cholesky factor of the Onsager matrix at the
+// face-averaged density (compute_nonnegative_rho_av, then
+// compute_sqrtLonsager_local with rhotot = sum of the averages).  Entry (r,
+// c) of face f in direction d goes to sqrtL[d*ns*ns + r + ns*c][f], the
+// column-major component order of the reference's ns^2-component multifab.
+void or_sqrtLonsager_fc(int dim, const int n[3], const fhd_stoch_params* sp, const fhd_mixture_params* mp,
+                        const double* const rho[], double* const sqrtL[]) {
+    Geo g(dim, n, 1.0);
+    Mix m = make_mix(mp);
+    const int ns = m.ns;
+    for (int d = 0; d < dim; d++) {
+        int e[3] = {0, 0, 0};
+        e[d] = 1;
+        forall(g, [&](int i, int j, int k) {
+            const long f = g.id(i, j, k), fm = g.id(i - e[0], j - e[1], k - e[2]);
+            double r1[FHD_MAX_SPECIES], r2[FHD_MAX_SPECIES], ra[FHD_MAX_SPECIES], L[FHD_MAX_SPECIES][FHD_MAX_SPECIES];
+            for (int s = 0; s < ns; s++) {
+                r1[s] = rho[s][fm];
+                r2[s] = rho[s][f];
+            }
+            rho_av(m, r1, r2, sp->dV, ra);
+            sqrtL_local(m, ra, sp->k_B, L);
+            for (int r = 0; r < ns; r++)
+                for (int c = 0; c < ns; c++) sqrtL[d * ns * ns + r + ns * c][f] = L[r][c];
+        });
+    }
+}
+
+// stochastic_mass_fluxdiv (stochastic_mass_fluxdiv.f90:37-116) with the
+// face factors given: flux = variance * sqrtL_face * sum_r w_r W_r (setval,
+// saxpy per random stage, matvec_mul, mult by the variance), corrected to a
+// zero species sum (correction_flux.f90:17-226), and its divergence
+// (compute_div, div_and_grad.f90:884-1035), added to div when increment.
+// W_fc[(r*dim + d)*ns + s]; flux (nullable) receives flux[d*ns + s].
+void or_stochastic_mass_fluxdiv(int dim, const int n[3], double dx, const fhd_stoch_params* sp,
+                                const fhd_mixture_params* mp, const double* const sqrtL[], double dt,
+                                const double* weights, int n_rngs, const double* const W_fc[], int increment,
+                                double* const div[], double* const flux_out[]) {
+    Geo g(dim, n, dx);
+    Mix m = make_mix(mp);
+    const int ns = m.ns;
+    const double variance = std::sqrt(2.0 * sp->k_B * m.var_mass / (sp->dV * dt));
+    std::vector<Vec> flux(dim * ns, Vec(g.nc));
+    for (int d = 0; d < dim; d++) {
+        forall(g, [&](int i, int j, int k) {
+            const long f = g.id(i, j, k);
+            double w[FHD_MAX_SPECIES], fs[FHD_MAX_SPECIES];
+            for (int s = 0; s < ns; s++) {
+                double acc = 0.0;
+                for (int rr = 0; rr < n_rngs; rr++) acc = acc + weights[rr] * W_fc[(rr * dim + d) * ns + s][f];
+                w[s] = acc;
+            }
+            for (int r = 0; r < ns; r++) {
+                double acc = 0.0;
+                for (int c = 0; c < ns; c++) acc = acc + sqrtL[d * ns * ns + r + ns * c][f] * w[c];
+                fs[r] = acc * variance;
+            }
+            if (m.correct && ns > 1) {
+                double sum = 0.0;
+                for (int s = 0; s < ns - 1; s++) sum = sum + fs[s];
+                fs[ns - 1] = -sum;
+            }
+            for (int s = 0; s < ns; s++) flux[d * ns + s][f] = fs[s];
+        });
+    }
+    const double dxinv = 1.0 / dx;
+    forall(g, [&](int i, int j, int k) {
+        const long f = g.id(i, j, k);
+        for (int s = 0; s < ns; s++) {
+            const double a = (flux[0 * ns + s][g.id(i + 1, j, k)] - flux[0 * ns + s][f]) * dxinv;
+            const double b = (flux[1 * ns + s][g.id(i, j + 1, k)] - flux[1 * ns + s][f]) * dxinv;
+            double v;
+            if (increment) {
+                v = div[s][f] + a + b;
+                if (dim == 3) v = v + (flux[2 * ns + s][g.id(i, j, k + 1)] - flux[2 * ns + s][f]) * dxinv;
+            } else {
+                v = a + b;
+                if (dim == 3) v = v + (flux[2 * ns + s][g.id(i, j, k + 1)] - flux[2 * ns + s][f]) * dxinv;
+            }
+            div[s][f] = v;
+        }
+    });
+    if (flux_out)
+        for (int q = 0; q < dim * ns; q++) std::copy(flux[q].begin(), flux[q].end(), flux_out[q]);
+}
+
+// rho W chi and the Onsager Cholesky factor at one state, trace species
+// included (test hook for compute_rhoWchi_local and
+// compute_sqrtLonsager_local)
+void or_mixture_trace_local(const fhd_mixture_params* mp, double k_B, const double* rho, double* rhowchi_out,
+                            double* sqrtL_out) {
+    Mix m = make_mix(mp);
+    double a[FHD_MAX_SPECIES][FHD_MAX_SPECIES], L[FHD_MAX_SPECIES][FHD_MAX_SPECIES];
+    rhowchi_local(m, rho, a);
+    sqrtL_local(m, rho, k_B, L);
+    for (int i = 0; i < m.ns; i++)
+        for (int j = 0; j < m.ns; j++) {
+            rhowchi_out[i * m.ns + j] = a[i][j];
+            sqrtL_out[i * m.ns + j] = L[i][j];
+        }
 }
 
 // ---------------------------------------------------------------------

@@ -151,6 +151,24 @@ int or_mass_fluxdiv(int dim, const int n[3], double dx, const fhd_stoch_params* 
 /* chi (Dbar2chi_iterative) and chol(L) at one state rho[ns] (row-major) */
 int or_mixture_local(const fhd_mixture_params* mp, double k_B, const double* rho,
                      double* chi, double* sqrtL);
+/* compute_sqrtLonsager_fc: per face of direction d the Onsager Cholesky
+ * factor at the face-averaged density; sqrtL[d*ns*ns + r + ns*c] */
+void or_sqrtLonsager_fc(int dim, const int n[3], const fhd_stoch_params* sp,
+                        const fhd_mixture_params* mp, const double* const rho[],
+                        double* const sqrtL[]);
+/* stochastic_mass_fluxdiv with given face factors; W_fc[(r*dim+d)*ns+s],
+ * flux (nullable) [d*ns+s]; div overwritten or, if increment, added to */
+void or_stochastic_mass_fluxdiv(int dim, const int n[3], double dx,
+                                const fhd_stoch_params* sp,
+                                const fhd_mixture_params* mp,
+                                const double* const sqrtL[], double dt,
+                                const double* weights, int n_rngs,
+                                const double* const W_fc[], int increment,
+                                double* const div[], double* const flux[]);
+/* rho W chi and the Onsager Cholesky factor at one state, trace species
+ * included (compute_rhoWchi_local, compute_sqrtLonsager_local) */
+void or_mixture_trace_local(const fhd_mixture_params* mp, double k_B, const double* rho,
+                            double* rhowchi_out, double* sqrtL_out);
 
 /* Discretisation-accuracy harness of exec/stokes_preconditioner
  * (main_driver.f90:354-387, test_type=0): on [0,1]^dim with n cells per

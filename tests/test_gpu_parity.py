@@ -217,6 +217,35 @@ def test_gmres_config1(cuda):
     assert abs(npr - npr_ref) <= 1e-12 * npr_ref
 
 
+@pytest.mark.parametrize("dim,n,visc,theta", [(2, [32, 32], 1, 0.0), (3, [16, 16, 16], -1, 20.0),
+                                                (3, [16, 8, 16], 2, 20.0)])
+@pytest.mark.parametrize("sf", [2.5, 1e-3])
+def test_gmres_scale_factor(cuda, dim, n, visc, theta, sf):
+    """scale_factor != 1 (gmres.f90:118-135, 442-459): the solve for
+    scale*x_p with scaled theta_alpha, rhs and viscosities, and a nonzero
+    initial pressure guess, matches the oracle; the caller's operands are
+    left as they were"""
+    pb = P.problem(dim, n, visc, dx=1.0, seed=21)
+    b_u, b_p = P.random_stokes(dim, n, seed=22)
+    rng = np.random.default_rng(23)
+    xp0 = rng.standard_normal(pb.nc)
+    xp0 -= xp0.mean()
+    params = O.default_params(gmres_rel_tol=1e-9, scale_factor=sf)
+    rc, ref_u, ref_p, npr_ref, st_ref = O.gmres(pb, params, theta, b_u, b_p, x_p0=xp0)
+    assert rc >= 0
+    with L.StokesSolver(dim, n, 1.0, visc, params=L.default_params(gmres_rel_tol=1e-9, scale_factor=sf)) as s:
+        x_u, x_p = zeros(pb.nc, dim, cuda), dev(xp0, cuda)
+        bu, beta = dev(b_u, cuda), dev(pb.beta, cuda)
+        status, npr, st = s.gmres(bu, dev(b_p, cuda), x_u, x_p, dev(pb.alpha_fc, cuda), beta,
+                                  dev(pb.beta_ed, cuda), dev(pb.gamma, cuda), theta)
+        assert np.array_equal(host(bu[0]), b_u[0]) and np.array_equal(host(beta), pb.beta)
+    assert status == rc
+    assert st["total_iters"] == st_ref.total_iters
+    for c in range(dim):
+        assert P.rel_inf([host(x_u[c])], [ref_u[c]]) < 1e-10
+    assert P.rel_inf([host(x_p)], [ref_p]) < 1e-10
+
+
 @pytest.mark.parametrize("visc", [1, -1, -2, 3])
 def test_gmres_3d_inertial(cuda, visc):
     dim, n = 3, [16, 16, 16]

@@ -21,7 +21,7 @@ pytestmark = pytest.mark.gpu
 # (every finest level here is too large for the single-CTA coarse kernel,
 # so the finest levels of both multigrids smooth through launches)
 CASES = [(3, [128, 64, 64], 1, "mixed"), (3, [32, 32, 32], -1, "fp64"), (3, [32, 16, 32], 2, "fp64"),
-         (2, [128, 128], 1, "mixed"), (2, [256, 128], -1, "fp64")]
+         (2, [128, 128], 1, "mixed"), (2, [256, 128], -1, "fp64"), (3, [256, 32, 32], 1, "mixed")]
 
 
 def _run(cuda, dim, n, visc, precision, tune, seed=71):
@@ -60,6 +60,8 @@ def test_every_candidate_matches_the_rules(cuda, dim, n, visc, precision):
     expect = {"colour"} if dim == 2 else {"colour", "tiled"}
     if dim == 3 and visc == 1 and precision == "mixed":
         expect.add("rowtile")
+        if n[0] >= 128:
+            expect.add("rowtile2")
     assert expect <= kinds
 
 
@@ -70,7 +72,7 @@ def test_tuned_plan_is_timed_cached_and_equal(cuda, dim, n, visc, precision):
     out2, info2 = _run(cuda, dim, n, visc, precision, 1)
     for info in (info1, info2):
         for lv in info:
-            assert lv["kind"] in ("colour", "tiled", "rowtile")
+            assert lv["kind"] in ("colour", "tiled", "rowtile", "rowtile2")
             assert lv["candidates"] >= 1 and lv["pair_us"] > 0
     # the second context reuses the first one's measurement
     assert info1 == info2
@@ -84,7 +86,12 @@ def test_imported_plan_is_used_untimed(cuda):
     dim, n, visc, precision = 3, [64, 64, 32], 1, "mixed"  # a shape no other test tunes
     cands = L.tune_candidates("stag", dim, n, precision, visc)
     idx = next(i for i, c in enumerate(cands) if c["kind"] == "tiled")
-    line = f"0:s:4:3:1:64x64x32 {idx}"
+    import torch
+    pr = torch.cuda.get_device_properties(cuda)
+    key = L.tune_key("stag", dim, n, precision, visc, sms=pr.multi_processor_count,
+                     smem_optin=pr.shared_memory_per_block_optin, smem_sm=pr.shared_memory_per_multiprocessor,
+                     device=cuda.index or 0)
+    line = f"{key} {idx}"
     assert L.tune_import(line + "\n") == 1
     ref, _ = _run(cuda, dim, n, visc, precision, 0)
     out, info = _run(cuda, dim, n, visc, precision, -1)

@@ -15,7 +15,16 @@ def kinds(c):
 
 def test_fp32_visc1_large_level_has_every_kind():
     c = L.tune_candidates("stag", 3, [256, 256, 256], "mixed", 1)
-    assert kinds(c) == {"colour", "tiled", "rowtile"}
+    assert kinds(c) == {"colour", "tiled", "rowtile", "rowtile2"}
+    # the two-cell form: whole warps per row, 3 red and 2 black passes of 4
+    # rows cover a 4- or 8-row tile and its ring rows
+    two = [x for x in c if x["kind"] == "rowtile2"]
+    assert {(x["y"], x["per_sm"], x["threads"]) for x in two} == {(4, 1, 256), (8, 1, 256)}
+    assert all(x["smem"] <= 232448 for x in two)
+    c128 = L.tune_candidates("stag", 3, [128, 128, 128], "mixed", 1)
+    assert {x["y"] for x in c128 if x["kind"] == "rowtile2"} == {4, 8, 16}
+    # no whole warp per row below 128 cells
+    assert "rowtile2" not in kinds(L.tune_candidates("stag", 3, [64, 64, 64], "mixed", 1))
     rows = [x for x in c if x["kind"] == "rowtile"]
     # one CTA per SM with the deep ring for 4- and 8-row tiles (256 or 512
     # compute threads); the short ring only where two CTAs fit on one SM
@@ -36,7 +45,7 @@ def test_fp32_visc1_large_level_has_every_kind():
 @pytest.mark.parametrize("prec,visc", [("fp64", 1), ("mixed", -1), ("mixed", 2)])
 def test_rowtile_only_for_fp32_constant_viscosity(prec, visc):
     c = L.tune_candidates("stag", 3, [128, 128, 128], prec, visc)
-    assert "rowtile" not in kinds(c)
+    assert "rowtile" not in kinds(c) and "rowtile2" not in kinds(c)
     assert {"colour", "tiled"} <= kinds(c)
     if prec == "fp64":
         for x in c:
@@ -75,22 +84,43 @@ def test_bad_arguments():
         L.tune_candidates("stag", 3, [1, 8, 8])
 
 
+K96S = L.tune_key("stag", 3, [96, 96, 96], "mixed", 1)
+K96C = L.tune_key("cc", 3, [96, 96, 96], "mixed", 1)
+
+
+def test_table_key_names_version_and_device():
+    ver = K96S.split(":")[0]
+    assert ver[0] == "v" and int(ver[1:]) >= 3
+    assert K96S == f"{ver}:0:s:4:3:1:96x96x96:148:232448:233472"
+    assert L.tune_key("cc", 3, [96, 96, 96], "fp64", 2, sms=132, smem_optin=232448, smem_sm=233472,
+                      device=1) == f"{ver}:1:c:8:3:0:96x96x96:132:232448:233472"
+    with pytest.raises(L.FhdError):
+        L.tune_key("stag", 4, [8, 8, 8])
+
+
 def test_table_import_export_roundtrip():
-    text = "0:s:4:3:1:96x96x96 11\n0:c:4:3:0:96x96x96 2\n"
+    text = f"{K96S} 11\n{K96C} 2\n"
     assert L.tune_import(text) == 2
     out = L.tune_export()
     for line in text.splitlines():
         assert line in out.splitlines()
     # re-importing replaces, and an empty text adds nothing
-    assert L.tune_import("0:s:4:3:1:96x96x96 3\n") == 1
-    assert "0:s:4:3:1:96x96x96 3" in L.tune_export().splitlines()
+    assert L.tune_import(f"{K96S} 3\n") == 1
+    assert f"{K96S} 3" in L.tune_export().splitlines()
     assert L.tune_import("") == 0
 
 
-@pytest.mark.parametrize("bad", ["0:s:4:3:1:96x96x96\n", "nonsense 1\n", "0:s:4:3:1:96x96x96 x\n",
-                                 "0:q:4:3:1:96x96x96 1\n", "0:s:4:3:1:96x96x96 1 2\n"])
+def test_table_import_skips_other_versions():
+    ver = K96S.split(":")[0]
+    other = "v1:" + K96S[len(ver) + 1:].replace("96x96x96", "88x88x88")
+    assert L.tune_import(f"{other} 4\n") == 0
+    assert other not in L.tune_export()
+
+
+@pytest.mark.parametrize("bad", [f"{K96S}\n", "nonsense 1\n", f"{K96S} x\n", K96S.replace(":s:", ":q:") + " 1\n",
+                                 f"{K96S} 1 2\n", "0:s:4:3:1:96x96x96 1\n"])
 def test_table_import_rejects_malformed_lines(bad):
     before = L.tune_export()
     with pytest.raises(L.FhdError):
-        L.tune_import("0:s:4:3:1:40x40x40 1\n" + bad)
+        L.tune_import(L.tune_key("stag", 3, [40, 40, 40]) + " 1\n" + bad)
     assert L.tune_export() == before
