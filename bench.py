@@ -556,8 +556,6 @@ def run_reference(args):
 # finest-level smoother kernel by the kind of plan the autotuner picked
 SMOOTHER_KERNEL = {
     "rowtile": "k_stag_rbx (finest-level row-tile fused red-black smooth of all three components)",
-    "rowtile2": "k_stag_rbx two-cell form (finest-level row-tile fused red-black smooth, two cells per thread "
-                "and row from 128-bit shared-memory accesses)",
     "tiled": "k_stag_rb (finest-level tiled fused red-black smooth)",
     "colour": "k_stag_gs (finest-level colour sweep)",
     "rules": "finest-level smoother of the fixed size rules",

@@ -140,6 +140,23 @@ typedef struct fhd_ctx fhd_ctx;
 int  fhd_ctx_create(int dim, const int n_cells[3], const double dx[3],
                     int visc_type, const fhd_gmres_params* params,
                     int precision_mode, fhd_ctx** out);
+/* The same context with the layout arguments of the driver's set-up
+ * (probin_common max_grid_size, bc_lo, bc_hi; main_driver.f90:392-393).
+ * bc codes: FHD_BC_PERIODIC (-1, FBoxLib's PERIODIC) in every direction;
+ * walls and reservoirs return FHD_ERR_UNSUPPORTED (they are not built).
+ * max_grid_size[d] (>= 1; below n_cells[d] it must divide it) sets the box
+ * layout the reference's staggered multigrid follows: with several boxes
+ * its hierarchy stops at the boxes' depth (compute_nlevs_mg over the boxes,
+ * stag_mg_layout.f90:179-222), and with stag_mg_bottom_solver 4 and
+ * n_cells/max_grid_size >= 2 in every direction its bottom is the "fancy"
+ * nested solve over the deeper levels of the domain (stag_mg_solver.f90:
+ * 447-555).  The pressure multigrid is FBoxLib's in the reference and keeps
+ * the whole-domain hierarchy here. */
+#define FHD_BC_PERIODIC (-1)
+int  fhd_ctx_create_bc(int dim, const int n_cells[3], const int max_grid_size[3],
+                       const int bc_lo[3], const int bc_hi[3], const double dx[3],
+                       int visc_type, const fhd_gmres_params* params,
+                       int precision_mode, fhd_ctx** out);
 int  fhd_ctx_destroy(fhd_ctx* ctx);
 /* CUDA stream (cudaStream_t) the context launches on; may be set by the
  * caller before any call (NULL = the context's own stream). */
@@ -187,8 +204,7 @@ int fhd_ctx_set_fused(fhd_ctx* ctx, int mode);
 int fhd_ctx_set_tune(fhd_ctx* ctx, int mode);
 /* Plan of staggered (which 0) or pressure (which 1) multigrid level `level`
  * after the last solve call: kind -1 fixed rules, 0 colour launches, 1 tiled
- * fused, 2 row-tile, 3 row-tile with two cells per thread and row;
- * ncand candidates considered; pair_us the measured time
+ * fused, 2 row-tile; ncand candidates considered; pair_us the measured time
  * of one smooth pair (0 when not timed); shape = {block x, block y, 0, 1,
  * threads} for colour launches, {tile x, tile y, z-runs, CTAs per SM,
  * compute threads} for fused smooths.  Any output pointer may be NULL.  No

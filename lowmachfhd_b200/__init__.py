@@ -65,7 +65,8 @@ class StokesSolver:
     Krylov storage and a CUDA stream."""
 
     def __init__(self, dim: int, n_cells: Sequence[int], dx: float | Sequence[float], visc_type: int,
-                 params: GmresParams | None = None, precision: str = "fp64"):
+                 params: GmresParams | None = None, precision: str = "fp64", max_grid_size=None, bc_lo=None,
+                 bc_hi=None):
         self.dim = int(dim)
         n = list(n_cells) + [1] * (3 - len(n_cells))
         self.n_cells = n[:3]
@@ -76,9 +77,18 @@ class StokesSolver:
         self.precision = precision
         mode = FHD_PREC_MIXED if precision == "mixed" else FHD_PREC_FP64
         h = C.c_void_p()
-        st = lib().fhd_ctx_create(self.dim, (C.c_int * 3)(*self.n_cells), (C.c_double * 3)(*dxs),
-                                  self.visc_type, C.byref(self.params), mode, C.byref(h))
-        check(st, "fhd_ctx_create")
+        if max_grid_size is None and bc_lo is None and bc_hi is None:
+            st = lib().fhd_ctx_create(self.dim, (C.c_int * 3)(*self.n_cells), (C.c_double * 3)(*dxs),
+                                      self.visc_type, C.byref(self.params), mode, C.byref(h))
+            check(st, "fhd_ctx_create")
+        else:
+            # the driver's layout: max_grid_size and the BoxLib boundary codes
+            # (-1 periodic), as fhd_ctx_create_bc takes them
+            i3 = lambda v, dflt: (C.c_int * 3)(*((list(v) if v is not None else [dflt] * 3) + [dflt] * 3)[:3])
+            st = lib().fhd_ctx_create_bc(self.dim, (C.c_int * 3)(*self.n_cells), i3(max_grid_size, 1 << 30),
+                                         i3(bc_lo, -1), i3(bc_hi, -1), (C.c_double * 3)(*dxs), self.visc_type,
+                                         C.byref(self.params), mode, C.byref(h))
+            check(st, "fhd_ctx_create_bc")
         self._h = h
 
     # ----------------------------------------------------------------
@@ -134,7 +144,7 @@ class StokesSolver:
         shape = (C.c_int * 5)()
         check(lib().fhd_ctx_tune_info(self._h, 0 if which == "stag" else 1, int(level), C.byref(kind),
                                       C.byref(nc), C.byref(us), shape), "fhd_ctx_tune_info")
-        names = {-1: "rules", 0: "colour", 1: "tiled", 2: "rowtile", 3: "rowtile2"}
+        names = {-1: "rules", 0: "colour", 1: "tiled", 2: "rowtile"}
         return {"kind": names[kind.value], "candidates": nc.value, "pair_us": us.value, "shape": list(shape)}
 
     def profile(self, enable: bool = True):
@@ -535,7 +545,7 @@ def tune_candidates(which: str, dim: int, n_cells, precision: str = "mixed", vis
     out = (C.c_int * (7 * 64))()
     k = check(lib().fhd_tune_candidates(0 if which == "stag" else 1, int(dim), n, prec, int(visc_type), int(sms),
                                         int(smem_optin), int(smem_sm), out, 64), "fhd_tune_candidates")
-    names = {0: "colour", 1: "tiled", 2: "rowtile", 3: "rowtile2"}
+    names = {0: "colour", 1: "tiled", 2: "rowtile"}
     return [dict(kind=names[out[7 * i]], x=out[7 * i + 1], y=out[7 * i + 2], zruns=out[7 * i + 3],
                  per_sm=out[7 * i + 4], smem=out[7 * i + 5], threads=out[7 * i + 6]) for i in range(min(k, 64))]
 

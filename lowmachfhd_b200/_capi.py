@@ -136,6 +136,9 @@ _PROTOS = {
     "fhd_gmres_params_default": (None, [C.POINTER(GmresParams)]),
     "fhd_ctx_create": (C.c_int, [C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double), C.c_int,
                                  C.POINTER(GmresParams), C.c_int, C.POINTER(_VP)]),
+    "fhd_ctx_create_bc": (C.c_int, [C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                    C.POINTER(C.c_int), C.POINTER(C.c_double), C.c_int, C.POINTER(GmresParams),
+                                    C.c_int, C.POINTER(_VP)]),
     "fhd_ctx_destroy": (C.c_int, [_VP]),
     "fhd_ctx_stream": (_VP, [_VP]),
     "fhd_ctx_set_stream": (C.c_int, [_VP, _VP]),

@@ -196,6 +196,18 @@ __device__ void cs_stag_residual(const Grid& g, const StagOp<T>& A, const CSStag
     __syncthreads();
 }
 
+// the operator of level m with a constant viscosity (visc_type > 0) loaded
+// into a register once, rather than after every block barrier
+template <typename T, int VISC>
+__device__ __forceinline__ StagOp<T> cs_op(const StagCoarseArgs<T>& a, int m) {
+    StagOp<T> A = a.A[m];
+    if constexpr (VISC > 0) {
+        A.beta0 = A.beta[0];
+        A.beta0_set = 1;
+    }
+    return A;
+}
+
 template <typename T, int DIM, int VISC>
 __global__ void __launch_bounds__(CS_THREADS) k_stag_coarse(const __grid_constant__ StagCoarseArgs<T> a) {
     extern __shared__ __align__(16) unsigned char cs_smem[];
@@ -219,8 +231,9 @@ __global__ void __launch_bounds__(CS_THREADS) k_stag_coarse(const __grid_constan
         CSStag<T> V, W;
         V.set(S, a.off[m], DIM, (int)g.nc);
         W.set(S, a.off[m + 1], DIM, (int)gc.nc);
-        cs_stag_smooths<T, DIM, VISC>(g, a.A[m], V, a.n_down, a.jacobi, a.omega);
-        cs_stag_residual<T, DIM, VISC>(g, a.A[m], V);
+        const StagOp<T> A = cs_op<T, VISC>(a, m);
+        cs_stag_smooths<T, DIM, VISC>(g, A, V, a.n_down, a.jacobi, a.omega);
+        cs_stag_residual<T, DIM, VISC>(g, A, V);
         for (int q = threadIdx.x; q < (int)gc.nc; q += nt) {
             int qi, qj, qk;
             cs_ijk(gc, q, qi, qj, qk);
@@ -241,7 +254,7 @@ __global__ void __launch_bounds__(CS_THREADS) k_stag_coarse(const __grid_constan
         const int m = a.nlev - 1;
         CSStag<T> V;
         V.set(S, a.off[m], DIM, (int)a.g[m].nc);
-        cs_stag_smooths<T, DIM, VISC>(a.g[m], a.A[m], V, a.n_bottom, a.jacobi, a.omega);
+        cs_stag_smooths<T, DIM, VISC>(a.g[m], cs_op<T, VISC>(a, m), V, a.n_bottom, a.jacobi, a.omega);
     }
     // up: prolong, smooth (stag_mg_solver.f90:380-420)
     for (int m = a.nlev - 2; m >= 0; m--) {
@@ -270,7 +283,7 @@ __global__ void __launch_bounds__(CS_THREADS) k_stag_coarse(const __grid_constan
             }
         }
         __syncthreads();
-        cs_stag_smooths<T, DIM, VISC>(g, a.A[m], V, a.n_up, a.jacobi, a.omega);
+        cs_stag_smooths<T, DIM, VISC>(g, cs_op<T, VISC>(a, m), V, a.n_up, a.jacobi, a.omega);
     }
     {
         CSStag<T> V;

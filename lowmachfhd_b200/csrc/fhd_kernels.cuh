@@ -90,6 +90,10 @@ struct StagOp {
     const T* gamma;
     const T* bed[3];  // 2D: node; 3D: xy, xz, yz
     T q;              // 1/dx^2
+    // constant-coefficient operators (visc_type > 0) read beta[0]; a kernel
+    // that loaded it once into a register sets beta0_set and beta0
+    int beta0_set = 0;
+    T beta0 = T(0);
 };
 
 template <int DIM>
@@ -159,7 +163,7 @@ __device__ __forceinline__ T stag_lface_acc(const StagOp<T>& A, const CellT& P, 
         diag = a + s * q;
         return ph * diag - (nb + cross) * q;
     } else {
-        const T b = ld(A.beta, 0);
+        const T b = A.beta0_set ? A.beta0 : ld(A.beta, 0);
         const T own_ = own(ex, ey, ez) + own(-ex, -ey, -ez);
         T oth_ = T(0), cross = T(0);
 #pragma unroll

@@ -53,7 +53,6 @@ struct RBXGeom {
     int ahead;    // stages in flight beyond the one awaited
     int per_sm;   // resident CTAs per SM the z-run split assumes
     int threads;  // compute threads (256 or 512)
-    int vw = 1;   // cells per thread and row: 1, or 2 in the two-cell form
 };
 
 struct RBGeom {
@@ -383,6 +382,12 @@ __device__ __forceinline__ void stag_rb_run(const Grid& g, const RBGeom& G, cons
 template <typename T, int VISC, int CFIX>
 __global__ void __launch_bounds__(RB_MAXTHREADS) k_stag_rb(Grid g, RBGeom G, StagOp<T> A, RBArgs<T> R, T omega) {
     extern __shared__ __align__(16) unsigned char rb_smraw[];
+    // the constant viscosity of visc_type > 0, loaded once (the staging
+    // asm clobbers memory, which would force a reload per row)
+    if constexpr (VISC > 0) {
+        A.beta0 = A.beta[0];
+        A.beta0_set = 1;
+    }
     if constexpr (CFIX >= 0) {
         stag_rb_run<T, VISC, CFIX>(g, G, A, R, omega, rb_smraw);
     } else {

@@ -51,29 +51,15 @@ constexpr int rbx_maxr(int nt) { return nt == 256 ? 5 : 3; }
 // RBX_MAXR * RBX_ROWSTEP from the start of a coefficient slot; shared memory
 // holds the coefficient ring, then the unknown ring, then a pad that covers
 // the last unknown slot's overrun.
-// The two-cell form (vw = 2): a thread owns the four cells x = 4q .. 4q+3
-// of a row and updates its two of the sweep's colour from one 128-bit load
-// per operand row; RBX2_RED passes of nt / (nx/4) rows cover a red sweep
-// (the tile and its ring rows), RBX2_BLACK passes a black one.
-constexpr int RBX2_RED = 3, RBX2_BLACK = 2;
-inline int rbx_pad(int nx, int rows, int nt = RBX_THREADS, int vw = 1) {
-    int over;
-    if (vw == 2) {
-        // red rows read up to row RG*RBX2_RED + 1 of a slot (y+1 of the last
-        // evaluated row, plus the two ring rows)
-        const int rg = nt / (nx / 4);
-        over = (rg * RBX2_RED + 2 - rows) * nx;
-    } else {
-        over = rbx_maxr(nt) * 2 * nt + 2 * nx - rows * nx;
-    }
+inline int rbx_pad(int nx, int rows, int nt = RBX_THREADS) {
+    const int over = rbx_maxr(nt) * 2 * nt + 2 * nx - rows * nx;
     return (over > 0 ? over : 0) + 32;
 }
 // ahead: stages in flight beyond the one awaited (RBX_AHEAD, or 1 for the
-// variant that fits two CTAs on an SM); nt: compute threads; vw: cells per
-// thread and row (1, or 2 in the two-cell form)
-inline size_t rbx_smem_bytes(int nx, int ty, int ahead = RBX_AHEAD, int nt = RBX_THREADS, int vw = 1) {
+// variant that fits two CTAs on an SM); nt: compute threads
+inline size_t rbx_smem_bytes(int nx, int ty, int ahead = RBX_AHEAD, int nt = RBX_THREADS) {
     return 64 + sizeof(float) * ((size_t)(3 + ahead) * 2 * (ty + 2) * nx + (size_t)(5 + ahead) * (ty + 4) * nx +
-                                 rbx_pad(nx, ty + 4, nt, vw));
+                                 rbx_pad(nx, ty + 4, nt));
 }
 
 // ---------------------------------------------------------------------
@@ -137,9 +123,14 @@ struct RBXArgs {
     unsigned* err;
 };
 
-template <int C, int AH, int NT, int VW>
-__device__ __forceinline__ void rbx_run(const Grid& g, const RBXGeom& G, const StagOp<float>& A, const RBXArgs& R,
+template <int C, int AH, int NT>
+__device__ __forceinline__ void rbx_run(const Grid& g, const RBXGeom& G, const StagOp<float>& A0, const RBXArgs& R,
                                         float omega, unsigned char* raw, int tile_y, int chunk) {
+    // the constant viscosity, loaded once: every asm statement below clobbers
+    // memory, which would make each sweep reload it from global memory
+    StagOp<float> A = A0;
+    A.beta0 = A0.beta[0];
+    A.beta0_set = 1;
     constexpr int NPH = 5 + AH;  // unknown planes k-1 .. k+3 + in flight
     constexpr int NCF = 3 + AH;  // coefficient planes k .. k+2 + in flight
     constexpr int MR = rbx_maxr(NT);  // rows per thread and red sweep
@@ -251,78 +242,6 @@ __device__ __forceinline__ void rbx_run(const Grid& g, const RBXGeom& G, const S
         for (int m = 0; m < NR; m++)
             if (lyb + m * RG < ly1) c0[m * ROWSTEP + lx] = nv[m];
     };
-    // the two-cell form (VW == 2, nx 128 or 256): thread q4 of a row owns
-    // the float4 x = 4 q4 .. 4 q4 + 3 and updates its two cells of the
-    // colour, x = 4 q4 + xpar and 4 q4 + xpar + 2.  A warp lies in one row
-    // (nx / 4 >= 32 threads per row), so xpar is warp-uniform.  The x
-    // neighbour outside the float4 comes from the next lane by a shuffle (from
-    // shared memory at a warp's edge).  The store writes the whole float4
-    // back: its other two cells have the other colour, which no thread
-    // writes during this sweep.
-    const int hq = nx >> 2;
-    const int RG2 = VW == 2 ? NT / hq : 1;
-    const int q4 = tid % hq, gr2 = tid / hq, lane = tid & 31;
-    const int xl = q4 == 0 ? nx - 1 : 4 * q4 - 1;
-    const int xr = q4 == hq - 1 ? 0 : 4 * q4 + 4;
-    auto sweep2 = [&](auto NRc, int sm, int sc, int sp, int scf, int p, int par, int ly0, int ly1) {
-        constexpr int NR = decltype(NRc)::value;
-        const int lyb = ly0 + gr2;
-        const int xpar = (y0 + lyb + p + par) & 1;  // RG2 is even: the same on all the thread's rows
-        const int o = (lyb + 2) * nx, co = (lyb + 1) * nx + 4 * q4;
-        const float* rowc = ph + sc * plane + o;
-        float* c0 = ph + sc * plane + o + 4 * q4;
-        const float* zm = ph + sm * plane + o + 4 * q4;
-        const float* zp = ph + sp * plane + o + 4 * q4;
-        const float* ca = cf + (scf * 2) * cplane + co;
-        const float* cr = ca + cplane;
-        CellF P;  // no index is read by the constant-coefficient stencil
-        P.base = 0;
-        P.oxm = P.oxp = P.oym = P.oyp = P.ozm = P.ozp = 0;
-        auto upd = [&](float cv, float xm, float xp, float ym, float yp, float zmv, float zpv, float al, float rh) {
-            float dg;
-            const float L = stag_lface_acc<float, 3, 1, C>(
-                A, P,
-                [&](int a, int b, int cz) {
-                    return cz < 0   ? zmv
-                           : cz > 0 ? zpv
-                           : b < 0  ? ym
-                           : b > 0  ? yp
-                           : a < 0  ? xm
-                           : a > 0  ? xp
-                                    : cv;
-                },
-                [&](int, int, int, int) { return 0.0f; }, [&]() { return al; }, dg);
-            return cv + sm_quot(omega * (rh - L), dg);
-        };
-        float4 nv[NR];
-#pragma unroll
-        for (int m = 0; m < NR; m++) {
-            const int r = m * RG2 * nx;
-            const float4 c4 = *reinterpret_cast<const float4*>(c0 + r);
-            const float4 y4m = *reinterpret_cast<const float4*>(c0 + r - nx);
-            const float4 y4p = *reinterpret_cast<const float4*>(c0 + r + nx);
-            const float4 z4m = *reinterpret_cast<const float4*>(zm + r);
-            const float4 z4p = *reinterpret_cast<const float4*>(zp + r);
-            const float4 a4 = *reinterpret_cast<const float4*>(ca + r);
-            const float4 r4 = *reinterpret_cast<const float4*>(cr + r);
-            float left = __shfl_up_sync(0xffffffffu, c4.w, 1);
-            float right = __shfl_down_sync(0xffffffffu, c4.x, 1);
-            if (lane == 0) left = rowc[r + xl];
-            if (lane == 31) right = rowc[r + xr];
-            float4 n4 = c4;
-            if (xpar == 0) {
-                n4.x = upd(c4.x, left, c4.y, y4m.x, y4p.x, z4m.x, z4p.x, a4.x, r4.x);
-                n4.z = upd(c4.z, c4.y, c4.w, y4m.z, y4p.z, z4m.z, z4p.z, a4.z, r4.z);
-            } else {
-                n4.y = upd(c4.y, c4.x, c4.z, y4m.y, y4p.y, z4m.y, z4p.y, a4.y, r4.y);
-                n4.w = upd(c4.w, c4.z, right, y4m.w, y4p.w, z4m.w, z4p.w, a4.w, r4.w);
-            }
-            nv[m] = n4;
-        }
-#pragma unroll
-        for (int m = 0; m < NR; m++)
-            if (lyb + m * RG2 < ly1) *reinterpret_cast<float4*>(c0 + m * RG2 * nx) = nv[m];
-    };
     // prologue: stages q = 0 .. 4 (unknown planes k0-2 .. k0+2, coefficient
     // planes k0-1 .. k0+1) and AHEAD more
     const bool producer = tid >= NT;
@@ -341,13 +260,8 @@ __device__ __forceinline__ void rbx_run(const Grid& g, const RBXGeom& G, const S
         for (int q = 0; q < 5; q++) ok = ok && wait_stage(q);
     if (__syncthreads_or(!ok)) goto fail;
     // red of k0-1 .. k0+1 read only black cells, which none of them writes
-    using R2Red = std::integral_constant<int, RBX2_RED>;
-    using R2Black = std::integral_constant<int, RBX2_BLACK>;
     if (!producer)
-        for (int p = k0 - 1; p <= k0 + 1; p++) {
-            if constexpr (VW == 2) sweep2(R2Red(), slot(p - 1), slot(p), slot(p + 1), pmod(p, NCF), p, 0, -1, TY + 1);
-            else sweep(RRed(), slot(p - 1), slot(p), slot(p + 1), pmod(p, NCF), p, 0, -1, TY + 1);
-        }
+        for (int p = k0 - 1; p <= k0 + 1; p++) sweep(RRed(), slot(p - 1), slot(p), slot(p + 1), pmod(p, NCF), p, 0, -1, TY + 1);
     // ring slots of unknown plane k-1 and coefficient plane k, advanced by one
     // per step
     sl = slot(k0 - 1);
@@ -379,15 +293,9 @@ __device__ __forceinline__ void rbx_run(const Grid& g, const RBXGeom& G, const S
         if (k + 3 - (k0 - 2) <= qend) ok = wait_stage(k + 3 - (k0 - 2));
         if (!ok) continue;  // leaves at the next barrier
         const int s1 = ring(sl, 1, NPH), s2 = ring(sl, 2, NPH);
-        if constexpr (VW == 2) {
-            sweep2(R2Black(), sl, s1, s2, scl, k, 1, 0, TY);
-            if (k + 2 <= kend)
-                sweep2(R2Red(), s2, ring(sl, 3, NPH), ring(sl, 4, NPH), ring(scl, 2, NCF), k + 2, 0, -1, TY + 1);
-        } else {
-            sweep(RBlack(), sl, s1, s2, scl, k, 1, 0, TY);
-            if (k + 2 <= kend)
-                sweep(RRed(), s2, ring(sl, 3, NPH), ring(sl, 4, NPH), ring(scl, 2, NCF), k + 2, 0, -1, TY + 1);
-        }
+        sweep(RBlack(), sl, s1, s2, scl, k, 1, 0, TY);
+        if (k + 2 <= kend)
+            sweep(RRed(), s2, ring(sl, 3, NPH), ring(sl, 4, NPH), ring(scl, 2, NCF), k + 2, 0, -1, TY + 1);
         sl = s1;
         scl = ring(scl, 1, NCF);
     }
@@ -415,8 +323,7 @@ fail:
 // AH stages in flight beyond the one awaited: RBX_AHEAD with one CTA per SM,
 // or 1 with two (smaller rings, half the shared memory)
 // NT compute threads (256, or 512 in the wide form) and one producer warp
-// VW cells per thread and row: 1, or 2 in the two-cell form
-template <int AH, int NT = RBX_THREADS, int VW = 1>
+template <int AH, int NT = RBX_THREADS>
 __global__ void __launch_bounds__(NT + 32, AH == 1 ? 2 : 1) k_stag_rbx(Grid g, RBXGeom G, StagOp<float> A,
                                                                        RBXArgs R, float omega) {
     extern __shared__ __align__(128) unsigned char rbx_raw[];
@@ -424,9 +331,9 @@ __global__ void __launch_bounds__(NT + 32, AH == 1 ? 2 : 1) k_stag_rbx(Grid g, R
     if (threadIdx.x == 0) mbar_init_fence();
     __syncthreads();
     const int tile_y = blockIdx.x, chunk = blockIdx.y;
-    if (blockIdx.z == 0) rbx_run<0, AH, NT, VW>(g, G, A, R, omega, rbx_raw, tile_y, chunk);
-    else if (blockIdx.z == 1) rbx_run<1, AH, NT, VW>(g, G, A, R, omega, rbx_raw, tile_y, chunk);
-    else rbx_run<2, AH, NT, VW>(g, G, A, R, omega, rbx_raw, tile_y, chunk);
+    if (blockIdx.z == 0) rbx_run<0, AH, NT>(g, G, A, R, omega, rbx_raw, tile_y, chunk);
+    else if (blockIdx.z == 1) rbx_run<1, AH, NT>(g, G, A, R, omega, rbx_raw, tile_y, chunk);
+    else rbx_run<2, AH, NT>(g, G, A, R, omega, rbx_raw, tile_y, chunk);
 }
 
 // geometry for a level (sms: multiprocessors of the device); false when the
@@ -435,31 +342,23 @@ __global__ void __launch_bounds__(NT + 32, AH == 1 ? 2 : 1) k_stag_rbx(Grid g, R
 // ahead: RBX_AHEAD, or 1 for two CTAs per SM where smem_sm (shared memory
 // of one SM) holds two.
 // nt: compute threads, 256 or (with the deep ring) 512.
-// vw: cells per thread and row, 1 or 2 (the two-cell form: nx 128 or 256,
-// 256 compute threads, the deep ring)
 inline bool rbx_geom(const Grid& g, int sms, size_t smem_max, RBXGeom& G, int ty_req = 0, int ahead = RBX_AHEAD,
-                     size_t smem_sm = 0, int nt = RBX_THREADS, int vw = 1) {
+                     size_t smem_sm = 0, int nt = RBX_THREADS) {
     if (ahead != RBX_AHEAD && ahead != 1) return false;
     if (nt != RBX_THREADS && !(nt == 512 && ahead == RBX_AHEAD)) return false;
-    if (vw != 1 && !(vw == 2 && nt == RBX_THREADS && ahead == RBX_AHEAD)) return false;
     const int MR = rbx_maxr(nt);
     G.ahead = ahead;
     G.threads = nt;
-    G.vw = vw;
     if (g.dim != 3) return false;
     const int nx = g.n[0], ny = g.n[1], nz = g.n[2];
     if (nx > RBX_MAXNX || nx < 64 || (nx & (nx - 1)) || (ny & 1) || (nz & 1) || nz < 4) return false;
     const int hx = nx / 2;
     if (nt % hx || hx % 16 || (nt / 32) % (hx / 16)) return false;
-    // the two-cell form: a warp within one row, an even number of rows per pass
-    const int hq = nx / 4, RG2 = nt / hq;
-    if (vw == 2 && (hq < 32 || nt % hq || (RG2 & 1))) return false;
     // tallest tile that fits the shared memory of one CTA per SM
     G.TY = 0;
     for (int ty = 32; ty >= 4; ty /= 2) {
         if (ny % ty || (ty_req > 0 && ty != ty_req)) continue;
-        if (vw == 2 && (ty + 2 > RBX2_RED * RG2 || ty > RBX2_BLACK * RG2)) continue;
-        const size_t smem = rbx_smem_bytes(nx, ty, ahead, nt, vw);
+        const size_t smem = rbx_smem_bytes(nx, ty, ahead, nt);
         if (smem <= smem_max) {
             G.TY = ty;
             G.smem = smem;
@@ -469,12 +368,9 @@ inline bool rbx_geom(const Grid& g, int sms, size_t smem_max, RBXGeom& G, int ty
     if (!G.TY) return false;
     // rows per thread and sweep (ring rows included) within MR
     const int RG = nt / hx;
-    if (vw == 1) {
-        while (ty_req == 0 && G.TY > 4 && (G.TY + 2 + RG - 1) / RG > MR) G.TY /= 2;
-        if ((G.TY + 2 + RG - 1) / RG > MR || (G.TY + RG - 1) / RG > MR - 1) return false;
-    }
-    if (ny % G.TY) return false;
-    G.smem = rbx_smem_bytes(nx, G.TY, ahead, nt, vw);
+    while (ty_req == 0 && G.TY > 4 && (G.TY + 2 + RG - 1) / RG > MR) G.TY /= 2;
+    if ((G.TY + 2 + RG - 1) / RG > MR || (G.TY + RG - 1) / RG > MR - 1 || ny % G.TY) return false;
+    G.smem = rbx_smem_bytes(nx, G.TY, ahead, nt);
     if (G.smem > smem_max) return false;
     // resident CTAs per SM (1 KB of each CTA's shared memory is reserved)
     G.per_sm = (ahead == 1 && 2 * (G.smem + 1024) <= smem_sm) ? 2 : 1;

@@ -84,12 +84,40 @@ Multigrid<float>& mg_of<float>(fhd_ctx* ctx) { return ctx->mg32; }
 // ---------------------------------------------------------------------
 // hierarchy construction (stag_mg_layout_build / mgt_macproj_precon_build)
 // ---------------------------------------------------------------------
+// levels of the multi-box staggered hierarchy and whether its bottom is the
+// fancy nested solve (stag_mg_layout.f90:21-107, stag_mg_solver.f90:97-101,
+// 447): boxes of max_grid_size cells where that is below the domain extent
+static void stag_box_layout(fhd_ctx* ctx, int ns_domain) {
+    ctx->stag_nl_box = 0;
+    ctx->stag_fancy = false;
+    bool any = false, multi = true;
+    int nb[3] = {ctx->n[0], ctx->n[1], ctx->n[2]};
+    for (int d = 0; d < ctx->dim; d++) {
+        const int m = ctx->mgs[d];
+        if (m <= 0 || m >= ctx->n[d]) {
+            multi = false;
+            continue;
+        }
+        nb[d] = m;
+        any = true;
+    }
+    if (!any) return;
+    const Grid gb = make_grid(ctx->dim, nb, ctx->dx);
+    const int nlb = nlevs_mg(gb, ctx->p.stag_mg_minwidth);
+    if (nlb >= ns_domain) return;
+    ctx->stag_nl_box = nlb;
+    ctx->stag_fancy = ctx->p.stag_mg_bottom_solver == 4 && multi;
+}
+
 template <typename T>
 static int build_mg(fhd_ctx* ctx, Multigrid<T>& M) {
     const int dim = ctx->dim;
     const int nE = dim == 2 ? 1 : 3;
     Arena& A = ctx->arena;
-    const int ns = nlevs_mg(ctx->g0, ctx->p.stag_mg_minwidth);
+    int ns = nlevs_mg(ctx->g0, ctx->p.stag_mg_minwidth);
+    stag_box_layout(ctx, ns);
+    // several boxes without the fancy bottom: the hierarchy of the boxes
+    if (ctx->stag_nl_box > 0 && !ctx->stag_fancy) ns = ctx->stag_nl_box;
     M.s.resize(ns);
     for (int l = 0; l < ns; l++) {
         StagLevel<T>& L = M.s[l];
@@ -511,10 +539,6 @@ static int stag_rbx_smooth(fhd_ctx* ctx, StagLevel<float>& L, const RBXGeom& G, 
     if (G.ahead == 1) {
         if (int rc = rb_allow_smem(k_stag_rbx<1>, G.smem, true)) return rc;
         k_stag_rbx<1><<<grd, RBX_BLOCK, G.smem, ctx->stream>>>(L.g, G, L.op(), R, (float)ctx->p.stag_mg_omega);
-    } else if (G.vw == 2) {
-        if (int rc = rb_allow_smem(k_stag_rbx<RBX_AHEAD, RBX_THREADS, 2>, G.smem)) return rc;
-        k_stag_rbx<RBX_AHEAD, RBX_THREADS, 2><<<grd, RBX_BLOCK, G.smem, ctx->stream>>>(L.g, G, L.op(), R,
-                                                                                   (float)ctx->p.stag_mg_omega);
     } else if (G.threads == 512) {
         if (int rc = rb_allow_smem(k_stag_rbx<RBX_AHEAD, 512>, G.smem)) return rc;
         k_stag_rbx<RBX_AHEAD, 512><<<grd, 512 + 32, G.smem, ctx->stream>>>(L.g, G, L.op(), R,
@@ -786,6 +810,57 @@ __global__ void __launch_bounds__(RED_THREADS) k_maxabs(i64 n, const T* a, RedSl
     }
 }
 
+template <typename T>
+static int stag_mg_run(fhd_ctx* ctx, Multigrid<T>& M);
+
+// one V-cycle of the multi-box hierarchy whose bottom, level lb, is the
+// fancy nested stag_mg_solver (stag_mg_solver.f90:447-555): levels lb ..
+// nl-1 of M form the re-boxed bottom problem's own hierarchy; its V-cycle
+// count is restored afterwards, as the reference restores vcycle_counter
+template <typename T>
+static int stag_vcycle_fancy(fhd_ctx* ctx, Multigrid<T>& M, int lb) {
+    const int nl = (int)M.s.size();
+    const int dim = ctx->dim;
+    cudaStream_t st = ctx->stream;
+    for (int l = 1; l < nl; l++)
+        for (int c = 0; c < dim; c++) FHD_CUDA_TRY(cudaMemsetAsync(M.s[l].phi[c], 0, sizeof(T) * M.s[l].g.nc, st));
+    for (int l = 0; l < lb; l++) {
+        StagLevel<T>& L = M.s[l];
+        StagLevel<T>& C = M.s[l + 1];
+        int rc = stag_smooths(ctx, L, ctx->p.stag_mg_nsmooths_down);
+        if (!rc) rc = stag_residual(ctx, L);
+        if (rc) return rc;
+        with_dim(dim, [&](auto D) {
+            constexpr int DIM = decltype(D)::value;
+            k_stag_restrict<T, DIM><<<cell_grid(C.g), cell_block(), 0, st>>>(L.g, C.g, L.tmp[0], L.tmp[1], L.tmp[2],
+                                                                           C.rhs[0], C.rhs[1], C.rhs[2], 0);
+            rc |= post(ctx);
+        });
+        if (rc) return rc;
+    }
+    Multigrid<T> B;  // a view of levels lb .. nl-1 (the levels' arrays are shared)
+    B.s.assign(M.s.begin() + lb, M.s.end());
+    const int vsaved = ctx->vcycles;
+    int rc = stag_mg_run(ctx, B);
+    ctx->vcycles = vsaved;
+    if (rc) return rc;
+    for (int l = lb - 1; l >= 0; l--) {
+        StagLevel<T>& L = M.s[l];
+        StagLevel<T>& C = M.s[l + 1];
+        with_dim(dim, [&](auto D) {
+            constexpr int DIM = decltype(D)::value;
+            k_stag_prolong<T, DIM><<<cell_grid(C.g), cell_block(), 0, st>>>(L.g, C.g, L.phi[0], L.phi[1], L.phi[2],
+                                                                          C.phi[0], C.phi[1], C.phi[2],
+                                                                          pair_aligned(dim, L.phi));
+            rc |= post(ctx);
+        });
+        if (rc) return rc;
+        rc = stag_smooths(ctx, L, ctx->p.stag_mg_nsmooths_up);
+        if (rc) return rc;
+    }
+    return 0;
+}
+
 // stag_mg_solver (stag_mg_solver.f90:37-863) on level-0 phi/rhs of M
 template <typename T>
 static int stag_mg_run(fhd_ctx* ctx, Multigrid<T>& M) {
@@ -798,15 +873,15 @@ static int stag_mg_run(fhd_ctx* ctx, Multigrid<T>& M) {
         int rc = stag_residual(ctx, L0);
         if (rc) return rc;
         for (int c = 0; c < dim; c++) {
-            k_maxabs<T><<<flat_blocks(nc), RED_THREADS, 0, ctx->stream>>>(nc, L0.tmp[c], slot(ctx, S_NRM + c));
+            k_maxabs<T><<<flat_blocks(nc), RED_THREADS, 0, ctx->stream>>>(nc, L0.tmp[c], slot(ctx, S_MG + c));
             FHD_POST(ctx);
         }
-        rc = sync_scalars(ctx, S_NRM, dim);
+        rc = sync_scalars(ctx, S_MG, dim);
         if (rc) return rc;
         bool allzero = true, anyzero = false;
         double rmax = 0;
         for (int c = 0; c < dim; c++) {
-            resid0[c] = ctx->hscal[S_NRM + c];
+            resid0[c] = ctx->hscal[S_MG + c];
             allzero = allzero && resid0[c] == 0.0;
             anyzero = anyzero || resid0[c] == 0.0;
             rmax = fmax(rmax, resid0[c]);
@@ -815,20 +890,25 @@ static int stag_mg_run(fhd_ctx* ctx, Multigrid<T>& M) {
         if (anyzero)
             for (int c = 0; c < dim; c++) resid0[c] = rmax;
     }
+    // the fancy bottom changes the cycle only when its nested solve may take
+    // more than one V-cycle: with one, the nested cycle smooths the shared
+    // level before and after it exactly as an intermediate level is smoothed
+    const bool nested = ctx->stag_fancy && maxv > 1 && M.s.size() == mg_of<T>(ctx).s.size() &&
+                        ctx->stag_nl_box > 1 && ctx->stag_nl_box < (int)M.s.size();
     for (int vc = 1; vc <= maxv; vc++) {
-        int rc = stag_vcycle(ctx, M);
+        int rc = nested ? stag_vcycle_fancy(ctx, M, ctx->stag_nl_box - 1) : stag_vcycle(ctx, M);
         if (rc) return rc;
         if (vc == maxv) break;
         rc = stag_residual(ctx, L0);
         if (rc) return rc;
         for (int c = 0; c < dim; c++) {
-            k_maxabs<T><<<flat_blocks(nc), RED_THREADS, 0, ctx->stream>>>(nc, L0.tmp[c], slot(ctx, S_NRM + c));
+            k_maxabs<T><<<flat_blocks(nc), RED_THREADS, 0, ctx->stream>>>(nc, L0.tmp[c], slot(ctx, S_MG + c));
             FHD_POST(ctx);
         }
-        rc = sync_scalars(ctx, S_NRM, dim);
+        rc = sync_scalars(ctx, S_MG, dim);
         if (rc) return rc;
         bool done = true;
-        for (int c = 0; c < dim; c++) done = done && (ctx->hscal[S_NRM + c] / resid0[c] < ctx->p.stag_mg_rel_tol);
+        for (int c = 0; c < dim; c++) done = done && (ctx->hscal[S_MG + c] / resid0[c] < ctx->p.stag_mg_rel_tol);
         if (done) break;
     }
     ctx->vcycles += dim * maxv;
@@ -992,14 +1072,11 @@ static std::vector<SmoothPlan> stag_cands(fhd_ctx* ctx, const StagLevel<T>& L) {
     colour_cands(v, L.g);
     rb_cands(v, L.g, 3, (int)sizeof(T), 2, ctx->smem_optin);
     if (std::is_same<T, float>::value && ctx->visc == 1)
-        // deep ring; short ring, two CTAs per SM; deep ring, 512 threads;
-        // deep ring, two cells per thread and row
-        for (int form = 0; form < 4; form++)
+        for (int form = 0; form < 3; form++)  // deep ring; short ring, two CTAs per SM; deep ring, 512 threads
             for (int ty = 4; ty <= 32; ty *= 2) {
                 RBXGeom X;
                 const int ahead = form == 1 ? 1 : RBX_AHEAD, nt = form == 2 ? 512 : RBX_THREADS;
-                const int vw = form == 3 ? 2 : 1;
-                if (!rbx_geom(L.g, ctx->sms, (size_t)ctx->smem_optin, X, ty, ahead, (size_t)ctx->smem_sm, nt, vw))
+                if (!rbx_geom(L.g, ctx->sms, (size_t)ctx->smem_optin, X, ty, ahead, (size_t)ctx->smem_sm, nt))
                     continue;
                 SmoothPlan p;
                 p.kind = 2;
@@ -1250,11 +1327,11 @@ static int cc_solve(fhd_ctx* ctx, Multigrid<T>& M) {
     const int maxv = ctx->p.mg_max_vcycles;
     double r0 = 1.0;
     if (maxv > 1) {
-        k_maxabs<T><<<flat_blocks(nc), RED_THREADS, 0, ctx->stream>>>(nc, C.rhs, slot(ctx, S_NRM));
+        k_maxabs<T><<<flat_blocks(nc), RED_THREADS, 0, ctx->stream>>>(nc, C.rhs, slot(ctx, S_MG));
         FHD_POST(ctx);
-        int rc = sync_scalars(ctx, S_NRM, 1);
+        int rc = sync_scalars(ctx, S_MG, 1);
         if (rc) return rc;
-        r0 = ctx->hscal[S_NRM];
+        r0 = ctx->hscal[S_MG];
         if (r0 == 0.0) return 0;
     }
     const int lc = cc_coarse_first(ctx, M);
@@ -1268,11 +1345,11 @@ static int cc_solve(fhd_ctx* ctx, Multigrid<T>& M) {
             rc |= post(ctx);
         });
         if (rc) return rc;
-        k_maxabs<T><<<flat_blocks(nc), RED_THREADS, 0, ctx->stream>>>(nc, C.tmp, slot(ctx, S_NRM));
+        k_maxabs<T><<<flat_blocks(nc), RED_THREADS, 0, ctx->stream>>>(nc, C.tmp, slot(ctx, S_MG));
         FHD_POST(ctx);
-        rc = sync_scalars(ctx, S_NRM, 1);
+        rc = sync_scalars(ctx, S_MG, 1);
         if (rc) return rc;
-        if (ctx->hscal[S_NRM] <= fmax(ctx->p.mg_rel_tol * r0, ctx->p.mg_abs_tol)) break;
+        if (ctx->hscal[S_MG] <= fmax(ctx->p.mg_rel_tol * r0, ctx->p.mg_abs_tol)) break;
     }
     ctx->vcycles += maxv;
     return 0;
@@ -1987,8 +2064,36 @@ const char* fhd_status_string(int s) {
 
 const char* fhd_last_error(void) { return g_last_error.c_str(); }
 
+static int ctx_create(int dim, const int n_cells[3], const int max_grid_size[3], const double dx[3], int visc_type,
+                      const fhd_gmres_params* params, int precision_mode, fhd_ctx** out);
+
 int fhd_ctx_create(int dim, const int n_cells[3], const double dx[3], int visc_type, const fhd_gmres_params* params,
                    int precision_mode, fhd_ctx** out) {
+    return ctx_create(dim, n_cells, nullptr, dx, visc_type, params, precision_mode, out);
+}
+
+int fhd_ctx_create_bc(int dim, const int n_cells[3], const int max_grid_size[3], const int bc_lo[3],
+                      const int bc_hi[3], const double dx[3], int visc_type, const fhd_gmres_params* params,
+                      int precision_mode, fhd_ctx** out) {
+    if (!out || !n_cells || !max_grid_size || !bc_lo || !bc_hi || (dim != 2 && dim != 3)) return FHD_ERR_BAD_ARG;
+    *out = nullptr;
+    for (int d = 0; d < dim; d++) {
+        if (bc_lo[d] != FHD_BC_PERIODIC || bc_hi[d] != FHD_BC_PERIODIC) {
+            set_last_error("fhd_ctx_create_bc: only periodic boundaries (bc code -1) are built; walls and "
+                           "reservoirs are not");
+            return FHD_ERR_UNSUPPORTED;
+        }
+        if (max_grid_size[d] < 1) return FHD_ERR_BAD_ARG;
+        if (max_grid_size[d] < n_cells[d] && n_cells[d] % max_grid_size[d] != 0) {
+            set_last_error("fhd_ctx_create_bc: max_grid_size must divide n_cells (boxes of equal size)");
+            return FHD_ERR_UNSUPPORTED;
+        }
+    }
+    return ctx_create(dim, n_cells, max_grid_size, dx, visc_type, params, precision_mode, out);
+}
+
+static int ctx_create(int dim, const int n_cells[3], const int max_grid_size[3], const double dx[3], int visc_type,
+                      const fhd_gmres_params* params, int precision_mode, fhd_ctx** out) {
     if (!out || !n_cells || !dx || (dim != 2 && dim != 3)) return FHD_ERR_BAD_ARG;
     *out = nullptr;
     if (visc_type == 0 || visc_type < -3 || visc_type > 3) return FHD_ERR_BAD_ARG;
@@ -2001,6 +2106,7 @@ int fhd_ctx_create(int dim, const int n_cells[3], const double dx[3], int visc_t
     fhd_ctx* c = new fhd_ctx();
     c->dim = dim;
     for (int d = 0; d < 3; d++) c->n[d] = (d < dim) ? n_cells[d] : 1;
+    for (int d = 0; d < 3; d++) c->mgs[d] = (max_grid_size && d < dim) ? max_grid_size[d] : 0;
     c->dx = dx[0];
     c->visc = visc_type;
     c->prec = precision_mode == FHD_PREC_MIXED ? FHD_PREC_MIXED : FHD_PREC_FP64;
@@ -2244,7 +2350,7 @@ int fhd_tune_candidates(int which, int dim, const int n_cells[3], int precision_
     for (int i = 0; i < (int)v.size() && i < max_out; i++) {
         const SmoothPlan& P = v[i];
         int* o = out + 7 * i;
-        o[0] = (P.kind == 2 && P.rbx.vw == 2) ? 3 : P.kind;
+        o[0] = P.kind;
         o[1] = P.kind == 0 ? P.bx : P.kind == 1 ? P.rb.TX : g.n[0];
         o[2] = P.kind == 0 ? P.by : P.kind == 1 ? P.rb.TY : P.rbx.TY;
         o[3] = P.kind == 1 ? P.rb.chunks : P.kind == 2 ? P.rbx.chunks : 0;
@@ -2266,8 +2372,7 @@ int fhd_ctx_tune_info(fhd_ctx* c, int which, int level, int* kind, int* ncand, d
         if (which == 1 && level < (int)c->mg64.c.size()) P = &c->mg64.c[level].plan;
     }
     if (!P) return FHD_ERR_BAD_ARG;
-    // kind 3 reports the two-cell form of the row-tile smooth
-    if (kind) *kind = (P->kind == 2 && P->rbx.vw == 2) ? 3 : P->kind;
+    if (kind) *kind = P->kind;
     if (ncand) *ncand = P->ncand;
     if (pair_us) *pair_us = P->us;
     if (shape) {

@@ -213,6 +213,13 @@ struct Multigrid {
 struct fhd_ctx {
     int dim = 2;
     int n[3] = {1, 1, 1};
+    // box layout of the level (probin_common max_grid_size; 0 = one box):
+    // the staggered multigrid of several boxes stops at the boxes' depth,
+    // or (stag_mg_bottom_solver 4, n/max_grid_size >= 2) solves its bottom
+    // by a nested solve over the deeper levels of the domain ("fancy")
+    int mgs[3] = {0, 0, 0};
+    int stag_nl_box = 0;      // levels of the box hierarchy (0: the domain's)
+    bool stag_fancy = false;  // nested bottom solve from level stag_nl_box - 1
     double dx = 1.0;
     int visc = 1;
     int prec = FHD_PREC_FP64;
@@ -292,6 +299,10 @@ constexpr int S_H = 0;        // H column, 1..m+1
 constexpr int S_NRM = 128;    // norm squares
 constexpr int S_MEAN = 140;   // mean sums
 constexpr int S_Y = 160;      // least-squares y (m <= 64)
+// the multigrids' own convergence checks (stag_mg_max_vcycles,
+// mg_max_vcycles > 1): apart from the norms GMRES holds across a
+// preconditioner application
+constexpr int S_MG = 232;
 
 inline RedSlot slot(fhd_ctx* c, int i) {
     RedSlot r;

@@ -356,3 +356,10 @@ def stochastic_mass_fluxdiv(dim, n, dx, sp, mp, sqrtL, dt, weights, W_fc, increm
                                      C.c_double(dt), C.cast(w, _DP), len(weights), _pp(W_fc), int(bool(increment)),
                                      _pp(div), _pp(flux) if flux is not None else None)
     return div, flux
+
+
+def set_max_grid_size(mgs=None):
+    """probin_common max_grid_size of the staggered multigrid's box layout
+    (module state of the oracle); None: one box"""
+    a = (C.c_int * 3)(*((list(mgs) + [0] * 3)[:3] if mgs else [0, 0, 0]))
+    lib().or_set_max_grid_size(a)

@@ -15,6 +15,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <functional>
 #include <vector>
 #ifdef _OPENMP
 #include <omp.h>
@@ -368,13 +369,52 @@ int nlevs_mg(const Geo& g, int minwidth) {
     return nl;
 }
 
-// stag_mg_solver (stag_mg_solver.f90:37-863), single box (the "fancy"
-// bottom solver needs n_cells/max_grid_size >= 2 and is never taken here)
+// The box layout of the level (probin_common max_grid_size), module state as
+// in the reference: boxes of max_grid_size cells per direction (which must
+// divide n_cells); 0 = one box covering the domain.
+int g_max_grid_size[3] = {0, 0, 0};
+
+// levels of the multi-box hierarchy (compute_nlevs_mg over boxes of
+// max_grid_size) and whether its bottom is the "fancy" nested solve
+// (stag_mg_solver.f90:97-101, 447): on when stag_mg_bottom_solver = 4 and
+// n_cells / max_grid_size >= 2 in every direction
+void box_layout(const Geo& g0, const fhd_gmres_params* p, int nl_domain, int* nl_box, bool* fancy) {
+    *nl_box = nl_domain;
+    *fancy = false;
+    bool multi = true, any = false;
+    int nb[3] = {g0.n[0], g0.n[1], g0.n[2]};
+    for (int d = 0; d < g0.dim; d++) {
+        const int m = g_max_grid_size[d];
+        if (m <= 0 || m >= g0.n[d]) {
+            multi = false;
+            continue;
+        }
+        nb[d] = m;
+        any = true;
+    }
+    if (!any) return;
+    Geo gb(g0.dim, nb, g0.dx);
+    *nl_box = nlevs_mg(gb, p->stag_mg_minwidth);
+    *fancy = (p->stag_mg_bottom_solver == 4) && multi;
+}
+
+// stag_mg_solver (stag_mg_solver.f90:37-863).  With one box the hierarchy
+// has compute_nlevs_mg(domain) levels.  With several boxes it has
+// compute_nlevs_mg(box) levels; its bottom is either nsmooths_bottom smooths
+// or, "fancy" (stag_mg_solver.f90:447-555), a nested stag_mg_solver on the
+// bottom grid re-boxed as one box (stag_mg_layout.f90:96-107), whose own
+// levels are the deeper levels of the domain hierarchy.
 int stag_mg(const Geo& g0, int visc, const fhd_gmres_params* p, const double* const alpha_fc[],
             const double* beta, const double* const beta_ed[], const double* gamma, double theta,
             double* const phi[], const double* const rhs[], double* hist = nullptr) {
     const int dim = g0.dim;
-    const int nl = nlevs_mg(g0, p->stag_mg_minwidth);
+    const int nl_domain = nlevs_mg(g0, p->stag_mg_minwidth);
+    int nl_box;
+    bool fancy;
+    box_layout(g0, p, nl_domain, &nl_box, &fancy);
+    // levels built: the whole domain hierarchy when the fancy bottom may
+    // descend it, else the box hierarchy
+    const int nl = fancy ? nl_domain : nl_box;
     std::vector<SLevel> L(nl);
     for (int l = 0; l < nl; l++) {
         L[l].g = (l == 0) ? g0 : L[l - 1].g.coarsen();
@@ -405,75 +445,86 @@ int stag_mg(const Geo& g0, int visc, const fhd_gmres_params* p, const double* co
         std::copy(phi[c], phi[c] + nc0, L[0].phi[c].begin());
         std::copy(rhs[c], rhs[c] + nc0, L[0].rhs[c].begin());
     }
-    // initial residual (stag_mg_solver.f90:259-313)
-    double resid0[3] = {0, 0, 0};
-    s_applyop(L[0], visc, 0);
-    for (int c = 0; c < dim; c++) {
-        const double* lp = L[0].Lphi[c].data();
-        const double* r = L[0].rhs[c].data();
-        resid0[c] = reduce_max(g0, [&](int i, int j, int k) { long f = g0.id(i, j, k); return std::fabs(lp[f] - r[f]); });
-    }
-    // L2 norm of the initial residual, for the per-V-cycle history that
-    // stag_mg_verbosity >= 1 prints (stag_mg_solver.f90:782-785)
-    double r0l2 = 0.0;
-    if (hist) {
-        for (int c = 0; c < dim; c++) {
-            const double* lp = L[0].Lphi[c].data();
-            const double* r = L[0].rhs[c].data();
-            r0l2 += reduce_sum(g0, [&](int i, int j, int k) { long f = g0.id(i, j, k); double d = lp[f] - r[f]; return d * d; });
-        }
-    }
-    bool allzero = true, anyzero = false;
-    double rmax = 0.0;
-    for (int c = 0; c < dim; c++) {
-        allzero = allzero && (resid0[c] == 0.0);
-        anyzero = anyzero || (resid0[c] == 0.0);
-        rmax = std::max(rmax, resid0[c]);
-    }
-    if (allzero) return 0;
-    if (anyzero)
-        for (int c = 0; c < dim; c++) resid0[c] = rmax;
-
     std::vector<int> colors;
     if (p->stag_mg_smoother == 0) colors.push_back(0);
     else for (int c = 1; c <= 2 * dim; c++) colors.push_back(c);
     const double omega = p->stag_mg_omega;
 
-    for (int vc = 1; vc <= p->stag_mg_max_vcycles; vc++) {
-        for (int l = 1; l < nl; l++)
-            for (int c = 0; c < dim; c++) std::fill(L[l].phi[c].begin(), L[l].phi[c].end(), 0.0);
-        for (int l = 0; l < nl - 1; l++) {
-            for (int m = 0; m < p->stag_mg_nsmooths_down; m++)
-                for (int col : colors) s_smooth(L[l], visc, omega, col);
-            s_applyop(L[l], visc, 0);
-            for (int c = 0; c < dim; c++) {
-                double* lp = L[l].Lphi[c].data();
-                const double* r = L[l].rhs[c].data();
-                for (long f = 0; f < L[l].g.nc; f++) lp[f] = -(lp[f] - r[f]);
-            }
-            s_restrict(L[l].g, L[l + 1].g, L[l].Lphi, L[l + 1].rhs, false);
-        }
-        for (int m = 0; m < p->stag_mg_nsmooths_bottom; m++)
-            for (int col : colors) s_smooth(L[nl - 1], visc, omega, col);
-        for (int l = nl - 2; l >= 0; l--) {
-            s_prolong_add(L[l].g, L[l + 1].g, L[l].phi, L[l + 1].phi);
-            for (int m = 0; m < p->stag_mg_nsmooths_up; m++)
-                for (int col : colors) s_smooth(L[l], visc, omega, col);
-        }
-        if (vc == p->stag_mg_max_vcycles && !hist) break;  // the final residual decides nothing
-        s_applyop(L[0], visc, 0);
-        bool done = true;
-        double rl2 = 0.0;
+    // V-cycles on levels l0 .. lend-1 with level l0's phi and rhs as the
+    // problem (one stag_mg_solver call); nest: the level whose bottom solve
+    // is a nested call on levels nest .. nl-1 (the fancy bottom), or -1
+    std::function<void(int, int, int, double*)> solve = [&](int l0, int lend, int nest, double* hst) {
+        const Geo& gl = L[l0].g;
+        // initial residual (stag_mg_solver.f90:259-313)
+        double resid0[3] = {0, 0, 0};
+        s_applyop(L[l0], visc, 0);
         for (int c = 0; c < dim; c++) {
-            const double* lp = L[0].Lphi[c].data();
-            const double* r = L[0].rhs[c].data();
-            double rr = reduce_max(g0, [&](int i, int j, int k) { long f = g0.id(i, j, k); return std::fabs(lp[f] - r[f]); });
-            done = done && (rr / resid0[c] < p->stag_mg_rel_tol);
-            if (hist) rl2 += reduce_sum(g0, [&](int i, int j, int k) { long f = g0.id(i, j, k); double d = lp[f] - r[f]; return d * d; });
+            const double* lp = L[l0].Lphi[c].data();
+            const double* r = L[l0].rhs[c].data();
+            resid0[c] = reduce_max(gl, [&](int i, int j, int k) { long f = gl.id(i, j, k); return std::fabs(lp[f] - r[f]); });
         }
-        if (hist) hist[vc - 1] = std::sqrt(rl2) / std::sqrt(r0l2);
-        if (done || vc == p->stag_mg_max_vcycles) break;
-    }
+        // L2 norm of the initial residual, for the per-V-cycle history that
+        // stag_mg_verbosity >= 1 prints (stag_mg_solver.f90:782-785)
+        double r0l2 = 0.0;
+        if (hst) {
+            for (int c = 0; c < dim; c++) {
+                const double* lp = L[l0].Lphi[c].data();
+                const double* r = L[l0].rhs[c].data();
+                r0l2 += reduce_sum(gl, [&](int i, int j, int k) { long f = gl.id(i, j, k); double d = lp[f] - r[f]; return d * d; });
+            }
+        }
+        bool allzero = true, anyzero = false;
+        double rmax = 0.0;
+        for (int c = 0; c < dim; c++) {
+            allzero = allzero && (resid0[c] == 0.0);
+            anyzero = anyzero || (resid0[c] == 0.0);
+            rmax = std::max(rmax, resid0[c]);
+        }
+        if (allzero) return;
+        if (anyzero)
+            for (int c = 0; c < dim; c++) resid0[c] = rmax;
+        const int bottom = nest >= 0 ? nest : lend - 1;
+        for (int vc = 1; vc <= p->stag_mg_max_vcycles; vc++) {
+            for (int l = l0 + 1; l < lend; l++)
+                for (int c = 0; c < dim; c++) std::fill(L[l].phi[c].begin(), L[l].phi[c].end(), 0.0);
+            for (int l = l0; l < bottom; l++) {
+                for (int m = 0; m < p->stag_mg_nsmooths_down; m++)
+                    for (int col : colors) s_smooth(L[l], visc, omega, col);
+                s_applyop(L[l], visc, 0);
+                for (int c = 0; c < dim; c++) {
+                    double* lp = L[l].Lphi[c].data();
+                    const double* r = L[l].rhs[c].data();
+                    for (long f = 0; f < L[l].g.nc; f++) lp[f] = -(lp[f] - r[f]);
+                }
+                s_restrict(L[l].g, L[l + 1].g, L[l].Lphi, L[l + 1].rhs, false);
+            }
+            if (nest >= 0) {
+                solve(nest, lend, -1, nullptr);  // theta_alpha = 1: the level's alpha carries it
+            } else {
+                for (int m = 0; m < p->stag_mg_nsmooths_bottom; m++)
+                    for (int col : colors) s_smooth(L[bottom], visc, omega, col);
+            }
+            for (int l = bottom - 1; l >= l0; l--) {
+                s_prolong_add(L[l].g, L[l + 1].g, L[l].phi, L[l + 1].phi);
+                for (int m = 0; m < p->stag_mg_nsmooths_up; m++)
+                    for (int col : colors) s_smooth(L[l], visc, omega, col);
+            }
+            if (vc == p->stag_mg_max_vcycles && !hst) break;  // the final residual decides nothing
+            s_applyop(L[l0], visc, 0);
+            bool done = true;
+            double rl2 = 0.0;
+            for (int c = 0; c < dim; c++) {
+                const double* lp = L[l0].Lphi[c].data();
+                const double* r = L[l0].rhs[c].data();
+                double rr = reduce_max(gl, [&](int i, int j, int k) { long f = gl.id(i, j, k); return std::fabs(lp[f] - r[f]); });
+                done = done && (rr / resid0[c] < p->stag_mg_rel_tol);
+                if (hst) rl2 += reduce_sum(gl, [&](int i, int j, int k) { long f = gl.id(i, j, k); double d = lp[f] - r[f]; return d * d; });
+            }
+            if (hst) hst[vc - 1] = std::sqrt(rl2) / std::sqrt(r0l2);
+            if (done || vc == p->stag_mg_max_vcycles) break;
+        }
+    };
+    solve(0, nl, fancy && nl_box < nl ? nl_box - 1 : -1, hist);
     for (int c = 0; c < dim; c++) std::copy(L[0].phi[c].begin(), L[0].phi[c].end(), phi[c]);
     return 0;
 }
@@ -1620,6 +1671,12 @@ int or_num_threads(void) {
 #else
     return 1;
 #endif
+}
+
+// probin_common max_grid_size for the staggered multigrid's box layout
+// (module state, as in the reference); 0 or >= n_cells: one box
+void or_set_max_grid_size(const int mgs[3]) {
+    for (int d = 0; d < 3; d++) g_max_grid_size[d] = mgs ? mgs[d] : 0;
 }
 
 int or_compute_nlevs_mg(int dim, const int n[3], int minwidth) {

@@ -20,6 +20,9 @@ extern "C" {
 #endif
 
 /* number of staggered MG levels (stag_mg_layout.f90:179-222) */
+/* max_grid_size of the level's box layout for the staggered multigrid
+ * (module state); NULL or zeros: one box */
+void or_set_max_grid_size(const int mgs[3]);
 int or_compute_nlevs_mg(int dim, const int n[3], int minwidth);
 
 /* stag_applyop_level with colour (stag_applyop.f90:70-1075); alpha_fc is

@@ -60,8 +60,6 @@ def test_every_candidate_matches_the_rules(cuda, dim, n, visc, precision):
     expect = {"colour"} if dim == 2 else {"colour", "tiled"}
     if dim == 3 and visc == 1 and precision == "mixed":
         expect.add("rowtile")
-        if n[0] >= 128:
-            expect.add("rowtile2")
     assert expect <= kinds
 
 
@@ -72,7 +70,7 @@ def test_tuned_plan_is_timed_cached_and_equal(cuda, dim, n, visc, precision):
     out2, info2 = _run(cuda, dim, n, visc, precision, 1)
     for info in (info1, info2):
         for lv in info:
-            assert lv["kind"] in ("colour", "tiled", "rowtile", "rowtile2")
+            assert lv["kind"] in ("colour", "tiled", "rowtile")
             assert lv["candidates"] >= 1 and lv["pair_us"] > 0
     # the second context reuses the first one's measurement
     assert info1 == info2

@@ -15,16 +15,7 @@ def kinds(c):
 
 def test_fp32_visc1_large_level_has_every_kind():
     c = L.tune_candidates("stag", 3, [256, 256, 256], "mixed", 1)
-    assert kinds(c) == {"colour", "tiled", "rowtile", "rowtile2"}
-    # the two-cell form: whole warps per row, 3 red and 2 black passes of 4
-    # rows cover a 4- or 8-row tile and its ring rows
-    two = [x for x in c if x["kind"] == "rowtile2"]
-    assert {(x["y"], x["per_sm"], x["threads"]) for x in two} == {(4, 1, 256), (8, 1, 256)}
-    assert all(x["smem"] <= 232448 for x in two)
-    c128 = L.tune_candidates("stag", 3, [128, 128, 128], "mixed", 1)
-    assert {x["y"] for x in c128 if x["kind"] == "rowtile2"} == {4, 8, 16}
-    # no whole warp per row below 128 cells
-    assert "rowtile2" not in kinds(L.tune_candidates("stag", 3, [64, 64, 64], "mixed", 1))
+    assert kinds(c) == {"colour", "tiled", "rowtile"}
     rows = [x for x in c if x["kind"] == "rowtile"]
     # one CTA per SM with the deep ring for 4- and 8-row tiles (256 or 512
     # compute threads); the short ring only where two CTAs fit on one SM
@@ -45,7 +36,7 @@ def test_fp32_visc1_large_level_has_every_kind():
 @pytest.mark.parametrize("prec,visc", [("fp64", 1), ("mixed", -1), ("mixed", 2)])
 def test_rowtile_only_for_fp32_constant_viscosity(prec, visc):
     c = L.tune_candidates("stag", 3, [128, 128, 128], prec, visc)
-    assert "rowtile" not in kinds(c) and "rowtile2" not in kinds(c)
+    assert "rowtile" not in kinds(c)
     assert {"colour", "tiled"} <= kinds(c)
     if prec == "fp64":
         for x in c:
