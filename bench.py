@@ -214,15 +214,53 @@ BATCH_STEPS = 20
 BATCH_SLOTS = 16
 
 
+def batch_realizations(count, seed):
+    """sides log-uniform in [32, 256] rounded to multiples of 8, eta ~
+    U[0.5, 5] (seeded)"""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    sides = np.clip(np.round(np.exp(rng.uniform(math.log(32), math.log(256), count)) / 8) * 8, 32, 256).astype(int)
+    return sides, rng.uniform(0.5, 5.0, count)
+
+
+def run_batch_solver(L, torch, dev, count=BATCH_REALIZATIONS, steps=BATCH_STEPS, seed=1):
+    """the same realizations through the batched solver (fhd_batch_*): every
+    box advanced together, one launch per multigrid level and operation for
+    all 512 boxes.  The call synchronises its own stream once per GMRES
+    cycle, so the time is host wall time around the synchronous call, after
+    one untimed warm-up step."""
+    sides, etas = batch_realizations(count, seed)
+    sizes = [(int(n), int(n)) for n in sides]
+    params = L.default_params(gmres_rel_tol=REL_TOL)
+    with L.Batch(sizes, 1.0, params=params, precision="mixed") as B:
+        u = [torch.zeros(B.total, dtype=torch.float64, device=dev) for _ in range(2)]
+        pi = torch.zeros(B.total, dtype=torch.float64, device=dev)
+        kT = [1.0] * count
+        torch.cuda.synchronize()
+        B.overdamped(u, pi, etas, kT, 0.1, 1, seed=seed, step0=0)
+        n0 = B.kernel_launches
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        status, iters = B.overdamped(u, pi, etas, kT, 0.1, steps, seed=seed, step0=1)
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+        launches = B.kernel_launches - n0
+        finite = bool(torch.isfinite(u[0]).all().item() and torch.isfinite(pi).all().item())
+        cells = B.total
+    return {"realizations": count, "steps_each": steps, "cells": cells,
+            "realization_steps_per_s": count * steps / wall, "wall_s": wall,
+            "timing": "host wall time around the synchronous call (one sync per GMRES cycle inside)",
+            "gmres_iters": int(sum(iters)), "gmres_iters_max_box": int(max(iters)),
+            "kernel_launches": launches, "launches_per_step": launches / steps,
+            "status": status, "finite": finite}
+
+
 def run_batched(L, count=BATCH_REALIZATIONS, steps=BATCH_STEPS, slots=BATCH_SLOTS, seed=1):
     """count 2D periodic realizations, sides log-uniform in [32, 256] rounded
     to multiples of 8 (seeded), eta ~ U[0.5, 5], `steps` overdamped steps
     each, FP32 preconditioner inside FP64 GMRES at 1e-8; all submitted at
     once to one server.  Returns realization-steps per second."""
-    import numpy as np
-    rng = np.random.default_rng(seed)
-    sides = np.clip(np.round(np.exp(rng.uniform(math.log(32), math.log(256), count)) / 8) * 8, 32, 256).astype(int)
-    etas = rng.uniform(0.5, 5.0, count)
+    sides, etas = batch_realizations(count, seed)
     reqs = [L.make_request(kind=L.FHD_REQ_OVERDAMPED, dim=2, n_cells=[int(n), int(n)], eta=float(e), kT=1.0,
                            dt=0.1, steps=steps, seed=5000 + i, precision=L.FHD_PREC_MIXED,
                            params=L.default_params(gmres_rel_tol=REL_TOL))
@@ -772,6 +810,7 @@ def main():
             "fp64_one_at_a_time": plain,
         }
         line["batched"] = run_batched(L)
+        line["batched"]["one_launch_per_level"] = run_batch_solver(L, torch, dev)
     if ws > 1:
         barrier(ws)
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:

@@ -660,6 +660,50 @@ int fhd_stochastic_mass_fluxdiv(fhd_ctx* ctx, const fhd_mixture_params* mp,
                                 double dt, const double* weights, int n_rngs,
                                 const fhd_multifab* W_fc, int increment);
 
+/* ------------------------------------------------------------------ */
+/* batched realizations: many independent 2D periodic boxes of uneven  */
+/* size solved together (no counterpart in the reference, whose driver */
+/* runs one problem per process)                                      */
+/* ------------------------------------------------------------------ */
+/* A batch of nboxes 2D periodic boxes, box b of n_cells[2b] x n_cells[2b+1]
+ * cells of side dx, with one multigrid hierarchy per box (compute_nlevs_mg
+ * each) packed level by level: every launch of a multigrid level or a
+ * Krylov pass covers all boxes, the coarse end of each box's V-cycles runs
+ * in one CTA per box, and GMRES's scalar control (Arnoldi coefficients,
+ * Givens rotations, stopping tests) runs on the device, one thread per box.
+ * Operator: visc_type 1 with a constant viscosity per box, density 1,
+ * precon_type 1 (apply_precon.f90:103-195), one V-cycle per multigrid call;
+ * precision_mode as fhd_ctx_create (FP32 multigrid in FP64 GMRES, or FP64).
+ * Vectors are device arrays of all boxes' cells concatenated in box order,
+ * each box in the canonical layout; fhd_batch_box_offset(B, b) is the first
+ * element of box b (b = nboxes: the total). */
+typedef struct fhd_batch fhd_batch;
+int fhd_batch_create(int nboxes, const int* n_cells, double dx,
+                     const fhd_gmres_params* params, int precision_mode,
+                     fhd_batch** out);
+int fhd_batch_destroy(fhd_batch* batch);
+long long fhd_batch_box_offset(fhd_batch* batch, int box);
+long long fhd_batch_kernel_launches(fhd_batch* batch);
+/* gmres (gmres.f90:32-491) of every box: b = (b_u x, b_u y, b_p), x the
+ * initial guess in and the solution out, eta[nboxes] (host) the boxes'
+ * viscosities, theta_alpha shared.  Each box follows exactly the steps it
+ * would take alone.  stats (nullable): nboxes records.  Returns the worst
+ * status of the boxes. */
+int fhd_batch_gmres(fhd_batch* batch, const double* const b[3],
+                    double* const x[3], const double* eta,
+                    double theta_alpha, fhd_solve_stats* stats);
+/* `steps` overdamped steps (advance_timestep_overdamped.f90:135-734) of
+ * every box, one species of density 1 (its density does not change): umac
+ * (2 face arrays) and pi in place; eta[nboxes], kT[nboxes] (host) per box;
+ * the two random stages of each step drawn on the device from Philox keyed
+ * by (seed, box) and counted by (element, field, step0 + step).
+ * gmres_iters (nullable): nboxes totals over the steps.  Returns the worst
+ * GMRES status. */
+int fhd_batch_overdamped(fhd_batch* batch, double* const umac[2], double* pi,
+                         const double* eta, const double* kT, double dt,
+                         int steps, unsigned long long seed, int step0,
+                         int* gmres_iters);
+
 #ifdef __cplusplus
 }
 #endif

@@ -23,7 +23,7 @@ from ._capi import (FHD_PREC_FP64, FHD_PREC_MIXED, FHD_REQ_INERTIAL, FHD_REQ_OVE
                     mixture_params)
 
 __all__ = ["StokesSolver", "GmresParams", "StochParams", "SolveStats", "MixtureParams", "mixture_params",
-           "Server", "StructureFactor", "tune_candidates", "tune_export", "tune_import", "tune_key", "Request", "RequestResult", "make_request", "fill_normal", "StepNoise", "philox4x32_10", "sched_simulate",
+           "Server", "Batch", "StructureFactor", "tune_candidates", "tune_export", "tune_import", "tune_key", "Request", "RequestResult", "make_request", "fill_normal", "StepNoise", "philox4x32_10", "sched_simulate",
            "FHD_REQ_OVERDAMPED", "FHD_REQ_INERTIAL",
            "default_params", "FhdError",
            "FHD_PREC_FP64", "FHD_PREC_MIXED", "lib", "fab_from_canonical", "fab_from_components", "canonical_from_fab", "FabArray"]
@@ -628,6 +628,81 @@ class StructureFactor:
             self.close()
         except Exception:
             pass
+
+
+class Batch:
+    """Many independent 2D periodic boxes of uneven size solved together
+    (fhd_batch_*): one launch per multigrid level and operation covers all
+    boxes, GMRES's scalar control runs on the device per box.  Vectors are
+    flat float64 CUDA tensors of all boxes' cells concatenated in box order
+    (offset(b) is box b's first element)."""
+
+    def __init__(self, n_cells, dx: float = 1.0, params: GmresParams | None = None, precision: str = "mixed"):
+        sizes = [(int(a), int(b)) for a, b in n_cells]
+        self.n_cells = sizes
+        self.params = params if params is not None else default_params()
+        arr = (C.c_int * (2 * len(sizes)))(*[v for ab in sizes for v in ab])
+        h = C.c_void_p()
+        mode = FHD_PREC_MIXED if precision == "mixed" else FHD_PREC_FP64
+        check(lib().fhd_batch_create(len(sizes), arr, float(dx), C.byref(self.params), mode, C.byref(h)),
+              "fhd_batch_create")
+        self._h = h
+
+    @property
+    def nboxes(self) -> int:
+        return len(self.n_cells)
+
+    def offset(self, box: int) -> int:
+        return int(lib().fhd_batch_box_offset(self._h, int(box)))
+
+    @property
+    def total(self) -> int:
+        return self.offset(self.nboxes)
+
+    @property
+    def kernel_launches(self) -> int:
+        return int(lib().fhd_batch_kernel_launches(self._h))
+
+    def box(self, t, b: int):
+        """box b's part of a packed vector t"""
+        return t[self.offset(b):self.offset(b + 1)]
+
+    def gmres(self, b, x, eta, theta_alpha: float = 0.0):
+        """gmres of every box: b and x lists of 3 packed tensors (u_x, u_y,
+        p); x in/out; eta per box.  Returns (worst status, per-box stats)."""
+        e = (C.c_double * self.nboxes)(*[float(v) for v in eta])
+        st = (SolveStats * self.nboxes)()
+        status = check(lib().fhd_batch_gmres(self._h, _dpp(b), _dpp(x), C.cast(e, _DP), float(theta_alpha), st),
+                       "fhd_batch_gmres")
+        return status, [st[i].as_dict() for i in range(self.nboxes)]
+
+    def overdamped(self, umac, pi, eta, kT, dt: float, steps: int, seed: int = 1, step0: int = 0):
+        """`steps` overdamped steps of every box in place (umac: 2 packed face
+        tensors, pi packed); returns (worst status, GMRES iterations per box)"""
+        e = (C.c_double * self.nboxes)(*[float(v) for v in eta])
+        k = (C.c_double * self.nboxes)(*[float(v) for v in kT])
+        it = (C.c_int * self.nboxes)()
+        status = check(lib().fhd_batch_overdamped(self._h, _dpp(umac), _dptr(pi), C.cast(e, _DP), C.cast(k, _DP),
+                                                  float(dt), int(steps), int(seed), int(step0), it),
+                       "fhd_batch_overdamped")
+        return status, list(it)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().fhd_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
 
 
 class Server:

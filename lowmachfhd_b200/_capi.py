@@ -140,6 +140,14 @@ _PROTOS = {
                                     C.POINTER(C.c_int), C.POINTER(C.c_double), C.c_int, C.POINTER(GmresParams),
                                     C.c_int, C.POINTER(_VP)]),
     "fhd_ctx_destroy": (C.c_int, [_VP]),
+    "fhd_batch_create": (C.c_int, [C.c_int, C.POINTER(C.c_int), C.c_double, C.POINTER(GmresParams), C.c_int,
+                                   C.POINTER(_VP)]),
+    "fhd_batch_destroy": (C.c_int, [_VP]),
+    "fhd_batch_box_offset": (C.c_longlong, [_VP, C.c_int]),
+    "fhd_batch_kernel_launches": (C.c_longlong, [_VP]),
+    "fhd_batch_gmres": (C.c_int, [_VP, _PP, _PP, _DP, C.c_double, C.POINTER(SolveStats)]),
+    "fhd_batch_overdamped": (C.c_int, [_VP, _PP, _DP, _DP, _DP, C.c_double, C.c_int, C.c_ulonglong, C.c_int,
+                                       C.POINTER(C.c_int)]),
     "fhd_ctx_stream": (_VP, [_VP]),
     "fhd_ctx_set_stream": (C.c_int, [_VP, _VP]),
     "fhd_ctx_kernel_launches": (C.c_longlong, [_VP]),

@@ -11,7 +11,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 SRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "_fhd_b200.so")
 SOURCES = ["fhd_solver.cu", "fhd_step.cu", "fhd_capi.cu", "fhd_noalloc.cu", "fhd_mass.cu", "fhd_server.cu",
-           "fhd_sk.cu", "fhd_mass_f32.cu"]
+           "fhd_sk.cu", "fhd_mass_f32.cu", "fhd_batch.cu"]
 # translation units whose FP32 arithmetic may contract into FMA (tolerance-
 # checked, no FP64 parity path inside)
 FMA_SOURCES = {"fhd_mass_f32.cu"}

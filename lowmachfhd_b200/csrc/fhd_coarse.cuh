@@ -202,14 +202,18 @@ template <typename T, int VISC>
 __device__ __forceinline__ StagOp<T> cs_op(const StagCoarseArgs<T>& a, int m) {
     StagOp<T> A = a.A[m];
     if constexpr (VISC > 0) {
-        A.beta0 = A.beta[0];
-        A.beta0_set = 1;
+        if (!A.beta0_set) {
+            A.beta0 = A.beta[0];
+            A.beta0_set = 1;
+        }
     }
     return A;
 }
 
+// the coarse end of one staggered V-cycle in the calling CTA (shared memory
+// from the dynamic allocation); also run per box by the batched solver
 template <typename T, int DIM, int VISC>
-__global__ void __launch_bounds__(CS_THREADS) k_stag_coarse(const __grid_constant__ StagCoarseArgs<T> a) {
+__device__ __forceinline__ void stag_coarse_run(const StagCoarseArgs<T>& a) {
     extern __shared__ __align__(16) unsigned char cs_smem[];
     T* S = reinterpret_cast<T*>(cs_smem);
     const int nt = blockDim.x;
@@ -294,6 +298,11 @@ __global__ void __launch_bounds__(CS_THREADS) k_stag_coarse(const __grid_constan
     }
 }
 
+template <typename T, int DIM, int VISC>
+__global__ void __launch_bounds__(CS_THREADS) k_stag_coarse(const __grid_constant__ StagCoarseArgs<T> a) {
+    stag_coarse_run<T, DIM, VISC>(a);
+}
+
 // ---------------------------------------------------------------------
 // pressure multigrid
 // ---------------------------------------------------------------------
@@ -350,8 +359,10 @@ __device__ void cs_cc_smooths(const Grid& g, const CCOp<T>& A, T* ph, const T* r
         }
 }
 
+// the coarse end of one pressure V-cycle in the calling CTA; also run per
+// box by the batched solver
 template <typename T, int DIM>
-__global__ void __launch_bounds__(CS_THREADS) k_cc_coarse(const __grid_constant__ CCCoarseArgs<T> a) {
+__device__ __forceinline__ void cc_coarse_run(const CCCoarseArgs<T>& a) {
     extern __shared__ __align__(16) unsigned char cs_smem[];
     T* S = reinterpret_cast<T*>(cs_smem);
     const int nt = blockDim.x;
@@ -410,6 +421,11 @@ __global__ void __launch_bounds__(CS_THREADS) k_cc_coarse(const __grid_constant_
         const T* ph = S + a.off[0];
         for (int f = threadIdx.x; f < nc; f += nt) a.phi[f] = ph[f];
     }
+}
+
+template <typename T, int DIM>
+__global__ void __launch_bounds__(CS_THREADS) k_cc_coarse(const __grid_constant__ CCCoarseArgs<T> a) {
+    cc_coarse_run<T, DIM>(a);
 }
 
 }  // namespace fhd

@@ -385,8 +385,10 @@ __global__ void __launch_bounds__(RB_MAXTHREADS) k_stag_rb(Grid g, RBGeom G, Sta
     // the constant viscosity of visc_type > 0, loaded once (the staging
     // asm clobbers memory, which would force a reload per row)
     if constexpr (VISC > 0) {
-        A.beta0 = A.beta[0];
-        A.beta0_set = 1;
+        if (!A.beta0_set) {
+            A.beta0 = A.beta[0];
+            A.beta0_set = 1;
+        }
     }
     if constexpr (CFIX >= 0) {
         stag_rb_run<T, VISC, CFIX>(g, G, A, R, omega, rb_smraw);

@@ -129,8 +129,10 @@ __device__ __forceinline__ void rbx_run(const Grid& g, const RBXGeom& G, const S
     // the constant viscosity, loaded once: every asm statement below clobbers
     // memory, which would make each sweep reload it from global memory
     StagOp<float> A = A0;
-    A.beta0 = A0.beta[0];
-    A.beta0_set = 1;
+    if (!A.beta0_set) {
+        A.beta0 = A0.beta[0];
+        A.beta0_set = 1;
+    }
     constexpr int NPH = 5 + AH;  // unknown planes k-1 .. k+3 + in flight
     constexpr int NCF = 3 + AH;  // coefficient planes k .. k+2 + in flight
     constexpr int MR = rbx_maxr(NT);  // rows per thread and red sweep
