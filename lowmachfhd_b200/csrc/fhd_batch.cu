@@ -26,6 +26,7 @@
 // T is the multigrid precision (float in the mixed mode); the Krylov
 // vectors and apply_matrix are FP64.
 #include <algorithm>
+#include <unordered_map>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -52,7 +53,7 @@ struct Lev {
 };
 
 // which boxes an operation covers
-enum Mode { M_ALL = 0, M_LIVE = 1, M_INNER = 2, M_PEND = 3 };
+enum Mode { M_ALL = 0, M_LIVE = 1, M_INNER = 2, M_PEND = 3, M_ZERO = 4 };
 
 // GMRES state of one box (gmres.f90:32-619)
 struct Ctl {
@@ -68,7 +69,49 @@ struct Ctl {
 };
 
 __device__ __forceinline__ bool covers(const Ctl& c, int mode) {
-    return mode == M_ALL ? true : mode == M_LIVE ? !c.done : mode == M_INNER ? c.inner != 0 : c.pend != 0;
+    return mode == M_ALL     ? true
+           : mode == M_LIVE  ? !c.done
+           : mode == M_INNER ? c.inner != 0
+           : mode == M_PEND  ? c.pend != 0
+                             : c.zero_x != 0;
+}
+
+// Every tile kernel runs on a grid sized to the GPU (a few CTAs per SM), not
+// one CTA per tile: a CTA owns the tiles q = blockIdx.x + r * gridDim.x of
+// the launch's table.  In rounds of 256 each thread tests one of them
+// against the mode, the covered ones are compacted in shared memory (in q
+// order), and the whole CTA runs f(tile, q) on each in turn.  A box that
+// sits out the operation then costs one load per tile instead of a CTA
+// launch, and a covered tile's work is the CTA's 256 threads on its 64 x 8
+// cells.  f is called by every thread of the CTA (it may synchronise); its
+// return ends that thread's part of the tile.
+template <class F>
+__device__ __forceinline__ void for_tiles(const Tile* tiles, int n, const Ctl* ctl, int mode, F f) {
+    __shared__ int s_q[256];
+    __shared__ int s_w[8];
+    const int tid = threadIdx.x + 32 * threadIdx.y;
+    const int lane = tid & 31, w = tid >> 5;
+    for (long long r0 = 0; (long long)blockIdx.x + r0 * gridDim.x < n; r0 += 256) {
+        const long long q = (long long)blockIdx.x + (r0 + tid) * gridDim.x;
+        bool live = false;
+        if (q < n) live = mode == M_ALL || covers(ctl[tiles[q].box], mode);
+        const unsigned bal = __ballot_sync(0xffffffffu, live);
+        if (lane == 0) s_w[w] = __popc(bal);
+        __syncthreads();
+        int base = 0, tot = 0;
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            base += k < w ? s_w[k] : 0;
+            tot += s_w[k];
+        }
+        if (live) s_q[base + __popc(bal & ((1u << lane) - 1u))] = (int)q;
+        __syncthreads();
+        for (int k = 0; k < tot; k++) {
+            const int qq = s_q[k];
+            f(tiles[qq], qq);
+        }
+        __syncthreads();
+    }
 }
 
 // the staggered operator of a box at a level: alpha = 1 (a read-only array
@@ -103,193 +146,196 @@ __device__ __forceinline__ CCOp<T> box_ccop(const T* ones, double dx) {
 // one colour of the 4-colour Gauss-Seidel (k_stag_gs): component C, faces
 // with (i+j) % 2 == par
 template <typename T, int C>
-__global__ void __launch_bounds__(256) kb_stag_gs(const Tile* tiles, const Lev* lev, int l, const Ctl* ctl, int mode,
+__global__ void __launch_bounds__(256) kb_stag_gs(const Tile* tiles, int n, const Lev* lev, int l, const Ctl* ctl, int mode,
                                                   T* const* phi, const T* const* rhs, const T* ones, T theta,
                                                   int par, T omega) {
-    const Tile t = tiles[blockIdx.x];
-    if (!covers(ctl[t.box], mode)) return;
-    const Lev L = lev[t.box * MAXL + l];
-    const int j = t.j0 + threadIdx.y;
-    const int i = t.i0 + 2 * threadIdx.x + ((j + par) & 1);
-    if (j >= L.g.n[1] || i >= L.g.n[0]) return;
-    CellF P;
-    P.set(L.g, i, j, 0);
-    T* p0 = phi[0] + L.off;
-    T* p1 = phi[1] + L.off;
-    const T* ph[3] = {p0, p1, nullptr};
-    T* pc = C == 0 ? p0 : p1;
-    const StagOp<T> A = box_op<T>(ones, theta, ctl[t.box].eta, L.g.dx);
-    const i64 f = P.id(0, 0, 0);
-    T dg;
-    const T Lv = stag_lface<T, 2, 1, C>(A, ph, P, dg);
-    pc[f] = pc[f] + sm_quot(omega * (ld(rhs[C] + L.off, f) - Lv), dg);
+    for_tiles(tiles, n, ctl, mode, [&](const Tile& t, int q) {
+        const Lev L = lev[t.box * MAXL + l];
+        const int j = t.j0 + threadIdx.y;
+        const int i = t.i0 + 2 * threadIdx.x + ((j + par) & 1);
+        if (j >= L.g.n[1] || i >= L.g.n[0]) return;
+        CellF P;
+        P.set(L.g, i, j, 0);
+        T* p0 = phi[0] + L.off;
+        T* p1 = phi[1] + L.off;
+        const T* ph[3] = {p0, p1, nullptr};
+        T* pc = C == 0 ? p0 : p1;
+        const StagOp<T> A = box_op<T>(ones, theta, ctl[t.box].eta, L.g.dx);
+        const i64 f = P.id(0, 0, 0);
+        T dg;
+        const T Lv = stag_lface<T, 2, 1, C>(A, ph, P, dg);
+        pc[f] = pc[f] + sm_quot(omega * (ld(rhs[C] + L.off, f) - Lv), dg);
+    });
 }
 
 // residual rhs - (theta alpha - L) phi of both components into tmp
 template <typename T>
-__global__ void __launch_bounds__(256) kb_stag_resid(const Tile* tiles, const Lev* lev, int l, const Ctl* ctl,
+__global__ void __launch_bounds__(256) kb_stag_resid(const Tile* tiles, int n, const Lev* lev, int l, const Ctl* ctl,
                                                      int mode, T* const* phi, const T* const* rhs, T* const* tmp,
                                                      const T* ones, T theta) {
-    const Tile t = tiles[blockIdx.x];
-    if (!covers(ctl[t.box], mode)) return;
-    const Lev L = lev[t.box * MAXL + l];
-    const int j = t.j0 + threadIdx.y;
-    if (j >= L.g.n[1]) return;
-    const StagOp<T> A = box_op<T>(ones, theta, ctl[t.box].eta, L.g.dx);
-    const T* ph[3] = {phi[0] + L.off, phi[1] + L.off, nullptr};
-#pragma unroll
-    for (int u = 0; u < 2; u++) {
-        const int i = t.i0 + threadIdx.x + 32 * u;
-        if (i >= L.g.n[0]) continue;
-        CellF P;
-        P.set(L.g, i, j, 0);
-        const i64 f = P.id(0, 0, 0);
-#pragma unroll
-        for (int c = 0; c < 2; c++) {
-            T dg;
-            const T Lv = stag_lface_c<T, 2, 1>(c, A, ph, P, dg);
-            tmp[c][L.off + f] = ld(rhs[c] + L.off, f) - Lv;
+    for_tiles(tiles, n, ctl, mode, [&](const Tile& t, int q) {
+        const Lev L = lev[t.box * MAXL + l];
+        const int j = t.j0 + threadIdx.y;
+        if (j >= L.g.n[1]) return;
+        const StagOp<T> A = box_op<T>(ones, theta, ctl[t.box].eta, L.g.dx);
+        const T* ph[3] = {phi[0] + L.off, phi[1] + L.off, nullptr};
+    #pragma unroll
+        for (int u = 0; u < 2; u++) {
+            const int i = t.i0 + threadIdx.x + 32 * u;
+            if (i >= L.g.n[0]) continue;
+            CellF P;
+            P.set(L.g, i, j, 0);
+            const i64 f = P.id(0, 0, 0);
+    #pragma unroll
+            for (int c = 0; c < 2; c++) {
+                T dg;
+                const T Lv = stag_lface_c<T, 2, 1>(c, A, ph, P, dg);
+                tmp[c][L.off + f] = ld(rhs[c] + L.off, f) - Lv;
+            }
         }
-    }
+    });
 }
 
 // stag_restriction of tmp (level l) into rhs (level l+1); the tiles are
 // level l+1's
 template <typename T>
-__global__ void __launch_bounds__(256) kb_stag_restrict(const Tile* tiles, const Lev* lev, int l, const Ctl* ctl,
+__global__ void __launch_bounds__(256) kb_stag_restrict(const Tile* tiles, int n, const Lev* lev, int l, const Ctl* ctl,
                                                         int mode, T* const* tmp, T* const* crhs) {
-    const Tile t = tiles[blockIdx.x];
-    if (!covers(ctl[t.box], mode)) return;
-    const Lev F = lev[t.box * MAXL + l], Q = lev[t.box * MAXL + l + 1];
-    const int j = t.j0 + threadIdx.y;
-    if (j >= Q.g.n[1]) return;
-#pragma unroll
-    for (int u = 0; u < 2; u++) {
-        const int i = t.i0 + threadIdx.x + 32 * u;
-        if (i >= Q.g.n[0]) continue;
-        Cell X;
-        X.nx = F.g.n[0]; X.ny = F.g.n[1]; X.nz = 1;
-        X.i = 2 * i; X.j = 2 * j; X.k = 0;
-        const i64 qc = (i64)i + (i64)Q.g.n[0] * j;
-#pragma unroll
-        for (int c = 0; c < 2; c++) {
-            const T* Fp = tmp[c] + F.off;
-            crhs[c][Q.off + qc] = stag_restrict_expr<T, 2>(
-                0, [&](int o, int pa, int pb) { return ld(Fp, comp_off_id<2>(X, c, o, pa, pb)); });
+    for_tiles(tiles, n, ctl, mode, [&](const Tile& t, int q) {
+        const Lev F = lev[t.box * MAXL + l], Q = lev[t.box * MAXL + l + 1];
+        const int j = t.j0 + threadIdx.y;
+        if (j >= Q.g.n[1]) return;
+    #pragma unroll
+        for (int u = 0; u < 2; u++) {
+            const int i = t.i0 + threadIdx.x + 32 * u;
+            if (i >= Q.g.n[0]) continue;
+            Cell X;
+            X.nx = F.g.n[0]; X.ny = F.g.n[1]; X.nz = 1;
+            X.i = 2 * i; X.j = 2 * j; X.k = 0;
+            const i64 qc = (i64)i + (i64)Q.g.n[0] * j;
+    #pragma unroll
+            for (int c = 0; c < 2; c++) {
+                const T* Fp = tmp[c] + F.off;
+                crhs[c][Q.off + qc] = stag_restrict_expr<T, 2>(
+                    0, [&](int o, int pa, int pb) { return ld(Fp, comp_off_id<2>(X, c, o, pa, pb)); });
+            }
         }
-    }
+    });
 }
 
 // stag_prolongation: fine phi (level l) += P coarse phi (level l+1); thread
 // per fine face, the tiles are level l's; phi is the per-level table from
 // level l on (phi[c] level l, phi[2 + c] level l+1)
 template <typename T>
-__global__ void __launch_bounds__(256) kb_stag_prolong(const Tile* tiles, const Lev* lev, int l, const Ctl* ctl,
+__global__ void __launch_bounds__(256) kb_stag_prolong(const Tile* tiles, int n, const Lev* lev, int l, const Ctl* ctl,
                                                        int mode, T* const* phi) {
-    const Tile t = tiles[blockIdx.x];
-    if (!covers(ctl[t.box], mode)) return;
-    const Lev F = lev[t.box * MAXL + l], Q = lev[t.box * MAXL + l + 1];
-    const int j = t.j0 + threadIdx.y;
-    if (j >= F.g.n[1]) return;
-#pragma unroll
-    for (int u = 0; u < 2; u++) {
-        const int i = t.i0 + threadIdx.x + 32 * u;
-        if (i >= F.g.n[0]) continue;
-        const int I[2] = {i, j};
-        Cell H;
-        H.nx = Q.g.n[0]; H.ny = Q.g.n[1]; H.nz = 1;
-        H.i = i >> 1; H.j = j >> 1; H.k = 0;
-        const i64 f = (i64)i + (i64)F.g.n[0] * j;
-#pragma unroll
-        for (int c = 0; c < 2; c++) {
-            const T* Cp = phi[2 + c] + Q.off;
-            const int ca = (c == 0) ? 1 : 0;
-            const int oa = (I[ca] & 1) ? 1 : -1;
-            const T v = stag_prolong_expr<T, 2>((I[c] & 1) == 0, oa, 0, [&](int o, int pa, int pb) {
-                return ld(Cp, comp_off_id<2>(H, c, o, pa, pb));
-            });
-            T* Fp = phi[c] + F.off;
-            Fp[f] = Fp[f] + v;
+    for_tiles(tiles, n, ctl, mode, [&](const Tile& t, int q) {
+        const Lev F = lev[t.box * MAXL + l], Q = lev[t.box * MAXL + l + 1];
+        const int j = t.j0 + threadIdx.y;
+        if (j >= F.g.n[1]) return;
+    #pragma unroll
+        for (int u = 0; u < 2; u++) {
+            const int i = t.i0 + threadIdx.x + 32 * u;
+            if (i >= F.g.n[0]) continue;
+            const int I[2] = {i, j};
+            Cell H;
+            H.nx = Q.g.n[0]; H.ny = Q.g.n[1]; H.nz = 1;
+            H.i = i >> 1; H.j = j >> 1; H.k = 0;
+            const i64 f = (i64)i + (i64)F.g.n[0] * j;
+    #pragma unroll
+            for (int c = 0; c < 2; c++) {
+                const T* Cp = phi[2 + c] + Q.off;
+                const int ca = (c == 0) ? 1 : 0;
+                const int oa = (I[ca] & 1) ? 1 : -1;
+                const T v = stag_prolong_expr<T, 2>((I[c] & 1) == 0, oa, 0, [&](int o, int pa, int pb) {
+                    return ld(Cp, comp_off_id<2>(H, c, o, pa, pb));
+                });
+                T* Fp = phi[c] + F.off;
+                Fp[f] = Fp[f] + v;
+            }
         }
-    }
+    });
 }
 
 // the coarse end of every covered box's V-cycle, one CTA per box
 template <typename T>
-__global__ void __launch_bounds__(CS_THREADS) kb_stag_coarse(const StagCoarseArgs<T>* args, const Ctl* ctl,
-                                                            int mode) {
-    if (!covers(ctl[blockIdx.x], mode)) return;
-    stag_coarse_run<T, 2, 1>(args[blockIdx.x]);
+__global__ void __launch_bounds__(CS_THREADS) kb_stag_coarse(const StagCoarseArgs<T>* args, const int* order,
+                                                            const Ctl* ctl, int mode) {
+    const int b = order[blockIdx.x];
+    if (!covers(ctl[b], mode)) return;
+    stag_coarse_run<T, 2, 1>(args[b]);
 }
 
 // ---------------------------------------------------------------------
 // pressure multigrid
 // ---------------------------------------------------------------------
 template <typename T>
-__global__ void __launch_bounds__(256) kb_cc_gsrb(const Tile* tiles, const Lev* lev, int l, const Ctl* ctl, int mode,
+__global__ void __launch_bounds__(256) kb_cc_gsrb(const Tile* tiles, int n, const Lev* lev, int l, const Ctl* ctl, int mode,
                                                   T* phi, const T* rhs, const T* ones, int par) {
-    const Tile t = tiles[blockIdx.x];
-    if (!covers(ctl[t.box], mode)) return;
-    const Lev L = lev[t.box * MAXL + l];
-    const int j = t.j0 + threadIdx.y;
-    const int i = t.i0 + 2 * threadIdx.x + ((j + par) & 1);
-    if (j >= L.g.n[1] || i >= L.g.n[0]) return;
-    CellF P;
-    P.set(L.g, i, j, 0);
-    const CCOp<T> A = box_ccop<T>(ones, L.g.dx);
-    T* ph = phi + L.off;
-    T dg;
-    const T Lv = cc_lap<T, 2>(A, ph, P, dg);
-    const i64 f = P.id(0, 0, 0);
-    ph[f] = ph[f] + sm_quot(ld(rhs + L.off, f) - Lv, dg);
+    for_tiles(tiles, n, ctl, mode, [&](const Tile& t, int q) {
+        const Lev L = lev[t.box * MAXL + l];
+        const int j = t.j0 + threadIdx.y;
+        const int i = t.i0 + 2 * threadIdx.x + ((j + par) & 1);
+        if (j >= L.g.n[1] || i >= L.g.n[0]) return;
+        CellF P;
+        P.set(L.g, i, j, 0);
+        const CCOp<T> A = box_ccop<T>(ones, L.g.dx);
+        T* ph = phi + L.off;
+        T dg;
+        const T Lv = cc_lap<T, 2>(A, ph, P, dg);
+        const i64 f = P.id(0, 0, 0);
+        ph[f] = ph[f] + sm_quot(ld(rhs + L.off, f) - Lv, dg);
+    });
 }
 
 // residual of level l averaged onto level l+1's rhs; tiles of level l+1
 template <typename T>
-__global__ void __launch_bounds__(256) kb_cc_resid_restrict(const Tile* tiles, const Lev* lev, int l, const Ctl* ctl,
+__global__ void __launch_bounds__(256) kb_cc_resid_restrict(const Tile* tiles, int n, const Lev* lev, int l, const Ctl* ctl,
                                                             int mode, const T* phi, const T* rhs, T* crhs,
                                                             const T* ones) {
-    const Tile t = tiles[blockIdx.x];
-    if (!covers(ctl[t.box], mode)) return;
-    const Lev F = lev[t.box * MAXL + l], Q = lev[t.box * MAXL + l + 1];
-    const int j = t.j0 + threadIdx.y;
-    if (j >= Q.g.n[1]) return;
-    const CCOp<T> A = box_ccop<T>(ones, F.g.dx);
-    const T* ph = phi + F.off;
-    const T* rh = rhs + F.off;
-#pragma unroll
-    for (int u = 0; u < 2; u++) {
-        const int i = t.i0 + threadIdx.x + 32 * u;
-        if (i >= Q.g.n[0]) continue;
-        crhs[Q.off + (i64)i + (i64)Q.g.n[0] * j] = cc_resid_avg<T, 2>(
-            A, F.g, i, j, 0, [&](i64 k) { return ld(ph, k); }, [&](i64 k) { return ld(rh, k); });
-    }
+    for_tiles(tiles, n, ctl, mode, [&](const Tile& t, int q) {
+        const Lev F = lev[t.box * MAXL + l], Q = lev[t.box * MAXL + l + 1];
+        const int j = t.j0 + threadIdx.y;
+        if (j >= Q.g.n[1]) return;
+        const CCOp<T> A = box_ccop<T>(ones, F.g.dx);
+        const T* ph = phi + F.off;
+        const T* rh = rhs + F.off;
+    #pragma unroll
+        for (int u = 0; u < 2; u++) {
+            const int i = t.i0 + threadIdx.x + 32 * u;
+            if (i >= Q.g.n[0]) continue;
+            crhs[Q.off + (i64)i + (i64)Q.g.n[0] * j] = cc_resid_avg<T, 2>(
+                A, F.g, i, j, 0, [&](i64 k) { return ld(ph, k); }, [&](i64 k) { return ld(rh, k); });
+        }
+    });
 }
 
 // phi (level l) += the parent cell's coarse phi (cphi, level l+1); tiles of
 // level l
 template <typename T>
-__global__ void __launch_bounds__(256) kb_cc_prolong(const Tile* tiles, const Lev* lev, int l, const Ctl* ctl,
+__global__ void __launch_bounds__(256) kb_cc_prolong(const Tile* tiles, int n, const Lev* lev, int l, const Ctl* ctl,
                                                      int mode, T* phi, const T* cphi) {
-    const Tile t = tiles[blockIdx.x];
-    if (!covers(ctl[t.box], mode)) return;
-    const Lev F = lev[t.box * MAXL + l], Q = lev[t.box * MAXL + l + 1];
-    const int j = t.j0 + threadIdx.y;
-    if (j >= F.g.n[1]) return;
-#pragma unroll
-    for (int u = 0; u < 2; u++) {
-        const int i = t.i0 + threadIdx.x + 32 * u;
-        if (i >= F.g.n[0]) continue;
-        const T cv = ld(cphi + Q.off, (i64)(i >> 1) + (i64)Q.g.n[0] * (j >> 1));
-        T* p = phi + F.off + (i64)i + (i64)F.g.n[0] * j;
-        *p = *p + cv;
-    }
+    for_tiles(tiles, n, ctl, mode, [&](const Tile& t, int q) {
+        const Lev F = lev[t.box * MAXL + l], Q = lev[t.box * MAXL + l + 1];
+        const int j = t.j0 + threadIdx.y;
+        if (j >= F.g.n[1]) return;
+    #pragma unroll
+        for (int u = 0; u < 2; u++) {
+            const int i = t.i0 + threadIdx.x + 32 * u;
+            if (i >= F.g.n[0]) continue;
+            const T cv = ld(cphi + Q.off, (i64)(i >> 1) + (i64)Q.g.n[0] * (j >> 1));
+            T* p = phi + F.off + (i64)i + (i64)F.g.n[0] * j;
+            *p = *p + cv;
+        }
+    });
 }
 
 template <typename T>
-__global__ void __launch_bounds__(CS_THREADS) kb_cc_coarse(const CCCoarseArgs<T>* args, const Ctl* ctl, int mode) {
-    if (!covers(ctl[blockIdx.x], mode)) return;
-    cc_coarse_run<T, 2>(args[blockIdx.x]);
+__global__ void __launch_bounds__(CS_THREADS) kb_cc_coarse(const CCCoarseArgs<T>* args, const int* order,
+                                                          const Ctl* ctl, int mode) {
+    const int b = order[blockIdx.x];
+    if (!covers(ctl[b], mode)) return;
+    cc_coarse_run<T, 2>(args[b]);
 }
 
 // ---------------------------------------------------------------------
@@ -297,79 +343,79 @@ __global__ void __launch_bounds__(CS_THREADS) kb_cc_coarse(const CCCoarseArgs<T>
 // ---------------------------------------------------------------------
 // the multigrid rhs from the FP64 input: b_u in the precision of T
 template <typename T>
-__global__ void __launch_bounds__(256) kb_to_T(const Tile* tiles, const Lev* lev, const Ctl* ctl, int mode,
+__global__ void __launch_bounds__(256) kb_to_T(const Tile* tiles, int n, const Lev* lev, const Ctl* ctl, int mode,
                                                const double* const* b, T* const* out) {
-    const Tile t = tiles[blockIdx.x];
-    if (!covers(ctl[t.box], mode)) return;
-    const Lev L = lev[t.box * MAXL];
-    const int j = t.j0 + threadIdx.y;
-    if (j >= L.g.n[1]) return;
-#pragma unroll
-    for (int u = 0; u < 2; u++) {
-        const int i = t.i0 + threadIdx.x + 32 * u;
-        if (i >= L.g.n[0]) continue;
-        const i64 f = L.off + (i64)i + (i64)L.g.n[0] * j;
-        out[0][f] = (T)b[0][f];
-        out[1][f] = (T)b[1][f];
-    }
+    for_tiles(tiles, n, ctl, mode, [&](const Tile& t, int q) {
+        const Lev L = lev[t.box * MAXL];
+        const int j = t.j0 + threadIdx.y;
+        if (j >= L.g.n[1]) return;
+    #pragma unroll
+        for (int u = 0; u < 2; u++) {
+            const int i = t.i0 + threadIdx.x + 32 * u;
+            if (i >= L.g.n[0]) continue;
+            const i64 f = L.off + (i64)i + (i64)L.g.n[0] * j;
+            out[0][f] = (T)b[0][f];
+            out[1][f] = (T)b[1][f];
+        }
+    });
 }
 
 // mac_rhs = D x_u* + b_p (k_div_plus)
 template <typename T>
-__global__ void __launch_bounds__(256) kb_div_plus(const Tile* tiles, const Lev* lev, const Ctl* ctl, int mode,
+__global__ void __launch_bounds__(256) kb_div_plus(const Tile* tiles, int n, const Lev* lev, const Ctl* ctl, int mode,
                                                    T* const* xu, const double* bp, T* out) {
-    const Tile t = tiles[blockIdx.x];
-    if (!covers(ctl[t.box], mode)) return;
-    const Lev L = lev[t.box * MAXL];
-    const int j = t.j0 + threadIdx.y;
-    if (j >= L.g.n[1]) return;
-    const T dxinv = (T)(1.0 / L.g.dx);
-    const T* u0 = xu[0] + L.off;
-    const T* u1 = xu[1] + L.off;
-#pragma unroll
-    for (int u = 0; u < 2; u++) {
-        const int i = t.i0 + threadIdx.x + 32 * u;
-        if (i >= L.g.n[0]) continue;
-        CellF P;
-        P.set(L.g, i, j, 0);
-        const i64 f = P.id(0, 0, 0);
-        const T s = (ld(u0, P.id(1, 0, 0)) - ld(u0, f)) * dxinv + (ld(u1, P.id(0, 1, 0)) - ld(u1, f)) * dxinv;
-        out[L.off + f] = s + (T)bp[L.off + f];
-    }
+    for_tiles(tiles, n, ctl, mode, [&](const Tile& t, int q) {
+        const Lev L = lev[t.box * MAXL];
+        const int j = t.j0 + threadIdx.y;
+        if (j >= L.g.n[1]) return;
+        const T dxinv = (T)(1.0 / L.g.dx);
+        const T* u0 = xu[0] + L.off;
+        const T* u1 = xu[1] + L.off;
+    #pragma unroll
+        for (int u = 0; u < 2; u++) {
+            const int i = t.i0 + threadIdx.x + 32 * u;
+            if (i >= L.g.n[0]) continue;
+            CellF P;
+            P.set(L.g, i, j, 0);
+            const i64 f = P.id(0, 0, 0);
+            const T s = (ld(u0, P.id(1, 0, 0)) - ld(u0, f)) * dxinv + (ld(u1, P.id(0, 1, 0)) - ld(u1, f)) * dxinv;
+            out[L.off + f] = s + (T)bp[L.off + f];
+        }
+    });
 }
 
 // x_u = x_u* - alphainv G Phi (k_sub_wgrad, alphainv = 1) and x_p = -beta
 // mac_rhs + theta Phi (k_schur, kind 0, visc_type 1)
 template <typename T>
-__global__ void __launch_bounds__(256) kb_precon_out(const Tile* tiles, const Lev* lev, const Ctl* ctl, int mode,
+__global__ void __launch_bounds__(256) kb_precon_out(const Tile* tiles, int n, const Lev* lev, const Ctl* ctl, int mode,
                                                      T* const* xu, const T* Phi, const T* mac_rhs, double theta,
                                                      double* const* x) {
-    const Tile t = tiles[blockIdx.x];
-    if (!covers(ctl[t.box], mode)) return;
-    const Lev L = lev[t.box * MAXL];
-    const int j = t.j0 + threadIdx.y;
-    if (j >= L.g.n[1]) return;
-    const T dxinv = (T)(1.0 / L.g.dx);
-    const double eta = ctl[t.box].eta;
-    const T* Ph = Phi + L.off;
-#pragma unroll
-    for (int u = 0; u < 2; u++) {
-        const int i = t.i0 + threadIdx.x + 32 * u;
-        if (i >= L.g.n[0]) continue;
-        CellF P;
-        P.set(L.g, i, j, 0);
-        const i64 f = P.id(0, 0, 0);
-        const T pc = ld(Ph, f);
-#pragma unroll
-        for (int c = 0; c < 2; c++) {
-            const T gp = (pc - ld(Ph, P.id(-(c == 0), -(c == 1), 0))) * dxinv;
-            x[c][L.off + f] = (double)(ld(xu[c] + L.off, f) + T(-1) * gp);
+    for_tiles(tiles, n, ctl, mode, [&](const Tile& t, int q) {
+        const Lev L = lev[t.box * MAXL];
+        const int j = t.j0 + threadIdx.y;
+        if (j >= L.g.n[1]) return;
+        const T dxinv = (T)(1.0 / L.g.dx);
+        const double eta = ctl[t.box].eta;
+        const T* Ph = Phi + L.off;
+    #pragma unroll
+        for (int u = 0; u < 2; u++) {
+            const int i = t.i0 + threadIdx.x + 32 * u;
+            if (i >= L.g.n[0]) continue;
+            CellF P;
+            P.set(L.g, i, j, 0);
+            const i64 f = P.id(0, 0, 0);
+            const T pc = ld(Ph, f);
+    #pragma unroll
+            for (int c = 0; c < 2; c++) {
+                const T gp = (pc - ld(Ph, P.id(-(c == 0), -(c == 1), 0))) * dxinv;
+                x[c][L.off + f] = (double)(ld(xu[c] + L.off, f) + T(-1) * gp);
+            }
+            double v = (double)mac_rhs[L.off + f] * -1.0;
+            v = v * eta;
+            v = v + (double)pc * theta;
+            x[2][L.off + f] = v;
         }
-        double v = (double)mac_rhs[L.off + f] * -1.0;
-        v = v * eta;
-        v = v + (double)pc * theta;
-        x[2][L.off + f] = v;
-    }
+    });
 }
 
 // ---------------------------------------------------------------------
@@ -386,6 +432,7 @@ __device__ __forceinline__ double tile_sum(double v) {
     double s = 0.0;
     if (t == 0)
         for (int w = 0; w < 8; w++) s += sh[w];
+    __syncthreads();  // sh is reused by the CTA's next tile
     return s;
 }
 
@@ -414,211 +461,211 @@ __global__ void __launch_bounds__(256) kb_seg_sum(int nbox, const double* part, 
 }
 
 // weighted dot <a, b> (pressure weighted by wp2) of the 3 components, per tile
-__global__ void __launch_bounds__(256) kb_dot(const Tile* tiles, const Lev* lev, const Ctl* ctl, int mode,
+__global__ void __launch_bounds__(256) kb_dot(const Tile* tiles, int n, const Lev* lev, const Ctl* ctl, int mode,
                                               const double* const* a, const double* const* b, double wp2,
                                               double* part) {
-    const Tile t = tiles[blockIdx.x];
-    if (!covers(ctl[t.box], mode)) return;
-    const Lev L = lev[t.box * MAXL];
-    const int j = t.j0 + threadIdx.y;
-    double s = 0.0;
-    if (j < L.g.n[1]) {
-#pragma unroll
-        for (int u = 0; u < 2; u++) {
-            const int i = t.i0 + threadIdx.x + 32 * u;
-            if (i >= L.g.n[0]) continue;
-            const i64 f = L.off + (i64)i + (i64)L.g.n[0] * j;
-            double su = 0.0;
-#pragma unroll
-            for (int c = 0; c < 3; c++) {
-                const double tt = a[c][f] * b[c][f];
-                su += c == 2 ? wp2 * tt : tt;
+    for_tiles(tiles, n, ctl, mode, [&](const Tile& t, int q) {
+        const Lev L = lev[t.box * MAXL];
+        const int j = t.j0 + threadIdx.y;
+        double s = 0.0;
+        if (j < L.g.n[1]) {
+    #pragma unroll
+            for (int u = 0; u < 2; u++) {
+                const int i = t.i0 + threadIdx.x + 32 * u;
+                if (i >= L.g.n[0]) continue;
+                const i64 f = L.off + (i64)i + (i64)L.g.n[0] * j;
+                double su = 0.0;
+    #pragma unroll
+                for (int c = 0; c < 3; c++) {
+                    const double tt = a[c][f] * b[c][f];
+                    su += c == 2 ? wp2 * tt : tt;
+                }
+                s += su;
             }
-            s += su;
         }
-    }
-    s = tile_sum(s);
-    if (threadIdx.x == 0 && threadIdx.y == 0) part[blockIdx.x] = s;
+        s = tile_sum(s);
+        if (threadIdx.x == 0 && threadIdx.y == 0) part[q] = s;
+    });
 }
 
 // sum of one component per tile (the null-space means)
-__global__ void __launch_bounds__(256) kb_sum(const Tile* tiles, const Lev* lev, const Ctl* ctl, int mode,
+__global__ void __launch_bounds__(256) kb_sum(const Tile* tiles, int n, const Lev* lev, const Ctl* ctl, int mode,
                                               const double* a, double* part) {
-    const Tile t = tiles[blockIdx.x];
-    if (!covers(ctl[t.box], mode)) return;
-    const Lev L = lev[t.box * MAXL];
-    const int j = t.j0 + threadIdx.y;
-    double s = 0.0;
-    if (j < L.g.n[1]) {
-#pragma unroll
-        for (int u = 0; u < 2; u++) {
-            const int i = t.i0 + threadIdx.x + 32 * u;
-            if (i < L.g.n[0]) s += a[L.off + (i64)i + (i64)L.g.n[0] * j];
+    for_tiles(tiles, n, ctl, mode, [&](const Tile& t, int q) {
+        const Lev L = lev[t.box * MAXL];
+        const int j = t.j0 + threadIdx.y;
+        double s = 0.0;
+        if (j < L.g.n[1]) {
+    #pragma unroll
+            for (int u = 0; u < 2; u++) {
+                const int i = t.i0 + threadIdx.x + 32 * u;
+                if (i < L.g.n[0]) s += a[L.off + (i64)i + (i64)L.g.n[0] * j];
+            }
         }
-    }
-    s = tile_sum(s);
-    if (threadIdx.x == 0 && threadIdx.y == 0) part[blockIdx.x] = s;
+        s = tile_sum(s);
+        if (threadIdx.x == 0 && threadIdx.y == 0) part[q] = s;
+    });
 }
 
 // a -= its box's mean (ctl.mean[which] / cells)
-__global__ void __launch_bounds__(256) kb_sub_mean(const Tile* tiles, const Lev* lev, const Ctl* ctl, int mode,
+__global__ void __launch_bounds__(256) kb_sub_mean(const Tile* tiles, int n, const Lev* lev, const Ctl* ctl, int mode,
                                                    double* a, int which) {
-    const Tile t = tiles[blockIdx.x];
-    if (!covers(ctl[t.box], mode)) return;
-    const Lev L = lev[t.box * MAXL];
-    const int j = t.j0 + threadIdx.y;
-    if (j >= L.g.n[1]) return;
-    const double m = ctl[t.box].mean[which] / (double)L.g.nc;
-#pragma unroll
-    for (int u = 0; u < 2; u++) {
-        const int i = t.i0 + threadIdx.x + 32 * u;
-        if (i < L.g.n[0]) {
-            double* p = a + L.off + (i64)i + (i64)L.g.n[0] * j;
-            *p = *p - m;
+    for_tiles(tiles, n, ctl, mode, [&](const Tile& t, int q) {
+        const Lev L = lev[t.box * MAXL];
+        const int j = t.j0 + threadIdx.y;
+        if (j >= L.g.n[1]) return;
+        const double m = ctl[t.box].mean[which] / (double)L.g.nc;
+    #pragma unroll
+        for (int u = 0; u < 2; u++) {
+            const int i = t.i0 + threadIdx.x + 32 * u;
+            if (i < L.g.n[0]) {
+                double* p = a + L.off + (i64)i + (i64)L.g.n[0] * j;
+                *p = *p - m;
+            }
         }
-    }
+    });
 }
 
 // ---------------------------------------------------------------------
 // apply_matrix and the Krylov vector passes (FP64)
 // ---------------------------------------------------------------------
 // out = A x (mode 0) or rhs - A x (mode 1) (k_stokes_apply)
-__global__ void __launch_bounds__(256) kb_stokes_apply(const Tile* tiles, const Lev* lev, const Ctl* ctl, int mode,
+__global__ void __launch_bounds__(256) kb_stokes_apply(const Tile* tiles, int n, const Lev* lev, const Ctl* ctl, int mode,
                                                        const double* const* x, const double* const* rhs,
                                                        double* const* out, int amode, const double* ones,
                                                        double theta) {
-    const Tile t = tiles[blockIdx.x];
-    if (!covers(ctl[t.box], mode)) return;
-    const Lev L = lev[t.box * MAXL];
-    const int j = t.j0 + threadIdx.y;
-    if (j >= L.g.n[1]) return;
-    const StagOp<double> A = box_op<double>(ones, theta, ctl[t.box].eta, L.g.dx);
-    const double dxinv = 1.0 / L.g.dx;
-    const double* phi[3] = {x[0] + L.off, x[1] + L.off, nullptr};
-    const double* p = x[2] + L.off;
-#pragma unroll
-    for (int u = 0; u < 2; u++) {
-        const int i = t.i0 + threadIdx.x + 32 * u;
-        if (i >= L.g.n[0]) continue;
-        CellF P;
-        P.set(L.g, i, j, 0);
-        const i64 f = P.id(0, 0, 0);
-        const double pc = ld(p, f);
-        double div = 0.0;
-#pragma unroll
-        for (int c = 0; c < 2; c++) {
-            double dg;
-            double Lv = stag_lface_c<double, 2, 1>(c, A, phi, P, dg);
-            const double gp = (pc - ld(p, P.id(-(c == 0), -(c == 1), 0))) * dxinv;
-            Lv = Lv + gp;
-            out[c][L.off + f] = amode ? ld(rhs[c] + L.off, f) - Lv : Lv;
-            div += (ld(phi[c], P.id(c == 0, c == 1, 0)) - ld(phi[c], f)) * dxinv;
+    for_tiles(tiles, n, ctl, mode, [&](const Tile& t, int q) {
+        const Lev L = lev[t.box * MAXL];
+        const int j = t.j0 + threadIdx.y;
+        if (j >= L.g.n[1]) return;
+        const StagOp<double> A = box_op<double>(ones, theta, ctl[t.box].eta, L.g.dx);
+        const double dxinv = 1.0 / L.g.dx;
+        const double* phi[3] = {x[0] + L.off, x[1] + L.off, nullptr};
+        const double* p = x[2] + L.off;
+    #pragma unroll
+        for (int u = 0; u < 2; u++) {
+            const int i = t.i0 + threadIdx.x + 32 * u;
+            if (i >= L.g.n[0]) continue;
+            CellF P;
+            P.set(L.g, i, j, 0);
+            const i64 f = P.id(0, 0, 0);
+            const double pc = ld(p, f);
+            double div = 0.0;
+    #pragma unroll
+            for (int c = 0; c < 2; c++) {
+                double dg;
+                double Lv = stag_lface_c<double, 2, 1>(c, A, phi, P, dg);
+                const double gp = (pc - ld(p, P.id(-(c == 0), -(c == 1), 0))) * dxinv;
+                Lv = Lv + gp;
+                out[c][L.off + f] = amode ? ld(rhs[c] + L.off, f) - Lv : Lv;
+                div += (ld(phi[c], P.id(c == 0, c == 1, 0)) - ld(phi[c], f)) * dxinv;
+            }
+            const double bp = div * -1.0;
+            out[2][L.off + f] = amode ? ld(rhs[2] + L.off, f) - bp : bp;
         }
-        const double bp = div * -1.0;
-        out[2][L.off + f] = amode ? ld(rhs[2] + L.off, f) - bp : bp;
-    }
+    });
 }
 
 // Modified Gram-Schmidt pass k (k_mgs): w -= h[k-1] V_{k-2} (k > 1), then
 // the tile's partial of <w, V_{k-1}> (or <w, w> when vnext is null)
-__global__ void __launch_bounds__(256) kb_mgs(const Tile* tiles, const Lev* lev, const Ctl* ctl, double* const* w,
+__global__ void __launch_bounds__(256) kb_mgs(const Tile* tiles, int n, const Lev* lev, const Ctl* ctl, double* const* w,
                                               const double* const* vprev, int hk, const double* const* vnext,
                                               double wp2, double* part) {
-    const Tile t = tiles[blockIdx.x];
-    if (!ctl[t.box].inner) return;
-    const Lev L = lev[t.box * MAXL];
-    const double h = vprev ? ctl[t.box].h[hk] : 0.0;
-    const int j = t.j0 + threadIdx.y;
-    double s = 0.0;
-    if (j < L.g.n[1]) {
-#pragma unroll
-        for (int u = 0; u < 2; u++) {
-            const int i = t.i0 + threadIdx.x + 32 * u;
-            if (i >= L.g.n[0]) continue;
-            const i64 f = L.off + (i64)i + (i64)L.g.n[0] * j;
-            double su = 0.0;
-#pragma unroll
-            for (int c = 0; c < 3; c++) {
-                double x = w[c][f];
-                if (vprev) {
-                    x = x - vprev[c][f] * h;
-                    w[c][f] = x;
+    for_tiles(tiles, n, ctl, M_INNER, [&](const Tile& t, int q) {
+        const Lev L = lev[t.box * MAXL];
+        const double h = vprev ? ctl[t.box].h[hk] : 0.0;
+        const int j = t.j0 + threadIdx.y;
+        double s = 0.0;
+        if (j < L.g.n[1]) {
+    #pragma unroll
+            for (int u = 0; u < 2; u++) {
+                const int i = t.i0 + threadIdx.x + 32 * u;
+                if (i >= L.g.n[0]) continue;
+                const i64 f = L.off + (i64)i + (i64)L.g.n[0] * j;
+                double su = 0.0;
+    #pragma unroll
+                for (int c = 0; c < 3; c++) {
+                    double x = w[c][f];
+                    if (vprev) {
+                        x = x - vprev[c][f] * h;
+                        w[c][f] = x;
+                    }
+                    const double y = vnext ? vnext[c][f] : x;
+                    const double tt = x * y;
+                    su += c == 2 ? wp2 * tt : tt;
                 }
-                const double y = vnext ? vnext[c][f] : x;
-                const double tt = x * y;
-                su += c == 2 ? wp2 * tt : tt;
+                s += su;
             }
-            s += su;
         }
-    }
-    s = tile_sum(s);
-    if (threadIdx.x == 0 && threadIdx.y == 0) part[blockIdx.x] = s;
+        s = tile_sum(s);
+        if (threadIdx.x == 0 && threadIdx.y == 0) part[q] = s;
+    });
 }
 
 // v = w / |w| with |w| = sqrt(ctl.h[hk]) (k_scale_by_norm), or w / norm_resid
 // (k_scale_div, hk < 0)
-__global__ void __launch_bounds__(256) kb_scale(const Tile* tiles, const Lev* lev, const Ctl* ctl,
+__global__ void __launch_bounds__(256) kb_scale(const Tile* tiles, int n, const Lev* lev, const Ctl* ctl,
                                                 double* const* v, const double* const* w, int hk) {
-    const Tile t = tiles[blockIdx.x];
-    const Ctl& c = ctl[t.box];
-    if (!c.inner) return;
-    const Lev L = lev[t.box * MAXL];
-    const int j = t.j0 + threadIdx.y;
-    if (j >= L.g.n[1]) return;
-    const double d = hk < 0 ? c.norm_resid : sqrt(c.h[hk]);
-#pragma unroll
-    for (int u = 0; u < 2; u++) {
-        const int i = t.i0 + threadIdx.x + 32 * u;
-        if (i >= L.g.n[0]) continue;
-        const i64 f = L.off + (i64)i + (i64)L.g.n[0] * j;
-#pragma unroll
-        for (int q = 0; q < 3; q++) v[q][f] = w[q][f] / d;
-    }
+    for_tiles(tiles, n, ctl, M_INNER, [&](const Tile& t, int q) {
+        const Ctl& c = ctl[t.box];
+        const Lev L = lev[t.box * MAXL];
+        const int j = t.j0 + threadIdx.y;
+        if (j >= L.g.n[1]) return;
+        const double d = hk < 0 ? c.norm_resid : sqrt(c.h[hk]);
+    #pragma unroll
+        for (int u = 0; u < 2; u++) {
+            const int i = t.i0 + threadIdx.x + 32 * u;
+            if (i >= L.g.n[0]) continue;
+            const i64 f = L.off + (i64)i + (i64)L.g.n[0] * j;
+    #pragma unroll
+            for (int q = 0; q < 3; q++) v[q][f] = w[q][f] / d;
+        }
+    });
 }
 
 // x += sum_k y_k V_{k-1} over the box's exit index (k_update_sol)
-__global__ void __launch_bounds__(256) kb_update_sol(const Tile* tiles, const Lev* lev, const Ctl* ctl,
+__global__ void __launch_bounds__(256) kb_update_sol(const Tile* tiles, int n, const Lev* lev, const Ctl* ctl,
                                                      double* const* x, const double* V, i64 vstride, i64 cstride) {
-    const Tile t = tiles[blockIdx.x];
-    const Ctl& c = ctl[t.box];
-    if (!c.pend) return;
-    const Lev L = lev[t.box * MAXL];
-    const int j = t.j0 + threadIdx.y;
-    if (j >= L.g.n[1]) return;
-    const int m = c.i_exit;
-#pragma unroll
-    for (int u = 0; u < 2; u++) {
-        const int i = t.i0 + threadIdx.x + 32 * u;
-        if (i >= L.g.n[0]) continue;
-        const i64 f = L.off + (i64)i + (i64)L.g.n[0] * j;
-        double acc[3] = {x[0][f], x[1][f], x[2][f]};
-        for (int it = 0; it < m; it++) {
-            const double yi = c.y[it + 1];
-#pragma unroll
-            for (int q = 0; q < 3; q++) acc[q] = acc[q] + V[it * vstride + (i64)q * cstride + f] * yi;
+    for_tiles(tiles, n, ctl, M_PEND, [&](const Tile& t, int q) {
+        const Ctl& c = ctl[t.box];
+        const Lev L = lev[t.box * MAXL];
+        const int j = t.j0 + threadIdx.y;
+        if (j >= L.g.n[1]) return;
+        const int m = c.i_exit;
+    #pragma unroll
+        for (int u = 0; u < 2; u++) {
+            const int i = t.i0 + threadIdx.x + 32 * u;
+            if (i >= L.g.n[0]) continue;
+            const i64 f = L.off + (i64)i + (i64)L.g.n[0] * j;
+            double acc[3] = {x[0][f], x[1][f], x[2][f]};
+            for (int it = 0; it < m; it++) {
+                const double yi = c.y[it + 1];
+    #pragma unroll
+                for (int q = 0; q < 3; q++) acc[q] = acc[q] + V[it * vstride + (i64)q * cstride + f] * yi;
+            }
+    #pragma unroll
+            for (int q = 0; q < 3; q++) x[q][f] = acc[q];
         }
-#pragma unroll
-        for (int q = 0; q < 3; q++) x[q][f] = acc[q];
-    }
+    });
 }
 
 // x = 0 for the boxes whose rhs is below gmres_abs_tol (gmres.f90:166-172)
-__global__ void __launch_bounds__(256) kb_zero_x(const Tile* tiles, const Lev* lev, const Ctl* ctl,
+__global__ void __launch_bounds__(256) kb_zero_x(const Tile* tiles, int n, const Lev* lev, const Ctl* ctl,
                                                  double* const* x) {
-    const Tile t = tiles[blockIdx.x];
-    if (!ctl[t.box].zero_x) return;
-    const Lev L = lev[t.box * MAXL];
-    const int j = t.j0 + threadIdx.y;
-    if (j >= L.g.n[1]) return;
-#pragma unroll
-    for (int u = 0; u < 2; u++) {
-        const int i = t.i0 + threadIdx.x + 32 * u;
-        if (i >= L.g.n[0]) continue;
-        const i64 f = L.off + (i64)i + (i64)L.g.n[0] * j;
-        x[0][f] = 0.0;
-        x[1][f] = 0.0;
-        x[2][f] = 0.0;
-    }
+    for_tiles(tiles, n, ctl, M_ZERO, [&](const Tile& t, int q) {
+        const Lev L = lev[t.box * MAXL];
+        const int j = t.j0 + threadIdx.y;
+        if (j >= L.g.n[1]) return;
+    #pragma unroll
+        for (int u = 0; u < 2; u++) {
+            const int i = t.i0 + threadIdx.x + 32 * u;
+            if (i >= L.g.n[0]) continue;
+            const i64 f = L.off + (i64)i + (i64)L.g.n[0] * j;
+            x[0][f] = 0.0;
+            x[1][f] = 0.0;
+            x[2][f] = 0.0;
+        }
+    });
 }
 
 // ---------------------------------------------------------------------
@@ -629,15 +676,24 @@ struct GParams {
     int m, max_iter, min_iter, max_outer;
 };
 
+// one warp per box: the control block zeroed word by word, keeping the
+// accumulated iteration count
 __global__ void kb_ctl_reset(int nbox, Ctl* ctl, const double* eta, const double* abs_tol) {
-    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    const int b = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
     if (b >= nbox) return;
     Ctl& c = ctl[b];
     const int acc = c.iters_acc;
-    memset(&c, 0, sizeof(Ctl));
-    c.iters_acc = acc;
-    c.eta = eta[b];
-    c.abs_tol = abs_tol[b];
+    __syncwarp();
+    unsigned long long* w = reinterpret_cast<unsigned long long*>(&c);
+    static_assert(sizeof(Ctl) % 8 == 0, "Ctl is a whole number of 8-byte words");
+    for (int k = lane; k < (int)(sizeof(Ctl) / 8); k += 32) w[k] = 0ull;
+    __syncwarp();
+    if (lane == 0) {
+        c.iters_acc = acc;
+        c.eta = eta[b];
+        c.abs_tol = abs_tol[b];
+    }
 }
 
 // after |M^-1 b|^2 (nrm[0]) and |b|^2 (nrm[1])
@@ -808,78 +864,80 @@ struct StepNoise {
 // cell entries sqrt(2) N(0,1) (field 2r + c), node entries N(0,1) (field
 // 4 + r) shared by the two components, scaled by sqrt(var_fac kT eta)
 template <typename T>
-__global__ void __launch_bounds__(256) kb_step_rhs(const Tile* tiles, const Lev* lev, const Ctl* ctl,
+__global__ void __launch_bounds__(256) kb_step_rhs(const Tile* tiles, int n, const Lev* lev, const Ctl* ctl,
                                                    const double* const* u, const double* p, double* const* rv,
                                                    double* rp, const double* ones, const double* kT, StepNoise N) {
-    const Tile t = tiles[blockIdx.x];
-    const Lev L = lev[t.box * MAXL];
-    const int j = t.j0 + threadIdx.y;
-    if (j >= L.g.n[1]) return;
-    const double eta = ctl[t.box].eta;
-    const StagOp<double> A = box_op<double>(ones, 0.0, eta, L.g.dx);
-    const double dxinv = 1.0 / L.g.dx;
-    const double* phi[3] = {u[0] + L.off, u[1] + L.off, nullptr};
-    const double* pp = p + L.off;
-    const T amp = (T)(sqrt(N.var_fac * kT[t.box]) * sqrt(eta));
-    const int nx = L.g.n[0], ny = L.g.n[1];
-    auto cell_w = [&](int ci, int cj, int comp) -> T {
-        const uint32_t e = (uint32_t)(wrapc(ci, nx) + nx * wrapc(cj, ny));
-        T s = T(0);
-        for (int r = 0; r < 2; r++)
-            if (N.w[r] != 0.0)
-                s = s + (T)N.w[r] * (T)(1.4142135623730951 * normal_at(N.seed, t.box, e, 2 * r + comp, N.step));
-        return amp * s;
-    };
-    auto node_w = [&](int ci, int cj) -> T {
-        const uint32_t e = (uint32_t)(wrapc(ci, nx) + nx * wrapc(cj, ny));
-        T s = T(0);
-        for (int r = 0; r < 2; r++)
-            if (N.w[r] != 0.0) s = s + (T)N.w[r] * (T)normal_at(N.seed, t.box, e, 4 + r, N.step);
-        return amp * s;
-    };
-#pragma unroll
-    for (int uu = 0; uu < 2; uu++) {
-        const int i = t.i0 + threadIdx.x + 32 * uu;
-        if (i >= nx) continue;
-        CellF P;
-        P.set(L.g, i, j, 0);
-        const i64 f = P.id(0, 0, 0);
-        const T dxi = (T)dxinv;
-        T dv[2];
-        dv[0] = (cell_w(i, j, 0) - cell_w(i - 1, j, 0)) * dxi + (node_w(i, j + 1) - node_w(i, j)) * dxi;
-        dv[1] = (node_w(i + 1, j) - node_w(i, j)) * dxi + (cell_w(i, j, 1) - cell_w(i, j - 1, 1)) * dxi;
-        const double pc = ld(pp, f);
-        double div = 0.0;
-#pragma unroll
-        for (int c = 0; c < 2; c++) {
-            double dg;
-            const double Lu = stag_lface_c<double, 2, 1>(c, A, phi, P, dg);  // -eta Lap u
-            const double gp = (pc - ld(pp, P.id(-(c == 0), -(c == 1), 0))) * dxinv;
-            double v = -gp;
-            v = v + (double)dv[c];
-            v = v + Lu * -1.0;
-            rv[c][L.off + f] = v;
-            div += (ld(phi[c], P.id(c == 0, c == 1, 0)) - ld(phi[c], f)) * dxinv;
+    for_tiles(tiles, n, ctl, M_ALL, [&](const Tile& t, int q) {
+        const Lev L = lev[t.box * MAXL];
+        const int j = t.j0 + threadIdx.y;
+        if (j >= L.g.n[1]) return;
+        const double eta = ctl[t.box].eta;
+        const StagOp<double> A = box_op<double>(ones, 0.0, eta, L.g.dx);
+        const double dxinv = 1.0 / L.g.dx;
+        const double* phi[3] = {u[0] + L.off, u[1] + L.off, nullptr};
+        const double* pp = p + L.off;
+        const T amp = (T)(sqrt(N.var_fac * kT[t.box]) * sqrt(eta));
+        const int nx = L.g.n[0], ny = L.g.n[1];
+        auto cell_w = [&](int ci, int cj, int comp) -> T {
+            const uint32_t e = (uint32_t)(wrapc(ci, nx) + nx * wrapc(cj, ny));
+            T s = T(0);
+            for (int r = 0; r < 2; r++)
+                if (N.w[r] != 0.0)
+                    s = s + (T)N.w[r] * (T)(1.4142135623730951 * normal_at(N.seed, t.box, e, 2 * r + comp, N.step));
+            return amp * s;
+        };
+        auto node_w = [&](int ci, int cj) -> T {
+            const uint32_t e = (uint32_t)(wrapc(ci, nx) + nx * wrapc(cj, ny));
+            T s = T(0);
+            for (int r = 0; r < 2; r++)
+                if (N.w[r] != 0.0) s = s + (T)N.w[r] * (T)normal_at(N.seed, t.box, e, 4 + r, N.step);
+            return amp * s;
+        };
+    #pragma unroll
+        for (int uu = 0; uu < 2; uu++) {
+            const int i = t.i0 + threadIdx.x + 32 * uu;
+            if (i >= nx) continue;
+            CellF P;
+            P.set(L.g, i, j, 0);
+            const i64 f = P.id(0, 0, 0);
+            const T dxi = (T)dxinv;
+            T dv[2];
+            dv[0] = (cell_w(i, j, 0) - cell_w(i - 1, j, 0)) * dxi + (node_w(i, j + 1) - node_w(i, j)) * dxi;
+            dv[1] = (node_w(i + 1, j) - node_w(i, j)) * dxi + (cell_w(i, j, 1) - cell_w(i, j - 1, 1)) * dxi;
+            const double pc = ld(pp, f);
+            double div = 0.0;
+    #pragma unroll
+            for (int c = 0; c < 2; c++) {
+                double dg;
+                const double Lu = stag_lface_c<double, 2, 1>(c, A, phi, P, dg);  // -eta Lap u
+                const double gp = (pc - ld(pp, P.id(-(c == 0), -(c == 1), 0))) * dxinv;
+                double v = -gp;
+                v = v + (double)dv[c];
+                v = v + Lu * -1.0;
+                rv[c][L.off + f] = v;
+                div += (ld(phi[c], P.id(c == 0, c == 1, 0)) - ld(phi[c], f)) * dxinv;
+            }
+            rp[L.off + f] = div;
         }
-        rp[L.off + f] = div;
-    }
+    });
 }
 
 // u += du, p += dp
-__global__ void __launch_bounds__(256) kb_axpy3(const Tile* tiles, const Lev* lev, double* const* a,
+__global__ void __launch_bounds__(256) kb_axpy3(const Tile* tiles, int n, const Lev* lev, double* const* a,
                                                 const double* const* d) {
-    const Tile t = tiles[blockIdx.x];
-    const Lev L = lev[t.box * MAXL];
-    const int j = t.j0 + threadIdx.y;
-    if (j >= L.g.n[1]) return;
-#pragma unroll
-    for (int u = 0; u < 2; u++) {
-        const int i = t.i0 + threadIdx.x + 32 * u;
-        if (i >= L.g.n[0]) continue;
-        const i64 f = L.off + (i64)i + (i64)L.g.n[0] * j;
-#pragma unroll
-        for (int q = 0; q < 3; q++) a[q][f] = a[q][f] + d[q][f];
-    }
+    for_tiles(tiles, n, nullptr, M_ALL, [&](const Tile& t, int q) {
+        const Lev L = lev[t.box * MAXL];
+        const int j = t.j0 + threadIdx.y;
+        if (j >= L.g.n[1]) return;
+    #pragma unroll
+        for (int u = 0; u < 2; u++) {
+            const int i = t.i0 + threadIdx.x + 32 * u;
+            if (i >= L.g.n[0]) continue;
+            const i64 f = L.off + (i64)i + (i64)L.g.n[0] * j;
+    #pragma unroll
+            for (int q = 0; q < 3; q++) a[q][f] = a[q][f] + d[q][f];
+        }
+    });
 }
 
 __global__ void kb_set_abs_tol(int nbox, const Ctl* ctl, double* abs_tol, double base, double rel) {
@@ -932,6 +990,10 @@ struct fhd_batch {
     void* cargs = nullptr;                // CCCoarseArgs<T>[nbox]
     std::vector<unsigned char> sargs_h;   // host copy of sargs
     size_t smem_s = 0, smem_c = 0;
+    // coarse-kernel CTA -> box, the boxes with the largest coarse hierarchy
+    // first (they set the launch's length; the small ones fill in behind)
+    int* ord_s = nullptr;
+    int* ord_c = nullptr;
     // FP64 level-0 vectors, three components each: b, x, r, w, tmp, V (m+1)
     i64 N0 = 0;
     double* vec = nullptr;                // all FP64 vectors
@@ -947,6 +1009,12 @@ struct fhd_batch {
     double* step = nullptr;
     double* dkT = nullptr;
     long long launches = 0;
+    std::unordered_map<const void*, int> occ;  // resident CTAs per SM of each tile kernel
+    // GMRES launch sequences as CUDA graphs: init, outer, inner (see gmres)
+    cudaGraphExec_t gx[3] = {nullptr, nullptr, nullptr};
+    long long gn[3] = {0, 0, 0};  // kernels in each
+    int g_ok = 0;
+    double g_theta = 0.0;
 };
 
 namespace {
@@ -1209,6 +1277,20 @@ int build(fhd_batch* B) {
     if (!B->sargs || !B->cargs) return FHD_ERR_OOM;
     cudaMemcpy(B->sargs, sa.data(), sizeof(StagCoarseArgs<T>) * nb, cudaMemcpyHostToDevice);
     cudaMemcpy(B->cargs, ca.data(), sizeof(CCCoarseArgs<T>) * nb, cudaMemcpyHostToDevice);
+    {
+        std::vector<int> os(nb), oc(nb);
+        for (int b = 0; b < nb; b++) os[b] = oc[b] = b;
+        auto work = [&](const std::vector<Lev>& v, int b, int l0) { return v[(size_t)b * MAXL + l0].g.nc; };
+        std::stable_sort(os.begin(), os.end(),
+                         [&](int a, int b) { return work(ls, a, B->lcs[a]) > work(ls, b, B->lcs[b]); });
+        std::stable_sort(oc.begin(), oc.end(),
+                         [&](int a, int b) { return work(lc, a, B->lcc[a]) > work(lc, b, B->lcc[b]); });
+        B->ord_s = dalloc<int>(B, nb);
+        B->ord_c = dalloc<int>(B, nb);
+        if (!B->ord_s || !B->ord_c) return FHD_ERR_OOM;
+        cudaMemcpy(B->ord_s, os.data(), sizeof(int) * nb, cudaMemcpyHostToDevice);
+        cudaMemcpy(B->ord_c, oc.data(), sizeof(int) * nb, cudaMemcpyHostToDevice);
+    }
     B->sargs_h.resize(sizeof(StagCoarseArgs<T>) * nb);
     memcpy(B->sargs_h.data(), sa.data(), B->sargs_h.size());
     if (B->smem_s > budget || B->smem_c > budget) return FHD_ERR_UNSUPPORTED;
@@ -1261,6 +1343,22 @@ inline int post(fhd_batch* B) {
 
 const dim3 TB(32, 8, 1);
 
+// grid of a tile kernel (for_tiles): its resident CTAs on every SM, at most
+// one CTA per tile
+template <class K>
+int tgrid(fhd_batch* B, K kern, int n) {
+    const void* key = reinterpret_cast<const void*>(kern);
+    auto it = B->occ.find(key);
+    int per = 1;
+    if (it == B->occ.end()) {
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, 256, 0) != cudaSuccess || per < 1) per = 1;
+        B->occ[key] = per;
+    } else {
+        per = it->second;
+    }
+    return std::max(1, std::min(n, per * B->sms));
+}
+
 // per-box sum of the tile partials into ctl.<which>
 int seg(fhd_batch* B, int mode, int which) {
     kb_seg_sum<<<(B->nbox * 32 + 255) / 256, 256, 0, B->stream>>>(B->nbox, B->part, B->dt0, B->ctl, mode, which);
@@ -1278,10 +1376,10 @@ int stag_smooth(fhd_batch* B, int l, int mode, T theta, int count) {
         for (int color = 1; color <= 4; color++) {
             const int par = (color + 1) & 1;
             if (color <= 2)
-                kb_stag_gs<T, 0><<<B->ntab_s[l], TB, 0, B->stream>>>(B->tab_s[l], B->dlev_s, l, B->ctl, mode, phi,
+                kb_stag_gs<T, 0><<<tgrid(B, kb_stag_gs<T, 0>, B->ntab_s[l]), TB, 0, B->stream>>>(B->tab_s[l], B->ntab_s[l], B->dlev_s, l, B->ctl, mode, phi,
                                                                     rhs, (const T*)B->ones, theta, par, omega);
             else
-                kb_stag_gs<T, 1><<<B->ntab_s[l], TB, 0, B->stream>>>(B->tab_s[l], B->dlev_s, l, B->ctl, mode, phi,
+                kb_stag_gs<T, 1><<<tgrid(B, kb_stag_gs<T, 1>, B->ntab_s[l]), TB, 0, B->stream>>>(B->tab_s[l], B->ntab_s[l], B->dlev_s, l, B->ctl, mode, phi,
                                                                     rhs, (const T*)B->ones, theta, par, omega);
             BPOST(B);
         }
@@ -1300,22 +1398,23 @@ int stag_vcycle(fhd_batch* B, int mode, T theta) {
         if (!B->ntab_s[l]) continue;
         int rc = stag_smooth<T>(B, l, mode, theta, B->p.stag_mg_nsmooths_down);
         if (rc) return rc;
-        kb_stag_resid<T><<<B->ntab_s[l], TB, 0, st>>>(B->tab_s[l], B->dlev_s, l, B->ctl, mode,
+        kb_stag_resid<T><<<tgrid(B, kb_stag_resid<T>, B->ntab_s[l]), TB, 0, st>>>(B->tab_s[l], B->ntab_s[l], B->dlev_s, l, B->ctl, mode,
                                                        (T* const*)(B->dsphi + 2 * l), (const T* const*)(B->dsrhs + 2 * l),
                                                        (T* const*)(B->dstmp + 2 * l), (const T*)B->ones, theta);
         BPOST(B);
         // the restriction's targets: level l+1 of the boxes smoothing level l
         // by launches (it may be their coarse kernel's first level)
-        kb_stag_restrict<T><<<B->nall_s[l + 1], TB, 0, st>>>(B->all_s[l + 1], B->dlev_s, l, B->ctl, mode,
+        kb_stag_restrict<T><<<tgrid(B, kb_stag_restrict<T>, B->nall_s[l + 1]), TB, 0, st>>>(B->all_s[l + 1], B->nall_s[l + 1], B->dlev_s, l, B->ctl, mode,
                                                             (T* const*)(B->dstmp + 2 * l),
                                                             (T* const*)(B->dsrhs + 2 * (l + 1)));
         BPOST(B);
     }
-    kb_stag_coarse<T><<<B->nbox, CS_THREADS, B->smem_s, st>>>((const StagCoarseArgs<T>*)B->sargs, B->ctl, mode);
+    kb_stag_coarse<T><<<B->nbox, CS_THREADS, B->smem_s, st>>>((const StagCoarseArgs<T>*)B->sargs, B->ord_s, B->ctl,
+                                                              mode);
     BPOST(B);
     for (int l = B->Ls - 2; l >= 0; l--) {
         if (!B->ntab_s[l]) continue;
-        kb_stag_prolong<T><<<B->ntab_s[l], TB, 0, st>>>(B->tab_s[l], B->dlev_s, l, B->ctl, mode,
+        kb_stag_prolong<T><<<tgrid(B, kb_stag_prolong<T>, B->ntab_s[l]), TB, 0, st>>>(B->tab_s[l], B->ntab_s[l], B->dlev_s, l, B->ctl, mode,
                                                          (T* const*)(B->dsphi + 2 * l));
         BPOST(B);
         int rc = stag_smooth<T>(B, l, mode, theta, B->p.stag_mg_nsmooths_up);
@@ -1333,7 +1432,7 @@ int cc_vcycle(fhd_batch* B, int mode) {
     auto smooth = [&](int l, int count) -> int {
         for (int s = 0; s < count; s++)
             for (int par = 0; par < 2; par++) {
-                kb_cc_gsrb<T><<<B->ntab_c[l], TB, 0, st>>>(B->tab_c[l], B->dlev_c, l, B->ctl, mode, (T*)B->cphi[l],
+                kb_cc_gsrb<T><<<tgrid(B, kb_cc_gsrb<T>, B->ntab_c[l]), TB, 0, st>>>(B->tab_c[l], B->ntab_c[l], B->dlev_c, l, B->ctl, mode, (T*)B->cphi[l],
                                                           (const T*)B->crhs[l], (const T*)B->ones, par);
                 BPOST(B);
             }
@@ -1343,16 +1442,17 @@ int cc_vcycle(fhd_batch* B, int mode) {
         if (!B->ntab_c[l]) continue;
         int rc = smooth(l, B->p.mg_nsmooths_down);
         if (rc) return rc;
-        kb_cc_resid_restrict<T><<<B->nall_c[l + 1], TB, 0, st>>>(B->all_c[l + 1], B->dlev_c, l, B->ctl, mode,
+        kb_cc_resid_restrict<T><<<tgrid(B, kb_cc_resid_restrict<T>, B->nall_c[l + 1]), TB, 0, st>>>(B->all_c[l + 1], B->nall_c[l + 1], B->dlev_c, l, B->ctl, mode,
                                                                 (const T*)B->cphi[l], (const T*)B->crhs[l],
                                                                 (T*)B->crhs[l + 1], (const T*)B->ones);
         BPOST(B);
     }
-    kb_cc_coarse<T><<<B->nbox, CS_THREADS, B->smem_c, st>>>((const CCCoarseArgs<T>*)B->cargs, B->ctl, mode);
+    kb_cc_coarse<T><<<B->nbox, CS_THREADS, B->smem_c, st>>>((const CCCoarseArgs<T>*)B->cargs, B->ord_c, B->ctl,
+                                                            mode);
     BPOST(B);
     for (int l = B->Lc - 2; l >= 0; l--) {
         if (!B->ntab_c[l]) continue;
-        kb_cc_prolong<T><<<B->ntab_c[l], TB, 0, st>>>(B->tab_c[l], B->dlev_c, l, B->ctl, mode, (T*)B->cphi[l],
+        kb_cc_prolong<T><<<tgrid(B, kb_cc_prolong<T>, B->ntab_c[l]), TB, 0, st>>>(B->tab_c[l], B->ntab_c[l], B->dlev_c, l, B->ctl, mode, (T*)B->cphi[l],
                                                       (const T*)B->cphi[l + 1]);
         BPOST(B);
         int rc = smooth(l, B->p.mg_nsmooths_up);
@@ -1368,25 +1468,25 @@ int precon(fhd_batch* B, int bv, int xv, int mode, double theta) {
     // level-0 velocity unknowns start at zero, rhs = b_u
     for (int c = 0; c < 2; c++)
         if (cudaMemsetAsync(B->sphi[c], 0, sizeof(T) * B->N0, st) != cudaSuccess) return FHD_ERR_CUDA;
-    kb_to_T<T><<<B->ntab0, TB, 0, st>>>(B->tab0, B->dlev_s, B->ctl, mode, vp(B, bv), (T* const*)B->dsrhs);
+    kb_to_T<T><<<tgrid(B, kb_to_T<T>, B->ntab0), TB, 0, st>>>(B->tab0, B->ntab0, B->dlev_s, B->ctl, mode, vp(B, bv), (T* const*)B->dsrhs);
     BPOST(B);
     int rc = stag_vcycle<T>(B, mode, (T)theta);
     if (rc) return rc;
-    kb_div_plus<T><<<B->ntab0, TB, 0, st>>>(B->tab0, B->dlev_s, B->ctl, mode, (T* const*)B->dsphi, vc(B, bv, 2),
+    kb_div_plus<T><<<tgrid(B, kb_div_plus<T>, B->ntab0), TB, 0, st>>>(B->tab0, B->ntab0, B->dlev_s, B->ctl, mode, (T* const*)B->dsphi, vc(B, bv, 2),
                                             (T*)B->crhs[0]);
     BPOST(B);
     if ((rc = cc_vcycle<T>(B, mode))) return rc;
-    kb_precon_out<T><<<B->ntab0, TB, 0, st>>>(B->tab0, B->dlev_s, B->ctl, mode, (T* const*)B->dsphi,
+    kb_precon_out<T><<<tgrid(B, kb_precon_out<T>, B->ntab0), TB, 0, st>>>(B->tab0, B->ntab0, B->dlev_s, B->ctl, mode, (T* const*)B->dsphi,
                                               (const T*)B->cphi[0], (const T*)B->crhs[0], theta, vp(B, xv));
     BPOST(B);
     // null space (apply_precon.f90:429-460): mean of p, and of u when theta = 0
     const int ncomp = theta == 0.0 ? 3 : 1;
     for (int q = 0; q < ncomp; q++) {
         const int c = q == 0 ? 2 : q - 1;
-        kb_sum<<<B->ntab0, TB, 0, st>>>(B->tab0, B->dlev_s, B->ctl, mode, vc(B, xv, c), B->part);
+        kb_sum<<<tgrid(B, kb_sum, B->ntab0), TB, 0, st>>>(B->tab0, B->ntab0, B->dlev_s, B->ctl, mode, vc(B, xv, c), B->part);
         BPOST(B);
         if ((rc = seg(B, mode, 2 + q))) return rc;
-        kb_sub_mean<<<B->ntab0, TB, 0, st>>>(B->tab0, B->dlev_s, B->ctl, mode, vc(B, xv, c), q);
+        kb_sub_mean<<<tgrid(B, kb_sub_mean, B->ntab0), TB, 0, st>>>(B->tab0, B->ntab0, B->dlev_s, B->ctl, mode, vc(B, xv, c), q);
         BPOST(B);
     }
     return 0;
@@ -1405,88 +1505,167 @@ void set_coarse_ops(fhd_batch* B, const double* eta, double theta) {
 }
 
 // batched GMRES (gmres.f90:32-491) on vectors b (V_B) and x (V_X) with the
-// per-box absolute tolerances in B->dabs; returns the worst status
-template <typename T>
-int gmres(fhd_batch* B, double theta) {
-    cudaStream_t st = B->stream;
-    const int nb = B->nbox, m = B->m;
-    const int cb = (nb + 127) / 128;
-    const double wp2 = B->p.p_norm_weight * B->p.p_norm_weight;
+// per-box absolute tolerances in B->dabs.  Three fixed launch sequences:
+//   init  -- control reset, |M^-1 b| and |b|, x = 0 where b is below the
+//            absolute tolerance;
+//   outer -- b - A x, its preconditioned norm, the stopping tests, and the
+//            number of boxes still running copied to pinned host memory;
+//   inner -- V_0 = r/|r|, the m Arnoldi slots (masked per box), the update
+//            of x.
+// Each is captured once as a CUDA graph (per theta: it is a kernel argument)
+// and replayed; the host reads the live count once per cycle.
+GParams gparams(const fhd_batch* B) {
     GParams P;
     P.rel_tol = B->p.gmres_rel_tol;
     P.wp = B->p.p_norm_weight;
-    P.m = m;
+    P.m = B->m;
     P.max_iter = B->p.gmres_max_iter;
     P.min_iter = B->p.gmres_min_iter;
     P.max_outer = B->p.gmres_max_outer;
-    kb_ctl_reset<<<cb, 128, 0, st>>>(nb, B->ctl, B->deta, B->dabs);
+    return P;
+}
+
+template <typename T>
+int gmres_init(fhd_batch* B, double theta) {
+    cudaStream_t st = B->stream;
+    const int nb = B->nbox, n0 = B->ntab0;
+    const double wp2 = B->p.p_norm_weight * B->p.p_norm_weight;
+    kb_ctl_reset<<<(nb * 32 + 255) / 256, 256, 0, st>>>(nb, B->ctl, B->deta, B->dabs);
     BPOST(B);
     int rc;
-    // |M^-1 b|, |b|
     if ((rc = precon<T>(B, V_B, V_TMP, M_ALL, theta))) return rc;
-    kb_dot<<<B->ntab0, TB, 0, st>>>(B->tab0, B->dlev_s, B->ctl, M_ALL, vp(B, V_TMP), vp(B, V_TMP), wp2, B->part);
+    kb_dot<<<tgrid(B, kb_dot, n0), TB, 0, st>>>(B->tab0, n0, B->dlev_s, B->ctl, M_ALL, vp(B, V_TMP), vp(B, V_TMP),
+                                               wp2, B->part);
     BPOST(B);
     if ((rc = seg(B, M_ALL, 0))) return rc;
-    kb_dot<<<B->ntab0, TB, 0, st>>>(B->tab0, B->dlev_s, B->ctl, M_ALL, vp(B, V_B), vp(B, V_B), wp2, B->part);
+    kb_dot<<<tgrid(B, kb_dot, n0), TB, 0, st>>>(B->tab0, n0, B->dlev_s, B->ctl, M_ALL, vp(B, V_B), vp(B, V_B), wp2,
+                                               B->part);
     BPOST(B);
     if ((rc = seg(B, M_ALL, 1))) return rc;
-    kb_ctl_init<<<cb, 128, 0, st>>>(nb, B->ctl);
+    kb_ctl_init<<<(nb + 127) / 128, 128, 0, st>>>(nb, B->ctl);
     BPOST(B);
-    kb_zero_x<<<B->ntab0, TB, 0, st>>>(B->tab0, B->dlev_s, B->ctl, vp(B, V_X));
+    kb_zero_x<<<tgrid(B, kb_zero_x, n0), TB, 0, st>>>(B->tab0, n0, B->dlev_s, B->ctl, vp(B, V_X));
     BPOST(B);
-    const i64 vstride = (i64)3 * B->N0;
-    for (int cycle = 0; cycle <= B->p.gmres_max_outer + 1; cycle++) {
-        // tmp = b - A x, r = M^-1 tmp, the stopping tests
-        kb_stokes_apply<<<B->ntab0, TB, 0, st>>>(B->tab0, B->dlev_s, B->ctl, M_LIVE, vp(B, V_X), vp(B, V_B),
-                                                 vp(B, V_TMP), 1, B->ones64, theta);
+    return 0;
+}
+
+template <typename T>
+int gmres_outer(fhd_batch* B, double theta) {
+    cudaStream_t st = B->stream;
+    const int nb = B->nbox, n0 = B->ntab0, cb = (nb + 127) / 128;
+    const double wp2 = B->p.p_norm_weight * B->p.p_norm_weight;
+    int rc;
+    // tmp = b - A x, r = M^-1 tmp, the stopping tests
+    kb_stokes_apply<<<tgrid(B, kb_stokes_apply, n0), TB, 0, st>>>(B->tab0, n0, B->dlev_s, B->ctl, M_LIVE,
+                                                                   vp(B, V_X), vp(B, V_B), vp(B, V_TMP), 1,
+                                                                   B->ones64, theta);
+    BPOST(B);
+    kb_dot<<<tgrid(B, kb_dot, n0), TB, 0, st>>>(B->tab0, n0, B->dlev_s, B->ctl, M_LIVE, vp(B, V_TMP), vp(B, V_TMP),
+                                               wp2, B->part);
+    BPOST(B);
+    if ((rc = seg(B, M_LIVE, 0))) return rc;
+    if ((rc = precon<T>(B, V_TMP, V_R, M_LIVE, theta))) return rc;
+    kb_dot<<<tgrid(B, kb_dot, n0), TB, 0, st>>>(B->tab0, n0, B->dlev_s, B->ctl, M_LIVE, vp(B, V_R), vp(B, V_R), wp2,
+                                               B->part);
+    BPOST(B);
+    if ((rc = seg(B, M_LIVE, 1))) return rc;
+    kb_ctl_outer<<<cb, 128, 0, st>>>(nb, B->ctl, gparams(B));
+    BPOST(B);
+    // boxes still running
+    if (cudaMemsetAsync(B->dlive, 0, sizeof(int), st) != cudaSuccess) return FHD_ERR_CUDA;
+    kb_count_live<<<cb, 128, 0, st>>>(nb, B->ctl, B->dlive);
+    BPOST(B);
+    if (cudaMemcpyAsync(B->hlive, B->dlive, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess)
+        return FHD_ERR_CUDA;
+    return 0;
+}
+
+template <typename T>
+int gmres_inner(fhd_batch* B, double theta) {
+    cudaStream_t st = B->stream;
+    const int nb = B->nbox, m = B->m, n0 = B->ntab0, cb = (nb + 127) / 128;
+    const double wp2 = B->p.p_norm_weight * B->p.p_norm_weight;
+    const GParams P = gparams(B);
+    int rc;
+    // V_0 = r / |r|
+    kb_scale<<<tgrid(B, kb_scale, n0), TB, 0, st>>>(B->tab0, n0, B->dlev_s, B->ctl, vp(B, V_V0), vp(B, V_R), -1);
+    BPOST(B);
+    for (int i = 1; i <= m; i++) {
+        kb_stokes_apply<<<tgrid(B, kb_stokes_apply, n0), TB, 0, st>>>(B->tab0, n0, B->dlev_s, B->ctl, M_INNER,
+                                                                       vp(B, V_V0 + i - 1), vp(B, V_V0 + i - 1),
+                                                                       vp(B, V_TMP), 0, B->ones64, theta);
         BPOST(B);
-        kb_dot<<<B->ntab0, TB, 0, st>>>(B->tab0, B->dlev_s, B->ctl, M_LIVE, vp(B, V_TMP), vp(B, V_TMP), wp2,
-                                        B->part);
-        BPOST(B);
-        if ((rc = seg(B, M_LIVE, 0))) return rc;
-        if ((rc = precon<T>(B, V_TMP, V_R, M_LIVE, theta))) return rc;
-        kb_dot<<<B->ntab0, TB, 0, st>>>(B->tab0, B->dlev_s, B->ctl, M_LIVE, vp(B, V_R), vp(B, V_R), wp2, B->part);
-        BPOST(B);
-        if ((rc = seg(B, M_LIVE, 1))) return rc;
-        kb_ctl_outer<<<cb, 128, 0, st>>>(nb, B->ctl, P);
-        BPOST(B);
-        // all boxes stopped?
-        if (cudaMemsetAsync(B->dlive, 0, sizeof(int), st) != cudaSuccess) return FHD_ERR_CUDA;
-        kb_count_live<<<cb, 128, 0, st>>>(nb, B->ctl, B->dlive);
-        BPOST(B);
-        if (cudaMemcpyAsync(B->hlive, B->dlive, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
-            cudaStreamSynchronize(st) != cudaSuccess)
-            return FHD_ERR_CUDA;
-        if (*B->hlive == 0) break;
-        // V_0 = r / |r|
-        kb_scale<<<B->ntab0, TB, 0, st>>>(B->tab0, B->dlev_s, B->ctl, vp(B, V_V0), vp(B, V_R), -1);
-        BPOST(B);
-        for (int i = 1; i <= m; i++) {
-            kb_stokes_apply<<<B->ntab0, TB, 0, st>>>(B->tab0, B->dlev_s, B->ctl, M_INNER, vp(B, V_V0 + i - 1),
-                                                     vp(B, V_V0 + i - 1), vp(B, V_TMP), 0, B->ones64, theta);
+        if ((rc = precon<T>(B, V_TMP, V_W, M_INNER, theta))) return rc;
+        for (int k = 1; k <= i; k++) {
+            kb_mgs<<<tgrid(B, kb_mgs, n0), TB, 0, st>>>(B->tab0, n0, B->dlev_s, B->ctl, vp(B, V_W),
+                                                       k > 1 ? vp(B, V_V0 + k - 2) : nullptr, k - 1,
+                                                       vp(B, V_V0 + k - 1), wp2, B->part);
             BPOST(B);
-            if ((rc = precon<T>(B, V_TMP, V_W, M_INNER, theta))) return rc;
-            for (int k = 1; k <= i; k++) {
-                kb_mgs<<<B->ntab0, TB, 0, st>>>(B->tab0, B->dlev_s, B->ctl, vp(B, V_W),
-                                                k > 1 ? vp(B, V_V0 + k - 2) : nullptr, k - 1, vp(B, V_V0 + k - 1),
-                                                wp2, B->part);
-                BPOST(B);
-                if ((rc = seg(B, M_INNER, 5 + k))) return rc;
-            }
-            kb_mgs<<<B->ntab0, TB, 0, st>>>(B->tab0, B->dlev_s, B->ctl, vp(B, V_W), vp(B, V_V0 + i - 1), i, nullptr,
-                                            wp2, B->part);
-            BPOST(B);
-            if ((rc = seg(B, M_INNER, 5 + i + 1))) return rc;
-            kb_scale<<<B->ntab0, TB, 0, st>>>(B->tab0, B->dlev_s, B->ctl, vp(B, V_V0 + i), vp(B, V_W), i + 1);
-            BPOST(B);
-            kb_ctl_inner<<<cb, 128, 0, st>>>(nb, B->ctl, i, P);
-            BPOST(B);
+            if ((rc = seg(B, M_INNER, 5 + k))) return rc;
         }
-        kb_update_sol<<<B->ntab0, TB, 0, st>>>(B->tab0, B->dlev_s, B->ctl, vp(B, V_X), vc(B, V_V0, 0), vstride,
-                                               B->N0);
+        kb_mgs<<<tgrid(B, kb_mgs, n0), TB, 0, st>>>(B->tab0, n0, B->dlev_s, B->ctl, vp(B, V_W), vp(B, V_V0 + i - 1),
+                                                   i, nullptr, wp2, B->part);
         BPOST(B);
-        kb_ctl_clear_pend<<<cb, 128, 0, st>>>(nb, B->ctl);
+        if ((rc = seg(B, M_INNER, 5 + i + 1))) return rc;
+        kb_scale<<<tgrid(B, kb_scale, n0), TB, 0, st>>>(B->tab0, n0, B->dlev_s, B->ctl, vp(B, V_V0 + i), vp(B, V_W),
+                                                       i + 1);
         BPOST(B);
+        kb_ctl_inner<<<cb, 128, 0, st>>>(nb, B->ctl, i, P);
+        BPOST(B);
+    }
+    kb_update_sol<<<tgrid(B, kb_update_sol, n0), TB, 0, st>>>(B->tab0, n0, B->dlev_s, B->ctl, vp(B, V_X),
+                                                               vc(B, V_V0, 0), (i64)3 * B->N0, B->N0);
+    BPOST(B);
+    kb_ctl_clear_pend<<<cb, 128, 0, st>>>(nb, B->ctl);
+    BPOST(B);
+    return 0;
+}
+
+// capture body() on the batch's stream as graph `which`; its kernel count is
+// added to the launch counter at every replay instead
+template <class F>
+int capture(fhd_batch* B, int which, F body) {
+    const long long n_before = B->launches;
+    if (cudaStreamBeginCapture(B->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return FHD_ERR_CUDA;
+    const int rc = body();
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(B->stream, &g);
+    B->gn[which] = B->launches - n_before;
+    B->launches = n_before;
+    if (rc || e != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        set_last_error(std::string("batched graph capture: ") + cudaGetErrorString(e));
+        return rc ? rc : FHD_ERR_CUDA;
+    }
+    if (B->gx[which]) cudaGraphExecDestroy(B->gx[which]);
+    B->gx[which] = nullptr;
+    const cudaError_t ei = cudaGraphInstantiate(&B->gx[which], g, 0);
+    cudaGraphDestroy(g);
+    return ei == cudaSuccess ? 0 : FHD_ERR_CUDA;
+}
+
+int replay(fhd_batch* B, int which) {
+    B->launches += B->gn[which];
+    return cudaGraphLaunch(B->gx[which], B->stream) == cudaSuccess ? 0 : FHD_ERR_CUDA;
+}
+
+template <typename T>
+int gmres(fhd_batch* B, double theta) {
+    int rc;
+    if (!B->g_ok || B->g_theta != theta) {
+        B->g_ok = 0;
+        if ((rc = capture(B, 0, [&] { return gmres_init<T>(B, theta); }))) return rc;
+        if ((rc = capture(B, 1, [&] { return gmres_outer<T>(B, theta); }))) return rc;
+        if ((rc = capture(B, 2, [&] { return gmres_inner<T>(B, theta); }))) return rc;
+        B->g_ok = 1;
+        B->g_theta = theta;
+    }
+    if ((rc = replay(B, 0))) return rc;
+    for (int cycle = 0; cycle <= B->p.gmres_max_outer + 1; cycle++) {
+        if ((rc = replay(B, 1))) return rc;
+        if (cudaStreamSynchronize(B->stream) != cudaSuccess) return FHD_ERR_CUDA;
+        if (*B->hlive == 0) break;
+        if ((rc = replay(B, 2))) return rc;
     }
     return 0;
 }
@@ -1577,6 +1756,8 @@ int fhd_batch_create(int nboxes, const int* n_cells, double dx, const fhd_gmres_
 int fhd_batch_destroy(fhd_batch* B) {
     if (!B) return FHD_ERR_BAD_ARG;
     if (B->stream) cudaStreamSynchronize(B->stream);
+    for (cudaGraphExec_t& g : B->gx)
+        if (g) cudaGraphExecDestroy(g);
     for (void* p : B->allocs) cudaFree(p);
     if (B->hlive) cudaFreeHost(B->hlive);
     if (B->stream) cudaStreamDestroy(B->stream);
@@ -1637,7 +1818,7 @@ int fhd_batch_overdamped(fhd_batch* B, double* const umac[2], double* pi, const 
         // right-hand side reads them
         std::vector<double> a0(nb, B->p.gmres_abs_tol);
         FHD_CUDA_TRY(cudaMemcpyAsync(B->dabs, a0.data(), sizeof(double) * nb, cudaMemcpyHostToDevice, st));
-        kb_ctl_reset<<<(nb + 127) / 128, 128, 0, st>>>(nb, B->ctl, B->deta, B->dabs);
+        kb_ctl_reset<<<(nb * 32 + 255) / 256, 256, 0, st>>>(nb, B->ctl, B->deta, B->dabs);
         if (int r0 = post(B)) return r0;
     }
     FHD_CUDA_TRY(cudaStreamSynchronize(st));
@@ -1664,10 +1845,10 @@ int fhd_batch_overdamped(fhd_batch* B, double* const umac[2], double* pi, const 
             N.w[1] = stage == 0 ? 0.0 : 1.0 / std::sqrt(2.0);
             N.var_fac = 2.0 / (B->dx * B->dx * h);  // variance_coef_mom 1, dV = dx^2 (unit depth)
             if (B->prec == FHD_PREC_MIXED)
-                kb_step_rhs<float><<<B->ntab0, TB, 0, st>>>(B->tab0, B->dlev_s, B->ctl, d_s, pi, vp(B, V_B),
+                kb_step_rhs<float><<<tgrid(B, kb_step_rhs<float>, B->ntab0), TB, 0, st>>>(B->tab0, B->ntab0, B->dlev_s, B->ctl, d_s, pi, vp(B, V_B),
                                                             vc(B, V_B, 2), B->ones64, B->dkT, N);
             else
-                kb_step_rhs<double><<<B->ntab0, TB, 0, st>>>(B->tab0, B->dlev_s, B->ctl, d_s, pi, vp(B, V_B),
+                kb_step_rhs<double><<<tgrid(B, kb_step_rhs<double>, B->ntab0), TB, 0, st>>>(B->tab0, B->ntab0, B->dlev_s, B->ctl, d_s, pi, vp(B, V_B),
                                                              vc(B, V_B, 2), B->ones64, B->dkT, N);
             if ((rc = post(B))) break;
             for (int c = 0; c < 3; c++)
@@ -1688,7 +1869,7 @@ int fhd_batch_overdamped(fhd_batch* B, double* const umac[2], double* pi, const 
                 rc = r2;
                 break;
             }
-            kb_axpy3<<<B->ntab0, TB, 0, st>>>(B->tab0, B->dlev_s, d_s, vp(B, V_X));
+            kb_axpy3<<<tgrid(B, kb_axpy3, B->ntab0), TB, 0, st>>>(B->tab0, B->ntab0, B->dlev_s, d_s, vp(B, V_X));
             if ((rc = post(B))) break;
             int w = 0;
             if ((rc = read_stats(B, nullptr, &w))) break;
