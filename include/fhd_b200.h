@@ -79,7 +79,7 @@ typedef struct fhd_gmres_params {
     double gmres_rel_tol, gmres_abs_tol;
     int    gmres_verbose, gmres_max_outer, gmres_max_inner;
     int    gmres_max_iter, gmres_min_iter;
-    int    gmres_spatial_order;    /* only 2 is supported */
+    int    gmres_spatial_order;    /* 2, or 4 with visc_type 1 (apply_matrix only) */
 } fhd_gmres_params;
 
 /* Fills the defaults of probin_gmres_init (probin_gmres.f90:122-163). */

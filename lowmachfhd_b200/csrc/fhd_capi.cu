@@ -285,9 +285,11 @@ int fhd_gmres(fhd_ctx* ctx, const fhd_multifab* b_u, const fhd_multifab* b_p, co
         return FHD_ERR_BAD_ARG;
     const int dim = ctx->dim;
     int rc;
+    // x needs gmres_spatial_order / 2 ghost cells (apply_matrix.f90:54-67)
+    const int xg = ctx->p.gmres_spatial_order == 4 ? 2 : 1;
     for (int c = 0; c < dim; c++)
-        if ((rc = check_mf(ctx, &x_u[c], 1)) || (rc = check_mf(ctx, &b_u[c], 0))) return rc;
-    if ((rc = check_mf(ctx, x_p, 1)) || (rc = check_mf(ctx, b_p, 0))) return rc;
+        if ((rc = check_mf(ctx, &x_u[c], xg)) || (rc = check_mf(ctx, &b_u[c], 0))) return rc;
+    if ((rc = check_mf(ctx, x_p, xg)) || (rc = check_mf(ctx, b_p, 0))) return rc;
     HostPath* H;
     if ((rc = host_arrays(ctx, H))) return rc;
     Operands o;
@@ -340,9 +342,11 @@ int fhd_apply_matrix(fhd_ctx* ctx, const fhd_multifab* b_u, const fhd_multifab* 
     if (!ctx || !b_u || !b_p || !x_u || !x_p || !alpha_fc || !beta || !beta_ed || !gamma) return FHD_ERR_BAD_ARG;
     const int dim = ctx->dim;
     int rc;
+    // x needs gmres_spatial_order / 2 ghost cells (apply_matrix.f90:54-67)
+    const int xg = ctx->p.gmres_spatial_order == 4 ? 2 : 1;
     for (int c = 0; c < dim; c++)
-        if ((rc = check_mf(ctx, &x_u[c], 1)) || (rc = check_mf(ctx, &b_u[c], 0))) return rc;
-    if ((rc = check_mf(ctx, x_p, 1)) || (rc = check_mf(ctx, b_p, 0))) return rc;
+        if ((rc = check_mf(ctx, &x_u[c], xg)) || (rc = check_mf(ctx, &b_u[c], 0))) return rc;
+    if ((rc = check_mf(ctx, x_p, xg)) || (rc = check_mf(ctx, b_p, 0))) return rc;
     HostPath* H;
     if ((rc = host_arrays(ctx, H))) return rc;
     Operands o;

@@ -1610,6 +1610,16 @@ int stokes_apply(fhd_ctx* ctx, CSVec<double> x, CSVec<double> rhs, SVec<double> 
     A.gamma = ctx->gamma;
     A.q = 1.0 / (ctx->dx * ctx->dx);
     int rc = 0;
+    if (ctx->p.gmres_spatial_order == 4) {
+        const double t1 = 1.0 / (12.0 * ctx->dx), t2 = 1.0 / (12.0 * ctx->dx * ctx->dx);
+        if (ctx->dim == 2)
+            k_stokes_apply4<2><<<cell_grid(ctx->g0), cell_block(), 0, ctx->stream>>>(ctx->g0, A, x, rhs, out, mode,
+                                                                                   1.0 / ctx->dx, t1, t2);
+        else
+            k_stokes_apply4<3><<<cell_grid(ctx->g0), cell_block(), 0, ctx->stream>>>(ctx->g0, A, x, rhs, out, mode,
+                                                                                   1.0 / ctx->dx, t1, t2);
+        return post(ctx);
+    }
     with_dim_visc(ctx->dim, ctx->visc, [&](auto D, auto V) {
         constexpr int DIM = decltype(D)::value, VISC = decltype(V)::value;
         k_stokes_apply<DIM, VISC><<<cell_grid(ctx->g0), cell_block(), 0, ctx->stream>>>(ctx->g0, A, x, rhs, out, mode,
@@ -2112,7 +2122,14 @@ static int ctx_create(int dim, const int n_cells[3], const int max_grid_size[3],
     c->prec = precision_mode == FHD_PREC_MIXED ? FHD_PREC_MIXED : FHD_PREC_FP64;
     if (params) c->p = *params;
     else fhd_gmres_params_default(&c->p);
-    if (c->p.gmres_spatial_order != 2 || c->p.gmres_max_inner < 1 || c->p.gmres_max_inner > 60) {
+    if (c->p.gmres_max_inner < 1 || c->p.gmres_max_inner > 60) {
+        delete c;
+        return FHD_ERR_UNSUPPORTED;
+    }
+    // gmres_spatial_order 4: stag_applyop_4o exists for visc_type 1 only
+    // (stag_applyop.f90:1355, 1506)
+    if (c->p.gmres_spatial_order != 2 && !(c->p.gmres_spatial_order == 4 && visc_type == 1)) {
+        set_last_error("gmres_spatial_order 4 supports visc_type 1 only; other orders are not defined");
         delete c;
         return FHD_ERR_UNSUPPORTED;
     }

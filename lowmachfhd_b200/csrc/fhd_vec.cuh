@@ -233,6 +233,52 @@ static __global__ void __launch_bounds__(256) k_stokes_apply(Grid g, StagOp<doub
     out.c[DIM][f] = mode ? ld(rhs.c[DIM], f) - bp : bp;
 }
 
+// the same with gmres_spatial_order = 4 (apply_matrix.f90:124-135): the
+// visc_type 1 operator of stag_applyop_4o_2d/_3d (stag_applyop.f90:1262-1510,
+// per direction +16 phi(+-1) - phi(+-2) over 12 dx^2, diagonal 30 dim over
+// 12 dx^2) and the gradient of compute_grad_4o (div_and_grad.f90:804-880,
+// (-p(+1) + 15 p - 15 p(-1) + p(-2)) / 12 dx); the divergence stays second
+// order.  Terms summed in the order of those loops.  The constant viscosity
+// is the first cell's (stag_applyop.f90:1306); t2 = 1/(12 dx^2),
+// t1 = 1/(12 dx).
+template <int DIM>
+static __global__ void __launch_bounds__(256) k_stokes_apply4(Grid g, StagOp<double> A, CSVec<double> x,
+                                                              CSVec<double> rhs, SVec<double> out, int mode,
+                                                              double dxinv, double t1, double t2) {
+    Cell P;
+    if (!cell_of_thread(g, P)) return;
+    const double b = ld(A.beta, 0);
+    const double* p = x.c[DIM];
+    const i64 f = P.id(0, 0, 0);
+    const double cdiag = DIM == 2 ? 60.0 : 90.0;
+    double div = 0.0;
+#pragma unroll
+    for (int c = 0; c < DIM; c++) {
+        const double* u = x.c[c];
+        double s = 0.0;
+#pragma unroll
+        for (int d = 0; d < DIM; d++) {
+            const int e0 = d == 0, e1 = d == 1, e2 = d == 2;
+            const double t = 16.0 * ld(u, P.id(e0, e1, e2));
+            s = d == 0 ? t : s + t;
+            s = s + 16.0 * ld(u, P.id(-e0, -e1, -e2));
+            s = s - 1.0 * ld(u, P.id(2 * e0, 2 * e1, 2 * e2));
+            s = s - 1.0 * ld(u, P.id(-2 * e0, -2 * e1, -2 * e2));
+        }
+        const double a = A.alpha_scale * ld(A.alpha[c], f);
+        double L = (a + cdiag * b * t2) * ld(u, f) - s * b * t2;
+        const int e0 = c == 0, e1 = c == 1, e2 = c == 2;
+        const double gp = (-ld(p, P.id(e0, e1, e2)) + 15.0 * ld(p, f) - 15.0 * ld(p, P.id(-e0, -e1, -e2)) +
+                           ld(p, P.id(-2 * e0, -2 * e1, -2 * e2))) *
+                          t1;
+        L = L + gp;
+        out.c[c][f] = mode ? ld(rhs.c[c], f) - L : L;
+        div += (ld(u, P.id(e0, e1, e2)) - ld(u, f)) * dxinv;
+    }
+    const double bp = div * -1.0;
+    out.c[DIM][f] = mode ? ld(rhs.c[DIM], f) - bp : bp;
+}
+
 // mac_rhs = D x_u + b_p  (apply_precon.f90:118-123)
 template <typename T, int DIM>
 static __global__ void __launch_bounds__(256) k_div_plus(Grid g, const T* u0, const T* u1, const T* u2, const double* bp,

@@ -177,12 +177,15 @@ def macproject(dim, n, dx, params, alphainv, rhs):
     return phi
 
 
-def apply_matrix(pb: Problem, theta, x_u, x_p):
+def apply_matrix(pb: Problem, theta, x_u, x_p, order=2):
+    """apply_matrix.f90:24-157; order = gmres_spatial_order (2, or 4 with
+    visc_type 1)"""
     b_u = [np.zeros(pb.nc) for _ in range(pb.dim)]
     b_p = np.zeros(pb.nc)
-    lib().or_apply_matrix(pb.dim, _n3(pb.n), C.c_double(pb.dx), pb.visc_type, _pp(b_u), _p(b_p),
-                          _pp(x_u), _p(x_p), _pp(pb.alpha_fc), _p(pb.beta), _pp(pb.beta_ed),
-                          _p(pb.gamma), C.c_double(theta))
+    rc = lib().or_apply_matrix_order(pb.dim, _n3(pb.n), C.c_double(pb.dx), pb.visc_type, _pp(b_u), _p(b_p),
+                                     _pp(x_u), _p(x_p), _pp(pb.alpha_fc), _p(pb.beta), _pp(pb.beta_ed),
+                                     _p(pb.gamma), C.c_double(theta), int(order))
+    assert rc == 0, rc
     return b_u, b_p
 
 
@@ -244,9 +247,9 @@ def advance_inertial(dim, n, dx, visc_type, params, sp, dt, umac, rho, pi, eta, 
     return rc, umac, rho, pi, st
 
 
-def accuracy_test(dim, n, prob_coeff, prob_sol, visc_type):
+def accuracy_test(dim, n, prob_coeff, prob_sol, visc_type, order=2):
     err = np.zeros(4)
-    rc = lib().or_accuracy_test(dim, n, prob_coeff, prob_sol, visc_type, _p(err))
+    rc = lib().or_accuracy_test_order(dim, n, prob_coeff, prob_sol, visc_type, int(order), _p(err))
     assert rc == 0
     return err[: dim + 1]
 

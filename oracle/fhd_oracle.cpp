@@ -694,10 +694,50 @@ double stag_l2(const Geo& g, const double* const u[]) {
     return std::sqrt(s);
 }
 
+// gmres_spatial_order = 4 (apply_matrix.f90:54-67, 124-135): the viscous
+// operator of stag_applyop_4o_2d/_3d (stag_applyop.f90:1262-1510, visc_type
+// 1 only) and the gradient of compute_grad_4o_2d/_3d (div_and_grad.f90:
+// 804-880); the divergence stays second order (apply_matrix.f90:143-147).
+// Summation order as in those loops: for each direction x, y, z the terms
+// +16 phi(+1), +16 phi(-1), -1 phi(+2), -1 phi(-2).
+static void apply_matrix_4o(const Geo& g, double* const b_u[], const double* const x_u[], const double* x_p,
+                            const Vec alpha[], double b) {
+    const int dim = g.dim;
+    const double t2 = 1.0 / (12.0 * g.dx * g.dx);
+    const double t1 = 1.0 / (12.0 * g.dx);
+    const double cdiag = dim == 2 ? 60.0 : 90.0;
+    for (int c = 0; c < dim; c++) {
+        const double* u = x_u[c];
+        double* out = b_u[c];
+        forall(g, [&](int i, int j, int k) {
+            const long f = g.id(i, j, k);
+            double s = 0.0;
+            for (int d = 0; d < dim; d++) {
+                const int e0 = d == 0, e1 = d == 1, e2 = d == 2;
+                const double t = 16.0 * u[g.id(i + e0, j + e1, k + e2)];
+                s = d == 0 ? t : s + t;
+                s = s + 16.0 * u[g.id(i - e0, j - e1, k - e2)];
+                s = s - 1.0 * u[g.id(i + 2 * e0, j + 2 * e1, k + 2 * e2)];
+                s = s - 1.0 * u[g.id(i - 2 * e0, j - 2 * e1, k - 2 * e2)];
+            }
+            const double L = (alpha[c][f] + cdiag * b * t2) * u[f] - s * b * t2;
+            // compute_grad_4o: (-p(+1) + 15 p(0) - 15 p(-1) + p(-2)) / (12 dx)
+            const int e0 = c == 0, e1 = c == 1, e2 = c == 2;
+            const double gp = (-x_p[g.id(i + e0, j + e1, k + e2)] + 15.0 * x_p[f] -
+                               15.0 * x_p[g.id(i - e0, j - e1, k - e2)] +
+                               x_p[g.id(i - 2 * e0, j - 2 * e1, k - 2 * e2)]) *
+                              t1;
+            out[f] = L + gp;
+        });
+    }
+}
+
 int apply_matrix_impl(const Geo& g, int visc, double* const b_u[], double* b_p, const double* const x_u[],
                       const double* x_p, const double* const alpha_fc[], const double* beta,
-                      const double* const beta_ed[], const double* gamma, double theta) {
+                      const double* const beta_ed[], const double* gamma, double theta, int order) {
     const int dim = g.dim;
+    // stag_applyop_4o supports visc_type 1 only (stag_applyop.f90:1355, 1506)
+    if (order != 2 && (order != 4 || visc != 1)) return -5;
     Vec alpha[3], bed[3];
     Vec vb(beta, beta + g.nc), vg(gamma, gamma + g.nc);
     for (int c = 0; c < dim; c++) {
@@ -705,18 +745,22 @@ int apply_matrix_impl(const Geo& g, int visc, double* const b_u[], double* b_p, 
         for (long f = 0; f < g.nc; f++) alpha[c][f] = alpha_fc[c][f] * theta;
     }
     for (int e = 0; e < n_edge(dim); e++) bed[e].assign(beta_ed[e], beta_ed[e] + g.nc);
-    const double* ph[3] = {x_u[0], x_u[1], dim == 3 ? x_u[2] : nullptr};
-    for (int c = 0; c < dim; c++) {
-        double* out = b_u[c];
-        forall(g, [&](int i, int j, int k) {
-            out[g.id(i, j, k)] = lface(g, visc, alpha, vb, vg, bed, ph, c, i, j, k, nullptr);
-        });
+    if (order == 4) {
+        apply_matrix_4o(g, b_u, x_u, x_p, alpha, beta[0]);
+    } else {
+        const double* ph[3] = {x_u[0], x_u[1], dim == 3 ? x_u[2] : nullptr};
+        for (int c = 0; c < dim; c++) {
+            double* out = b_u[c];
+            forall(g, [&](int i, int j, int k) {
+                out[g.id(i, j, k)] = lface(g, visc, alpha, vb, vg, bed, ph, c, i, j, k, nullptr);
+            });
+        }
+        std::vector<Vec> gp(dim, Vec(g.nc));
+        double* gpp[3] = {gp[0].data(), gp[1].data(), dim == 3 ? gp[2].data() : nullptr};
+        c_grad(g, x_p, gpp);
+        for (int c = 0; c < dim; c++)
+            for (long f = 0; f < g.nc; f++) b_u[c][f] = b_u[c][f] + gp[c][f];
     }
-    std::vector<Vec> gp(dim, Vec(g.nc));
-    double* gpp[3] = {gp[0].data(), gp[1].data(), dim == 3 ? gp[2].data() : nullptr};
-    c_grad(g, x_p, gpp);
-    for (int c = 0; c < dim; c++)
-        for (long f = 0; f < g.nc; f++) b_u[c][f] = b_u[c][f] + gp[c][f];
     c_div(g, x_u, b_p, false);
     for (long f = 0; f < g.nc; f++) b_p[f] = b_p[f] * -1.0;
     return 0;
@@ -981,7 +1025,7 @@ int gmres_impl(const Geo& g, int visc, const fhd_gmres_params* p, const double* 
     };
     auto matrix = [&](double* const out_u[], double* out_p, const double* const in_u[], const double* in_p) {
         return apply_matrix_impl(g, visc, out_u, out_p, in_u, in_p, alpha_fc, beta.data(), bedp, gamma.data(),
-                                 theta);
+                                 theta, p->gmres_spatial_order);
     };
     auto snorm = [&](const double* const u[], const double* pp) {
         double nu = stag_l2(g, u);
@@ -1727,7 +1771,16 @@ int or_apply_matrix(int dim, const int n[3], double dx, int visc_type, double* c
                     const double* const x_u[], const double* x_p, const double* const alpha_fc[],
                     const double* beta, const double* const beta_ed[], const double* gamma, double theta_alpha) {
     Geo g(dim, n, dx);
-    return apply_matrix_impl(g, visc_type, b_u, b_p, x_u, x_p, alpha_fc, beta, beta_ed, gamma, theta_alpha);
+    return apply_matrix_impl(g, visc_type, b_u, b_p, x_u, x_p, alpha_fc, beta, beta_ed, gamma, theta_alpha, 2);
+}
+
+int or_apply_matrix_order(int dim, const int n[3], double dx, int visc_type, double* const b_u[], double* b_p,
+                          const double* const x_u[], const double* x_p, const double* const alpha_fc[],
+                          const double* beta, const double* const beta_ed[], const double* gamma,
+                          double theta_alpha, int order) {
+    Geo g(dim, n, dx);
+    return apply_matrix_impl(g, visc_type, b_u, b_p, x_u, x_p, alpha_fc, beta, beta_ed, gamma, theta_alpha,
+                             order);
 }
 
 int or_apply_precon(int dim, const int n[3], double dx, int visc_type, const fhd_gmres_params* p,
@@ -2389,7 +2442,7 @@ struct Exact {
 };
 }  // namespace
 
-int or_accuracy_test(int dim, int n, int prob_coeff, int prob_sol, int visc_type, double* err) {
+int or_accuracy_test_order(int dim, int n, int prob_coeff, int prob_sol, int visc_type, int order, double* err) {
     int nn[3] = {n, n, dim == 3 ? n : 1};
     const double dx = 1.0 / n;
     Geo g(dim, nn, dx);
@@ -2422,7 +2475,9 @@ int or_accuracy_test(int dim, int n, int prob_coeff, int prob_sol, int visc_type
     double* bup[3] = {bu[0].data(), bu[1].data(), dim == 3 ? bu[2].data() : nullptr};
     const double* ap[3] = {alpha[0].data(), alpha[1].data(), dim == 3 ? alpha[2].data() : nullptr};
     const double* cbed[3] = {bedp[0], bedp[1], bedp[2]};
-    apply_matrix_impl(g, visc_type, bup, bp.data(), xup, xp.data(), ap, beta.data(), cbed, gamma.data(), 0.0);
+    if (int rc = apply_matrix_impl(g, visc_type, bup, bp.data(), xup, xp.data(), ap, beta.data(), cbed,
+                                   gamma.data(), 0.0, order))
+        return rc;
     for (int c = 0; c < dim; c++) {
         const Vec& F = fu[c];
         const Vec& B = bu[c];
@@ -2430,6 +2485,10 @@ int or_accuracy_test(int dim, int n, int prob_coeff, int prob_sol, int visc_type
     }
     err[dim] = reduce_max(g, [&](int i, int j, int k) { long f = g.id(i, j, k); return std::fabs(fpv[f] - bp[f]); });
     return 0;
+}
+
+int or_accuracy_test(int dim, int n, int prob_coeff, int prob_sol, int visc_type, double* err) {
+    return or_accuracy_test_order(dim, n, prob_coeff, prob_sol, visc_type, 2, err);
 }
 
 }  // extern "C"

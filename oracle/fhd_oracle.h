@@ -64,6 +64,15 @@ int or_apply_matrix(int dim, const int n[3], double dx, int visc_type,
                     const double* const beta_ed[], const double* gamma,
                     double theta_alpha);
 
+/* apply_matrix with gmres_spatial_order = order (2, or 4 with visc_type 1:
+ * stag_applyop_4o and compute_grad_4o); nonzero for an unsupported pair */
+int or_apply_matrix_order(int dim, const int n[3], double dx, int visc_type,
+                          double* const b_u[], double* b_p,
+                          const double* const x_u[], const double* x_p,
+                          const double* const alpha_fc[], const double* beta,
+                          const double* const beta_ed[], const double* gamma,
+                          double theta_alpha, int order);
+
 int or_apply_precon(int dim, const int n[3], double dx, int visc_type,
                     const fhd_gmres_params* p,
                     const double* const b_u[], const double* b_p,
@@ -180,6 +189,9 @@ void or_mixture_trace_local(const fhd_mixture_params* mp, double k_B, const doub
  * {1,31}. */
 int or_accuracy_test(int dim, int n, int prob_coeff, int prob_sol,
                      int visc_type, double* err);
+/* the same with apply_matrix of spatial order `order` (2 or 4) */
+int or_accuracy_test_order(int dim, int n, int prob_coeff, int prob_sol,
+                           int visc_type, int order, double* err);
 
 /* number of OpenMP threads the oracle uses */
 int or_num_threads(void);
