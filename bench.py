@@ -61,8 +61,9 @@ def parse():
     ap.add_argument("--only", choices=["mixed", "fp64"], default=None, help="run one precision only")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving and batched legs")
-    ap.add_argument("--probe", choices=["stagmg"], default=None,
-                    help="profiling probe: K stag_mg_solver calls (one V-cycle each) on one grid")
+    ap.add_argument("--probe", choices=["stagmg", "gmres", "stochm"], default=None,
+                    help="profiling probe on one single-fluid 3D grid: K stag_mg_solver calls (one V-cycle "
+                         "each), K GMRES solves (theta 20, 1e-8), or K stochastic_m_fluxdiv calls")
     ap.add_argument("--precision", choices=["mixed", "fp64"], default="fp64", help="precision of --probe")
     ap.add_argument("--tune", type=int, default=-1,
                     help="smoother autotuner mode of --probe (fhd_ctx_set_tune: -1 tune, 0 fixed rules, 2+k "
@@ -71,8 +72,9 @@ def parse():
 
 
 def run_probe(args):
-    """K staggered multigrid solves on a random right-hand side (a small,
-    self-contained workload for kernel captures)."""
+    """K staggered multigrid solves, GMRES solves or stochastic momentum
+    flux evaluations on random single-fluid data (small, self-contained
+    workloads for kernel captures)."""
     import torch
 
     import lowmachfhd_b200 as L
@@ -89,18 +91,43 @@ def run_probe(args):
     rhs = [torch.randn(nc, generator=g, **f64).to(dev) for _ in range(3)]
     phi = [torch.zeros(nc, device=dev, **f64) for _ in range(3)]
     zero = torch.zeros(nc, device=dev, **f64)
+    if args.probe == "gmres":
+        s.close()
+        s = L.StokesSolver(3, [n, n, n], 1.0, 1, params=L.default_params(gmres_rel_tol=REL_TOL),
+                           precision=args.precision)
+        s.set_tune(args.tune)
+        bp = torch.randn(nc, generator=g, **f64)
+        bp = (bp - bp.mean()).to(dev)
+        x_p = torch.zeros(nc, device=dev, **f64)
+
+        def call():
+            for c in range(3):
+                phi[c].zero_()
+            x_p.zero_()
+            s.gmres(rhs, bp, phi, x_p, alpha, one, [one, one, one], zero, 20.0)
+    elif args.probe == "stochm":
+        sp = L.StochParams(k_B=KT, variance_coef_mom=1.0, dV=DX ** 3, stoch_stress_form=1, filtering_width=0)
+        W_cc = [torch.randn(nc, generator=g, **f64).to(dev) for _ in range(3)]
+        W_ed = [torch.randn(nc, generator=g, **f64).to(dev) for _ in range(6)]
+
+        def call():
+            s.stochastic_m_fluxdiv(sp, phi, False, one, [one, one, one], one, [one, one, one], DT, [1.0],
+                                   W_cc, W_ed)
+    else:
+        def call():
+            s.stag_mg_solver(alpha, one, [one, one, one], zero, 20.0, phi, rhs)
     # the warm-up calls pick the smoother plans (autotuner); the NVTX range
     # "probe" holds only the measured calls, so that a profiler can be
     # restricted to them (ncu --nvtx --nvtx-include "probe/")
     for _ in range(args.warmup):
-        s.stag_mg_solver(alpha, one, [one, one, one], zero, 20.0, phi, rhs)
+        call()
     torch.cuda.synchronize()
     torch.cuda.nvtx.range_push("probe")
     for _ in range(args.steps):
-        s.stag_mg_solver(alpha, one, [one, one, one], zero, 20.0, phi, rhs)
+        call()
     torch.cuda.synchronize()
     torch.cuda.nvtx.range_pop()
-    print(json.dumps({"probe": "stagmg", "n": n, "precision": args.precision, "calls": args.warmup + args.steps,
+    print(json.dumps({"probe": args.probe, "n": n, "precision": args.precision, "calls": args.warmup + args.steps,
                       "launches": s.kernel_launches, "plan_level0": s.tune_info("stag", 0)}))
     s.close()
     return 0
