@@ -45,8 +45,9 @@ constexpr int RB_CHUNKS = 3;                // 16-byte copies per thread per pla
 // geometry of the row-tile smoother (fhd_rbx.cuh: rbx_geom)
 struct RBXGeom {
     int TY;       // tile rows (divides ny)
-    int KZ;       // planes of the longest z-run
-    int tiles_y, chunks;
+    int KZ;       // plane steps of the longest CTA stretch
+    int tiles_y;
+    int chunks;   // CTAs of the launch (k_stag_rbx: stretches of the work)
     int rows;     // TY + 4 staged unknown rows
     int crows;    // TY + 2 staged coefficient rows
     size_t smem;  // bytes of dynamic shared memory

@@ -35,6 +35,7 @@ constexpr int RBX_THREADS = 256;  // compute threads (the wide form: 512)
 constexpr int RBX_AHEAD = 3;
 constexpr int RBX_MAXNX = 256;
 constexpr long RBX_SPIN = 1L << 22;     // try_wait polls before a wait gives up
+constexpr int RBX_MINRUN = 4;           // shortest z-run of a (tile, component) item
 // a thread updates the cells of one x column on rows gr, gr + RG, ..: with
 // RG = RBX_THREADS / (nx / 2) its rows lie RBX_ROWSTEP elements apart for
 // every nx, at most RBX_MAXR of them per sweep
@@ -115,6 +116,19 @@ __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.
 // ---------------------------------------------------------------------
 // the kernel
 // ---------------------------------------------------------------------
+// Cut b of P over the work of `items` items of nz planes each, flattened
+// item by item: W * b / P, moved to the item's edge when it would leave a
+// run shorter than RBX_MINRUN planes.  The move is non-decreasing in the
+// cut, so the cuts stay ordered.  With P = items * c the cuts are the edges
+// of c equal z-runs per item.
+__host__ __device__ inline long rbx_cut(long items, int nz, long b, long P) {
+    const long W = items * nz;
+    long x = W * b / P;
+    const long k = x % nz;
+    if (k != 0 && k < RBX_MINRUN) x -= k;
+    else if (k != 0 && nz - k < RBX_MINRUN) x += nz - k;
+    return x;
+}
 struct RBXArgs {
     const float* src[3];
     float* dst[3];
@@ -123,9 +137,14 @@ struct RBXArgs {
     unsigned* err;
 };
 
+// One z-run of one (tile, component) item: planes k0 .. kend-1 of tile row
+// tile_y.  qb: stages this CTA has issued before the run (its earlier runs),
+// so that every mbarrier keeps counting its phases across runs; nstages
+// returns the run's stage count.  False when a staging wait timed out.
 template <int C, int AH, int NT>
-__device__ __forceinline__ void rbx_run(const Grid& g, const RBXGeom& G, const StagOp<float>& A0, const RBXArgs& R,
-                                        float omega, unsigned char* raw, int tile_y, int chunk) {
+__device__ __forceinline__ bool rbx_run(const Grid& g, const RBXGeom& G, const StagOp<float>& A0, const RBXArgs& R,
+                                        float omega, unsigned char* raw, int tile_y, int k0, int kend, int qb,
+                                        int& nstages) {
     // the constant viscosity, loaded once: every asm statement below clobbers
     // memory, which would make each sweep reload it from global memory
     StagOp<float> A = A0;
@@ -142,7 +161,6 @@ __device__ __forceinline__ void rbx_run(const Grid& g, const RBXGeom& G, const S
     const int tid = threadIdx.x;
     const i64 nxy = (i64)nx * ny;
     const int y0 = tile_y * TY;
-    const int k0 = (int)((long)chunk * nz / G.chunks), kend = (int)((long)(chunk + 1) * nz / G.chunks);
     unsigned long long* bar = reinterpret_cast<unsigned long long*>(raw);
     const int plane = rows * nx, cplane = crows * nx;
     float* cf = reinterpret_cast<float*>(raw + 64);  // [slot][0 alpha, 1 rhs][crows][nx]
@@ -162,7 +180,7 @@ __device__ __forceinline__ void rbx_run(const Grid& g, const RBXGeom& G, const S
     auto issue = [&](int q) {
         const int lane = tid - NT;
         const int j = q + k0 - 2;
-        const int s = q % NPH;
+        const int s = (qb + q) % NPH;
         if (lane == 0) mbar_expect_tx(&bar[s], (unsigned)(sizeof(float) * (plane + (j >= k0 ? 2 * cplane : 0))));
         __syncwarp();
         auto copy = [&](float* sdst, const float* gplane, int nrows, int ring) {
@@ -182,7 +200,9 @@ __device__ __forceinline__ void rbx_run(const Grid& g, const RBXGeom& G, const S
         }
     };
     // wait for stage q; false on time-out
-    auto wait_stage = [&](int q) { return mbar_wait_bounded(&bar[q % NPH], (unsigned)((q / NPH) & 1)); };
+    auto wait_stage = [&](int q) {
+        return mbar_wait_bounded(&bar[(qb + q) % NPH], (unsigned)(((qb + q) / NPH) & 1));
+    };
 
     const int hx = nx >> 1;           // cells of one colour per row
     const int RG = NT / hx;  // rows updated at once
@@ -254,7 +274,7 @@ __device__ __forceinline__ void rbx_run(const Grid& g, const RBXGeom& G, const S
     }
     using RRed = std::integral_constant<int, MR>;
     using RBlack = std::integral_constant<int, MR - 1>;
-    auto slot = [&](int p) { return pmod(p - (k0 - 2), NPH); };
+    auto slot = [&](int p) { return pmod(p - (k0 - 2) + qb, NPH); };
     auto ring = [](int v, int d, int n) { return v + d >= n ? v + d - n : v + d; };
     int sl, scl;
     bool ok = true;
@@ -285,7 +305,7 @@ __device__ __forceinline__ void rbx_run(const Grid& g, const RBXGeom& G, const S
                 issued = qn + 1;
             }
             if (tid == lead && k > k0) {
-                const float* sp = ph + pmod(k - 1 - (k0 - 2), NPH) * plane + 2 * nx;
+                const float* sp = ph + pmod(k - 1 - (k0 - 2) + qb, NPH) * plane + 2 * nx;
                 bulk_s2g(dst + (i64)(k - 1) * nxy + (i64)y0 * nx, sp, (unsigned)(sizeof(float) * TY * nx));
                 bulk_commit();
             }
@@ -304,12 +324,13 @@ __device__ __forceinline__ void rbx_run(const Grid& g, const RBXGeom& G, const S
     fence_proxy_async();
     if (__syncthreads_or(!ok)) goto fail;
     if (tid == lead) {
-        const float* sp = ph + pmod(kend - 1 - (k0 - 2), NPH) * plane + 2 * nx;
+        const float* sp = ph + pmod(kend - 1 - (k0 - 2) + qb, NPH) * plane + 2 * nx;
         bulk_s2g(dst + (i64)(kend - 1) * nxy + (i64)y0 * nx, sp, (unsigned)(sizeof(float) * TY * nx));
         bulk_commit();
         bulk_wait0();
     }
-    return;
+    nstages = qend + 1;
+    return true;
 fail:
     // a stage did not arrive in time: flag it, let the copies in flight
     // land (bounded) and leave
@@ -320,6 +341,7 @@ fail:
         // barriers were re-armed
         for (int q = issued > NPH ? issued - NPH : 0; q < issued; q++) wait_stage(q);
     }
+    return false;
 }
 
 // AH stages in flight beyond the one awaited: RBX_AHEAD with one CTA per SM,
@@ -332,10 +354,31 @@ __global__ void __launch_bounds__(NT + 32, AH == 1 ? 2 : 1) k_stag_rbx(Grid g, R
     if (threadIdx.x < 5 + AH) mbar_init(reinterpret_cast<unsigned long long*>(rbx_raw) + threadIdx.x, 1);
     if (threadIdx.x == 0) mbar_init_fence();
     __syncthreads();
-    const int tile_y = blockIdx.x, chunk = blockIdx.y;
-    if (blockIdx.z == 0) rbx_run<0, AH, NT>(g, G, A, R, omega, rbx_raw, tile_y, chunk);
-    else if (blockIdx.z == 1) rbx_run<1, AH, NT>(g, G, A, R, omega, rbx_raw, tile_y, chunk);
-    else rbx_run<2, AH, NT>(g, G, A, R, omega, rbx_raw, tile_y, chunk);
+    // The work is tiles_y * 3 items (tile row, component) of nz planes each,
+    // flattened item by item; CTA b takes the stretch between rbx_cut(b)
+    // and rbx_cut(b + 1), one z-run per item it touches.
+    const int nz = g.n[2];
+    const long items = (long)G.tiles_y * 3;
+    long s = rbx_cut(items, nz, blockIdx.x, gridDim.x);
+    const long e = rbx_cut(items, nz, (long)blockIdx.x + 1, gridDim.x);
+    int qb = 0;
+    for (bool first = true; s < e; first = false) {
+        const long item = s / nz;
+        const int k0 = (int)(s % nz);
+        const int kend = (int)(e - s < (long)(nz - k0) ? k0 + (e - s) : nz);
+        const int comp = (int)(item % 3), tile_y = (int)(item / 3);
+        // the previous run's last store has read its slot, and every thread
+        // is done with the staged planes, before this run refills them
+        if (!first) __syncthreads();
+        int n = 0;
+        bool ok;
+        if (comp == 0) ok = rbx_run<0, AH, NT>(g, G, A, R, omega, rbx_raw, tile_y, k0, kend, qb, n);
+        else if (comp == 1) ok = rbx_run<1, AH, NT>(g, G, A, R, omega, rbx_raw, tile_y, k0, kend, qb, n);
+        else ok = rbx_run<2, AH, NT>(g, G, A, R, omega, rbx_raw, tile_y, k0, kend, qb, n);
+        if (!ok) return;  // the error word is set; every thread leaves
+        qb += n;
+        s += kend - k0;
+    }
 }
 
 // geometry for a level (sms: multiprocessors of the device); false when the
@@ -380,23 +423,44 @@ inline bool rbx_geom(const Grid& g, int sms, size_t smem_max, RBXGeom& G, int ty
     G.rows = G.TY + 4;
     G.crows = G.TY + 2;
     G.tiles_y = ny / G.TY;
-    // z-runs: nz split into `chunks` runs of nz/chunks planes (rounded), the
-    // count that gives the busiest SM (one CTA per SM) the fewest plane
-    // steps, each run paying five prologue planes
-    long best = -1;
-    G.chunks = 0;
-    for (int c = 1; c <= nz / 4; c++) {
-        const long items = (long)G.tiles_y * 3 * c;
-        const long slots = (long)sms * G.per_sm;
-        const long rounds = (items + slots - 1) / slots;
-        const long cost = rounds * ((nz + c - 1) / c + 5);
-        if (best < 0 || cost < best) {
-            best = cost;
-            G.chunks = c;
+    // CTAs of the launch: each takes a stretch of the tiles_y * 3 * nz plane
+    // steps (rbx_cut).  The grid with the fewest plane steps on the busiest
+    // SM wins, a z-run's prologue counted as five plane steps: one CTA per
+    // resident slot (stretches cross item edges), or c equal z-runs per item
+    // (one item per CTA, in waves when they outnumber the slots).
+    const long items = (long)G.tiles_y * 3;
+    const long work = items * nz;
+    const long slots = (long)sms * G.per_sm;
+    auto cost_of = [&](long P) {
+        long worst = 0;
+        for (long b = 0; b < P; b++) {
+            long s0 = rbx_cut(items, nz, b, P);
+            const long e0 = rbx_cut(items, nz, b + 1, P);
+            long steps = 0;
+            while (s0 < e0) {
+                const long k0 = s0 % nz;
+                const long len = e0 - s0 < nz - k0 ? e0 - s0 : nz - k0;
+                steps += len + 5;
+                s0 += len;
+            }
+            worst = steps > worst ? steps : worst;
         }
-    }
-    if (!G.chunks) return false;
-    G.KZ = (nz + G.chunks - 1) / G.chunks;
+        return ((P + slots - 1) / slots) * worst;
+    };
+    long best = -1, bestP = 0;
+    auto consider = [&](long P) {
+        if (P < 1 || work < P * RBX_MINRUN) return;
+        const long c = cost_of(P);
+        if (best < 0 || c < best) {
+            best = c;
+            bestP = P;
+        }
+    };
+    consider(slots);
+    for (int c = 1; c <= nz / 4; c++) consider(items * c);
+    if (bestP < 1) return false;
+    G.chunks = (int)bestP;
+    G.KZ = (int)((work + G.chunks - 1) / G.chunks);  // plane steps of the longest stretch
     return true;
 }
 

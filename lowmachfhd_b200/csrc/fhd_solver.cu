@@ -535,7 +535,7 @@ static int stag_rbx_smooth(fhd_ctx* ctx, StagLevel<float>& L, const RBXGeom& G, 
         ctx->prof_bytes += rb_smooth_bytes(ctx, L);
         ctx->prof_launches++;
     }
-    const dim3 grd(G.tiles_y, G.chunks, 3);
+    const dim3 grd(G.chunks, 1, 1);
     if (G.ahead == 1) {
         if (int rc = rb_allow_smem(k_stag_rbx<1>, G.smem, true)) return rc;
         k_stag_rbx<1><<<grd, RBX_BLOCK, G.smem, ctx->stream>>>(L.g, G, L.op(), R, (float)ctx->p.stag_mg_omega);
@@ -1016,7 +1016,7 @@ static std::map<std::string, int> g_tune_import;  // imported choices (candidate
 // list: the device's SM count and shared-memory limits, and the version of
 // the candidate lists (bumped whenever a list or its order changes), so a
 // table from another GPU model or library version selects nothing.
-constexpr int TUNE_CANDS_VERSION = 3;
+constexpr int TUNE_CANDS_VERSION = 4;
 
 static std::string tune_key_of(int dev, int which, int elem, int dim, int visc, const int n[3], int sms, int optin,
                                int smem_sm) {
