@@ -254,6 +254,17 @@ def accuracy_test(dim, n, prob_coeff, prob_sol, visc_type, order=2):
     return err[: dim + 1]
 
 
+PERIODIC, NO_SLIP_WALL, SLIP_WALL = -1, 100, 200
+
+
+def set_walls(bc_lo=(PERIODIC,) * 3, bc_hi=(PERIODIC,) * 3):
+    """boundary codes of the grids later calls build (bc.f90 codes)"""
+    lo = (C.c_int * 3)(*[int(b) for b in bc_lo])
+    hi = (C.c_int * 3)(*[int(b) for b in bc_hi])
+    rc = lib().or_set_walls(lo, hi)
+    assert rc == 0, rc
+
+
 def compute_nlevs_mg(dim, n, minwidth=2):
     return lib().or_compute_nlevs_mg(dim, _n3(n), minwidth)
 

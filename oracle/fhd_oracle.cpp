@@ -25,18 +25,30 @@ namespace {
 
 typedef std::vector<double> Vec;
 
+// Domain walls of the grids built from here on (or_set_walls): per direction
+// and side 0 = periodic, -1 = no-slip wall, +1 = slip wall (the sign the
+// transverse velocity takes in the ghost cell behind the wall).
+static int g_wl[3] = {0, 0, 0}, g_wh[3] = {0, 0, 0};
+
 struct Geo {
     int dim = 2;
     int n[3] = {1, 1, 1};
     long nc = 1;
     double dx = 1.0;
+    int wl[3] = {0, 0, 0}, wh[3] = {0, 0, 0};
     Geo() {}
     Geo(int d, const int nn[3], double h) : dim(d), dx(h) {
         n[0] = nn[0];
         n[1] = nn[1];
         n[2] = (d == 3) ? nn[2] : 1;
         nc = (long)n[0] * n[1] * n[2];
+        for (int q = 0; q < 3; q++) {
+            wl[q] = q < d ? g_wl[q] : 0;
+            wh[q] = q < d ? g_wh[q] : 0;
+        }
     }
+    bool wall(int d) const { return wl[d] != 0; }
+    bool any_wall() const { return wall(0) || wall(1) || wall(2); }
     inline long id(int i, int j, int k) const {
         if (i < 0) i += n[0]; else if (i >= n[0]) i -= n[0];
         if (j < 0) j += n[1]; else if (j >= n[1]) j -= n[1];
@@ -48,6 +60,48 @@ struct Geo {
         return Geo(dim, nn, dx * 2.0);
     }
 };
+
+// Velocity component c at face (i, j, k), which may lie one face beyond the
+// domain: the ghost-cell rules of multifab_physbc_domainvel and
+// multifab_physbc_macvel (multifab_physbc_stag.f90:91-173, 957-1116), homogeneous.
+// Across a wall the normal component is zero (the high wall face, index n,
+// included: it is not stored), the transverse one is the first interior
+// value times the wall's sign (-1 no-slip, +1 slip); periodic directions wrap.
+inline double vel(const Geo& g, const double* u, int c, int i, int j, int k) {
+    int q[3] = {i, j, k};
+    double sg = 1.0;
+    for (int d = 0; d < g.dim; d++) {
+        if (!g.wall(d)) continue;
+        if (q[d] < 0) {
+            if (d == c) return 0.0;
+            sg *= g.wl[d];
+            q[d] = 0;
+        } else if (q[d] >= g.n[d]) {
+            if (d == c) return 0.0;
+            sg *= g.wh[d];
+            q[d] = g.n[d] - 1;
+        }
+    }
+    return sg * u[g.id(q[0], q[1], q[2])];
+}
+
+// the face of component c at cell (i, j, k) lies on a wall (index 0 in a
+// wall direction c; the high wall face is not stored)
+inline bool wall_face(const Geo& g, int c, int i, int j, int k) {
+    const int q[3] = {i, j, k};
+    return g.wall(c) && q[c] == 0;
+}
+
+// zero the wall faces of a face vector (multifab_physbc_domainvel)
+inline void zero_wall_faces(const Geo& g, double* const u[]) {
+    for (int c = 0; c < g.dim; c++) {
+        if (!g.wall(c)) continue;
+        for (int k = 0; k < g.n[2]; k++)
+            for (int j = 0; j < g.n[1]; j++)
+                for (int i = 0; i < g.n[0]; i++)
+                    if (wall_face(g, c, i, j, k)) u[c][g.id(i, j, k)] = 0.0;
+    }
+}
 
 inline int edge_of(int dim, int c, int d) {
     if (dim == 2) return 0;
@@ -170,6 +224,22 @@ inline double lface(const Geo& g, int visc, const Vec* alpha, const Vec& beta,
     // constant coefficients: beta, gamma taken from the first cell
     // (stag_applyop.f90:654-656 'b = beta(xlo(1),xlo(2),xlo(3))')
     const double b = beta[0], cg = gamma[0];
+    if (g.any_wall()) {
+        // walls (visc_type 1): the neighbours through the ghost rules
+        const double own = vel(g, phi[c], c, i + ec[0], j + ec[1], k + ec[2]) +
+                           vel(g, phi[c], c, i - ec[0], j - ec[1], k - ec[2]);
+        double oth = 0.0;
+        for (int d = 0; d < dim; d++) {
+            if (d == c) continue;
+            int ed[3] = {0, 0, 0};
+            ed[d] = 1;
+            oth += vel(g, phi[c], c, i + ed[0], j + ed[1], k + ed[2]) +
+                   vel(g, phi[c], c, i - ed[0], j - ed[1], k - ed[2]);
+        }
+        const double diag = a + (2.0 * dim) * b * q;
+        if (diag_out) *diag_out = diag;
+        return ph * diag - (own + oth) * b * q;
+    }
     const double own = phi[c][fpc] + phi[c][fmc];
     double oth = 0.0, cross = 0.0;
     for (int d = 0; d < dim; d++) {
@@ -214,7 +284,10 @@ void s_applyop(SLevel& L, int visc, int color) {
         double* out = L.Lphi[c].data();
         forall(g, [&](int i, int j, int k) {
             if (!in_color(color, c, i, j, k)) return;
-            out[g.id(i, j, k)] = lface(g, visc, L.alpha, L.beta, L.gamma, L.bed, ph, c, i, j, k, nullptr);
+            // Lphi on physical domain boundaries is zero (stag_applyop.f90:201-205)
+            out[g.id(i, j, k)] = wall_face(g, c, i, j, k)
+                                     ? 0.0
+                                     : lface(g, visc, L.alpha, L.beta, L.gamma, L.bed, ph, c, i, j, k, nullptr);
         });
     }
 }
@@ -246,7 +319,8 @@ void s_smooth(SLevel& L, int visc, double omega, int color) {
         forall(g, [&](int i, int j, int k) {
             if (!in_color(color, c, i, j, k)) return;
             long f = g.id(i, j, k);
-            p[f] = p[f] + omega * (r[f] - lp[f]) / dg[f];
+            // wall faces stay zero (multifab_physbc_domainvel after each colour)
+            p[f] = wall_face(g, c, i, j, k) ? 0.0 : p[f] + omega * (r[f] - lp[f]) / dg[f];
         });
     }
 }
@@ -335,7 +409,8 @@ void s_prolong_add(const Geo& gf, const Geo& gc, Vec* fine, const Vec* coarse) {
                 q[c] += o;
                 q[a] += pa;
                 if (b >= 0) q[b] += pb;
-                return C[gc.id(q[0], q[1], q[2])];
+                // the coarse ghost cells: multifab_physbc_macvel after the coarse smooths
+                return gc.any_wall() ? vel(gc, C, c, q[0], q[1], q[2]) : C[gc.id(q[0], q[1], q[2])];
             };
             long f = gf.id(i, j, k);
             bool even = (I[c] % 2 == 0);
@@ -352,6 +427,10 @@ void s_prolong_add(const Geo& gf, const Geo& gc, Vec* fine, const Vec* coarse) {
             }
             F[f] = F[f] + v;
         });
+    }
+    if (gf.any_wall()) {
+        double* fp[3] = {fine[0].data(), fine[1].data(), dim == 3 ? fine[2].data() : nullptr};
+        zero_wall_faces(gf, fp);
     }
 }
 
@@ -408,6 +487,7 @@ int stag_mg(const Geo& g0, int visc, const fhd_gmres_params* p, const double* co
             const double* beta, const double* const beta_ed[], const double* gamma, double theta,
             double* const phi[], const double* const rhs[], double* hist = nullptr) {
     const int dim = g0.dim;
+    if (g0.any_wall() && visc != 1) return FHD_ERR_UNSUPPORTED;  // walls: visc_type 1
     const int nl_domain = nlevs_mg(g0, p->stag_mg_minwidth);
     int nl_box;
     bool fancy;
@@ -496,7 +576,17 @@ int stag_mg(const Geo& g0, int visc, const fhd_gmres_params* p, const double* co
                     const double* r = L[l].rhs[c].data();
                     for (long f = 0; f < L[l].g.nc; f++) lp[f] = -(lp[f] - r[f]);
                 }
+                if (L[l].g.any_wall()) {
+                    // residual and restricted rhs zero on walls (stag_mg_solver.f90:420-440)
+                    double* lp[3] = {L[l].Lphi[0].data(), L[l].Lphi[1].data(), dim == 3 ? L[l].Lphi[2].data() : nullptr};
+                    zero_wall_faces(L[l].g, lp);
+                }
                 s_restrict(L[l].g, L[l + 1].g, L[l].Lphi, L[l + 1].rhs, false);
+                if (L[l + 1].g.any_wall()) {
+                    double* cr[3] = {L[l + 1].rhs[0].data(), L[l + 1].rhs[1].data(),
+                                     dim == 3 ? L[l + 1].rhs[2].data() : nullptr};
+                    zero_wall_faces(L[l + 1].g, cr);
+                }
             }
             if (nest >= 0) {
                 solve(nest, lend, -1, nullptr);  // theta_alpha = 1: the level's alpha carries it
@@ -620,6 +710,12 @@ int macproject_impl(const Geo& g0, const fhd_gmres_params* p, double* phi, const
     }
     for (int d = 0; d < dim; d++) std::copy(ainv[d], ainv[d] + g0.nc, L[0].a[d].begin());
     for (int l = 1; l < nl; l++) s_restrict(L[l - 1].g, L[l].g, L[l - 1].a, L[l].a, true);
+    // walls: homogeneous Neumann, no flux through a wall face (with the
+    // periodic index wrap the high wall face is face 0 as well)
+    for (int l = 0; l < nl && g0.any_wall(); l++) {
+        double* ap[3] = {L[l].a[0].data(), L[l].a[1].data(), dim == 3 ? L[l].a[2].data() : nullptr};
+        zero_wall_faces(L[l].g, ap);
+    }
     std::copy(rhs, rhs + g0.nc, L[0].rhs.begin());
     const double r0 = reduce_max(g0, [&](int i, int j, int k) { return std::fabs(rhs[g0.id(i, j, k)]); });
     if (r0 > 0.0) {
@@ -658,7 +754,9 @@ void c_grad(const Geo& g, const double* p, double* const gp[]) {
         e[d] = 1;
         forall(g, [&](int i, int j, int k) {
             long f = g.id(i, j, k);
-            gp[d][f] = (p[f] - p[g.id(i - e[0], j - e[1], k - e[2])]) * dxinv;
+            // at a wall the pressure ghost is the interior value (first-order
+            // extrapolation), so the gradient there is zero (div_and_grad.f90:540-556)
+            gp[d][f] = wall_face(g, d, i, j, k) ? 0.0 : (p[f] - p[g.id(i - e[0], j - e[1], k - e[2])]) * dxinv;
         });
     }
 }
@@ -738,6 +836,8 @@ int apply_matrix_impl(const Geo& g, int visc, double* const b_u[], double* b_p, 
     const int dim = g.dim;
     // stag_applyop_4o supports visc_type 1 only (stag_applyop.f90:1355, 1506)
     if (order != 2 && (order != 4 || visc != 1)) return -5;
+    // walls: visc_type 1, second order
+    if (g.any_wall() && (visc != 1 || order != 2)) return -5;
     Vec alpha[3], bed[3];
     Vec vb(beta, beta + g.nc), vg(gamma, gamma + g.nc);
     for (int c = 0; c < dim; c++) {
@@ -752,7 +852,8 @@ int apply_matrix_impl(const Geo& g, int visc, double* const b_u[], double* b_p, 
         for (int c = 0; c < dim; c++) {
             double* out = b_u[c];
             forall(g, [&](int i, int j, int k) {
-                out[g.id(i, j, k)] = lface(g, visc, alpha, vb, vg, bed, ph, c, i, j, k, nullptr);
+                out[g.id(i, j, k)] =
+                    wall_face(g, c, i, j, k) ? 0.0 : lface(g, visc, alpha, vb, vg, bed, ph, c, i, j, k, nullptr);
             });
         }
         std::vector<Vec> gp(dim, Vec(g.nc));
@@ -974,8 +1075,13 @@ int apply_precon_impl(const Geo& g, int visc, const fhd_gmres_params* p, const d
     // null space (apply_precon.f90:429-460)
     const double mean_p = sum(g, x_p) / (double)nc;
     for (long f = 0; f < nc; f++) x_p[f] = x_p[f] - mean_p;
-    if (theta == 0.0) {
+    // the velocity problem is singular too when theta = 0 and no wall is
+    // no-slip; then the mean of each periodic direction's component goes
+    bool no_slip = false;
+    for (int d = 0; d < dim; d++) no_slip = no_slip || g.wl[d] == -1 || g.wh[d] == -1;
+    if (theta == 0.0 && !no_slip) {
         for (int c = 0; c < dim; c++) {
+            if (g.wall(c)) continue;
             const double mu = sum(g, x_u[c]) / (double)nc;
             for (long f = 0; f < nc; f++) x_u[c][f] = x_u[c][f] - mu;
         }
@@ -1721,6 +1827,26 @@ int or_num_threads(void) {
 // (module state, as in the reference); 0 or >= n_cells: one box
 void or_set_max_grid_size(const int mgs[3]) {
     for (int d = 0; d < 3; d++) g_max_grid_size[d] = mgs ? mgs[d] : 0;
+}
+
+int or_set_walls(const int bc_lo[3], const int bc_hi[3]) {
+    auto code = [](int b, int& w) {
+        if (b == -1) w = 0;
+        else if (b == 100) w = -1;
+        else if (b == 200) w = 1;
+        else return false;
+        return true;
+    };
+    int lo[3], hi[3];
+    for (int d = 0; d < 3; d++) {
+        if (!code(bc_lo[d], lo[d]) || !code(bc_hi[d], hi[d])) return FHD_ERR_UNSUPPORTED;
+        if ((lo[d] == 0) != (hi[d] == 0)) return FHD_ERR_BAD_ARG;  // periodic on both sides or neither
+    }
+    for (int d = 0; d < 3; d++) {
+        g_wl[d] = lo[d];
+        g_wh[d] = hi[d];
+    }
+    return 0;
 }
 
 int or_compute_nlevs_mg(int dim, const int n[3], int minwidth) {

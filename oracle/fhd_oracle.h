@@ -193,6 +193,12 @@ int or_accuracy_test(int dim, int n, int prob_coeff, int prob_sol,
 int or_accuracy_test_order(int dim, int n, int prob_coeff, int prob_sol,
                            int visc_type, int order, double* err);
 
+/* Domain boundaries of the grids the following calls build: per direction
+ * bc codes -1 (periodic), 100 (no-slip wall), 200 (slip wall), as in bc.f90;
+ * a direction is periodic on both sides or on neither.  Walls are
+ * homogeneous (zero wall velocity) and need visc_type 1. */
+int or_set_walls(const int bc_lo[3], const int bc_hi[3]);
+
 /* number of OpenMP threads the oracle uses */
 int or_num_threads(void);
 

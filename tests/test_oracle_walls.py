@@ -1,0 +1,145 @@
+"""Homogeneous walls in the oracle (multifab_physbc_stag.f90:91-1116 ghost
+rules, stag_applyop.f90:201-205, stag_mg_solver.f90:360-440, the null-space
+step of apply_precon.f90:429-460).
+
+The reference stores no results for wall problems without inhomogeneous
+boundary values, so the restatement is checked by two exact properties:
+  * a slip wall is a mirror: the Stokes solve on a box with slip walls equals
+    the periodic solve on the box doubled across the walls, with the
+    tangential velocity and the pressure mirrored evenly and the normal
+    velocity oddly;
+  * plane Poiseuille flow between no-slip walls converges to the parabolic
+    profile at second order.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from tests import problems as P
+
+
+@pytest.fixture(autouse=True)
+def periodic_afterwards():
+    yield
+    O.set_walls()
+
+
+def doubled(dim, n, wall_dir, u, p):
+    """mirror a wall-domain field across its high wall in direction wall_dir"""
+    shape = [n[d] for d in reversed(range(dim))]  # (z, y, x)
+    ax = dim - 1 - wall_dir
+    out_u = []
+    for c in range(dim):
+        a = u[c].reshape(shape)
+        if c == wall_dir:
+            # faces j = 0 .. n-1 at y = j h; face 2n - j mirrors face j, oddly
+            m = -np.flip(a, axis=ax)
+            m = np.roll(m, 1, axis=ax)
+            idx = [slice(None)] * dim
+            idx[ax] = 0
+            m[tuple(idx)] = 0.0  # face n (the mirror of face n) is the wall
+            out_u.append(np.concatenate([a, m], axis=ax).ravel())
+        else:
+            out_u.append(np.concatenate([a, np.flip(a, axis=ax)], axis=ax).ravel())
+    q = p.reshape(shape)
+    out_p = np.concatenate([q, np.flip(q, axis=ax)], axis=ax).ravel()
+    return out_u, out_p
+
+
+def half(dim, n2, wall_dir, x):
+    shape = [n2[d] for d in reversed(range(dim))]
+    ax = dim - 1 - wall_dir
+    a = x.reshape(shape)
+    idx = [slice(None)] * dim
+    idx[ax] = slice(0, shape[ax] // 2)
+    return a[tuple(idx)].ravel()
+
+
+@pytest.mark.parametrize("dim,n,wall_dir", [(2, [16, 16], 1), (2, [16, 8], 0), (3, [8, 8, 8], 2)])
+@pytest.mark.parametrize("theta", [0.0, 2.0])
+def test_slip_walls_mirror_the_periodic_solve(dim, n, wall_dir, theta):
+    rng = np.random.default_rng(3)
+    nc = int(np.prod(n))
+    b_u = [rng.standard_normal(nc) for _ in range(dim)]
+    b_p = rng.standard_normal(nc)
+    b_p -= b_p.mean()
+    # the normal rhs on the wall faces is zero
+    shape = [n[d] for d in reversed(range(dim))]
+    ax = dim - 1 - wall_dir
+    a = b_u[wall_dir].reshape(shape)
+    idx = [slice(None)] * dim
+    idx[ax] = 0
+    a[tuple(idx)] = 0.0
+    b_u[wall_dir] = a.ravel()
+    if theta == 0.0:
+        # consistent rhs: the periodic directions' velocity means are free
+        for c in range(dim):
+            if c != wall_dir:
+                b_u[c] = b_u[c] - b_u[c].mean()
+    params = O.default_params(gmres_rel_tol=1e-12)
+    bc = [-1] * 3
+    bc[wall_dir] = O.SLIP_WALL
+    O.set_walls(bc, bc)
+    pb = P.problem(dim, n, 1, dx=1.0, seed=4)
+    rc, x_u, x_p, _, st = O.gmres(pb, params, theta, b_u, b_p)
+    assert rc in (0, 3)
+    O.set_walls()
+    n2 = list(n)
+    n2[wall_dir] *= 2
+    pb2 = P.problem(dim, n2, 1, dx=1.0, seed=4)
+    bu2, bp2 = doubled(dim, n, wall_dir, b_u, b_p)
+    rc2, y_u, y_p, _, _ = O.gmres(pb2, params, theta, bu2, bp2)
+    assert rc2 in (0, 3)
+    for c in range(dim):
+        got = half(dim, n2, wall_dir, y_u[c])
+        assert P.rel_inf([x_u[c]], [got]) < 1e-8, c
+    got_p = half(dim, n2, wall_dir, y_p)
+    assert P.rel_inf([x_p - x_p.mean()], [got_p - got_p.mean()]) < 1e-8
+
+
+def poiseuille_error(n):
+    """channel periodic in x, no-slip walls in y, unit forcing in x, theta 0:
+    the discrete u_x against eta^-1 y (L - y) / 2"""
+    dim = 2
+    nn = [8, n]
+    nc = 8 * n
+    h = 1.0 / n
+    O.set_walls([-1, O.NO_SLIP_WALL, -1], [-1, O.NO_SLIP_WALL, -1])
+    pb = P.problem(dim, nn, 1, dx=h, seed=5)
+    eta = pb.beta[0]
+    b_u = [np.ones(nc), np.zeros(nc)]
+    b_p = np.zeros(nc)
+    rc, x_u, x_p, _, st = O.gmres(pb, O.default_params(gmres_rel_tol=1e-12), 0.0, b_u, b_p)
+    O.set_walls()
+    assert rc in (0, 3)
+    y = (np.arange(n) + 0.5) * h
+    exact = np.tile(y * (1.0 - y) / (2.0 * eta), (8, 1)).T.ravel()  # (y, x) order: x fastest
+    assert np.max(np.abs(x_u[1])) < 1e-10  # no cross flow
+    return np.max(np.abs(x_u[0] - exact)) / np.max(exact)
+
+
+def test_poiseuille_converges_at_second_order():
+    e1, e2, e3 = poiseuille_error(8), poiseuille_error(16), poiseuille_error(32)
+    assert e1 < 0.05
+    assert 3.5 < e1 / e2 < 4.5
+    assert 3.5 < e2 / e3 < 4.5
+
+
+def test_walls_need_visc_type_one():
+    O.set_walls([-1, O.NO_SLIP_WALL, -1], [-1, O.NO_SLIP_WALL, -1])
+    pb = P.problem(2, [8, 8], -1, dx=1.0, seed=6)
+    u, p = P.random_stokes(2, [8, 8], seed=7)
+    with pytest.raises(AssertionError):
+        O.apply_matrix(pb, 1.0, u, p)
+
+
+def test_wall_faces_of_apply_matrix_are_zero():
+    """A x has zero on the wall faces (stag_applyop.f90:201-205 and a zero
+    pressure gradient there)"""
+    O.set_walls([O.NO_SLIP_WALL, -1, -1], [O.SLIP_WALL, -1, -1])
+    pb = P.problem(2, [12, 8], 1, dx=0.5, seed=8)
+    u, p = P.random_stokes(2, [12, 8], seed=9)
+    u[0].reshape(8, 12)[:, 0] = 0.0
+    b_u, _ = O.apply_matrix(pb, 1.5, u, p)
+    assert np.all(b_u[0].reshape(8, 12)[:, 0] == 0.0)
+    assert np.any(b_u[0].reshape(8, 12)[:, 1:] != 0.0)
