@@ -142,8 +142,17 @@ int  fhd_ctx_create(int dim, const int n_cells[3], const double dx[3],
                     int precision_mode, fhd_ctx** out);
 /* The same context with the layout arguments of the driver's set-up
  * (probin_common max_grid_size, bc_lo, bc_hi; main_driver.f90:392-393).
- * bc codes: FHD_BC_PERIODIC (-1, FBoxLib's PERIODIC) in every direction;
- * walls and reservoirs return FHD_ERR_UNSUPPORTED (they are not built).
+ * bc codes (bc.f90:24-44): FHD_BC_PERIODIC (-1), FHD_BC_NO_SLIP_WALL (100)
+ * and FHD_BC_SLIP_WALL (200); a direction is periodic on both sides or on
+ * neither.  Walls are homogeneous (the wall velocity is zero) and apply the
+ * ghost rules of multifab_physbc_domainvel / multifab_physbc_macvel
+ * (multifab_physbc_stag.f90:91-1116) throughout the Stokes solve; they are
+ * built for visc_type 1, precon_type 1 without the BFBt Schur complement,
+ * the colour smoother, gmres_spatial_order 2 and one box, and the timestep
+ * and stochastic-flux entries refuse a context with walls.  In a wall
+ * direction a face array keeps n faces: face 0 is the low wall face (held at
+ * zero) and the high wall face is not stored.  Reservoirs and other codes
+ * return FHD_ERR_UNSUPPORTED.
  * max_grid_size[d] (>= 1; below n_cells[d] it must divide it) sets the box
  * layout the reference's staggered multigrid follows: with several boxes
  * its hierarchy stops at the boxes' depth (compute_nlevs_mg over the boxes,
@@ -153,6 +162,8 @@ int  fhd_ctx_create(int dim, const int n_cells[3], const double dx[3],
  * 447-555).  The pressure multigrid is FBoxLib's in the reference and keeps
  * the whole-domain hierarchy here. */
 #define FHD_BC_PERIODIC (-1)
+#define FHD_BC_NO_SLIP_WALL 100
+#define FHD_BC_SLIP_WALL 200
 int  fhd_ctx_create_bc(int dim, const int n_cells[3], const int max_grid_size[3],
                        const int bc_lo[3], const int bc_hi[3], const double dx[3],
                        int visc_type, const fhd_gmres_params* params,

@@ -30,6 +30,11 @@ FHD_ERR_NO_DEVICE = -9
 FHD_PREC_FP64 = 0
 FHD_PREC_MIXED = 1
 
+# boundary codes of fhd_ctx_create_bc (bc.f90:24-44)
+FHD_BC_PERIODIC = -1
+FHD_BC_NO_SLIP_WALL = 100
+FHD_BC_SLIP_WALL = 200
+
 
 class GmresParams(C.Structure):
     """fhd_gmres_params: mirror of namelist probin_gmres (probin_gmres.f90:12-163)."""

@@ -1264,6 +1264,7 @@ static int check_mix(const fhd_mixture_params* mp) {
 extern "C" int fhd_dev_compute_sqrtLonsager_fc(fhd_ctx* ctx, const fhd_mixture_params* mp,
                                                const fhd_stoch_params* sp, const double* const rho[],
                                                double* const sqrtLonsager_fc[]) {
+    if (int wr = refuse_walls(ctx, "fhd_dev_compute_sqrtLonsager_fc")) return wr;
     if (!ctx || !mp || !sp || !rho || !sqrtLonsager_fc) return FHD_ERR_BAD_ARG;
     if (int rc = check_mix(mp)) return rc;
     const MixDev m = make_mixdev(mp, sp);
@@ -1285,6 +1286,7 @@ extern "C" int fhd_dev_stochastic_mass_fluxdiv(fhd_ctx* ctx, const fhd_mixture_p
                                                const double* const W_fc[], int increment,
                                                double* const stoch_mass_fluxdiv[],
                                                double* const stoch_mass_flux[]) {
+    if (int wr = refuse_walls(ctx, "fhd_dev_stochastic_mass_fluxdiv")) return wr;
     if (!ctx || !mp || !sp || !sqrtLonsager_fc || !weights || !W_fc || !stoch_mass_fluxdiv || !(dt > 0.0))
         return FHD_ERR_BAD_ARG;
     if (n_rngs < 1 || n_rngs > 4) {
@@ -1319,6 +1321,7 @@ extern "C" int fhd_dev_stochastic_mass_fluxdiv(fhd_ctx* ctx, const fhd_mixture_p
 extern "C" int fhd_dev_compute_mass_fluxdiv(fhd_ctx* ctx, const fhd_mixture_params* mp, const fhd_stoch_params* sp,
                                             const double* const rho[], double dt, const double* weights, int n_rngs,
                                             const double* const W_fc[], double* const out[]) {
+    if (int wr = refuse_walls(ctx, "fhd_dev_compute_mass_fluxdiv")) return wr;
     if (!ctx || !mp || !sp || !rho || !weights || !W_fc || !out) return FHD_ERR_BAD_ARG;
     const int rc = fhd::mass_fluxdiv(ctx, mp, sp, rho, dt, weights, n_rngs, W_fc, out);
     if (rc < 0) return rc;

@@ -195,6 +195,32 @@ static int build_mg(fhd_ctx* ctx, Multigrid<T>& M) {
 // coefficient hierarchy for the current operator (stag_mg_solver.f90:
 // 200-230; alphainv of apply_precon.f90:73-76 coarsened for the pressure
 // multigrid as face averages)
+// zero the wall faces of a face vector of level grid g (no-op without walls)
+template <typename T>
+static int zero_walls(fhd_ctx* ctx, const Grid& g, T* u0, T* u1, T* u2) {
+    if (!ctx->has_walls) return 0;
+    int rc = 0;
+    with_dim(ctx->dim, [&](auto D) {
+        constexpr int DIM = decltype(D)::value;
+        k_zero_walls<T, DIM><<<cell_grid(g), cell_block(), 0, ctx->stream>>>(g, ctx->walls, u0, u1, u2);
+        rc |= post(ctx);
+    });
+    return rc;
+}
+
+// the wall smoother is two-pass on every staggered level: the diagonal
+// arrays that only odd-extent levels have otherwise
+template <typename T>
+static int wall_diag(fhd_ctx* ctx) {
+    for (auto& L : mg_of<T>(ctx).s)
+        for (int c = 0; c < ctx->dim; c++)
+            if (!L.diag[c]) {
+                L.diag[c] = ctx->arena.alloc<T>(L.g.nc);
+                if (!L.diag[c]) return FHD_ERR_OOM;
+            }
+    return 0;
+}
+
 template <typename T>
 static int prepare_T(fhd_ctx* ctx) {
     Multigrid<T>& M = mg_of<T>(ctx);
@@ -285,6 +311,10 @@ static int prepare_T(fhd_ctx* ctx) {
             });
             if (rc) return rc;
         }
+        // walls: no flux through a wall face (with the periodic index wrap
+        // of the pressure kernels the high wall face is face 0 as well)
+        for (size_t l = 0; l < M.c.size(); l++)
+            if (int rc = zero_walls<T>(ctx, M.c[l].g, M.c[l].a[0], M.c[l].a[1], M.c[l].a[2])) return rc;
     }
     // the BFBt pressure multigrid: mu^-1 = 1/diag(viscous operator)
     // (apply_precon.f90:589), coarsened as alpha^-1 is
@@ -595,6 +625,27 @@ static int stag_smooths_planned(fhd_ctx* ctx, StagLevel<T>& L, const SmoothPlan&
 template <typename T>
 static int stag_smooths(fhd_ctx* ctx, StagLevel<T>& L, int count) {
     const int dim = ctx->dim;
+    if (ctx->has_walls) {
+        // the colours of the reference's smoother, each as Lphi and the
+        // diagonal of its faces, then the update (the wall faces stay zero)
+        const StagOp<T> A = L.op();
+        const T omega = (T)ctx->p.stag_mg_omega;
+        int rc = 0;
+        for (int m = 0; m < count && !rc; m++)
+            for (int color = 1; color <= 2 * dim && !rc; color++)
+                with_dim(dim, [&](auto D) {
+                    constexpr int DIM = decltype(D)::value;
+                    k_stag_color_apply_w<T, DIM><<<cell_grid(L.g), cell_block(), 0, ctx->stream>>>(
+                        L.g, ctx->walls, A, L.phi[0], L.phi[1], L.phi[2], L.rhs[0], L.rhs[1], L.rhs[2], L.tmp[0],
+                        L.tmp[1], L.tmp[2], L.diag[0], L.diag[1], L.diag[2], color);
+                    rc |= post(ctx);
+                    k_stag_color_update<T, DIM><<<cell_grid(L.g), cell_block(), 0, ctx->stream>>>(
+                        L.g, L.phi[0], L.phi[1], L.phi[2], L.rhs[0], L.rhs[1], L.rhs[2], L.tmp[0], L.tmp[1],
+                        L.tmp[2], L.diag[0], L.diag[1], L.diag[2], color, omega);
+                    rc |= post(ctx);
+                });
+        return rc;
+    }
     int m0 = 0;
     RBGeom G;
     const bool aligned = stag_aligned(L, dim);
@@ -644,6 +695,16 @@ template <typename T>
 static int stag_residual(fhd_ctx* ctx, StagLevel<T>& L) {
     int rc = 0;
     const StagOp<T> A = L.op();
+    if (ctx->has_walls) {
+        with_dim(ctx->dim, [&](auto D) {
+            constexpr int DIM = decltype(D)::value;
+            k_stag_apply_w<T, DIM><<<cell_grid(L.g), cell_block(), 0, ctx->stream>>>(
+                L.g, ctx->walls, A, L.phi[0], L.phi[1], L.phi[2], L.tmp[0], L.tmp[1], L.tmp[2], L.rhs[0], L.rhs[1],
+                L.rhs[2], 1);
+            rc |= post(ctx);
+        });
+        return rc;
+    }
     with_dim_visc(ctx->dim, ctx->visc, [&](auto D, auto V) {
         constexpr int DIM = decltype(D)::value, VISC = decltype(V)::value;
         k_stag_apply<T, DIM, VISC><<<cell_grid(L.g), cell_block(), 0, ctx->stream>>>(
@@ -683,6 +744,8 @@ static int coarse_first(fhd_ctx* ctx, int n, F bytes) {
 template <typename T>
 static int stag_coarse_first(fhd_ctx* ctx, Multigrid<T>& M) {
     const int dim = ctx->dim;
+    // the single-CTA coarse kernel knows no walls: every level by launches
+    if (ctx->has_walls) return (int)M.s.size();
     return coarse_first(ctx, (int)M.s.size(),
                         [&](int l) { return (size_t)(3 * dim) * (size_t)M.s[l].g.nc * sizeof(T); });
 }
@@ -754,6 +817,8 @@ static int stag_vcycle(fhd_ctx* ctx, Multigrid<T>& M) {
                                                                            C.rhs[0], C.rhs[1], C.rhs[2], 0);
             rc |= post(ctx);
         });
+        // the restricted residual is zero on the coarse wall faces
+        if (!rc) rc = zero_walls<T>(ctx, C.g, C.rhs[0], C.rhs[1], C.rhs[2]);
         if (rc) return rc;
     }
     int rc = lc < nl ? stag_coarse(ctx, M, lc) : stag_smooths(ctx, M.s[nl - 1], ctx->p.stag_mg_nsmooths_bottom);
@@ -761,13 +826,21 @@ static int stag_vcycle(fhd_ctx* ctx, Multigrid<T>& M) {
     for (int l = lt - 1; l >= 0; l--) {
         StagLevel<T>& L = M.s[l];
         StagLevel<T>& C = M.s[l + 1];
-        with_dim(dim, [&](auto D) {
-            constexpr int DIM = decltype(D)::value;
-            k_stag_prolong<T, DIM><<<cell_grid(C.g), cell_block(), 0, st>>>(L.g, C.g, L.phi[0], L.phi[1], L.phi[2],
-                                                                          C.phi[0], C.phi[1], C.phi[2],
-                                                                          pair_aligned(dim, L.phi));
-            rc |= post(ctx);
-        });
+        if (ctx->has_walls) {
+            with_dim(dim, [&](auto D) {
+                constexpr int DIM = decltype(D)::value;
+                k_stag_prolong_w<T, DIM><<<cell_grid(L.g), cell_block(), 0, st>>>(
+                    L.g, C.g, ctx->walls, L.phi[0], L.phi[1], L.phi[2], C.phi[0], C.phi[1], C.phi[2]);
+                rc |= post(ctx);
+            });
+        } else {
+            with_dim(dim, [&](auto D) {
+                constexpr int DIM = decltype(D)::value;
+                k_stag_prolong<T, DIM><<<cell_grid(C.g), cell_block(), 0, st>>>(
+                    L.g, C.g, L.phi[0], L.phi[1], L.phi[2], C.phi[0], C.phi[1], C.phi[2], pair_aligned(dim, L.phi));
+                rc |= post(ctx);
+            });
+        }
         if (rc) return rc;
         rc = stag_smooths(ctx, L, ctx->p.stag_mg_nsmooths_up);
         if (rc) return rc;
@@ -868,6 +941,7 @@ static int stag_mg_run(fhd_ctx* ctx, Multigrid<T>& M) {
     const int maxv = ctx->p.stag_mg_max_vcycles;
     StagLevel<T>& L0 = M.s[0];
     const i64 nc = L0.g.nc;
+    if (int rc = zero_walls<T>(ctx, L0.g, L0.phi[0], L0.phi[1], L0.phi[2])) return rc;
     double resid0[3] = {0, 0, 0};
     if (maxv > 1) {
         int rc = stag_residual(ctx, L0);
@@ -1224,7 +1298,9 @@ static int tune_levels_locked(fhd_ctx* ctx, Multigrid<T>& M, std::vector<T*>& sc
 template <typename T>
 static int tune_levels(fhd_ctx* ctx) {
     Multigrid<T>& M = mg_of<T>(ctx);
-    if (ctx->tune_mode == 0) {
+    // (with walls the staggered levels smooth with the wall colours and the
+    // pressure levels keep the fixed rules)
+    if (ctx->tune_mode == 0 || ctx->has_walls) {
         for (auto& L : M.s) L.plan = SmoothPlan();
         for (auto& C : M.c) C.plan = SmoothPlan();
         return 0;
@@ -1491,6 +1567,8 @@ static int precon_T(fhd_ctx* ctx, CSVec<double> b, SVec<double> x) {
                 x.c[1], DIM == 3 ? x.c[2] : nullptr, (T)(1.0 / g.dx));
             rc |= post(ctx);
         });
+        // the pressure gradient is zero on wall faces: x_u keeps x_u* there (zero)
+        if (!rc) rc = zero_walls<double>(ctx, g, x.c[0], x.c[1], dim == 3 ? x.c[2] : nullptr);
         if (rc) return rc;
         const int kind = (pt == 1 || theta == 0.0) ? 0 : 1;
         if ((rc = bfbt ? visc_schur(fabs(theta) > 0.0, 0) : schur(kind, 1, 0))) return rc;
@@ -1545,14 +1623,16 @@ static int precon_T(fhd_ctx* ctx, CSVec<double> b, SVec<double> x) {
         }
         if ((rc = phi_to_x())) return rc;
     }
-    // null space: mean of p, and of u when theta_alpha = 0 (all walls are
-    // periodic here, so no no-slip wall exists) -- apply_precon.f90:429-460
+    // null space: mean of p, and of u when theta_alpha = 0 and no wall is
+    // no-slip, for the periodic directions -- apply_precon.f90:429-460
     k_sum<double><<<nb, RED_THREADS, 0, st>>>(nc, x.c[dim], slot(ctx, S_MEAN));
     FHD_POST(ctx);
     k_sub_mean<double><<<nb, 256, 0, st>>>(nc, x.c[dim], ctx->dscal + S_MEAN, (double)nc);
     FHD_POST(ctx);
-    if (theta == 0.0) {
+    if (theta == 0.0 && !ctx->noslip) {
         for (int c = 0; c < dim; c++) {
+            // the velocity means go for periodic directions only
+            if (ctx->walls.lo[c] != 0) continue;
             k_sum<double><<<nb, RED_THREADS, 0, st>>>(nc, x.c[c], slot(ctx, S_MEAN + 1 + c));
             FHD_POST(ctx);
             k_sub_mean<double><<<nb, 256, 0, st>>>(nc, x.c[c], ctx->dscal + S_MEAN + 1 + c, (double)nc);
@@ -1610,6 +1690,15 @@ int stokes_apply(fhd_ctx* ctx, CSVec<double> x, CSVec<double> rhs, SVec<double> 
     A.gamma = ctx->gamma;
     A.q = 1.0 / (ctx->dx * ctx->dx);
     int rc = 0;
+    if (ctx->has_walls) {
+        with_dim(ctx->dim, [&](auto D) {
+            constexpr int DIM = decltype(D)::value;
+            k_stokes_apply_w<DIM><<<cell_grid(ctx->g0), cell_block(), 0, ctx->stream>>>(
+                ctx->g0, ctx->walls, A, x, rhs, out, mode, 1.0 / ctx->dx);
+            rc |= post(ctx);
+        });
+        return rc;
+    }
     if (ctx->p.gmres_spatial_order == 4) {
         const double t1 = 1.0 / (12.0 * ctx->dx), t2 = 1.0 / (12.0 * ctx->dx * ctx->dx);
         if (ctx->dim == 2)
@@ -2087,19 +2176,60 @@ int fhd_ctx_create_bc(int dim, const int n_cells[3], const int max_grid_size[3],
                       int precision_mode, fhd_ctx** out) {
     if (!out || !n_cells || !max_grid_size || !bc_lo || !bc_hi || (dim != 2 && dim != 3)) return FHD_ERR_BAD_ARG;
     *out = nullptr;
+    Walls W = {{0, 0, 0}, {0, 0, 0}};
+    bool any = false, noslip = false;
+    auto sign = [](int code, int& w) {
+        if (code == FHD_BC_PERIODIC) w = 0;
+        else if (code == FHD_BC_NO_SLIP_WALL) w = -1;
+        else if (code == FHD_BC_SLIP_WALL) w = 1;
+        else return false;
+        return true;
+    };
     for (int d = 0; d < dim; d++) {
-        if (bc_lo[d] != FHD_BC_PERIODIC || bc_hi[d] != FHD_BC_PERIODIC) {
-            set_last_error("fhd_ctx_create_bc: only periodic boundaries (bc code -1) are built; walls and "
-                           "reservoirs are not");
+        if (!sign(bc_lo[d], W.lo[d]) || !sign(bc_hi[d], W.hi[d])) {
+            set_last_error("fhd_ctx_create_bc: bc codes -1 (periodic), 100 (no-slip wall) and 200 (slip wall) "
+                           "are built; reservoirs and other codes are not");
             return FHD_ERR_UNSUPPORTED;
         }
+        if ((W.lo[d] == 0) != (W.hi[d] == 0)) {
+            set_last_error("fhd_ctx_create_bc: a direction is periodic on both sides or on neither");
+            return FHD_ERR_BAD_ARG;
+        }
+        any = any || W.lo[d] != 0;
+        noslip = noslip || W.lo[d] < 0 || W.hi[d] < 0;
         if (max_grid_size[d] < 1) return FHD_ERR_BAD_ARG;
         if (max_grid_size[d] < n_cells[d] && n_cells[d] % max_grid_size[d] != 0) {
             set_last_error("fhd_ctx_create_bc: max_grid_size must divide n_cells (boxes of equal size)");
             return FHD_ERR_UNSUPPORTED;
         }
     }
-    return ctx_create(dim, n_cells, max_grid_size, dx, visc_type, params, precision_mode, out);
+    if (any) {
+        fhd_gmres_params p;
+        if (params) p = *params;
+        else fhd_gmres_params_default(&p);
+        bool boxes = false;
+        for (int d = 0; d < dim; d++) boxes = boxes || max_grid_size[d] < n_cells[d];
+        if (visc_type != 1 || p.precon_type != 1 || p.visc_schur_approx != 0 || p.stag_mg_smoother == 0 ||
+            p.gmres_spatial_order != 2 || boxes) {
+            set_last_error("fhd_ctx_create_bc: walls are built for visc_type 1, precon_type 1 without the BFBt "
+                           "Schur complement, the colour smoother, second order and one box");
+            return FHD_ERR_UNSUPPORTED;
+        }
+    }
+    const int rc = ctx_create(dim, n_cells, max_grid_size, dx, visc_type, params, precision_mode, out);
+    if (rc == FHD_OK && any) {
+        fhd_ctx* c = *out;
+        c->walls = W;
+        c->has_walls = true;
+        c->noslip = noslip;
+        const int r2 = c->prec == FHD_PREC_MIXED ? wall_diag<float>(c) : wall_diag<double>(c);
+        if (r2 != FHD_OK) {
+            fhd_ctx_destroy(c);
+            *out = nullptr;
+            return r2;
+        }
+    }
+    return rc;
 }
 
 static int ctx_create(int dim, const int n_cells[3], const int max_grid_size[3], const double dx[3], int visc_type,

@@ -11,6 +11,7 @@
 #include "../../include/fhd_b200.h"
 #include "fhd_vec.cuh"
 #include "fhd_rb.cuh"
+#include "fhd_walls.cuh"
 
 namespace fhd {
 
@@ -218,6 +219,11 @@ struct fhd_ctx {
     // or (stag_mg_bottom_solver 4, n/max_grid_size >= 2) solves its bottom
     // by a nested solve over the deeper levels of the domain ("fancy")
     int mgs[3] = {0, 0, 0};
+    // domain walls (fhd_ctx_create_bc bc codes 100 no-slip, 200 slip): the
+    // ghost sign per direction and side, 0 where periodic
+    fhd::Walls walls = {{0, 0, 0}, {0, 0, 0}};
+    bool has_walls = false;
+    bool noslip = false;  // some wall is no-slip
     int stag_nl_box = 0;      // levels of the box hierarchy (0: the domain's)
     bool stag_fancy = false;  // nested bottom solve from level stag_nl_box - 1
     double dx = 1.0;
@@ -291,6 +297,14 @@ struct fhd_ctx {
     double prof_bytes = 0.0;
     long long prof_launches = 0;
 };
+
+// the timestep and stochastic-flux entries are built for periodic boxes
+inline int refuse_walls(const fhd_ctx* ctx, const char* what) {
+    if (!ctx || !ctx->has_walls) return 0;
+    fhd::set_last_error(std::string(what) + ": the context has walls; the timesteps and stochastic fluxes are built "
+                                       "for periodic boxes");
+    return FHD_ERR_UNSUPPORTED;
+}
 
 namespace fhd {
 constexpr int NSCAL = 256;

@@ -743,6 +743,7 @@ int fhd_dev_advance_overdamped(fhd_ctx* ctx, const fhd_stoch_params* sp, const f
                                const double* const eta_ed[], const double* kappa, const double* temperature,
                                const double* const temperature_ed[], const double* const W_cc[],
                                const double* const W_ed[], const double* const W_mass[], fhd_solve_stats* stats2) {
+    if (int wr = refuse_walls(ctx, "fhd_dev_advance_overdamped")) return wr;
     if (!ctx || !sp || !umac || !rho || !pi || !eta || !eta_ed || !kappa || !temperature || !temperature_ed ||
         !W_cc || !W_ed || (mp && !W_mass) || !(dt > 0.0))
         return FHD_ERR_BAD_ARG;
@@ -757,6 +758,7 @@ int fhd_dev_stochastic_m_fluxdiv(fhd_ctx* ctx, const fhd_stoch_params* sp, doubl
                                  const double* eta, const double* const eta_ed[], const double* temperature,
                                  const double* const temperature_ed[], double dt, const double* weights, int n_rngs,
                                  const double* const W_cc[], const double* const W_ed[]) {
+    if (int wr = refuse_walls(ctx, "fhd_dev_stochastic_m_fluxdiv")) return wr;
     if (!ctx || !sp || !force || !eta || !eta_ed || !temperature || !temperature_ed || !weights || !W_cc || !W_ed)
         return FHD_ERR_BAD_ARG;
     int rc = stoch_launch(ctx, sp, force, increment, eta, eta_ed, temperature, temperature_ed, dt, weights, n_rngs,
@@ -770,6 +772,7 @@ int fhd_dev_advance_inertial(fhd_ctx* ctx, const fhd_stoch_params* sp, double dt
                              double* pi, const double* eta, const double* const eta_ed[], const double* kappa,
                              const double* temperature, const double* const temperature_ed[],
                              const double* const W_cc[], const double* const W_ed[], fhd_solve_stats* stats2) {
+    if (int wr = refuse_walls(ctx, "fhd_dev_advance_inertial")) return wr;
     if (!ctx || !sp || !umac || !rho || !pi || !eta || !eta_ed || !kappa || !temperature || !temperature_ed ||
         !W_cc || !W_ed || !(dt > 0.0))
         return FHD_ERR_BAD_ARG;
@@ -788,6 +791,7 @@ int fhd_dev_advance_inertial_multispecies(fhd_ctx* ctx, const fhd_stoch_params* 
                                           const double* temperature, const double* const temperature_ed[],
                                           const double* const W_cc[], const double* const W_ed[],
                                           const double* const W_mass[], fhd_solve_stats* stats2) {
+    if (int wr = refuse_walls(ctx, "fhd_dev_advance_inertial_multispecies")) return wr;
     if (!ctx || !sp || !mp || !umac || !rho || !pi || !mass_fluxdiv || !eta || !eta_ed || !kappa || !temperature ||
         !temperature_ed || !W_cc || !W_ed || !W_mass || !(dt > 0.0))
         return FHD_ERR_BAD_ARG;
