@@ -422,11 +422,23 @@ int advance_inertial_ms(fhd_ctx* ctx, const fhd_stoch_params* sp, const fhd_mixt
     };
     // -S = sum_i -F_i/rhobar_i into rhs_p (advance_timestep_inertial.f90:420-430)
     auto rhs_p_from_fluxes = [&]() -> int {
-        FHD_CUDA_TRY(cudaMemsetAsync(rhs_p, 0, sizeof(double) * nc, st));
-        if (!mp) return 0;
-        for (int s = 0; s < ns; s++) {
-            int r2 = lin_n(ctx, 1, one(rhs_p), 1, {{-1.0 / mp->rhobar[s], cs(one(fluxdiv[s]))}});
-            if (r2) return r2;
+        if (!mp) {
+            FHD_CUDA_TRY(cudaMemsetAsync(rhs_p, 0, sizeof(double) * nc, st));
+            return 0;
+        }
+        // the species in order, up to four per pass, on a sum that starts
+        // at zero (bitwise one pass per species after zeroing)
+        for (int s0 = 0; s0 < ns; s0 += 4) {
+            Lin Ls;
+            memset(&Ls, 0, sizeof(Ls));
+            Ls.nt = ns - s0 < 4 ? ns - s0 : 4;
+            for (int t = 0; t < Ls.nt; t++) {
+                Ls.a[t] = -1.0 / mp->rhobar[s0 + t];
+                Ls.x[t][0] = fluxdiv[s0 + t];
+            }
+            k_lin<<<nb, 256, 0, st>>>(nc, 1, one(rhs_p), Ls, s0 > 0 ? 1 : 0);
+            ctx->launches++;
+            FHD_CUDA_TRY(cudaPeekAtLastError());
         }
         return 0;
     };
@@ -467,34 +479,35 @@ int advance_inertial_ms(fhd_ctx* ctx, const fhd_stoch_params* sp, const fhd_mixt
         k_avg_face<DIM><<<cell_grid(g), cell_block(), 0, st>>>(g, rhotot, rfn.c[0], rfn.c[1], rfn.c[2]);
     });
     species_fc(rho);
-    // Steps 3-4: predictor Crank-Nicolson right-hand side
+    // Steps 3-4: predictor Crank-Nicolson right-hand side.  The terms are
+    // formed first; two multi-term passes then add them in the order of
+    // the reference's accumulation, each term in turn on the running sum,
+    // which is bitwise the sum of one pass per term.  The explicit half of
+    // the viscous term appears twice (0.5 L u of the right-hand side and of
+    // -A u^n); both are the same L u.
+    const bool with_stoch = sp->variance_coef_mom != 0.0;
     k_mul<<<nb, 256, 0, st>>>(nc, dim, mold, cs(rfo), cs(u));
     ctx->launches++;
-    if ((rc = lin(ctx, rhs_v, 0, {{1.0 / dt, cs(mold)}}))) return rc;
     launch_dim([&](auto D) {
         constexpr int DIM = decltype(D)::value;
         k_grad<DIM><<<cell_grid(g), cell_block(), 0, st>>>(g, pi, gpi, dxinv);
     });
-    if ((rc = lin(ctx, rhs_v, 1, {{-1.0, cs(gpi)}}))) return rc;
     launch_dim([&](auto D) {
         constexpr int DIM = decltype(D)::value;
         k_adv_m<DIM><<<cell_grid(g), cell_block(), 0, st>>>(g, cs(u), cs(mold), adv, 0, dxinv);
     });
-    if ((rc = lin(ctx, rhs_v, 1, {{1.0, cs(adv)}}))) return rc;
     if ((rc = diff_m(ctx, diff, cs(u), eta, eta_ed, kappa))) return rc;
-    if ((rc = lin(ctx, rhs_v, 1, {{0.5, cs(diff)}}))) return rc;
-    if (sp->variance_coef_mom != 0.0) {
-        if ((rc = stoch_launch(ctx, sp, stoch.c, 0, eta, eta_ed, temperature, temperature_ed, dt, w1, 1, W_cc, W_ed)))
-            return rc;
-        if ((rc = lin(ctx, rhs_v, 1, {{1.0, cs(stoch)}}))) return rc;
-    }
+    if ((rc = lin(ctx, rhs_v, 0, {{1.0 / dt, cs(mold)}, {-1.0, cs(gpi)}, {1.0, cs(adv)}, {0.5, cs(diff)}}))) return rc;
+    if (with_stoch &&
+        (rc = stoch_launch(ctx, sp, stoch.c, 0, eta, eta_ed, temperature, temperature_ed, dt, w1, 1, W_cc, W_ed)))
+        return rc;
     if ((rc = mass_fluxes(W_mass))) return rc;
     if ((rc = rhs_p_from_fluxes())) return rc;
     k_mul<<<nb, 256, 0, st>>>(nc, dim, mtemp, cs(rfn), cs(u));
     ctx->launches++;
-    if ((rc = lin(ctx, rhs_v, 1, {{-1.0 / dt, cs(mtemp)}}))) return rc;
-    if ((rc = diff_m(ctx, mtemp, cs(u), eta, eta_ed, kappa))) return rc;
-    if ((rc = lin(ctx, rhs_v, 1, {{0.5, cs(mtemp)}}))) return rc;
+    if (with_stoch) rc = lin(ctx, rhs_v, 1, {{1.0, cs(stoch)}, {-1.0 / dt, cs(mtemp)}, {0.5, cs(diff)}});
+    else rc = lin(ctx, rhs_v, 1, {{-1.0 / dt, cs(mtemp)}, {0.5, cs(diff)}});
+    if (rc) return rc;
     for (int s = 0; s < ns; s++) {
         if (mp) FHD_CUDA_TRY(cudaMemcpyAsync(rupd[s], fluxdiv[s], sizeof(double) * nc, cudaMemcpyDeviceToDevice, st));
         else FHD_CUDA_TRY(cudaMemsetAsync(rupd[s], 0, sizeof(double) * nc, st));
@@ -544,32 +557,30 @@ int advance_inertial_ms(fhd_ctx* ctx, const fhd_stoch_params* sp, const fhd_mixt
             constexpr int DIM = decltype(D)::value;
             k_avg_face<DIM><<<cell_grid(g), cell_block(), 0, st>>>(g, rhotot, rfn.c[0], rfn.c[1], rfn.c[2]);
         });
-        // Steps 6-7: corrector Crank-Nicolson right-hand side
-        if ((rc2 = lin(ctx, rhs_v, 0, {{1.0 / dt, cs(mold)}}))) break;
+        // Steps 6-7: corrector Crank-Nicolson right-hand side, its terms
+        // added in the reference's order by two multi-term passes (the
+        // first with the predictor's L u^n, the second with L u*)
         launch_dim([&](auto D) {
             constexpr int DIM = decltype(D)::value;
             k_grad<DIM><<<cell_grid(g), cell_block(), 0, st>>>(g, pi, gpi, dxinv);
         });
-        if ((rc2 = lin(ctx, rhs_v, 1, {{-1.0, cs(gpi)}}))) break;
         launch_dim([&](auto D) {
             constexpr int DIM = decltype(D)::value;
             k_adv_m<DIM><<<cell_grid(g), cell_block(), 0, st>>>(g, cs(u), cs(mtemp), adv, 1, dxinv);
         });
-        if ((rc2 = lin(ctx, rhs_v, 1, {{0.5, cs(adv)}}))) break;
-        if ((rc2 = lin(ctx, rhs_v, 1, {{0.5, cs(diff)}}))) break;
-        if (sp->variance_coef_mom != 0.0) {
-            if ((rc2 = stoch_launch(ctx, sp, stoch.c, 1, eta, eta_ed, temperature, temperature_ed, dt, w1, 1, W_cc,
-                                    W_ed)))
-                break;
-            if ((rc2 = lin(ctx, rhs_v, 1, {{0.5, cs(stoch)}}))) break;
-        }
+        if ((rc2 = lin(ctx, rhs_v, 0, {{1.0 / dt, cs(mold)}, {-1.0, cs(gpi)}, {0.5, cs(adv)}, {0.5, cs(diff)}})))
+            break;
+        if (with_stoch && (rc2 = stoch_launch(ctx, sp, stoch.c, 1, eta, eta_ed, temperature, temperature_ed, dt, w1,
+                                              1, W_cc, W_ed)))
+            break;
         if ((rc2 = mass_fluxes(W_mass ? W_mass + dim * ns : nullptr))) break;
         if ((rc2 = rhs_p_from_fluxes())) break;
         k_mul<<<nb, 256, 0, st>>>(nc, dim, mtemp, cs(rfn), cs(u));
         ctx->launches++;
-        if ((rc2 = lin(ctx, rhs_v, 1, {{-1.0 / dt, cs(mtemp)}}))) break;
         if ((rc2 = diff_m(ctx, diff, cs(u), eta, eta_ed, kappa))) break;
-        if ((rc2 = lin(ctx, rhs_v, 1, {{0.5, cs(diff)}}))) break;
+        if (with_stoch) rc2 = lin(ctx, rhs_v, 1, {{0.5, cs(stoch)}, {-1.0 / dt, cs(mtemp)}, {0.5, cs(diff)}});
+        else rc2 = lin(ctx, rhs_v, 1, {{-1.0 / dt, cs(mtemp)}, {0.5, cs(diff)}});
+        if (rc2) break;
         launch_dim([&](auto D) {
             constexpr int DIM = decltype(D)::value;
             k_div_inc<DIM><<<cell_grid(g), cell_block(), 0, st>>>(g, cs(u), rhs_p, dxinv);
