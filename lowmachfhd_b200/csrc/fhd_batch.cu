@@ -384,40 +384,6 @@ __global__ void __launch_bounds__(256) kb_div_plus(const Tile* tiles, int n, con
     });
 }
 
-// x_u = x_u* - alphainv G Phi (k_sub_wgrad, alphainv = 1) and x_p = -beta
-// mac_rhs + theta Phi (k_schur, kind 0, visc_type 1)
-template <typename T>
-__global__ void __launch_bounds__(256) kb_precon_out(const Tile* tiles, int n, const Lev* lev, const Ctl* ctl, int mode,
-                                                     T* const* xu, const T* Phi, const T* mac_rhs, double theta,
-                                                     double* const* x) {
-    for_tiles(tiles, n, ctl, mode, [&](const Tile& t, int q) {
-        const Lev L = lev[t.box * MAXL];
-        const int j = t.j0 + threadIdx.y;
-        if (j >= L.g.n[1]) return;
-        const T dxinv = (T)(1.0 / L.g.dx);
-        const double eta = ctl[t.box].eta;
-        const T* Ph = Phi + L.off;
-    #pragma unroll
-        for (int u = 0; u < 2; u++) {
-            const int i = t.i0 + threadIdx.x + 32 * u;
-            if (i >= L.g.n[0]) continue;
-            CellF P;
-            P.set(L.g, i, j, 0);
-            const i64 f = P.id(0, 0, 0);
-            const T pc = ld(Ph, f);
-    #pragma unroll
-            for (int c = 0; c < 2; c++) {
-                const T gp = (pc - ld(Ph, P.id(-(c == 0), -(c == 1), 0))) * dxinv;
-                x[c][L.off + f] = (double)(ld(xu[c] + L.off, f) + T(-1) * gp);
-            }
-            double v = (double)mac_rhs[L.off + f] * -1.0;
-            v = v * eta;
-            v = v + (double)pc * theta;
-            x[2][L.off + f] = v;
-        }
-    });
-}
-
 // ---------------------------------------------------------------------
 // per-box reductions: tile partials, then one warp per box in fixed order
 // ---------------------------------------------------------------------
@@ -435,6 +401,74 @@ __device__ __forceinline__ double tile_sum(double v) {
     __syncthreads();  // sh is reused by the CTA's next tile
     return s;
 }
+// three sums at once, each in tile_sum's order (valid in thread (0, 0))
+__device__ __forceinline__ void tile_sum3(double (&v)[3]) {
+    __shared__ double sh3[3][8];
+    const int t = threadIdx.x + 32 * threadIdx.y;
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        v[c] = warp_sum(v[c]);
+        if ((t & 31) == 0) sh3[c][t >> 5] = v[c];
+    }
+    __syncthreads();
+    if (t == 0)
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            double s = 0.0;
+            for (int w = 0; w < 8; w++) s += sh3[c][w];
+            v[c] = s;
+        }
+    __syncthreads();  // sh3 is reused by the CTA's next tile
+}
+
+// x_u = x_u* - alphainv G Phi (k_sub_wgrad, alphainv = 1) and x_p = -beta
+// mac_rhs + theta Phi (k_schur, kind 0, visc_type 1); with nsum > 0 also
+// the tile sums of x_p, x_u, x_v (the first nsum of them) into part[c *
+// pstride + tile], each added in the order of a separate sum pass over the
+// stored values
+template <typename T>
+__global__ void __launch_bounds__(256) kb_precon_out(const Tile* tiles, int n, const Lev* lev, const Ctl* ctl, int mode,
+                                                     T* const* xu, const T* Phi, const T* mac_rhs, double theta,
+                                                     double* const* x, int nsum, double* part, i64 pstride) {
+    for_tiles(tiles, n, ctl, mode, [&](const Tile& t, int q) {
+        const Lev L = lev[t.box * MAXL];
+        const int j = t.j0 + threadIdx.y;
+        double sm[3] = {0.0, 0.0, 0.0};
+        if (j < L.g.n[1]) {
+            const T dxinv = (T)(1.0 / L.g.dx);
+            const double eta = ctl[t.box].eta;
+            const T* Ph = Phi + L.off;
+    #pragma unroll
+            for (int u = 0; u < 2; u++) {
+                const int i = t.i0 + threadIdx.x + 32 * u;
+                if (i >= L.g.n[0]) continue;
+                CellF P;
+                P.set(L.g, i, j, 0);
+                const i64 f = P.id(0, 0, 0);
+                const T pc = ld(Ph, f);
+    #pragma unroll
+                for (int c = 0; c < 2; c++) {
+                    const T gp = (pc - ld(Ph, P.id(-(c == 0), -(c == 1), 0))) * dxinv;
+                    const double xv = (double)(ld(xu[c] + L.off, f) + T(-1) * gp);
+                    x[c][L.off + f] = xv;
+                    sm[1 + c] += xv;
+                }
+                double v = (double)mac_rhs[L.off + f] * -1.0;
+                v = v * eta;
+                v = v + (double)pc * theta;
+                x[2][L.off + f] = v;
+                sm[0] += v;
+            }
+        }
+        if (nsum > 0) {
+            tile_sum3(sm);
+            if (threadIdx.x == 0 && threadIdx.y == 0)
+    #pragma unroll
+                for (int c = 0; c < 3; c++)
+                    if (c < nsum) part[c * pstride + q] = sm[c];
+        }
+    });
+}
 
 // sum over one box's tile partials into *dst(box)
 template <class Dst>
@@ -447,16 +481,19 @@ __device__ __forceinline__ void seg_finish(const double* part, const int* t0, in
     if (lane == 0) dst(s);
 }
 
-// one warp per box: ctl[b].<field> = sum of its partials
-__global__ void __launch_bounds__(256) kb_seg_sum(int nbox, const double* part, const int* t0, Ctl* ctl, int mode,
-                                                  int which) {
-    const int box = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+// one warp per box and field: ctl[b].<field which + c> = sum of its
+// partials part[c * pstride + ..], c < ncomp
+__global__ void __launch_bounds__(256) kb_seg_sum(int nbox, const double* part, i64 pstride, int ncomp, const int* t0,
+                                                  Ctl* ctl, int mode, int which) {
+    const int wg = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int box = wg / ncomp, comp = wg % ncomp;
     if (box >= nbox || !covers(ctl[box], mode)) return;
-    seg_finish(part, t0, box, [&](double s) {
+    const int fld = which + comp;
+    seg_finish(part + comp * pstride, t0, box, [&](double s) {
         Ctl& c = ctl[box];
-        if (which < 2) c.nrm[which] = s;
-        else if (which < 5) c.mean[which - 2] = s;
-        else c.h[which - 5] = s;
+        if (fld < 2) c.nrm[fld] = s;
+        else if (fld < 5) c.mean[fld - 2] = s;
+        else c.h[fld - 5] = s;
     });
 }
 
@@ -488,39 +525,23 @@ __global__ void __launch_bounds__(256) kb_dot(const Tile* tiles, int n, const Le
     });
 }
 
-// sum of one component per tile (the null-space means)
-__global__ void __launch_bounds__(256) kb_sum(const Tile* tiles, int n, const Lev* lev, const Ctl* ctl, int mode,
-                                              const double* a, double* part) {
-    for_tiles(tiles, n, ctl, mode, [&](const Tile& t, int q) {
-        const Lev L = lev[t.box * MAXL];
-        const int j = t.j0 + threadIdx.y;
-        double s = 0.0;
-        if (j < L.g.n[1]) {
-    #pragma unroll
-            for (int u = 0; u < 2; u++) {
-                const int i = t.i0 + threadIdx.x + 32 * u;
-                if (i < L.g.n[0]) s += a[L.off + (i64)i + (i64)L.g.n[0] * j];
-            }
-        }
-        s = tile_sum(s);
-        if (threadIdx.x == 0 && threadIdx.y == 0) part[q] = s;
-    });
-}
-
-// a -= its box's mean (ctl.mean[which] / cells)
-__global__ void __launch_bounds__(256) kb_sub_mean(const Tile* tiles, int n, const Lev* lev, const Ctl* ctl, int mode,
-                                                   double* a, int which) {
+// x_p -= its box's mean (ctl.mean[0] / cells), and with ncomp = 3 also
+// x_u, x_v (ctl.mean[1], mean[2])
+__global__ void __launch_bounds__(256) kb_sub_means(const Tile* tiles, int n, const Lev* lev, const Ctl* ctl, int mode,
+                                                    double* const* x, int ncomp) {
     for_tiles(tiles, n, ctl, mode, [&](const Tile& t, int q) {
         const Lev L = lev[t.box * MAXL];
         const int j = t.j0 + threadIdx.y;
         if (j >= L.g.n[1]) return;
-        const double m = ctl[t.box].mean[which] / (double)L.g.nc;
+        const Ctl& cb = ctl[t.box];
+        const double cells = (double)L.g.nc;
+        for (int c = 0; c < ncomp; c++) {
+            const double m = cb.mean[c] / cells;
+            double* a = x[c == 0 ? 2 : c - 1] + L.off + (i64)L.g.n[0] * j;
     #pragma unroll
-        for (int u = 0; u < 2; u++) {
-            const int i = t.i0 + threadIdx.x + 32 * u;
-            if (i < L.g.n[0]) {
-                double* p = a + L.off + (i64)i + (i64)L.g.n[0] * j;
-                *p = *p - m;
+            for (int u = 0; u < 2; u++) {
+                const int i = t.i0 + threadIdx.x + 32 * u;
+                if (i < L.g.n[0]) a[i] = a[i] - m;
             }
         }
     });
@@ -1305,7 +1326,7 @@ int build(fhd_batch* B) {
     B->dvp = dalloc<double*>(B, (i64)nvec * 3);
     B->step = dalloc<double>(B, (i64)6 * B->N0);
     B->ctl = dalloc<Ctl>(B, nb);
-    B->part = dalloc<double>(B, B->ntab0);
+    B->part = dalloc<double>(B, 3 * B->ntab0);  // three fields of tile partials
     B->deta = dalloc<double>(B, nb);
     B->dabs = dalloc<double>(B, nb);
     B->dkT = dalloc<double>(B, nb);
@@ -1360,8 +1381,9 @@ int tgrid(fhd_batch* B, K kern, int n) {
 }
 
 // per-box sum of the tile partials into ctl.<which>
-int seg(fhd_batch* B, int mode, int which) {
-    kb_seg_sum<<<(B->nbox * 32 + 255) / 256, 256, 0, B->stream>>>(B->nbox, B->part, B->dt0, B->ctl, mode, which);
+int seg(fhd_batch* B, int mode, int which, int ncomp = 1) {
+    kb_seg_sum<<<(B->nbox * ncomp * 32 + 255) / 256, 256, 0, B->stream>>>(B->nbox, B->part, (i64)B->ntab0, ncomp,
+                                                                          B->dt0, B->ctl, mode, which);
     BPOST(B);
     return 0;
 }
@@ -1476,19 +1498,17 @@ int precon(fhd_batch* B, int bv, int xv, int mode, double theta) {
                                             (T*)B->crhs[0]);
     BPOST(B);
     if ((rc = cc_vcycle<T>(B, mode))) return rc;
-    kb_precon_out<T><<<tgrid(B, kb_precon_out<T>, B->ntab0), TB, 0, st>>>(B->tab0, B->ntab0, B->dlev_s, B->ctl, mode, (T* const*)B->dsphi,
-                                              (const T*)B->cphi[0], (const T*)B->crhs[0], theta, vp(B, xv));
-    BPOST(B);
-    // null space (apply_precon.f90:429-460): mean of p, and of u when theta = 0
+    // null space (apply_precon.f90:429-460): mean of p, and of u when theta
+    // = 0, summed per tile by the output pass
     const int ncomp = theta == 0.0 ? 3 : 1;
-    for (int q = 0; q < ncomp; q++) {
-        const int c = q == 0 ? 2 : q - 1;
-        kb_sum<<<tgrid(B, kb_sum, B->ntab0), TB, 0, st>>>(B->tab0, B->ntab0, B->dlev_s, B->ctl, mode, vc(B, xv, c), B->part);
-        BPOST(B);
-        if ((rc = seg(B, mode, 2 + q))) return rc;
-        kb_sub_mean<<<tgrid(B, kb_sub_mean, B->ntab0), TB, 0, st>>>(B->tab0, B->ntab0, B->dlev_s, B->ctl, mode, vc(B, xv, c), q);
-        BPOST(B);
-    }
+    kb_precon_out<T><<<tgrid(B, kb_precon_out<T>, B->ntab0), TB, 0, st>>>(
+        B->tab0, B->ntab0, B->dlev_s, B->ctl, mode, (T* const*)B->dsphi, (const T*)B->cphi[0], (const T*)B->crhs[0],
+        theta, vp(B, xv), ncomp, B->part, (i64)B->ntab0);
+    BPOST(B);
+    if ((rc = seg(B, mode, 2, ncomp))) return rc;
+    kb_sub_means<<<tgrid(B, kb_sub_means, B->ntab0), TB, 0, st>>>(B->tab0, B->ntab0, B->dlev_s, B->ctl, mode,
+                                                                  vp(B, xv), ncomp);
+    BPOST(B);
     return 0;
 }
 
