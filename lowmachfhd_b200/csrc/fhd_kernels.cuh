@@ -178,6 +178,22 @@ __device__ __forceinline__ T stag_lface_acc(const StagOp<T>& A, const CellT& P, 
         }
         if constexpr (VISC == 1) {
             diag = a + T(2 * DIM) * b * q;
+            if constexpr (sizeof(T) == 4) {
+                // FP32 (the multigrid of the mixed-precision solve): the
+                // transverse pairs summed without the leading zero and b q
+                // formed once (uniform, hoisted out of the smoother loops)
+                T o2 = T(0);
+                bool first = true;
+#pragma unroll
+                for (int d = 0; d < DIM; d++) {
+                    if (d == C) continue;
+                    const int dx_ = (d == 0), dy_ = (d == 1), dz_ = (d == 2);
+                    const T pr = own(dx_, dy_, dz_) + own(-dx_, -dy_, -dz_);
+                    o2 = first ? pr : o2 + pr;
+                    first = false;
+                }
+                return ph * diag - (own_ + o2) * (b * q);
+            }
             return ph * diag - (own_ + oth_) * b * q;
         } else if constexpr (VISC == 2) {
             diag = a + T(2 * DIM + 2) * b * q;

@@ -12,12 +12,14 @@
 //     y0-2 .. y0+TY+1, alpha and rhs rows y0-1 .. y0+TY) with 1D
 //     cp.async.bulk copies, one per array and contiguous run of rows (the
 //     periodic y wrap splits a run), completing on the stage's mbarrier;
-//   * the finished plane's TY interior rows, contiguous in shared and in
-//     global memory, leave as one bulk store;
 //   * eight compute warps update four to five cells per thread and plane
 //     step, every update one evaluation of stag_lface_acc on shared memory
-//     (the same expression as the colour kernels and the oracle); the
-//     producer warp only copies.
+//     (the same expression as the colour kernels and the oracle);
+//   * the finished plane's TY interior rows, contiguous in shared and in
+//     global memory, are written by the compute threads with 16-byte
+//     stores at the next plane step.  A bulk store from the producer warp
+//     queued behind that step's loads, and the producer then waited for it
+//     before refilling the slot; the producer warp now only loads.
 //
 // Every mbarrier wait is bounded; a wait that runs out sets *err, and the
 // CTA leaves together (after its copies in flight have landed, again with a
@@ -100,16 +102,6 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned by
                  "l"(src), "r"(bytes), "r"(smem_u32(b))
                  : "memory");
 }
-__device__ __forceinline__ void bulk_s2g(void* dst, const void* src, unsigned bytes) {
-    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;\n" ::"l"(dst), "r"(smem_u32(src)),
-                 "r"(bytes)
-                 : "memory");
-}
-__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;\n" ::: "memory"); }
-// the bulk stores issued by this thread have finished reading shared memory
-__device__ __forceinline__ void bulk_wait_read0() { asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory"); }
-// ... and have completed
-__device__ __forceinline__ void bulk_wait0() { asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory"); }
 // generic-proxy shared-memory accesses ordered before later async-proxy ones
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
 
@@ -264,10 +256,18 @@ __device__ __forceinline__ bool rbx_run(const Grid& g, const RBXGeom& G, const S
         for (int m = 0; m < NR; m++)
             if (lyb + m * RG < ly1) c0[m * ROWSTEP + lx] = nv[m];
     };
+    // the TY rows of the finished plane p, contiguous in shared and in global
+    // memory, stored by the compute threads
+    auto put_plane = [&](int p) {
+        const float4* sp = reinterpret_cast<const float4*>(ph + pmod(p - (k0 - 2) + qb, NPH) * plane + 2 * nx);
+        float4* gp = reinterpret_cast<float4*>(dst + (i64)p * nxy + (i64)y0 * nx);
+        const int n4 = (TY * nx) >> 2;
+        for (int e = tid; e < n4; e += NT) gp[e] = sp[e];
+    };
     // prologue: stages q = 0 .. 4 (unknown planes k0-2 .. k0+2, coefficient
     // planes k0-1 .. k0+1) and AHEAD more
     const bool producer = tid >= NT;
-    const int lead = NT;  // producer lane 0: stores and clean-up
+    const int lead = NT;  // producer lane 0: clean-up after a wait ran out
     if (producer) {
         for (int q = 0; q < 5 + AH && q <= qend; q++) issue(q);
         issued = 5 + AH < qend + 1 ? 5 + AH : qend + 1;
@@ -289,28 +289,23 @@ __device__ __forceinline__ bool rbx_run(const Grid& g, const RBXGeom& G, const S
     sl = slot(k0 - 1);
     scl = pmod(k0, NCF);
     for (int k = k0; k < kend; k++) {
-        // this thread's shared-memory writes of the previous step become
-        // visible to the bulk store issued below
+        // this thread's shared-memory accesses of the previous steps are
+        // ordered before the bulk copies that refill their slots
         fence_proxy_async();
         if (__syncthreads_or(!ok)) goto fail;
         if (producer) {
-            // the store of plane k-2 (issued last step) has read its slot,
-            // which stage k+3+AHEAD refills
-            if (tid == lead) bulk_wait_read0();
-            __syncwarp();
-            fence_proxy_async();
+            // stage k+3+AHEAD refills the slot of unknown plane k-2 (last
+            // read by the black update and the store of step k-1) and the
+            // coefficient slot of plane k-1
             const int qn = k + 3 + AH - (k0 - 2);
             if (qn <= qend) {
                 issue(qn);
                 issued = qn + 1;
             }
-            if (tid == lead && k > k0) {
-                const float* sp = ph + pmod(k - 1 - (k0 - 2) + qb, NPH) * plane + 2 * nx;
-                bulk_s2g(dst + (i64)(k - 1) * nxy + (i64)y0 * nx, sp, (unsigned)(sizeof(float) * TY * nx));
-                bulk_commit();
-            }
             continue;
         }
+        // plane k-1 is final since the black update of step k-1
+        if (k > k0) put_plane(k - 1);
         // stage k+3: unknown plane k+3, coefficient plane k+2
         if (k + 3 - (k0 - 2) <= qend) ok = wait_stage(k + 3 - (k0 - 2));
         if (!ok) continue;  // leaves at the next barrier
@@ -323,11 +318,9 @@ __device__ __forceinline__ bool rbx_run(const Grid& g, const RBXGeom& G, const S
     }
     fence_proxy_async();
     if (__syncthreads_or(!ok)) goto fail;
-    if (tid == lead) {
-        const float* sp = ph + pmod(kend - 1 - (k0 - 2) + qb, NPH) * plane + 2 * nx;
-        bulk_s2g(dst + (i64)(kend - 1) * nxy + (i64)y0 * nx, sp, (unsigned)(sizeof(float) * TY * nx));
-        bulk_commit();
-        bulk_wait0();
+    if (!producer) {
+        put_plane(kend - 1);
+        fence_proxy_async();  // before the next run's copies refill the slot
     }
     nstages = qend + 1;
     return true;
@@ -336,7 +329,6 @@ fail:
     // land (bounded) and leave
     if (tid == lead) {
         atomicOr(R.err, 1u);
-        bulk_wait0();
         // stages before the last NPH issued completed before their
         // barriers were re-armed
         for (int q = issued > NPH ? issued - NPH : 0; q < issued; q++) wait_stage(q);
@@ -367,8 +359,8 @@ __global__ void __launch_bounds__(NT + 32, AH == 1 ? 2 : 1) k_stag_rbx(Grid g, R
         const int k0 = (int)(s % nz);
         const int kend = (int)(e - s < (long)(nz - k0) ? k0 + (e - s) : nz);
         const int comp = (int)(item % 3), tile_y = (int)(item / 3);
-        // the previous run's last store has read its slot, and every thread
-        // is done with the staged planes, before this run refills them
+        // every thread is done with the staged planes (the previous run's
+        // last plane stored from its slot) before this run refills them
         if (!first) __syncthreads();
         int n = 0;
         bool ok;
@@ -424,10 +416,15 @@ inline bool rbx_geom(const Grid& g, int sms, size_t smem_max, RBXGeom& G, int ty
     G.crows = G.TY + 2;
     G.tiles_y = ny / G.TY;
     // CTAs of the launch: each takes a stretch of the tiles_y * 3 * nz plane
-    // steps (rbx_cut).  The grid with the fewest plane steps on the busiest
-    // SM wins, a z-run's prologue counted as five plane steps: one CTA per
-    // resident slot (stretches cross item edges), or c equal z-runs per item
-    // (one item per CTA, in waves when they outnumber the slots).
+    // steps (rbx_cut).  Candidates: c equal z-runs per item (one item per
+    // CTA, in waves when they outnumber the slots), or one CTA per resident
+    // slot with stretches that cross item edges.  The cost is the plane steps
+    // on the busiest SM, a z-run's prologue counted as five.  With equal
+    // z-runs the CTAs of neighbouring row tiles march in step, so the halo
+    // rows that both stage are read from DRAM once; stretches desynchronise
+    // them and the halo rows are read again (about a quarter more DRAM
+    // traffic at 8-row tiles).  Stretches are therefore taken only when they
+    // save a tenth of the plane steps.
     const long items = (long)G.tiles_y * 3;
     const long work = items * nz;
     const long slots = (long)sms * G.per_sm;
@@ -456,8 +453,14 @@ inline bool rbx_geom(const Grid& g, int sms, size_t smem_max, RBXGeom& G, int ty
             bestP = P;
         }
     };
-    consider(slots);
     for (int c = 1; c <= nz / 4; c++) consider(items * c);
+    if (slots % items != 0 && work >= slots * RBX_MINRUN) {
+        const long cs = cost_of(slots);
+        if (best < 0 || 10 * cs <= 9 * best) {
+            best = cs;
+            bestP = slots;
+        }
+    }
     if (bestP < 1) return false;
     G.chunks = (int)bestP;
     G.KZ = (int)((work + G.chunks - 1) / G.chunks);  // plane steps of the longest stretch
