@@ -307,7 +307,16 @@ int fhd_dev_gmres(fhd_ctx* ctx,
  *       (index r*6 + 2*edge_set + comp, edge sets xy, xz, yz).
  * The random arrays follow fill_m_stochastic (stochastic_m_fluxdiv.f90:
  * 781-860): for the symmetric form the cell entries carry variance 2 and
- * comp 1 of every edge entry equals comp 0. */
+ * comp 1 of every edge entry equals comp 0.
+ * Walls (fhd_ctx_create_bc codes 100, 200): an edge set that contains a
+ * wall direction d (2D: the nodes contain x and y; 3D: xy, xz, yz) has
+ * n[d] + 1 planes in d, the last one on the high wall; the arrays W_ed,
+ * eta_ed and temperature_ed of that set have these extents (x fastest).
+ * The edges on a no-slip wall are multiplied by sqrt(2), those on a slip
+ * wall set to zero (mflux_bc_2d / _3d, stochastic_m_fluxdiv.f90:363-451),
+ * and the normal component of force on a wall face is set to zero
+ * (multifab_physbc_domainvel), with or without increment.  The host-fab
+ * entry fhd_stochastic_m_fluxdiv refuses walls. */
 int fhd_dev_stochastic_m_fluxdiv(fhd_ctx* ctx, const fhd_stoch_params* sp,
                                  double* const force[], int increment,
                                  const double* eta, const double* const eta_ed[],
@@ -371,7 +380,12 @@ int fhd_dev_compute_sqrtLonsager_fc(fhd_ctx* ctx, const fhd_mixture_params* mp,
  * to stoch_mass_fluxdiv[i] or added to it when increment (increment_in).
  * W_fc[(r*dim+d)*nspecies+i] as in fhd_dev_compute_mass_fluxdiv.
  * stoch_mass_flux (nullable): dim*nspecies face arrays [d*ns+i] receiving the
- * flux.  FP64.  nspecies 2..5, n_rngs 1..4. */
+ * flux.  FP64.  nspecies 2..5, n_rngs 1..4.
+ * Walls (fhd_ctx_create_bc codes 100, 200): the flux through a wall face is
+ * zero (stoch_mass_bc, stochastic_mass_fluxdiv.f90:216-368); the face
+ * arrays keep the periodic layout (face 0 of a wall direction is the low
+ * wall, the high wall face is not stored).  The host-fab entry
+ * fhd_stochastic_mass_fluxdiv refuses walls. */
 int fhd_dev_stochastic_mass_fluxdiv(fhd_ctx* ctx, const fhd_mixture_params* mp,
                                     const fhd_stoch_params* sp,
                                     const double* const sqrtLonsager_fc[],

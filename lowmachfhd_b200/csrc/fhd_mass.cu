@@ -1219,6 +1219,22 @@ static int sqrtL_fc_T(fhd_ctx* ctx, const MixDev& m, const double* const rho[], 
     return 0;
 }
 
+// plane 0 of direction d of up to FHD_MAX_SPECIES face arrays set to zero
+struct WallPlane {
+    double* a[FHD_MAX_SPECIES];
+};
+__global__ void k_zero_plane(Grid g, int d, int n, WallPlane w) {
+    const i64 t = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    const int u = d == 0 ? 1 : 0, v = d == 2 ? 1 : 2;  // the other two directions
+    const i64 nu = g.n[u];
+    if (t >= nu * g.n[v]) return;
+    int q[3] = {0, 0, 0};
+    q[u] = (int)(t % nu);
+    q[v] = (int)(t / nu);
+    const i64 f = (i64)q[0] + (i64)g.n[0] * ((i64)q[1] + (i64)g.n[1] * q[2]);
+    for (int s = 0; s < n; s++) w.a[s][f] = 0.0;
+}
+
 template <int NS>
 static int stoch_mass_T(fhd_ctx* ctx, const MixDev& m, const double* const sqrtL[], double dt, const double* weights,
                         int n_rngs, const double* const W[], int increment, double* const div[],
@@ -1237,6 +1253,16 @@ static int stoch_mass_T(fhd_ctx* ctx, const MixDev& m, const double* const sqrtL
         k_stoch_mass_flux<NS><<<cell_grid(g), cell_block(), 0, ctx->stream>>>(g, m, n_rngs, variance, a);
         ctx->launches++;
         FHD_CUDA_TRY(cudaPeekAtLastError());
+        if (ctx->has_walls && ctx->walls.lo[d] != 0) {
+            // stoch_mass_bc (stochastic_mass_fluxdiv.f90:216-368): no flux
+            // through a wall face (the high wall face, not stored, reads as
+            // face 0 in the divergence's periodic wrap)
+            WallPlane wp;
+            for (int sp = 0; sp < NS; sp++) wp.a[sp] = flux[d * NS + sp];
+            k_zero_plane<<<dim3((ctx->g0.nc / g.n[d] + 255) / 256), 256, 0, ctx->stream>>>(g, d, NS, wp);
+            ctx->launches++;
+            FHD_CUDA_TRY(cudaPeekAtLastError());
+        }
     }
     DivArgs a;
     memset(&a, 0, sizeof(a));
@@ -1286,7 +1312,6 @@ extern "C" int fhd_dev_stochastic_mass_fluxdiv(fhd_ctx* ctx, const fhd_mixture_p
                                                const double* const W_fc[], int increment,
                                                double* const stoch_mass_fluxdiv[],
                                                double* const stoch_mass_flux[]) {
-    if (int wr = refuse_walls(ctx, "fhd_dev_stochastic_mass_fluxdiv")) return wr;
     if (!ctx || !mp || !sp || !sqrtLonsager_fc || !weights || !W_fc || !stoch_mass_fluxdiv || !(dt > 0.0))
         return FHD_ERR_BAD_ARG;
     if (n_rngs < 1 || n_rngs > 4) {

@@ -301,8 +301,7 @@ struct fhd_ctx {
 // the timestep and stochastic-flux entries are built for periodic boxes
 inline int refuse_walls(const fhd_ctx* ctx, const char* what) {
     if (!ctx || !ctx->has_walls) return 0;
-    fhd::set_last_error(std::string(what) + ": the context has walls; the timesteps and stochastic fluxes are built "
-                                       "for periodic boxes");
+    fhd::set_last_error(std::string(what) + ": the context has walls; this entry is built for periodic boxes");
     return FHD_ERR_UNSUPPORTED;
 }
 

@@ -72,6 +72,77 @@ __global__ void __launch_bounds__(256) k_stoch_m(Grid g, StochArgs a, double* o0
     for (int c = 0; c < DIM; c++) o[c][f] = increment ? o[c][f] + (double)dv[c] : (double)dv[c];
 }
 
+// Walls (fhd_walls.cuh): edge set e (2D the nodes; 3D xy, xz, yz) has one
+// more plane in a wall direction of the set, holding the edges on the high
+// wall; ext[e] are its extents.
+struct EdgeExt {
+    int ext[3][3];
+};
+__device__ __forceinline__ void edge_dirs_d(int dim, int e, int& a, int& b) {
+    a = (dim == 3 && e == 2) ? 1 : 0;
+    b = (dim == 3 && e != 0) ? 2 : 1;
+}
+// the scaled random stress on edge (i, j, k) of set e with the wall rules
+// of mflux_bc_2d / _3d (stochastic_m_fluxdiv.f90:363-451): times sqrt(2) on
+// a no-slip wall, zero on a slip wall, the boundaries of x, then y, then z
+template <typename T, int DIM>
+__device__ __forceinline__ T stoch_ed_w(const StochArgs& a, const Grid& g, const fhd::Walls& W, const EdgeExt& X,
+                                        int e, int comp, int i, int j, int k) {
+    constexpr int nE = DIM == 2 ? 1 : 3;
+    int da, db;
+    edge_dirs_d(DIM, e, da, db);
+    int q[3] = {i, j, k};
+#pragma unroll
+    for (int d = 0; d < 3; d++)
+        if (X.ext[e][d] == g.n[d]) q[d] = wrapc(q[d], g.n[d]);
+    const i64 f = (i64)q[0] + (i64)X.ext[e][0] * ((i64)q[1] + (i64)X.ext[e][1] * q[2]);
+    T v = stoch_ed<T>(a, nE, e, comp, f);
+    const int ds[2] = {da, db};
+#pragma unroll
+    for (int t = 0; t < 2; t++) {
+        const int d = ds[t];
+        if (W.lo[d] == 0) continue;
+        const int side = q[d] == 0 ? W.lo[d] : (q[d] == g.n[d] ? W.hi[d] : 0);
+        if (side < 0) v = (T)1.4142135623730951 * v;
+        else if (side > 0) v = T(0);
+    }
+    return v;
+}
+
+// k_stoch_m with walls: edges through stoch_ed_w, and the normal component
+// on a wall face zero (multifab_physbc_domainvel), increment or not
+template <typename T, int DIM>
+__global__ void __launch_bounds__(256) k_stoch_m_w(Grid g, fhd::Walls W, EdgeExt X, StochArgs a, double* o0,
+                                                   double* o1, double* o2, int increment) {
+    Cell P;
+    if (!cell_of_thread(g, P)) return;
+    const i64 f = P.id(0, 0, 0);
+    const T dxi = (T)a.dxinv;
+    const int i = P.i, j = P.j, k = P.k;
+    auto E = [&](int e, int comp, int ii, int jj, int kk) { return stoch_ed_w<T, DIM>(a, g, W, X, e, comp, ii, jj, kk); };
+    T dv[3];
+    if constexpr (DIM == 2) {
+        dv[0] = (stoch_cc<T>(a, 2, 0, f) - stoch_cc<T>(a, 2, 0, P.id(-1, 0, 0))) * dxi +
+                (E(0, 0, i, j + 1, k) - E(0, 0, i, j, k)) * dxi;
+        dv[1] = (E(0, 1, i + 1, j, k) - E(0, 1, i, j, k)) * dxi +
+                (stoch_cc<T>(a, 2, 1, f) - stoch_cc<T>(a, 2, 1, P.id(0, -1, 0))) * dxi;
+    } else {
+        dv[0] = (stoch_cc<T>(a, 3, 0, f) - stoch_cc<T>(a, 3, 0, P.id(-1, 0, 0))) * dxi +
+                (E(0, 0, i, j + 1, k) - E(0, 0, i, j, k)) * dxi + (E(1, 0, i, j, k + 1) - E(1, 0, i, j, k)) * dxi;
+        dv[1] = (E(0, 1, i + 1, j, k) - E(0, 1, i, j, k)) * dxi +
+                (stoch_cc<T>(a, 3, 1, f) - stoch_cc<T>(a, 3, 1, P.id(0, -1, 0))) * dxi +
+                (E(2, 0, i, j, k + 1) - E(2, 0, i, j, k)) * dxi;
+        dv[2] = (E(1, 1, i + 1, j, k) - E(1, 1, i, j, k)) * dxi + (E(2, 1, i, j + 1, k) - E(2, 1, i, j, k)) * dxi +
+                (stoch_cc<T>(a, 3, 2, f) - stoch_cc<T>(a, 3, 2, P.id(0, 0, -1))) * dxi;
+    }
+    double* o[3] = {o0, o1, o2};
+#pragma unroll
+    for (int c = 0; c < DIM; c++) {
+        if (fhd::on_wall(W, c, i, j, k)) o[c][f] = 0.0;
+        else o[c][f] = increment ? o[c][f] + (double)dv[c] : (double)dv[c];
+    }
+}
+
 int stoch_launch(fhd_ctx* ctx, const fhd_stoch_params* sp, double* const force[], int increment, const double* eta,
                  const double* const eta_ed[], const double* T, const double* const T_ed[], double dt,
                  const double* weights, int n_rngs, const double* const W_cc[], const double* const W_ed[]) {
@@ -97,6 +168,26 @@ int stoch_launch(fhd_ctx* ctx, const fhd_stoch_params* sp, double* const force[]
     const Grid g = ctx->g0;
     double* f2 = dim == 3 ? force[2] : nullptr;
     const bool mixed = ctx->prec == FHD_PREC_MIXED;
+    if (ctx->has_walls) {
+        EdgeExt X;
+        for (int e = 0; e < 3; e++) {
+            const int da = (dim == 3 && e == 2) ? 1 : 0, db = (dim == 3 && e != 0) ? 2 : 1;
+            for (int d = 0; d < 3; d++)
+                X.ext[e][d] = g.n[d] + ((d == da || d == db) && d < dim && ctx->walls.lo[d] != 0 ? 1 : 0);
+        }
+        with_dim(dim, [&](auto D) {
+            constexpr int DIM = decltype(D)::value;
+            if (mixed)
+                k_stoch_m_w<float, DIM><<<cell_grid(g), cell_block(), 0, ctx->stream>>>(g, ctx->walls, X, a, force[0],
+                                                                                      force[1], f2, increment);
+            else
+                k_stoch_m_w<double, DIM><<<cell_grid(g), cell_block(), 0, ctx->stream>>>(g, ctx->walls, X, a, force[0],
+                                                                                       force[1], f2, increment);
+        });
+        ctx->launches++;
+        FHD_CUDA_TRY(cudaPeekAtLastError());
+        return 0;
+    }
     with_dim(dim, [&](auto D) {
         constexpr int DIM = decltype(D)::value;
         if (mixed)
@@ -769,7 +860,6 @@ int fhd_dev_stochastic_m_fluxdiv(fhd_ctx* ctx, const fhd_stoch_params* sp, doubl
                                  const double* eta, const double* const eta_ed[], const double* temperature,
                                  const double* const temperature_ed[], double dt, const double* weights, int n_rngs,
                                  const double* const W_cc[], const double* const W_ed[]) {
-    if (int wr = refuse_walls(ctx, "fhd_dev_stochastic_m_fluxdiv")) return wr;
     if (!ctx || !sp || !force || !eta || !eta_ed || !temperature || !temperature_ed || !weights || !W_cc || !W_ed)
         return FHD_ERR_BAD_ARG;
     int rc = stoch_launch(ctx, sp, force, increment, eta, eta_ed, temperature, temperature_ed, dt, weights, n_rngs,

@@ -61,6 +61,33 @@ struct Geo {
     }
 };
 
+// Extents of edge set e (edge_dirs): n[d], plus one in a wall direction d
+// of the set, whose last plane holds the edges on the high wall (the
+// reference's nodal multifab has hi+1 there and draws independent values
+// for it).
+inline void edge_ext(const Geo& g, int e, long m[3]) {
+    int a = 0, b = 1;
+    if (g.dim == 3) { a = e == 2 ? 1 : 0; b = e == 0 ? 1 : 2; }
+    for (int d = 0; d < 3; d++) m[d] = g.n[d] + ((d == a || d == b) && g.wall(d) ? 1 : 0);
+}
+inline long edge_count(const Geo& g, int e) {
+    long m[3];
+    edge_ext(g, e, m);
+    return m[0] * m[1] * m[2];
+}
+// index of edge (i, j, k) of set e: periodic directions wrap, wall
+// directions of the set take 0 .. n[d]
+inline long edge_id(const Geo& g, int e, int i, int j, int k) {
+    long m[3];
+    edge_ext(g, e, m);
+    int q[3] = {i, j, k};
+    for (int d = 0; d < 3; d++) {
+        if (m[d] != g.n[d]) continue;
+        if (q[d] < 0) q[d] += g.n[d]; else if (q[d] >= g.n[d]) q[d] -= g.n[d];
+    }
+    return q[0] + m[0] * (q[1] + m[1] * (long)q[2]);
+}
+
 // Velocity component c at face (i, j, k), which may lie one face beyond the
 // domain: the ghost-cell rules of multifab_physbc_domainvel and
 // multifab_physbc_macvel (multifab_physbc_stag.f90:91-173, 957-1116), homogeneous.
@@ -112,6 +139,13 @@ inline int edge_of(int dim, int c, int d) {
 }
 
 inline int n_edge(int dim) { return dim == 2 ? 1 : 3; }
+
+// Edge set e of a dim-D grid: its two nodal directions a < b (2D: the
+// nodes, x and y; 3D: xy, xz, yz).
+inline void edge_dirs(int dim, int e, int& a, int& b) {
+    if (dim == 2) { a = 0; b = 1; }
+    else { a = e == 2 ? 1 : 0; b = e == 0 ? 1 : 2; }
+}
 
 template <class F>
 inline void forall(const Geo& g, F f) {
@@ -1278,39 +1312,73 @@ int stoch_m_impl(const Geo& g, const fhd_stoch_params* sp, double* const force[]
     const int dim = g.dim, nE = n_edge(dim);
     const long nc = g.nc;
     if (sp->filtering_width != 0) return FHD_ERR_UNSUPPORTED;
-    std::vector<Vec> fcc(dim, Vec(nc, 0.0)), fed(2 * nE, Vec(nc, 0.0));
+    long ne[3] = {0, 0, 0};
+    for (int e = 0; e < nE; e++) ne[e] = edge_count(g, e);
+    std::vector<Vec> fcc(dim, Vec(nc, 0.0)), fed(2 * nE);
+    for (int e = 0; e < 2 * nE; e++) fed[e].assign(ne[e / 2], 0.0);
     for (int r = 0; r < n_rngs; r++) {
         for (int c = 0; c < dim; c++)
             for (long f = 0; f < nc; f++) fcc[c][f] = fcc[c][f] + weights[r] * W_cc[r * dim + c][f];
         for (int e = 0; e < 2 * nE; e++)
-            for (long f = 0; f < nc; f++) fed[e][f] = fed[e][f] + weights[r] * W_ed[r * 2 * nE + e][f];
+            for (long f = 0; f < ne[e / 2]; f++) fed[e][f] = fed[e][f] + weights[r] * W_ed[r * 2 * nE + e][f];
     }
     const double variance = std::sqrt(sp->variance_coef_mom * 2.0 * sp->k_B / (sp->dV * dt));
     for (int c = 0; c < dim; c++)
         for (long f = 0; f < nc; f++) fcc[c][f] = (variance * fcc[c][f]) * std::sqrt(eta[f] * T[f]);
     for (int e = 0; e < nE; e++)
         for (int comp = 0; comp < 2; comp++)
-            for (long f = 0; f < nc; f++)
+            for (long f = 0; f < ne[e]; f++)
                 fed[2 * e + comp][f] = (variance * fed[2 * e + comp][f]) * std::sqrt(eta_ed[e][f] * T_ed[e][f]);
+    if (g.any_wall()) {
+        // mflux_bc_2d / _3d (stochastic_m_fluxdiv.f90:363-451): the edges on a
+        // no-slip wall times sqrt(2), on a slip wall zero; the boundaries of
+        // x, then y, then z, each low side before its high side
+        for (int e = 0; e < nE; e++) {
+            int a, b;
+            edge_dirs(dim, e, a, b);
+            long m[3];
+            edge_ext(g, e, m);
+            for (long f = 0; f < ne[e]; f++) {
+                const int q[3] = {(int)(f % m[0]), (int)((f / m[0]) % m[1]), (int)(f / (m[0] * m[1]))};
+                for (int d : {a, b}) {
+                    if (!g.wall(d)) continue;
+                    int side = 0;
+                    if (q[d] == 0) side = g.wl[d];
+                    else if (q[d] == g.n[d]) side = g.wh[d];
+                    if (side == 0) continue;
+                    for (int comp = 0; comp < 2; comp++) {
+                        double& v = fed[2 * e + comp][f];
+                        v = side < 0 ? std::sqrt(2.0) * v : 0.0;
+                    }
+                }
+            }
+        }
+    }
     const double dxinv = 1.0 / g.dx;
+    auto E = [&](int e, int comp, int i, int j, int k) { return fed[2 * e + comp][edge_id(g, e, i, j, k)]; };
     forall(g, [&](int i, int j, int k) {
         long f = g.id(i, j, k);
         double dv[3];
         if (dim == 2) {
             // stoch_m_force_2d (stochastic_m_fluxdiv.f90:453-506)
-            dv[0] = (fcc[0][f] - fcc[0][g.id(i - 1, j, k)]) * dxinv + (fed[0][g.id(i, j + 1, k)] - fed[0][f]) * dxinv;
-            dv[1] = (fed[1][g.id(i + 1, j, k)] - fed[1][f]) * dxinv + (fcc[1][f] - fcc[1][g.id(i, j - 1, k)]) * dxinv;
+            dv[0] = (fcc[0][f] - fcc[0][g.id(i - 1, j, k)]) * dxinv + (E(0, 0, i, j + 1, k) - E(0, 0, i, j, k)) * dxinv;
+            dv[1] = (E(0, 1, i + 1, j, k) - E(0, 1, i, j, k)) * dxinv + (fcc[1][f] - fcc[1][g.id(i, j - 1, k)]) * dxinv;
         } else {
             // stoch_m_force_3d (stochastic_m_fluxdiv.f90:508-600); edge
             // arrays fed[2e+comp] for e = xy, xz, yz
-            dv[0] = (fcc[0][f] - fcc[0][g.id(i - 1, j, k)]) * dxinv + (fed[0][g.id(i, j + 1, k)] - fed[0][f]) * dxinv
-                  + (fed[2][g.id(i, j, k + 1)] - fed[2][f]) * dxinv;
-            dv[1] = (fed[1][g.id(i + 1, j, k)] - fed[1][f]) * dxinv + (fcc[1][f] - fcc[1][g.id(i, j - 1, k)]) * dxinv
-                  + (fed[4][g.id(i, j, k + 1)] - fed[4][f]) * dxinv;
-            dv[2] = (fed[3][g.id(i + 1, j, k)] - fed[3][f]) * dxinv + (fed[5][g.id(i, j + 1, k)] - fed[5][f]) * dxinv
+            dv[0] = (fcc[0][f] - fcc[0][g.id(i - 1, j, k)]) * dxinv + (E(0, 0, i, j + 1, k) - E(0, 0, i, j, k)) * dxinv
+                  + (E(1, 0, i, j, k + 1) - E(1, 0, i, j, k)) * dxinv;
+            dv[1] = (E(0, 1, i + 1, j, k) - E(0, 1, i, j, k)) * dxinv + (fcc[1][f] - fcc[1][g.id(i, j - 1, k)]) * dxinv
+                  + (E(2, 0, i, j, k + 1) - E(2, 0, i, j, k)) * dxinv;
+            dv[2] = (E(1, 1, i + 1, j, k) - E(1, 1, i, j, k)) * dxinv + (E(2, 1, i, j + 1, k) - E(2, 1, i, j, k)) * dxinv
                   + (fcc[2][f] - fcc[2][g.id(i, j, k - 1)]) * dxinv;
         }
-        for (int c = 0; c < dim; c++) force[c][f] = increment ? force[c][f] + dv[c] : dv[c];
+        const int q[3] = {i, j, k};
+        for (int c = 0; c < dim; c++) {
+            // multifab_physbc_domainvel: the normal component on a wall face is zero
+            if (g.wall(c) && q[c] == 0) force[c][f] = 0.0;
+            else force[c][f] = increment ? force[c][f] + dv[c] : dv[c];
+        }
     });
     return 0;
 }
@@ -1961,6 +2029,7 @@ int step_impl(const Geo& g, int visc_type, const fhd_gmres_params* p_in, const f
               const double* eta, const double* const eta_ed[], const double* kappa, const double* temperature,
               const double* const temperature_ed[], const double* const W_cc[], const double* const W_ed[],
               const double* const W_mass[], fhd_solve_stats* stats2) {
+    if (g.any_wall()) return FHD_ERR_UNSUPPORTED;  // the timesteps are built for periodic boxes
     const int dim = g.dim;
     const long nc = g.nc;
     const int nE = n_edge(dim);
@@ -2163,6 +2232,7 @@ int overdamped_impl(const Geo& g, int visc_type, const fhd_gmres_params* p_in, c
                     const double* eta, const double* const eta_ed[], const double* kappa, const double* temperature,
                     const double* const temperature_ed[], const double* const W_cc[], const double* const W_ed[],
                     const double* const W_mass[], fhd_solve_stats* stats2) {
+    if (g.any_wall()) return FHD_ERR_UNSUPPORTED;  // the timesteps are built for periodic boxes
     const int dim = g.dim;
     const long nc = g.nc;
     const int nE = n_edge(dim);
@@ -2402,10 +2472,14 @@ void or_stochastic_mass_fluxdiv(int dim, const int n[3], double dx, const fhd_st
         forall(g, [&](int i, int j, int k) {
             const long f = g.id(i, j, k);
             double w[FHD_MAX_SPECIES], fs[FHD_MAX_SPECIES];
+            // stoch_mass_bc (stochastic_mass_fluxdiv.f90:216-368): the random
+            // field is zero on a wall face (no-slip or slip)
+            const int q[3] = {i, j, k};
+            const bool on_wall = g.wall(d) && q[d] == 0;
             for (int s = 0; s < ns; s++) {
                 double acc = 0.0;
                 for (int rr = 0; rr < n_rngs; rr++) acc = acc + weights[rr] * W_fc[(rr * dim + d) * ns + s][f];
-                w[s] = acc;
+                w[s] = on_wall ? 0.0 : acc;
             }
             for (int r = 0; r < ns; r++) {
                 double acc = 0.0;

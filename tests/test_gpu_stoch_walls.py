@@ -1,0 +1,101 @@
+"""Walls in the stochastic fluxes through the C ABI against the oracle:
+fhd_dev_stochastic_m_fluxdiv (mflux_bc_2d / _3d, stochastic_m_fluxdiv.f90:
+363-451, the high wall's edge planes, zero normal force on wall faces) and
+fhd_dev_stochastic_mass_fluxdiv (stoch_mass_bc, stochastic_mass_fluxdiv.f90:
+216-368), FP64 and mixed; the host-fab entries refuse walls."""
+import numpy as np
+import pytest
+
+import lowmachfhd_b200 as L
+import oracle as O
+from tests import problems as P
+from tests.test_gpu_parity import dev, host
+from tests.test_oracle_stoch_walls import SP, W8, fields
+
+pytestmark = pytest.mark.gpu
+
+NS, SL, PE = L.FHD_BC_NO_SLIP_WALL, L.FHD_BC_SLIP_WALL, L.FHD_BC_PERIODIC
+
+CASES = [
+    (2, [16, 8], [PE, NS, PE], [PE, NS, PE]),
+    (2, [8, 16], [SL, PE, PE], [NS, PE, PE]),
+    (2, [16, 16], [NS, SL, PE], [SL, NS, PE]),
+    (3, [8, 8, 8], [PE, PE, NS], [PE, PE, NS]),
+    (3, [16, 8, 8], [NS, SL, PE], [NS, SL, PE]),
+    (3, [8, 8, 8], [NS, NS, SL], [SL, NS, NS]),
+]
+
+
+@pytest.fixture(autouse=True)
+def periodic_afterwards():
+    yield
+    O.set_walls()
+
+
+def solver(dim, n, bc_lo, bc_hi, precision="fp64"):
+    return L.StokesSolver(dim, n, 0.5, 1, precision=precision, bc_lo=bc_lo, bc_hi=bc_hi)
+
+
+@pytest.mark.parametrize("dim,n,bc_lo,bc_hi", CASES)
+@pytest.mark.parametrize("increment", [False, True])
+def test_stochastic_m_fluxdiv_walls(cuda, dim, n, bc_lo, bc_hi, increment):
+    nc = P.nc_of(dim, n)
+    eta, T, eta_ed, T_ed, W_cc, W_ed = fields(dim, n, bc_lo, 11)
+    force0 = [np.random.default_rng(12).standard_normal(nc) for _ in range(dim)]
+    O.set_walls(bc_lo, bc_hi)
+    ref = O.stochastic_m_fluxdiv(dim, n, 0.5, O.StochParams(**SP), eta, eta_ed, T, T_ed, 0.1, W8, W_cc, W_ed,
+                                 force=force0, increment=increment)
+    with solver(dim, n, bc_lo, bc_hi) as s:
+        f = dev(force0, cuda)
+        s.stochastic_m_fluxdiv(L.StochParams(**SP), f, increment, dev(eta, cuda), dev(eta_ed, cuda), dev(T, cuda),
+                               dev(T_ed, cuda), 0.1, W8, dev(W_cc, cuda), dev(W_ed, cuda))
+    assert P.rel_inf(host(f), ref) < 1e-13
+
+
+def test_stochastic_m_fluxdiv_walls_mixed(cuda):
+    """the FP32 arithmetic of a mixed-precision context: relative error of
+    FP32 roundoff on the summed stress"""
+    dim, n, bc_lo, bc_hi = 3, [16, 8, 8], [NS, SL, PE], [NS, SL, PE]
+    nc = P.nc_of(dim, n)
+    eta, T, eta_ed, T_ed, W_cc, W_ed = fields(dim, n, bc_lo, 13)
+    O.set_walls(bc_lo, bc_hi)
+    ref = O.stochastic_m_fluxdiv(dim, n, 0.5, O.StochParams(**SP), eta, eta_ed, T, T_ed, 0.1, W8, W_cc, W_ed)
+    with solver(dim, n, bc_lo, bc_hi, precision="mixed") as s:
+        f = dev([np.zeros(nc) for _ in range(dim)], cuda)
+        s.stochastic_m_fluxdiv(L.StochParams(**SP), f, False, dev(eta, cuda), dev(eta_ed, cuda), dev(T, cuda),
+                               dev(T_ed, cuda), 0.1, W8, dev(W_cc, cuda), dev(W_ed, cuda))
+    got = host(f)
+    assert P.rel_inf(got, ref) < 1e-5
+    for c in range(2):  # the wall faces stay exactly zero
+        a = got[c].reshape(8, 8, 16)
+        assert np.all((a[:, :, 0] if c == 0 else a[:, 0, :]) == 0.0)
+
+
+@pytest.mark.parametrize("dim,n,bc_lo,bc_hi", [CASES[0], CASES[2], CASES[4], CASES[5]])
+def test_stochastic_mass_fluxdiv_walls(cuda, dim, n, bc_lo, bc_hi):
+    ns = 3
+    nc = P.nc_of(dim, n)
+    rng = np.random.default_rng(14)
+    sqrtL = [rng.standard_normal(nc) for _ in range(dim * ns * ns)]
+    W_fc = [rng.standard_normal(nc) for _ in range(2 * dim * ns)]
+    div0 = [rng.standard_normal(nc) for _ in range(ns)]
+    spk = dict(k_B=1.0, variance_coef_mom=1.0, dV=1.0, stoch_stress_form=1, filtering_width=0)
+    O.set_walls(bc_lo, bc_hi)
+    ref_div, ref_flux = O.stochastic_mass_fluxdiv(dim, n, 0.5, O.StochParams(**spk),
+                                                  O.mixture_params([1.0, 2.0, 3.0], [1.0, 0.5, 2.0]), sqrtL, 0.1,
+                                                  W8, W_fc, increment=True, div0=div0, want_flux=True)
+    with solver(dim, n, bc_lo, bc_hi) as s:
+        div = dev(div0, cuda)
+        flux = dev([np.zeros(nc) for _ in range(dim * ns)], cuda)
+        s.stochastic_mass_fluxdiv(L.mixture_params([1.0, 2.0, 3.0], [1.0, 0.5, 2.0]), L.StochParams(**spk),
+                                  dev(sqrtL, cuda), 0.1, W8, dev(W_fc, cuda), div, flux, increment=True)
+    assert P.rel_inf(host(div), ref_div) < 1e-12
+    assert P.rel_inf(host(flux), ref_flux) < 1e-12
+
+
+def test_host_fab_entries_refuse_walls(cuda):
+    with solver(2, [16, 16], [PE, NS, PE], [PE, NS, PE]) as s:
+        assert L._capi.lib().fhd_stochastic_m_fluxdiv(s._h, None, None, 0, None, None, None, None, 0.1, None, 1,
+                                                     None, None) == L._capi.FHD_ERR_UNSUPPORTED
+        assert L._capi.lib().fhd_stochastic_mass_fluxdiv(s._h, None, None, None, None, None, None, None, 0.1,
+                                                        None, 1, None, 0) == L._capi.FHD_ERR_UNSUPPORTED

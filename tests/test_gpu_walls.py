@@ -154,13 +154,14 @@ def test_one_sided_periodic_is_refused(cuda):
 
 
 def test_timestep_entries_refuse_walls(cuda):
-    """the stochastic flux and timestep entries are built for periodic boxes"""
+    """the timestep entries are built for periodic boxes: refused before any
+    array is read"""
     n = [16, 16]
     nc = 256
     with solver(2, n, [PE, NS, PE], [PE, NS, PE]) as s:
         sp = L.StochParams(k_B=1.0, variance_coef_mom=1.0, dV=1.0, stoch_stress_form=1, filtering_width=0)
         one = dev(np.ones(nc), cuda)
         with pytest.raises(L.FhdError) as e:
-            s.stochastic_m_fluxdiv(sp, zeros(nc, 2, cuda), False, one, [one], one, [one], 0.1, [1.0],
-                                   zeros(nc, 2, cuda), zeros(nc, 2, cuda))
+            s.advance_timestep_inertial(sp, 0.1, zeros(nc, 2, cuda), one, one, one, [one], one, one, [one],
+                                        zeros(nc, 2, cuda), zeros(nc, 2, cuda))
         assert e.value.status == L._capi.FHD_ERR_UNSUPPORTED
