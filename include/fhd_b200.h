@@ -351,7 +351,10 @@ int fhd_dev_advance_inertial(fhd_ctx* ctx, const fhd_stoch_params* sp,
  * of species i.  rho: nspecies cell arrays.  W_fc[(r*dim+d)*nspecies+i]:
  * N(0,1) field of rng r on the faces of direction d for species i
  * (fill_mass_stochastic, stochastic_mass_fluxdiv.f90:182-214).  Uses k_B
- * and dV of sp.  nspecies 2..5. */
+ * and dV of sp.  nspecies 2..5.
+ * Walls (fhd_ctx_create_bc codes 100, 200): no flux through a wall face
+ * (first-order extrapolated concentrations, scalar_bc in
+ * inhomogeneous_bc_val.f90:21-54, and stoch_mass_bc). */
 int fhd_dev_compute_mass_fluxdiv(fhd_ctx* ctx, const fhd_mixture_params* mp,
                                  const fhd_stoch_params* sp,
                                  const double* const rho[], double dt,
@@ -366,7 +369,11 @@ int fhd_dev_compute_mass_fluxdiv(fhd_ctx* ctx, const fhd_mixture_params* mp,
  * subsystem).  rho: nspecies cell arrays.  sqrtLonsager_fc: dim*ns*ns face
  * arrays, entry (r, c) of direction d at index d*ns*ns + r + ns*c (the
  * column-major component order of the reference's ns^2-component
- * multifab).  FP64.  nspecies 2..5. */
+ * multifab).  FP64.  nspecies 2..5.
+ * Walls (fhd_ctx_create_bc codes 100, 200): on a wall face the ghost cell is
+ * the first-order extrapolation of the interior cell (scalar_bc,
+ * inhomogeneous_bc_val.f90:21-54).  The host-fab entry
+ * fhd_compute_sqrtLonsager_fc refuses walls. */
 int fhd_dev_compute_sqrtLonsager_fc(fhd_ctx* ctx, const fhd_mixture_params* mp,
                                     const fhd_stoch_params* sp,
                                     const double* const rho[],

@@ -487,6 +487,8 @@ int fhd_stag_mg_solve(fhd_ctx* ctx, const fhd_multifab* alpha_fc, const fhd_mult
 int fhd_compute_sqrtLonsager_fc(fhd_ctx* ctx, const fhd_mixture_params* mp, const fhd_stoch_params* sp,
                                 const fhd_multifab* rho, const fhd_multifab* rhotot,
                                 const fhd_multifab* sqrtLonsager_fc) {
+    // the periodic scatter would give the high wall face the low one's value
+    if (int wr = refuse_walls(ctx, "fhd_compute_sqrtLonsager_fc (host fabs)")) return wr;
     if (!ctx || !mp || !sp || !rho || !sqrtLonsager_fc) return FHD_ERR_BAD_ARG;
     if (mp->nspecies < 2 || mp->nspecies > 5) return FHD_ERR_UNSUPPORTED;
     const int dim = ctx->dim, ns = mp->nspecies;

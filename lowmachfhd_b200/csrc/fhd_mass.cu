@@ -838,13 +838,22 @@ __device__ __forceinline__ void d_stoch_face(const MixDev& m, int d, i64 f, cons
 // SM to hide the dependent chains)
 template <typename T, int NS, int DIM>
 __global__ void __launch_bounds__(128, (sizeof(T) == 4 && NS <= 4) ? 8 : 1)
-    k_mass_flux(Grid g, MixDev m, int d, const double* const* __restrict__ rho,
+    k_mass_flux(Grid g, MixDev m, int d, int wall, const double* const* __restrict__ rho,
                 const T* const* __restrict__ rwc, const T* const* __restrict__ xc,
                 const double* const* __restrict__ W, int n_rngs, const double* wts, T variance, T dxinv,
                 T* const* flux, TraceList tl) {
     Cell P;
     if (!cell_of_thread(g, P)) return;
     const i64 f = P.id(0, 0, 0);
+    if (wall && (d == 0 ? P.i : (d == 1 ? P.j : P.k)) == 0) {
+        // a wall face (wall: direction d has walls): the concentrations'
+        // ghost cells are first-order extrapolated (scalar_bc,
+        // inhomogeneous_bc_val.f90:21-54), so the diffusive flux vanishes,
+        // and stoch_mass_bc zeroes the random field there
+#pragma unroll
+        for (int s = 0; s < NS; s++) flux[d * NS + s][f] = T(0);
+        return;
+    }
     const i64 fm = P.id(-(d == 0), -(d == 1), -(d == 2));
     T fd[NS];
     {
@@ -932,11 +941,15 @@ struct SqrtLArgs {
 // compute_sqrtLonsager_fc (mass_flux_utilities.f90:1096-1229): every face
 // of direction d
 template <int NS>
-__global__ void __launch_bounds__(128) k_sqrtL_fc(Grid g, MixDev m, int d, SqrtLArgs a) {
+// (wall: direction d has walls; on a wall face the ghost cell is the
+// first-order extrapolation of the interior cell, scalar_bc,
+// inhomogeneous_bc_val.f90:21-54)
+__global__ void __launch_bounds__(128) k_sqrtL_fc(Grid g, MixDev m, int d, int wall, SqrtLArgs a) {
     Cell P;
     if (!cell_of_thread(g, P)) return;
     const i64 f = P.id(0, 0, 0);
-    const i64 fm = P.id(-(d == 0), -(d == 1), -(d == 2));
+    const bool wf = wall && (d == 0 ? P.i : (d == 1 ? P.j : P.k)) == 0;
+    const i64 fm = wf ? f : P.id(-(d == 0), -(d == 1), -(d == 2));
     double L[NS][NS];
     d_face_sqrtL<double, NS>(m, a.rho, f, fm, L);
 #pragma unroll
@@ -1109,8 +1122,8 @@ static int mass_fluxdiv_T(fhd_ctx* ctx, MassBufs& B, const MixDev& m, const doub
         with_dim(dim, [&](auto D) {
             constexpr int DIM = decltype(D)::value;
             k_mass_flux<T, NS, DIM><<<dim3((g.n[0] + 31) / 32, (g.n[1] + 3) / 4, g.n[2]), dim3(32, 4, 1), 0, st>>>(
-                g, m, d, d_rho, (const T* const*)d_rwc, (const T* const*)d_xc, d_W, n_rngs, B.wts, variance, dxinv,
-                d_flux, B.tl);
+                g, m, d, ctx->has_walls && ctx->walls.lo[d] != 0, d_rho, (const T* const*)d_rwc, (const T* const*)d_xc,
+                d_W, n_rngs, B.wts, variance, dxinv, d_flux, B.tl);
             k_mass_flux_trace<T, NS, DIM><<<nbt, 128, 0, st>>>(g, m, d, d_rho, d_W, n_rngs, B.wts, variance, d_flux,
                                                                B.tl);
         });
@@ -1211,8 +1224,8 @@ static int sqrtL_fc_T(fhd_ctx* ctx, const MixDev& m, const double* const rho[], 
         memset(&a, 0, sizeof(a));
         for (int s = 0; s < NS; s++) a.rho[s] = rho[s];
         for (int q = 0; q < NS * NS; q++) a.out[q] = sqrtL[d * NS * NS + q];
-        k_sqrtL_fc<NS><<<dim3((g.n[0] + 31) / 32, (g.n[1] + 3) / 4, g.n[2]), dim3(32, 4, 1), 0, ctx->stream>>>(g, m,
-                                                                                                           d, a);
+        k_sqrtL_fc<NS><<<dim3((g.n[0] + 31) / 32, (g.n[1] + 3) / 4, g.n[2]), dim3(32, 4, 1), 0, ctx->stream>>>(
+            g, m, d, ctx->has_walls && ctx->walls.lo[d] != 0, a);
         ctx->launches++;
         FHD_CUDA_TRY(cudaPeekAtLastError());
     }
@@ -1290,7 +1303,6 @@ static int check_mix(const fhd_mixture_params* mp) {
 extern "C" int fhd_dev_compute_sqrtLonsager_fc(fhd_ctx* ctx, const fhd_mixture_params* mp,
                                                const fhd_stoch_params* sp, const double* const rho[],
                                                double* const sqrtLonsager_fc[]) {
-    if (int wr = refuse_walls(ctx, "fhd_dev_compute_sqrtLonsager_fc")) return wr;
     if (!ctx || !mp || !sp || !rho || !sqrtLonsager_fc) return FHD_ERR_BAD_ARG;
     if (int rc = check_mix(mp)) return rc;
     const MixDev m = make_mixdev(mp, sp);
@@ -1346,7 +1358,6 @@ extern "C" int fhd_dev_stochastic_mass_fluxdiv(fhd_ctx* ctx, const fhd_mixture_p
 extern "C" int fhd_dev_compute_mass_fluxdiv(fhd_ctx* ctx, const fhd_mixture_params* mp, const fhd_stoch_params* sp,
                                             const double* const rho[], double dt, const double* weights, int n_rngs,
                                             const double* const W_fc[], double* const out[]) {
-    if (int wr = refuse_walls(ctx, "fhd_dev_compute_mass_fluxdiv")) return wr;
     if (!ctx || !mp || !sp || !rho || !weights || !W_fc || !out) return FHD_ERR_BAD_ARG;
     const int rc = fhd::mass_fluxdiv(ctx, mp, sp, rho, dt, weights, n_rngs, W_fc, out);
     if (rc < 0) return rc;

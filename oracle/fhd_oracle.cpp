@@ -1819,6 +1819,15 @@ int mass_fluxdiv_impl(const Geo& g, const Mix& m, const fhd_stoch_params* sp, co
         e[d] = 1;
         forall(g, [&](int i, int j, int k) {
             const long f = g.id(i, j, k), fm = g.id(i - e[0], j - e[1], k - e[2]);
+            const int q[3] = {i, j, k};
+            if (g.wall(d) && q[d] == 0) {
+                // a wall face: the concentrations' ghost cells are first-order
+                // extrapolated (scalar_bc, inhomogeneous_bc_val.f90:21-54), so
+                // grad x and the diffusive flux vanish, and stoch_mass_bc
+                // zeroes the random field there
+                for (int s = 0; s < ns; s++) flux[d * ns + s][f] = 0.0;
+                return;
+            }
             // diffusive: rhoWchi face average times grad(molar concentration)
             double gx[FHD_MAX_SPECIES], fd[FHD_MAX_SPECIES], fs[FHD_MAX_SPECIES];
             for (int s = 0; s < ns; s++) gx[s] = (xcc[s][f] - xcc[s][fm]) * dxinv;
@@ -2439,7 +2448,11 @@ void or_sqrtLonsager_fc(int dim, const int n[3], const fhd_stoch_params* sp, con
         int e[3] = {0, 0, 0};
         e[d] = 1;
         forall(g, [&](int i, int j, int k) {
-            const long f = g.id(i, j, k), fm = g.id(i - e[0], j - e[1], k - e[2]);
+            const int q[3] = {i, j, k};
+            // on a wall face the ghost cell is the first-order extrapolation of
+            // the interior cell (scalar_bc, inhomogeneous_bc_val.f90:21-54)
+            const long f = g.id(i, j, k),
+                       fm = (g.wall(d) && q[d] == 0) ? f : g.id(i - e[0], j - e[1], k - e[2]);
             double r1[FHD_MAX_SPECIES], r2[FHD_MAX_SPECIES], ra[FHD_MAX_SPECIES], L[FHD_MAX_SPECIES][FHD_MAX_SPECIES];
             for (int s = 0; s < ns; s++) {
                 r1[s] = rho[s][fm];

@@ -1,8 +1,10 @@
-"""Walls in the stochastic fluxes through the C ABI against the oracle:
-fhd_dev_stochastic_m_fluxdiv (mflux_bc_2d / _3d, stochastic_m_fluxdiv.f90:
-363-451, the high wall's edge planes, zero normal force on wall faces) and
-fhd_dev_stochastic_mass_fluxdiv (stoch_mass_bc, stochastic_mass_fluxdiv.f90:
-216-368), FP64 and mixed; the host-fab entries refuse walls."""
+"""Walls in the stochastic and mass fluxes through the C ABI against the
+oracle: fhd_dev_stochastic_m_fluxdiv (mflux_bc_2d / _3d,
+stochastic_m_fluxdiv.f90:363-451, the high wall's edge planes, zero normal
+force on wall faces), fhd_dev_stochastic_mass_fluxdiv (stoch_mass_bc,
+stochastic_mass_fluxdiv.f90:216-368), fhd_dev_compute_mass_fluxdiv and
+fhd_dev_compute_sqrtLonsager_fc (first-order extrapolated concentrations at
+walls, scalar_bc), FP64 and mixed; the host-fab entries refuse walls."""
 import numpy as np
 import pytest
 
@@ -95,7 +97,41 @@ def test_stochastic_mass_fluxdiv_walls(cuda, dim, n, bc_lo, bc_hi):
 
 def test_host_fab_entries_refuse_walls(cuda):
     with solver(2, [16, 16], [PE, NS, PE], [PE, NS, PE]) as s:
+        assert L._capi.lib().fhd_compute_sqrtLonsager_fc(s._h, None, None, None, None,
+                                                        None) == L._capi.FHD_ERR_UNSUPPORTED
         assert L._capi.lib().fhd_stochastic_m_fluxdiv(s._h, None, None, 0, None, None, None, None, 0.1, None, 1,
                                                      None, None) == L._capi.FHD_ERR_UNSUPPORTED
         assert L._capi.lib().fhd_stochastic_mass_fluxdiv(s._h, None, None, None, None, None, None, None, 0.1,
                                                         None, 1, None, 0) == L._capi.FHD_ERR_UNSUPPORTED
+
+
+@pytest.mark.parametrize("dim,n,bc_lo,bc_hi", [CASES[2], CASES[4], CASES[5]])
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-12), ("mixed", 1e-5)])
+def test_compute_mass_fluxdiv_walls(cuda, dim, n, bc_lo, bc_hi, precision, tol):
+    from tests.test_gpu_multispecies import lmix
+    from tests.test_oracle_multispecies import mass_fields, mix, state
+    ns = 3
+    sp = dict(k_B=1e-4, variance_coef_mom=1.0, dV=1.0, stoch_stress_form=1, filtering_width=0)
+    rho = state(dim, n, ns, amp=1e-2)
+    W = mass_fields(dim, n, ns, n_rngs=2)
+    O.set_walls(bc_lo, bc_hi)
+    ref = O.mass_fluxdiv(dim, n, 1.0, O.StochParams(**sp), mix(ns), rho, 0.05, [0.7, -0.3], W)
+    with L.StokesSolver(dim, n, 1.0, 1, precision=precision, bc_lo=bc_lo, bc_hi=bc_hi) as s:
+        out = dev([np.zeros(P.nc_of(dim, n)) for _ in range(ns)], cuda)
+        s.compute_mass_fluxdiv(lmix(ns), L.StochParams(**sp), dev(rho, cuda), 0.05, [0.7, -0.3], dev(W, cuda), out)
+    assert P.rel_inf(host(out), ref) < tol
+
+
+@pytest.mark.parametrize("dim,n,bc_lo,bc_hi", [CASES[0], CASES[4]])
+def test_compute_sqrtLonsager_fc_walls(cuda, dim, n, bc_lo, bc_hi):
+    from tests.test_gpu_multispecies import lmix
+    from tests.test_oracle_multispecies import mix, state
+    ns = 3
+    sp = dict(k_B=1e-4, variance_coef_mom=1.0, dV=1.0, stoch_stress_form=1, filtering_width=0)
+    rho = state(dim, n, ns, amp=1e-2)
+    O.set_walls(bc_lo, bc_hi)
+    ref = O.sqrtLonsager_fc(dim, n, O.StochParams(**sp), mix(ns), rho)
+    with solver(dim, n, bc_lo, bc_hi) as s:
+        out = dev([np.zeros(P.nc_of(dim, n)) for _ in range(dim * ns * ns)], cuda)
+        s.compute_sqrtLonsager_fc(lmix(ns), L.StochParams(**sp), dev(rho, cuda), out)
+    assert P.rel_inf(host(out), ref) < 1e-12

@@ -152,3 +152,46 @@ def test_stoch_mass_wall_faces_and_conservation():
         assert np.all(fx[:, :, 0] == 0.0) and np.all(fz[0] == 0.0)
         assert np.any(flux[1 * ns + s] != 0.0)
         assert abs(div[s].sum()) < 1e-10 * np.abs(div[s]).sum()
+
+
+def test_mass_fluxdiv_walls_zero_faces_and_conservation():
+    """compute_mass_fluxdiv with walls: no diffusive or random flux through a
+    wall face, and each species' divergence sums to zero"""
+    from tests.test_oracle_multispecies import mass_fields, mix, state
+    dim, n, ns = 3, [8, 6, 4], 3
+    bc = [NS, PE, SL]
+    mp = mix(ns)
+    sp = O.StochParams(k_B=1e-4, variance_coef_mom=1.0, dV=1.0, stoch_stress_form=1, filtering_width=0)
+    rho = state(dim, n, ns, amp=1e-2)
+    W = mass_fields(dim, n, ns, n_rngs=1)
+    O.set_walls(bc, bc)
+    div, flux = O.mass_fluxdiv(dim, n, 1.0, sp, mp, rho, 0.05, [1.0], W, want_flux=True)
+    for s in range(ns):
+        assert np.all(flux[0 * ns + s].reshape(4, 6, 8)[:, :, 0] == 0.0)
+        assert np.all(flux[2 * ns + s].reshape(4, 6, 8)[0] == 0.0)
+        assert np.any(flux[0 * ns + s].reshape(4, 6, 8)[:, :, 1:] != 0.0)
+        assert abs(div[s].sum()) < 1e-10 * np.abs(div[s]).sum()
+
+
+def test_sqrtL_wall_faces_use_the_extrapolated_ghost():
+    """on a wall face the factor is the periodic one with the wrapped
+    neighbour replaced by the interior cell (first-order extrapolation);
+    the other faces are unchanged"""
+    from tests.test_oracle_multispecies import mix, state
+    dim, n, ns = 2, [8, 6], 3
+    mp = mix(ns)
+    sp = O.StochParams(k_B=1e-4, variance_coef_mom=1.0, dV=1.0, stoch_stress_form=1, filtering_width=0)
+    rho = state(dim, n, ns, amp=1e-2)
+    O.set_walls([NS, PE, PE], [SL, PE, PE])
+    got = O.sqrtLonsager_fc(dim, n, sp, mp, rho)
+    O.set_walls()
+    per = O.sqrtLonsager_fc(dim, n, sp, mp, rho)
+    mod = [r.reshape(6, 8).copy() for r in rho]
+    for r in mod:
+        r[:, 7] = r[:, 0]  # the wrapped neighbour of face 0 becomes the interior cell
+    ghost = O.sqrtLonsager_fc(dim, n, sp, mp, [r.ravel() for r in mod])
+    for q in range(ns * ns):
+        g = got[q].reshape(6, 8)
+        assert np.array_equal(g[:, 0], ghost[q].reshape(6, 8)[:, 0])
+        assert np.array_equal(g[:, 1:], per[q].reshape(6, 8)[:, 1:])
+        assert np.array_equal(got[ns * ns + q], per[ns * ns + q])  # y faces: periodic
