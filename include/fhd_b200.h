@@ -433,7 +433,12 @@ int fhd_dev_advance_inertial_multispecies(fhd_ctx* ctx, const fhd_stoch_params* 
  * with n_rngs = 2), W_mass 2*dim*nspecies face arrays
  * (W_mass[(r*dim+d)*nspecies+i]; NULL without a mixture).  The predictor
  * weighs the stages (1, 0) over dt/2, the corrector (1/sqrt2, 1/sqrt2)
- * over dt.  stats (nullable) receives the two solves' diagnostics. */
+ * over dt.  stats (nullable) receives the two solves' diagnostics.
+ * Walls (fhd_ctx_create_bc codes 100, 200, visc_type 1): the Stokes solve,
+ * the stochastic and mass fluxes carry their wall rules (W_ed, eta_ed and
+ * temperature_ed then have the high wall's edge planes, as for
+ * fhd_dev_stochastic_m_fluxdiv), the pressure gradient is zero on a wall
+ * face, and umac's wall faces (zero on entry) stay zero. */
 int fhd_dev_advance_overdamped(fhd_ctx* ctx, const fhd_stoch_params* sp,
                                const fhd_mixture_params* mp, double dt,
                                double* const umac[], double* const rho[], double* pi,

@@ -399,11 +399,22 @@ static int diff_m(fhd_ctx* ctx, SVec<double> out, CSVec<double> u, const double*
     A.gamma = kappa;
     A.q = 1.0 / (ctx->dx * ctx->dx);
     const Grid g = ctx->g0;
-    with_dim_visc(ctx->dim, ctx->visc, [&](auto D, auto V) {
-        constexpr int DIM = decltype(D)::value, VISC = decltype(V)::value;
-        k_stag_apply<double, DIM, VISC><<<cell_grid(g), cell_block(), 0, ctx->stream>>>(
-            g, A, u.c[0], u.c[1], u.c[2], out.c[0], out.c[1], out.c[2], nullptr, nullptr, nullptr, 0);
-    });
+    if (ctx->has_walls) {
+        // visc_type 1 with the wall ghost rules; zero on the wall faces
+        // (stag_applyop.f90:201-205)
+        with_dim(ctx->dim, [&](auto D) {
+            constexpr int DIM = decltype(D)::value;
+            k_stag_apply_w<double, DIM><<<cell_grid(g), cell_block(), 0, ctx->stream>>>(
+                g, ctx->walls, A, u.c[0], u.c[1], u.c[2], out.c[0], out.c[1], out.c[2], nullptr, nullptr, nullptr,
+                0);
+        });
+    } else {
+        with_dim_visc(ctx->dim, ctx->visc, [&](auto D, auto V) {
+            constexpr int DIM = decltype(D)::value, VISC = decltype(V)::value;
+            k_stag_apply<double, DIM, VISC><<<cell_grid(g), cell_block(), 0, ctx->stream>>>(
+                g, A, u.c[0], u.c[1], u.c[2], out.c[0], out.c[1], out.c[2], nullptr, nullptr, nullptr, 0);
+        });
+    }
     ctx->launches++;
     FHD_CUDA_TRY(cudaPeekAtLastError());
     Lin L;
@@ -767,6 +778,11 @@ int advance_overdamped(fhd_ctx* ctx, const fhd_stoch_params* sp, const fhd_mixtu
         launch_dim([&](auto D) {
             constexpr int DIM = decltype(D)::value;
             k_grad<DIM><<<cell_grid(g), cell_block(), 0, st>>>(g, pi, gpi, dxinv);
+            // at a wall the pressure ghost is the interior value (first-order
+            // extrapolation): no gradient on a wall face (div_and_grad.f90:540-556)
+            if (ctx->has_walls)
+                k_zero_walls<double, DIM><<<cell_grid(g), cell_block(), 0, st>>>(g, ctx->walls, gpi.c[0], gpi.c[1],
+                                                                                DIM == 3 ? gpi.c[2] : nullptr);
         });
         if ((r2 = lin(ctx, rhs_v, 0, {{-1.0, cs(gpi)}}))) return r2;
         if (sp->variance_coef_mom != 0.0 &&
@@ -845,7 +861,6 @@ int fhd_dev_advance_overdamped(fhd_ctx* ctx, const fhd_stoch_params* sp, const f
                                const double* const eta_ed[], const double* kappa, const double* temperature,
                                const double* const temperature_ed[], const double* const W_cc[],
                                const double* const W_ed[], const double* const W_mass[], fhd_solve_stats* stats2) {
-    if (int wr = refuse_walls(ctx, "fhd_dev_advance_overdamped")) return wr;
     if (!ctx || !sp || !umac || !rho || !pi || !eta || !eta_ed || !kappa || !temperature || !temperature_ed ||
         !W_cc || !W_ed || (mp && !W_mass) || !(dt > 0.0))
         return FHD_ERR_BAD_ARG;

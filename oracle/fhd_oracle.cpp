@@ -2241,7 +2241,6 @@ int overdamped_impl(const Geo& g, int visc_type, const fhd_gmres_params* p_in, c
                     const double* eta, const double* const eta_ed[], const double* kappa, const double* temperature,
                     const double* const temperature_ed[], const double* const W_cc[], const double* const W_ed[],
                     const double* const W_mass[], fhd_solve_stats* stats2) {
-    if (g.any_wall()) return FHD_ERR_UNSUPPORTED;  // the timesteps are built for periodic boxes
     const int dim = g.dim;
     const long nc = g.nc;
     const int nE = n_edge(dim);
