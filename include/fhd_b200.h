@@ -148,8 +148,9 @@ int  fhd_ctx_create(int dim, const int n_cells[3], const double dx[3],
  * ghost rules of multifab_physbc_domainvel / multifab_physbc_macvel
  * (multifab_physbc_stag.f90:91-1116) throughout the Stokes solve; they are
  * built for visc_type 1, precon_type 1 without the BFBt Schur complement,
- * the colour smoother, gmres_spatial_order 2 and one box, and the timestep
- * and stochastic-flux entries refuse a context with walls.  In a wall
+ * the colour smoother, gmres_spatial_order 2 and one box; the device flux
+ * and timestep entries carry the wall rules of their parts, the host-fab
+ * flux entries refuse a context with walls.  In a wall
  * direction a face array keeps n faces: face 0 is the low wall face (held at
  * zero) and the high wall face is not stored.  Reservoirs and other codes
  * return FHD_ERR_UNSUPPORTED.
@@ -333,7 +334,10 @@ int fhd_dev_stochastic_m_fluxdiv(fhd_ctx* ctx, const fhd_stoch_params* sp,
  * 777-784).  umac, rho, pi are advanced in place.  W_cc/W_ed hold this
  * step's random fields as for fhd_dev_stochastic_m_fluxdiv with n_rngs = 1;
  * predictor and corrector use the same fields, as the reference does.
- * stats (nullable) receives the two solves' diagnostics. */
+ * stats (nullable) receives the two solves' diagnostics.
+ * Walls (fhd_ctx_create_bc codes 100, 200, visc_type 1): as for
+ * fhd_dev_advance_overdamped, and the momentum advection's update is zero
+ * on a wall face (mk_advective_m_fluxdiv.f90:80-85). */
 int fhd_dev_advance_inertial(fhd_ctx* ctx, const fhd_stoch_params* sp,
                              double dt, double* const umac[], double* rho,
                              double* pi, const double* eta,
@@ -408,7 +412,8 @@ int fhd_dev_stochastic_mass_fluxdiv(fhd_ctx* ctx, const fhd_mixture_params* mp,
  * (from the previous step or compute_mass_fluxdiv at start-up) and F^{n+1}
  * on exit.  W_mass: 2*dim*nspecies face arrays, first the fields of the
  * previous corrector (the predictor reuses them, as the reference does
- * between fill_mass_stochastic calls), then this step's new fields. */
+ * between fill_mass_stochastic calls), then this step's new fields.
+ * Walls: as for fhd_dev_advance_inertial. */
 int fhd_dev_advance_inertial_multispecies(fhd_ctx* ctx, const fhd_stoch_params* sp,
                                           const fhd_mixture_params* mp, double dt,
                                           double* const umac[], double* const rho[],

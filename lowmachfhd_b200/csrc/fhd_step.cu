@@ -548,6 +548,20 @@ int advance_inertial_ms(fhd_ctx* ctx, const fhd_stoch_params* sp, const fhd_mixt
         with_dim(dim, fn);
         ctx->launches++;
     };
+    // walls: the pressure gradient (first-order extrapolated pressure,
+    // div_and_grad.f90:540-556) and the advective update
+    // (mk_advective_m_fluxdiv.f90:80-85) are zero on a wall face.  With u and
+    // m zero on the wall faces the periodic stencils read no other value
+    // across a wall: every flux through a wall carries the wall's zero normal
+    // velocity, and the reads past the high wall wrap to the low wall face.
+    auto zero_wall_faces = [&](SVec<double> v) {
+        if (!ctx->has_walls) return;
+        launch_dim([&](auto D) {
+            constexpr int DIM = decltype(D)::value;
+            k_zero_walls<double, DIM><<<cell_grid(g), cell_block(), 0, st>>>(g, ctx->walls, v.c[0], v.c[1],
+                                                                            DIM == 3 ? v.c[2] : nullptr);
+        });
+    };
     // eta/2, kappa/2 for the solves (advance_timestep_inertial.f90:467-474)
     k_copy_conv<double, double><<<nb, 256, 0, st>>>(nc, eta_h, eta, 0.5);
     k_copy_conv<double, double><<<nb, 256, 0, st>>>(nc, kap_h, kappa, 0.5);
@@ -598,6 +612,8 @@ int advance_inertial_ms(fhd_ctx* ctx, const fhd_stoch_params* sp, const fhd_mixt
         constexpr int DIM = decltype(D)::value;
         k_adv_m<DIM><<<cell_grid(g), cell_block(), 0, st>>>(g, cs(u), cs(mold), adv, 0, dxinv);
     });
+    zero_wall_faces(gpi);
+    zero_wall_faces(adv);
     if ((rc = diff_m(ctx, diff, cs(u), eta, eta_ed, kappa))) return rc;
     if ((rc = lin(ctx, rhs_v, 0, {{1.0 / dt, cs(mold)}, {-1.0, cs(gpi)}, {1.0, cs(adv)}, {0.5, cs(diff)}}))) return rc;
     if (with_stoch &&
@@ -670,6 +686,8 @@ int advance_inertial_ms(fhd_ctx* ctx, const fhd_stoch_params* sp, const fhd_mixt
             constexpr int DIM = decltype(D)::value;
             k_adv_m<DIM><<<cell_grid(g), cell_block(), 0, st>>>(g, cs(u), cs(mtemp), adv, 1, dxinv);
         });
+        zero_wall_faces(gpi);
+        zero_wall_faces(adv);
         if ((rc2 = lin(ctx, rhs_v, 0, {{1.0 / dt, cs(mold)}, {-1.0, cs(gpi)}, {0.5, cs(adv)}, {0.5, cs(diff)}})))
             break;
         if (with_stoch && (rc2 = stoch_launch(ctx, sp, stoch.c, 1, eta, eta_ed, temperature, temperature_ed, dt, w1,
@@ -888,7 +906,6 @@ int fhd_dev_advance_inertial(fhd_ctx* ctx, const fhd_stoch_params* sp, double dt
                              double* pi, const double* eta, const double* const eta_ed[], const double* kappa,
                              const double* temperature, const double* const temperature_ed[],
                              const double* const W_cc[], const double* const W_ed[], fhd_solve_stats* stats2) {
-    if (int wr = refuse_walls(ctx, "fhd_dev_advance_inertial")) return wr;
     if (!ctx || !sp || !umac || !rho || !pi || !eta || !eta_ed || !kappa || !temperature || !temperature_ed ||
         !W_cc || !W_ed || !(dt > 0.0))
         return FHD_ERR_BAD_ARG;
@@ -907,7 +924,6 @@ int fhd_dev_advance_inertial_multispecies(fhd_ctx* ctx, const fhd_stoch_params* 
                                           const double* temperature, const double* const temperature_ed[],
                                           const double* const W_cc[], const double* const W_ed[],
                                           const double* const W_mass[], fhd_solve_stats* stats2) {
-    if (int wr = refuse_walls(ctx, "fhd_dev_advance_inertial_multispecies")) return wr;
     if (!ctx || !sp || !mp || !umac || !rho || !pi || !mass_fluxdiv || !eta || !eta_ed || !kappa || !temperature ||
         !temperature_ed || !W_cc || !W_ed || !W_mass || !(dt > 0.0))
         return FHD_ERR_BAD_ARG;

@@ -1434,6 +1434,10 @@ void adv_m(const Geo& g, const double* const u[], const double* const m[], doubl
                 s += (flux(i + ed[0], j + ed[1], k + ed[2]) - flux(i, j, k)) * dxinv;
             }
             upd[c][f] = increment ? upd[c][f] - s : -s;
+            // the advective update on a wall face is zero (multifab_physbc_domainvel,
+            // mk_advective_m_fluxdiv.f90:80-85); the stencil above reads past a
+            // wall only in fluxes that carry the wall's zero normal velocity
+            if (wall_face(g, c, i, j, k)) upd[c][f] = 0.0;
         });
     }
 }
@@ -2038,7 +2042,6 @@ int step_impl(const Geo& g, int visc_type, const fhd_gmres_params* p_in, const f
               const double* eta, const double* const eta_ed[], const double* kappa, const double* temperature,
               const double* const temperature_ed[], const double* const W_cc[], const double* const W_ed[],
               const double* const W_mass[], fhd_solve_stats* stats2) {
-    if (g.any_wall()) return FHD_ERR_UNSUPPORTED;  // the timesteps are built for periodic boxes
     const int dim = g.dim;
     const long nc = g.nc;
     const int nE = n_edge(dim);

@@ -1,7 +1,7 @@
 """Homogeneous no-slip and slip walls (fhd_ctx_create_bc bc codes 100, 200)
 through the C ABI against the oracle: apply_matrix, one staggered V-cycle,
 apply_precon and GMRES in FP64 (same iteration counts), the mixed-precision
-solve, and the options and entries that refuse walls."""
+solve, and the options that refuse walls."""
 import numpy as np
 import pytest
 
@@ -151,17 +151,3 @@ def test_one_sided_periodic_is_refused(cuda):
     with pytest.raises(L.FhdError) as e:
         L.StokesSolver(2, [16, 16], 1.0, 1, bc_lo=[PE, NS, PE], bc_hi=[PE, PE, PE])
     assert e.value.status == L._capi.FHD_ERR_BAD_ARG
-
-
-def test_timestep_entries_refuse_walls(cuda):
-    """the timestep entries are built for periodic boxes: refused before any
-    array is read"""
-    n = [16, 16]
-    nc = 256
-    with solver(2, n, [PE, NS, PE], [PE, NS, PE]) as s:
-        sp = L.StochParams(k_B=1.0, variance_coef_mom=1.0, dV=1.0, stoch_stress_form=1, filtering_width=0)
-        one = dev(np.ones(nc), cuda)
-        with pytest.raises(L.FhdError) as e:
-            s.advance_timestep_inertial(sp, 0.1, zeros(nc, 2, cuda), one, one, one, [one], one, one, [one],
-                                        zeros(nc, 2, cuda), zeros(nc, 2, cuda))
-        assert e.value.status == L._capi.FHD_ERR_UNSUPPORTED
