@@ -317,7 +317,8 @@ int fhd_dev_gmres(fhd_ctx* ctx,
  * wall set to zero (mflux_bc_2d / _3d, stochastic_m_fluxdiv.f90:363-451),
  * and the normal component of force on a wall face is set to zero
  * (multifab_physbc_domainvel), with or without increment.  The host-fab
- * entry fhd_stochastic_m_fluxdiv refuses walls. */
+ * entry fhd_stochastic_m_fluxdiv takes these planes from the nodal fabs'
+ * plane hi+1 (one whole-domain fab per edge multifab). */
 int fhd_dev_stochastic_m_fluxdiv(fhd_ctx* ctx, const fhd_stoch_params* sp,
                                  double* const force[], int increment,
                                  const double* eta, const double* const eta_ed[],
@@ -651,7 +652,10 @@ int fhd_apply_matrix(fhd_ctx* ctx,
  *   (stochastic_m_fluxdiv.f90:42-53).  The module-global random storage
  *   mflux_cc/mflux_nd/mflux_ed of the reference is passed explicitly:
  *   W_cc[r] is a dim-component cell multifab, W_ed[r*nE+e] a 2-component
- *   node (2D, nE=1) or edge (3D, nE=3) multifab. */
+ *   node (2D, nE=1) or edge (3D, nE=3) multifab.  With walls every edge
+ *   multifab (eta_ed, temperature_ed, W_ed) is one whole-domain fab, nodal
+ *   in its edge set's directions; its plane hi+1 in a wall direction is the
+ *   high wall's (FHD_ERR_BAD_ARG otherwise). */
 int fhd_stochastic_m_fluxdiv(fhd_ctx* ctx, const fhd_stoch_params* sp,
                              const fhd_multifab* stoch_m_force, int increment,
                              const fhd_multifab* eta,

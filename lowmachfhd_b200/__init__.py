@@ -336,6 +336,20 @@ class StokesSolver:
             float(dt), C.cast(w, _DP), len(weights), _mf_vec(W_fc, keep), int(bool(increment))),
             "fhd_stochastic_mass_fluxdiv")
 
+    def stochastic_m_fluxdiv_fab(self, sp: StochParams, stoch_m_force, increment, eta, eta_ed, temperature,
+                                 temperature_ed, dt, weights, W_cc, W_ed):
+        """stochastic_m_fluxdiv on host multifabs: stoch_m_force (dim face
+        multifabs, in/out), eta and temperature cell multifabs, eta_ed and
+        temperature_ed node (2D) or edge (3D) multifabs, W_cc[r] the
+        dim-component cell multifab of stage r, W_ed[r*nE+e] the 2-component
+        node/edge multifab of stage r and edge set e"""
+        keep = []
+        w = (C.c_double * len(weights))(*[float(x) for x in weights])
+        return check(lib().fhd_stochastic_m_fluxdiv(
+            self._h, C.byref(sp), _mf_vec(stoch_m_force, keep), int(bool(increment)), _mf(eta, keep),
+            _mf_vec(eta_ed, keep), _mf(temperature, keep), _mf_vec(temperature_ed, keep), float(dt),
+            C.cast(w, _DP), len(weights), _mf_vec(W_cc, keep), _mf_vec(W_ed, keep)), "fhd_stochastic_m_fluxdiv")
+
 
 def stag_mg_solver_noalloc(dim, n_cells, dx, visc_type, params, alpha_fc, beta_cc, beta_ed, gamma_cc,
                            theta_alpha, phi_fc, rhs_fc, stream=None):

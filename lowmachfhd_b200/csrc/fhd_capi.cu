@@ -48,6 +48,24 @@ __global__ void k_gather(Grid g, FabDesc d, const double* __restrict__ fab, doub
     }
 }
 
+// One whole-domain fab -> the wall-extended layout of an edge set: the
+// cells lo..hi, plus the nodal plane hi+1 in the directions with xt[d] = 1
+// (a wall direction in which the fab is nodal: the high wall's edges, which
+// the reference draws independently).  Extents m[d] = n[d] + xt[d].
+struct EdgeGather {
+    int xt[3], m[3];
+};
+__global__ void k_gather_ext(FabDesc d, EdgeGather X, int dim, const double* __restrict__ fab, double* out) {
+    const int bx = X.m[0], by = X.m[1], bz = X.m[2];
+    const i64 n = (i64)bx * by * bz;
+    for (i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x; t < n; t += (i64)gridDim.x * blockDim.x) {
+        const int a = (int)(t % bx), b = (int)((t / bx) % by), c = (int)(t / ((i64)bx * by));
+        const i64 src = (i64)(a + d.ng) + (i64)d.ext[0] * ((i64)(b + (dim > 1 ? d.ng : 0)) +
+                                                             (i64)d.ext[1] * (i64)(c + (dim > 2 ? d.ng : 0)));
+        out[t] = fab[src];
+    }
+}
+
 // canonical -> whole fab (valid, nodal duplicate and ghosts)
 __global__ void k_scatter(Grid g, FabDesc d, const double* __restrict__ in, double* fab) {
     const i64 n = (i64)d.ext[0] * d.ext[1] * d.ext[2];
@@ -108,6 +126,38 @@ int mf_to_dev(fhd_ctx* ctx, const fhd_multifab* mf, double* dst) {
         ctx->launches++;
         FHD_CUDA_TRY(cudaPeekAtLastError());
     }
+    return 0;
+}
+
+// an edge multifab of set e (2D the nodes; 3D xy, xz, yz) in a context with
+// walls -> the wall-extended layout; the multifab must be one whole-domain
+// fab, nodal exactly in the set's directions
+static int mf_to_dev_edge(fhd_ctx* ctx, const fhd_multifab* mf, int e, double* dst) {
+    const int dim = ctx->dim;
+    const int da = (dim == 3 && e == 2) ? 1 : 0, db = (dim == 3 && e != 0) ? 2 : 1;
+    if (mf->nfabs != 1) {
+        set_last_error("edge multifab with walls: one whole-domain fab expected");
+        return FHD_ERR_BAD_ARG;
+    }
+    const fhd_fab& f = mf->fabs[0];
+    FabDesc d = desc_of(f, dim);
+    EdgeGather X;
+    for (int k = 0; k < 3; k++) {
+        const bool in_set = k < dim && (k == da || k == db);
+        if (k < dim && (d.lo[k] != 0 || d.hi[k] != ctx->n[k] - 1 || d.nodal[k] != (in_set ? 1 : 0))) {
+            set_last_error("edge multifab with walls: one whole-domain fab, nodal in the edge set's directions");
+            return FHD_ERR_BAD_ARG;
+        }
+        X.xt[k] = in_set && ctx->walls.lo[k] != 0 ? 1 : 0;
+        X.m[k] = (k < dim ? ctx->n[k] : 1) + X.xt[k];
+    }
+    HostPath& H = host_path(ctx);
+    const i64 ne = fab_elems(d);
+    if (int rc = ensure_stage(ctx, H, ne)) return rc;
+    FHD_CUDA_TRY(cudaMemcpyAsync(H.stage, f.data, sizeof(double) * ne, cudaMemcpyHostToDevice, ctx->stream));
+    k_gather_ext<<<flat_blocks((i64)X.m[0] * X.m[1] * X.m[2]), 256, 0, ctx->stream>>>(d, X, dim, H.stage, dst);
+    ctx->launches++;
+    FHD_CUDA_TRY(cudaPeekAtLastError());
     return 0;
 }
 
@@ -368,8 +418,6 @@ int fhd_stochastic_m_fluxdiv(fhd_ctx* ctx, const fhd_stoch_params* sp, const fhd
                              int increment, const fhd_multifab* eta, const fhd_multifab* eta_ed,
                              const fhd_multifab* temperature, const fhd_multifab* temperature_ed, double dt,
                              const double* weights, int n_rngs, const fhd_multifab* W_cc, const fhd_multifab* W_ed) {
-    // walls need the high-wall edge planes, which the periodic gather drops
-    if (int wr = refuse_walls(ctx, "fhd_stochastic_m_fluxdiv (host fabs)")) return wr;
     if (!ctx || !sp || !stoch_m_force || !eta || !eta_ed || !temperature || !temperature_ed || !weights || !W_cc ||
         !W_ed || n_rngs < 1 || n_rngs > 4)
         return FHD_ERR_BAD_ARG;
@@ -379,10 +427,24 @@ int fhd_stochastic_m_fluxdiv(fhd_ctx* ctx, const fhd_stoch_params* sp, const fhd
     // and the component-split random fields
     const int ncc = n_rngs * dim, ned = n_rngs * 2 * nE;
     const int total = dim + 2 + 2 * nE + ncc + ned;
+    // with walls an edge set that contains a wall direction has the high
+    // wall's plane too (the device entry's wall-extended layout)
+    i64 ne[3] = {nc, nc, nc};
+    if (ctx->has_walls)
+        for (int e = 0; e < nE; e++) {
+            const int da = (dim == 3 && e == 2) ? 1 : 0, db = (dim == 3 && e != 0) ? 2 : 1;
+            ne[e] = 1;
+            for (int k = 0; k < dim; k++) ne[e] *= ctx->n[k] + ((k == da || k == db) && ctx->walls.lo[k] != 0 ? 1 : 0);
+        }
+    auto elems_of = [&](int i) -> i64 {
+        if (i >= dim + 2 && i < dim + 2 + 2 * nE) return ne[(i - dim - 2) % nE];  // eta_ed, T_ed
+        if (i >= dim + 2 + 2 * nE + ncc) return ne[((i - dim - 2 - 2 * nE - ncc) / 2) % nE];  // W_ed
+        return nc;
+    };
     std::vector<double*> A(total, nullptr);
     int rc = 0;
     for (int i = 0; i < total && !rc; i++)
-        if (cudaMalloc(&A[i], sizeof(double) * nc) != cudaSuccess) rc = FHD_ERR_OOM;
+        if (cudaMalloc(&A[i], sizeof(double) * elems_of(i)) != cudaSuccess) rc = FHD_ERR_OOM;
     auto cleanup = [&]() {
         for (double* p : A)
             if (p) cudaFree(p);
@@ -415,9 +477,14 @@ int fhd_stochastic_m_fluxdiv(fhd_ctx* ctx, const fhd_stoch_params* sp, const fhd
         if (rc) break;
         if ((rc = check_mf(ctx, eta, 0)) || (rc = mf_to_dev(ctx, eta, d_eta))) break;
         if ((rc = check_mf(ctx, temperature, 0)) || (rc = mf_to_dev(ctx, temperature, d_T))) break;
+        // an edge multifab: the periodic gather, or with walls the extended one
+        auto edge_to_dev = [&](const fhd_multifab* mf, int e, double* dst) {
+            return ctx->has_walls ? mf_to_dev_edge(ctx, mf, e, dst) : mf_to_dev(ctx, mf, dst);
+        };
         for (int e = 0; e < nE && !rc; e++) {
-            if ((rc = check_mf(ctx, &eta_ed[e], 0)) || (rc = mf_to_dev(ctx, &eta_ed[e], d_eed[e]))) break;
-            if ((rc = check_mf(ctx, &temperature_ed[e], 0)) || (rc = mf_to_dev(ctx, &temperature_ed[e], d_Ted[e]))) break;
+            if ((rc = check_mf(ctx, &eta_ed[e], 0)) || (rc = edge_to_dev(&eta_ed[e], e, d_eed[e]))) break;
+            if ((rc = check_mf(ctx, &temperature_ed[e], 0)) || (rc = edge_to_dev(&temperature_ed[e], e, d_Ted[e])))
+                break;
         }
         if (rc) break;
         std::vector<fhd_fab> store;
@@ -439,7 +506,7 @@ int fhd_stochastic_m_fluxdiv(fhd_ctx* ctx, const fhd_stoch_params* sp, const fhd
                 if (rc) break;
                 for (int comp = 0; comp < 2 && !rc; comp++) {
                     comp_mf(W_ed[r * nE + e], comp, store, one);
-                    rc = mf_to_dev(ctx, &one, d_Wed[r * 2 * nE + 2 * e + comp]);
+                    rc = edge_to_dev(&one, e, d_Wed[r * 2 * nE + 2 * e + comp]);
                     if (!rc) rc = cudaStreamSynchronize(ctx->stream) == cudaSuccess ? 0 : FHD_ERR_CUDA;
                 }
             }

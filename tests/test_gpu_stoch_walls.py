@@ -4,7 +4,9 @@ stochastic_m_fluxdiv.f90:363-451, the high wall's edge planes, zero normal
 force on wall faces), fhd_dev_stochastic_mass_fluxdiv (stoch_mass_bc,
 stochastic_mass_fluxdiv.f90:216-368), fhd_dev_compute_mass_fluxdiv and
 fhd_dev_compute_sqrtLonsager_fc (first-order extrapolated concentrations at
-walls, scalar_bc), FP64 and mixed; the host-fab entries refuse walls."""
+walls, scalar_bc), FP64 and mixed; the host-fab fhd_stochastic_m_fluxdiv
+with the high wall's edge planes taken from the nodal fabs, and the other
+host-fab flux entries' refusal."""
 import numpy as np
 import pytest
 
@@ -99,8 +101,6 @@ def test_host_fab_entries_refuse_walls(cuda):
     with solver(2, [16, 16], [PE, NS, PE], [PE, NS, PE]) as s:
         assert L._capi.lib().fhd_compute_sqrtLonsager_fc(s._h, None, None, None, None,
                                                         None) == L._capi.FHD_ERR_UNSUPPORTED
-        assert L._capi.lib().fhd_stochastic_m_fluxdiv(s._h, None, None, 0, None, None, None, None, 0.1, None, 1,
-                                                     None, None) == L._capi.FHD_ERR_UNSUPPORTED
         assert L._capi.lib().fhd_stochastic_mass_fluxdiv(s._h, None, None, None, None, None, None, None, 0.1,
                                                         None, 1, None, 0) == L._capi.FHD_ERR_UNSUPPORTED
 
@@ -135,3 +135,67 @@ def test_compute_sqrtLonsager_fc_walls(cuda, dim, n, bc_lo, bc_hi):
         out = dev([np.zeros(P.nc_of(dim, n)) for _ in range(dim * ns * ns)], cuda)
         s.compute_sqrtLonsager_fc(lmix(ns), L.StochParams(**sp), dev(rho, cuda), out)
     assert P.rel_inf(host(out), ref) < 1e-12
+
+
+def edge_fab(xs, dim, n, e, bc_lo, ng):
+    """wall-extended edge arrays of set e (one per component) -> one
+    whole-domain nodal fab: in a wall direction of the set the nodal plane
+    hi+1 is the high wall's, elsewhere the duplicated plane wraps"""
+    dirs = (0, 1) if dim == 2 else [(0, 1), (0, 2), (1, 2)][e]
+    nodal = [1 if d in dirs else 0 for d in range(dim)]
+    shape = tuple(reversed([n[d] + (1 if (d in dirs and bc_lo[d] != PE) else 0) for d in range(dim)]))
+    idx = []
+    for d in range(dim):
+        r = np.arange(-ng, n[d] + nodal[d] + ng)
+        idx.append(np.clip(r, 0, shape[dim - 1 - d] - 1) if bc_lo[d] != PE else np.mod(r, n[d]))
+    comps = []
+    for x in xs:
+        a = x.reshape(shape)
+        sub = a[np.ix_(idx[1], idx[0])] if dim == 2 else a[np.ix_(idx[2], idx[1], idx[0])]
+        comps.append(np.asfortranarray(sub.T))
+    data = np.asfortranarray(np.stack(comps, axis=-1)) if len(comps) > 1 else comps[0]
+    pad = [0] * (3 - dim)
+    return L.FabArray(data, [0] * dim + pad, [k - 1 for k in n[:dim]] + pad, nodal + pad, ng, ncomp=len(xs))
+
+
+@pytest.mark.parametrize("dim,n,bc_lo,bc_hi", [CASES[0], CASES[4], CASES[5]])
+def test_stochastic_m_fluxdiv_host_fabs_walls(cuda, dim, n, bc_lo, bc_hi):
+    nE = 1 if dim == 2 else 3
+    eta, T, eta_ed, T_ed, W_cc, W_ed = fields(dim, n, bc_lo, 15)
+    rng = np.random.default_rng(16)
+    force0 = [rng.standard_normal(P.nc_of(dim, n)) for _ in range(dim)]
+    O.set_walls(bc_lo, bc_hi)
+    ref = O.stochastic_m_fluxdiv(dim, n, 0.5, O.StochParams(**SP), eta, eta_ed, T, T_ed, 0.1, W8, W_cc, W_ed,
+                                 force=force0, increment=True)
+    ng = 1
+    cell = [0] * dim
+    force = [L.fab_from_canonical(force0[c], dim, n, [int(d == c) for d in range(dim)], 0) for c in range(dim)]
+    with solver(dim, n, bc_lo, bc_hi) as s:
+        s.stochastic_m_fluxdiv_fab(
+            L.StochParams(**SP), force, True, L.fab_from_canonical(eta, dim, n, cell, ng),
+            [edge_fab([eta_ed[e]], dim, n, e, bc_lo, ng) for e in range(nE)],
+            L.fab_from_canonical(T, dim, n, cell, ng), [edge_fab([T_ed[e]], dim, n, e, bc_lo, ng) for e in range(nE)],
+            0.1, W8, [L.fab_from_components(W_cc[r * dim:(r + 1) * dim], dim, n, cell, ng) for r in range(2)],
+            [edge_fab(W_ed[(r * nE + e) * 2:(r * nE + e) * 2 + 2], dim, n, e, bc_lo, ng)
+             for r in range(2) for e in range(nE)])
+    got = [L.canonical_from_fab(f, dim, n) for f in force]
+    assert P.rel_inf(got, ref) < 1e-13
+
+
+def test_stochastic_m_fluxdiv_host_fabs_walls_checks_the_edge_fabs(cuda):
+    """with walls an edge multifab must be one whole-domain fab, nodal in its
+    set's directions (else its high-wall plane is not there)"""
+    dim, n, bc_lo, bc_hi = CASES[0]
+    eta, T, eta_ed, T_ed, W_cc, W_ed = fields(dim, n, bc_lo, 17)
+    cell = [0, 0]
+    nc = P.nc_of(dim, n)
+    force = [L.fab_from_canonical(np.zeros(nc), dim, n, [int(d == c) for d in range(dim)], 0) for c in range(dim)]
+    wrong = L.fab_from_canonical(np.ones(nc), dim, n, cell, 1)  # a cell fab where a node fab belongs
+    with solver(dim, n, bc_lo, bc_hi) as s:
+        with pytest.raises(L.FhdError) as e:
+            s.stochastic_m_fluxdiv_fab(
+                L.StochParams(**SP), force, False, L.fab_from_canonical(eta, dim, n, cell, 1), [wrong],
+                L.fab_from_canonical(T, dim, n, cell, 1), [edge_fab([T_ed[0]], dim, n, 0, bc_lo, 1)], 0.1, W8,
+                [L.fab_from_components(W_cc[r * 2:(r + 1) * 2], dim, n, cell, 1) for r in range(2)],
+                [edge_fab(W_ed[2 * r:2 * r + 2], dim, n, 0, bc_lo, 1) for r in range(2)])
+        assert e.value.status == L._capi.FHD_ERR_BAD_ARG
