@@ -397,7 +397,8 @@ int fhd_dev_compute_sqrtLonsager_fc(fhd_ctx* ctx, const fhd_mixture_params* mp,
  * zero (stoch_mass_bc, stochastic_mass_fluxdiv.f90:216-368); the face
  * arrays keep the periodic layout (face 0 of a wall direction is the low
  * wall, the high wall face is not stored).  The host-fab entry
- * fhd_stochastic_mass_fluxdiv refuses walls. */
+ * fhd_stochastic_mass_fluxdiv takes walls too: the high wall face of a
+ * flux fab, zero, is written from face 0. */
 int fhd_dev_stochastic_mass_fluxdiv(fhd_ctx* ctx, const fhd_mixture_params* mp,
                                     const fhd_stoch_params* sp,
                                     const double* const sqrtLonsager_fc[],

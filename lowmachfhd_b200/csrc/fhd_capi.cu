@@ -584,7 +584,6 @@ int fhd_stochastic_mass_fluxdiv(fhd_ctx* ctx, const fhd_mixture_params* mp, cons
                                 const fhd_multifab* sqrtLonsager_fc, const fhd_multifab* stoch_mass_fluxdiv,
                                 const fhd_multifab* stoch_mass_flux, double dt, const double* weights, int n_rngs,
                                 const fhd_multifab* W_fc, int increment) {
-    if (int wr = refuse_walls(ctx, "fhd_stochastic_mass_fluxdiv (host fabs)")) return wr;
     if (!ctx || !mp || !sp || !sqrtLonsager_fc || !stoch_mass_fluxdiv || !weights || !W_fc || !(dt > 0.0))
         return FHD_ERR_BAD_ARG;
     if (mp->nspecies < 2 || mp->nspecies > 5 || n_rngs < 1 || n_rngs > 4) return FHD_ERR_UNSUPPORTED;

@@ -6,7 +6,9 @@ stochastic_mass_fluxdiv.f90:216-368), fhd_dev_compute_mass_fluxdiv and
 fhd_dev_compute_sqrtLonsager_fc (first-order extrapolated concentrations at
 walls, scalar_bc), FP64 and mixed; the host-fab fhd_stochastic_m_fluxdiv
 with the high wall's edge planes taken from the nodal fabs, and the other
-host-fab flux entries' refusal."""
+host-fab fhd_stochastic_mass_fluxdiv (the high wall face of a flux fab is
+zero, as the periodic scatter writes it), and the refusal of the host-fab
+fhd_compute_sqrtLonsager_fc."""
 import numpy as np
 import pytest
 
@@ -101,8 +103,6 @@ def test_host_fab_entries_refuse_walls(cuda):
     with solver(2, [16, 16], [PE, NS, PE], [PE, NS, PE]) as s:
         assert L._capi.lib().fhd_compute_sqrtLonsager_fc(s._h, None, None, None, None,
                                                         None) == L._capi.FHD_ERR_UNSUPPORTED
-        assert L._capi.lib().fhd_stochastic_mass_fluxdiv(s._h, None, None, None, None, None, None, None, 0.1,
-                                                        None, 1, None, 0) == L._capi.FHD_ERR_UNSUPPORTED
 
 
 @pytest.mark.parametrize("dim,n,bc_lo,bc_hi", [CASES[2], CASES[4], CASES[5]])
@@ -199,3 +199,30 @@ def test_stochastic_m_fluxdiv_host_fabs_walls_checks_the_edge_fabs(cuda):
                 [L.fab_from_components(W_cc[r * 2:(r + 1) * 2], dim, n, cell, 1) for r in range(2)],
                 [edge_fab(W_ed[2 * r:2 * r + 2], dim, n, 0, bc_lo, 1) for r in range(2)])
         assert e.value.status == L._capi.FHD_ERR_BAD_ARG
+
+
+@pytest.mark.parametrize("dim,n,bc_lo,bc_hi", [CASES[2], CASES[4]])
+def test_stochastic_mass_fluxdiv_host_fabs_walls(cuda, dim, n, bc_lo, bc_hi):
+    from tests.test_gpu_boundary import assert_mf, face_nodal, mf
+    from tests.test_gpu_multispecies import lmix
+    from tests.test_oracle_multispecies import mass_fields, mix, state
+    ns = 3
+    nc = P.nc_of(dim, n)
+    sp = dict(k_B=1e-4, variance_coef_mom=1.0, dV=1.0, stoch_stress_form=1, filtering_width=0)
+    rho = state(dim, n, ns, amp=1e-2)
+    W = mass_fields(dim, n, ns, n_rngs=2)
+    div0 = [np.random.default_rng(18).standard_normal(nc) for _ in range(ns)]
+    O.set_walls(bc_lo, bc_hi)
+    sqL = O.sqrtLonsager_fc(dim, n, O.StochParams(**sp), mix(ns), rho)
+    ref_div, ref_flux = O.stochastic_mass_fluxdiv(dim, n, 1.0, O.StochParams(**sp), mix(ns), sqL, 0.05, [0.7, -0.3],
+                                                  W, increment=True, div0=div0, want_flux=True)
+    L_f = [mf(sqL[d * ns * ns:(d + 1) * ns * ns], dim, n, face_nodal(dim, d), 0, 1) for d in range(dim)]
+    W_f = [mf(W[q * ns:(q + 1) * ns], dim, n, face_nodal(dim, q % dim), 0, 1) for q in range(2 * dim)]
+    div_f = mf(div0, dim, n, [0] * dim, 1, 1)
+    flux_f = [mf([np.zeros(nc)] * ns, dim, n, face_nodal(dim, d), 0, 1) for d in range(dim)]
+    with L.StokesSolver(dim, n, 1.0, 1, bc_lo=bc_lo, bc_hi=bc_hi) as s:
+        s.stochastic_mass_fluxdiv_fab(lmix(ns), L.StochParams(**sp), mf(rho, dim, n, [0] * dim, 1, 1), None, L_f,
+                                      div_f, flux_f, 0.05, [0.7, -0.3], W_f, increment=True)
+    assert_mf(div_f, ref_div, dim, n, [0] * dim, 1, 1, 1e-12)
+    for d in range(dim):
+        assert_mf(flux_f[d], ref_flux[d * ns:(d + 1) * ns], dim, n, face_nodal(dim, d), 0, 1, 1e-12)
