@@ -61,9 +61,10 @@ def parse():
     ap.add_argument("--only", choices=["mixed", "fp64"], default=None, help="run one precision only")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving and batched legs")
-    ap.add_argument("--probe", choices=["stagmg", "gmres", "stochm"], default=None,
+    ap.add_argument("--probe", choices=["stagmg", "gmres", "stochm", "batch"], default=None,
                     help="profiling probe on one single-fluid 3D grid: K stag_mg_solver calls (one V-cycle "
-                         "each), K GMRES solves (theta 20, 1e-8), or K stochastic_m_fluxdiv calls")
+                         "each), K GMRES solves (theta 20, 1e-8), or K stochastic_m_fluxdiv calls; or (batch) "
+                         "K batched overdamped steps of the 512 2D realizations after one warm-up step")
     ap.add_argument("--precision", choices=["mixed", "fp64"], default="fp64", help="precision of --probe")
     ap.add_argument("--tune", type=int, default=-1,
                     help="smoother autotuner mode of --probe (fhd_ctx_set_tune: -1 tune, 0 fixed rules, 2+k "
@@ -79,6 +80,10 @@ def run_probe(args):
 
     import lowmachfhd_b200 as L
     dev = torch.device("cuda:0")
+    if args.probe == "batch":
+        r = run_batch_solver(L, torch, dev, count=BATCH_REALIZATIONS, steps=args.steps)
+        print(json.dumps({"probe": "batch", **r}))
+        return 0
     n = args.n
     nc = n ** 3
     s = L.StokesSolver(3, [n, n, n], 1.0, 1, params=L.default_params(gmres_max_inner=1),

@@ -5,9 +5,9 @@ force on wall faces), fhd_dev_stochastic_mass_fluxdiv (stoch_mass_bc,
 stochastic_mass_fluxdiv.f90:216-368), fhd_dev_compute_mass_fluxdiv and
 fhd_dev_compute_sqrtLonsager_fc (first-order extrapolated concentrations at
 walls, scalar_bc), FP64 and mixed; the host-fab fhd_stochastic_m_fluxdiv
-with the high wall's edge planes taken from the nodal fabs, and the other
-host-fab fhd_stochastic_mass_fluxdiv (the high wall face of a flux fab is
-zero, as the periodic scatter writes it), and the refusal of the host-fab
+(the high wall's edge planes taken from the nodal fabs) and
+fhd_stochastic_mass_fluxdiv (the high wall face of a flux fab is zero, as
+the periodic scatter writes it), and the refusal of the host-fab
 fhd_compute_sqrtLonsager_fc."""
 import numpy as np
 import pytest
