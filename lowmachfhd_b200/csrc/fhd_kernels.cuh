@@ -106,6 +106,32 @@ struct Off {
     static constexpr int x = (D == 0), y = (D == 1), z = (D == 2);
 };
 
+// visc_type 1: the diagonal alpha_scale alpha + 2 dim beta q (a = alpha_scale
+// alpha), and in FP32 the operator given that diagonal, with the transverse
+// pairs summed without a leading zero and b q formed once.  stag_lface_acc
+// and the row-tile smoother (which stages the diagonal in place of alpha)
+// evaluate these expressions, so their results agree bit for bit.
+template <typename T, int DIM>
+__device__ __forceinline__ T stag_diag1(T a, T b, T q) {
+    return a + T(2 * DIM) * b * q;
+}
+template <typename T, int DIM, int C, class Own>
+__device__ __forceinline__ T stag_l1_f32(Own own, T diag, T bq) {
+    constexpr int ex = (C == 0), ey = (C == 1), ez = (C == 2);
+    const T own_ = own(ex, ey, ez) + own(-ex, -ey, -ez);
+    T o2 = T(0);
+    bool first = true;
+#pragma unroll
+    for (int d = 0; d < DIM; d++) {
+        if (d == C) continue;
+        const int dx_ = (d == 0), dy_ = (d == 1), dz_ = (d == 2);
+        const T pr = own(dx_, dy_, dz_) + own(-dx_, -dy_, -dz_);
+        o2 = first ? pr : o2 + pr;
+        first = false;
+    }
+    return own(0, 0, 0) * diag - (own_ + o2) * bq;
+}
+
 // (alpha_scale*alpha - L) phi on the face of component C at cell P, and the
 // diagonal coefficient: the stencils of stag_applyop_2d/_3d
 // (stag_applyop.f90:212-1075) and the 'fac' of stag_mg_update
@@ -177,23 +203,9 @@ __device__ __forceinline__ T stag_lface_acc(const StagOp<T>& A, const CellT& P, 
             }
         }
         if constexpr (VISC == 1) {
-            diag = a + T(2 * DIM) * b * q;
-            if constexpr (sizeof(T) == 4) {
-                // FP32 (the multigrid of the mixed-precision solve): the
-                // transverse pairs summed without the leading zero and b q
-                // formed once (uniform, hoisted out of the smoother loops)
-                T o2 = T(0);
-                bool first = true;
-#pragma unroll
-                for (int d = 0; d < DIM; d++) {
-                    if (d == C) continue;
-                    const int dx_ = (d == 0), dy_ = (d == 1), dz_ = (d == 2);
-                    const T pr = own(dx_, dy_, dz_) + own(-dx_, -dy_, -dz_);
-                    o2 = first ? pr : o2 + pr;
-                    first = false;
-                }
-                return ph * diag - (own_ + o2) * (b * q);
-            }
+            diag = stag_diag1<T, DIM>(a, b, q);
+            // FP32 (the multigrid of the mixed-precision solve): stag_l1_f32
+            if constexpr (sizeof(T) == 4) return stag_l1_f32<T, DIM, C>(own, diag, b * q);
             return ph * diag - (own_ + oth_) * b * q;
         } else if constexpr (VISC == 2) {
             diag = a + T(2 * DIM + 2) * b * q;

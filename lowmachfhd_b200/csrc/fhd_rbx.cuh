@@ -9,7 +9,7 @@
 // recomputed, and with the planes staged by the bulk-copy engine:
 //
 //   * a producer warp copies the staged rows of a plane (unknown rows
-//     y0-2 .. y0+TY+1, alpha and rhs rows y0-1 .. y0+TY) with 1D
+//     y0-2 .. y0+TY+1, diagonal and rhs rows y0-1 .. y0+TY) with 1D
 //     cp.async.bulk copies, one per array and contiguous run of rows (the
 //     periodic y wrap splits a run), completing on the stage's mbarrier;
 //   * eight compute warps update four to five cells per thread and plane
@@ -125,7 +125,7 @@ struct RBXArgs {
     const float* src[3];
     float* dst[3];
     const float* rhs[3];
-    const float* alpha[3];
+    const float* diag[3];  // the visc_type 1 diagonal (stag_diag1), staged in place of alpha
     unsigned* err;
 };
 
@@ -144,6 +144,7 @@ __device__ __forceinline__ bool rbx_run(const Grid& g, const RBXGeom& G, const S
         A.beta0 = A0.beta[0];
         A.beta0_set = 1;
     }
+    const float bq = A.beta0 * A.q;
     constexpr int NPH = 5 + AH;  // unknown planes k-1 .. k+3 + in flight
     constexpr int NCF = 3 + AH;  // coefficient planes k .. k+2 + in flight
     constexpr int MR = rbx_maxr(NT);  // rows per thread and red sweep
@@ -155,18 +156,18 @@ __device__ __forceinline__ bool rbx_run(const Grid& g, const RBXGeom& G, const S
     const int y0 = tile_y * TY;
     unsigned long long* bar = reinterpret_cast<unsigned long long*>(raw);
     const int plane = rows * nx, cplane = crows * nx;
-    float* cf = reinterpret_cast<float*>(raw + 64);  // [slot][0 alpha, 1 rhs][crows][nx]
+    float* cf = reinterpret_cast<float*>(raw + 64);  // [slot][0 diagonal, 1 rhs][crows][nx]
     float* ph = cf + NCF * 2 * cplane;          // [slot][rows][nx]
     const float* src = R.src[C];
     float* dst = R.dst[C];
-    const float* alpha = R.alpha[C];
+    const float* diag = R.diag[C];
     const float* rhs = R.rhs[C];
     // stage j = unknown plane j (always) + coefficient plane j-1 (for
     // j >= k0); q = j - (k0 - 2) counts the stages of this CTA from 0
     const int qend = kend + 1 - (k0 - 2);  // last stage index
     // stage q issued by the producer warp: lane 0 arms the barrier with the
     // stage's bytes, then lane 0 copies the unknown rows, lanes 1 and 2 the
-    // alpha and rhs rows.  A tile's rows are consecutive in global memory
+    // diagonal and rhs rows.  A tile's rows are consecutive in global memory
     // except across the periodic y wrap, so each array goes as one to three
     // contiguous copies.
     auto issue = [&](int q) {
@@ -188,7 +189,7 @@ __device__ __forceinline__ bool rbx_run(const Grid& g, const RBXGeom& G, const S
         if (j >= k0 && (lane == 1 || lane == 2)) {
             const int cs = pmod(j - 1, NCF);
             const i64 zo = (i64)wrapc(j - 1, nz) * nxy;
-            copy(cf + (cs * 2 + lane - 1) * cplane, (lane == 1 ? alpha : rhs) + zo, crows, 1);
+            copy(cf + (cs * 2 + lane - 1) * cplane, (lane == 1 ? diag : rhs) + zo, crows, 1);
         }
     };
     // wait for stage q; false on time-out
@@ -229,17 +230,15 @@ __device__ __forceinline__ bool rbx_run(const Grid& g, const RBXGeom& G, const S
         const float* zp = ph + sp * plane + o + lx;
         const float* ca = cf + (scf * 2) * cplane + co;
         const float* cr = ca + cplane;
-        CellF P;  // no index is read by the constant-coefficient stencil
-        P.base = 0;
-        P.oxm = P.oxp = P.oym = P.oyp = P.ozm = P.ozp = 0;
         float nv[NR];
 #pragma unroll
         for (int m = 0; m < NR; m++) {
             const int r = m * ROWSTEP;
             const float* c = c0 + r;
-            float dg;
-            const float L = stag_lface_acc<float, 3, 1, C>(
-                A, P,
+            // ca holds the diagonal (stag_diag1), which stag_lface_acc forms
+            // from alpha; stag_l1_f32 is its FP32 visc_type 1 operator
+            const float dg = ca[r];
+            const float L = stag_l1_f32<float, 3, C>(
                 [&](int a, int b, int cz) {
                     return cz < 0   ? zm[r]
                            : cz > 0 ? zp[r]
@@ -249,7 +248,7 @@ __device__ __forceinline__ bool rbx_run(const Grid& g, const RBXGeom& G, const S
                            : a > 0  ? c[lxp]
                                     : c[lx];
                 },
-                [&](int, int, int, int) { return 0.0f; }, [&]() { return ca[r]; }, dg);
+                dg, bq);
             nv[m] = c[lx] + sm_quot(omega * (cr[r] - L), dg);
         }
 #pragma unroll

@@ -156,6 +156,14 @@ static int build_mg(fhd_ctx* ctx, Multigrid<T>& M) {
                 L.alpha[c] = L.own_alpha0[c];
             }
         }
+        // the levels the row-tile smoother can take (rbx_geom: FP32, 3D,
+        // visc_type 1, x extent 64 to 256)
+        if (!std::is_same<T, double>::value && dim == 3 && ctx->visc == 1 && L.g.n[0] >= 64 &&
+            L.g.n[0] <= RBX_MAXNX)
+            for (int c = 0; c < 3; c++) {
+                L.rbx_diag[c] = A.alloc<T>(nc);
+                if (!L.rbx_diag[c]) return FHD_ERR_OOM;
+            }
     }
     const int ncl = nlevs_mg(ctx->g0, ctx->p.mg_minwidth);
     M.c.resize(ncl);
@@ -219,6 +227,16 @@ static int wall_diag(fhd_ctx* ctx) {
                 if (!L.diag[c]) return FHD_ERR_OOM;
             }
     return 0;
+}
+
+// the visc_type 1 diagonal of one component (stag_diag1, the expression of
+// stag_lface_acc) for the row-tile smoother; beta is constant (beta[0])
+template <typename T, int DIM>
+__global__ void __launch_bounds__(256) k_stag_diag1(i64 n, T* out, const T* alpha, T alpha_scale, const T* beta,
+                                                    T q) {
+    const T b = beta[0];
+    for (i64 f = blockIdx.x * (i64)blockDim.x + threadIdx.x; f < n; f += (i64)gridDim.x * blockDim.x)
+        out[f] = stag_diag1<T, DIM>(alpha_scale * alpha[f], b, q);
 }
 
 template <typename T>
@@ -291,6 +309,15 @@ static int prepare_T(fhd_ctx* ctx) {
         }
         if (rc) return rc;
         C.alpha_scale = T(1);
+    }
+    for (StagLevel<T>& L : M.s) {
+        if (!L.rbx_diag[0]) continue;
+        const StagOp<T> A = L.op();
+        const int nb = flat_blocks(L.g.nc);
+        for (int c = 0; c < 3; c++) {
+            k_stag_diag1<T, 3><<<nb, 256, 0, st>>>(L.g.nc, L.rbx_diag[c], L.alpha[c], L.alpha_scale, L.beta, A.q);
+            FHD_POST(ctx);
+        }
     }
     // pressure multigrid coefficients: alphainv on the finest level
     {
@@ -556,8 +583,9 @@ static int stag_rbx_smooth(fhd_ctx* ctx, StagLevel<float>& L, const RBXGeom& G, 
         R.src[c] = a[c];
         R.dst[c] = b[c];
         R.rhs[c] = L.rhs[c];
-        R.alpha[c] = L.alpha[c];
+        R.diag[c] = L.rbx_diag[c];
     }
+    if (!R.diag[0]) return FHD_ERR_UNSUPPORTED;
     R.err = ctx->dev_err;
     const bool timed = ctx->prof && L.g.nc == ctx->g0.nc;
     if (timed) {
@@ -588,7 +616,7 @@ static bool stag_aligned(const StagLevel<T>& L, int dim) {
     bool aligned = true;
     for (int c = 0; c < dim; c++)
         aligned = aligned && rb_aligned(L.phi[c]) && rb_aligned(L.tmp[c]) && rb_aligned(L.rhs[c]) &&
-                  rb_aligned(L.alpha[c]);
+                  rb_aligned(L.alpha[c]) && (!L.rbx_diag[c] || rb_aligned(L.rbx_diag[c]));
     return aligned;
 }
 

@@ -169,6 +169,9 @@ struct StagLevel {
     T* rhs[3] = {nullptr, nullptr, nullptr};
     T* tmp[3] = {nullptr, nullptr, nullptr};   // residual / L phi
     T* diag[3] = {nullptr, nullptr, nullptr};  // two-pass smoother
+    // the visc_type 1 diagonal alpha_scale alpha + 2 dim beta q, staged by the
+    // row-tile smoother in place of alpha (FP32 3D levels 64 to 256 wide)
+    T* rbx_diag[3] = {nullptr, nullptr, nullptr};
     StagOp<T> op() const {
         StagOp<T> A;
         for (int c = 0; c < 3; c++) { A.alpha[c] = alpha[c]; A.bed[c] = bed[c]; }
