@@ -139,9 +139,11 @@ static uint64_t request_bytes(const fhd_request* r) {
     const int m = r->params.gmres_max_inner;
     const double s = r->precision == FHD_PREC_MIXED ? 4.0 : 8.0;
     // multigrid: per level phi, rhs, tmp, alpha (dim each), beta, gamma,
-    // edges; cc: a (dim), phi, rhs, tmp; level sums to 8/7 (3D) or 4/3 (2D)
+    // edges, in mixed 3D the row-tile smoother's diagonal (dim); cc: a (dim),
+    // phi, rhs, tmp; level sums to 8/7 (3D) or 4/3 (2D)
     const double lv = dim == 3 ? 8.0 / 7.0 : 4.0 / 3.0;
-    const double mg = (4.0 * dim + 2 + nE + dim + 3 + 2 * dim + 1) * s * lv;
+    const double rbx = (r->precision == FHD_PREC_MIXED && dim == 3) ? dim : 0;
+    const double mg = (4.0 * dim + 2 + nE + dim + 3 + 2 * dim + 1 + rbx) * s * lv;
     const double krylov = (double)(m + 1 + 4) * (dim + 1) * 8.0;
     const double step = (39.0 + ns * (2 + dim)) * 8.0;
     const double mass = ns > 1 ? (ns * ns + ns + dim * ns) * s : 0.0;
