@@ -815,8 +815,9 @@ def main():
                      "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": (achieved / hbm) if achieved else None,
                      # ncu DRAM read + write of one launch of the same kernel
-                     # on the 256^3 finest level (622.7 + 178.5 MB)
-                     "traffic": (622.7 + 178.5) * 1e6,
+                     # on the 256^3 finest level (635.5 + 181.4 MB; the
+                     # capture summarised in profiles/k_stag_rbx_256cube_mixed.md)
+                     "traffic": (635.5 + 181.4) * 1e6,
                      "traffic_source": "ncu capture of one 256^3 launch",
                      "peak_kind": peak_kind, "launches_timed": n_l,
                      "avg_launch_us": (ms_l / n_l * 1e3) if n_l else None,
