@@ -815,8 +815,7 @@ def main():
                      "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": (achieved / hbm) if achieved else None,
                      # ncu DRAM read + write of one launch of the same kernel
-                     # on the 256^3 finest level (635.5 + 181.4 MB; the
-                     # capture summarised in profiles/k_stag_rbx_256cube_mixed.md)
+                     # on the 256^3 finest level (635.5 + 181.4 MB)
                      "traffic": (635.5 + 181.4) * 1e6,
                      "traffic_source": "ncu capture of one 256^3 launch",
                      "peak_kind": peak_kind, "launches_timed": n_l,
