@@ -377,8 +377,9 @@ int fhd_dev_compute_mass_fluxdiv(fhd_ctx* ctx, const fhd_mixture_params* mp,
  * multifab).  FP64.  nspecies 2..5.
  * Walls (fhd_ctx_create_bc codes 100, 200): on a wall face the ghost cell is
  * the first-order extrapolation of the interior cell (scalar_bc,
- * inhomogeneous_bc_val.f90:21-54).  The host-fab entry
- * fhd_compute_sqrtLonsager_fc refuses walls. */
+ * inhomogeneous_bc_val.f90:21-54).  The high wall face is not stored; the
+ * host-fab entry fhd_compute_sqrtLonsager_fc writes it (the last cell with
+ * its extrapolated ghost) into the face fab's nodal plane hi+1. */
 int fhd_dev_compute_sqrtLonsager_fc(fhd_ctx* ctx, const fhd_mixture_params* mp,
                                     const fhd_stoch_params* sp,
                                     const double* const rho[],

@@ -551,11 +551,57 @@ int fhd_stag_mg_solve(fhd_ctx* ctx, const fhd_multifab* alpha_fc, const fhd_mult
     return rc;
 }
 
+// walls: the high wall face of direction d is the fab's nodal plane hi+1,
+// which the periodic scatter fills from face 0; write the wall's own factors
+// (sqrtL_high_wall_plane) there.  One whole-domain fab, nodal in d; in the
+// other directions its ghost positions wrap where periodic and clamp at a
+// wall.
+static int put_sqrtL_high_wall(fhd_ctx* ctx, const fhd_mixture_params* mp, const fhd_stoch_params* sp,
+                               const double* const rho[], int d, int ncomp, const fhd_multifab& mf) {
+    const int dim = ctx->dim;
+    if (mf.nfabs != 1) {
+        set_last_error("compute_sqrtLonsager_fc with walls: one whole-domain fab per direction expected");
+        return FHD_ERR_BAD_ARG;
+    }
+    const fhd_fab& f = mf.fabs[0];
+    const FabDesc fd = desc_of(f, dim);
+    for (int k = 0; k < dim; k++)
+        if (fd.lo[k] != 0 || fd.hi[k] != ctx->n[k] - 1 || fd.nodal[k] != (k == d ? 1 : 0)) {
+            set_last_error("compute_sqrtLonsager_fc with walls: one whole-domain face fab per direction expected");
+            return FHD_ERR_BAD_ARG;
+        }
+    const int u = d == 0 ? 1 : 0, v = d == 2 ? 1 : 2;
+    const i64 nu = ctx->n[u], nv = v < dim ? ctx->n[v] : 1, np = nu * nv;
+    DevArrays P;
+    if (int rc = P.alloc(ncomp, np)) return rc;
+    if (int rc = sqrtL_high_wall_plane(ctx, mp, sp, rho, d, P.a.data())) return rc;
+    std::vector<double> h((size_t)np);
+    const i64 ne = fab_elems(fd);
+    for (int q = 0; q < ncomp; q++) {
+        FHD_CUDA_TRY(cudaMemcpy(h.data(), P.a[q], sizeof(double) * np, cudaMemcpyDeviceToHost));
+        double* base = f.data + (i64)q * ne;
+        auto pos = [&](int k, int e) {  // fab offset e along direction k -> cell index
+            const int c = e - fd.ng;
+            if (ctx->walls.lo[k] == 0) return ((c % ctx->n[k]) + ctx->n[k]) % ctx->n[k];
+            return c < 0 ? 0 : (c >= ctx->n[k] ? ctx->n[k] - 1 : c);
+        };
+        const int eu = fd.ext[u], ev = v < dim ? fd.ext[v] : 1;
+        for (int b = 0; b < ev; b++)
+            for (int a = 0; a < eu; a++) {
+                int o[3] = {0, 0, 0};
+                o[d] = fd.ng + ctx->n[d];  // the nodal plane hi+1
+                o[u] = a;
+                if (v < dim) o[v] = b;
+                const i64 src = (i64)pos(u, a) + nu * (v < dim ? (i64)pos(v, b) : 0);
+                base[(i64)o[0] + (i64)fd.ext[0] * ((i64)o[1] + (i64)fd.ext[1] * o[2])] = h[(size_t)src];
+            }
+    }
+    return 0;
+}
+
 int fhd_compute_sqrtLonsager_fc(fhd_ctx* ctx, const fhd_mixture_params* mp, const fhd_stoch_params* sp,
                                 const fhd_multifab* rho, const fhd_multifab* rhotot,
                                 const fhd_multifab* sqrtLonsager_fc) {
-    // the periodic scatter would give the high wall face the low one's value
-    if (int wr = refuse_walls(ctx, "fhd_compute_sqrtLonsager_fc (host fabs)")) return wr;
     if (!ctx || !mp || !sp || !rho || !sqrtLonsager_fc) return FHD_ERR_BAD_ARG;
     if (mp->nspecies < 2 || mp->nspecies > 5) return FHD_ERR_UNSUPPORTED;
     const int dim = ctx->dim, ns = mp->nspecies;
@@ -575,6 +621,9 @@ int fhd_compute_sqrtLonsager_fc(fhd_ctx* ctx, const fhd_mixture_params* mp, cons
     for (int d = 0; d < dim; d++) {
         std::vector<const double*> src(d_L + d * ns * ns, d_L + (d + 1) * ns * ns);
         if ((rc = dev_to_mf_comps(ctx, src.data(), ns * ns, sqrtLonsager_fc[d]))) return rc;
+        if (ctx->has_walls && ctx->walls.lo[d] != 0 &&
+            (rc = put_sqrtL_high_wall(ctx, mp, sp, crho.data(), d, ns * ns, sqrtLonsager_fc[d])))
+            return rc;
     }
     return 0;
 }

@@ -1300,6 +1300,54 @@ static int check_mix(const fhd_mixture_params* mp) {
 }
 }  // namespace fhd
 
+namespace fhd {
+// the factors on the high wall face of direction d (not stored in the
+// periodic layout): the last cell layer i_d = n_d - 1 with its extrapolated
+// ghost (scalar_bc, inhomogeneous_bc_val.f90:21-54), one value per cell of
+// the layer, in-plane index u + n_u v over the two other directions u < v
+template <int NS>
+__global__ void __launch_bounds__(128) k_sqrtL_hi_plane(Grid g, MixDev m, int d, SqrtLArgs a) {
+    const int u = d == 0 ? 1 : 0, v = d == 2 ? 1 : 2;
+    const i64 nu = g.n[u], np = nu * g.n[v];
+    for (i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x; t < np; t += (i64)gridDim.x * blockDim.x) {
+        int q[3] = {0, 0, 0};
+        q[d] = g.n[d] - 1;
+        q[u] = (int)(t % nu);
+        q[v] = (int)(t / nu);
+        const i64 f = (i64)q[0] + (i64)g.n[0] * ((i64)q[1] + (i64)g.n[1] * q[2]);
+        double L[NS][NS];
+        d_face_sqrtL<double, NS>(m, a.rho, f, f, L);
+#pragma unroll
+        for (int r = 0; r < NS; r++)
+#pragma unroll
+            for (int c = 0; c < NS; c++) a.out[r + NS * c][t] = L[r][c];
+    }
+}
+
+int sqrtL_high_wall_plane(fhd_ctx* ctx, const fhd_mixture_params* mp, const fhd_stoch_params* sp,
+                          const double* const rho[], int d, double* const plane[]) {
+    if (int rc = check_mix(mp)) return rc;
+    const MixDev m = make_mixdev(mp, sp);
+    SqrtLArgs a;
+    memset(&a, 0, sizeof(a));
+    for (int s = 0; s < m.ns; s++) a.rho[s] = rho[s];
+    for (int q = 0; q < m.ns * m.ns; q++) a.out[q] = plane[q];
+    const Grid g = ctx->g0;
+    const i64 np = g.nc / g.n[d];
+    const int nb = (int)((np + 127) / 128);
+    switch (m.ns) {
+        case 2: k_sqrtL_hi_plane<2><<<nb, 128, 0, ctx->stream>>>(g, m, d, a); break;
+        case 3: k_sqrtL_hi_plane<3><<<nb, 128, 0, ctx->stream>>>(g, m, d, a); break;
+        case 4: k_sqrtL_hi_plane<4><<<nb, 128, 0, ctx->stream>>>(g, m, d, a); break;
+        default: k_sqrtL_hi_plane<5><<<nb, 128, 0, ctx->stream>>>(g, m, d, a); break;
+    }
+    ctx->launches++;
+    FHD_CUDA_TRY(cudaPeekAtLastError());
+    FHD_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    return 0;
+}
+}  // namespace fhd
+
 extern "C" int fhd_dev_compute_sqrtLonsager_fc(fhd_ctx* ctx, const fhd_mixture_params* mp,
                                                const fhd_stoch_params* sp, const double* const rho[],
                                                double* const sqrtLonsager_fc[]) {

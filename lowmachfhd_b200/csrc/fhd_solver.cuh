@@ -338,4 +338,9 @@ int sync_scalars(fhd_ctx* ctx, int first, int count);
 int dev_err_check(fhd_ctx* ctx);
 int mass_fluxdiv(fhd_ctx* ctx, const fhd_mixture_params* mp, const fhd_stoch_params* sp, const double* const rho[],
                  double dt, const double* weights, int n_rngs, const double* const W[], double* const fluxdiv[]);
+// compute_sqrtLonsager_fc on the high wall face of direction d (stored by
+// neither layout): plane[r + ns*c] holds nc / n[d] values, in-plane index
+// u + n_u v over the other two directions u < v
+int sqrtL_high_wall_plane(fhd_ctx* ctx, const fhd_mixture_params* mp, const fhd_stoch_params* sp,
+                          const double* const rho[], int d, double* const plane[]);
 }  // namespace fhd

@@ -7,8 +7,8 @@ fhd_dev_compute_sqrtLonsager_fc (first-order extrapolated concentrations at
 walls, scalar_bc), FP64 and mixed; the host-fab fhd_stochastic_m_fluxdiv
 (the high wall's edge planes taken from the nodal fabs) and
 fhd_stochastic_mass_fluxdiv (the high wall face of a flux fab is zero, as
-the periodic scatter writes it), and the refusal of the host-fab
-fhd_compute_sqrtLonsager_fc."""
+the periodic scatter writes it), and the host-fab
+fhd_compute_sqrtLonsager_fc (the high wall face written from its own plane)."""
 import numpy as np
 import pytest
 
@@ -97,12 +97,6 @@ def test_stochastic_mass_fluxdiv_walls(cuda, dim, n, bc_lo, bc_hi):
                                   dev(sqrtL, cuda), 0.1, W8, dev(W_fc, cuda), div, flux, increment=True)
     assert P.rel_inf(host(div), ref_div) < 1e-12
     assert P.rel_inf(host(flux), ref_flux) < 1e-12
-
-
-def test_host_fab_entries_refuse_walls(cuda):
-    with solver(2, [16, 16], [PE, NS, PE], [PE, NS, PE]) as s:
-        assert L._capi.lib().fhd_compute_sqrtLonsager_fc(s._h, None, None, None, None,
-                                                        None) == L._capi.FHD_ERR_UNSUPPORTED
 
 
 @pytest.mark.parametrize("dim,n,bc_lo,bc_hi", [CASES[2], CASES[4], CASES[5]])
@@ -226,3 +220,38 @@ def test_stochastic_mass_fluxdiv_host_fabs_walls(cuda, dim, n, bc_lo, bc_hi):
     assert_mf(div_f, ref_div, dim, n, [0] * dim, 1, 1, 1e-12)
     for d in range(dim):
         assert_mf(flux_f[d], ref_flux[d * ns:(d + 1) * ns], dim, n, face_nodal(dim, d), 0, 1, 1e-12)
+
+
+@pytest.mark.parametrize("dim,n,bc_lo,bc_hi", [CASES[0], CASES[4]])
+def test_compute_sqrtLonsager_fc_host_fabs_walls(cuda, dim, n, bc_lo, bc_hi):
+    """faces 0 .. n-1 as the device entry, and the fab's nodal plane hi+1 of
+    a wall direction the high wall's own factor: the last cell with its
+    extrapolated ghost, which is face 0 of the density flipped along d"""
+    from tests.test_gpu_boundary import face_nodal, mf
+    from tests.test_gpu_multispecies import lmix
+    from tests.test_oracle_multispecies import mix, state
+    ns = 3
+    sp = dict(k_B=1e-4, variance_coef_mom=1.0, dV=1.0, stoch_stress_form=1, filtering_width=0)
+    rho = state(dim, n, ns, amp=1e-2)
+    shape = [n[k] for k in reversed(range(dim))]
+    O.set_walls(bc_lo, bc_hi)
+    ref = O.sqrtLonsager_fc(dim, n, O.StochParams(**sp), mix(ns), rho)
+    out = [mf([np.zeros(P.nc_of(dim, n))] * (ns * ns), dim, n, face_nodal(dim, d), 0, 1) for d in range(dim)]
+    with solver(dim, n, bc_lo, bc_hi) as s:
+        s.compute_sqrtLonsager_fc_fab(lmix(ns), L.StochParams(**sp), mf(rho, dim, n, [0] * dim, 1, 1), None, out)
+    scale = max(float(np.max(np.abs(x))) for x in ref)
+    for d in range(dim):
+        data = out[d][0].data
+        flip = None
+        if bc_lo[d] != PE:
+            ax = dim - 1 - d
+            flip = O.sqrtLonsager_fc(dim, n, O.StochParams(**sp), mix(ns),
+                                     [np.flip(r.reshape(shape), axis=ax).ravel() for r in rho])
+        for q in range(ns * ns):
+            arr = data[..., q]
+            got = arr[tuple(slice(0, n[k]) for k in range(dim))].T.ravel()
+            assert np.max(np.abs(got - ref[d * ns * ns + q])) <= 1e-12 * scale
+            if flip is not None:
+                hi_plane = np.take(arr, n[d], axis=d)  # Fortran axes: x, y, (z) without d
+                want = np.take(flip[d * ns * ns + q].reshape(shape), 0, axis=dim - 1 - d).T
+                assert np.max(np.abs(hi_plane - want)) <= 1e-12 * scale
