@@ -301,13 +301,6 @@ struct fhd_ctx {
     long long prof_launches = 0;
 };
 
-// the timestep and stochastic-flux entries are built for periodic boxes
-inline int refuse_walls(const fhd_ctx* ctx, const char* what) {
-    if (!ctx || !ctx->has_walls) return 0;
-    fhd::set_last_error(std::string(what) + ": the context has walls; this entry is built for periodic boxes");
-    return FHD_ERR_UNSUPPORTED;
-}
-
 namespace fhd {
 constexpr int NSCAL = 256;
 // scalar slots
