@@ -1116,9 +1116,10 @@ static std::map<std::string, int> g_tune_import;  // imported choices (candidate
 
 // A plan is keyed by the level shape and by what decides the candidate
 // list: the device's SM count and shared-memory limits, and the version of
-// the candidate lists (bumped whenever a list or its order changes), so a
-// table from another GPU model or library version selects nothing.
-constexpr int TUNE_CANDS_VERSION = 4;
+// the candidate lists (bumped whenever a list, its order or a candidate's
+// kernel changes), so a table from another GPU model or library version
+// selects nothing.
+constexpr int TUNE_CANDS_VERSION = 5;
 
 static std::string tune_key_of(int dev, int which, int elem, int dim, int visc, const int n[3], int sms, int optin,
                                int smem_sm) {
