@@ -1,4 +1,5 @@
-"""Fluctuation-dissipation balance of the discrete operators with walls.
+"""Fluctuation-dissipation balance of the discrete operators, with walls and
+periodic.
 
 With eta = T = 1, unit variance and the non-symmetric stress (stoch_stress_form
 0), the stochastic momentum flux divergence (stochastic_m_fluxdiv.f90:42-602)
@@ -28,13 +29,15 @@ def periodic_afterwards():
     O.set_walls()
 
 
-def stochastic_map(dim, n, bc_lo):
-    """the columns of D: the divergence for each unit noise entry"""
+def stochastic_map(dim, n, bc_lo, form=0):
+    """the columns of D: the divergence for each unit noise entry (form 1:
+    the symmetric stress, cell noise of variance 2 and one noise shared by
+    both components of an edge, as fill_m_stochastic draws them)"""
     nc = int(np.prod(n[:dim]))
     nE = 1 if dim == 2 else 3
     ne = [int(np.prod(edge_shape(dim, n, e, bc_lo))) for e in range(nE)]
     # variance sqrt(vc 2 k_B / (dV dt)) = 1
-    sp = O.StochParams(k_B=0.5, variance_coef_mom=1.0, dV=1.0, stoch_stress_form=0, filtering_width=0)
+    sp = O.StochParams(k_B=0.5, variance_coef_mom=1.0, dV=1.0, stoch_stress_form=form, filtering_width=0)
     one = np.ones(nc)
     one_ed = [np.ones(m) for m in ne]
     W_cc0 = [np.zeros(nc) for _ in range(dim)]
@@ -48,21 +51,29 @@ def stochastic_map(dim, n, bc_lo):
     for c in range(dim):
         for i in range(nc):
             W = [w.copy() for w in W_cc0]
-            W[c][i] = 1.0
+            W[c][i] = np.sqrt(2.0) if form == 1 else 1.0
             apply(W, W_ed0)
     for q in range(2 * nE):
+        if form == 1 and q % 2 == 1:
+            continue  # the second component carries the first one's noise
         for i in range(ne[q // 2]):
             W = [w.copy() for w in W_ed0]
             W[q][i] = 1.0
+            if form == 1:
+                W[q + 1][i] = 1.0
             apply(W_cc0, W)
     return np.array(cols).T
 
 
-def minus_viscous(dim, n):
-    """the matrix of -L u (apply_matrix with theta 0 and zero pressure)"""
+def minus_viscous(dim, n, visc=1):
+    """the matrix of -L u (apply_matrix with theta 0 and zero pressure),
+    eta = 1"""
     nc = int(np.prod(n[:dim]))
-    pb = P.problem(dim, n, 1, dx=1.0, seed=1)
+    pb = P.problem(dim, n, visc, dx=1.0, seed=1)
     pb.beta[:] = 1.0
+    for e in pb.beta_ed:
+        e[:] = 1.0
+    pb.gamma[:] = 0.0
     cols = []
     for c in range(dim):
         for i in range(nc):
@@ -122,3 +133,13 @@ def test_the_balance_fails_without_the_wall_factor():
                 Dm[:, 2 * nc + comp * ne + idx] /= np.sqrt(2.0)
     Dm = Dm[keep]
     assert np.max(np.abs(Dm @ Dm.T - A)) > 0.1 * np.max(np.abs(A))
+
+
+@pytest.mark.parametrize("dim,n", [(2, [6, 4]), (3, [4, 4, 4])])
+@pytest.mark.parametrize("form,visc", [(0, 1), (1, 2)])
+def test_periodic_covariance_is_the_viscous_operator(dim, n, form, visc):
+    """periodic box: the non-symmetric stress balances visc_type 1 (eta
+    Lap u), the symmetric one visc_type 2 (div eta (grad u + grad u^T))"""
+    D = stochastic_map(dim, n, [PE, PE, PE], form)
+    A = minus_viscous(dim, n, visc)
+    assert np.max(np.abs(D @ D.T - A)) < 1e-12 * np.max(np.abs(A))
