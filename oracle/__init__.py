@@ -177,6 +177,17 @@ def macproject(dim, n, dx, params, alphainv, rhs):
     return phi
 
 
+def macproject_history(dim, n, dx, params, alphainv, rhs):
+    """per-V-cycle L2 residual ratios of the pressure multigrid from a zero
+    guess (mg_max_vcycles cycles, no stopping test)"""
+    phi = np.zeros(int(np.prod(n[:dim])))
+    hist = np.zeros(params.mg_max_vcycles)
+    rc = lib().or_macproject_history(dim, _n3(n), C.c_double(dx), C.byref(params), _p(phi), _pp(alphainv), _p(rhs),
+                                     _p(hist))
+    assert rc == 0
+    return hist
+
+
 def apply_matrix(pb: Problem, theta, x_u, x_p, order=2):
     """apply_matrix.f90:24-157; order = gmres_spatial_order (2, or 4 with
     visc_type 1)"""

@@ -730,7 +730,7 @@ void c_vcycle(std::vector<CLevel>& L, int l, const fhd_gmres_params* p) {
 }
 
 int macproject_impl(const Geo& g0, const fhd_gmres_params* p, double* phi, const double* const ainv[],
-                    const double* rhs) {
+                    const double* rhs, double* hist = nullptr) {
     const int dim = g0.dim;
     const int nl = nlevs_mg(g0, p->mg_minwidth);
     std::vector<CLevel> L(nl);
@@ -752,7 +752,23 @@ int macproject_impl(const Geo& g0, const fhd_gmres_params* p, double* phi, const
     }
     std::copy(rhs, rhs + g0.nc, L[0].rhs.begin());
     const double r0 = reduce_max(g0, [&](int i, int j, int k) { return std::fabs(rhs[g0.id(i, j, k)]); });
-    if (r0 > 0.0) {
+    if (hist) {
+        // the L2 residual after each of mg_max_vcycles V-cycles over the
+        // initial one, without the stopping test (the reference's multigrid
+        // residual histories, run_result/Mg_StagMg_performance)
+        auto l2 = [&](bool with_phi) {
+            CLevel& C = L[0];
+            return std::sqrt(reduce_sum(g0, [&](int i, int j, int k) {
+                const double r = C.rhs[g0.id(i, j, k)] - (with_phi ? c_lap(g0, C.a, C.phi.data(), i, j, k, nullptr) : 0.0);
+                return r * r;
+            }));
+        };
+        const double n0 = l2(false);
+        for (int vc = 0; vc < p->mg_max_vcycles; vc++) {
+            c_vcycle(L, 0, p);
+            hist[vc] = n0 > 0.0 ? l2(true) / n0 : 0.0;
+        }
+    } else if (r0 > 0.0) {
         for (int vc = 1; vc <= p->mg_max_vcycles; vc++) {
             c_vcycle(L, 0, p);
             if (vc == p->mg_max_vcycles) break;
@@ -1972,6 +1988,12 @@ int or_macproject(int dim, const int n[3], double dx, const fhd_gmres_params* p,
                   const double* const alphainv_fc[], const double* rhs) {
     Geo g(dim, n, dx);
     return macproject_impl(g, p, phi, alphainv_fc, rhs);
+}
+
+int or_macproject_history(int dim, const int n[3], double dx, const fhd_gmres_params* p, double* phi,
+                          const double* const alphainv_fc[], const double* rhs, double* hist) {
+    Geo g(dim, n, dx);
+    return macproject_impl(g, p, phi, alphainv_fc, rhs, hist);
 }
 
 int or_apply_matrix(int dim, const int n[3], double dx, int visc_type, double* const b_u[], double* b_p,

@@ -56,6 +56,10 @@ int or_macproject(int dim, const int n[3], double dx,
                   const fhd_gmres_params* p,
                   double* phi, const double* const alphainv_fc[],
                   const double* rhs);
+/* the same with the L2 residual ratio after each of mg_max_vcycles
+ * V-cycles (no stopping test) in hist */
+int or_macproject_history(int dim, const int n[3], double dx, const fhd_gmres_params* p, double* phi,
+                          const double* const alphainv_fc[], const double* rhs, double* hist);
 
 int or_apply_matrix(int dim, const int n[3], double dx, int visc_type,
                     double* const b_u[], double* b_p,
