@@ -143,3 +143,46 @@ def test_wall_faces_of_apply_matrix_are_zero():
     b_u, _ = O.apply_matrix(pb, 1.5, u, p)
     assert np.all(b_u[0].reshape(8, 12)[:, 0] == 0.0)
     assert np.any(b_u[0].reshape(8, 12)[:, 1:] != 0.0)
+
+
+# per-V-cycle reductions at the end of the reference's stored 64^3 staggered
+# multigrid histories (run_result/Mg_StagMg_performance/3d_{periodic,
+# dirichelt,slip}_precon_finegridGS_8botsmooth_vel.dat, column 2)
+STAG_REF_LAST = {"periodic": 0.0973, "noslip": 0.1007, "slip": 0.1479}
+
+
+def _stag_rates(bc, seed=10):
+    dim, n = 3, [64, 64, 64]
+    nc = 64 ** 3
+    rng = np.random.default_rng(seed)
+    O.set_walls(bc, bc)
+    pb = O.Problem(dim, n, 1.0, 1, [np.ones(nc)] * 3, np.ones(nc), [np.ones(nc)] * 3, np.zeros(nc))
+    rhs = [rng.uniform(size=nc) for _ in range(3)]
+    rhs = [r - r.mean() for r in rhs]
+    if bc[0] != -1:
+        for c in range(3):
+            a = rhs[c].reshape(64, 64, 64)
+            idx = [slice(None)] * 3
+            idx[2 - c] = 0
+            a[tuple(idx)] = 0.0
+    p = O.default_params(stag_mg_max_vcycles=11, stag_mg_rel_tol=1e-16)
+    h = O.stag_mg_history(pb, p, 0.0, rhs)
+    O.set_walls()
+    return h[1:] / h[:-1]
+
+
+def test_wall_multigrid_rates_match_the_reference_histories():
+    """The staggered multigrid on 64^3 steady Stokes velocity problems walled
+    on every side: the per-V-cycle reduction after ten cycles lies within 15 %
+    of the reference's stored histories, and slip walls slow the cycle by the
+    reference's factor (1.53 against periodic) while no-slip walls barely do
+    (1.04).  A behavioural pin of the wall rules in the smoother, residual and
+    transfers; the stored runs' right-hand sides are not recorded."""
+    last = {k: _stag_rates(bc)[-1] for k, bc in
+            [("periodic", [-1] * 3), ("noslip", [O.NO_SLIP_WALL] * 3), ("slip", [O.SLIP_WALL] * 3)]}
+    for k, v in last.items():
+        assert abs(v - STAG_REF_LAST[k]) < 0.15 * STAG_REF_LAST[k], (k, v)
+    ratio = last["slip"] / last["periodic"]
+    ref_ratio = STAG_REF_LAST["slip"] / STAG_REF_LAST["periodic"]
+    assert abs(ratio - ref_ratio) < 0.1 * ref_ratio, (ratio, ref_ratio)
+    assert 1.0 <= last["noslip"] / last["periodic"] < 1.1
