@@ -94,7 +94,11 @@ typedef struct fhd_stoch_params {
     double variance_coef_mom;
     double dV;
     int    stoch_stress_form;      /* 0 non-symmetric, 1 symmetric */
-    int    filtering_width;        /* only 0 is supported */
+    int    filtering_width;        /* 0 off; 1, 2 or 4: the stress filter of
+                                      filter_stoch_m_flux (stochastic_m_fluxdiv.f90:
+                                      604-778), periodic boxes only (walls:
+                                      FHD_ERR_UNSUPPORTED); another width, or one
+                                      above a domain side: FHD_ERR_BAD_ARG */
 } fhd_stoch_params;
 
 /* Multispecies mixture parameters (namelist probin_multispecies,

@@ -208,7 +208,8 @@ class StokesSolver:
 
     def stochastic_m_fluxdiv(self, sp: StochParams, stoch_m_force, increment, eta, eta_ed, temperature,
                              temperature_ed, dt, weights, W_cc, W_ed):
-        """stochastic_m_fluxdiv (stochastic_m_fluxdiv.f90:42-602).
+        """stochastic_m_fluxdiv (stochastic_m_fluxdiv.f90:42-778), with the
+        stress filter of sp.filtering_width 1, 2 or 4 on periodic boxes.
         W_cc: n_rngs*dim cell tensors, W_ed: n_rngs*2*nE node/edge tensors."""
         w = (C.c_double * len(weights))(*[float(x) for x in weights])
         return check(lib().fhd_dev_stochastic_m_fluxdiv(self._h, C.byref(sp), _dpp(stoch_m_force),

@@ -263,6 +263,9 @@ struct fhd_ctx {
     // inertial-step work arrays (allocated on the first step)
     bool step_ready = false;
     double* sb[128] = {nullptr};
+    // the filtered stochastic stresses (filtering_width != 0): two sets of
+    // dim + 2 * edge-set arrays in the context's precision, on first use
+    void* stoch_filt = nullptr;
     // CUDA graphs of the preconditioner applications inside GMRES, keyed by
     // the operand pointers and the prepared coefficients (-1 auto, 0 off,
     // 1 on)

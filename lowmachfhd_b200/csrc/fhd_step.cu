@@ -1,9 +1,10 @@
 // fhd_step.cu -- stochastic momentum flux divergence and the device-resident
 // inertial predictor-corrector step of a single-species fluid.
 //
-// stochastic_m_fluxdiv.f90:42-602 (periodic, filtering_width = 0) and
+// stochastic_m_fluxdiv.f90:42-778 (homogeneous walls through mflux_bc; the
+// stress filter of filtering_width 1, 2, 4 on periodic boxes) and
 // advance_timestep_inertial.f90:45-923 (nspecies = 1, centred advection,
-// no gravity, periodic walls).
+// no gravity; periodic boxes or homogeneous walls).
 #include <cmath>
 #include <cstring>
 
@@ -143,13 +144,145 @@ __global__ void __launch_bounds__(256) k_stoch_m_w(Grid g, fhd::Walls W, EdgeExt
     }
 }
 
+// ---------------------------------------------------------------------
+// filtering_width 1, 2 or 4: the scaled stresses are written out, smoothed
+// by the separable filter of filter_stoch_m_flux (x, then y, then z;
+// stochastic_m_fluxdiv.f90:604-778) and then differenced
+// (stochastic_m_fluxdiv.f90:172-174, 226-230).  Array q of the stress set
+// s (q*nc + f): the dim cell stresses, then edge set e component comp at
+// dim + 2e + comp.  Periodic boxes.
+// ---------------------------------------------------------------------
+template <typename T, int DIM>
+__global__ void __launch_bounds__(256) k_stoch_stress(Grid g, StochArgs a, T* __restrict__ s) {
+    Cell P;
+    if (!cell_of_thread(g, P)) return;
+    constexpr int nE = DIM == 2 ? 1 : 3;
+    const i64 f = P.id(0, 0, 0), nc = g.nc;
+#pragma unroll
+    for (int c = 0; c < DIM; c++) s[c * nc + f] = stoch_cc<T>(a, DIM, c, f);
+#pragma unroll
+    for (int q = 0; q < 2 * nE; q++) s[(DIM + q) * nc + f] = stoch_ed<T>(a, nE, q / 2, q % 2, f);
+}
+
+// one filter pass along direction D over the nq arrays of the set; the
+// terms in the order of filter_stoch_m_flux, each division by a power of
+// two written as the exact product
+template <typename T, int W, int D>
+__global__ void __launch_bounds__(256) k_stoch_filter(Grid g, const T* __restrict__ in, T* __restrict__ out,
+                                                      int nq) {
+    Cell P;
+    if (!cell_of_thread(g, P)) return;
+    const i64 nc = g.nc, f = P.id(0, 0, 0);
+    i64 o[2 * W + 1];
+#pragma unroll
+    for (int s = -W; s <= W; s++) o[s + W] = P.id(D == 0 ? s : 0, D == 1 ? s : 0, D == 2 ? s : 0);
+    for (int q = 0; q < nq; q++) {
+        const T* a = in + q * nc;
+        auto at = [&](int s) { return ld(a, o[s + W]); };
+        T v;
+        if constexpr (W == 1) {
+            v = at(0) * T(0.5) + at(-1) * T(0.25) + at(1) * T(0.25);
+        } else if constexpr (W == 2) {
+            v = (T(5) * at(0)) * T(0.125) - at(-2) * T(0.0625) + at(-1) * T(0.25) - at(2) * T(0.0625) +
+                at(1) * T(0.25);
+        } else {
+            v = (T(93) * at(0)) * T(0.0078125) + (T(7) * at(-1)) * T(0.03125) - (T(7) * at(-2)) * T(0.015625) +
+                at(-3) * T(0.03125) - at(-4) * T(0.00390625) + (T(7) * at(1)) * T(0.03125) -
+                (T(7) * at(2)) * T(0.015625) + at(3) * T(0.03125) - at(4) * T(0.00390625);
+        }
+        out[q * nc + f] = v;
+    }
+}
+
+// k_stoch_m with the stresses read from the (filtered) set s
+template <typename T, int DIM>
+__global__ void __launch_bounds__(256) k_stoch_div(Grid g, const T* __restrict__ s, double* o0, double* o1,
+                                                   double* o2, int increment, double dxinv) {
+    Cell P;
+    if (!cell_of_thread(g, P)) return;
+    const i64 f = P.id(0, 0, 0), nc = g.nc;
+    const T dxi = (T)dxinv;
+    auto C = [&](int c, i64 q) { return ld(s + c * nc, q); };
+    auto E = [&](int e, int comp, i64 q) { return ld(s + (DIM + 2 * e + comp) * nc, q); };
+    T dv[3];
+    if constexpr (DIM == 2) {
+        dv[0] = (C(0, f) - C(0, P.id(-1, 0, 0))) * dxi + (E(0, 0, P.id(0, 1, 0)) - E(0, 0, f)) * dxi;
+        dv[1] = (E(0, 1, P.id(1, 0, 0)) - E(0, 1, f)) * dxi + (C(1, f) - C(1, P.id(0, -1, 0))) * dxi;
+    } else {
+        dv[0] = (C(0, f) - C(0, P.id(-1, 0, 0))) * dxi + (E(0, 0, P.id(0, 1, 0)) - E(0, 0, f)) * dxi +
+                (E(1, 0, P.id(0, 0, 1)) - E(1, 0, f)) * dxi;
+        dv[1] = (E(0, 1, P.id(1, 0, 0)) - E(0, 1, f)) * dxi + (C(1, f) - C(1, P.id(0, -1, 0))) * dxi +
+                (E(2, 0, P.id(0, 0, 1)) - E(2, 0, f)) * dxi;
+        dv[2] = (E(1, 1, P.id(1, 0, 0)) - E(1, 1, f)) * dxi + (E(2, 1, P.id(0, 1, 0)) - E(2, 1, f)) * dxi +
+                (C(2, f) - C(2, P.id(0, 0, -1))) * dxi;
+    }
+    double* o[3] = {o0, o1, o2};
+#pragma unroll
+    for (int c = 0; c < DIM; c++) o[c][f] = increment ? o[c][f] + (double)dv[c] : (double)dv[c];
+}
+
+template <typename T, int DIM>
+static int stoch_filtered(fhd_ctx* ctx, const StochArgs& a, int width, double* const force[], int increment) {
+    constexpr int nq = DIM + (DIM == 2 ? 2 : 6);
+    const Grid g = ctx->g0;
+    const i64 nc = g.nc;
+    if (!ctx->stoch_filt) {
+        ctx->stoch_filt = ctx->arena.alloc<T>(2 * (i64)nq * nc);
+        if (!ctx->stoch_filt) {
+            set_last_error("stochastic_m_fluxdiv: out of device memory for the filtered stresses");
+            return FHD_ERR_OOM;
+        }
+    }
+    T* s = (T*)ctx->stoch_filt;
+    T* t = s + (i64)nq * nc;
+    const dim3 gr = cell_grid(g), bl = cell_block();
+    k_stoch_stress<T, DIM><<<gr, bl, 0, ctx->stream>>>(g, a, s);
+    ctx->launches++;
+    for (int d = 0; d < DIM; d++) {
+        auto pass = [&](auto Wc) {
+            constexpr int W = decltype(Wc)::value;
+            if (d == 0) k_stoch_filter<T, W, 0><<<gr, bl, 0, ctx->stream>>>(g, s, t, nq);
+            else if (d == 1) k_stoch_filter<T, W, 1><<<gr, bl, 0, ctx->stream>>>(g, s, t, nq);
+            else k_stoch_filter<T, W, 2><<<gr, bl, 0, ctx->stream>>>(g, s, t, nq);
+        };
+        if (width == 1) pass(std::integral_constant<int, 1>());
+        else if (width == 2) pass(std::integral_constant<int, 2>());
+        else pass(std::integral_constant<int, 4>());
+        ctx->launches++;
+        T* x = s;
+        s = t;
+        t = x;
+    }
+    k_stoch_div<T, DIM><<<gr, bl, 0, ctx->stream>>>(g, s, force[0], force[1], DIM == 3 ? force[2] : nullptr,
+                                                     increment, a.dxinv);
+    ctx->launches++;
+    FHD_CUDA_TRY(cudaPeekAtLastError());
+    return 0;
+}
+
 int stoch_launch(fhd_ctx* ctx, const fhd_stoch_params* sp, double* const force[], int increment, const double* eta,
                  const double* const eta_ed[], const double* T, const double* const T_ed[], double dt,
                  const double* weights, int n_rngs, const double* const W_cc[], const double* const W_ed[]) {
     const int dim = ctx->dim, nE = dim == 2 ? 1 : 3;
-    if (n_rngs < 1 || n_rngs > 4 || sp->filtering_width != 0) {
-        set_last_error("stochastic_m_fluxdiv: n_rngs must be 1..4 and filtering_width 0");
+    const int width = sp->filtering_width;
+    if (n_rngs < 1 || n_rngs > 4) {
+        set_last_error("stochastic_m_fluxdiv: n_rngs must be 1..4");
         return FHD_ERR_UNSUPPORTED;
+    }
+    if (width != 0 && width != 1 && width != 2 && width != 4) {
+        set_last_error("stochastic_m_fluxdiv: filtering_width must be 0, 1, 2 or 4");
+        return FHD_ERR_BAD_ARG;
+    }
+    if (width != 0) {
+        if (ctx->has_walls) {
+            set_last_error("stochastic_m_fluxdiv: filtering_width != 0 is built for periodic boxes only");
+            return FHD_ERR_UNSUPPORTED;
+        }
+        for (int d = 0; d < dim; d++)
+            if (ctx->g0.n[d] < width) {
+                set_last_error("stochastic_m_fluxdiv: the filter is wider than the domain");
+                return FHD_ERR_BAD_ARG;
+            }
     }
     StochArgs a;
     memset(&a, 0, sizeof(a));
@@ -168,6 +301,15 @@ int stoch_launch(fhd_ctx* ctx, const fhd_stoch_params* sp, double* const force[]
     const Grid g = ctx->g0;
     double* f2 = dim == 3 ? force[2] : nullptr;
     const bool mixed = ctx->prec == FHD_PREC_MIXED;
+    if (width != 0) {
+        int rc = 0;
+        with_dim(dim, [&](auto D) {
+            constexpr int DIM = decltype(D)::value;
+            rc = mixed ? stoch_filtered<float, DIM>(ctx, a, width, force, increment)
+                       : stoch_filtered<double, DIM>(ctx, a, width, force, increment);
+        });
+        return rc;
+    }
     if (ctx->has_walls) {
         EdgeExt X;
         for (int e = 0; e < 3; e++) {

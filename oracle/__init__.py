@@ -222,13 +222,17 @@ def gmres(pb: Problem, params, theta, b_u, b_p, x_u0=None, x_p0=None):
 
 
 def stochastic_m_fluxdiv(dim, n, dx, sp, eta, eta_ed, temp, temp_ed, dt, weights, W_cc, W_ed,
-                         force=None, increment=False):
+                         force=None, increment=False, status=False):
+    """the divergence on the faces; with status=True the pair (status,
+    force) instead of asserting status 0"""
     nc = int(np.prod(n[:dim]))
     force = [np.zeros(nc) for _ in range(dim)] if force is None else [f.copy() for f in force]
     w = np.ascontiguousarray(weights, np.float64)
     rc = lib().or_stochastic_m_fluxdiv(dim, _n3(n), C.c_double(dx), C.byref(sp), _pp(force),
                                        int(increment), _p(eta), _pp(eta_ed), _p(temp), _pp(temp_ed),
                                        C.c_double(dt), _p(w), len(weights), _pp(W_cc), _pp(W_ed))
+    if status:
+        return rc, force
     assert rc == 0, rc
     return force
 

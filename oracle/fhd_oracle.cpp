@@ -1319,15 +1319,45 @@ done:
     return status;
 }
 
-// stochastic_m_fluxdiv (stochastic_m_fluxdiv.f90:42-602), periodic,
-// filtering_width = 0
+// One pass of filter_stoch_m_flux (stochastic_m_fluxdiv.f90:604-778) along
+// direction d over a periodic array: the symmetric smoothing stencil of
+// width 1, 2 or 4 taps a side, the terms summed in the order written there.
+// The ghosts it reads are the periodic images of the previous pass
+// (multifab_fill_boundary between the passes); n[d] >= width.
+static void filter_pass(const Geo& g, Vec& a, int d, int width) {
+    Vec out(a.size());
+    const int e[3] = {d == 0, d == 1, d == 2};
+    forall(g, [&](int i, int j, int k) {
+        auto at = [&](int s) { return a[g.id(i + s * e[0], j + s * e[1], k + s * e[2])]; };
+        double v;
+        if (width == 1)
+            v = at(0) / 2 + at(-1) / 4 + at(1) / 4;
+        else if (width == 2)
+            v = 5 * at(0) / 8 - at(-2) / 16 + at(-1) / 4 - at(2) / 16 + at(1) / 4;
+        else
+            v = 93 * at(0) / 128 + 7 * at(-1) / 32 - 7 * at(-2) / 64 + at(-3) / 32 - at(-4) / 256 +
+                7 * at(1) / 32 - 7 * at(2) / 64 + at(3) / 32 - at(4) / 256;
+        out[g.id(i, j, k)] = v;
+    });
+    a.swap(out);
+}
+
+// stochastic_m_fluxdiv (stochastic_m_fluxdiv.f90:42-602); filtering_width
+// 1, 2 or 4 filters the scaled stresses (x, then y, then z) before the
+// divergence (:172-174, :226-230), periodic boxes only
 int stoch_m_impl(const Geo& g, const fhd_stoch_params* sp, double* const force[], int increment,
                  const double* eta, const double* const eta_ed[], const double* T, const double* const T_ed[],
                  double dt, const double* weights, int n_rngs, const double* const W_cc[],
                  const double* const W_ed[]) {
     const int dim = g.dim, nE = n_edge(dim);
     const long nc = g.nc;
-    if (sp->filtering_width != 0) return FHD_ERR_UNSUPPORTED;
+    const int width = sp->filtering_width;
+    if (width != 0) {
+        if (width != 1 && width != 2 && width != 4) return FHD_ERR_BAD_ARG;
+        if (g.any_wall()) return FHD_ERR_UNSUPPORTED;
+        for (int d = 0; d < dim; d++)
+            if (g.n[d] < width) return FHD_ERR_BAD_ARG;
+    }
     long ne[3] = {0, 0, 0};
     for (int e = 0; e < nE; e++) ne[e] = edge_count(g, e);
     std::vector<Vec> fcc(dim, Vec(nc, 0.0)), fed(2 * nE);
@@ -1369,6 +1399,12 @@ int stoch_m_impl(const Geo& g, const fhd_stoch_params* sp, double* const force[]
                 }
             }
         }
+    }
+    if (width != 0) {
+        for (auto& a : fed)
+            for (int d = 0; d < dim; d++) filter_pass(g, a, d, width);
+        for (auto& a : fcc)
+            for (int d = 0; d < dim; d++) filter_pass(g, a, d, width);
     }
     const double dxinv = 1.0 / g.dx;
     auto E = [&](int e, int comp, int i, int j, int k) { return fed[2 * e + comp][edge_id(g, e, i, j, k)]; };
