@@ -201,6 +201,23 @@ int fhd_ctx_set_coarse(fhd_ctx* ctx, int mode);
  * default: on where the level allows, 0: colour launches).  The colour
  * sweeps of stag_mg_solver.f90:360-396, evaluated in the same order. */
 int fhd_ctx_set_fused(fhd_ctx* ctx, int mode);
+/* Moving no-slip walls: the namelist arrays wallspeed_lo / wallspeed_hi of
+ * probin_common, in their Fortran layout (MAX_SPACEDIM-1, MAX_SPACEDIM):
+ * element [t + 2 d] is the speed of the t-th tangential velocity component
+ * (the components other than d, ascending) on the wall normal to direction d
+ * -- the constant values of inhomogeneous_bc_val_2d / _3d
+ * (src_lowMach/inhomogeneous_bc_val.f90:84-145, 274-372; not the prob_type
+ * 12 profiles).  The timesteps (fhd_dev_advance_overdamped, _inertial,
+ * _inertial_multispecies) then take each diffusive_m_fluxdiv of their
+ * velocity with the tangential ghost 2 v_bc - u behind those walls
+ * (physbc_macvel_*_inhomogeneous, multifab_physbc_stag.f90:1118-1160),
+ * which puts their solves in delta form with homogeneous walls
+ * (advance_timestep_inertial.f90:408-440).  The Stokes-solve entries stay
+ * homogeneous, as gmres and apply_matrix are in the reference.  A speed on
+ * a periodic side is ignored; a nonzero speed on a slip wall (where the
+ * reference reads a traction) returns FHD_ERR_UNSUPPORTED.  Zero speeds
+ * (the default) are the standing walls. */
+int fhd_ctx_set_wall_speed(fhd_ctx* ctx, const double wallspeed_lo[6], const double wallspeed_hi[6]);
 /* Smoother autotuner.  Each multigrid level that smooths through launches
  * (staggered and pressure multigrids, above the single-block coarse end) can
  * smooth as colour launches with one of four thread-block shapes, as the

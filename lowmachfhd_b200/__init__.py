@@ -130,6 +130,15 @@ class StokesSolver:
         launch each: 1 or -1 (default) on, 0 one launch per colour"""
         check(lib().fhd_ctx_set_fused(self._h, int(mode)), "fhd_ctx_set_fused")
 
+    def set_wall_speed(self, wallspeed_lo=None, wallspeed_hi=None):
+        """moving no-slip walls for the timesteps: wallspeed_lo / wallspeed_hi
+        of probin_common, six values each in the Fortran layout (speed of the
+        t-th tangential component on the wall normal to d at [t + 2 d]);
+        None is all zero (standing walls)"""
+        a = (C.c_double * 6)(*([0.0] * 6 if wallspeed_lo is None else [float(x) for x in wallspeed_lo]))
+        b = (C.c_double * 6)(*([0.0] * 6 if wallspeed_hi is None else [float(x) for x in wallspeed_hi]))
+        check(lib().fhd_ctx_set_wall_speed(self._h, C.cast(a, _DP), C.cast(b, _DP)), "fhd_ctx_set_wall_speed")
+
     def set_tune(self, mode: int):
         """smoother autotuner: 1 or -1 (default) time the candidate plans of
         each level shape once per process and keep the fastest, 0 the fixed

@@ -160,6 +160,7 @@ _PROTOS = {
     "fhd_ctx_set_coarse": (C.c_int, [_VP, C.c_int]),
     "fhd_ctx_set_fused": (C.c_int, [_VP, C.c_int]),
     "fhd_ctx_set_tune": (C.c_int, [_VP, C.c_int]),
+    "fhd_ctx_set_wall_speed": (C.c_int, [_VP, _DP, _DP]),
     "fhd_tune_export": (C.c_longlong, [C.c_char_p, C.c_longlong]),
     "fhd_tune_import": (C.c_int, [C.c_char_p]),
     "fhd_tune_key": (C.c_longlong, [C.c_int, C.c_int, C.POINTER(C.c_int), C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,

@@ -2410,6 +2410,32 @@ int fhd_ctx_set_fused(fhd_ctx* c, int mode) {
     return FHD_OK;
 }
 
+int fhd_ctx_set_wall_speed(fhd_ctx* c, const double wallspeed_lo[6], const double wallspeed_hi[6]) {
+    if (!c || !wallspeed_lo || !wallspeed_hi) return FHD_ERR_BAD_ARG;
+    double v[2][6];
+    bool any = false;
+    for (int side = 0; side < 2; side++)
+        for (int d = 0; d < 3; d++)
+            for (int t = 0; t < 2; t++) {
+                const int q = t + 2 * d;
+                const double s = side ? wallspeed_hi[q] : wallspeed_lo[q];
+                const int w = side ? c->walls.hi[d] : c->walls.lo[d];
+                // only the speeds of this context's walls count (a periodic
+                // side keeps its speed unused, as in the reference)
+                const bool used = d < c->dim && t < c->dim - 1 && w != 0;
+                if (used && s != 0.0 && w > 0) {
+                    set_last_error("fhd_ctx_set_wall_speed: a slip wall takes no speed (its value is a traction)");
+                    return FHD_ERR_UNSUPPORTED;
+                }
+                if (used && !std::isfinite(s)) return FHD_ERR_BAD_ARG;
+                v[side][q] = used ? s : 0.0;
+                any = any || v[side][q] != 0.0;
+            }
+    memcpy(c->wall_speed, v, sizeof(v));
+    c->moving_walls = any;
+    return FHD_OK;
+}
+
 int fhd_ctx_set_tune(fhd_ctx* c, int mode) {
     if (!c || mode < -1 || mode > 64) return FHD_ERR_BAD_ARG;
     if (cudaStreamSynchronize(c->stream) != cudaSuccess) return FHD_ERR_CUDA;

@@ -227,6 +227,10 @@ struct fhd_ctx {
     fhd::Walls walls = {{0, 0, 0}, {0, 0, 0}};
     bool has_walls = false;
     bool noslip = false;  // some wall is no-slip
+    // tangential speeds of moving no-slip walls (fhd_ctx_set_wall_speed):
+    // [side][t + 2 d], zero on periodic sides
+    double wall_speed[2][6] = {{0, 0, 0, 0, 0, 0}, {0, 0, 0, 0, 0, 0}};
+    bool moving_walls = false;
     int stag_nl_box = 0;      // levels of the box hierarchy (0: the domain's)
     bool stag_fancy = false;  // nested bottom solve from level stag_nl_box - 1
     double dx = 1.0;

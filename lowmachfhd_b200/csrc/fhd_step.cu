@@ -526,8 +526,51 @@ static SVec<double> one(double* a) {
     return v;
 }
 
+// Moving no-slip walls (fhd_ctx_set_wall_speed): behind such a wall the
+// tangential ghost is 2 v_bc - u (physbc_macvel_2d_inhomogeneous /
+// _3d_inhomogeneous, multifab_physbc_stag.f90:1118-1160) where the
+// homogeneous operator has -u, so +L u (visc_type 1, beta of the first
+// cell) gains 2 v_bc beta / dx^2 on the faces of the first row beside the
+// wall.  Walls in direction order, the low side first, one addition each.
+struct WallSpeed {
+    double v[2][6];  // [side][t + 2 d]
+};
+template <int DIM>
+__global__ void __launch_bounds__(256) k_wall_speed(Grid g, fhd::Walls W, WallSpeed S, const double* eta,
+                                                    double* o0, double* o1, double* o2, double q) {
+    Cell P;
+    if (!cell_of_thread(g, P)) return;
+    const i64 f = P.id(0, 0, 0);
+    const int at[3] = {P.i, P.j, P.k};
+    const double b = ld(eta, 0);
+    double* o[3] = {o0, o1, o2};
+#pragma unroll
+    for (int c = 0; c < DIM; c++) {
+        if (fhd::on_wall(W, c, P.i, P.j, P.k)) continue;
+        double v = 0.0;
+        bool any = false;
+#pragma unroll
+        for (int d = 0; d < DIM; d++) {
+            if (d == c) continue;
+            const int t = c - (c > d ? 1 : 0);
+            if (W.lo[d] < 0 && at[d] == 0 && S.v[0][t + 2 * d] != 0.0) {
+                if (!any) v = o[c][f];
+                v = v + ((2.0 * S.v[0][t + 2 * d]) * b) * q;
+                any = true;
+            }
+            if (W.hi[d] < 0 && at[d] == g.n[d] - 1 && S.v[1][t + 2 * d] != 0.0) {
+                if (!any) v = o[c][f];
+                v = v + ((2.0 * S.v[1][t + 2 * d]) * b) * q;
+                any = true;
+            }
+        }
+        if (any) o[c][f] = v;
+    }
+}
+
 // diffusive_m_fluxdiv (diffusive_m_fluxdiv.f90:25-...): -(stag_applyop with
-// alpha = 0) applied to u, written to out
+// alpha = 0) applied to u, written to out; with moving walls the velocity's
+// ghosts carry their speeds (every call here is on the step's velocity)
 static int diff_m(fhd_ctx* ctx, SVec<double> out, CSVec<double> u, const double* eta, const double* const eta_ed[],
                   const double* kappa) {
     StagOp<double> A;
@@ -566,6 +609,17 @@ static int diff_m(fhd_ctx* ctx, SVec<double> out, CSVec<double> u, const double*
     for (int c = 0; c < ctx->dim; c++) L.x[0][c] = out.c[c];
     k_lin<<<flat_blocks(g.nc), 256, 0, ctx->stream>>>(g.nc, ctx->dim, out, L, 0);
     ctx->launches++;
+    if (ctx->has_walls && ctx->moving_walls) {
+        // after the sign flip: the term belongs to +L u
+        WallSpeed S;
+        memcpy(S.v, ctx->wall_speed, sizeof(S.v));
+        with_dim(ctx->dim, [&](auto D) {
+            constexpr int DIM = decltype(D)::value;
+            k_wall_speed<DIM><<<cell_grid(g), cell_block(), 0, ctx->stream>>>(g, ctx->walls, S, eta, out.c[0],
+                                                                             out.c[1], out.c[2], A.q);
+        });
+        ctx->launches++;
+    }
     FHD_CUDA_TRY(cudaPeekAtLastError());
     return 0;
 }

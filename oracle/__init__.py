@@ -280,6 +280,15 @@ def set_walls(bc_lo=(PERIODIC,) * 3, bc_hi=(PERIODIC,) * 3):
     assert rc == 0, rc
 
 
+def set_wall_speed(lo=None, hi=None):
+    """wallspeed_lo / wallspeed_hi (probin_common) for the steps: six values
+    each, speed (t, d) of the t-th tangential component on the wall normal
+    to d at [t + 2 d]; None is all zero"""
+    a = (C.c_double * 6)(*([0.0] * 6 if lo is None else [float(x) for x in lo]))
+    b = (C.c_double * 6)(*([0.0] * 6 if hi is None else [float(x) for x in hi]))
+    lib().or_set_wall_speed(a, b)
+
+
 def compute_nlevs_mg(dim, n, minwidth=2):
     return lib().or_compute_nlevs_mg(dim, _n3(n), minwidth)
 

@@ -29,6 +29,13 @@ typedef std::vector<double> Vec;
 // and side 0 = periodic, -1 = no-slip wall, +1 = slip wall (the sign the
 // transverse velocity takes in the ghost cell behind the wall).
 static int g_wl[3] = {0, 0, 0}, g_wh[3] = {0, 0, 0};
+// Tangential speeds of moving no-slip walls (or_set_wall_speed), the
+// namelist arrays wallspeed_lo / wallspeed_hi of probin_common in their
+// Fortran layout: speed (t, d) of the t-th tangential component (the
+// components other than d, ascending) on the wall normal to d at [t + 2 d];
+// the constant values of inhomogeneous_bc_val_2d / _3d
+// (src_lowMach/inhomogeneous_bc_val.f90:84-145, 274-372).
+static double g_ws[2][6] = {{0, 0, 0, 0, 0, 0}, {0, 0, 0, 0, 0, 0}};
 
 struct Geo {
     int dim = 2;
@@ -324,6 +331,51 @@ void s_applyop(SLevel& L, int visc, int color) {
                                      : lface(g, visc, L.alpha, L.beta, L.gamma, L.bed, ph, c, i, j, k, nullptr);
         });
     }
+}
+
+// A wall speed is taken on no-slip walls only: on a slip wall the reference
+// reads the value as a traction (DIR_TRACT, multifab_physbc_stag.f90:
+// 1151-1160), which is not built.  A speed on a periodic side is ignored, as
+// there.
+int wall_speed_check(const Geo& g) {
+    for (int d = 0; d < g.dim; d++)
+        for (int side = 0; side < 2; side++)
+            for (int t = 0; t < g.dim - 1; t++)
+                if (g_ws[side][t + 2 * d] != 0.0 && (side ? g.wh[d] : g.wl[d]) > 0) return FHD_ERR_UNSUPPORTED;
+    return 0;
+}
+
+// The part of diffusive_m_fluxdiv that moving no-slip walls add.  Behind
+// such a wall the tangential ghost is 2 v_bc - u
+// (physbc_macvel_2d_inhomogeneous / _3d_inhomogeneous,
+// multifab_physbc_stag.f90:1118-1160) where the homogeneous rule has -u, so
+// +L u (visc_type 1, beta of the first cell) gains 2 v_bc beta / dx^2 on the
+// faces of the first row beside the wall.  The steps take every
+// diffusive_m_fluxdiv of the velocity with those ghosts: that is how they put
+// the solve in delta form with homogeneous walls
+// (advance_timestep_overdamped.f90:310-333, advance_timestep_inertial.f90:
+// 408-440).  Walls in direction order, the low side first, one addition each.
+void wall_speed_term(const Geo& g, double beta0, double* const out[]) {
+    const int dim = g.dim;
+    const double q = 1.0 / (g.dx * g.dx);
+    for (int d = 0; d < dim; d++)
+        for (int side = 0; side < 2; side++) {
+            if ((side ? g.wh[d] : g.wl[d]) >= 0) continue;
+            const int row = side ? g.n[d] - 1 : 0;
+            int t = 0;
+            for (int c = 0; c < dim; c++) {
+                if (c == d) continue;
+                const double v = g_ws[side][t + 2 * d];
+                t++;
+                if (v == 0.0) continue;
+                forall(g, [&](int i, int j, int k) {
+                    const int at[3] = {i, j, k};
+                    if (at[d] != row || wall_face(g, c, i, j, k)) return;
+                    const long f = g.id(i, j, k);
+                    out[c][f] = out[c][f] + ((2.0 * v) * beta0) * q;
+                });
+            }
+        }
 }
 
 // one colour of the smoother: applyop(colour) then stag_mg_update(colour)
@@ -1982,6 +2034,13 @@ int or_set_walls(const int bc_lo[3], const int bc_hi[3]) {
     return 0;
 }
 
+void or_set_wall_speed(const double lo[6], const double hi[6]) {
+    for (int q = 0; q < 6; q++) {
+        g_ws[0][q] = lo ? lo[q] : 0.0;
+        g_ws[1][q] = hi ? hi[q] : 0.0;
+    }
+}
+
 int or_compute_nlevs_mg(int dim, const int n[3], int minwidth) {
     Geo g(dim, n, 1.0);
     return nlevs_mg(g, minwidth);
@@ -2104,6 +2163,7 @@ int step_impl(const Geo& g, int visc_type, const fhd_gmres_params* p_in, const f
     const long nc = g.nc;
     const int nE = n_edge(dim);
     const int ns = mix ? mix->ns : 1;
+    if (int rc = wall_speed_check(g)) return rc;
     fhd_gmres_params p = *p_in;
     const double theta = 1.0 / dt;
     auto fvec = [&](std::vector<Vec>& v) { v.assign(dim, Vec(nc, 0.0)); };
@@ -2135,6 +2195,7 @@ int step_impl(const Geo& g, int visc_type, const fhd_gmres_params* p_in, const f
         s_applyop(L, visc_type, 0);
         for (int c = 0; c < dim; c++)
             for (long f = 0; f < nc; f++) out[c][f] = L.Lphi[c][f] * -1.0;
+        wall_speed_term(g, eta[0], out);
     };
     auto sum_species = [&](double* const* r, double* out) {
         for (long f = 0; f < nc; f++) {
@@ -2306,6 +2367,7 @@ int overdamped_impl(const Geo& g, int visc_type, const fhd_gmres_params* p_in, c
     const long nc = g.nc;
     const int nE = n_edge(dim);
     const int ns = mix ? mix->ns : 1;
+    if (int rc = wall_speed_check(g)) return rc;
     fhd_gmres_params p = *p_in;
     auto fvec = [&](std::vector<Vec>& v) { v.assign(dim, Vec(nc, 0.0)); };
     auto ptrs = [&](std::vector<Vec>& v, double** out) { for (int c = 0; c < dim; c++) out[c] = v[c].data(); };
@@ -2329,6 +2391,7 @@ int overdamped_impl(const Geo& g, int visc_type, const fhd_gmres_params* p_in, c
         s_applyop(L, visc_type, 0);
         for (int c = 0; c < dim; c++)
             for (long f = 0; f < nc; f++) out[c][f] = L.Lphi[c][f] * -1.0;
+        wall_speed_term(g, eta[0], out);
     };
     auto sum_species = [&](double* const* r, double* out) {
         for (long f = 0; f < nc; f++) {

@@ -202,6 +202,7 @@ int or_accuracy_test_order(int dim, int n, int prob_coeff, int prob_sol,
  * a direction is periodic on both sides or on neither.  Walls are
  * homogeneous (zero wall velocity) and need visc_type 1. */
 int or_set_walls(const int bc_lo[3], const int bc_hi[3]);
+void or_set_wall_speed(const double wallspeed_lo[6], const double wallspeed_hi[6]);
 
 /* number of OpenMP threads the oracle uses */
 int or_num_threads(void);
