@@ -169,6 +169,12 @@ int  fhd_ctx_create(int dim, const int n_cells[3], const double dx[3],
 #define FHD_BC_PERIODIC (-1)
 #define FHD_BC_NO_SLIP_WALL 100
 #define FHD_BC_SLIP_WALL 200
+/* Reservoirs (bc.f90): walls for the velocity, the pressure and the
+ * stochastic momentum flux, as the reference's bc tower and mflux_bc treat
+ * them; their mass exchange is not built, so the mass-flux entries and the
+ * multispecies steps return FHD_ERR_UNSUPPORTED on such a context. */
+#define FHD_BC_NO_SLIP_RESERVOIR 101
+#define FHD_BC_SLIP_RESERVOIR 201
 int  fhd_ctx_create_bc(int dim, const int n_cells[3], const int max_grid_size[3],
                        const int bc_lo[3], const int bc_hi[3], const double dx[3],
                        int visc_type, const fhd_gmres_params* params,

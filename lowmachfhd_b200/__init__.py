@@ -18,7 +18,7 @@ from typing import Sequence
 import numpy as np
 
 from . import _capi
-from ._capi import (FHD_BC_NO_SLIP_WALL, FHD_BC_PERIODIC, FHD_BC_SLIP_WALL, FHD_PREC_FP64, FHD_PREC_MIXED, FHD_REQ_INERTIAL, FHD_REQ_OVERDAMPED, Fab, FhdError,
+from ._capi import (FHD_BC_NO_SLIP_RESERVOIR, FHD_BC_NO_SLIP_WALL, FHD_BC_PERIODIC, FHD_BC_SLIP_RESERVOIR, FHD_BC_SLIP_WALL, FHD_PREC_FP64, FHD_PREC_MIXED, FHD_REQ_INERTIAL, FHD_REQ_OVERDAMPED, Fab, FhdError,
                     GmresParams, MixtureParams, Multifab, Request, RequestResult, SolveStats, StochParams, check, lib,
                     mixture_params)
 
@@ -26,7 +26,7 @@ __all__ = ["StokesSolver", "GmresParams", "StochParams", "SolveStats", "MixtureP
            "Server", "Batch", "StructureFactor", "tune_candidates", "tune_export", "tune_import", "tune_key", "Request", "RequestResult", "make_request", "fill_normal", "StepNoise", "philox4x32_10", "sched_simulate",
            "FHD_REQ_OVERDAMPED", "FHD_REQ_INERTIAL",
            "default_params", "FhdError",
-           "FHD_PREC_FP64", "FHD_PREC_MIXED", "FHD_BC_PERIODIC", "FHD_BC_NO_SLIP_WALL", "FHD_BC_SLIP_WALL", "lib", "fab_from_canonical", "fab_from_components", "canonical_from_fab", "FabArray"]
+           "FHD_PREC_FP64", "FHD_PREC_MIXED", "FHD_BC_PERIODIC", "FHD_BC_NO_SLIP_WALL", "FHD_BC_SLIP_WALL", "FHD_BC_NO_SLIP_RESERVOIR", "FHD_BC_SLIP_RESERVOIR", "lib", "fab_from_canonical", "fab_from_components", "canonical_from_fab", "FabArray"]
 
 
 def default_params(**overrides) -> GmresParams:

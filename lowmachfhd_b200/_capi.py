@@ -34,6 +34,8 @@ FHD_PREC_MIXED = 1
 FHD_BC_PERIODIC = -1
 FHD_BC_NO_SLIP_WALL = 100
 FHD_BC_SLIP_WALL = 200
+FHD_BC_NO_SLIP_RESERVOIR = 101
+FHD_BC_SLIP_RESERVOIR = 201
 
 
 class GmresParams(C.Structure):

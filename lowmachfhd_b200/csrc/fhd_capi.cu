@@ -603,6 +603,7 @@ int fhd_compute_sqrtLonsager_fc(fhd_ctx* ctx, const fhd_mixture_params* mp, cons
                                 const fhd_multifab* rho, const fhd_multifab* rhotot,
                                 const fhd_multifab* sqrtLonsager_fc) {
     if (!ctx || !mp || !sp || !rho || !sqrtLonsager_fc) return FHD_ERR_BAD_ARG;
+    if (int r0 = fhd::refuse_reservoirs(ctx, "fhd_compute_sqrtLonsager_fc")) return r0;
     if (mp->nspecies < 2 || mp->nspecies > 5) return FHD_ERR_UNSUPPORTED;
     const int dim = ctx->dim, ns = mp->nspecies;
     int rc;
@@ -635,6 +636,7 @@ int fhd_stochastic_mass_fluxdiv(fhd_ctx* ctx, const fhd_mixture_params* mp, cons
                                 const fhd_multifab* W_fc, int increment) {
     if (!ctx || !mp || !sp || !sqrtLonsager_fc || !stoch_mass_fluxdiv || !weights || !W_fc || !(dt > 0.0))
         return FHD_ERR_BAD_ARG;
+    if (int r0 = fhd::refuse_reservoirs(ctx, "fhd_stochastic_mass_fluxdiv")) return r0;
     if (mp->nspecies < 2 || mp->nspecies > 5 || n_rngs < 1 || n_rngs > 4) return FHD_ERR_UNSUPPORTED;
     const int dim = ctx->dim, ns = mp->nspecies;
     int rc;

@@ -1352,6 +1352,7 @@ extern "C" int fhd_dev_compute_sqrtLonsager_fc(fhd_ctx* ctx, const fhd_mixture_p
                                                const fhd_stoch_params* sp, const double* const rho[],
                                                double* const sqrtLonsager_fc[]) {
     if (!ctx || !mp || !sp || !rho || !sqrtLonsager_fc) return FHD_ERR_BAD_ARG;
+    if (int rc = fhd::refuse_reservoirs(ctx, "compute_sqrtLonsager_fc")) return rc;
     if (int rc = check_mix(mp)) return rc;
     const MixDev m = make_mixdev(mp, sp);
     int rc;
@@ -1374,6 +1375,7 @@ extern "C" int fhd_dev_stochastic_mass_fluxdiv(fhd_ctx* ctx, const fhd_mixture_p
                                                double* const stoch_mass_flux[]) {
     if (!ctx || !mp || !sp || !sqrtLonsager_fc || !weights || !W_fc || !stoch_mass_fluxdiv || !(dt > 0.0))
         return FHD_ERR_BAD_ARG;
+    if (int rc = fhd::refuse_reservoirs(ctx, "stochastic_mass_fluxdiv")) return rc;
     if (n_rngs < 1 || n_rngs > 4) {
         set_last_error("stochastic_mass_fluxdiv: n_rngs must be 1..4");
         return FHD_ERR_UNSUPPORTED;
@@ -1407,6 +1409,7 @@ extern "C" int fhd_dev_compute_mass_fluxdiv(fhd_ctx* ctx, const fhd_mixture_para
                                             const double* const rho[], double dt, const double* weights, int n_rngs,
                                             const double* const W_fc[], double* const out[]) {
     if (!ctx || !mp || !sp || !rho || !weights || !W_fc || !out) return FHD_ERR_BAD_ARG;
+    if (int r0 = fhd::refuse_reservoirs(ctx, "compute_mass_fluxdiv")) return r0;
     const int rc = fhd::mass_fluxdiv(ctx, mp, sp, rho, dt, weights, n_rngs, W_fc, out);
     if (rc < 0) return rc;
     // like every device entry point, the call returns with its work done

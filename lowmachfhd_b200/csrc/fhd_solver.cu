@@ -2206,18 +2206,21 @@ int fhd_ctx_create_bc(int dim, const int n_cells[3], const int max_grid_size[3],
     if (!out || !n_cells || !max_grid_size || !bc_lo || !bc_hi || (dim != 2 && dim != 3)) return FHD_ERR_BAD_ARG;
     *out = nullptr;
     Walls W = {{0, 0, 0}, {0, 0, 0}};
-    bool any = false, noslip = false;
-    auto sign = [](int code, int& w) {
+    bool any = false, noslip = false, res = false;
+    // reservoirs are walls for everything the context's solves see
+    // (refuse_reservoirs)
+    auto sign = [&res](int code, int& w) {
         if (code == FHD_BC_PERIODIC) w = 0;
-        else if (code == FHD_BC_NO_SLIP_WALL) w = -1;
-        else if (code == FHD_BC_SLIP_WALL) w = 1;
+        else if (code == FHD_BC_NO_SLIP_WALL || code == FHD_BC_NO_SLIP_RESERVOIR) w = -1;
+        else if (code == FHD_BC_SLIP_WALL || code == FHD_BC_SLIP_RESERVOIR) w = 1;
         else return false;
+        res = res || code == FHD_BC_NO_SLIP_RESERVOIR || code == FHD_BC_SLIP_RESERVOIR;
         return true;
     };
     for (int d = 0; d < dim; d++) {
         if (!sign(bc_lo[d], W.lo[d]) || !sign(bc_hi[d], W.hi[d])) {
-            set_last_error("fhd_ctx_create_bc: bc codes -1 (periodic), 100 (no-slip wall) and 200 (slip wall) "
-                           "are built; reservoirs and other codes are not");
+            set_last_error("fhd_ctx_create_bc: bc codes -1 (periodic), 100 (no-slip wall), 200 (slip wall), 101 "
+                           "and 201 (reservoirs) are built; other codes are not");
             return FHD_ERR_UNSUPPORTED;
         }
         if ((W.lo[d] == 0) != (W.hi[d] == 0)) {
@@ -2251,6 +2254,7 @@ int fhd_ctx_create_bc(int dim, const int n_cells[3], const int max_grid_size[3],
         c->walls = W;
         c->has_walls = true;
         c->noslip = noslip;
+        c->reservoirs = res;
         const int r2 = c->prec == FHD_PREC_MIXED ? wall_diag<float>(c) : wall_diag<double>(c);
         if (r2 != FHD_OK) {
             fhd_ctx_destroy(c);

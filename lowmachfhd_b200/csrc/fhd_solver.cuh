@@ -227,6 +227,7 @@ struct fhd_ctx {
     fhd::Walls walls = {{0, 0, 0}, {0, 0, 0}};
     bool has_walls = false;
     bool noslip = false;  // some wall is no-slip
+    bool reservoirs = false;  // some wall is a reservoir (bc codes 101, 201)
     // tangential speeds of moving no-slip walls (fhd_ctx_set_wall_speed):
     // [side][t + 2 d], zero on periodic sides
     double wall_speed[2][6] = {{0, 0, 0, 0, 0, 0}, {0, 0, 0, 0, 0, 0}};
@@ -309,6 +310,22 @@ struct fhd_ctx {
 };
 
 namespace fhd {
+// Reservoirs (bc codes 101 NO_SLIP_RESERVOIR, 201 SLIP_RESERVOIR) are no-slip
+// and slip walls for the velocity and the pressure (the NO_SLIP / SLIP
+// ranges of adv_bc_level_build and ell_bc_level_build, src_lowMach/
+// define_bc_tower.f90:225-250, 301-355) and for the stochastic momentum flux
+// (mflux_bc_2d / _3d,
+// stochastic_m_fluxdiv.f90:363-451).  Their mass exchange -- Dirichlet
+// concentrations on the boundary face (scalar_bc, inhomogeneous_bc_val.f90:
+// 39-41) and the sqrt(2) random flux through it (stoch_mass_bc,
+// stochastic_mass_fluxdiv.f90:216-368) -- is not built: the mass-flux entries
+// and the multispecies steps refuse a context with reservoirs.
+inline int refuse_reservoirs(const fhd_ctx* c, const char* where) {
+    if (!c->reservoirs) return 0;
+    set_last_error(std::string(where) + ": the mass exchange of reservoirs (bc codes 101, 201) is not built");
+    return FHD_ERR_UNSUPPORTED;
+}
+
 constexpr int NSCAL = 256;
 // scalar slots
 constexpr int S_H = 0;        // H column, 1..m+1

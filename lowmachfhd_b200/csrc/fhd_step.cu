@@ -1078,6 +1078,8 @@ int fhd_dev_advance_overdamped(fhd_ctx* ctx, const fhd_stoch_params* sp, const f
     if (!ctx || !sp || !umac || !rho || !pi || !eta || !eta_ed || !kappa || !temperature || !temperature_ed ||
         !W_cc || !W_ed || (mp && !W_mass) || !(dt > 0.0))
         return FHD_ERR_BAD_ARG;
+    if (mp)
+        if (int r0 = fhd::refuse_reservoirs(ctx, "advance_timestep_overdamped (multispecies)")) return r0;
     int rc = advance_overdamped(ctx, sp, mp, dt, umac, rho, pi, eta, eta_ed, kappa, temperature, temperature_ed, W_cc,
                                 W_ed, W_mass, stats2);
     if (rc < 0) return rc;
@@ -1123,6 +1125,7 @@ int fhd_dev_advance_inertial_multispecies(fhd_ctx* ctx, const fhd_stoch_params* 
     if (!ctx || !sp || !mp || !umac || !rho || !pi || !mass_fluxdiv || !eta || !eta_ed || !kappa || !temperature ||
         !temperature_ed || !W_cc || !W_ed || !W_mass || !(dt > 0.0))
         return FHD_ERR_BAD_ARG;
+    if (int r0 = fhd::refuse_reservoirs(ctx, "advance_timestep_inertial_multispecies")) return r0;
     int rc = advance_inertial_ms(ctx, sp, mp, dt, umac, rho, pi, mass_fluxdiv, eta, eta_ed, kappa, temperature,
                                  temperature_ed, W_cc, W_ed, W_mass, stats2);
     if (rc < 0) return rc;

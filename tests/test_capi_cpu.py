@@ -72,7 +72,8 @@ def test_layout_context_rejects_walls_and_uneven_boxes_before_device():
     """fhd_ctx_create_bc takes the driver's max_grid_size, bc_lo and bc_hi:
     periodic, no-slip (100) and slip (200) codes, a direction periodic on
     both sides or on neither, walls with one box only, boxes that divide the
-    domain; reservoirs are not built"""
+    domain; reservoirs (101, 201) are accepted as walls, the closed and
+    impermeable codes are not built"""
     lib = _capi.lib()
     h = C.c_void_p()
     p = L.default_params()
@@ -80,13 +81,13 @@ def test_layout_context_rejects_walls_and_uneven_boxes_before_device():
     dx = (C.c_double * 3)(1.0, 1.0, 1.0)
     per = (C.c_int * 3)(-1, -1, -1)
     wall = (C.c_int * 3)(-1, 100, -1)
-    reservoir = (C.c_int * 3)(-1, 101, -1)
+    closed = (C.c_int * 3)(-1, 102, -1)
     mgs = (C.c_int * 3)(16, 16, 16)
     one = (C.c_int * 3)(32, 32, 32)
     assert lib.fhd_ctx_create_bc(3, n, one, wall, per, dx, 1, C.byref(p), 0, C.byref(h)) == _capi.FHD_ERR_BAD_ARG
-    assert lib.fhd_ctx_create_bc(3, n, one, reservoir, reservoir, dx, 1, C.byref(p), 0,
+    assert lib.fhd_ctx_create_bc(3, n, one, closed, closed, dx, 1, C.byref(p), 0,
                                  C.byref(h)) == _capi.FHD_ERR_UNSUPPORTED
-    assert b"reservoirs" in lib.fhd_last_error()
+    assert b"other codes are not" in lib.fhd_last_error()
     assert lib.fhd_ctx_create_bc(3, n, mgs, wall, wall, dx, 1, C.byref(p), 0, C.byref(h)) == _capi.FHD_ERR_UNSUPPORTED
     assert b"one box" in lib.fhd_last_error()
     assert lib.fhd_ctx_create_bc(3, n, one, wall, wall, dx, -1, C.byref(p), 0, C.byref(h)) == _capi.FHD_ERR_UNSUPPORTED

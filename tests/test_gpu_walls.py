@@ -137,7 +137,7 @@ def test_mixed_precision_walls(cuda):
 
 
 @pytest.mark.parametrize("kw", [dict(visc=-1), dict(visc=2), dict(precon_type=2), dict(stag_mg_smoother=0),
-                                dict(gmres_spatial_order=4), dict(code=101), dict(code=201)])
+                                dict(gmres_spatial_order=4), dict(code=102), dict(code=203)])
 def test_unsupported_wall_options(cuda, kw):
     visc = kw.pop("visc", 1)
     code = kw.pop("code", NS)
