@@ -661,9 +661,9 @@ static int stag_smooths(fhd_ctx* ctx, StagLevel<T>& L, int count) {
         int rc = 0;
         for (int m = 0; m < count && !rc; m++)
             for (int color = 1; color <= 2 * dim && !rc; color++)
-                with_dim(dim, [&](auto D) {
-                    constexpr int DIM = decltype(D)::value;
-                    k_stag_color_apply_w<T, DIM><<<cell_grid(L.g), cell_block(), 0, ctx->stream>>>(
+                with_dim_wall_visc(dim, ctx->visc, [&](auto D, auto V) {
+                    constexpr int DIM = decltype(D)::value, VISC = decltype(V)::value;
+                    k_stag_color_apply_w<T, DIM, VISC><<<cell_grid(L.g), cell_block(), 0, ctx->stream>>>(
                         L.g, ctx->walls, A, L.phi[0], L.phi[1], L.phi[2], L.rhs[0], L.rhs[1], L.rhs[2], L.tmp[0],
                         L.tmp[1], L.tmp[2], L.diag[0], L.diag[1], L.diag[2], color);
                     rc |= post(ctx);
@@ -724,9 +724,9 @@ static int stag_residual(fhd_ctx* ctx, StagLevel<T>& L) {
     int rc = 0;
     const StagOp<T> A = L.op();
     if (ctx->has_walls) {
-        with_dim(ctx->dim, [&](auto D) {
-            constexpr int DIM = decltype(D)::value;
-            k_stag_apply_w<T, DIM><<<cell_grid(L.g), cell_block(), 0, ctx->stream>>>(
+        with_dim_wall_visc(ctx->dim, ctx->visc, [&](auto D, auto V) {
+            constexpr int DIM = decltype(D)::value, VISC = decltype(V)::value;
+            k_stag_apply_w<T, DIM, VISC><<<cell_grid(L.g), cell_block(), 0, ctx->stream>>>(
                 L.g, ctx->walls, A, L.phi[0], L.phi[1], L.phi[2], L.tmp[0], L.tmp[1], L.tmp[2], L.rhs[0], L.rhs[1],
                 L.rhs[2], 1);
             rc |= post(ctx);
@@ -1720,9 +1720,9 @@ int stokes_apply(fhd_ctx* ctx, CSVec<double> x, CSVec<double> rhs, SVec<double> 
     A.q = 1.0 / (ctx->dx * ctx->dx);
     int rc = 0;
     if (ctx->has_walls) {
-        with_dim(ctx->dim, [&](auto D) {
-            constexpr int DIM = decltype(D)::value;
-            k_stokes_apply_w<DIM><<<cell_grid(ctx->g0), cell_block(), 0, ctx->stream>>>(
+        with_dim_wall_visc(ctx->dim, ctx->visc, [&](auto D, auto V) {
+            constexpr int DIM = decltype(D)::value, VISC = decltype(V)::value;
+            k_stokes_apply_w<DIM, VISC><<<cell_grid(ctx->g0), cell_block(), 0, ctx->stream>>>(
                 ctx->g0, ctx->walls, A, x, rhs, out, mode, 1.0 / ctx->dx);
             rc |= post(ctx);
         });
@@ -2241,9 +2241,9 @@ int fhd_ctx_create_bc(int dim, const int n_cells[3], const int max_grid_size[3],
         else fhd_gmres_params_default(&p);
         bool boxes = false;
         for (int d = 0; d < dim; d++) boxes = boxes || max_grid_size[d] < n_cells[d];
-        if (visc_type != 1 || p.precon_type != 1 || p.visc_schur_approx != 0 || p.stag_mg_smoother == 0 ||
+        if ((visc_type != 1 && visc_type != 2) || p.precon_type != 1 || p.visc_schur_approx != 0 || p.stag_mg_smoother == 0 ||
             p.gmres_spatial_order != 2 || boxes) {
-            set_last_error("fhd_ctx_create_bc: walls are built for visc_type 1, precon_type 1 without the BFBt "
+            set_last_error("fhd_ctx_create_bc: walls are built for visc_type 1 or 2, precon_type 1 without the BFBt "
                            "Schur complement, the colour smoother, second order and one box");
             return FHD_ERR_UNSUPPORTED;
         }

@@ -587,9 +587,9 @@ static int diff_m(fhd_ctx* ctx, SVec<double> out, CSVec<double> u, const double*
     if (ctx->has_walls) {
         // visc_type 1 with the wall ghost rules; zero on the wall faces
         // (stag_applyop.f90:201-205)
-        with_dim(ctx->dim, [&](auto D) {
-            constexpr int DIM = decltype(D)::value;
-            k_stag_apply_w<double, DIM><<<cell_grid(g), cell_block(), 0, ctx->stream>>>(
+        with_dim_wall_visc(ctx->dim, ctx->visc, [&](auto D, auto V) {
+            constexpr int DIM = decltype(D)::value, VISC = decltype(V)::value;
+            k_stag_apply_w<double, DIM, VISC><<<cell_grid(g), cell_block(), 0, ctx->stream>>>(
                 g, ctx->walls, A, u.c[0], u.c[1], u.c[2], out.c[0], out.c[1], out.c[2], nullptr, nullptr, nullptr,
                 0);
         });

@@ -1,6 +1,6 @@
 // fhd_walls.cuh -- homogeneous domain walls (zero wall velocity) for the
-// staggered Stokes solve with visc_type 1: no-slip and slip walls in any
-// direction, the other directions periodic.
+// staggered Stokes solve with visc_type 1 or 2 (constant coefficients): no-slip
+// and slip walls in any direction, the other directions periodic.
 //
 // The reference imposes walls through ghost cells, refilled after every
 // operation of the solve (multifab_physbc_domainvel / multifab_physbc_macvel,
@@ -56,34 +56,40 @@ __device__ __forceinline__ T wall_vel(const Grid& g, const Walls& W, const T* u,
     return sg * ld(u, (i64)q[0] + (i64)g.n[0] * ((i64)q[1] + (i64)g.n[1] * (DIM == 3 ? q[2] : 0)));
 }
 
-// (theta alpha - L) phi of component C at face (i, j, k), visc_type 1: the
-// expression of stag_lface_acc with the neighbours under the wall rules
-template <typename T, int DIM, int C>
+// (theta alpha - L) phi of component C at face (i, j, k), constant
+// coefficients, visc_type 1 or 2: the expression of stag_lface_acc with every
+// neighbour under the wall rules (visc_type 2 also reads the other
+// components around the face: their values on and behind a wall come from
+// wall_vel as well, as the reference's ghost cells give them to the uniform
+// stencil of stag_applyop_level)
+template <typename T, int DIM, int VISC, int C>
 __device__ __forceinline__ T stag_lface_w(const Grid& g, const Walls& W, const StagOp<T>& A, const T* const* phi,
                                           int i, int j, int k, T& dg) {
+    static_assert(VISC == 1 || VISC == 2, "walls: visc_type 1 or 2");
     CellF P;
     P.set(g, i, j, k);
     const T* pc = phi[C];
-    return stag_lface_acc<T, DIM, 1, C>(
+    return stag_lface_acc<T, DIM, VISC, C>(
         A, P,
         [&](int a, int b, int c) {
             return (a == 0 && b == 0 && c == 0) ? ld(pc, P.base) : wall_vel<T, DIM>(g, W, pc, C, i + a, j + b, k + c);
         },
-        [&](int, int, int, int) { return T(0); }, [&]() { return ld(A.alpha[C], P.base); }, dg);
+        [&](int d, int a, int b, int c) { return wall_vel<T, DIM>(g, W, phi[d], d, i + a, j + b, k + c); },
+        [&]() { return ld(A.alpha[C], P.base); }, dg);
 }
 
-template <typename T, int DIM>
+template <typename T, int DIM, int VISC>
 __device__ __forceinline__ T stag_lface_w_c(int c, const Grid& g, const Walls& W, const StagOp<T>& A,
                                             const T* const* phi, int i, int j, int k, T& dg) {
-    if (c == 0) return stag_lface_w<T, DIM, 0>(g, W, A, phi, i, j, k, dg);
-    if (DIM == 3 && c == 2) return stag_lface_w<T, DIM, (DIM == 3 ? 2 : 1)>(g, W, A, phi, i, j, k, dg);
-    return stag_lface_w<T, DIM, 1>(g, W, A, phi, i, j, k, dg);
+    if (c == 0) return stag_lface_w<T, DIM, VISC, 0>(g, W, A, phi, i, j, k, dg);
+    if (DIM == 3 && c == 2) return stag_lface_w<T, DIM, VISC, (DIM == 3 ? 2 : 1)>(g, W, A, phi, i, j, k, dg);
+    return stag_lface_w<T, DIM, VISC, 1>(g, W, A, phi, i, j, k, dg);
 }
 
 // first pass of a colour (stag_applyop_level(colour) of stag_mg_solver.f90:
 // 360-396): Lphi and the diagonal of the colour's faces into Lo, Do.  A wall
 // face gets Lo = rhs, Do = 1, so that k_stag_color_update leaves it at zero.
-template <typename T, int DIM>
+template <typename T, int DIM, int VISC>
 __global__ void __launch_bounds__(256) k_stag_color_apply_w(Grid g, Walls W, StagOp<T> A, const T* p0, const T* p1,
                                                             const T* p2, const T* r0, const T* r1, const T* r2,
                                                             T* L0, T* L1, T* L2, T* D0, T* D1, T* D2, int color) {
@@ -104,14 +110,14 @@ __global__ void __launch_bounds__(256) k_stag_color_apply_w(Grid g, Walls W, Sta
             continue;
         }
         T dg;
-        Lo[c][f] = stag_lface_w_c<T, DIM>(c, g, W, A, ph, P.i, P.j, P.k, dg);
+        Lo[c][f] = stag_lface_w_c<T, DIM, VISC>(c, g, W, A, ph, P.i, P.j, P.k, dg);
         Do[c][f] = dg;
     }
 }
 
 // residual rhs - (theta alpha - L) phi (mode 1) or Lphi (mode 0), zero on
 // the wall faces
-template <typename T, int DIM>
+template <typename T, int DIM, int VISC>
 __global__ void __launch_bounds__(256) k_stag_apply_w(Grid g, Walls W, StagOp<T> A, const T* p0, const T* p1,
                                                       const T* p2, T* o0, T* o1, T* o2, const T* r0, const T* r1,
                                                       const T* r2, int mode) {
@@ -128,7 +134,7 @@ __global__ void __launch_bounds__(256) k_stag_apply_w(Grid g, Walls W, StagOp<T>
             continue;
         }
         T dg;
-        const T L = stag_lface_w_c<T, DIM>(c, g, W, A, phi, P.i, P.j, P.k, dg);
+        const T L = stag_lface_w_c<T, DIM, VISC>(c, g, W, A, phi, P.i, P.j, P.k, dg);
         out[c][f] = mode ? ld(rhs[c], f) - L : L;
     }
 }
@@ -181,7 +187,7 @@ __global__ void __launch_bounds__(256) k_zero_walls(Grid g, Walls W, T* u0, T* u
 
 // apply_matrix (apply_matrix.f90:117-147) with walls: zero Lphi and pressure
 // gradient on the wall faces; mode 1 returns rhs - A x
-template <int DIM>
+template <int DIM, int VISC>
 static __global__ void __launch_bounds__(256) k_stokes_apply_w(Grid g, Walls W, StagOp<double> A, CSVec<double> x,
                                                                CSVec<double> rhs, SVec<double> out, int mode,
                                                                double dxinv) {
@@ -198,7 +204,7 @@ static __global__ void __launch_bounds__(256) k_stokes_apply_w(Grid g, Walls W, 
         double L = 0.0;
         if (!on_wall(W, c, P.i, P.j, P.k)) {
             double dg;
-            L = stag_lface_w_c<double, DIM>(c, g, W, A, phi, P.i, P.j, P.k, dg);
+            L = stag_lface_w_c<double, DIM, VISC>(c, g, W, A, phi, P.i, P.j, P.k, dg);
             const double gp = (pc - ld(p, P.id(-dx_, -dy_, -dz_))) * dxinv;
             L = L + gp;
         }
@@ -207,6 +213,13 @@ static __global__ void __launch_bounds__(256) k_stokes_apply_w(Grid g, Walls W, 
     }
     const double bp = div * -1.0;
     out.c[DIM][f] = mode ? ld(rhs.c[DIM], f) - bp : bp;
+}
+
+// host dispatch of the wall kernels on the context's visc_type (1 or 2)
+template <class F>
+inline void with_wall_visc(int visc, F&& f) {
+    if (visc == 2) f(std::integral_constant<int, 2>());
+    else f(std::integral_constant<int, 1>());
 }
 
 }  // namespace fhd
