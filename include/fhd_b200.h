@@ -148,13 +148,15 @@ int  fhd_ctx_create(int dim, const int n_cells[3], const double dx[3],
  * (probin_common max_grid_size, bc_lo, bc_hi; main_driver.f90:392-393).
  * bc codes (bc.f90:24-44): FHD_BC_PERIODIC (-1), FHD_BC_NO_SLIP_WALL (100)
  * and FHD_BC_SLIP_WALL (200); a direction is periodic on both sides or on
- * neither.  Walls are homogeneous (the wall velocity is zero) and apply the
- * ghost rules of multifab_physbc_domainvel / multifab_physbc_macvel
- * (multifab_physbc_stag.f90:91-1116) throughout the Stokes solve; they are
+ * neither.  The Stokes solve sees homogeneous walls (zero wall velocity)
+ * through the ghost rules of multifab_physbc_domainvel /
+ * multifab_physbc_macvel (multifab_physbc_stag.f90:91-1116); moving no-slip
+ * walls enter the timesteps only (fhd_ctx_set_wall_speed).  Walls are
  * built for visc_type 1 or 2, precon_type 1 without the BFBt Schur complement,
- * the colour smoother, gmres_spatial_order 2 and one box; the device flux
- * and timestep entries carry the wall rules of their parts, the host-fab
- * flux entries refuse a context with walls.  In a wall
+ * the colour smoother, gmres_spatial_order 2 and one box; the device and
+ * host-fab flux entries and the timesteps carry the wall rules of their
+ * parts.  Reservoir codes 101 and 201 are walls here
+ * (FHD_BC_NO_SLIP_RESERVOIR).  In a wall
  * direction a face array keeps n faces: face 0 is the low wall face (held at
  * zero) and the high wall face is not stored.  Reservoirs and other codes
  * return FHD_ERR_UNSUPPORTED.
