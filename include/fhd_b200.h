@@ -152,7 +152,7 @@ int  fhd_ctx_create(int dim, const int n_cells[3], const double dx[3],
  * through the ghost rules of multifab_physbc_domainvel /
  * multifab_physbc_macvel (multifab_physbc_stag.f90:91-1116); moving no-slip
  * walls enter the timesteps only (fhd_ctx_set_wall_speed).  Walls are
- * built for visc_type 1 or 2, precon_type 1 without the BFBt Schur complement,
+ * built for visc_type 1, 2 or 3, precon_type 1 without the BFBt Schur complement,
  * the colour smoother, gmres_spatial_order 2 and one box; the device and
  * host-fab flux entries and the timesteps carry the wall rules of their
  * parts.  Reservoir codes 101 and 201 are walls here
@@ -365,7 +365,7 @@ int fhd_dev_stochastic_m_fluxdiv(fhd_ctx* ctx, const fhd_stoch_params* sp,
  * step's random fields as for fhd_dev_stochastic_m_fluxdiv with n_rngs = 1;
  * predictor and corrector use the same fields, as the reference does.
  * stats (nullable) receives the two solves' diagnostics.
- * Walls (fhd_ctx_create_bc codes 100, 200, visc_type 1 or 2): as for
+ * Walls (fhd_ctx_create_bc codes 100, 200, visc_type 1, 2 or 3): as for
  * fhd_dev_advance_overdamped, and the momentum advection's update is zero
  * on a wall face (mk_advective_m_fluxdiv.f90:80-85). */
 int fhd_dev_advance_inertial(fhd_ctx* ctx, const fhd_stoch_params* sp,
@@ -471,7 +471,7 @@ int fhd_dev_advance_inertial_multispecies(fhd_ctx* ctx, const fhd_stoch_params* 
  * (W_mass[(r*dim+d)*nspecies+i]; NULL without a mixture).  The predictor
  * weighs the stages (1, 0) over dt/2, the corrector (1/sqrt2, 1/sqrt2)
  * over dt.  stats (nullable) receives the two solves' diagnostics.
- * Walls (fhd_ctx_create_bc codes 100, 200, visc_type 1 or 2): the Stokes solve,
+ * Walls (fhd_ctx_create_bc codes 100, 200, visc_type 1, 2 or 3): the Stokes solve,
  * the stochastic and mass fluxes carry their wall rules (W_ed, eta_ed and
  * temperature_ed then have the high wall's edge planes, as for
  * fhd_dev_stochastic_m_fluxdiv), the pressure gradient is zero on a wall

@@ -2241,9 +2241,9 @@ int fhd_ctx_create_bc(int dim, const int n_cells[3], const int max_grid_size[3],
         else fhd_gmres_params_default(&p);
         bool boxes = false;
         for (int d = 0; d < dim; d++) boxes = boxes || max_grid_size[d] < n_cells[d];
-        if ((visc_type != 1 && visc_type != 2) || p.precon_type != 1 || p.visc_schur_approx != 0 || p.stag_mg_smoother == 0 ||
+        if (visc_type < 1 || p.precon_type != 1 || p.visc_schur_approx != 0 || p.stag_mg_smoother == 0 ||
             p.gmres_spatial_order != 2 || boxes) {
-            set_last_error("fhd_ctx_create_bc: walls are built for visc_type 1 or 2, precon_type 1 without the BFBt "
+            set_last_error("fhd_ctx_create_bc: walls are built for visc_type 1, 2 or 3, precon_type 1 without the BFBt "
                            "Schur complement, the colour smoother, second order and one box");
             return FHD_ERR_UNSUPPORTED;
         }

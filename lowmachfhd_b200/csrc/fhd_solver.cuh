@@ -105,7 +105,7 @@ inline void with_dim(int dim, F&& f) {
     else f(std::integral_constant<int, 3>());
 }
 
-// (dim, visc_type 1 or 2) for the wall kernels
+// (dim, visc_type 1, 2 or 3) for the wall kernels
 template <class F>
 inline void with_dim_wall_visc(int dim, int visc, F&& f) {
     with_dim(dim, [&](auto D) { with_wall_visc(visc, [&](auto V) { f(D, V); }); });

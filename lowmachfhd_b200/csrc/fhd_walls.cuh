@@ -1,5 +1,5 @@
 // fhd_walls.cuh -- homogeneous domain walls (zero wall velocity) for the
-// staggered Stokes solve with visc_type 1 or 2 (constant coefficients): no-slip
+// staggered Stokes solve with visc_type 1, 2 or 3 (constant coefficients): no-slip
 // and slip walls in any direction, the other directions periodic.
 //
 // The reference imposes walls through ghost cells, refilled after every
@@ -57,15 +57,15 @@ __device__ __forceinline__ T wall_vel(const Grid& g, const Walls& W, const T* u,
 }
 
 // (theta alpha - L) phi of component C at face (i, j, k), constant
-// coefficients, visc_type 1 or 2: the expression of stag_lface_acc with every
-// neighbour under the wall rules (visc_type 2 also reads the other
+// coefficients, visc_type 1, 2 or 3: the expression of stag_lface_acc with every
+// neighbour under the wall rules (visc_type 2 and 3 also read the other
 // components around the face: their values on and behind a wall come from
 // wall_vel as well, as the reference's ghost cells give them to the uniform
 // stencil of stag_applyop_level)
 template <typename T, int DIM, int VISC, int C>
 __device__ __forceinline__ T stag_lface_w(const Grid& g, const Walls& W, const StagOp<T>& A, const T* const* phi,
                                           int i, int j, int k, T& dg) {
-    static_assert(VISC == 1 || VISC == 2, "walls: visc_type 1 or 2");
+    static_assert(VISC >= 1 && VISC <= 3, "walls: visc_type 1, 2 or 3");
     CellF P;
     P.set(g, i, j, k);
     const T* pc = phi[C];
@@ -215,10 +215,11 @@ static __global__ void __launch_bounds__(256) k_stokes_apply_w(Grid g, Walls W, 
     out.c[DIM][f] = mode ? ld(rhs.c[DIM], f) - bp : bp;
 }
 
-// host dispatch of the wall kernels on the context's visc_type (1 or 2)
+// host dispatch of the wall kernels on the context's visc_type (1, 2 or 3)
 template <class F>
 inline void with_wall_visc(int visc, F&& f) {
     if (visc == 2) f(std::integral_constant<int, 2>());
+    else if (visc == 3) f(std::integral_constant<int, 3>());
     else f(std::integral_constant<int, 1>());
 }
 

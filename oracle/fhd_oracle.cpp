@@ -266,7 +266,7 @@ inline double lface(const Geo& g, int visc, const Vec* alpha, const Vec& beta,
     // (stag_applyop.f90:654-656 'b = beta(xlo(1),xlo(2),xlo(3))')
     const double b = beta[0], cg = gamma[0];
     if (g.any_wall()) {
-        // walls (visc_type 1 or 2): every neighbour through the ghost rules,
+        // walls (visc_type 1, 2, 3): every neighbour through the ghost rules,
         // the uniform stencil of stag_applyop_level on ghost cells filled by
         // multifab_physbc_macvel / _domainvel
         const double own = vel(g, phi[c], c, i + ec[0], j + ec[1], k + ec[2]) +
@@ -278,7 +278,7 @@ inline double lface(const Geo& g, int visc, const Vec* alpha, const Vec& beta,
             ed[d] = 1;
             oth += vel(g, phi[c], c, i + ed[0], j + ed[1], k + ed[2]) +
                    vel(g, phi[c], c, i - ed[0], j - ed[1], k - ed[2]);
-            if (visc == 2)
+            if (visc != 1)
                 cross += vel(g, phi[d], d, i + ed[0], j + ed[1], k + ed[2]) - vel(g, phi[d], d, i, j, k) -
                          vel(g, phi[d], d, i - ec[0] + ed[0], j - ec[1] + ed[1], k - ec[2] + ed[2]) +
                          vel(g, phi[d], d, i - ec[0], j - ec[1], k - ec[2]);
@@ -287,6 +287,11 @@ inline double lface(const Geo& g, int visc, const Vec* alpha, const Vec& beta,
             const double diag = a + (2.0 * dim + 2.0) * b * q;
             if (diag_out) *diag_out = diag;
             return ph * diag - (2.0 * own + oth + cross) * b * q;
+        }
+        if (visc == 3) {
+            const double diag = a + ((8.0 / 3.0 + 2.0 * (dim - 1)) * b + 2.0 * cg) * q;
+            if (diag_out) *diag_out = diag;
+            return ph * diag - (own * ((4.0 / 3.0) * b + cg) + oth * b + cross * ((1.0 / 3.0) * b + cg)) * q;
         }
         const double diag = a + (2.0 * dim) * b * q;
         if (diag_out) *diag_out = diag;
@@ -584,7 +589,7 @@ int stag_mg(const Geo& g0, int visc, const fhd_gmres_params* p, const double* co
             const double* beta, const double* const beta_ed[], const double* gamma, double theta,
             double* const phi[], const double* const rhs[], double* hist = nullptr) {
     const int dim = g0.dim;
-    if (g0.any_wall() && visc != 1 && visc != 2) return FHD_ERR_UNSUPPORTED;  // walls: visc_type 1 or 2
+    if (g0.any_wall() && visc < 1) return FHD_ERR_UNSUPPORTED;  // walls: visc_type 1, 2 or 3
     const int nl_domain = nlevs_mg(g0, p->stag_mg_minwidth);
     int nl_box;
     bool fancy;
@@ -949,8 +954,8 @@ int apply_matrix_impl(const Geo& g, int visc, double* const b_u[], double* b_p, 
     const int dim = g.dim;
     // stag_applyop_4o supports visc_type 1 only (stag_applyop.f90:1355, 1506)
     if (order != 2 && (order != 4 || visc != 1)) return -5;
-    // walls: visc_type 1 or 2, second order
-    if (g.any_wall() && ((visc != 1 && visc != 2) || order != 2)) return -5;
+    // walls: visc_type 1, 2 or 3, second order
+    if (g.any_wall() && (visc < 1 || order != 2)) return -5;
     Vec alpha[3], bed[3];
     Vec vb(beta, beta + g.nc), vg(gamma, gamma + g.nc);
     for (int c = 0; c < dim; c++) {

@@ -136,7 +136,7 @@ def test_mixed_precision_walls(cuda):
     assert P.rel_inf([host(x_p)], [ref_p]) < 1e-8
 
 
-@pytest.mark.parametrize("kw", [dict(visc=-1), dict(visc=3), dict(precon_type=2), dict(stag_mg_smoother=0),
+@pytest.mark.parametrize("kw", [dict(visc=-1), dict(visc=-2), dict(precon_type=2), dict(stag_mg_smoother=0),
                                 dict(gmres_spatial_order=4), dict(code=102), dict(code=203)])
 def test_unsupported_wall_options(cuda, kw):
     visc = kw.pop("visc", 1)

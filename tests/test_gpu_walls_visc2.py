@@ -1,4 +1,4 @@
-"""Walls with visc_type 2 (constant coefficients) on the GPU against the
+"""Walls with visc_type 2 and 3 (constant coefficients) on the GPU against the
 oracle: apply_matrix, one V-cycle of the staggered multigrid, GMRES (FP64,
 same iteration count; mixed precision to the FP64 solution) and the
 overdamped and inertial steps.  The wall stencil is the uniform one of
@@ -24,18 +24,19 @@ def periodic_afterwards():
     O.set_walls()
 
 
-def solver(dim, n, bc_lo, bc_hi, precision="fp64", **params):
-    return L.StokesSolver(dim, n, 1.0, 2, params=L.default_params(**params), precision=precision, bc_lo=bc_lo,
+def solver(dim, n, bc_lo, bc_hi, precision="fp64", visc=2, **params):
+    return L.StokesSolver(dim, n, 1.0, visc, params=L.default_params(**params), precision=precision, bc_lo=bc_lo,
                           bc_hi=bc_hi)
 
 
 @pytest.mark.parametrize("dim,n,bc_lo,bc_hi", CASES)
-def test_apply_matrix_walls_visc2(cuda, dim, n, bc_lo, bc_hi):
+@pytest.mark.parametrize("visc", [2, 3])
+def test_apply_matrix_walls_visc2(cuda, dim, n, bc_lo, bc_hi, visc):
     O.set_walls(bc_lo, bc_hi)
-    pb = P.problem(dim, n, 2, dx=1.0, seed=41)
+    pb = P.problem(dim, n, visc, dx=1.0, seed=41)
     u, p = wall_rhs(dim, n, bc_lo, 42, 1.0)
     ref_u, ref_p = O.apply_matrix(pb, 2.0, u, p)
-    with solver(dim, n, bc_lo, bc_hi) as s:
+    with solver(dim, n, bc_lo, bc_hi, visc=visc) as s:
         b_u, b_p = zeros(pb.nc, dim, cuda), zeros(pb.nc, 1, cuda)[0]
         s.apply_matrix(b_u, b_p, dev(u, cuda), dev(p, cuda), dev(pb.alpha_fc, cuda), dev(pb.beta, cuda),
                        dev(pb.beta_ed, cuda), dev(pb.gamma, cuda), 2.0)
@@ -58,15 +59,15 @@ def test_stag_mg_one_vcycle_walls_visc2(cuda, dim, n, bc_lo, bc_hi):
 
 
 @pytest.mark.parametrize("dim,n,bc_lo,bc_hi", CASES)
-@pytest.mark.parametrize("theta", [0.0, 2.0])
-def test_gmres_walls_visc2(cuda, dim, n, bc_lo, bc_hi, theta):
+@pytest.mark.parametrize("theta,visc", [(0.0, 2), (2.0, 2), (2.0, 3)])
+def test_gmres_walls_visc2(cuda, dim, n, bc_lo, bc_hi, theta, visc):
     O.set_walls(bc_lo, bc_hi)
-    pb = P.problem(dim, n, 2, dx=1.0, seed=45)
+    pb = P.problem(dim, n, visc, dx=1.0, seed=45)
     b_u, b_p = wall_rhs(dim, n, bc_lo, 46, theta)
     rc, ref_u, ref_p, npr_ref, st_ref = O.gmres(pb, O.default_params(gmres_rel_tol=1e-9), theta, b_u, b_p)
     assert rc == 0
     for precision, tol in (("fp64", 1e-10), ("mixed", 1e-7)):
-        with solver(dim, n, bc_lo, bc_hi, precision=precision, gmres_rel_tol=1e-9) as s:
+        with solver(dim, n, bc_lo, bc_hi, precision=precision, visc=visc, gmres_rel_tol=1e-9) as s:
             x_u, x_p = zeros(pb.nc, dim, cuda), zeros(pb.nc, 1, cuda)[0]
             status, npr, st = s.gmres(dev(b_u, cuda), dev(b_p, cuda), x_u, x_p, dev(pb.alpha_fc, cuda),
                                       dev(pb.beta, cuda), dev(pb.beta_ed, cuda), dev(pb.gamma, cuda), theta)

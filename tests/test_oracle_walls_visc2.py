@@ -1,5 +1,6 @@
-"""Walls with visc_type 2 (constant coefficients, L = beta (lap u + grad div u))
-in the oracle: the uniform stencil of stag_applyop_level on the ghost cells
+"""Walls with visc_type 2 and 3 (constant coefficients; visc_type 2:
+L = beta (lap u + grad div u), visc_type 3: beta lap u + (beta / 3 + gamma)
+grad div u) in the oracle: the uniform stencil of stag_applyop_level on the ghost cells
 of multifab_physbc_stag.f90, whose cross terms read the other velocity
 components on and behind the walls.  Exact checks:
   * on a discretely divergence-free field the visc_type 2 operator equals the
@@ -59,7 +60,9 @@ def divergence(n, u, walls):
 
 @pytest.mark.parametrize("bc_lo,bc_hi", [([PE, NS, PE], [PE, NS, PE]), ([SL, NS, PE], [NS, SL, PE]),
                                          ([NS, PE, PE], [SL, PE, PE])])
-def test_visc2_equals_visc1_on_divergence_free_fields(bc_lo, bc_hi):
+@pytest.mark.parametrize("visc", [2, 3])
+def test_visc2_equals_visc1_on_divergence_free_fields(bc_lo, bc_hi, visc):
+    """visc_type 3 too: its extra part is (beta / 3 + gamma) grad div u"""
     n = [12, 10]
     walls = [bc_lo[0] != PE, bc_lo[1] != PE]
     O.set_walls(bc_lo, bc_hi)
@@ -67,7 +70,7 @@ def test_visc2_equals_visc1_on_divergence_free_fields(bc_lo, bc_hi):
     assert np.max(np.abs(divergence(n, u, walls))) < 1e-13
     p = np.zeros(120)
     pb1 = P.problem(2, n, 1, dx=0.5, seed=4)
-    pb2 = P.problem(2, n, 2, dx=0.5, seed=4)
+    pb2 = P.problem(2, n, visc, dx=0.5, seed=4)
     assert pb1.beta[0] == pb2.beta[0]
     a1, _ = O.apply_matrix(pb1, 1.0, u, p)
     a2, _ = O.apply_matrix(pb2, 1.0, u, p)
