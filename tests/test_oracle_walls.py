@@ -125,7 +125,7 @@ def test_poiseuille_converges_at_second_order():
     assert 3.5 < e2 / e3 < 4.5
 
 
-def test_walls_need_visc_type_one():
+def test_walls_refuse_variable_viscosity():
     O.set_walls([-1, O.NO_SLIP_WALL, -1], [-1, O.NO_SLIP_WALL, -1])
     pb = P.problem(2, [8, 8], -1, dx=1.0, seed=6)
     u, p = P.random_stokes(2, [8, 8], seed=7)
